@@ -1,0 +1,247 @@
+/*
+ * paracfd_b200.h -- C ABI of the B200-native ParaCFD per-timestep solver path.
+ *
+ * The boundary sits exactly where the reference hands host topology to its device
+ * classes: a caller builds (or imports) the static 2:1 brick hierarchy and the
+ * composite cut-cell pressure system once, passes them here as flat arrays, and then
+ * drives projection / cell-momentum / surface-load work that stays resident in HBM.
+ *
+ * Reference interfaces replaced (paths inside the ParaCFD project):
+ *   pcfd_system_create            DeviceAmrFields + DeviceCompositeAmrProjection +
+ *                                 DeviceCompositeCellMomentumTransport constructors
+ *                                 (src/core/fluid/external_aero_core.cpp:220-228; the topology
+ *                                 consumed is CompositeAmrPressureSystem, amr_pressure.h:193-260,
+ *                                 and AmrHierarchy, amr_grid.h:86-118)
+ *   pcfd_pressure_apply           DeviceCompositeAmrPressureOperator::apply / apply_orthogonal
+ *                                 (src/core/fluid/amr_pressure.h:299-300)
+ *   pcfd_pressure_diagonal        CompositeAmrPressureSystem::diagonal_cpu (amr_pressure.h:259)
+ *   pcfd_pressure_precondition    DeviceCompositeAmrPressureSolver::apply_preconditioner
+ *                                 (amr_pressure.h:405)
+ *   pcfd_pressure_solve           DeviceCompositeAmrPressureSolver::solve (amr_pressure.h:363)
+ *   pcfd_projection_divergence    DeviceCompositeAmrProjection::compute_divergence (amr_pressure.h:475)
+ *   pcfd_projection_rhs           DeviceCompositeAmrProjection::build_projection_rhs (amr_pressure.h:476)
+ *   pcfd_projection_correct       DeviceCompositeAmrProjection::correct_fluxes (amr_pressure.h:477)
+ *   pcfd_projection_project       DeviceCompositeAmrProjection::project (amr_pressure.h:478)
+ *   pcfd_set/get_* state          DeviceAmrFields::upload/download, upload/download_special_fluxes,
+ *                                 upload_pressure, DeviceCompositeCellMomentumTransport::
+ *                                 upload_state/download_state (amr_fields.h:57-58,
+ *                                 amr_pressure.h:462-483, amr_advection.h:286-287)
+ *
+ * Conventions: every entry point returns a pcfd_status; on failure
+ * pcfd_last_error_message() (thread-local) says why.  No exception crosses the ABI.
+ * "_host" entry points take caller-owned host buffers and copy in/out (they synchronise);
+ * "_device" entry points take device pointers on the system's stream.  Array sizes are
+ * stated in the comments: S = storage_size (pressure DOF slots, covered bricks included),
+ * B = total brick slots over all levels (S = B * bs^3), F = B * (bs+1) * bs^2 faces per
+ * component.  A system object is used by one host thread at a time.
+ */
+#ifndef PARACFD_B200_H
+#define PARACFD_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum pcfd_status {
+    PCFD_OK = 0,
+    PCFD_INVALID_ARG = 1,
+    PCFD_CUDA_ERROR = 2,
+    PCFD_NOT_CONVERGED = 3,
+    PCFD_TOPOLOGY_UNRESOLVED = 4,
+    PCFD_OUT_OF_MEMORY = 5,
+    PCFD_TIMEOUT = 6,
+    PCFD_INTERNAL = 7
+} pcfd_status;
+
+/* Brick flags, bit-identical to BrickFlags (amr_grid.h:27-32). */
+enum {
+    PCFD_BRICK_XMIN = 1u << 0, PCFD_BRICK_XMAX = 1u << 1, PCFD_BRICK_YMIN = 1u << 2,
+    PCFD_BRICK_YMAX = 1u << 3, PCFD_BRICK_ZMIN = 1u << 4, PCFD_BRICK_ZMAX = 1u << 5,
+    PCFD_BRICK_EMBEDDED_BOUNDARY = 1u << 6, PCFD_BRICK_COVERED = 1u << 7
+};
+
+/* One AMR level (AmrLevel + BrickMetadata, amr_grid.h:34-64). */
+typedef struct pcfd_level {
+    double h;                    /* cell size of this level */
+    int32_t brick_count;         /* bricks stored on this level, covered ones included */
+    int32_t level_offset;        /* first pressure DOF of this level (= brick slot * bs^3) */
+    const int32_t* coord;        /* [brick_count][3] integer brick coordinates */
+    const double* origin;        /* [brick_count][3] world origin of the brick */
+    const int32_t* neighbors;    /* [brick_count][6] same-level neighbour (-x,+x,-y,+y,-z,+z), -1 none */
+    const uint32_t* flags;       /* [brick_count] PCFD_BRICK_* */
+    const int32_t* children;     /* [brick_count][8] fine children or -1; may be NULL on the finest level */
+} pcfd_level;
+
+/* Compact pressure connections: CoarseFinePressureConnection (amr_pressure.h:101-121), SoA. */
+typedef struct pcfd_connections {
+    int32_t count;
+    const int32_t* coarse_dof;
+    const int32_t* fine_dof;
+    const double* open_area;
+    const double* centre_distance;
+    const double* normal_distance;
+    const int8_t* axis;
+    const int8_t* direction;            /* +1: coarse_dof is the lower-axis side */
+    const double* face_centroid;        /* [count][3] */
+    const double* orthogonal_gradient_factor;
+    const int32_t* lower_gradient_node;
+    const int32_t* upper_gradient_node;
+    const double* nonorthogonal_correction; /* [count][3] */
+    const double* upper_gradient_weight;
+} pcfd_connections;
+
+/* RegularPressureCorrection (amr_pressure.h:141-155), SoA. */
+typedef struct pcfd_regular_corrections {
+    int32_t count;
+    const int32_t* lower_dof;
+    const int32_t* upper_dof;
+    const int32_t* level;
+    const int32_t* brick;
+    const int32_t* ijk;                 /* [count][3] positive-face index in the owning brick */
+    const int8_t* axis;
+    const double* open_area;
+    const double* two_point_delta;
+    const int32_t* lower_gradient_node;
+    const int32_t* upper_gradient_node;
+    const double* nonorthogonal_correction; /* [count][3] */
+    const double* upper_gradient_weight;
+} pcfd_regular_corrections;
+
+/* CompositeSurfacePressurePatch (amr_pressure.h:156-165), SoA. */
+typedef struct pcfd_surface_patches {
+    int32_t count;
+    const double* area;
+    const double* centroid;             /* [count][3] */
+    const double* normal;               /* [count][3], minus -> plus */
+    const int32_t* plus_dof;
+    const int32_t* minus_dof;
+} pcfd_surface_patches;
+
+/* CompositeBoundaryPressureFace (amr_pressure.h:166-170), SoA. */
+typedef struct pcfd_boundary_faces {
+    int32_t count;
+    const int32_t* dof;
+    const double* outward_area;         /* [count][3] */
+    const double* centroid;             /* [count][3] */
+} pcfd_boundary_faces;
+
+/* Complete static topology: AmrHierarchy + CompositeAmrPressureSystem. */
+typedef struct pcfd_topology {
+    int32_t brick_size;
+    int32_t level_count;
+    const pcfd_level* levels;
+    double domain_lo[3], domain_hi[3];
+    int32_t storage_size;
+    int32_t pressure_outlet_xmax;
+    const uint8_t* active;                  /* [S] */
+    const uint8_t* freestream_connected;    /* [S] may be NULL (treated as active) */
+    const uint8_t* cut_face_mask;           /* [S] +X/+Y/+Z suppression bits */
+    const double* volume;                   /* [S] */
+    const double* centroid;                 /* [S][3] */
+    const int32_t* preconditioner_aggregate;/* [S] level-0 aggregate DOF or -1 */
+    pcfd_connections coarse_fine;
+    pcfd_connections embedded;
+    pcfd_regular_corrections regular;
+    int32_t gradient_node_count;            /* compact WLS pressure-gradient stencil */
+    const int32_t* gradient_dof;            /* [nodes] */
+    const int32_t* gradient_offset;         /* [nodes+1] */
+    const int32_t* gradient_neighbour;      /* [nnz] */
+    const double* gradient_weight;          /* [nnz][3] */
+    int32_t gauge_count;
+    const int32_t* gauge_dof;
+    const double* gauge_coefficient;
+    pcfd_surface_patches patches;
+    pcfd_boundary_faces boundary_faces;
+    int32_t retained_count;                 /* face_state_retained_dofs */
+    const int32_t* retained_dofs;
+} pcfd_topology;
+
+/* Precision of the multigrid preconditioner inside the FP64 outer Krylov solve. */
+typedef enum pcfd_mg_precision {
+    PCFD_MG_FP64 = 0,   /* reference-equivalent arithmetic (parity mode) */
+    PCFD_MG_FP32 = 1    /* FP32 smoother/coarse levels, FP64 outer recurrence */
+} pcfd_mg_precision;
+
+typedef struct pcfd_options {
+    int32_t mg_precision;            /* pcfd_mg_precision */
+    int32_t device;                  /* CUDA device ordinal */
+    void* stream;                    /* cudaStream_t or NULL for a library-owned stream */
+} pcfd_options;
+
+/* AmrGpuSolveResult (amr_pressure.h:337-351), trimmed to what the solver reports. */
+typedef struct pcfd_solve_result {
+    int32_t iterations;
+    double relative_residual;
+    int32_t converged;
+    int32_t preconditioner_applications;
+    int32_t recycle_rejections;
+} pcfd_solve_result;
+
+typedef struct pcfd_system pcfd_system;
+
+const char* pcfd_last_error_message(void);
+const char* pcfd_version(void);
+
+/* Topology upload + device allocation (all static arrays copied; caller may free inputs). */
+pcfd_status pcfd_system_create(const pcfd_topology* topology, const pcfd_options* options,
+                               pcfd_system** out);
+void pcfd_system_destroy(pcfd_system* system);
+/* Sizes: storage_size, brick slots, faces per component, coarse/fine and EB connection counts. */
+pcfd_status pcfd_system_sizes(const pcfd_system* system, int64_t* storage_size, int64_t* bricks,
+                              int64_t* faces_per_component, int64_t* coarse_fine_count,
+                              int64_t* embedded_count);
+pcfd_status pcfd_system_synchronize(pcfd_system* system);
+
+/* ---- pressure operator (FP64) -------------------------------------------------------- */
+/* out = A p (orthogonal != 0: two-point part only, as apply_orthogonal). p, out: [S]. */
+pcfd_status pcfd_pressure_apply_host(pcfd_system* system, const double* p, double* out,
+                                     int32_t orthogonal);
+pcfd_status pcfd_pressure_apply_device(pcfd_system* system, const double* d_p, double* d_out,
+                                       int32_t orthogonal);
+/* Jacobi diagonal used by the smoother (diagonal_cpu semantics). diag: [S]. */
+pcfd_status pcfd_pressure_diagonal_host(pcfd_system* system, double* diag);
+/* z = M^-1 r with the reference-structured V-cycle (FP64 or FP32 per options). [S]. */
+pcfd_status pcfd_pressure_precondition_host(pcfd_system* system, const double* r, double* z);
+/* Solve A x = b. warm_start != 0 keeps x as the initial guess. x, b: [S]. */
+pcfd_status pcfd_pressure_solve_host(pcfd_system* system, double* x, const double* b,
+                                     double tolerance, int32_t max_iterations, int32_t warm_start,
+                                     pcfd_solve_result* result);
+
+/* ---- resident flow state (FP32 fields, FP64 pressure) --------------------------------- */
+/* Faces in brick-slot order, per brick (bs+1)*bs*bs for u ((k*bs+j)*(bs+1)+i), bs*(bs+1)*bs
+ * for v ((k*(bs+1)+j)*bs+i), bs*bs*(bs+1) for w ((k*bs+j)*bs+i).  u, v, w: [F]. */
+pcfd_status pcfd_set_faces_host(pcfd_system* system, const float* u, const float* v, const float* w);
+pcfd_status pcfd_get_faces_host(pcfd_system* system, float* u, float* v, float* w);
+/* Compact special velocities: coarse/fine tiles [count_cf], EB apertures [count_eb]. */
+pcfd_status pcfd_set_special_host(pcfd_system* system, const float* coarse_fine, const float* embedded);
+pcfd_status pcfd_get_special_host(pcfd_system* system, float* coarse_fine, float* embedded);
+/* FP64 solve pressure [S]; the FP32 shadow is refreshed from it. */
+pcfd_status pcfd_set_pressure_host(pcfd_system* system, const double* p);
+pcfd_status pcfd_get_pressure_host(pcfd_system* system, double* p);
+pcfd_status pcfd_get_pressure_shadow_host(pcfd_system* system, float* p32);
+
+/* ---- projection ------------------------------------------------------------------------- */
+/* divergence [S] (FP32) = integrated aperture flux / volume. */
+pcfd_status pcfd_projection_divergence_host(pcfd_system* system, float* divergence);
+/* rhs [S] (FP64) = -(rho/dt) * integrated aperture flux. */
+pcfd_status pcfd_projection_rhs_host(pcfd_system* system, double rho, double dt, double* rhs);
+/* Gradient correction of all face kinds from the resident FP64 pressure. */
+pcfd_status pcfd_projection_correct(pcfd_system* system, double rho, double dt);
+/* build rhs -> solve -> (if converged) shadow, correct, divergence. */
+pcfd_status pcfd_projection_project(pcfd_system* system, double rho, double dt, double tolerance,
+                                    int32_t max_iterations, int32_t warm_start,
+                                    pcfd_solve_result* result);
+
+/* ---- instrumentation ---------------------------------------------------------------------- */
+/* Average device time of one launch sequence of `which` (0 full apply, 1 orthogonal apply,
+ * 2 preconditioner, 3 divergence, 4 flux correction, 5 FP64 dot), measured with CUDA events on
+ * the system stream over `iterations` back-to-back repetitions on resident scratch vectors. */
+pcfd_status pcfd_time_kernel(pcfd_system* system, int32_t which, int32_t iterations, double* ms_per_launch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,736 @@
+// ref_shim.cpp -- exposes the reference ParaCFD preprocessing and host parity operators
+// through flat C entry points.  Test infrastructure only (see ref_shim.h).  Everything that
+// computes here is the reference's own code (AmrHierarchy::build_static,
+// build_amr_embedded_boundary_atlas, build_composite_amr_pressure_system, apply_cpu,
+// diagonal_cpu, composite_amr_*_cpu); this file only builds analytic fixtures, in the
+// pattern of the reference's tools/physics_contract_probe.cpp:19-67, and converts layouts.
+#include "ref_shim.h"
+
+#include "core/fluid/amr_eb.h"
+#include "core/fluid/amr_pressure.h"
+#include "core/geometry/mesh_clip.h"
+#include "core/geometry/model_placement.h"
+#include "core/paraglider_config.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+using namespace paracfd::core;
+
+namespace
+{
+    thread_local std::string g_error;
+
+    // ---- analytic fixtures ------------------------------------------------------------
+    // Axis-aligned box solid of half extents `half` under a rigid placement (the
+    // reference's manufactured-contract fixture, tools/physics_contract_probe.cpp:39-67).
+    TriMesh box_mesh(Vec3d half)
+    {
+        TriMesh mesh;
+        for (int vertex = 0; vertex < 8; ++vertex)
+            for (int axis = 0; axis < 3; ++axis)
+            {
+                const double value = (vertex & (1 << axis)) ? half[axis] : -half[axis];
+                mesh.positions_fp64.push_back(value);
+                mesh.positions.push_back(float(value));
+                mesh.normals.push_back(0);
+            }
+        const int faces[6][4] = {{0, 4, 6, 2}, {1, 3, 7, 5}, {0, 1, 5, 4}, {2, 6, 7, 3}, {0, 2, 3, 1}, {4, 5, 7, 6}};
+        for (int face = 0; face < 6; ++face)
+            for (int t = 0; t < 2; ++t)
+            {
+                for (int corner : {0, t + 1, t + 2}) mesh.indices.push_back(faces[face][corner]);
+                mesh.source_face_ids.push_back(face);
+            }
+        for (int axis = 0; axis < 3; ++axis)
+        {
+            mesh.bbox_min[axis] = float(-half[axis]);
+            mesh.bbox_max[axis] = float(half[axis]);
+        }
+        return mesh;
+    }
+
+    class PlacedBox final : public ClosedSolidGeometry
+    {
+        Vec3d half_;
+        ModelPlacement inverse_;
+        Aabb3d bounds_;
+
+    public:
+        PlacedBox(Vec3d half, const ModelPlacement& placement) : half_(half)
+        {
+            if (!inverse_placement(placement, inverse_)) throw std::runtime_error("invalid box placement");
+            for (int vertex = 0; vertex < 8; ++vertex)
+            {
+                Vec3d p;
+                placement.apply((vertex & 1) ? half.x : -half.x, (vertex & 2) ? half.y : -half.y,
+                                (vertex & 4) ? half.z : -half.z, p.x, p.y, p.z);
+                bounds_.expand(p);
+            }
+        }
+        const Aabb3d& bounds() const override { return bounds_; }
+        void classify_points(const Vec3d* points, std::size_t count, double tolerance,
+                             ClosedSolidPointLocation* locations) const override
+        {
+            for (std::size_t q = 0; q < count; ++q)
+            {
+                Vec3d p;
+                inverse_.apply(points[q].x, points[q].y, points[q].z, p.x, p.y, p.z);
+                double distance = -1e30;
+                for (int axis = 0; axis < 3; ++axis) distance = std::max(distance, std::abs(p[axis]) - half_[axis]);
+                locations[q] = distance > tolerance ? ClosedSolidPointLocation::outside
+                             : (distance < -tolerance ? ClosedSolidPointLocation::inside
+                                                       : ClosedSolidPointLocation::boundary);
+            }
+        }
+    };
+
+    // NACA 4-digit section (published thickness/camber formulas; the closed trailing edge
+    // uses -0.1036 for the x^4 coefficient).  Returns a closed polygon in (x, z), counter-
+    // clockwise, starting at the trailing edge along the upper surface.
+    std::vector<std::array<double, 2>> naca_polygon(int digits, int points_per_side, double chord)
+    {
+        const double m = (digits / 1000) / 100.0, p = ((digits / 100) % 10) / 10.0, t = (digits % 100) / 100.0;
+        auto evaluate = [&](double x, bool upper) {
+            const double yt = 5 * t * (0.2969 * std::sqrt(x) - 0.1260 * x - 0.3516 * x * x + 0.2843 * x * x * x - 0.1036 * x * x * x * x);
+            double yc = 0, slope = 0;
+            if (m > 0 && p > 0)
+            {
+                if (x < p) { yc = m / (p * p) * (2 * p * x - x * x); slope = 2 * m / (p * p) * (p - x); }
+                else { yc = m / ((1 - p) * (1 - p)) * ((1 - 2 * p) + 2 * p * x - x * x); slope = 2 * m / ((1 - p) * (1 - p)) * (p - x); }
+            }
+            const double theta = std::atan(slope);
+            if (upper) return std::array<double, 2>{(x - yt * std::sin(theta)) * chord, (yc + yt * std::cos(theta)) * chord};
+            return std::array<double, 2>{(x + yt * std::sin(theta)) * chord, (yc - yt * std::cos(theta)) * chord};
+        };
+        std::vector<std::array<double, 2>> polygon;
+        const double pi = std::acos(-1.0);
+        for (int q = 0; q < points_per_side; ++q)   // upper: TE -> LE
+        {
+            const double beta = pi * (1.0 - double(q) / points_per_side);
+            polygon.push_back(evaluate(0.5 * (1 - std::cos(beta)), true));
+        }
+        for (int q = 0; q < points_per_side; ++q)   // lower: LE -> TE (TE point shared once)
+        {
+            const double beta = pi * double(q) / points_per_side;
+            polygon.push_back(evaluate(0.5 * (1 - std::cos(beta)), false));
+        }
+        polygon[0] = {chord, 0.0};
+        return polygon;   // upper TE..LE then lower LE..(just before TE): counter-clockwise in (x,z)?
+    }
+
+    double polygon_signed_area(const std::vector<std::array<double, 2>>& poly)
+    {
+        double a = 0;
+        for (std::size_t q = 0; q < poly.size(); ++q)
+        {
+            const auto& p0 = poly[q];
+            const auto& p1 = poly[(q + 1) % poly.size()];
+            a += p0[0] * p1[1] - p1[0] * p0[1];
+        }
+        return 0.5 * a;
+    }
+
+    // Extruded section along +Y between y0 and y1, placed by `place` (section (x,z) -> world).
+    // Caps are emitted when `caps` is set.  The solid below classifies against the same polygon.
+    struct SectionPlacement
+    {
+        double cos_a = 1, sin_a = 0, pivot_x = 0, pivot_z = 0, tx = 0, tz = 0;
+        void to_world(double x, double z, double& wx, double& wz) const
+        {
+            const double dx = x - pivot_x, dz = z - pivot_z;
+            wx = pivot_x + tx + cos_a * dx + sin_a * dz;
+            wz = pivot_z + tz - sin_a * dx + cos_a * dz;
+        }
+        void to_section(double wx, double wz, double& x, double& z) const
+        {
+            const double dx = wx - pivot_x - tx, dz = wz - pivot_z - tz;
+            x = pivot_x + cos_a * dx - sin_a * dz;
+            z = pivot_z + sin_a * dx + cos_a * dz;
+        }
+    };
+
+    TriMesh extruded_mesh(const std::vector<std::array<double, 2>>& poly, const SectionPlacement& place,
+                          double y0, double y1, bool caps)
+    {
+        TriMesh mesh;
+        const int n = int(poly.size());
+        auto push = [&](double x, double y, double z) {
+            double wx, wz;
+            place.to_world(x, z, wx, wz);
+            mesh.positions_fp64.insert(mesh.positions_fp64.end(), {wx, y, wz});
+            mesh.positions.insert(mesh.positions.end(), {float(wx), float(y), float(wz)});
+            mesh.normals.insert(mesh.normals.end(), {0.f, 0.f, 0.f});
+        };
+        for (int q = 0; q < n; ++q) push(poly[q][0], y0, poly[q][1]);
+        for (int q = 0; q < n; ++q) push(poly[q][0], y1, poly[q][1]);
+        // Polygon is CCW in (x,z); with +Y out of the (z,x) plane the outward side normal
+        // of edge (a->b) for a solid to the left follows from the winding below.
+        for (int q = 0; q < n; ++q)
+        {
+            const uint32_t a0 = q, b0 = (q + 1) % n, a1 = n + q, b1 = n + (q + 1) % n;
+            mesh.indices.insert(mesh.indices.end(), {a0, a1, b1, a0, b1, b0});
+            mesh.source_face_ids.push_back(0);
+            mesh.source_face_ids.push_back(0);
+        }
+        if (caps)
+        {
+            // fan around vertex 0 (convex enough for a fan? not in general) -> use centre point
+            double cx = 0, cz = 0;
+            for (auto& p : poly) { cx += p[0]; cz += p[1]; }
+            cx /= n; cz /= n;
+            const uint32_t c0 = uint32_t(mesh.positions.size() / 3);
+            push(cx, y0, cz);
+            const uint32_t c1 = c0 + 1;
+            push(cx, y1, cz);
+            for (int q = 0; q < n; ++q)
+            {
+                const uint32_t a = q, b = (q + 1) % n;
+                mesh.indices.insert(mesh.indices.end(), {c0, b, a});
+                mesh.source_face_ids.push_back(1);
+                mesh.indices.insert(mesh.indices.end(), {c1, uint32_t(n + a), uint32_t(n + b)});
+                mesh.source_face_ids.push_back(2);
+            }
+        }
+        // Make the winding outward: compute signed volume and flip if negative.
+        double volume = 0;
+        for (std::size_t t = 0; t < mesh.indices.size() / 3; ++t)
+        {
+            const double* p0 = &mesh.positions_fp64[3 * mesh.indices[3 * t]];
+            const double* p1 = &mesh.positions_fp64[3 * mesh.indices[3 * t + 1]];
+            const double* p2 = &mesh.positions_fp64[3 * mesh.indices[3 * t + 2]];
+            volume += p0[0] * (p1[1] * p2[2] - p1[2] * p2[1]) - p0[1] * (p1[0] * p2[2] - p1[2] * p2[0]) +
+                      p0[2] * (p1[0] * p2[1] - p1[1] * p2[0]);
+        }
+        if (volume < 0)
+            for (std::size_t t = 0; t < mesh.indices.size() / 3; ++t) std::swap(mesh.indices[3 * t + 1], mesh.indices[3 * t + 2]);
+        float bmin[3] = {1e30f, 1e30f, 1e30f}, bmax[3] = {-1e30f, -1e30f, -1e30f};
+        for (std::size_t v = 0; v < mesh.positions.size() / 3; ++v)
+            for (int a = 0; a < 3; ++a)
+            {
+                bmin[a] = std::min(bmin[a], mesh.positions[3 * v + a]);
+                bmax[a] = std::max(bmax[a], mesh.positions[3 * v + a]);
+            }
+        for (int a = 0; a < 3; ++a) { mesh.bbox_min[a] = bmin[a]; mesh.bbox_max[a] = bmax[a]; }
+        return mesh;
+    }
+
+    class ExtrudedSection final : public ClosedSolidGeometry
+    {
+        std::vector<std::array<double, 2>> poly_;
+        SectionPlacement place_;
+        double y0_, y1_;
+        bool finite_;
+        Aabb3d bounds_;
+
+    public:
+        ExtrudedSection(std::vector<std::array<double, 2>> poly, SectionPlacement place, double y0, double y1, bool finite)
+            : poly_(std::move(poly)), place_(place), y0_(y0), y1_(y1), finite_(finite)
+        {
+            for (auto& p : poly_)
+            {
+                double wx, wz;
+                place_.to_world(p[0], p[1], wx, wz);
+                bounds_.expand(Vec3d{wx, y0_, wz});
+                bounds_.expand(Vec3d{wx, y1_, wz});
+            }
+        }
+        const Aabb3d& bounds() const override { return bounds_; }
+        void classify_points(const Vec3d* points, std::size_t count, double tolerance,
+                             ClosedSolidPointLocation* locations) const override
+        {
+            const int n = int(poly_.size());
+            for (std::size_t q = 0; q < count; ++q)
+            {
+                double x, z;
+                place_.to_section(points[q].x, points[q].z, x, z);
+                bool inside = false;
+                double d2 = 1e300;
+                for (int e = 0, f = n - 1; e < n; f = e++)
+                {
+                    const double xa = poly_[f][0], za = poly_[f][1], xb = poly_[e][0], zb = poly_[e][1];
+                    if (((zb > z) != (za > z)) && (x < (xa - xb) * (z - zb) / (za - zb) + xb)) inside = !inside;
+                    const double ex = xb - xa, ez = zb - za, len2 = ex * ex + ez * ez;
+                    double s = len2 > 0 ? ((x - xa) * ex + (z - za) * ez) / len2 : 0;
+                    s = std::clamp(s, 0.0, 1.0);
+                    const double dx = x - (xa + s * ex), dz = z - (za + s * ez);
+                    d2 = std::min(d2, dx * dx + dz * dz);
+                }
+                double signed_distance = inside ? -std::sqrt(d2) : std::sqrt(d2);
+                if (finite_)
+                {
+                    const double y = points[q].y;
+                    const double dy = std::max(y0_ - y, y - y1_);   // >0 outside the span
+                    if (signed_distance < 0) signed_distance = std::max(signed_distance, dy);
+                    else if (dy > 0) signed_distance = std::sqrt(signed_distance * signed_distance + dy * dy);
+                }
+                locations[q] = signed_distance > tolerance ? ClosedSolidPointLocation::outside
+                             : (signed_distance < -tolerance ? ClosedSolidPointLocation::inside
+                                                              : ClosedSolidPointLocation::boundary);
+            }
+        }
+    };
+
+    // ---- case object --------------------------------------------------------------------
+    struct RefCase
+    {
+        ParagliderConfig config;
+        TriMesh wing;
+        std::unique_ptr<TriangleBvh> bvh;
+        ClosedSolidGeometryPtr solid;
+        AmrHierarchy hierarchy;
+        AmrEmbeddedBoundaryAtlas atlas;
+        CompositeAmrPressureSystem system;
+        // exported flat arrays
+        std::vector<pcfd_level> levels;
+        std::vector<std::vector<int32_t>> coord, neighbors, children;
+        std::vector<std::vector<double>> origin;
+        std::vector<std::vector<uint32_t>> flags;
+        std::vector<double> centroid;
+        struct Conn
+        {
+            std::vector<int32_t> coarse, fine, lower_node, upper_node;
+            std::vector<double> area, centre, normal_distance, face_centroid, factor, correction, weight;
+            std::vector<int8_t> axis, direction;
+        } cf, eb;
+        std::vector<int32_t> rc_lower, rc_upper, rc_level, rc_brick, rc_ijk, rc_lower_node, rc_upper_node;
+        std::vector<int8_t> rc_axis;
+        std::vector<double> rc_area, rc_delta, rc_correction, rc_weight;
+        std::vector<double> gradient_weight;
+        std::vector<int32_t> gauge_dof;
+        std::vector<double> gauge_coefficient;
+        std::vector<double> patch_area, patch_centroid, patch_normal;
+        std::vector<int32_t> patch_plus, patch_minus;
+        std::vector<int32_t> bf_dof;
+        std::vector<double> bf_area, bf_centroid;
+        std::vector<int32_t> retained;
+    };
+
+    void export_connections(const std::vector<CoarseFinePressureConnection>& in, RefCase::Conn& out)
+    {
+        for (const auto& e : in)
+        {
+            out.coarse.push_back(e.coarse_dof);
+            out.fine.push_back(e.fine_dof);
+            out.area.push_back(e.open_area);
+            out.centre.push_back(e.centre_distance);
+            out.normal_distance.push_back(e.normal_distance);
+            out.axis.push_back(e.axis);
+            out.direction.push_back(e.direction);
+            for (int a = 0; a < 3; ++a) out.face_centroid.push_back(e.face_centroid[a]);
+            out.factor.push_back(e.orthogonal_gradient_factor);
+            out.lower_node.push_back(e.lower_gradient_node);
+            out.upper_node.push_back(e.upper_gradient_node);
+            for (int a = 0; a < 3; ++a) out.correction.push_back(e.nonorthogonal_correction[a]);
+            out.weight.push_back(e.upper_gradient_weight);
+        }
+    }
+    pcfd_connections view_connections(RefCase::Conn& c)
+    {
+        pcfd_connections v{};
+        v.count = int32_t(c.coarse.size());
+        v.coarse_dof = c.coarse.data(); v.fine_dof = c.fine.data(); v.open_area = c.area.data();
+        v.centre_distance = c.centre.data(); v.normal_distance = c.normal_distance.data();
+        v.axis = c.axis.data(); v.direction = c.direction.data(); v.face_centroid = c.face_centroid.data();
+        v.orthogonal_gradient_factor = c.factor.data(); v.lower_gradient_node = c.lower_node.data();
+        v.upper_gradient_node = c.upper_node.data(); v.nonorthogonal_correction = c.correction.data();
+        v.upper_gradient_weight = c.weight.data();
+        return v;
+    }
+
+    void export_case(RefCase& rc)
+    {
+        const auto& levels = rc.hierarchy.levels();
+        const int L = int(levels.size());
+        rc.levels.resize(L);
+        rc.coord.resize(L); rc.neighbors.resize(L); rc.children.resize(L); rc.origin.resize(L); rc.flags.resize(L);
+        for (int l = 0; l < L; ++l)
+        {
+            const AmrLevel& lev = levels[l];
+            for (const BrickMetadata& b : lev.bricks)
+            {
+                rc.coord[l].insert(rc.coord[l].end(), {b.coord.x, b.coord.y, b.coord.z});
+                rc.origin[l].insert(rc.origin[l].end(), {b.origin.x, b.origin.y, b.origin.z});
+                for (int f = 0; f < 6; ++f) rc.neighbors[l].push_back(b.same_level_neighbor[f]);
+                for (int c = 0; c < 8; ++c) rc.children[l].push_back(b.children[c]);
+                rc.flags[l].push_back(b.flags);
+            }
+            pcfd_level& v = rc.levels[l];
+            v.h = lev.h;
+            v.brick_count = int32_t(lev.bricks.size());
+            v.level_offset = rc.system.level_offset[l];
+            v.coord = rc.coord[l].data();
+            v.origin = rc.origin[l].data();
+            v.neighbors = rc.neighbors[l].data();
+            v.flags = rc.flags[l].data();
+            v.children = rc.children[l].data();
+        }
+        const auto& s = rc.system;
+        for (const Vec3d& c : s.centroid) rc.centroid.insert(rc.centroid.end(), {c.x, c.y, c.z});
+        export_connections(s.coarse_fine, rc.cf);
+        export_connections(s.embedded, rc.eb);
+        for (const auto& r : s.regular_pressure_corrections)
+        {
+            rc.rc_lower.push_back(r.lower_dof); rc.rc_upper.push_back(r.upper_dof);
+            rc.rc_level.push_back(r.level); rc.rc_brick.push_back(r.brick);
+            rc.rc_ijk.insert(rc.rc_ijk.end(), {r.i, r.j, r.k});
+            rc.rc_axis.push_back(r.axis); rc.rc_area.push_back(r.open_area); rc.rc_delta.push_back(r.two_point_delta);
+            rc.rc_lower_node.push_back(r.lower_gradient_node); rc.rc_upper_node.push_back(r.upper_gradient_node);
+            for (int a = 0; a < 3; ++a) rc.rc_correction.push_back(r.nonorthogonal_correction[a]);
+            rc.rc_weight.push_back(r.upper_gradient_weight);
+        }
+        for (const Vec3d& w : s.pressure_gradient_weight) rc.gradient_weight.insert(rc.gradient_weight.end(), {w.x, w.y, w.z});
+        for (const auto& g : s.gauges) { rc.gauge_dof.push_back(g.dof); rc.gauge_coefficient.push_back(g.coefficient); }
+        for (const auto& p : s.surface_patches)
+        {
+            rc.patch_area.push_back(p.area);
+            rc.patch_centroid.insert(rc.patch_centroid.end(), {p.centroid.x, p.centroid.y, p.centroid.z});
+            rc.patch_normal.insert(rc.patch_normal.end(), {p.normal.x, p.normal.y, p.normal.z});
+            rc.patch_plus.push_back(p.plus_dof); rc.patch_minus.push_back(p.minus_dof);
+        }
+        for (const auto& f : s.boundary_faces)
+        {
+            rc.bf_dof.push_back(f.dof);
+            rc.bf_area.insert(rc.bf_area.end(), {f.outward_area.x, f.outward_area.y, f.outward_area.z});
+            rc.bf_centroid.insert(rc.bf_centroid.end(), {f.centroid.x, f.centroid.y, f.centroid.z});
+        }
+        rc.retained.assign(s.face_state_retained_dofs.begin(), s.face_state_retained_dofs.end());
+    }
+
+    // Compact per-brick face layout <-> reference ghosted AmrHostFields.
+    std::size_t u_compact(int bs, std::size_t slot, int i, int j, int k) { return slot * std::size_t((bs + 1) * bs * bs) + std::size_t((k * bs + j) * (bs + 1) + i); }
+    std::size_t v_compact(int bs, std::size_t slot, int i, int j, int k) { return slot * std::size_t((bs + 1) * bs * bs) + std::size_t((k * (bs + 1) + j) * bs + i); }
+    std::size_t w_compact(int bs, std::size_t slot, int i, int j, int k) { return slot * std::size_t((bs + 1) * bs * bs) + std::size_t((k * bs + j) * bs + i); }
+
+    void to_host_fields(const RefCase& rc, const float* u, const float* v, const float* w, AmrHostFields& fields)
+    {
+        const int bs = rc.system.brick_size;
+        for (int l = 0; l < int(rc.hierarchy.levels().size()); ++l)
+        {
+            auto& lv = fields.levels()[l];
+            const auto& lay = lv.layout;
+            const int nb = int(rc.hierarchy.levels()[l].bricks.size());
+            const std::size_t slot0 = std::size_t(rc.system.level_offset[l]) / std::size_t(bs * bs * bs);
+            for (int b = 0; b < nb; ++b)
+                for (int k = 0; k < bs; ++k)
+                    for (int j = 0; j < bs; ++j)
+                        for (int i = 0; i <= bs; ++i)
+                        {
+                            lv.u[lay.u_index(b, i, j, k)] = u[u_compact(bs, slot0 + b, i, j, k)];
+                            lv.v[lay.v_index(b, j, i, k)] = v[v_compact(bs, slot0 + b, j, i, k)];
+                            lv.w[lay.w_index(b, j, k, i)] = w[w_compact(bs, slot0 + b, j, k, i)];
+                        }
+        }
+    }
+    void from_host_fields(const RefCase& rc, const AmrHostFields& fields, float* u, float* v, float* w)
+    {
+        const int bs = rc.system.brick_size;
+        for (int l = 0; l < int(rc.hierarchy.levels().size()); ++l)
+        {
+            const auto& lv = fields.levels()[l];
+            const auto& lay = lv.layout;
+            const int nb = int(rc.hierarchy.levels()[l].bricks.size());
+            const std::size_t slot0 = std::size_t(rc.system.level_offset[l]) / std::size_t(bs * bs * bs);
+            for (int b = 0; b < nb; ++b)
+                for (int k = 0; k < bs; ++k)
+                    for (int j = 0; j < bs; ++j)
+                        for (int i = 0; i <= bs; ++i)
+                        {
+                            u[u_compact(bs, slot0 + b, i, j, k)] = lv.u[lay.u_index(b, i, j, k)];
+                            v[v_compact(bs, slot0 + b, j, i, k)] = lv.v[lay.v_index(b, j, i, k)];
+                            w[w_compact(bs, slot0 + b, j, k, i)] = lv.w[lay.w_index(b, j, k, i)];
+                        }
+        }
+    }
+
+    CompositeAmrFluxes special_from(const RefCase& rc, const double* cf, const double* eb)
+    {
+        CompositeAmrFluxes f = make_zero_composite_fluxes(rc.system);
+        for (std::size_t q = 0; q < f.coarse_fine_velocity.size(); ++q) f.coarse_fine_velocity[q] = cf ? cf[q] : 0.0;
+        for (std::size_t q = 0; q < f.embedded_velocity.size(); ++q) f.embedded_velocity[q] = eb ? eb[q] : 0.0;
+        return f;
+    }
+
+    template <class F> int guarded(F&& f)
+    {
+        try { f(); return 0; }
+        catch (const std::exception& e) { g_error = e.what(); return 1; }
+        catch (...) { g_error = "unknown exception"; return 1; }
+    }
+}
+
+extern "C" {
+
+const char* ref_last_error(void) { return g_error.c_str(); }
+
+void ref_default_params(int32_t kind, ref_case_params* p)
+{
+    std::memset(p, 0, sizeof(*p));
+    p->kind = kind;
+    p->naca_digits = 12;
+    p->section_points = 48;
+    p->max_levels = 2;
+    p->brick_size = 8;
+    p->base_cell_size = 0.125;
+    p->chord = 1.0;
+    p->span = 2.0;
+    p->aoa_deg = 4.0;
+    p->surface_refinement_distance = 0.2;
+    p->wing_refinement_distance = 0.2;
+    p->wake_length = 0.5;
+    p->wake_radius = 0.5;
+    p->min_volume_fraction = 0.005;
+    if (kind == REF_CASE_NACA_SLAB)
+    {
+        // Single uniform level over 4c x 2c x 2c (chord 1): the plain-method case, scaled by
+        // base_cell_size (1/32 gives 128 x 64 x 64 cells).
+        p->max_levels = 1;
+        p->base_cell_size = 1.0 / 32.0;
+        p->domain_lo[0] = -1.0; p->domain_lo[1] = -1.0; p->domain_lo[2] = -1.0;
+        p->domain_hi[0] = 3.0; p->domain_hi[1] = 1.0; p->domain_hi[2] = 1.0;
+        p->min_volume_fraction = 0.25;
+    }
+}
+
+void* ref_case_create(const ref_case_params* p)
+{
+    RefCase* rc = nullptr;
+    const int status = guarded([&] {
+        auto owned = std::make_unique<RefCase>();
+        RefCase& c = *owned;
+        ParagliderConfig& config = c.config;
+        config.amr.brick_size = p->brick_size;
+        config.amr.max_levels = p->max_levels;
+        config.amr.base_cell_size = p->base_cell_size;
+        config.amr.wing_refinement_distance = p->wing_refinement_distance;
+        config.amr.surface_refinement_distance = p->surface_refinement_distance;
+        config.amr.wake_length = p->wake_length;
+        config.amr.wake_radius = p->wake_radius;
+        config.amr.min_volume_fraction = p->min_volume_fraction;
+        Aabb3d domain;
+        if (p->kind == REF_CASE_BOX || p->kind == REF_CASE_BOX_CROPPED)
+        {
+            // tools/physics_contract_probe.cpp:110-138 (box and --cropped variants)
+            const bool cropped = p->kind == REF_CASE_BOX_CROPPED;
+            const Vec3d half{0.6, 0.8, 0.18};
+            TriMesh source = box_mesh(half);
+            config.freestream.speed = 2;
+            config.domain = {1.25, 1.25, 1.25, 1.25, false};
+            const double pitch = 0.31, yaw = cropped ? 0 : 0.17, cp = std::cos(pitch), sp = std::sin(pitch),
+                         ca = std::cos(yaw), sa = std::sin(yaw);
+            const double rotation[9] = {ca * cp, -sa, ca * sp, sa * cp, ca, sa * sp, -sp, 0, cp};
+            std::copy(rotation, rotation + 9, config.placement.m);
+            if (cropped)
+            {
+                source = clip_mesh_to_axis_slab(source, 1, -0.25, 0.25);
+                config.domain.lateral_margin = 0;
+                config.amr.base_cell_size = 0.0625;
+                config.amr.max_levels = 1;
+            }
+            config.placement = frame_wing_for_external_domain(source, config.placement, config.domain.upstream_margin,
+                config.domain.lateral_margin, config.domain.vertical_margin, config.amr.base_cell_size * config.amr.brick_size);
+            c.wing = placed_mesh(source, config.placement);
+            c.solid = std::make_shared<PlacedBox>(half, config.placement);
+            domain = automatic_flow_domain(c.wing, config.domain);
+        }
+        else
+        {
+            auto poly = naca_polygon(p->naca_digits, p->section_points, p->chord);
+            if (polygon_signed_area(poly) < 0) std::reverse(poly.begin(), poly.end());
+            SectionPlacement place;
+            const double a = p->aoa_deg * std::acos(-1.0) / 180.0;
+            place.cos_a = std::cos(a); place.sin_a = std::sin(a);
+            place.pivot_x = 0.25 * p->chord; place.pivot_z = 0;
+            for (int q = 0; q < 3; ++q) { domain.lo[q] = p->domain_lo[q]; domain.hi[q] = p->domain_hi[q]; }
+            const bool slab = p->kind == REF_CASE_NACA_SLAB;
+            const double half_span = 0.5 * p->span;
+            if (slab)
+            {
+                // Section extruded beyond the slab and clipped at the side walls (slip walls
+                // meet the solid): same construction as the reference's cropped contract.
+                TriMesh longer = extruded_mesh(poly, place, -half_span - 0.5, half_span + 0.5, true);
+                c.wing = clip_mesh_to_axis_slab(longer, 1, domain.lo.y, domain.hi.y);
+                c.solid = std::make_shared<ExtrudedSection>(poly, place, -1e9, 1e9, false);
+            }
+            else
+            {
+                c.wing = extruded_mesh(poly, place, -half_span, half_span, true);
+                c.solid = std::make_shared<ExtrudedSection>(poly, place, -half_span, half_span, true);
+            }
+        }
+        c.bvh = std::make_unique<TriangleBvh>(c.wing);
+        c.hierarchy = AmrHierarchy::build_static(domain, c.wing, *c.bvh, config.amr, config.domain.half_wing_symmetry);
+        EmbeddedBoundaryBuildOptions eb;
+        eb.min_volume_fraction = config.amr.min_volume_fraction;
+        eb.retain_signed_bracketed_small_roots_for_face_state = true;
+        eb.min_aperture_area_fraction = config.amr.min_aperture_area_fraction;
+        eb.closed_solid = c.solid;
+        c.atlas = build_amr_embedded_boundary_atlas(c.hierarchy, c.wing, *c.bvh, eb);
+        if (!c.atlas.ready_for_flow())
+            throw std::runtime_error("reference EB atlas has " + std::to_string(c.atlas.unresolved_count()) + " unresolved cells");
+        CompositeAmrPressureBuildOptions options;
+        options.pressure_outlet_xmax = true;
+        c.system = build_composite_amr_pressure_system(c.hierarchy, c.atlas, options);
+        c.system.hierarchy = &c.hierarchy;
+        export_case(c);
+        rc = owned.release();
+    });
+    return status == 0 ? rc : nullptr;
+}
+
+void ref_case_destroy(void* handle) { delete static_cast<RefCase*>(handle); }
+
+int ref_case_topology(void* handle, pcfd_topology* out)
+{
+    return guarded([&] {
+        RefCase& c = *static_cast<RefCase*>(handle);
+        const auto& s = c.system;
+        std::memset(out, 0, sizeof(*out));
+        out->brick_size = s.brick_size;
+        out->level_count = int32_t(c.levels.size());
+        out->levels = c.levels.data();
+        for (int a = 0; a < 3; ++a) { out->domain_lo[a] = c.hierarchy.domain().lo[a]; out->domain_hi[a] = c.hierarchy.domain().hi[a]; }
+        out->storage_size = s.storage_size;
+        out->pressure_outlet_xmax = s.pressure_outlet_xmax ? 1 : 0;
+        out->active = s.active.data();
+        out->freestream_connected = s.freestream_connected.data();
+        out->cut_face_mask = s.cut_face_mask.data();
+        out->volume = s.volume.data();
+        out->centroid = c.centroid.data();
+        out->preconditioner_aggregate = s.preconditioner_aggregate.data();
+        out->coarse_fine = view_connections(c.cf);
+        out->embedded = view_connections(c.eb);
+        pcfd_regular_corrections& r = out->regular;
+        r.count = int32_t(c.rc_lower.size());
+        r.lower_dof = c.rc_lower.data(); r.upper_dof = c.rc_upper.data(); r.level = c.rc_level.data();
+        r.brick = c.rc_brick.data(); r.ijk = c.rc_ijk.data(); r.axis = c.rc_axis.data();
+        r.open_area = c.rc_area.data(); r.two_point_delta = c.rc_delta.data();
+        r.lower_gradient_node = c.rc_lower_node.data(); r.upper_gradient_node = c.rc_upper_node.data();
+        r.nonorthogonal_correction = c.rc_correction.data(); r.upper_gradient_weight = c.rc_weight.data();
+        out->gradient_node_count = int32_t(s.pressure_gradient_dof.size());
+        out->gradient_dof = s.pressure_gradient_dof.data();
+        out->gradient_offset = s.pressure_gradient_offset.data();
+        out->gradient_neighbour = s.pressure_gradient_neighbour.data();
+        out->gradient_weight = c.gradient_weight.data();
+        out->gauge_count = int32_t(c.gauge_dof.size());
+        out->gauge_dof = c.gauge_dof.data();
+        out->gauge_coefficient = c.gauge_coefficient.data();
+        out->patches.count = int32_t(c.patch_area.size());
+        out->patches.area = c.patch_area.data(); out->patches.centroid = c.patch_centroid.data();
+        out->patches.normal = c.patch_normal.data(); out->patches.plus_dof = c.patch_plus.data();
+        out->patches.minus_dof = c.patch_minus.data();
+        out->boundary_faces.count = int32_t(c.bf_dof.size());
+        out->boundary_faces.dof = c.bf_dof.data(); out->boundary_faces.outward_area = c.bf_area.data();
+        out->boundary_faces.centroid = c.bf_centroid.data();
+        out->retained_count = int32_t(c.retained.size());
+        out->retained_dofs = c.retained.data();
+    });
+}
+
+int ref_case_summary(void* handle, int64_t* o)
+{
+    return guarded([&] {
+        RefCase& c = *static_cast<RefCase*>(handle);
+        const auto& s = c.system;
+        int64_t active = 0;
+        for (auto a : s.active) active += a ? 1 : 0;
+        o[0] = int64_t(c.hierarchy.levels().size()); o[1] = s.storage_size; o[2] = active;
+        o[3] = int64_t(s.coarse_fine.size()); o[4] = int64_t(s.embedded.size());
+        o[5] = int64_t(s.regular_pressure_corrections.size()); o[6] = int64_t(s.pressure_gradient_dof.size());
+        o[7] = int64_t(s.gauges.size()); o[8] = int64_t(s.surface_patches.size());
+        o[9] = int64_t(s.boundary_faces.size()); o[10] = int64_t(c.atlas.unresolved_count());
+        o[11] = int64_t(s.face_state_retained_dofs.size());
+    });
+}
+
+int ref_case_level_counts(void* handle, int64_t* o)
+{
+    return guarded([&] {
+        RefCase& c = *static_cast<RefCase*>(handle);
+        for (std::size_t l = 0; l < c.hierarchy.levels().size(); ++l)
+        {
+            o[2 * l] = int64_t(c.hierarchy.levels()[l].bricks.size());
+            o[2 * l + 1] = int64_t(c.hierarchy.levels()[l].active_bricks);
+        }
+    });
+}
+
+int ref_apply_cpu(void* handle, const double* p, double* out)
+{
+    return guarded([&] {
+        RefCase& c = *static_cast<RefCase*>(handle);
+        std::vector<double> in(p, p + c.system.storage_size), result;
+        c.system.apply_cpu(in, result);
+        std::copy(result.begin(), result.end(), out);
+    });
+}
+
+int ref_diagonal_cpu(void* handle, double* diag)
+{
+    return guarded([&] {
+        RefCase& c = *static_cast<RefCase*>(handle);
+        std::vector<double> d;
+        c.system.diagonal_cpu(d);
+        std::copy(d.begin(), d.end(), diag);
+    });
+}
+
+int ref_divergence_cpu(void* handle, const float* u, const float* v, const float* w, const double* cf,
+                       const double* eb, double* divergence)
+{
+    return guarded([&] {
+        RefCase& c = *static_cast<RefCase*>(handle);
+        AmrHostFields fields(c.hierarchy);
+        to_host_fields(c, u, v, w, fields);
+        std::vector<double> div;
+        composite_amr_divergence_cpu(c.system, fields, special_from(c, cf, eb), div);
+        std::copy(div.begin(), div.end(), divergence);
+    });
+}
+
+int ref_rhs_cpu(void* handle, const float* u, const float* v, const float* w, const double* cf,
+                const double* eb, double rho, double dt, double* rhs)
+{
+    return guarded([&] {
+        RefCase& c = *static_cast<RefCase*>(handle);
+        AmrHostFields fields(c.hierarchy);
+        to_host_fields(c, u, v, w, fields);
+        std::vector<double> r;
+        composite_amr_projection_rhs_cpu(c.system, fields, special_from(c, cf, eb), rho, dt, r);
+        std::copy(r.begin(), r.end(), rhs);
+    });
+}
+
+int ref_correct_fluxes_cpu(void* handle, const double* pressure, double rho, double dt, float* u, float* v,
+                           float* w, double* cf, double* eb)
+{
+    return guarded([&] {
+        RefCase& c = *static_cast<RefCase*>(handle);
+        AmrHostFields fields(c.hierarchy);
+        to_host_fields(c, u, v, w, fields);
+        CompositeAmrFluxes special = special_from(c, cf, eb);
+        std::vector<double> p(pressure, pressure + c.system.storage_size);
+        composite_amr_correct_fluxes_cpu(c.system, p, rho, dt, fields, special);
+        from_host_fields(c, fields, u, v, w);
+        if (cf) std::copy(special.coarse_fine_velocity.begin(), special.coarse_fine_velocity.end(), cf);
+        if (eb) std::copy(special.embedded_velocity.begin(), special.embedded_velocity.end(), eb);
+    });
+}
+
+int ref_pressure_gradients_cpu(void* handle, const double* pressure, double* gradient3)
+{
+    return guarded([&] {
+        RefCase& c = *static_cast<RefCase*>(handle);
+        std::vector<double> p(pressure, pressure + c.system.storage_size);
+        const auto g = composite_pressure_gradients_cpu(c.system, p);
+        for (std::size_t q = 0; q < g.size(); ++q)
+            for (int a = 0; a < 3; ++a) gradient3[3 * q + a] = g[q][a];
+    });
+}
+
+}  // extern "C"

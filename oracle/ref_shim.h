@@ -1,0 +1,63 @@
+/*
+ * ref_shim.h -- flat C entry points into the reference ParaCFD host code, compiled from the
+ * reference's own sources into oracle/_ref/libparacfd_ref.so.  TEST INFRASTRUCTURE ONLY:
+ * the product never links this; tests and the CPU-baseline arm use it as the checker.
+ */
+#ifndef PCFD_REF_SHIM_H
+#define PCFD_REF_SHIM_H
+#include <stdint.h>
+#include "../include/paracfd_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { REF_CASE_BOX = 0, REF_CASE_NACA_SLAB = 1, REF_CASE_NACA_WING = 2, REF_CASE_BOX_CROPPED = 3 };
+
+typedef struct ref_case_params {
+    int32_t kind;            /* REF_CASE_* */
+    int32_t naca_digits;     /* e.g. 12 for 0012, 4412 */
+    int32_t section_points;  /* polygon points per surface */
+    int32_t max_levels;
+    int32_t brick_size;
+    double base_cell_size;
+    double chord;
+    double span;             /* full span of the wing (NACA_WING) / slab width (NACA_SLAB) */
+    double aoa_deg;
+    double domain_lo[3], domain_hi[3];   /* explicit flow domain for the NACA cases */
+    double surface_refinement_distance;
+    double wing_refinement_distance;
+    double wake_length, wake_radius;
+    double min_volume_fraction;
+} ref_case_params;
+
+void ref_default_params(int32_t kind, ref_case_params* params);
+/* Builds hierarchy -> EB atlas -> composite pressure system with the reference code. */
+void* ref_case_create(const ref_case_params* params);
+void ref_case_destroy(void* handle);
+const char* ref_last_error(void);
+/* Fills a topology view whose arrays live inside the handle. */
+int ref_case_topology(void* handle, pcfd_topology* out);
+/* Summary numbers: [levels, storage, active dofs, coarse_fine, embedded, regular corr,
+ * gradient nodes, gauges, patches, boundary faces, unresolved cells, retained] */
+int ref_case_summary(void* handle, int64_t* out12);
+/* Per level: coarsest-first brick count and active brick count, [levels][2]. */
+int ref_case_level_counts(void* handle, int64_t* out);
+
+/* Reference host operators (FP64), DOF-indexed vectors of length S. */
+int ref_apply_cpu(void* handle, const double* p, double* out);
+int ref_diagonal_cpu(void* handle, double* diag);
+/* Faces in the compact per-brick layout of paracfd_b200.h; special velocities in double. */
+int ref_divergence_cpu(void* handle, const float* u, const float* v, const float* w,
+                       const double* cf, const double* eb, double* divergence);
+int ref_rhs_cpu(void* handle, const float* u, const float* v, const float* w,
+                const double* cf, const double* eb, double rho, double dt, double* rhs);
+/* In/out faces and special velocities. */
+int ref_correct_fluxes_cpu(void* handle, const double* pressure, double rho, double dt,
+                           float* u, float* v, float* w, double* cf, double* eb);
+int ref_pressure_gradients_cpu(void* handle, const double* pressure, double* gradient3);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

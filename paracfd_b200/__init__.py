@@ -1,0 +1,143 @@
+"""paracfd_b200 -- B200-native (sm_100a) ParaCFD per-timestep solver path.
+
+Host mirror of the reference's device classes (DeviceCompositeAmrPressureOperator / Solver,
+DeviceCompositeAmrProjection, reference src/core/fluid/amr_pressure.h:292-584) over the C ABI
+in include/paracfd_b200.h.  All compute runs in ``libparacfd_b200.so``; this module only moves
+host arrays across the boundary.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import capi
+from .capi import Options, SolveResult, Topology, check, ptr
+
+MG_FP64, MG_FP32 = 0, 1
+
+
+class CompositeSystem:
+    """Resident topology + state on one GPU (one host thread at a time)."""
+
+    def __init__(self, topology: Topology, mg_precision: int = MG_FP64, device: int = 0):
+        self._lib = capi.load()
+        self._topology = topology   # keep the caller's arrays alive during creation
+        opts = Options(mg_precision, device, None)
+        handle = C.c_void_p()
+        check(self._lib.pcfd_system_create(C.byref(topology), C.byref(opts), C.byref(handle)))
+        self.handle = handle
+        sizes = [C.c_int64() for _ in range(5)]
+        check(self._lib.pcfd_system_sizes(self.handle, *[C.byref(x) for x in sizes]))
+        self.storage_size, self.bricks, self.faces, self.coarse_fine_count, self.embedded_count = (x.value for x in sizes)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._lib.pcfd_system_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- pressure operator / solver -------------------------------------------------------
+    def _vec(self, x, dtype=np.float64):
+        x = np.ascontiguousarray(x, dtype=dtype)
+        if x.shape != (self.storage_size,):
+            raise ValueError(f"expected a vector of {self.storage_size} DOFs")
+        return x
+
+    def apply(self, p, orthogonal: bool = False) -> np.ndarray:
+        p = self._vec(p)
+        out = np.empty(self.storage_size)
+        check(self._lib.pcfd_pressure_apply_host(self.handle, ptr(p, C.c_double), ptr(out, C.c_double), int(orthogonal)))
+        return out
+
+    def diagonal(self) -> np.ndarray:
+        out = np.empty(self.storage_size)
+        check(self._lib.pcfd_pressure_diagonal_host(self.handle, ptr(out, C.c_double)))
+        return out
+
+    def precondition(self, r) -> np.ndarray:
+        r = self._vec(r)
+        out = np.empty(self.storage_size)
+        check(self._lib.pcfd_pressure_precondition_host(self.handle, ptr(r, C.c_double), ptr(out, C.c_double)))
+        return out
+
+    def solve(self, b, tolerance: float, max_iterations: int, x0=None):
+        b = self._vec(b)
+        x = self._vec(x0).copy() if x0 is not None else np.zeros(self.storage_size)
+        res = SolveResult()
+        check(self._lib.pcfd_pressure_solve_host(self.handle, ptr(x, C.c_double), ptr(b, C.c_double), tolerance,
+                                                 max_iterations, int(x0 is not None), C.byref(res)))
+        return x, res.as_dict()
+
+    # ---- resident state ---------------------------------------------------------------------
+    def set_faces(self, u, v, w):
+        u, v, w = (np.ascontiguousarray(a, np.float32) for a in (u, v, w))
+        check(self._lib.pcfd_set_faces_host(self.handle, ptr(u, C.c_float), ptr(v, C.c_float), ptr(w, C.c_float)))
+
+    def get_faces(self):
+        u, v, w = (np.empty(self.faces, np.float32) for _ in range(3))
+        check(self._lib.pcfd_get_faces_host(self.handle, ptr(u, C.c_float), ptr(v, C.c_float), ptr(w, C.c_float)))
+        return u, v, w
+
+    def set_special(self, coarse_fine, embedded):
+        cf = np.ascontiguousarray(coarse_fine, np.float32)
+        eb = np.ascontiguousarray(embedded, np.float32)
+        check(self._lib.pcfd_set_special_host(self.handle, ptr(cf, C.c_float), ptr(eb, C.c_float)))
+
+    def get_special(self):
+        cf = np.empty(self.coarse_fine_count, np.float32)
+        eb = np.empty(self.embedded_count, np.float32)
+        check(self._lib.pcfd_get_special_host(self.handle, ptr(cf, C.c_float), ptr(eb, C.c_float)))
+        return cf, eb
+
+    def set_pressure(self, p):
+        p = self._vec(p)
+        check(self._lib.pcfd_set_pressure_host(self.handle, ptr(p, C.c_double)))
+
+    def get_pressure(self) -> np.ndarray:
+        out = np.empty(self.storage_size)
+        check(self._lib.pcfd_get_pressure_host(self.handle, ptr(out, C.c_double)))
+        return out
+
+    def get_pressure_shadow(self) -> np.ndarray:
+        out = np.empty(self.storage_size, np.float32)
+        check(self._lib.pcfd_get_pressure_shadow_host(self.handle, ptr(out, C.c_float)))
+        return out
+
+    def time_kernel(self, which: int, iterations: int = 20) -> float:
+        """Milliseconds per launch sequence, CUDA events on the system stream."""
+        ms = C.c_double()
+        check(self._lib.pcfd_time_kernel(self.handle, which, iterations, C.byref(ms)))
+        return ms.value
+
+    # ---- projection -------------------------------------------------------------------------
+    def divergence(self) -> np.ndarray:
+        out = np.empty(self.storage_size, np.float32)
+        check(self._lib.pcfd_projection_divergence_host(self.handle, ptr(out, C.c_float)))
+        return out
+
+    def projection_rhs(self, rho: float, dt: float) -> np.ndarray:
+        out = np.empty(self.storage_size)
+        check(self._lib.pcfd_projection_rhs_host(self.handle, rho, dt, ptr(out, C.c_double)))
+        return out
+
+    def correct_fluxes(self, rho: float, dt: float):
+        check(self._lib.pcfd_projection_correct(self.handle, rho, dt))
+
+    def project(self, rho: float, dt: float, tolerance: float, max_iterations: int, warm_start: bool = False):
+        res = SolveResult()
+        status = self._lib.pcfd_projection_project(self.handle, rho, dt, tolerance, max_iterations, int(warm_start), C.byref(res))
+        if status not in (capi.PCFD_OK, 3):   # 3 = NOT_CONVERGED is reported in the result
+            check(status)
+        return res.as_dict()

@@ -1,0 +1,163 @@
+"""ctypes mirror of include/paracfd_b200.h and the loader for the in-tree native library.
+
+The Python layer is a thin host: every compute call goes through the C ABI into
+``libparacfd_b200.so`` (hand-written sm_100a kernels).  Loading fails loudly when the library
+is missing; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBRARY_PATH = os.path.join(_HERE, "libparacfd_b200.so")
+
+PCFD_OK = 0
+STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "CUDA_ERROR", 3: "NOT_CONVERGED",
+                4: "TOPOLOGY_UNRESOLVED", 5: "OUT_OF_MEMORY", 6: "TIMEOUT", 7: "INTERNAL"}
+
+BRICK_XMIN, BRICK_XMAX, BRICK_YMIN, BRICK_YMAX, BRICK_ZMIN, BRICK_ZMAX = (1 << q for q in range(6))
+BRICK_EMBEDDED_BOUNDARY, BRICK_COVERED = 1 << 6, 1 << 7
+
+_i32p = C.POINTER(C.c_int32)
+_u32p = C.POINTER(C.c_uint32)
+_u8p = C.POINTER(C.c_uint8)
+_i8p = C.POINTER(C.c_int8)
+_f64p = C.POINTER(C.c_double)
+_f32p = C.POINTER(C.c_float)
+
+
+class Level(C.Structure):
+    _fields_ = [("h", C.c_double), ("brick_count", C.c_int32), ("level_offset", C.c_int32),
+                ("coord", _i32p), ("origin", _f64p), ("neighbors", _i32p), ("flags", _u32p),
+                ("children", _i32p)]
+
+
+class Connections(C.Structure):
+    _fields_ = [("count", C.c_int32), ("coarse_dof", _i32p), ("fine_dof", _i32p),
+                ("open_area", _f64p), ("centre_distance", _f64p), ("normal_distance", _f64p),
+                ("axis", _i8p), ("direction", _i8p), ("face_centroid", _f64p),
+                ("orthogonal_gradient_factor", _f64p), ("lower_gradient_node", _i32p),
+                ("upper_gradient_node", _i32p), ("nonorthogonal_correction", _f64p),
+                ("upper_gradient_weight", _f64p)]
+
+
+class RegularCorrections(C.Structure):
+    _fields_ = [("count", C.c_int32), ("lower_dof", _i32p), ("upper_dof", _i32p),
+                ("level", _i32p), ("brick", _i32p), ("ijk", _i32p), ("axis", _i8p),
+                ("open_area", _f64p), ("two_point_delta", _f64p),
+                ("lower_gradient_node", _i32p), ("upper_gradient_node", _i32p),
+                ("nonorthogonal_correction", _f64p), ("upper_gradient_weight", _f64p)]
+
+
+class SurfacePatches(C.Structure):
+    _fields_ = [("count", C.c_int32), ("area", _f64p), ("centroid", _f64p), ("normal", _f64p),
+                ("plus_dof", _i32p), ("minus_dof", _i32p)]
+
+
+class BoundaryFaces(C.Structure):
+    _fields_ = [("count", C.c_int32), ("dof", _i32p), ("outward_area", _f64p),
+                ("centroid", _f64p)]
+
+
+class Topology(C.Structure):
+    _fields_ = [("brick_size", C.c_int32), ("level_count", C.c_int32),
+                ("levels", C.POINTER(Level)),
+                ("domain_lo", C.c_double * 3), ("domain_hi", C.c_double * 3),
+                ("storage_size", C.c_int32), ("pressure_outlet_xmax", C.c_int32),
+                ("active", _u8p), ("freestream_connected", _u8p), ("cut_face_mask", _u8p),
+                ("volume", _f64p), ("centroid", _f64p), ("preconditioner_aggregate", _i32p),
+                ("coarse_fine", Connections), ("embedded", Connections),
+                ("regular", RegularCorrections),
+                ("gradient_node_count", C.c_int32), ("gradient_dof", _i32p),
+                ("gradient_offset", _i32p), ("gradient_neighbour", _i32p),
+                ("gradient_weight", _f64p),
+                ("gauge_count", C.c_int32), ("gauge_dof", _i32p), ("gauge_coefficient", _f64p),
+                ("patches", SurfacePatches), ("boundary_faces", BoundaryFaces),
+                ("retained_count", C.c_int32), ("retained_dofs", _i32p)]
+
+
+class Options(C.Structure):
+    _fields_ = [("mg_precision", C.c_int32), ("device", C.c_int32), ("stream", C.c_void_p)]
+
+
+class SolveResult(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("relative_residual", C.c_double),
+                ("converged", C.c_int32), ("preconditioner_applications", C.c_int32),
+                ("recycle_rejections", C.c_int32)]
+
+    def as_dict(self):
+        return {"iterations": self.iterations, "relative_residual": self.relative_residual,
+                "converged": bool(self.converged),
+                "preconditioner_applications": self.preconditioner_applications,
+                "recycle_rejections": self.recycle_rejections}
+
+
+def ptr(array: np.ndarray | None, ctype):
+    """Pointer to a contiguous numpy array (None -> NULL)."""
+    if array is None:
+        return C.cast(None, C.POINTER(ctype))
+    if not array.flags["C_CONTIGUOUS"]:
+        raise ValueError("array must be C-contiguous")
+    return array.ctypes.data_as(C.POINTER(ctype))
+
+
+# Exported symbols and their argument types; also the list the CPU tests check.
+SIGNATURES = {
+    "pcfd_last_error_message": (C.c_char_p, []),
+    "pcfd_version": (C.c_char_p, []),
+    "pcfd_system_create": (C.c_int, [C.POINTER(Topology), C.POINTER(Options), C.POINTER(C.c_void_p)]),
+    "pcfd_system_destroy": (None, [C.c_void_p]),
+    "pcfd_system_sizes": (C.c_int, [C.c_void_p] + [C.POINTER(C.c_int64)] * 5),
+    "pcfd_system_synchronize": (C.c_int, [C.c_void_p]),
+    "pcfd_pressure_apply_host": (C.c_int, [C.c_void_p, _f64p, _f64p, C.c_int32]),
+    "pcfd_pressure_apply_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]),
+    "pcfd_pressure_diagonal_host": (C.c_int, [C.c_void_p, _f64p]),
+    "pcfd_pressure_precondition_host": (C.c_int, [C.c_void_p, _f64p, _f64p]),
+    "pcfd_pressure_solve_host": (C.c_int, [C.c_void_p, _f64p, _f64p, C.c_double, C.c_int32,
+                                           C.c_int32, C.POINTER(SolveResult)]),
+    "pcfd_set_faces_host": (C.c_int, [C.c_void_p, _f32p, _f32p, _f32p]),
+    "pcfd_get_faces_host": (C.c_int, [C.c_void_p, _f32p, _f32p, _f32p]),
+    "pcfd_set_special_host": (C.c_int, [C.c_void_p, _f32p, _f32p]),
+    "pcfd_get_special_host": (C.c_int, [C.c_void_p, _f32p, _f32p]),
+    "pcfd_set_pressure_host": (C.c_int, [C.c_void_p, _f64p]),
+    "pcfd_get_pressure_host": (C.c_int, [C.c_void_p, _f64p]),
+    "pcfd_get_pressure_shadow_host": (C.c_int, [C.c_void_p, _f32p]),
+    "pcfd_projection_divergence_host": (C.c_int, [C.c_void_p, _f32p]),
+    "pcfd_projection_rhs_host": (C.c_int, [C.c_void_p, C.c_double, C.c_double, _f64p]),
+    "pcfd_projection_correct": (C.c_int, [C.c_void_p, C.c_double, C.c_double]),
+    "pcfd_projection_project": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double,
+                                          C.c_int32, C.c_int32, C.POINTER(SolveResult)]),
+    "pcfd_time_kernel": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
+}
+
+_lib = None
+
+
+def load(path: str = LIBRARY_PATH):
+    """Load the native library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"paracfd_b200 native library missing: {path}; run __graft_entry__.build()")
+    lib = C.CDLL(path)
+    for name, (restype, argtypes) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = restype
+        fn.argtypes = argtypes
+    _lib = lib
+    return lib
+
+
+class PcfdError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+def check(status: int):
+    if status != PCFD_OK:
+        raise PcfdError(status, load().pcfd_last_error_message().decode(errors="replace"))

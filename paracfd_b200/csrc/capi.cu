@@ -1,0 +1,487 @@
+// capi.cu -- the extern "C" boundary (include/paracfd_b200.h): topology validation and upload,
+// resident state transfer, and the projection entry points.  Every entry point converts C++
+// exceptions into a status code plus a thread-local message; no exception crosses the ABI.
+#include "pcfd_internal.h"
+
+#include <cmath>
+#include <cstring>
+#include <memory>
+
+namespace pcfd
+{
+    namespace
+    {
+        thread_local std::string g_error;
+
+        template <class F> pcfd_status guarded(F&& f)
+        {
+            try
+            {
+                f();
+                return PCFD_OK;
+            }
+            catch (const Error& e) { g_error = e.what(); return e.status; }
+            catch (const std::bad_alloc&) { g_error = "host allocation failed"; return PCFD_OUT_OF_MEMORY; }
+            catch (const std::exception& e) { g_error = e.what(); return PCFD_INTERNAL; }
+            catch (...) { g_error = "unknown failure"; return PCFD_INTERNAL; }
+        }
+
+        // diagonal_cpu semantics (reference amr_pressure.cpp:525-543), host FP64.
+        std::vector<double> host_diagonal(const pcfd_topology& t)
+        {
+            const int bs = t.brick_size, c3 = bs * bs * bs;
+            std::vector<double> d(size_t(t.storage_size), 0.0);
+            auto add = [&](int a, int b, double c) {
+                if (a < 0 || b < 0 || a == b || !t.active[a] || !t.active[b]) return;
+                d[a] += c;
+                d[b] += c;
+            };
+            for (int l = 0; l < t.level_count; ++l)
+            {
+                const pcfd_level& lev = t.levels[l];
+                for (int brick = 0; brick < lev.brick_count; ++brick)
+                {
+                    if (lev.flags[brick] & PCFD_BRICK_COVERED) continue;
+                    for (int k = 0; k < bs; ++k)
+                        for (int j = 0; j < bs; ++j)
+                            for (int i = 0; i < bs; ++i)
+                            {
+                                const int a = lev.level_offset + brick * c3 + (k * bs + j) * bs + i;
+                                if (!t.active[a]) continue;
+                                for (int axis = 0; axis < 3; ++axis)
+                                {
+                                    if (t.cut_face_mask[a] & (1u << axis)) continue;
+                                    int c[3] = {i, j, k};
+                                    ++c[axis];
+                                    if (c[axis] < bs) add(a, lev.level_offset + brick * c3 + (c[2] * bs + c[1]) * bs + c[0], lev.h);
+                                    else
+                                    {
+                                        const int nb = lev.neighbors[brick * 6 + 2 * axis + 1];
+                                        if (nb >= 0 && !(lev.flags[nb] & PCFD_BRICK_COVERED))
+                                        {
+                                            c[axis] = 0;
+                                            add(a, lev.level_offset + nb * c3 + (c[2] * bs + c[1]) * bs + c[0], lev.h);
+                                        }
+                                    }
+                                }
+                                if (t.pressure_outlet_xmax && (lev.flags[brick] & PCFD_BRICK_XMAX) && i == bs - 1) d[a] += 2.0 * lev.h;
+                            }
+                }
+            }
+            auto factor = [](const pcfd_connections& c, int e) {
+                const double f = c.orthogonal_gradient_factor[e];
+                return f > 0 ? f : (c.normal_distance[e] > 0 ? 1.0 / c.normal_distance[e] : 0.0);
+            };
+            for (int e = 0; e < t.coarse_fine.count; ++e)
+                add(t.coarse_fine.coarse_dof[e], t.coarse_fine.fine_dof[e], t.coarse_fine.open_area[e] * factor(t.coarse_fine, e));
+            for (int e = 0; e < t.embedded.count; ++e)
+                add(t.embedded.coarse_dof[e], t.embedded.fine_dof[e], t.embedded.open_area[e] * factor(t.embedded, e));
+            for (int e = 0; e < t.regular.count; ++e)
+                add(t.regular.lower_dof[e], t.regular.upper_dof[e], t.regular.open_area[e] * t.regular.two_point_delta[e]);
+            for (int g = 0; g < t.gauge_count; ++g)
+                if (t.gauge_dof[g] >= 0 && t.active[t.gauge_dof[g]]) d[t.gauge_dof[g]] += t.gauge_coefficient[g];
+            return d;
+        }
+
+        void validate(const pcfd_topology& t)
+        {
+            require(t.brick_size > 0 && t.brick_size <= 32, "brick_size must be in 1..32");
+            require(t.level_count > 0 && t.levels, "topology needs at least one level");
+            require(t.storage_size > 0 && t.active && t.cut_face_mask && t.volume && t.preconditioner_aggregate,
+                    "topology per-DOF arrays missing");
+            const int64_t c3 = int64_t(t.brick_size) * t.brick_size * t.brick_size;
+            int64_t expected = 0;
+            for (int l = 0; l < t.level_count; ++l)
+            {
+                const pcfd_level& lev = t.levels[l];
+                require(lev.level_offset == expected, "level_offset does not follow brick order");
+                require(lev.h > 0 && std::isfinite(lev.h), "level cell size must be positive");
+                require(lev.brick_count >= 0 && (lev.brick_count == 0 || (lev.neighbors && lev.flags && lev.coord)),
+                        "level brick arrays missing");
+                for (int b = 0; b < lev.brick_count * 6; ++b)
+                    require(lev.neighbors[b] >= -1 && lev.neighbors[b] < lev.brick_count, "brick neighbour out of range");
+                expected += int64_t(lev.brick_count) * c3;
+            }
+            require(expected <= t.storage_size, "storage_size smaller than the brick slots");
+            require(t.storage_size < (int64_t(1) << 31), "storage_size exceeds 32-bit DOF indexing");
+            auto check_conn = [&](const pcfd_connections& c, const char* what) {
+                for (int e = 0; e < c.count; ++e)
+                    require(c.coarse_dof[e] >= 0 && c.coarse_dof[e] < t.storage_size && c.fine_dof[e] >= 0 &&
+                                c.fine_dof[e] < t.storage_size && c.axis[e] >= 0 && c.axis[e] < 3,
+                            std::string("invalid ") + what + " connection");
+            };
+            check_conn(t.coarse_fine, "coarse/fine");
+            check_conn(t.embedded, "embedded");
+            for (int e = 0; e < t.regular.count; ++e)
+                require(t.regular.lower_dof[e] >= 0 && t.regular.lower_dof[e] < t.storage_size && t.regular.upper_dof[e] >= 0 &&
+                            t.regular.upper_dof[e] < t.storage_size && t.regular.level[e] >= 0 && t.regular.level[e] < t.level_count,
+                        "invalid regular correction");
+            for (int q = 0; q < t.gradient_node_count; ++q)
+                require(t.gradient_dof[q] >= 0 && t.gradient_dof[q] < t.storage_size, "invalid gradient node");
+            if (t.gradient_node_count)
+                for (int q = 0; q < t.gradient_offset[t.gradient_node_count]; ++q)
+                    require(t.gradient_neighbour[q] >= 0 && t.gradient_neighbour[q] < t.storage_size, "invalid gradient neighbour");
+            for (int g = 0; g < t.gauge_count; ++g)
+                require(t.gauge_dof[g] >= 0 && t.gauge_dof[g] < t.storage_size, "invalid gauge");
+        }
+
+        void create(const pcfd_topology& t, const pcfd_options* options, System& s)
+        {
+            validate(t);
+            s.device = options ? options->device : 0;
+            s.mg_precision = options ? options->mg_precision : PCFD_MG_FP64;
+            cuda_check(cudaSetDevice(s.device), "cudaSetDevice");
+            if (options && options->stream) s.stream = static_cast<cudaStream_t>(options->stream);
+            else
+            {
+                cuda_check(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking), "create stream");
+                s.own_stream = true;
+            }
+            s.bs = t.brick_size;
+            s.bs3 = s.bs * s.bs * s.bs;
+            s.levels = t.level_count;
+            s.S = t.storage_size;
+            s.outlet = t.pressure_outlet_xmax != 0;
+            s.full_nonorthogonal = t.gradient_node_count > 0;
+            // brick slots
+            std::vector<int> brick_level, nbr, active_list;
+            std::vector<uint32_t> flags;
+            s.level_h.resize(s.levels);
+            s.level_slot0.resize(s.levels);
+            int slot0 = 0;
+            for (int l = 0; l < s.levels; ++l)
+            {
+                const pcfd_level& lev = t.levels[l];
+                s.level_h[l] = lev.h;
+                s.level_slot0[l] = slot0;
+                for (int b = 0; b < lev.brick_count; ++b)
+                {
+                    brick_level.push_back(l);
+                    flags.push_back(lev.flags[b]);
+                    for (int f = 0; f < 6; ++f)
+                    {
+                        const int n = lev.neighbors[b * 6 + f];
+                        nbr.push_back(n >= 0 && !(lev.flags[n] & PCFD_BRICK_COVERED) ? slot0 + n : -1);
+                    }
+                    if (!(lev.flags[b] & PCFD_BRICK_COVERED)) active_list.push_back(slot0 + b);
+                }
+                slot0 += lev.brick_count;
+            }
+            s.B = slot0;
+            s.structured = s.B * s.bs3;
+            s.faces = int64_t(s.B) * (s.bs + 1) * s.bs * s.bs;
+            s.active_bricks = int(active_list.size());
+            s.brick_level.upload(brick_level);
+            s.brick_nbr.upload(nbr);
+            s.brick_flags.upload(flags);
+            s.active_brick_list.upload(active_list);
+            s.d_level_h.upload(s.level_h);
+            // per DOF
+            s.h_active.assign(t.active, t.active + s.S);
+            s.h_volume.assign(t.volume, t.volume + s.S);
+            s.active.upload(s.h_active);
+            s.cut_face_mask.upload(std::vector<uint8_t>(t.cut_face_mask, t.cut_face_mask + s.S));
+            s.volume.upload(s.h_volume);
+            s.aggregate.upload(std::vector<int>(t.preconditioner_aggregate, t.preconditioner_aggregate + s.S));
+            const std::vector<double> diag = host_diagonal(t);
+            s.diagonal.upload(diag);
+            build_operator(s, t);
+            build_multigrid(s, t, diag);
+            // Krylov storage
+            for (DBuf<double>* v : {&s.r, &s.z, &s.dvec, &s.Ad, &s.t, &s.correction, &s.defect, &s.scratch_p, &s.scratch_out,
+                                     &s.integrated, &s.rhs, &s.pressure})
+                v->alloc(size_t(s.S));
+            if (s.full_nonorthogonal)
+            {
+                s.gmres_v.alloc(size_t(System::gmres_restart + 1) * s.S);
+                s.gmres_z.alloc(size_t(System::gmres_restart) * s.S);
+                s.recycle_u.alloc(size_t(System::recycle_capacity) * s.S);
+                s.recycle_c.alloc(size_t(System::recycle_capacity) * s.S);
+            }
+            s.dot_partial.alloc(4096);
+            s.dot_result.alloc(16);
+            cuda_check(cudaMallocHost(&s.pinned, 16 * sizeof(double)), "pinned scalars");
+            // flow state
+            s.u.alloc(size_t(s.faces)); s.v.alloc(size_t(s.faces)); s.w.alloc(size_t(s.faces));
+            s.divergence.alloc(size_t(s.S));
+            s.pressure32.alloc(size_t(s.S));
+            build_projection(s, t);
+            cuda_check(cudaDeviceSynchronize(), "system setup");
+        }
+
+        System& sys(pcfd_system* p)
+        {
+            require(p != nullptr, "null system");
+            return *reinterpret_cast<System*>(p);
+        }
+
+        template <class T> void h2d(System& s, T* dst, const T* src, size_t n)
+        {
+            require(src != nullptr || n == 0, "null host buffer");
+            if (n) cuda_check(cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyHostToDevice, s.stream), "host to device");
+        }
+        template <class T> void d2h(System& s, T* dst, const T* src, size_t n)
+        {
+            require(dst != nullptr || n == 0, "null host buffer");
+            if (n) cuda_check(cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyDeviceToHost, s.stream), "device to host");
+        }
+        void sync(System& s) { cuda_check(cudaStreamSynchronize(s.stream), "synchronize"); }
+    }
+
+    System::~System()
+    {
+        if (pinned) cudaFreeHost(pinned);
+        if (own_stream && stream) cudaStreamDestroy(stream);
+    }
+}
+
+using namespace pcfd;
+
+extern "C" {
+
+const char* pcfd_last_error_message(void) { return g_error.c_str(); }
+const char* pcfd_version(void) { return "paracfd_b200 0.1 (sm_100a)"; }
+
+pcfd_status pcfd_system_create(const pcfd_topology* topology, const pcfd_options* options, pcfd_system** out)
+{
+    return guarded([&] {
+        require(topology && out, "null topology or output handle");
+        *out = nullptr;
+        auto s = std::make_unique<System>();
+        create(*topology, options, *s);
+        *out = reinterpret_cast<pcfd_system*>(s.release());
+    });
+}
+
+void pcfd_system_destroy(pcfd_system* system)
+{
+    if (!system) return;
+    System* s = reinterpret_cast<System*>(system);
+    cudaStreamSynchronize(s->stream);
+    delete s;
+}
+
+pcfd_status pcfd_system_sizes(const pcfd_system* system, int64_t* storage, int64_t* bricks, int64_t* faces, int64_t* cf, int64_t* eb)
+{
+    return guarded([&] {
+        require(system != nullptr, "null system");
+        const System& s = *reinterpret_cast<const System*>(system);
+        if (storage) *storage = s.S;
+        if (bricks) *bricks = s.B;
+        if (faces) *faces = s.faces;
+        if (cf) *cf = s.cf_count;
+        if (eb) *eb = s.eb_count;
+    });
+}
+
+pcfd_status pcfd_system_synchronize(pcfd_system* system)
+{
+    return guarded([&] { sync(sys(system)); });
+}
+
+pcfd_status pcfd_pressure_apply_host(pcfd_system* system, const double* p, double* out, int32_t orthogonal)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        h2d(s, s.scratch_p.p, p, size_t(s.S));
+        launch_apply(s, s.scratch_p, s.scratch_out, orthogonal != 0);
+        d2h(s, out, s.scratch_out.p, size_t(s.S));
+        sync(s);
+    });
+}
+
+pcfd_status pcfd_pressure_apply_device(pcfd_system* system, const double* d_p, double* d_out, int32_t orthogonal)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(d_p && d_out, "null device vector");
+        launch_apply(s, d_p, d_out, orthogonal != 0);
+    });
+}
+
+pcfd_status pcfd_pressure_diagonal_host(pcfd_system* system, double* diag)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        d2h(s, diag, s.diagonal.p, size_t(s.S));
+        sync(s);
+    });
+}
+
+pcfd_status pcfd_pressure_precondition_host(pcfd_system* system, const double* r, double* z)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        h2d(s, s.scratch_p.p, r, size_t(s.S));
+        apply_preconditioner(s, s.scratch_p, s.scratch_out);
+        d2h(s, z, s.scratch_out.p, size_t(s.S));
+        sync(s);
+    });
+}
+
+pcfd_status pcfd_pressure_solve_host(pcfd_system* system, double* x, const double* b, double tolerance, int32_t max_iterations,
+                                     int32_t warm_start, pcfd_solve_result* result)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(tolerance > 0 && max_iterations >= 0, "invalid solve tolerance or iteration budget");
+        h2d(s, s.scratch_p.p, b, size_t(s.S));
+        if (warm_start) h2d(s, s.scratch_out.p, x, size_t(s.S));
+        const pcfd_solve_result r = solve(s, s.scratch_out, s.scratch_p, tolerance, max_iterations, warm_start != 0);
+        d2h(s, x, s.scratch_out.p, size_t(s.S));
+        sync(s);
+        if (result) *result = r;
+    });
+}
+
+pcfd_status pcfd_set_faces_host(pcfd_system* system, const float* u, const float* v, const float* w)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        h2d(s, s.u.p, u, size_t(s.faces)); h2d(s, s.v.p, v, size_t(s.faces)); h2d(s, s.w.p, w, size_t(s.faces));
+        sync(s);
+    });
+}
+pcfd_status pcfd_get_faces_host(pcfd_system* system, float* u, float* v, float* w)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        d2h(s, u, s.u.p, size_t(s.faces)); d2h(s, v, s.v.p, size_t(s.faces)); d2h(s, w, s.w.p, size_t(s.faces));
+        sync(s);
+    });
+}
+pcfd_status pcfd_set_special_host(pcfd_system* system, const float* cf, const float* eb)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        h2d(s, s.special.p, cf, size_t(s.cf_count));
+        h2d(s, s.special.p + s.cf_count, eb, size_t(s.eb_count));
+        sync(s);
+    });
+}
+pcfd_status pcfd_get_special_host(pcfd_system* system, float* cf, float* eb)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        d2h(s, cf, s.special.p, size_t(s.cf_count));
+        d2h(s, eb, s.special.p + s.cf_count, size_t(s.eb_count));
+        sync(s);
+    });
+}
+pcfd_status pcfd_set_pressure_host(pcfd_system* system, const double* p)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        for (int q = 0; q < s.S; ++q) require(std::isfinite(p[q]), "non-finite pressure state");
+        h2d(s, s.pressure.p, p, size_t(s.S));
+        launch_convert_pressure(s);
+        sync(s);
+    });
+}
+pcfd_status pcfd_get_pressure_host(pcfd_system* system, double* p)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        d2h(s, p, s.pressure.p, size_t(s.S));
+        sync(s);
+    });
+}
+pcfd_status pcfd_get_pressure_shadow_host(pcfd_system* system, float* p32)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        d2h(s, p32, s.pressure32.p, size_t(s.S));
+        sync(s);
+    });
+}
+
+pcfd_status pcfd_projection_divergence_host(pcfd_system* system, float* divergence)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        launch_integrated_flux(s);
+        launch_normalize(s, 0.0, false);
+        if (divergence) d2h(s, divergence, s.divergence.p, size_t(s.S));
+        sync(s);
+    });
+}
+
+pcfd_status pcfd_projection_rhs_host(pcfd_system* system, double rho, double dt, double* rhs)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(rho > 0 && dt > 0, "projection rho/dt must be positive");
+        launch_integrated_flux(s);
+        launch_normalize(s, rho / dt, true);
+        if (rhs) d2h(s, rhs, s.rhs.p, size_t(s.S));
+        sync(s);
+    });
+}
+
+pcfd_status pcfd_projection_correct(pcfd_system* system, double rho, double dt)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(rho > 0 && dt > 0, "projection correction rho/dt must be positive");
+        launch_correct_fluxes(s, rho, dt);
+        sync(s);
+    });
+}
+
+pcfd_status pcfd_projection_project(pcfd_system* system, double rho, double dt, double tolerance, int32_t max_iterations,
+                                    int32_t warm_start, pcfd_solve_result* result)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(rho > 0 && dt > 0, "projection rho/dt must be positive");
+        launch_integrated_flux(s);
+        launch_normalize(s, rho / dt, true);
+        const pcfd_solve_result r = solve(s, s.pressure, s.rhs, tolerance, max_iterations, warm_start != 0);
+        if (r.converged)
+        {
+            launch_convert_pressure(s);
+            launch_correct_fluxes(s, rho, dt);
+            launch_integrated_flux(s);
+            launch_normalize(s, 0.0, false);
+        }
+        sync(s);
+        if (result) *result = r;
+        if (!r.converged) throw Error(PCFD_NOT_CONVERGED, "pressure solve did not reach the tolerance");
+    });
+}
+
+pcfd_status pcfd_time_kernel(pcfd_system* system, int32_t which, int32_t iterations, double* ms_per_launch)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(iterations > 0 && ms_per_launch, "invalid timing request");
+        auto once = [&]() {
+            switch (which)
+            {
+            case 0: launch_apply(s, s.scratch_p, s.scratch_out, false); break;
+            case 1: launch_apply(s, s.scratch_p, s.scratch_out, true); break;
+            case 2: apply_preconditioner(s, s.scratch_p, s.scratch_out); break;
+            case 3: launch_integrated_flux(s); launch_normalize(s, 0.0, false); break;
+            case 4: launch_correct_fluxes(s, 1.0, 1e-3); break;
+            case 5: device_dot(s, s.scratch_p, s.scratch_out); break;
+            default: throw Error(PCFD_INVALID_ARG, "unknown kernel id");
+            }
+        };
+        once();
+        sync(s);
+        cudaEvent_t start, stop;
+        cuda_check(cudaEventCreate(&start), "event");
+        cuda_check(cudaEventCreate(&stop), "event");
+        cuda_check(cudaEventRecord(start, s.stream), "event record");
+        for (int q = 0; q < iterations; ++q) once();
+        cuda_check(cudaEventRecord(stop, s.stream), "event record");
+        cuda_check(cudaEventSynchronize(stop), "event sync");
+        float ms = 0;
+        cuda_check(cudaEventElapsedTime(&ms, start, stop), "event time");
+        cudaEventDestroy(start);
+        cudaEventDestroy(stop);
+        *ms_per_launch = double(ms) / iterations;
+    });
+}
+
+}  // extern "C"

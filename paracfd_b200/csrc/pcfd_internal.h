@@ -1,0 +1,231 @@
+// pcfd_internal.h -- device-resident system state behind the C ABI.
+//
+// Layout in HBM (one allocation per array, all levels concatenated in reference DOF order):
+//   * pressure-DOF vectors: [S] with S = B*bs^3 + appended EB root fragments.  DOF numbering is
+//     the reference's level_offset + brick*bs^3 + (k*bs+j)*bs+i (amr_pressure.cpp:213-216), so a
+//     brick is a contiguous 4 KiB FP64 tile (bs = 8).  Covered-brick slots exist but no kernel
+//     reads or writes them; they stay zero.
+//   * faces: per brick slot the interior MAC faces only, (bs+1)*bs*bs per component (no ghost
+//     ring: 576 floats per brick instead of the reference's 1100, amr_fields.h:20-30).  A face
+//     shared by two same-level bricks is stored in both, as the reference does.
+//   * active brick list: every kernel over bricks is launched over the compact list of
+//     non-covered brick slots of all levels at once (one launch instead of one per level).
+#pragma once
+
+#include "../../include/paracfd_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace pcfd
+{
+    struct Error : std::runtime_error
+    {
+        pcfd_status status;
+        Error(pcfd_status s, const std::string& m) : std::runtime_error(m), status(s) {}
+    };
+
+    inline void cuda_check(cudaError_t e, const char* what)
+    {
+        if (e == cudaSuccess) return;
+        const pcfd_status s = e == cudaErrorMemoryAllocation ? PCFD_OUT_OF_MEMORY : PCFD_CUDA_ERROR;
+        throw Error(s, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+    inline void require(bool ok, const std::string& what)
+    {
+        if (!ok) throw Error(PCFD_INVALID_ARG, what);
+    }
+
+    // Owning device buffer.
+    template <class T> struct DBuf
+    {
+        T* p = nullptr;
+        size_t n = 0;
+        DBuf() = default;
+        DBuf(const DBuf&) = delete;
+        DBuf& operator=(const DBuf&) = delete;
+        DBuf(DBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+        DBuf& operator=(DBuf&& o) noexcept
+        {
+            if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+            return *this;
+        }
+        ~DBuf() { release(); }
+        void release()
+        {
+            if (p) cudaFree(p);
+            p = nullptr;
+            n = 0;
+        }
+        void alloc(size_t count, bool zero = true)
+        {
+            release();
+            n = count;
+            if (!count) return;
+            cuda_check(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
+            if (zero) cuda_check(cudaMemset(p, 0, count * sizeof(T)), "cudaMemset");
+        }
+        void upload(const std::vector<T>& host)
+        {
+            alloc(host.size(), false);
+            if (!host.empty()) cuda_check(cudaMemcpy(p, host.data(), host.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
+        }
+        operator T*() const { return p; }
+    };
+
+    // Compact non-orthogonal / two-point edge set used by the irregular operator gather.
+    struct IrregularOperator
+    {
+        int incident_dofs = 0, connection_count = 0, regular_count = 0;
+        DBuf<int> incident_dof, incident_offset, incident_edge;
+        DBuf<int8_t> incident_sign;
+        // connections (coarse/fine then embedded), geometrically ordered endpoints
+        DBuf<int> conn_lower, conn_upper, conn_lower_node, conn_upper_node;
+        DBuf<double> conn_coefficient, conn_correction, conn_upper_weight, conn_area;
+        // regular corrections
+        DBuf<int> reg_lower, reg_upper, reg_lower_node, reg_upper_node;
+        DBuf<double> reg_coefficient, reg_correction, reg_upper_weight, reg_area, reg_delta;
+        // WLS gradient nodes
+        int gradient_nodes = 0;
+        DBuf<int> grad_dof, grad_offset, grad_neighbour;
+        DBuf<double> grad_weight;
+        DBuf<double> gradient;   // [nodes][3] scratch
+        // gauges
+        int gauges = 0;
+        DBuf<int> gauge_dof;
+        DBuf<double> gauge_coefficient;
+    };
+
+    // One level of the aggregation multigrid (host-built CSR, reference amr_pressure.cu:915-1083).
+    template <class T> struct MgLevel
+    {
+        int cells = 0;
+        DBuf<int> row_offset, neighbour, aggregate, restrict_offset, restrict_dof;
+        DBuf<T> coefficient, diagonal, rhs, x, temporary, residual;
+    };
+
+    struct Scalars;   // device scalar block for the Krylov recurrences
+
+    struct System
+    {
+        // sizes
+        int bs = 0, bs3 = 0, levels = 0, S = 0, B = 0, structured = 0, active_bricks = 0;
+        int64_t faces = 0;   // per component
+        bool outlet = true, full_nonorthogonal = false;
+        int mg_precision = PCFD_MG_FP64;
+        cudaStream_t stream = nullptr;
+        bool own_stream = false;
+        int device = 0;
+
+        // host copies of topology needed after setup
+        std::vector<double> level_h;
+        std::vector<int> level_slot0;           // first brick slot of each level
+        std::vector<uint8_t> h_active;
+        std::vector<double> h_volume;
+        int cf_count = 0, eb_count = 0;
+
+        // per brick slot
+        DBuf<int> brick_level;                  // [B]
+        DBuf<int> brick_nbr;                    // [B][6] active same-level neighbour slot or -1
+        DBuf<uint32_t> brick_flags;             // [B]
+        DBuf<int> active_brick_list;            // [active_bricks]
+        DBuf<double> d_level_h;                 // [levels]
+
+        // per DOF
+        DBuf<uint8_t> active, cut_face_mask;
+        DBuf<double> volume, diagonal;
+        DBuf<int> aggregate;                    // preconditioner aggregate (level-0 DOF)
+
+        IrregularOperator irr;
+
+        // multigrid (FP64 parity mode and FP32 mode share structure)
+        int base_offset = 0, base_cells = 0;
+        DBuf<int> base_restrict_offset, base_restrict_dof;
+        std::vector<MgLevel<double>> mg64;
+        std::vector<MgLevel<float>> mg32;
+        DBuf<float> diagonal32;
+
+        // Krylov vectors
+        DBuf<double> r, z, dvec, Ad, t, correction, defect, scratch_p, scratch_out;
+        DBuf<double> gmres_v, gmres_z, recycle_u, recycle_c;
+        int recycle_count = 0;
+        static constexpr int gmres_restart = 24;
+        static constexpr int recycle_capacity = 3;
+        DBuf<double> dot_partial;               // reduction scratch
+        DBuf<double> dot_result;                // device scalars
+        double* pinned = nullptr;               // pinned host scalars
+
+        // projection state
+        DBuf<float> u, v, w;                    // [faces] each
+        DBuf<float> special;                    // [cf + eb]
+        DBuf<double> special_area, special_factor, special_correction, special_upper_weight;
+        DBuf<int> special_lower, special_upper, special_lower_node, special_upper_node;
+        int special_incident_dofs = 0;
+        DBuf<int> special_incident_dof, special_incident_offset, special_incident_edge;
+        DBuf<int8_t> special_incident_sign;
+        DBuf<double> integrated;                // [S]
+        DBuf<float> divergence;                 // [S]
+        DBuf<double> rhs, pressure;             // [S]
+        DBuf<float> pressure32;                 // [S]
+        // regular correction face addresses (face array index, mirror or -1)
+        DBuf<int64_t> reg_face, reg_mirror;
+        DBuf<int8_t> reg_axis;
+        // coarse/fine tile <-> face synchronisation
+        int cf_groups = 0;
+        DBuf<int64_t> cf_fine_face, cf_group_face;
+        DBuf<int8_t> cf_axis, cf_group_axis;
+        DBuf<int> cf_group_offset, cf_group_member;
+        DBuf<double> cf_group_area;
+
+        ~System();
+    };
+
+    // ---- kernels / launchers (pressure.cu) ----
+    void launch_apply(System& s, const double* p, double* out, bool orthogonal_only);
+    void launch_apply32(System& s, const float* p, float* out);
+    double device_dot(System& s, const double* a, const double* b);
+    void build_operator(System& s, const pcfd_topology& t);
+    void build_multigrid(System& s, const pcfd_topology& t, const std::vector<double>& diagonal);
+    void apply_preconditioner(System& s, const double* r, double* z);
+    pcfd_solve_result solve(System& s, double* x, const double* b, double tolerance, int max_iterations, bool warm);
+    // vector helpers
+    void vec_copy_active(System& s, const double* src, double* dst);
+    void vec_subtract(System& s, double* residual, const double* value);   // r = active ? r - v : 0
+    void vec_axpy_active(System& s, double* y, const double* x, double a);
+    void vec_scaled_copy_active(System& s, double* dst, const double* src, double a);
+    void vec_zero(System& s, double* x);
+    void vec_update_solution_residual(System& s, double* x, double* r, const double* d, const double* Ad, double alpha);
+    void vec_update_direction(System& s, const double* z, double* d, double beta);
+
+    // ---- projection (projection.cu) ----
+    void build_projection(System& s, const pcfd_topology& t);
+    void launch_integrated_flux(System& s);
+    void launch_normalize(System& s, double rho_over_dt, bool with_rhs);
+    void launch_correct_fluxes(System& s, double rho, double dt);
+    void launch_convert_pressure(System& s);
+
+    // face array index helpers (compact per-brick layout)
+    __host__ __device__ inline int64_t u_face(int bs, int64_t slot, int i, int j, int k)
+    {
+        return slot * int64_t((bs + 1) * bs * bs) + int64_t((k * bs + j) * (bs + 1) + i);
+    }
+    __host__ __device__ inline int64_t v_face(int bs, int64_t slot, int i, int j, int k)
+    {
+        return slot * int64_t((bs + 1) * bs * bs) + int64_t((k * (bs + 1) + j) * bs + i);
+    }
+    __host__ __device__ inline int64_t w_face(int bs, int64_t slot, int i, int j, int k)
+    {
+        return slot * int64_t((bs + 1) * bs * bs) + int64_t((k * bs + j) * bs + i);
+    }
+    __host__ __device__ inline int64_t axis_face(int bs, int axis, int64_t slot, int i, int j, int k)
+    {
+        return axis == 0 ? u_face(bs, slot, i, j, k) : (axis == 1 ? v_face(bs, slot, i, j, k) : w_face(bs, slot, i, j, k));
+    }
+
+    constexpr int kThreads = 256;
+    inline int blocks_for(int64_t n, int threads = kThreads) { return int((n + threads - 1) / threads); }
+}

@@ -1,0 +1,501 @@
+// pressure.cu -- FP64 composite pressure operator, deterministic reductions, the
+// reference-structured multigrid preconditioner and the outer Krylov solvers.
+//
+// Operator semantics follow CompositeAmrPressureSystem::apply_cpu / diagonal_cpu
+// (reference src/core/fluid/amr_pressure.cpp:498-543) with FP64 geometry coefficients, and
+// the device operator of src/core/fluid/amr_pressure.cu:72-179, 825-834 (structured 7-point
+// FV Laplacian + deterministic per-DOF incidence gather of the compact edges + WLS
+// non-orthogonal correction + gauges).  The B200 design differs in how the work is laid out:
+// one CTA per active 8^3 brick stages the FP64 pressure tile and its six face halos in shared
+// memory (coalesced 16-byte loads), so every brick is read from HBM once per apply and the
+// per-level launch loop and the output memset of the reference disappear.
+#include "pcfd_internal.h"
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <numeric>
+#include <unordered_map>
+
+namespace pcfd
+{
+    // ==================================================================================
+    // structured operator
+    // ==================================================================================
+    namespace
+    {
+        // Shared-memory staged 7-point apply for bs = 8.  Tile index (k+1)*100+(j+1)*10+(i+1).
+        template <class T>
+        __global__ void __launch_bounds__(256) structured_apply8_kernel(
+            const int* __restrict__ brick_list, const int* __restrict__ brick_level,
+            const int* __restrict__ nbr, const uint32_t* __restrict__ flags,
+            const double* __restrict__ level_h, const uint8_t* __restrict__ active,
+            const uint8_t* __restrict__ cut, const T* __restrict__ p, T* __restrict__ out, int outlet)
+        {
+            constexpr int BS = 8, N = 10, C3 = 512;
+            __shared__ T tile[N * N * N];
+            __shared__ uint8_t act[N * N * N];
+            __shared__ uint8_t cm[N * N * N];
+            const int slot = brick_list[blockIdx.x];
+            const int tid = threadIdx.x;
+            const int64_t base = int64_t(slot) * C3;
+            // interior: 512 values, 2 per thread
+            for (int c = tid; c < C3; c += 256)
+            {
+                const int i = c & 7, j = (c >> 3) & 7, k = c >> 6;
+                const int s = (k + 1) * 100 + (j + 1) * 10 + (i + 1);
+                tile[s] = p[base + c];
+                act[s] = active[base + c];
+                cm[s] = cut[base + c];
+            }
+            // halos: 6 faces x 64 cells
+            for (int e = tid; e < 6 * 64; e += 256)
+            {
+                const int face = e >> 6, a = e & 7, b = (e >> 3) & 7;
+                const int axis = face >> 1, positive = face & 1;
+                int i, j, k, hi, hj, hk;   // neighbour-local cell and halo tile position
+                const int inner = positive ? 0 : BS - 1, halo = positive ? BS + 1 : 0;
+                if (axis == 0) { i = inner; j = a; k = b; hi = halo; hj = a + 1; hk = b + 1; }
+                else if (axis == 1) { i = a; j = inner; k = b; hi = a + 1; hj = halo; hk = b + 1; }
+                else { i = a; j = b; k = inner; hi = a + 1; hj = b + 1; hk = halo; }
+                const int s = hk * 100 + hj * 10 + hi;
+                const int n = nbr[slot * 6 + face];
+                if (n >= 0)
+                {
+                    const int64_t q = int64_t(n) * C3 + (k * BS + j) * BS + i;
+                    tile[s] = p[q];
+                    act[s] = active[q];
+                    cm[s] = cut[q];
+                }
+                else
+                {
+                    tile[s] = T(0);
+                    act[s] = 0;
+                    cm[s] = 0;
+                }
+            }
+            __syncthreads();
+            const T h = T(level_h[brick_level[slot]]);
+            const bool xmax = outlet && (flags[slot] & PCFD_BRICK_XMAX);
+            for (int c = tid; c < C3; c += 256)
+            {
+                const int i = c & 7, j = (c >> 3) & 7, k = c >> 6;
+                const int s = (k + 1) * 100 + (j + 1) * 10 + (i + 1);
+                T value = T(0);
+                if (act[s])
+                {
+                    const T pa = tile[s];
+                    const uint8_t mine = cm[s];
+                    // -x, +x, -y, +y, -z, +z ; the lower cell of the face owns its cut bit
+                    if (act[s - 1] && !(cm[s - 1] & 1)) value += h * (pa - tile[s - 1]);
+                    if (act[s + 1] && !(mine & 1)) value += h * (pa - tile[s + 1]);
+                    if (act[s - 10] && !(cm[s - 10] & 2)) value += h * (pa - tile[s - 10]);
+                    if (act[s + 10] && !(mine & 2)) value += h * (pa - tile[s + 10]);
+                    if (act[s - 100] && !(cm[s - 100] & 4)) value += h * (pa - tile[s - 100]);
+                    if (act[s + 100] && !(mine & 4)) value += h * (pa - tile[s + 100]);
+                    if (xmax && i == BS - 1) value += T(2) * h * pa;
+                }
+                out[base + c] = value;
+            }
+        }
+
+        // Generic brick size (one thread per cell, global loads).
+        template <class T>
+        __global__ void structured_apply_generic_kernel(
+            const int* __restrict__ brick_list, int brick_count, int bs, const int* __restrict__ brick_level,
+            const int* __restrict__ nbr, const uint32_t* __restrict__ flags, const double* __restrict__ level_h,
+            const uint8_t* __restrict__ active, const uint8_t* __restrict__ cut, const T* __restrict__ p,
+            T* __restrict__ out, int outlet)
+        {
+            const int c3 = bs * bs * bs;
+            const int64_t work = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+            if (work >= int64_t(brick_count) * c3) return;
+            const int slot = brick_list[work / c3], local = int(work % c3);
+            const int i = local % bs, j = (local / bs) % bs, k = local / (bs * bs);
+            const int64_t a = int64_t(slot) * c3 + local;
+            if (!active[a]) { out[a] = T(0); return; }
+            const T h = T(level_h[brick_level[slot]]);
+            T value = T(0);
+            const int coord[3] = {i, j, k};
+            for (int axis = 0; axis < 3; ++axis)
+                for (int sign = -1; sign <= 1; sign += 2)
+                {
+                    int q[3] = {i, j, k};
+                    q[axis] += sign;
+                    int64_t b = -1;
+                    if (q[axis] >= 0 && q[axis] < bs) b = int64_t(slot) * c3 + (q[2] * bs + q[1]) * bs + q[0];
+                    else
+                    {
+                        const int n = nbr[slot * 6 + 2 * axis + (sign > 0)];
+                        if (n >= 0) { q[axis] = sign > 0 ? 0 : bs - 1; b = int64_t(n) * c3 + (q[2] * bs + q[1]) * bs + q[0]; }
+                    }
+                    const int64_t lower = sign > 0 ? a : b;
+                    if (b >= 0 && active[b] && !(cut[lower] & (1u << axis))) value += h * (p[a] - p[b]);
+                }
+            if (outlet && (flags[slot] & PCFD_BRICK_XMAX) && coord[0] == bs - 1) value += T(2) * h * p[a];
+            out[a] = value;
+        }
+
+        __global__ void zero_range_kernel(double* x, int64_t begin, int64_t end)
+        {
+            const int64_t q = begin + int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+            if (q < end) x[q] = 0.0;
+        }
+
+        // Deterministic per-DOF gather of the compact two-point edges (connections first, then
+        // regular corrections), reference amr_pressure.cu:105-134 with FP64 coefficients.
+        __global__ void irregular_orthogonal_gather_kernel(
+            const int* __restrict__ incident_dof, const int* __restrict__ incident_offset,
+            const int* __restrict__ incident_edge, const int8_t* __restrict__ incident_sign, int incident_dofs,
+            int connection_count, const int* __restrict__ conn_lower, const int* __restrict__ conn_upper,
+            const double* __restrict__ conn_coefficient, const int* __restrict__ reg_lower,
+            const int* __restrict__ reg_upper, const double* __restrict__ reg_coefficient,
+            const uint8_t* __restrict__ active, const double* __restrict__ p, double* __restrict__ out)
+        {
+            const int node = blockIdx.x * blockDim.x + threadIdx.x;
+            if (node >= incident_dofs) return;
+            double sum = 0.0;
+            for (int q = incident_offset[node]; q < incident_offset[node + 1]; ++q)
+            {
+                const int e = incident_edge[q];
+                int a, b;
+                double coefficient;
+                if (e < connection_count) { a = conn_lower[e]; b = conn_upper[e]; coefficient = conn_coefficient[e]; }
+                else { const int r = e - connection_count; a = reg_lower[r]; b = reg_upper[r]; coefficient = reg_coefficient[r]; }
+                if (active[a] && active[b]) sum += double(incident_sign[q]) * (coefficient * (p[a] - p[b]));
+            }
+            out[incident_dof[node]] += sum;
+        }
+
+        __global__ void reconstruct_gradient_kernel(const int* __restrict__ dof, const int* __restrict__ offset,
+            const int* __restrict__ neighbour, const double* __restrict__ weight, const double* __restrict__ p,
+            double* __restrict__ gradient, int nodes)
+        {
+            const int node = blockIdx.x * blockDim.x + threadIdx.x;
+            if (node >= nodes) return;
+            const double centre = p[dof[node]];
+            double gx = 0, gy = 0, gz = 0;
+            for (int q = offset[node]; q < offset[node + 1]; ++q)
+            {
+                const double d = p[neighbour[q]] - centre;
+                gx += weight[3 * q] * d;
+                gy += weight[3 * q + 1] * d;
+                gz += weight[3 * q + 2] * d;
+            }
+            gradient[3 * node] = gx;
+            gradient[3 * node + 1] = gy;
+            gradient[3 * node + 2] = gz;
+        }
+
+        __device__ inline double face_derivative(const double* gradient, int lower_node, int upper_node,
+                                                 const double* correction, double upper_weight)
+        {
+            const double lw = 1.0 - upper_weight;
+            double derivative = 0.0;
+            for (int c = 0; c < 3; ++c)
+                derivative += correction[c] * (lw * gradient[3 * lower_node + c] + upper_weight * gradient[3 * upper_node + c]);
+            return derivative;
+        }
+
+        // WLS affine-exact non-orthogonal correction gather (amr_pressure.cu:135-178).
+        __global__ void irregular_nonorthogonal_gather_kernel(
+            const int* __restrict__ incident_dof, const int* __restrict__ incident_offset,
+            const int* __restrict__ incident_edge, const int8_t* __restrict__ incident_sign, int incident_dofs,
+            int connection_count, const int* __restrict__ conn_lower, const int* __restrict__ conn_upper,
+            const int* __restrict__ conn_lower_node, const int* __restrict__ conn_upper_node,
+            const double* __restrict__ conn_correction, const double* __restrict__ conn_upper_weight,
+            const double* __restrict__ conn_area, const int* __restrict__ reg_lower, const int* __restrict__ reg_upper,
+            const int* __restrict__ reg_lower_node, const int* __restrict__ reg_upper_node,
+            const double* __restrict__ reg_correction, const double* __restrict__ reg_upper_weight,
+            const double* __restrict__ reg_area, const double* __restrict__ gradient,
+            const uint8_t* __restrict__ active, double* __restrict__ out)
+        {
+            const int node = blockIdx.x * blockDim.x + threadIdx.x;
+            if (node >= incident_dofs) return;
+            double sum = 0.0;
+            for (int q = incident_offset[node]; q < incident_offset[node + 1]; ++q)
+            {
+                const int e = incident_edge[q];
+                int a, b, ln, un;
+                const double* corr;
+                double uw, area;
+                if (e < connection_count)
+                {
+                    a = conn_lower[e]; b = conn_upper[e]; ln = conn_lower_node[e]; un = conn_upper_node[e];
+                    corr = conn_correction + 3 * e; uw = conn_upper_weight[e]; area = conn_area[e];
+                }
+                else
+                {
+                    const int r = e - connection_count;
+                    a = reg_lower[r]; b = reg_upper[r]; ln = reg_lower_node[r]; un = reg_upper_node[r];
+                    corr = reg_correction + 3 * r; uw = reg_upper_weight[r]; area = reg_area[r];
+                }
+                if (!active[a] || !active[b] || ln < 0 || un < 0) continue;
+                const double flux = -area * face_derivative(gradient, ln, un, corr, uw);
+                sum += double(incident_sign[q]) * flux;
+            }
+            out[incident_dof[node]] += sum;
+        }
+
+        __global__ void gauge_apply_kernel(const int* dof, const double* coefficient, int count, const double* p, double* out)
+        {
+            const int q = blockIdx.x * blockDim.x + threadIdx.x;
+            if (q < count) out[dof[q]] += coefficient[q] * p[dof[q]];
+        }
+    }
+
+    void launch_apply(System& s, const double* p, double* out, bool orthogonal_only)
+    {
+        if (s.active_bricks)
+        {
+            if (s.bs == 8)
+                structured_apply8_kernel<double><<<s.active_bricks, 256, 0, s.stream>>>(
+                    s.active_brick_list, s.brick_level, s.brick_nbr, s.brick_flags, s.d_level_h, s.active,
+                    s.cut_face_mask, p, out, s.outlet ? 1 : 0);
+            else
+                structured_apply_generic_kernel<double><<<blocks_for(int64_t(s.active_bricks) * s.bs3), kThreads, 0, s.stream>>>(
+                    s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr, s.brick_flags, s.d_level_h,
+                    s.active, s.cut_face_mask, p, out, s.outlet ? 1 : 0);
+        }
+        if (s.S > s.structured)
+            zero_range_kernel<<<blocks_for(s.S - s.structured), kThreads, 0, s.stream>>>(out, s.structured, s.S);
+        IrregularOperator& o = s.irr;
+        if (o.incident_dofs)
+            irregular_orthogonal_gather_kernel<<<blocks_for(o.incident_dofs), kThreads, 0, s.stream>>>(
+                o.incident_dof, o.incident_offset, o.incident_edge, o.incident_sign, o.incident_dofs, o.connection_count,
+                o.conn_lower, o.conn_upper, o.conn_coefficient, o.reg_lower, o.reg_upper, o.reg_coefficient, s.active, p, out);
+        if (o.gauges)
+            gauge_apply_kernel<<<blocks_for(o.gauges), kThreads, 0, s.stream>>>(o.gauge_dof, o.gauge_coefficient, o.gauges, p, out);
+        if (!orthogonal_only && o.gradient_nodes)
+        {
+            reconstruct_gradient_kernel<<<blocks_for(o.gradient_nodes), kThreads, 0, s.stream>>>(
+                o.grad_dof, o.grad_offset, o.grad_neighbour, o.grad_weight, p, o.gradient, o.gradient_nodes);
+            if (o.incident_dofs)
+                irregular_nonorthogonal_gather_kernel<<<blocks_for(o.incident_dofs), kThreads, 0, s.stream>>>(
+                    o.incident_dof, o.incident_offset, o.incident_edge, o.incident_sign, o.incident_dofs, o.connection_count,
+                    o.conn_lower, o.conn_upper, o.conn_lower_node, o.conn_upper_node, o.conn_correction, o.conn_upper_weight,
+                    o.conn_area, o.reg_lower, o.reg_upper, o.reg_lower_node, o.reg_upper_node, o.reg_correction,
+                    o.reg_upper_weight, o.reg_area, o.gradient, s.active, out);
+        }
+        cuda_check(cudaGetLastError(), "launch pressure operator");
+    }
+
+    // ==================================================================================
+    // deterministic FP64 reductions
+    // ==================================================================================
+    namespace
+    {
+        constexpr int kDotBlocks = 592;   // 4 x 148 SMs, fixed so the summation order never changes
+
+        __device__ inline double warp_sum(double v)
+        {
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            return v;
+        }
+        __device__ inline double block_sum(double v, double* shared)
+        {
+            v = warp_sum(v);
+            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+            if (lane == 0) shared[warp] = v;
+            __syncthreads();
+            v = threadIdx.x < (blockDim.x >> 5) ? shared[threadIdx.x] : 0.0;
+            if (warp == 0) v = warp_sum(v);
+            return v;
+        }
+        __global__ void __launch_bounds__(256) dot_partial_kernel(const double* __restrict__ a, const double* __restrict__ b,
+            const uint8_t* __restrict__ active, int64_t n, double* __restrict__ partial)
+        {
+            __shared__ double shared[8];
+            double v = 0.0;
+            for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += int64_t(gridDim.x) * blockDim.x)
+                if (active[q]) v += a[q] * b[q];
+            v = block_sum(v, shared);
+            if (threadIdx.x == 0) partial[blockIdx.x] = v;
+        }
+        __global__ void __launch_bounds__(256) dot_final_kernel(const double* __restrict__ partial, int count, double* __restrict__ result)
+        {
+            __shared__ double shared[8];
+            double v = 0.0;
+            for (int q = threadIdx.x; q < count; q += blockDim.x) v += partial[q];
+            v = block_sum(v, shared);
+            if (threadIdx.x == 0) *result = v;
+        }
+    }
+
+    double device_dot(System& s, const double* a, const double* b)
+    {
+        dot_partial_kernel<<<kDotBlocks, 256, 0, s.stream>>>(a, b, s.active, s.S, s.dot_partial);
+        dot_final_kernel<<<1, 256, 0, s.stream>>>(s.dot_partial, kDotBlocks, s.dot_result);
+        cuda_check(cudaMemcpyAsync(s.pinned, s.dot_result, sizeof(double), cudaMemcpyDeviceToHost, s.stream), "dot readback");
+        cuda_check(cudaStreamSynchronize(s.stream), "dot synchronize");
+        return s.pinned[0];
+    }
+
+    // ==================================================================================
+    // vector kernels (active-masked, reference amr_pressure.cu:180-199)
+    // ==================================================================================
+    namespace
+    {
+        __global__ void copy_active_kernel(const double* src, double* dst, const uint8_t* active, int64_t n)
+        {
+            const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+            if (q < n) dst[q] = active[q] ? src[q] : 0.0;
+        }
+        __global__ void subtract_kernel(double* r, const double* v, const uint8_t* active, int64_t n)
+        {
+            const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+            if (q < n) r[q] = active[q] ? r[q] - v[q] : 0.0;
+        }
+        __global__ void axpy_active_kernel(double* y, const double* x, double a, const uint8_t* active, int64_t n)
+        {
+            const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+            if (q < n && active[q]) y[q] += a * x[q];
+        }
+        __global__ void scaled_copy_active_kernel(double* dst, const double* src, double a, const uint8_t* active, int64_t n)
+        {
+            const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+            if (q < n) dst[q] = active[q] ? a * src[q] : 0.0;
+        }
+        __global__ void update_solution_residual_kernel(double* x, double* r, const double* d, const double* Ad, double alpha,
+                                                        const uint8_t* active, int64_t n)
+        {
+            const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+            if (q < n && active[q]) { x[q] += alpha * d[q]; r[q] -= alpha * Ad[q]; }
+        }
+        __global__ void update_direction_kernel(const double* z, double* d, double beta, const uint8_t* active, int64_t n)
+        {
+            const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+            if (q < n) d[q] = active[q] ? z[q] + beta * d[q] : 0.0;
+        }
+    }
+    void vec_copy_active(System& s, const double* src, double* dst)
+    {
+        copy_active_kernel<<<blocks_for(s.S), kThreads, 0, s.stream>>>(src, dst, s.active, s.S);
+    }
+    void vec_subtract(System& s, double* r, const double* v)
+    {
+        subtract_kernel<<<blocks_for(s.S), kThreads, 0, s.stream>>>(r, v, s.active, s.S);
+    }
+    void vec_axpy_active(System& s, double* y, const double* x, double a)
+    {
+        axpy_active_kernel<<<blocks_for(s.S), kThreads, 0, s.stream>>>(y, x, a, s.active, s.S);
+    }
+    void vec_scaled_copy_active(System& s, double* dst, const double* src, double a)
+    {
+        scaled_copy_active_kernel<<<blocks_for(s.S), kThreads, 0, s.stream>>>(dst, src, a, s.active, s.S);
+    }
+    void vec_update_solution_residual(System& s, double* x, double* r, const double* d, const double* Ad, double alpha)
+    {
+        update_solution_residual_kernel<<<blocks_for(s.S), kThreads, 0, s.stream>>>(x, r, d, Ad, alpha, s.active, s.S);
+    }
+    void vec_update_direction(System& s, const double* z, double* d, double beta)
+    {
+        update_direction_kernel<<<blocks_for(s.S), kThreads, 0, s.stream>>>(z, d, beta, s.active, s.S);
+    }
+    void vec_zero(System& s, double* x)
+    {
+        cuda_check(cudaMemsetAsync(x, 0, size_t(s.S) * sizeof(double), s.stream), "zero vector");
+    }
+
+    // ==================================================================================
+    // operator setup (host)
+    // ==================================================================================
+    namespace
+    {
+        double gradient_factor(const pcfd_connections& c, int e)
+        {
+            // pressure_gradient_factor (amr_pressure.h:122-126)
+            const double f = c.orthogonal_gradient_factor[e];
+            return f > 0 ? f : (c.normal_distance[e] > 0 ? 1.0 / c.normal_distance[e] : 0.0);
+        }
+    }
+
+    void build_operator(System& s, const pcfd_topology& t)
+    {
+        IrregularOperator& o = s.irr;
+        const int cf = t.coarse_fine.count, eb = t.embedded.count, nc = cf + eb;
+        o.connection_count = nc;
+        std::vector<int> lower(nc), upper(nc), lnode(nc), unode(nc);
+        std::vector<double> coefficient(nc), correction(size_t(nc) * 3), weight(nc), area(nc);
+        for (int e = 0; e < nc; ++e)
+        {
+            const pcfd_connections& c = e < cf ? t.coarse_fine : t.embedded;
+            const int q = e < cf ? e : e - cf;
+            const bool forward = c.direction[q] > 0;
+            lower[e] = forward ? c.coarse_dof[q] : c.fine_dof[q];
+            upper[e] = forward ? c.fine_dof[q] : c.coarse_dof[q];
+            coefficient[e] = c.open_area[q] * gradient_factor(c, q);
+            lnode[e] = c.lower_gradient_node[q];
+            unode[e] = c.upper_gradient_node[q];
+            for (int a = 0; a < 3; ++a) correction[3 * e + a] = c.nonorthogonal_correction[3 * q + a];
+            weight[e] = c.upper_gradient_weight[q];
+            area[e] = c.open_area[q];
+        }
+        o.conn_lower.upload(lower); o.conn_upper.upload(upper); o.conn_coefficient.upload(coefficient);
+        o.conn_lower_node.upload(lnode); o.conn_upper_node.upload(unode); o.conn_correction.upload(correction);
+        o.conn_upper_weight.upload(weight); o.conn_area.upload(area);
+
+        const pcfd_regular_corrections& rc = t.regular;
+        o.regular_count = rc.count;
+        std::vector<int> rl(rc.count), ru(rc.count), rln(rc.count), run(rc.count);
+        std::vector<double> rcoef(rc.count), rcorr(size_t(rc.count) * 3), rw(rc.count), ra(rc.count), rd(rc.count);
+        for (int e = 0; e < rc.count; ++e)
+        {
+            rl[e] = rc.lower_dof[e]; ru[e] = rc.upper_dof[e];
+            rln[e] = rc.lower_gradient_node[e]; run[e] = rc.upper_gradient_node[e];
+            rcoef[e] = rc.open_area[e] * rc.two_point_delta[e];
+            for (int a = 0; a < 3; ++a) rcorr[3 * e + a] = rc.nonorthogonal_correction[3 * e + a];
+            rw[e] = rc.upper_gradient_weight[e]; ra[e] = rc.open_area[e]; rd[e] = rc.two_point_delta[e];
+        }
+        o.reg_lower.upload(rl); o.reg_upper.upload(ru); o.reg_lower_node.upload(rln); o.reg_upper_node.upload(run);
+        o.reg_coefficient.upload(rcoef); o.reg_correction.upload(rcorr); o.reg_upper_weight.upload(rw);
+        o.reg_area.upload(ra); o.reg_delta.upload(rd);
+
+        // Deterministic incidence: (dof, edge, sign) sorted, reference amr_pressure.cu:774-813.
+        struct Incident { int dof, edge; int8_t sign; };
+        std::vector<Incident> inc;
+        inc.reserve(size_t(2) * (nc + rc.count));
+        auto add = [&](int a, int b, int encoded) {
+            if (a < 0 || b < 0 || a >= s.S || b >= s.S || a == b || !t.active[a] || !t.active[b]) return;
+            inc.push_back({a, encoded, 1});
+            inc.push_back({b, encoded, -1});
+        };
+        for (int e = 0; e < nc; ++e) add(lower[e], upper[e], e);
+        for (int e = 0; e < rc.count; ++e) add(rl[e], ru[e], nc + e);
+        std::sort(inc.begin(), inc.end(), [](const Incident& a, const Incident& b) {
+            if (a.dof != b.dof) return a.dof < b.dof;
+            if (a.edge != b.edge) return a.edge < b.edge;
+            return a.sign < b.sign;
+        });
+        std::vector<int> idof, ioff, iedge;
+        std::vector<int8_t> isign;
+        for (size_t q = 0; q < inc.size(); ++q)
+        {
+            if (q == 0 || inc[q].dof != inc[q - 1].dof) { idof.push_back(inc[q].dof); ioff.push_back(int(q)); }
+            iedge.push_back(inc[q].edge);
+            isign.push_back(inc[q].sign);
+        }
+        ioff.push_back(int(inc.size()));
+        o.incident_dofs = int(idof.size());
+        o.incident_dof.upload(idof); o.incident_offset.upload(ioff); o.incident_edge.upload(iedge); o.incident_sign.upload(isign);
+
+        o.gradient_nodes = t.gradient_node_count;
+        if (o.gradient_nodes)
+        {
+            const int nnz = t.gradient_offset[o.gradient_nodes];
+            o.grad_dof.upload(std::vector<int>(t.gradient_dof, t.gradient_dof + o.gradient_nodes));
+            o.grad_offset.upload(std::vector<int>(t.gradient_offset, t.gradient_offset + o.gradient_nodes + 1));
+            o.grad_neighbour.upload(std::vector<int>(t.gradient_neighbour, t.gradient_neighbour + nnz));
+            o.grad_weight.upload(std::vector<double>(t.gradient_weight, t.gradient_weight + size_t(nnz) * 3));
+            o.gradient.alloc(size_t(o.gradient_nodes) * 3);
+        }
+        o.gauges = t.gauge_count;
+        if (o.gauges)
+        {
+            o.gauge_dof.upload(std::vector<int>(t.gauge_dof, t.gauge_dof + o.gauges));
+            o.gauge_coefficient.upload(std::vector<double>(t.gauge_coefficient, t.gauge_coefficient + o.gauges));
+        }
+    }
+}
