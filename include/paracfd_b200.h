@@ -169,6 +169,7 @@ typedef struct pcfd_options {
     int32_t mg_precision;            /* pcfd_mg_precision */
     int32_t device;                  /* CUDA device ordinal */
     void* stream;                    /* cudaStream_t or NULL for a library-owned stream */
+    double momentum_min_volume_fraction; /* AmrConfig::min_volume_fraction (small-cell groups) */
 } pcfd_options;
 
 /* AmrGpuSolveResult (amr_pressure.h:337-351), trimmed to what the solver reports. */
@@ -179,6 +180,37 @@ typedef struct pcfd_solve_result {
     int32_t preconditioner_applications;
     int32_t recycle_rejections;
 } pcfd_solve_result;
+
+/* Physical case and solver settings used by the time step (ParagliderConfig's freestream and
+ * solver blocks, src/core/paraglider_config.h:10-58, and ExternalAeroExecutionOptions,
+ * src/core/fluid/external_aero_core.h:106-120). */
+typedef struct pcfd_case {
+    double speed;                    /* freestream speed along +X [m/s] */
+    double rho;                      /* density [kg/m^3] */
+    double nu;                       /* kinematic viscosity [m^2/s] */
+    double cfl;
+    double smagorinsky_cs;
+    double projection_tolerance;     /* relative residual of the pressure solve */
+    int32_t projection_max_iterations;
+    int32_t smooth_wall;             /* apply the Spalding smooth-wall model */
+    int32_t pressure_impulse;        /* apply the projected pressure traction to cell momentum */
+} pcfd_case;
+
+/* ExternalAeroStepStats (external_aero_core.h:61-83), device-timed. */
+typedef struct pcfd_step_stats {
+    double dt;
+    double physical_time;
+    double max_abs_velocity;         /* max |cell velocity component| before the step */
+    double max_abs_special_velocity; /* max |2:1 tile or EB aperture velocity| before the step */
+    double max_outflow_rate;         /* conservative CFL rate [1/s] */
+    double cfl_velocity;
+    double effective_cfl;
+    double max_diffusion_rate;
+    int32_t diffusion_substeps;
+    pcfd_solve_result pressure;
+    double step_ms;                  /* CUDA-event time of the whole step on the system stream */
+    double projection_ms;
+} pcfd_step_stats;
 
 typedef struct pcfd_system pcfd_system;
 
@@ -234,6 +266,38 @@ pcfd_status pcfd_projection_correct(pcfd_system* system, double rho, double dt);
 pcfd_status pcfd_projection_project(pcfd_system* system, double rho, double dt, double tolerance,
                                     int32_t max_iterations, int32_t warm_start,
                                     pcfd_solve_result* result);
+
+/* ---- cell momentum (DeviceCompositeCellMomentumTransport, amr_advection.h:269-405) ---------- */
+/* Collocated FP32 control-volume velocity [S] per component. */
+pcfd_status pcfd_momentum_set_state_host(pcfd_system* system, const float* x, const float* y, const float* z);
+pcfd_status pcfd_momentum_get_state_host(pcfd_system* system, float* x, float* y, float* z);
+/* MUSCL/minmod conservative transport (step, amr_advection.h:292-293). */
+pcfd_status pcfd_momentum_transport(pcfd_system* system, double dt, double freestream_speed, int32_t external_aero);
+/* Smagorinsky viscosity + sub-cycled explicit diffusion (diffuse_smagorinsky, amr_advection.h:297). */
+pcfd_status pcfd_momentum_smagorinsky(pcfd_system* system, double nu, double cs, double dt, double* rate,
+                                      int32_t* substeps);
+/* Implicit Spalding smooth wall (apply_smooth_fabric_wall_model, amr_advection.h:300). */
+pcfd_status pcfd_momentum_smooth_wall(pcfd_system* system, double dt, double nu);
+/* Per wall side (patch plus side, then minus side, in patch order) force/density [3*sides]. */
+pcfd_status pcfd_momentum_wall_forces_host(pcfd_system* system, float* force_per_density, int64_t* sides);
+/* Pressure traction of the resident FP32 pressure shadow (apply_projected_pressure_gradient,
+ * amr_advection.h:304; physical_boundaries=0 gives apply_pressure_impulse(...,false)). */
+pcfd_status pcfd_momentum_pressure_impulse(pcfd_system* system, double dt, double rho, int32_t physical_boundaries,
+                                           int32_t redistribute);
+/* Cell -> face normal velocities (reconstruct_fluxes, amr_advection.h:307). */
+pcfd_status pcfd_momentum_reconstruct_fluxes(pcfd_system* system);
+/* External aerodynamic face conditions (DeviceAmrFields::apply_external_aero_boundaries, amr_fields.h:63). */
+pcfd_status pcfd_apply_external_boundaries(pcfd_system* system, double freestream_speed);
+/* out[0] max |cell velocity|, out[1] max outflow rate [1/s], out[2] max |special velocity|. */
+pcfd_status pcfd_momentum_cfl(pcfd_system* system, int32_t external_aero, double out[3]);
+
+/* ---- time step (ExternalAeroCore, external_aero_core.h:124-182) ------------------------------ */
+pcfd_status pcfd_core_configure(pcfd_system* system, const pcfd_case* config);
+/* Freestream state, reconstruction, first projection (ExternalAeroCore::initialize). */
+pcfd_status pcfd_core_initialize(pcfd_system* system, pcfd_step_stats* stats);
+/* One time step (ExternalAeroCore::step): CFL, transport, LES diffusion, wall, reconstruction,
+ * boundaries, projection, pressure traction.  Time advances only when the solve converged. */
+pcfd_status pcfd_core_step(pcfd_system* system, pcfd_step_stats* stats);
 
 /* ---- instrumentation ---------------------------------------------------------------------- */
 /* Average device time of one launch sequence of `which` (0 full apply, 1 orthogonal apply,

@@ -29,6 +29,12 @@ class CaseParams(C.Structure):
                 ("wake_radius", C.c_double), ("min_volume_fraction", C.c_double)]
 
 
+class CoreCase(C.Structure):
+    _fields_ = [("speed", C.c_double), ("rho", C.c_double), ("nu", C.c_double), ("cfl", C.c_double),
+                ("smagorinsky_cs", C.c_double), ("projection_tolerance", C.c_double),
+                ("projection_max_iterations", C.c_int32)]
+
+
 _lib = None
 
 
@@ -57,6 +63,20 @@ def lib():
         L.ref_rhs_cpu.argtypes = [vp, f32p, f32p, f32p, f64p, f64p, C.c_double, C.c_double, f64p]
         L.ref_correct_fluxes_cpu.argtypes = [vp, f64p, C.c_double, C.c_double, f32p, f32p, f32p, f64p, f64p]
         L.ref_pressure_gradients_cpu.argtypes = [vp, f64p, f64p]
+        L.ref_transport_cpu.argtypes = [vp, f32p, f32p, f32p, f64p, f64p, C.c_double, C.c_int, C.c_double, f32p, f32p, f32p]
+        L.ref_smagorinsky_viscosity_cpu.argtypes = [vp, f32p, f32p, f32p, C.c_double, C.c_double, f64p]
+        L.ref_diffuse_smagorinsky_cpu.argtypes = [vp, C.c_double, C.c_double, C.c_double, f32p, f32p, f32p]
+        L.ref_diffuse_cpu.argtypes = [vp, C.c_double, C.c_double, f32p, f32p, f32p]
+        L.ref_wall_cpu.argtypes = [vp, C.c_double, C.c_double, C.c_double, f32p, f32p, f32p, f64p, C.POINTER(C.c_int64)]
+        L.ref_impulse_cpu.argtypes = [vp, f64p, C.c_double, C.c_double, C.c_int, f32p, f32p, f32p]
+        L.ref_reconstruct_cpu.argtypes = [vp, f32p, f32p, f32p, f32p, f32p, f32p, f64p, f64p]
+        L.ref_outflow_rate_cpu.argtypes = [vp, f32p, f32p, f32p, f64p, f64p, C.c_int, f64p]
+        L.ref_core_create.restype = vp
+        L.ref_core_create.argtypes = [vp, C.POINTER(CoreCase)]
+        L.ref_core_destroy.argtypes = [vp]
+        L.ref_core_initialize.argtypes = [vp, f64p]
+        L.ref_core_step.argtypes = [vp, f64p]
+        L.ref_core_state.argtypes = [vp, f32p, f32p, f32p, f64p]
         _lib = L
     return _lib
 
@@ -146,6 +166,105 @@ class RefCase:
         _check(lib().ref_pressure_gradients_cpu(self.handle, ptr(np.ascontiguousarray(pressure, np.float64), C.c_double),
                                                 ptr(out, C.c_double)))
         return out
+
+
+    # ---- cell-momentum host twins (state arrays are copied; new arrays returned) -------------
+    @staticmethod
+    def _state(x, y, z):
+        return tuple(np.array(a, np.float32) for a in (x, y, z))
+
+    def transport(self, u, v, w, cf, eb, dt, state, external=False, freestream=0.0):
+        x, y, z = self._state(*state)
+        _check(lib().ref_transport_cpu(self.handle, ptr(u, C.c_float), ptr(v, C.c_float), ptr(w, C.c_float),
+                                       ptr(np.asarray(cf, np.float64), C.c_double), ptr(np.asarray(eb, np.float64), C.c_double),
+                                       dt, int(external), freestream, ptr(x, C.c_float), ptr(y, C.c_float), ptr(z, C.c_float)))
+        return x, y, z
+
+    def smagorinsky_viscosity(self, state, nu, cs):
+        x, y, z = self._state(*state)
+        out = np.zeros(self.n)
+        _check(lib().ref_smagorinsky_viscosity_cpu(self.handle, ptr(x, C.c_float), ptr(y, C.c_float), ptr(z, C.c_float), nu, cs,
+                                                   ptr(out, C.c_double)))
+        return out
+
+    def diffuse_smagorinsky(self, state, nu, cs, dt):
+        x, y, z = self._state(*state)
+        _check(lib().ref_diffuse_smagorinsky_cpu(self.handle, nu, cs, dt, ptr(x, C.c_float), ptr(y, C.c_float), ptr(z, C.c_float)))
+        return x, y, z
+
+    def wall(self, state, nu, dt, rho):
+        x, y, z = self._state(*state)
+        sides = C.c_int64()
+        forces = np.zeros(6 * max(1, self.summary["patches"]))
+        _check(lib().ref_wall_cpu(self.handle, nu, dt, rho, ptr(x, C.c_float), ptr(y, C.c_float), ptr(z, C.c_float),
+                                  ptr(forces, C.c_double), C.byref(sides)))
+        return (x, y, z), forces[: 3 * sides.value].reshape(-1, 3)
+
+    def impulse(self, pressure, dt, rho, state, physical=True):
+        x, y, z = self._state(*state)
+        _check(lib().ref_impulse_cpu(self.handle, ptr(np.ascontiguousarray(pressure, np.float64), C.c_double), dt, rho, int(physical),
+                                     ptr(x, C.c_float), ptr(y, C.c_float), ptr(z, C.c_float)))
+        return x, y, z
+
+    def reconstruct(self, state, u, v, w):
+        x, y, z = self._state(*state)
+        u, v, w = (np.array(a, np.float32) for a in (u, v, w))
+        cf = np.zeros(self.summary["coarse_fine"])
+        eb = np.zeros(self.summary["embedded"])
+        _check(lib().ref_reconstruct_cpu(self.handle, ptr(x, C.c_float), ptr(y, C.c_float), ptr(z, C.c_float), ptr(u, C.c_float),
+                                         ptr(v, C.c_float), ptr(w, C.c_float), ptr(cf, C.c_double), ptr(eb, C.c_double)))
+        return u, v, w, cf, eb
+
+    def outflow_rate(self, u, v, w, cf, eb, external=True):
+        out = C.c_double()
+        _check(lib().ref_outflow_rate_cpu(self.handle, ptr(u, C.c_float), ptr(v, C.c_float), ptr(w, C.c_float),
+                                          ptr(np.asarray(cf, np.float64), C.c_double), ptr(np.asarray(eb, np.float64), C.c_double),
+                                          int(external), C.byref(out)))
+        return out.value
+
+
+class RefCore:
+    """The reference's own ExternalAeroCore (its CUDA path) on a fixture; needs a GPU."""
+
+    def __init__(self, case: RefCase, speed=10.0, rho=1.225, nu=1.5e-5, cfl=0.5, cs=0.10, tolerance=1e-8, max_iterations=600):
+        self.case = case
+        cfg = CoreCase(speed, rho, nu, cfl, cs, tolerance, max_iterations)
+        self.handle = lib().ref_core_create(case.handle, C.byref(cfg))
+        if not self.handle:
+            raise RuntimeError("reference core: " + lib().ref_last_error().decode(errors="replace"))
+
+    @staticmethod
+    def _stats(a):
+        return {"dt": a[0], "gpu_step_ms": a[1], "projection_ms": a[2], "iterations": int(a[3]), "converged": bool(a[4]),
+                "relative_residual": a[5]}
+
+    def initialize(self):
+        a = np.zeros(6)
+        _check(lib().ref_core_initialize(self.handle, ptr(a, C.c_double)))
+        return self._stats(a)
+
+    def step(self):
+        a = np.zeros(6)
+        _check(lib().ref_core_step(self.handle, ptr(a, C.c_double)))
+        return self._stats(a)
+
+    def state(self):
+        n = self.case.n
+        x, y, z = (np.zeros(n, np.float32) for _ in range(3))
+        p = np.zeros(n)
+        _check(lib().ref_core_state(self.handle, ptr(x, C.c_float), ptr(y, C.c_float), ptr(z, C.c_float), ptr(p, C.c_double)))
+        return (x, y, z), p
+
+    def close(self):
+        if self.handle:
+            lib().ref_core_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def box_case(**kw) -> RefCase:

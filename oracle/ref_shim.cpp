@@ -8,6 +8,8 @@
 
 #include "core/fluid/amr_eb.h"
 #include "core/fluid/amr_pressure.h"
+#include "core/fluid/amr_advection.h"
+#include "core/fluid/external_aero_core.h"
 #include "core/geometry/mesh_clip.h"
 #include "core/geometry/model_placement.h"
 #include "core/paraglider_config.h"
@@ -546,7 +548,15 @@ void* ref_case_create(const ref_case_params* p)
             const double a = p->aoa_deg * std::acos(-1.0) / 180.0;
             place.cos_a = std::cos(a); place.sin_a = std::sin(a);
             place.pivot_x = 0.25 * p->chord; place.pivot_z = 0;
-            for (int q = 0; q < 3; ++q) { domain.lo[q] = p->domain_lo[q]; domain.hi[q] = p->domain_hi[q]; }
+            // centre the placed section vertically on z = 0
+            double zmin = 1e300, zmax = -1e300, xmin = 1e300, xmax = -1e300;
+            for (const auto& pt : poly)
+            {
+                double wx, wz;
+                place.to_world(pt[0], pt[1], wx, wz);
+                zmin = std::min(zmin, wz); zmax = std::max(zmax, wz); xmin = std::min(xmin, wx); xmax = std::max(xmax, wx);
+            }
+            place.tz = -0.5 * (zmin + zmax);
             const bool slab = p->kind == REF_CASE_NACA_SLAB;
             const double half_span = 0.5 * p->span;
             if (slab)
@@ -554,7 +564,7 @@ void* ref_case_create(const ref_case_params* p)
                 // Section extruded beyond the slab and clipped at the side walls (slip walls
                 // meet the solid): same construction as the reference's cropped contract.
                 TriMesh longer = extruded_mesh(poly, place, -half_span - 0.5, half_span + 0.5, true);
-                c.wing = clip_mesh_to_axis_slab(longer, 1, domain.lo.y, domain.hi.y);
+                c.wing = clip_mesh_to_axis_slab(longer, 1, p->domain_lo[1], p->domain_hi[1]);
                 c.solid = std::make_shared<ExtrudedSection>(poly, place, -1e9, 1e9, false);
             }
             else
@@ -562,6 +572,15 @@ void* ref_case_create(const ref_case_params* p)
                 c.wing = extruded_mesh(poly, place, -half_span, half_span, true);
                 c.solid = std::make_shared<ExtrudedSection>(poly, place, -half_span, half_span, true);
             }
+            // Express the requested box as the reference's automatic-domain margins so that
+            // ExternalAeroCore, which always derives its domain from them, builds this grid too.
+            config.domain.upstream_margin = double(c.wing.bbox_min[0]) - p->domain_lo[0];
+            // (1e-9 short of the box so the brick-count ceil cannot round up by one brick)
+            config.domain.downstream_margin = p->domain_hi[0] - double(c.wing.bbox_max[0]) - 1e-9;
+            config.domain.lateral_margin = slab ? 0.0 : 0.5 * ((p->domain_hi[1] - p->domain_lo[1]) - (double(c.wing.bbox_max[1]) - double(c.wing.bbox_min[1])) - 1e-9);
+            config.domain.vertical_margin = 0.5 * ((p->domain_hi[2] - p->domain_lo[2]) - (double(c.wing.bbox_max[2]) - double(c.wing.bbox_min[2])) - 1e-9);
+            config.domain.half_wing_symmetry = false;
+            domain = automatic_flow_domain(c.wing, config.domain);
         }
         c.bvh = std::make_unique<TriangleBvh>(c.wing);
         c.hierarchy = AmrHierarchy::build_static(domain, c.wing, *c.bvh, config.amr, config.domain.half_wing_symmetry);
@@ -730,6 +749,179 @@ int ref_pressure_gradients_cpu(void* handle, const double* pressure, double* gra
         const auto g = composite_pressure_gradients_cpu(c.system, p);
         for (std::size_t q = 0; q < g.size(); ++q)
             for (int a = 0; a < 3; ++a) gradient3[3 * q + a] = g[q][a];
+    });
+}
+
+
+}  // extern "C"
+
+namespace
+{
+    CompositeCellMomentumState state_from(const RefCase& c, const float* x, const float* y, const float* z)
+    {
+        CompositeCellMomentumState st;
+        const int n = c.system.storage_size;
+        st.x.assign(x, x + n); st.y.assign(y, y + n); st.z.assign(z, z + n);
+        return st;
+    }
+    void state_to(const CompositeCellMomentumState& st, float* x, float* y, float* z)
+    {
+        std::copy(st.x.begin(), st.x.end(), x); std::copy(st.y.begin(), st.y.end(), y); std::copy(st.z.begin(), st.z.end(), z);
+    }
+    struct RefCore
+    {
+        RefCase* owner = nullptr;
+        std::unique_ptr<ExternalAeroCore> core;
+    };
+    void fill_stats(const ExternalAeroStepStats& s, double* o)
+    {
+        o[0] = s.dt; o[1] = s.gpu_step_ms; o[2] = s.projection_ms; o[3] = s.pressure.iterations;
+        o[4] = s.pressure.converged ? 1 : 0; o[5] = s.pressure.relative_residual;
+    }
+}
+
+extern "C" {
+
+int ref_transport_cpu(void* handle, const float* u, const float* v, const float* w, const double* cf, const double* eb,
+                      double dt, int external, double freestream, float* x, float* y, float* z)
+{
+    return guarded([&] {
+        RefCase& c = *static_cast<RefCase*>(handle);
+        AmrHostFields fields(c.hierarchy);
+        to_host_fields(c, u, v, w, fields);
+        CompositeCellMomentumState st = state_from(c, x, y, z);
+        conservative_composite_cell_momentum_cpu(c.system, fields, special_from(c, cf, eb), dt, st, external != 0, freestream);
+        state_to(st, x, y, z);
+    });
+}
+
+int ref_smagorinsky_viscosity_cpu(void* handle, const float* x, const float* y, const float* z, double nu, double cs, double* viscosity)
+{
+    return guarded([&] {
+        RefCase& c = *static_cast<RefCase*>(handle);
+        const auto vis = composite_cell_smagorinsky_viscosity_cpu(c.system, state_from(c, x, y, z), nu, cs);
+        std::copy(vis.begin(), vis.end(), viscosity);
+    });
+}
+
+int ref_diffuse_smagorinsky_cpu(void* handle, double nu, double cs, double dt, float* x, float* y, float* z)
+{
+    return guarded([&] {
+        RefCase& c = *static_cast<RefCase*>(handle);
+        CompositeCellMomentumState st = state_from(c, x, y, z);
+        diffuse_composite_cell_momentum_smagorinsky_cpu(c.system, nu, cs, dt, st);
+        state_to(st, x, y, z);
+    });
+}
+
+int ref_diffuse_cpu(void* handle, double nu, double dt, float* x, float* y, float* z)
+{
+    return guarded([&] {
+        RefCase& c = *static_cast<RefCase*>(handle);
+        CompositeCellMomentumState st = state_from(c, x, y, z);
+        diffuse_composite_cell_momentum_cpu(c.system, nu, dt, st);
+        state_to(st, x, y, z);
+    });
+}
+
+int ref_wall_cpu(void* handle, double nu, double dt, double rho, float* x, float* y, float* z, double* forces, int64_t* sides)
+{
+    return guarded([&] {
+        RefCase& c = *static_cast<RefCase*>(handle);
+        CompositeCellMomentumState st = state_from(c, x, y, z);
+        const auto loads = apply_composite_cell_smooth_fabric_wall_cpu(c.system, nu, dt, rho, st);
+        state_to(st, x, y, z);
+        if (sides) *sides = int64_t(loads.size());
+        if (forces)
+            for (std::size_t q = 0; q < loads.size(); ++q)
+                for (int a = 0; a < 3; ++a) forces[3 * q + a] = loads[q].force[a];
+    });
+}
+
+int ref_impulse_cpu(void* handle, const double* pressure, double dt, double rho, int physical, float* x, float* y, float* z)
+{
+    return guarded([&] {
+        RefCase& c = *static_cast<RefCase*>(handle);
+        CompositeCellMomentumState st = state_from(c, x, y, z);
+        std::vector<double> p(pressure, pressure + c.system.storage_size);
+        apply_composite_cell_pressure_impulse_cpu(c.system, p, dt, rho, st, physical != 0);
+        state_to(st, x, y, z);
+    });
+}
+
+int ref_reconstruct_cpu(void* handle, const float* x, const float* y, const float* z, float* u, float* v, float* w, double* cf, double* eb)
+{
+    return guarded([&] {
+        RefCase& c = *static_cast<RefCase*>(handle);
+        AmrHostFields fields(c.hierarchy);
+        to_host_fields(c, u, v, w, fields);
+        CompositeAmrFluxes fluxes;
+        reconstruct_composite_cell_fluxes_cpu(c.system, state_from(c, x, y, z), fields, fluxes);
+        from_host_fields(c, fields, u, v, w);
+        if (cf) std::copy(fluxes.coarse_fine_velocity.begin(), fluxes.coarse_fine_velocity.end(), cf);
+        if (eb) std::copy(fluxes.embedded_velocity.begin(), fluxes.embedded_velocity.end(), eb);
+    });
+}
+
+int ref_outflow_rate_cpu(void* handle, const float* u, const float* v, const float* w, const double* cf, const double* eb,
+                         int external, double* rate)
+{
+    return guarded([&] {
+        RefCase& c = *static_cast<RefCase*>(handle);
+        AmrHostFields fields(c.hierarchy);
+        to_host_fields(c, u, v, w, fields);
+        *rate = composite_cell_max_outflow_rate_cpu(c.system, fields, special_from(c, cf, eb), external != 0);
+    });
+}
+
+void* ref_core_create(void* case_handle, const ref_core_case* cfg)
+{
+    RefCore* out = nullptr;
+    guarded([&] {
+        RefCase& c = *static_cast<RefCase*>(case_handle);
+        auto core = std::make_unique<RefCore>();
+        core->owner = &c;
+        ParagliderConfig config = c.config;
+        config.freestream.speed = cfg->speed;
+        config.freestream.rho = cfg->rho;
+        config.freestream.nu = cfg->nu;
+        config.solver.cfl = cfg->cfl;
+        config.solver.smagorinsky_cs = cfg->smagorinsky_cs;
+        config.solver.projection_tolerance = cfg->projection_tolerance;
+        config.solver.projection_max_iterations = cfg->projection_max_iterations;
+        ExternalAeroExecutionOptions options;
+        options.closed_solid = c.solid;
+        core->core = std::make_unique<ExternalAeroCore>(c.wing, *c.bvh, config, options);
+        out = core.release();
+    });
+    return out;
+}
+
+void ref_core_destroy(void* core) { delete static_cast<RefCore*>(core); }
+
+int ref_core_initialize(void* core, double* stats)
+{
+    return guarded([&] { fill_stats(static_cast<RefCore*>(core)->core->initialize(), stats); });
+}
+
+int ref_core_step(void* core, double* stats)
+{
+    return guarded([&] { fill_stats(static_cast<RefCore*>(core)->core->step(), stats); });
+}
+
+int ref_core_state(void* core, float* x, float* y, float* z, double* pressure)
+{
+    return guarded([&] {
+        ExternalAeroCore& c = *static_cast<RefCore*>(core)->core;
+        CompositeCellMomentumState st;
+        if (!c.download_cell_momentum_state(st)) throw std::runtime_error("reference core has no cell momentum");
+        state_to(st, x, y, z);
+        if (pressure)
+        {
+            std::vector<double> p;
+            c.download_pressure(p);
+            std::copy(p.begin(), p.end(), pressure);
+        }
     });
 }
 

@@ -57,6 +57,37 @@ int ref_correct_fluxes_cpu(void* handle, const double* pressure, double rho, dou
                            float* u, float* v, float* w, double* cf, double* eb);
 int ref_pressure_gradients_cpu(void* handle, const double* pressure, double* gradient3);
 
+/* Cell-momentum host twins (reference amr_advection.cu:874-1100).  State x,y,z: FP32 [S], in/out. */
+int ref_transport_cpu(void* handle, const float* u, const float* v, const float* w, const double* cf,
+                      const double* eb, double dt, int external, double freestream, float* x, float* y, float* z);
+int ref_smagorinsky_viscosity_cpu(void* handle, const float* x, const float* y, const float* z, double nu,
+                                  double cs, double* viscosity);
+int ref_diffuse_smagorinsky_cpu(void* handle, double nu, double cs, double dt, float* x, float* y, float* z);
+int ref_diffuse_cpu(void* handle, double nu, double dt, float* x, float* y, float* z);
+/* forces: 3 per wall side in patch order (plus side then minus side); returns side count in *sides */
+int ref_wall_cpu(void* handle, double nu, double dt, double rho, float* x, float* y, float* z, double* forces,
+                 int64_t* sides);
+int ref_impulse_cpu(void* handle, const double* pressure, double dt, double rho, int physical, float* x, float* y,
+                    float* z);
+/* faces (compact layout) and special velocities are outputs; faces start from the given values */
+int ref_reconstruct_cpu(void* handle, const float* x, const float* y, const float* z, float* u, float* v, float* w,
+                        double* cf, double* eb);
+int ref_outflow_rate_cpu(void* handle, const float* u, const float* v, const float* w, const double* cf,
+                         const double* eb, int external, double* rate);
+
+/* The reference's own GPU path (ExternalAeroCore on the fixture), for the sm_100a baseline arm. */
+typedef struct ref_core_case {
+    double speed, rho, nu, cfl, smagorinsky_cs, projection_tolerance;
+    int32_t projection_max_iterations;
+} ref_core_case;
+void* ref_core_create(void* case_handle, const ref_core_case* config);
+void ref_core_destroy(void* core);
+/* stats: [dt, gpu_step_ms, projection_ms, iterations, converged, residual] */
+int ref_core_initialize(void* core, double* stats6);
+int ref_core_step(void* core, double* stats6);
+/* Cell-momentum state [S] (FP32) and the FP32 pressure shadow widened to double [S]. */
+int ref_core_state(void* core, float* x, float* y, float* z, double* pressure);
+
 #ifdef __cplusplus
 }
 #endif

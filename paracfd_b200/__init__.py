@@ -20,10 +20,11 @@ MG_FP64, MG_FP32 = 0, 1
 class CompositeSystem:
     """Resident topology + state on one GPU (one host thread at a time)."""
 
-    def __init__(self, topology: Topology, mg_precision: int = MG_FP64, device: int = 0):
+    def __init__(self, topology: Topology, mg_precision: int = MG_FP64, device: int = 0,
+                 momentum_min_volume_fraction: float = 0.0):
         self._lib = capi.load()
         self._topology = topology   # keep the caller's arrays alive during creation
-        opts = Options(mg_precision, device, None)
+        opts = Options(mg_precision, device, None, momentum_min_volume_fraction)
         handle = C.c_void_p()
         check(self._lib.pcfd_system_create(C.byref(topology), C.byref(opts), C.byref(handle)))
         self.handle = handle
@@ -141,3 +142,65 @@ class CompositeSystem:
         if status not in (capi.PCFD_OK, 3):   # 3 = NOT_CONVERGED is reported in the result
             check(status)
         return res.as_dict()
+
+    # ---- cell momentum ---------------------------------------------------------------------------
+    def set_state(self, x, y, z):
+        x, y, z = (self._vec(a, np.float32) for a in (x, y, z))
+        check(self._lib.pcfd_momentum_set_state_host(self.handle, ptr(x, C.c_float), ptr(y, C.c_float), ptr(z, C.c_float)))
+
+    def get_state(self):
+        x, y, z = (np.empty(self.storage_size, np.float32) for _ in range(3))
+        check(self._lib.pcfd_momentum_get_state_host(self.handle, ptr(x, C.c_float), ptr(y, C.c_float), ptr(z, C.c_float)))
+        return x, y, z
+
+    def transport(self, dt: float, freestream: float = 0.0, external_aero: bool = False):
+        check(self._lib.pcfd_momentum_transport(self.handle, dt, freestream, int(external_aero)))
+
+    def smagorinsky(self, nu: float, cs: float, dt: float):
+        rate, sub = C.c_double(), C.c_int32()
+        check(self._lib.pcfd_momentum_smagorinsky(self.handle, nu, cs, dt, C.byref(rate), C.byref(sub)))
+        return rate.value, sub.value
+
+    def smooth_wall(self, dt: float, nu: float):
+        check(self._lib.pcfd_momentum_smooth_wall(self.handle, dt, nu))
+
+    def wall_forces(self) -> np.ndarray:
+        sides = C.c_int64()
+        check(self._lib.pcfd_momentum_wall_forces_host(self.handle, ptr(None, C.c_float), C.byref(sides)))
+        out = np.empty(3 * sides.value, np.float32)
+        check(self._lib.pcfd_momentum_wall_forces_host(self.handle, ptr(out, C.c_float), C.byref(sides)))
+        return out.reshape(-1, 3)
+
+    def pressure_impulse(self, dt: float, rho: float, physical_boundaries: bool = True, redistribute: bool = True):
+        check(self._lib.pcfd_momentum_pressure_impulse(self.handle, dt, rho, int(physical_boundaries), int(redistribute)))
+
+    def reconstruct_fluxes(self):
+        check(self._lib.pcfd_momentum_reconstruct_fluxes(self.handle))
+
+    def apply_external_boundaries(self, speed: float):
+        check(self._lib.pcfd_apply_external_boundaries(self.handle, speed))
+
+    def cfl(self, external_aero: bool = True):
+        out = np.zeros(3)
+        check(self._lib.pcfd_momentum_cfl(self.handle, int(external_aero), ptr(out, C.c_double)))
+        return {"max_abs_velocity": out[0], "max_outflow_rate": out[1], "max_abs_special_velocity": out[2]}
+
+    # ---- time step (ExternalAeroCore surface) --------------------------------------------------
+    def configure(self, speed=10.0, rho=1.225, nu=1.5e-5, cfl=0.5, smagorinsky_cs=0.10,
+                  projection_tolerance=1e-8, projection_max_iterations=600, smooth_wall=True,
+                  pressure_impulse=True):
+        case = capi.Case(speed, rho, nu, cfl, smagorinsky_cs, projection_tolerance, projection_max_iterations,
+                         int(smooth_wall), int(pressure_impulse))
+        check(self._lib.pcfd_core_configure(self.handle, C.byref(case)))
+
+    def initialize(self) -> dict:
+        stats = capi.StepStats()
+        check(self._lib.pcfd_core_initialize(self.handle, C.byref(stats)))
+        return stats.as_dict()
+
+    def step(self) -> dict:
+        stats = capi.StepStats()
+        status = self._lib.pcfd_core_step(self.handle, C.byref(stats))
+        if status not in (capi.PCFD_OK, 3):
+            check(status)
+        return stats.as_dict()

@@ -80,7 +80,8 @@ class Topology(C.Structure):
 
 
 class Options(C.Structure):
-    _fields_ = [("mg_precision", C.c_int32), ("device", C.c_int32), ("stream", C.c_void_p)]
+    _fields_ = [("mg_precision", C.c_int32), ("device", C.c_int32), ("stream", C.c_void_p),
+                ("momentum_min_volume_fraction", C.c_double)]
 
 
 class SolveResult(C.Structure):
@@ -93,6 +94,26 @@ class SolveResult(C.Structure):
                 "converged": bool(self.converged),
                 "preconditioner_applications": self.preconditioner_applications,
                 "recycle_rejections": self.recycle_rejections}
+
+
+class Case(C.Structure):
+    _fields_ = [("speed", C.c_double), ("rho", C.c_double), ("nu", C.c_double), ("cfl", C.c_double),
+                ("smagorinsky_cs", C.c_double), ("projection_tolerance", C.c_double),
+                ("projection_max_iterations", C.c_int32), ("smooth_wall", C.c_int32),
+                ("pressure_impulse", C.c_int32)]
+
+
+class StepStats(C.Structure):
+    _fields_ = [("dt", C.c_double), ("physical_time", C.c_double), ("max_abs_velocity", C.c_double),
+                ("max_abs_special_velocity", C.c_double), ("max_outflow_rate", C.c_double),
+                ("cfl_velocity", C.c_double), ("effective_cfl", C.c_double),
+                ("max_diffusion_rate", C.c_double), ("diffusion_substeps", C.c_int32),
+                ("pressure", SolveResult), ("step_ms", C.c_double), ("projection_ms", C.c_double)]
+
+    def as_dict(self):
+        out = {name: getattr(self, name) for name, _ in self._fields_ if name != "pressure"}
+        out["pressure"] = self.pressure.as_dict()
+        return out
 
 
 def ptr(array: np.ndarray | None, ctype):
@@ -131,6 +152,20 @@ SIGNATURES = {
     "pcfd_projection_project": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double,
                                           C.c_int32, C.c_int32, C.POINTER(SolveResult)]),
     "pcfd_time_kernel": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
+    "pcfd_momentum_set_state_host": (C.c_int, [C.c_void_p, _f32p, _f32p, _f32p]),
+    "pcfd_momentum_get_state_host": (C.c_int, [C.c_void_p, _f32p, _f32p, _f32p]),
+    "pcfd_momentum_transport": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_int32]),
+    "pcfd_momentum_smagorinsky": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double,
+                                            C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
+    "pcfd_momentum_smooth_wall": (C.c_int, [C.c_void_p, C.c_double, C.c_double]),
+    "pcfd_momentum_wall_forces_host": (C.c_int, [C.c_void_p, _f32p, C.POINTER(C.c_int64)]),
+    "pcfd_momentum_pressure_impulse": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_int32, C.c_int32]),
+    "pcfd_momentum_reconstruct_fluxes": (C.c_int, [C.c_void_p]),
+    "pcfd_apply_external_boundaries": (C.c_int, [C.c_void_p, C.c_double]),
+    "pcfd_momentum_cfl": (C.c_int, [C.c_void_p, C.c_int32, _f64p]),
+    "pcfd_core_configure": (C.c_int, [C.c_void_p, C.POINTER(Case)]),
+    "pcfd_core_initialize": (C.c_int, [C.c_void_p, C.POINTER(StepStats)]),
+    "pcfd_core_step": (C.c_int, [C.c_void_p, C.POINTER(StepStats)]),
 }
 
 _lib = None

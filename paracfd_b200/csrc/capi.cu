@@ -1,7 +1,7 @@
 // capi.cu -- the extern "C" boundary (include/paracfd_b200.h): topology validation and upload,
 // resident state transfer, and the projection entry points.  Every entry point converts C++
 // exceptions into a status code plus a thread-local message; no exception crosses the ABI.
-#include "pcfd_internal.h"
+#include "momentum.h"
 
 #include <cmath>
 #include <cstring>
@@ -206,6 +206,11 @@ namespace pcfd
             s.divergence.alloc(size_t(s.S));
             s.pressure32.alloc(size_t(s.S));
             build_projection(s, t);
+            s.h_connected = t.freestream_connected ? std::vector<uint8_t>(t.freestream_connected, t.freestream_connected + s.S)
+                                                   : s.h_active;
+            s.h_finest = t.levels[t.level_count - 1].h;
+            s.momentum = new Momentum();
+            build_momentum(s, *s.momentum, t, options ? options->momentum_min_volume_fraction : 0.0);
             cuda_check(cudaDeviceSynchronize(), "system setup");
         }
 
@@ -230,6 +235,7 @@ namespace pcfd
 
     System::~System()
     {
+        delete momentum;
         if (pinned) cudaFreeHost(pinned);
         if (own_stream && stream) cudaStreamDestroy(stream);
     }
@@ -447,6 +453,153 @@ pcfd_status pcfd_projection_project(pcfd_system* system, double rho, double dt, 
         sync(s);
         if (result) *result = r;
         if (!r.converged) throw Error(PCFD_NOT_CONVERGED, "pressure solve did not reach the tolerance");
+    });
+}
+
+pcfd_status pcfd_momentum_set_state_host(pcfd_system* system, const float* x, const float* y, const float* z)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        Momentum& m = momentum_of(s);
+        h2d(s, m.x.p, x, size_t(s.S)); h2d(s, m.y.p, y, size_t(s.S)); h2d(s, m.z.p, z, size_t(s.S));
+        h2d(s, m.xn.p, x, size_t(s.S)); h2d(s, m.yn.p, y, size_t(s.S)); h2d(s, m.zn.p, z, size_t(s.S));
+        sync(s);
+    });
+}
+
+pcfd_status pcfd_momentum_get_state_host(pcfd_system* system, float* x, float* y, float* z)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        Momentum& m = momentum_of(s);
+        d2h(s, x, m.x.p, size_t(s.S)); d2h(s, y, m.y.p, size_t(s.S)); d2h(s, z, m.z.p, size_t(s.S));
+        sync(s);
+    });
+}
+
+pcfd_status pcfd_momentum_transport(pcfd_system* system, double dt, double freestream_speed, int32_t external_aero)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(dt > 0 && freestream_speed >= 0, "invalid cell momentum timestep");
+        momentum_transport(s, momentum_of(s), float(dt), float(freestream_speed), external_aero != 0);
+        sync(s);
+    });
+}
+
+pcfd_status pcfd_momentum_smagorinsky(pcfd_system* system, double nu, double cs, double dt, double* rate, int32_t* substeps)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(nu >= 0 && cs >= 0 && dt > 0, "invalid Smagorinsky timestep");
+        Momentum& m = momentum_of(s);
+        const double r = momentum_smagorinsky(s, m, float(nu), float(cs), float(dt));
+        sync(s);
+        if (rate) *rate = r;
+        if (substeps) *substeps = m.last_substeps;
+    });
+}
+
+pcfd_status pcfd_momentum_smooth_wall(pcfd_system* system, double dt, double nu)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(dt > 0 && nu > 0, "invalid smooth-wall timestep");
+        momentum_wall(s, momentum_of(s), float(dt), float(nu));
+        sync(s);
+    });
+}
+
+pcfd_status pcfd_momentum_wall_forces_host(pcfd_system* system, float* force, int64_t* sides)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        Momentum& m = momentum_of(s);
+        if (sides) *sides = m.nW;
+        if (force) d2h(s, force, m.w_force.p, size_t(m.nW) * 3);
+        sync(s);
+    });
+}
+
+pcfd_status pcfd_momentum_pressure_impulse(pcfd_system* system, double dt, double rho, int32_t physical_boundaries, int32_t redistribute)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(dt > 0 && rho > 0, "invalid pressure impulse");
+        Momentum& m = momentum_of(s);
+        const int groups = m.nG;
+        if (!redistribute) m.nG = 0;
+        try { momentum_pressure_impulse(s, m, float(dt), float(rho), physical_boundaries != 0); }
+        catch (...) { m.nG = groups; throw; }
+        m.nG = groups;
+        sync(s);
+    });
+}
+
+pcfd_status pcfd_momentum_reconstruct_fluxes(pcfd_system* system)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        momentum_reconstruct_fluxes(s, momentum_of(s));
+        sync(s);
+    });
+}
+
+pcfd_status pcfd_apply_external_boundaries(pcfd_system* system, double speed)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        momentum_external_boundaries(s, float(speed));
+        sync(s);
+    });
+}
+
+pcfd_status pcfd_momentum_cfl(pcfd_system* system, int32_t external_aero, double out[3])
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(out != nullptr, "null output");
+        float r[4];
+        momentum_cfl(s, momentum_of(s), external_aero != 0, r);
+        for (int q = 0; q < 3; ++q) out[q] = r[q];
+    });
+}
+
+pcfd_status pcfd_core_configure(pcfd_system* system, const pcfd_case* config)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(config != nullptr, "null case");
+        const pcfd_case& c = *config;
+        require(c.speed >= 0 && c.rho > 0 && c.nu >= 0 && c.cfl > 0 && c.smagorinsky_cs >= 0 && c.projection_tolerance > 0 &&
+                    c.projection_max_iterations > 0,
+                "invalid case configuration");
+        s.config = c;
+        s.configured = true;
+        s.initialized = false;
+        s.physical_time = 0.0;
+    });
+}
+
+pcfd_status pcfd_core_initialize(pcfd_system* system, pcfd_step_stats* stats)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        pcfd_step_stats local;
+        core_initialize(s, local);
+        if (stats) *stats = local;
+        if (!s.initialized) throw Error(PCFD_NOT_CONVERGED, "initial projection did not converge");
+    });
+}
+
+pcfd_status pcfd_core_step(pcfd_system* system, pcfd_step_stats* stats)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        pcfd_step_stats local;
+        core_step(s, local);
+        if (stats) *stats = local;
+        if (!local.pressure.converged) throw Error(PCFD_NOT_CONVERGED, "pressure solve did not converge; time not advanced");
     });
 }
 

@@ -1,0 +1,145 @@
+// core.cu -- time-step orchestration (ExternalAeroCore::initialize / step, reference
+// src/core/fluid/external_aero_core.cpp:245-328) and the momentum entry points of the C ABI.
+//
+// Differences by design: every stage is enqueued on one stream with no device-wide syncs; the
+// only host reads inside a step are the fused CFL reduction (4 floats), the diffusion spectral
+// rate (1 float) and the Krylov scalars of the pressure solve.
+#include "momentum.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace pcfd
+{
+    namespace
+    {
+        thread_local std::string* g_core_error = nullptr;
+
+        __global__ void init_state_kernel(const uint8_t* active, const uint8_t* connected, int64_t n, float speed, float* x, float* y,
+                                          float* z, float* xn, float* yn, float* zn)
+        {
+            const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+            if (q >= n) return;
+            const float vx = active[q] && connected[q] ? speed : 0.0f;
+            x[q] = xn[q] = vx;
+            y[q] = yn[q] = 0.0f;
+            z[q] = zn[q] = 0.0f;
+        }
+
+        // X-boundary faces of the initial state: freestream where the adjacent CV is connected.
+        __global__ void init_x_boundary_kernel(const int* brick_list, int nbricks, int bs, const uint32_t* flags, const uint8_t* active,
+                                               const uint8_t* connected, float speed, float* u)
+        {
+            const int64_t work = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+            if (work >= int64_t(nbricks) * bs * bs) return;
+            const int slot = brick_list[work / (bs * bs)], r = int(work % (bs * bs)), j = r % bs, k = r / bs;
+            const uint32_t fl = flags[slot];
+            const int64_t base = int64_t(slot) * bs * bs * bs + (k * bs + j) * bs;
+            if (fl & PCFD_BRICK_XMIN) { const int64_t q = base; u[u_face(bs, slot, 0, j, k)] = active[q] && connected[q] ? speed : 0.0f; }
+            if (fl & PCFD_BRICK_XMAX) { const int64_t q = base + bs - 1; u[u_face(bs, slot, bs, j, k)] = active[q] && connected[q] ? speed : 0.0f; }
+        }
+    }
+
+    Momentum& momentum_of(System& s)
+    {
+        require(s.momentum && s.momentum->ready, "cell-momentum topology was not built");
+        return *s.momentum;
+    }
+
+    pcfd_solve_result project(System& s, double rho, double dt, double tolerance, int max_iterations, bool warm)
+    {
+        launch_integrated_flux(s);
+        launch_normalize(s, rho / dt, true);
+        const pcfd_solve_result r = solve(s, s.pressure, s.rhs, tolerance, max_iterations, warm);
+        if (r.converged)
+        {
+            launch_convert_pressure(s);
+            launch_correct_fluxes(s, rho, dt);
+            launch_integrated_flux(s);
+            launch_normalize(s, 0.0, false);
+        }
+        return r;
+    }
+
+    void core_initialize(System& s, pcfd_step_stats& stats)
+    {
+        require(s.configured, "core is not configured");
+        Momentum& m = momentum_of(s);
+        const pcfd_case& c = s.config;
+        const float speed = float(c.speed);
+        DBuf<uint8_t> connected;
+        connected.upload(s.h_connected);
+        init_state_kernel<<<blocks_for(s.S), kThreads, 0, s.stream>>>(s.active, connected, s.S, speed, m.x, m.y, m.z, m.xn, m.yn, m.zn);
+        cuda_check(cudaMemsetAsync(s.u, 0, size_t(s.faces) * sizeof(float), s.stream), "clear faces");
+        cuda_check(cudaMemsetAsync(s.v, 0, size_t(s.faces) * sizeof(float), s.stream), "clear faces");
+        cuda_check(cudaMemsetAsync(s.w, 0, size_t(s.faces) * sizeof(float), s.stream), "clear faces");
+        cuda_check(cudaMemsetAsync(s.special, 0, size_t(s.cf_count + s.eb_count) * sizeof(float), s.stream), "clear special");
+        momentum_reconstruct_fluxes(s, m);
+        if (s.active_bricks)
+            init_x_boundary_kernel<<<blocks_for(int64_t(s.active_bricks) * s.bs * s.bs), kThreads, 0, s.stream>>>(
+                s.active_brick_list, s.active_bricks, s.bs, s.brick_flags, s.active, connected, speed, s.u);
+        momentum_external_boundaries(s, speed);
+        const double maximum = std::max(1e-9, std::abs(c.speed));
+        const double dt = c.cfl * s.h_finest / maximum;
+        vec_zero(s, s.pressure);
+        std::memset(&stats, 0, sizeof(stats));
+        stats.pressure = project(s, c.rho, dt, c.projection_tolerance, c.projection_max_iterations, false);
+        if (c.pressure_impulse && stats.pressure.converged) momentum_pressure_impulse(s, m, float(dt), float(c.rho), true);
+        float cfl[4];
+        momentum_cfl(s, m, true, cfl);
+        stats.dt = dt;
+        stats.max_abs_velocity = cfl[0];
+        stats.max_abs_special_velocity = cfl[2];
+        stats.cfl_velocity = maximum;
+        stats.effective_cfl = maximum * dt / s.h_finest;
+        s.initialized = stats.pressure.converged != 0;
+        stats.physical_time = s.physical_time;
+        cuda_check(cudaStreamSynchronize(s.stream), "initialize");
+    }
+
+    void core_step(System& s, pcfd_step_stats& stats)
+    {
+        require(s.initialized, "the core needs a converged initialization before stepping");
+        Momentum& m = momentum_of(s);
+        const pcfd_case& c = s.config;
+        cudaEvent_t e0, e1, p0, p1;
+        cuda_check(cudaEventCreate(&e0), "event"); cuda_check(cudaEventCreate(&e1), "event");
+        cuda_check(cudaEventCreate(&p0), "event"); cuda_check(cudaEventCreate(&p1), "event");
+        cuda_check(cudaEventRecord(e0, s.stream), "event");
+        std::memset(&stats, 0, sizeof(stats));
+        float cfl[4];
+        momentum_cfl(s, m, true, cfl);
+        if (!std::isfinite(cfl[0]) || !std::isfinite(cfl[1]) || !std::isfinite(cfl[2]))
+            throw Error(PCFD_INTERNAL, "non-finite cell or special velocity before the time step");
+        const double cfl_rate = std::max({1e-9, std::abs(c.speed) / s.h_finest, double(cfl[1])});
+        const double dt_value = c.cfl / cfl_rate;
+        const float dt = float(dt_value), nu = float(c.nu), cs = float(c.smagorinsky_cs), speed = float(c.speed), rho = float(c.rho);
+        momentum_transport(s, m, dt, speed, true);
+        stats.max_diffusion_rate = momentum_smagorinsky(s, m, nu, cs, dt);
+        stats.diffusion_substeps = m.last_substeps;
+        if (c.smooth_wall) momentum_wall(s, m, dt, nu);
+        momentum_reconstruct_fluxes(s, m);
+        momentum_external_boundaries(s, speed);
+        cuda_check(cudaEventRecord(p0, s.stream), "event");
+        stats.pressure = project(s, double(rho), dt_value, c.projection_tolerance, c.projection_max_iterations, true);
+        cuda_check(cudaEventRecord(p1, s.stream), "event");
+        if (c.pressure_impulse && stats.pressure.converged) momentum_pressure_impulse(s, m, dt, rho, true);
+        cuda_check(cudaEventRecord(e1, s.stream), "event");
+        cuda_check(cudaEventSynchronize(e1), "step");
+        float ms = 0, pms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventElapsedTime(&pms, p0, p1);
+        cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(p0); cudaEventDestroy(p1);
+        stats.dt = dt_value;
+        stats.max_abs_velocity = cfl[0];
+        stats.max_abs_special_velocity = cfl[2];
+        stats.max_outflow_rate = cfl[1];
+        stats.cfl_velocity = cfl_rate * s.h_finest;
+        stats.effective_cfl = cfl_rate * dt_value;
+        stats.step_ms = ms;
+        stats.projection_ms = pms;
+        if (stats.pressure.converged) s.physical_time += dt_value;
+        stats.physical_time = s.physical_time;
+    }
+}

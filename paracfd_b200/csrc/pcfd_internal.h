@@ -181,6 +181,14 @@ namespace pcfd
         DBuf<int> cf_group_offset, cf_group_member;
         DBuf<double> cf_group_area;
 
+        // cell-momentum transport and time-step orchestration
+        struct Momentum* momentum = nullptr;
+        std::vector<uint8_t> h_connected;       // freestream_connected
+        std::vector<int> xface_dof;             // [bricks with XMIN/XMAX faces] helper for initialisation
+        pcfd_case config{};
+        bool configured = false, initialized = false;
+        double physical_time = 0.0, h_finest = 0.0;
+
         ~System();
     };
 
