@@ -217,6 +217,38 @@ typedef struct pcfd_system pcfd_system;
 const char* pcfd_last_error_message(void);
 const char* pcfd_version(void);
 
+/* ---- preprocessing: closed wing surface -> brick hierarchy + composite system ------------
+ * Replaces AmrHierarchy::build_static (amr_grid.cpp:222-261) and the composite pressure
+ * builder (build_composite_amr_pressure_system, amr_pressure.cpp:247-301 with its finalisation
+ * :24-189).  With solid != 0 the cells whose centres lie inside the closed, outward-oriented
+ * surface become solid and every fluid/solid face a wall patch (a Cartesian stand-in for the
+ * reference's polyhedral cut-cell atlas, build_amr_embedded_boundary_atlas, amr_eb.h:69-70). */
+typedef struct pcfd_mesh {
+    int64_t vertex_count;
+    const double* positions;         /* [vertex_count][3] metres */
+    int64_t triangle_count;
+    const uint32_t* indices;         /* [triangle_count][3] */
+} pcfd_mesh;
+
+typedef struct pcfd_amr_config {     /* AmrConfig subset (paraglider_config.h:27-43) */
+    double domain_lo[3], domain_hi[3];   /* requested flow domain (padded to whole bricks) */
+    double base_cell_size;
+    int32_t max_levels;
+    int32_t brick_size;
+    double wing_refinement_distance;
+    double surface_refinement_distance;
+    double wake_length;
+    double wake_radius;
+    int32_t anchor_y_min;            /* half-wing symmetry plane at Y-min */
+} pcfd_amr_config;
+
+typedef struct pcfd_built_topology pcfd_built_topology;
+/* Fills *view with arrays owned by *out (valid until pcfd_topology_free). */
+pcfd_status pcfd_topology_build(const pcfd_mesh* surface, const pcfd_amr_config* config, int32_t solid,
+                                pcfd_built_topology** out, pcfd_topology* view);
+void pcfd_topology_free(pcfd_built_topology* topology);
+const char* pcfd_builder_last_error(void);
+
 /* Topology upload + device allocation (all static arrays copied; caller may free inputs). */
 pcfd_status pcfd_system_create(const pcfd_topology* topology, const pcfd_options* options,
                                pcfd_system** out);
@@ -299,11 +331,26 @@ pcfd_status pcfd_core_initialize(pcfd_system* system, pcfd_step_stats* stats);
  * boundaries, projection, pressure traction.  Time advances only when the solve converged. */
 pcfd_status pcfd_core_step(pcfd_system* system, pcfd_step_stats* stats);
 
+/* Integrated surface loads (AerodynamicLoads, src/core/aero_loads.h:33-53). */
+typedef struct pcfd_loads {
+    double pressure_force[3], pressure_moment[3];
+    double viscous_force[3], viscous_moment[3];
+    double total_force[3], total_moment[3];
+    double cl, cd, cs;               /* NaN unless reference_area > 0 and the case is configured */
+} pcfd_loads;
+/* compute_pressure_loads (+ accumulate_viscous_loads when include_viscous) of the resident
+ * pressure shadow and wall forces (aero_loads.cpp:183-204); device FP64 sums, 12-double readback. */
+pcfd_status pcfd_core_loads(pcfd_system* system, double pressure_reference, const double moment_origin[3],
+                            double reference_area, int32_t include_viscous, pcfd_loads* out);
+
 /* ---- instrumentation ---------------------------------------------------------------------- */
 /* Average device time of one launch sequence of `which` (0 full apply, 1 orthogonal apply,
  * 2 preconditioner, 3 divergence, 4 flux correction, 5 FP64 dot), measured with CUDA events on
  * the system stream over `iterations` back-to-back repetitions on resident scratch vectors. */
 pcfd_status pcfd_time_kernel(pcfd_system* system, int32_t which, int32_t iterations, double* ms_per_launch);
+/* Device-timeline markers on the system stream (slots 0..7) for whole-job timing. */
+pcfd_status pcfd_event_record(pcfd_system* system, int32_t slot);
+pcfd_status pcfd_event_elapsed(pcfd_system* system, int32_t start_slot, int32_t stop_slot, double* ms);
 
 #ifdef __cplusplus
 }

@@ -77,6 +77,10 @@ def lib():
         L.ref_core_initialize.argtypes = [vp, f64p]
         L.ref_core_step.argtypes = [vp, f64p]
         L.ref_core_state.argtypes = [vp, f32p, f32p, f32p, f64p]
+        L.ref_pressure_loads.argtypes = [vp, f64p, C.c_double, f64p, f64p]
+        L.ref_case_from_mesh.restype = vp
+        L.ref_case_from_mesh.argtypes = [f64p, C.c_int64, C.POINTER(C.c_uint32), C.c_int64, f64p, f64p, C.c_double,
+                                         C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double]
         _lib = L
     return _lib
 
@@ -100,9 +104,9 @@ def default_params(kind: int, **overrides) -> CaseParams:
 class RefCase:
     """Reference preprocessing result (hierarchy + EB atlas + composite pressure system)."""
 
-    def __init__(self, params: CaseParams):
+    def __init__(self, params: CaseParams | None, handle=None):
         self.params = params
-        self.handle = lib().ref_case_create(C.byref(params))
+        self.handle = handle if handle is not None else lib().ref_case_create(C.byref(params))
         if not self.handle:
             raise RuntimeError("reference case build failed: " + lib().ref_last_error().decode(errors="replace"))
         self.topology = Topology()
@@ -215,6 +219,13 @@ class RefCase:
                                          ptr(v, C.c_float), ptr(w, C.c_float), ptr(cf, C.c_double), ptr(eb, C.c_double)))
         return u, v, w, cf, eb
 
+    def pressure_loads(self, pressure, pressure_reference=0.0, origin=(0.0, 0.0, 0.0)):
+        out = np.zeros(6)
+        o = np.ascontiguousarray(origin, np.float64)
+        _check(lib().ref_pressure_loads(self.handle, ptr(np.ascontiguousarray(pressure, np.float64), C.c_double),
+                                        pressure_reference, ptr(o, C.c_double), ptr(out, C.c_double)))
+        return out[:3], out[3:]
+
     def outflow_rate(self, u, v, w, cf, eb, external=True):
         out = C.c_double()
         _check(lib().ref_outflow_rate_cpu(self.handle, ptr(u, C.c_float), ptr(v, C.c_float), ptr(w, C.c_float),
@@ -265,6 +276,22 @@ class RefCore:
             self.close()
         except Exception:
             pass
+
+
+def case_from_mesh(vertices, triangles, domain_lo, domain_hi, base_cell_size, max_levels, brick_size=8,
+                   wing_refinement_distance=1.0, surface_refinement_distance=0.35, wake_length=8.0,
+                   wake_radius=2.0) -> RefCase:
+    """Reference hierarchy + embedded-boundary-free composite system for an arbitrary mesh."""
+    v = np.ascontiguousarray(vertices, np.float64)
+    t = np.ascontiguousarray(triangles, np.uint32)
+    lo = np.ascontiguousarray(domain_lo, np.float64)
+    hi = np.ascontiguousarray(domain_hi, np.float64)
+    handle = lib().ref_case_from_mesh(ptr(v, C.c_double), len(v), ptr(t, C.c_uint32), len(t), ptr(lo, C.c_double),
+                                      ptr(hi, C.c_double), base_cell_size, max_levels, brick_size,
+                                      wing_refinement_distance, surface_refinement_distance, wake_length, wake_radius)
+    if not handle:
+        raise RuntimeError("reference mesh case failed: " + lib().ref_last_error().decode(errors="replace"))
+    return RefCase(None, handle=handle)
 
 
 def box_case(**kw) -> RefCase:

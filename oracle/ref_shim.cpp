@@ -874,6 +874,66 @@ int ref_outflow_rate_cpu(void* handle, const float* u, const float* v, const flo
     });
 }
 
+int ref_pressure_loads(void* handle, const double* pressure, double pref, const double* origin, double* out)
+{
+    return guarded([&] {
+        RefCase& c = *static_cast<RefCase*>(handle);
+        std::vector<double> p(pressure, pressure + c.system.storage_size);
+        FreestreamConfig fs;
+        AeroReferenceConfig rf;
+        rf.moment_origin = {origin[0], origin[1], origin[2]};
+        const auto loads = compute_pressure_loads(c.system, p, c.wing.triangle_count() + 1, fs, rf, pref);
+        for (int a = 0; a < 3; ++a) { out[a] = loads.pressure_force[a]; out[3 + a] = loads.pressure_moment[a]; }
+    });
+}
+
+void* ref_case_from_mesh(const double* positions, int64_t vertices, const uint32_t* indices, int64_t triangles,
+                         const double* lo, const double* hi, double h, int32_t levels, int32_t bs, double wing_distance,
+                         double surface_distance, double wake_length, double wake_radius)
+{
+    RefCase* rc = nullptr;
+    guarded([&] {
+        auto owned = std::make_unique<RefCase>();
+        RefCase& c = *owned;
+        TriMesh mesh;
+        float bmin[3] = {1e30f, 1e30f, 1e30f}, bmax[3] = {-1e30f, -1e30f, -1e30f};
+        for (int64_t v = 0; v < vertices; ++v)
+            for (int a = 0; a < 3; ++a)
+            {
+                const double x = positions[3 * v + a];
+                mesh.positions_fp64.push_back(x);
+                mesh.positions.push_back(float(x));
+                mesh.normals.push_back(0.f);
+                bmin[a] = std::min(bmin[a], float(x));
+                bmax[a] = std::max(bmax[a], float(x));
+            }
+        for (int64_t t = 0; t < triangles; ++t)
+        {
+            for (int k = 0; k < 3; ++k) mesh.indices.push_back(indices[3 * t + k]);
+            mesh.source_face_ids.push_back(0);
+        }
+        for (int a = 0; a < 3; ++a) { mesh.bbox_min[a] = bmin[a]; mesh.bbox_max[a] = bmax[a]; }
+        c.wing = mesh;
+        c.bvh = std::make_unique<TriangleBvh>(c.wing);
+        c.config.amr.base_cell_size = h;
+        c.config.amr.max_levels = levels;
+        c.config.amr.brick_size = bs;
+        c.config.amr.wing_refinement_distance = wing_distance;
+        c.config.amr.surface_refinement_distance = surface_distance;
+        c.config.amr.wake_length = wake_length;
+        c.config.amr.wake_radius = wake_radius;
+        Aabb3d domain;
+        domain.lo = {lo[0], lo[1], lo[2]};
+        domain.hi = {hi[0], hi[1], hi[2]};
+        c.hierarchy = AmrHierarchy::build_static(domain, c.wing, *c.bvh, c.config.amr, false);
+        c.system = build_composite_amr_pressure_system(c.hierarchy, true);
+        c.system.hierarchy = &c.hierarchy;
+        export_case(c);
+        rc = owned.release();
+    });
+    return rc;
+}
+
 void* ref_core_create(void* case_handle, const ref_core_case* cfg)
 {
     RefCore* out = nullptr;

@@ -75,6 +75,18 @@ int ref_reconstruct_cpu(void* handle, const float* x, const float* y, const floa
 int ref_outflow_rate_cpu(void* handle, const float* u, const float* v, const float* w, const double* cf,
                          const double* eb, int external, double* rate);
 
+/* compute_pressure_loads (aero_loads.cpp:183-195) of a DOF pressure vector: out = [F(3), M(3)]. */
+int ref_pressure_loads(void* handle, const double* pressure, double pressure_reference, const double* origin,
+                       double* out6);
+
+/* Hierarchy from an arbitrary closed mesh (AmrHierarchy::build_static on the given requested
+ * domain) and the composite pressure system WITHOUT an embedded-boundary atlas (the reference's
+ * build_composite_amr_pressure_system(hierarchy) overload). */
+void* ref_case_from_mesh(const double* positions, int64_t vertices, const uint32_t* indices, int64_t triangles,
+                         const double* domain_lo, const double* domain_hi, double base_cell_size, int32_t max_levels,
+                         int32_t brick_size, double wing_refinement_distance, double surface_refinement_distance,
+                         double wake_length, double wake_radius);
+
 /* The reference's own GPU path (ExternalAeroCore on the fixture), for the sm_100a baseline arm. */
 typedef struct ref_core_case {
     double speed, rho, nu, cfl, smagorinsky_cs, projection_tolerance;

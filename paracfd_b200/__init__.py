@@ -17,6 +17,55 @@ from .capi import Options, SolveResult, Topology, check, ptr
 MG_FP64, MG_FP32 = 0, 1
 
 
+class BuiltTopology:
+    """Brick hierarchy + composite pressure system built from a closed wing surface
+    (``pcfd_topology_build``).  ``topology`` is the C view consumed by CompositeSystem."""
+
+    def __init__(self, vertices: np.ndarray, triangles: np.ndarray, domain_lo, domain_hi, base_cell_size: float,
+                 max_levels: int, brick_size: int = 8, wing_refinement_distance: float = 1.0,
+                 surface_refinement_distance: float = 0.35, wake_length: float = 8.0, wake_radius: float = 2.0,
+                 anchor_y_min: bool = False, solid: bool = True):
+        self._lib = capi.load()
+        self._vertices = np.ascontiguousarray(vertices, np.float64)
+        self._triangles = np.ascontiguousarray(triangles, np.uint32)
+        mesh = capi.Mesh(len(self._vertices), ptr(self._vertices, C.c_double), len(self._triangles),
+                         ptr(self._triangles, C.c_uint32))
+        cfg = capi.AmrConfig()
+        cfg.domain_lo[:] = list(domain_lo)
+        cfg.domain_hi[:] = list(domain_hi)
+        cfg.base_cell_size = base_cell_size
+        cfg.max_levels = max_levels
+        cfg.brick_size = brick_size
+        cfg.wing_refinement_distance = wing_refinement_distance
+        cfg.surface_refinement_distance = surface_refinement_distance
+        cfg.wake_length = wake_length
+        cfg.wake_radius = wake_radius
+        cfg.anchor_y_min = int(anchor_y_min)
+        self.config = cfg
+        self.topology = Topology()
+        handle = C.c_void_p()
+        status = self._lib.pcfd_topology_build(C.byref(mesh), C.byref(cfg), int(solid), C.byref(handle), C.byref(self.topology))
+        if status != capi.PCFD_OK:
+            raise capi.PcfdError(status, self._lib.pcfd_builder_last_error().decode(errors="replace"))
+        self.handle = handle
+        t = self.topology
+        self.storage_size = t.storage_size
+        self.brick_counts = [t.levels[l].brick_count for l in range(t.level_count)]
+        self.active = np.ctypeslib.as_array(t.active, shape=(t.storage_size,))
+        self.leaf_cells = int(self.active.sum())
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._lib.pcfd_topology_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class CompositeSystem:
     """Resident topology + state on one GPU (one host thread at a time)."""
 
@@ -204,3 +253,19 @@ class CompositeSystem:
         if status not in (capi.PCFD_OK, 3):
             check(status)
         return stats.as_dict()
+
+    def loads(self, pressure_reference: float = 0.0, moment_origin=(0.0, 0.0, 0.0), reference_area: float = 0.0,
+              include_viscous: bool = True) -> dict:
+        out = capi.Loads()
+        origin = np.ascontiguousarray(moment_origin, np.float64)
+        check(self._lib.pcfd_core_loads(self.handle, pressure_reference, ptr(origin, C.c_double), reference_area,
+                                        int(include_viscous), C.byref(out)))
+        return out.as_dict()
+
+    def event_record(self, slot: int):
+        check(self._lib.pcfd_event_record(self.handle, slot))
+
+    def event_elapsed(self, start: int, stop: int) -> float:
+        ms = C.c_double()
+        check(self._lib.pcfd_event_elapsed(self.handle, start, stop, C.byref(ms)))
+        return ms.value

@@ -43,6 +43,7 @@ def _run(cmd: list[str]) -> None:
 def build(verbose: bool = False, extra_flags: list[str] | None = None) -> str:
     os.makedirs(OBJ, exist_ok=True)
     sources = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+    host_sources = sorted(glob.glob(os.path.join(CSRC, "*.cpp")))
     headers = sorted(glob.glob(os.path.join(CSRC, "*.h"))) + [os.path.join(ROOT, "include", "paracfd_b200.h")]
     flags = NVCC_FLAGS + (extra_flags or [])
     jobs = []
@@ -52,6 +53,12 @@ def build(verbose: bool = False, extra_flags: list[str] | None = None) -> str:
         objects.append(obj)
         if _newer(obj, [src] + headers):
             jobs.append([NVCC] + flags + ["-c", src, "-o", obj])
+    for src in host_sources:
+        obj = os.path.join(OBJ, os.path.basename(src) + ".o")
+        objects.append(obj)
+        if _newer(obj, [src] + headers):
+            jobs.append([os.environ.get("CXX", "g++"), "-std=c++17", "-O3", "-fPIC", "-I" + os.path.join(ROOT, "include"),
+                         "-c", src, "-o", obj])
     with ThreadPoolExecutor(max_workers=min(8, max(1, len(jobs)))) as pool:
         for cmd in jobs:
             if verbose:

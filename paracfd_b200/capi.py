@@ -116,6 +116,32 @@ class StepStats(C.Structure):
         return out
 
 
+class Loads(C.Structure):
+    _fields_ = [("pressure_force", C.c_double * 3), ("pressure_moment", C.c_double * 3),
+                ("viscous_force", C.c_double * 3), ("viscous_moment", C.c_double * 3),
+                ("total_force", C.c_double * 3), ("total_moment", C.c_double * 3),
+                ("cl", C.c_double), ("cd", C.c_double), ("cs", C.c_double)]
+
+    def as_dict(self):
+        out = {}
+        for name, kind in self._fields_:
+            v = getattr(self, name)
+            out[name] = list(v) if hasattr(v, "__len__") else v
+        return out
+
+
+class Mesh(C.Structure):
+    _fields_ = [("vertex_count", C.c_int64), ("positions", _f64p), ("triangle_count", C.c_int64),
+                ("indices", _u32p)]
+
+
+class AmrConfig(C.Structure):
+    _fields_ = [("domain_lo", C.c_double * 3), ("domain_hi", C.c_double * 3), ("base_cell_size", C.c_double),
+                ("max_levels", C.c_int32), ("brick_size", C.c_int32), ("wing_refinement_distance", C.c_double),
+                ("surface_refinement_distance", C.c_double), ("wake_length", C.c_double),
+                ("wake_radius", C.c_double), ("anchor_y_min", C.c_int32)]
+
+
 def ptr(array: np.ndarray | None, ctype):
     """Pointer to a contiguous numpy array (None -> NULL)."""
     if array is None:
@@ -166,6 +192,13 @@ SIGNATURES = {
     "pcfd_core_configure": (C.c_int, [C.c_void_p, C.POINTER(Case)]),
     "pcfd_core_initialize": (C.c_int, [C.c_void_p, C.POINTER(StepStats)]),
     "pcfd_core_step": (C.c_int, [C.c_void_p, C.POINTER(StepStats)]),
+    "pcfd_topology_build": (C.c_int, [C.POINTER(Mesh), C.POINTER(AmrConfig), C.c_int32, C.POINTER(C.c_void_p),
+                                      C.POINTER(Topology)]),
+    "pcfd_topology_free": (None, [C.c_void_p]),
+    "pcfd_core_loads": (C.c_int, [C.c_void_p, C.c_double, _f64p, C.c_double, C.c_int32, C.POINTER(Loads)]),
+    "pcfd_event_record": (C.c_int, [C.c_void_p, C.c_int32]),
+    "pcfd_event_elapsed": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
+    "pcfd_builder_last_error": (C.c_char_p, []),
 }
 
 _lib = None

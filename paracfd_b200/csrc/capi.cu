@@ -5,6 +5,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <memory>
 
 namespace pcfd
@@ -211,6 +212,7 @@ namespace pcfd
             s.h_finest = t.levels[t.level_count - 1].h;
             s.momentum = new Momentum();
             build_momentum(s, *s.momentum, t, options ? options->momentum_min_volume_fraction : 0.0);
+            build_loads(s, t);
             cuda_check(cudaDeviceSynchronize(), "system setup");
         }
 
@@ -235,6 +237,9 @@ namespace pcfd
 
     System::~System()
     {
+        for (cudaEvent_t& e : markers)
+            if (e) cudaEventDestroy(e);
+        destroy_loads(*this);
         delete momentum;
         if (pinned) cudaFreeHost(pinned);
         if (own_stream && stream) cudaStreamDestroy(stream);
@@ -600,6 +605,57 @@ pcfd_status pcfd_core_step(pcfd_system* system, pcfd_step_stats* stats)
         core_step(s, local);
         if (stats) *stats = local;
         if (!local.pressure.converged) throw Error(PCFD_NOT_CONVERGED, "pressure solve did not converge; time not advanced");
+    });
+}
+
+pcfd_status pcfd_event_record(pcfd_system* system, int32_t slot)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(slot >= 0 && slot < 8, "event slot must be 0..7");
+        if (!s.markers[slot]) cuda_check(cudaEventCreate(&s.markers[slot]), "create marker");
+        cuda_check(cudaEventRecord(s.markers[slot], s.stream), "record marker");
+    });
+}
+
+pcfd_status pcfd_event_elapsed(pcfd_system* system, int32_t a, int32_t b, double* ms)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(a >= 0 && a < 8 && b >= 0 && b < 8 && s.markers[a] && s.markers[b] && ms, "invalid marker slots");
+        cuda_check(cudaEventSynchronize(s.markers[b]), "marker sync");
+        float v = 0;
+        cuda_check(cudaEventElapsedTime(&v, s.markers[a], s.markers[b]), "marker elapsed");
+        *ms = v;
+    });
+}
+
+pcfd_status pcfd_core_loads(pcfd_system* system, double pressure_reference, const double moment_origin[3], double reference_area,
+                            int32_t include_viscous, pcfd_loads* out)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(out != nullptr, "null loads output");
+        const double zero[3] = {0, 0, 0};
+        const double rho = s.configured ? s.config.rho : 1.0;
+        double r[12];
+        compute_loads(s, pressure_reference, moment_origin ? moment_origin : zero, rho, include_viscous != 0, r);
+        std::memset(out, 0, sizeof(*out));
+        for (int a = 0; a < 3; ++a)
+        {
+            out->pressure_force[a] = r[a];
+            out->pressure_moment[a] = r[3 + a];
+            out->viscous_force[a] = r[6 + a];
+            out->viscous_moment[a] = r[9 + a];
+            out->total_force[a] = r[a] + r[6 + a];
+            out->total_moment[a] = r[3 + a] + r[9 + a];
+        }
+        const double q = s.configured ? 0.5 * s.config.rho * s.config.speed * s.config.speed : 0.0;
+        const double nan = std::numeric_limits<double>::quiet_NaN();
+        const bool valid = q > 0 && reference_area > 0;
+        out->cd = valid ? out->total_force[0] / (q * reference_area) : nan;
+        out->cs = valid ? out->total_force[1] / (q * reference_area) : nan;
+        out->cl = valid ? out->total_force[2] / (q * reference_area) : nan;
     });
 }
 

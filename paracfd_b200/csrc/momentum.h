@@ -77,6 +77,11 @@ namespace pcfd
     // [max |v| over cells, max outflow rate, max |special velocity|, max EB cfl rate]
     void momentum_cfl(System& s, Momentum& m, bool external_aero, float out[4]);
 
+    // surface loads (loads.cu): out = [pressure F(3), pressure M(3), viscous F(3), viscous M(3)]
+    void build_loads(System& s, const pcfd_topology& t);
+    void destroy_loads(System& s);
+    void compute_loads(System& s, double pref, const double origin[3], double rho, bool viscous, double out[12]);
+
     // time step (core.cu)
     Momentum& momentum_of(System& s);
     pcfd_solve_result project(System& s, double rho, double dt, double tolerance, int max_iterations, bool warm);

@@ -475,6 +475,14 @@ namespace pcfd
         std::vector<uint8_t> deferred(S, 0);
         for (const Edge& e : edges) { deferred[e.a] = 1; deferred[e.b] = 1; }
         for (int q = 0; q < S; ++q) if (special[q] || group_of[q] >= 0 || q >= s.structured) deferred[q] = 1;
+        // Structured slots whose control volume absorbed a merged fragment are not h^3: their
+        // update must divide by the stored volume, which only the per-DOF pass reads.
+        for (int q = 0; q < s.structured; ++q)
+        {
+            if (!t.active[q]) continue;
+            const double h = t.levels[slot_level[q / c3]].h;
+            if (float(t.volume[q]) != float(h * h * h)) deferred[q] = 1;
+        }
         for (const Side& sd : sides) deferred[sd.dof] = 1;
         for (int f = 0; f < m.nB; ++f) if (active(t.boundary_faces.dof[f])) deferred[t.boundary_faces.dof[f]] = 1;
         std::vector<int> d_of(S, -1), d_dof;

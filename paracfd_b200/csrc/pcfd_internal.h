@@ -183,6 +183,8 @@ namespace pcfd
 
         // cell-momentum transport and time-step orchestration
         struct Momentum* momentum = nullptr;
+        void* loads = nullptr;                  // surface-load integration state (loads.cu)
+        cudaEvent_t markers[8] = {};
         std::vector<uint8_t> h_connected;       // freestream_connected
         std::vector<int> xface_dof;             // [bricks with XMIN/XMAX faces] helper for initialisation
         pcfd_case config{};
