@@ -78,6 +78,13 @@ def lib():
         L.ref_core_step.argtypes = [vp, f64p]
         L.ref_core_state.argtypes = [vp, f32p, f32p, f32p, f64p]
         L.ref_pressure_loads.argtypes = [vp, f64p, C.c_double, f64p, f64p]
+        L.ref_import_topology.restype = vp
+        L.ref_import_topology.argtypes = [C.POINTER(Topology)]
+        L.ref_device_core_create.restype = vp
+        L.ref_device_core_create.argtypes = [vp, C.POINTER(CoreCase), C.c_double]
+        L.ref_device_core_destroy.argtypes = [vp]
+        L.ref_device_core_initialize.argtypes = [vp, f64p]
+        L.ref_device_core_step.argtypes = [vp, f64p]
         L.ref_case_from_mesh.restype = vp
         L.ref_case_from_mesh.argtypes = [f64p, C.c_int64, C.POINTER(C.c_uint32), C.c_int64, f64p, f64p, C.c_double,
                                          C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double]
@@ -276,6 +283,44 @@ class RefCore:
             self.close()
         except Exception:
             pass
+
+
+def import_topology(topology: Topology) -> RefCase:
+    """The reference's hierarchy/system objects holding an externally built topology."""
+    handle = lib().ref_import_topology(C.byref(topology))
+    if not handle:
+        raise RuntimeError("reference import failed: " + lib().ref_last_error().decode(errors="replace"))
+    return RefCase(None, handle=handle)
+
+
+class RefDeviceCore(RefCore):
+    """The reference's device classes driven with ExternalAeroCore's step sequence on any case."""
+
+    def __init__(self, case: RefCase, speed=10.0, rho=1.225, nu=1.5e-5, cfl=0.5, cs=0.10, tolerance=1e-8, max_iterations=600,
+                 min_volume_fraction=0.25):
+        self.case = case
+        cfg = CoreCase(speed, rho, nu, cfl, cs, tolerance, max_iterations)
+        self.handle = lib().ref_device_core_create(case.handle, C.byref(cfg), min_volume_fraction)
+        if not self.handle:
+            raise RuntimeError("reference device core: " + lib().ref_last_error().decode(errors="replace"))
+
+    def initialize(self):
+        a = np.zeros(6)
+        _check(lib().ref_device_core_initialize(self.handle, ptr(a, C.c_double)))
+        return self._stats(a)
+
+    def step(self):
+        a = np.zeros(6)
+        _check(lib().ref_device_core_step(self.handle, ptr(a, C.c_double)))
+        return self._stats(a)
+
+    def state(self):
+        raise NotImplementedError
+
+    def close(self):
+        if self.handle:
+            lib().ref_device_core_destroy(self.handle)
+            self.handle = None
 
 
 def case_from_mesh(vertices, triangles, domain_lo, domain_hi, base_cell_size, max_levels, brick_size=8,

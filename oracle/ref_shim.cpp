@@ -15,6 +15,8 @@
 #include "core/paraglider_config.h"
 
 #include <algorithm>
+#include <chrono>
+#include <cuda_runtime.h>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -932,6 +934,234 @@ void* ref_case_from_mesh(const double* positions, int64_t vertices, const uint32
         rc = owned.release();
     });
     return rc;
+}
+
+void* ref_import_topology(const pcfd_topology* t)
+{
+    RefCase* rc = nullptr;
+    guarded([&] {
+        auto owned = std::make_unique<RefCase>();
+        RefCase& c = *owned;
+        const int bs = t->brick_size;
+        const double h0 = t->levels[0].h;
+        Aabb3d domain;
+        domain.lo = {t->domain_lo[0], t->domain_lo[1], t->domain_lo[2]};
+        // a hair inside the padded box so the brick count is not rounded up
+        domain.hi = {t->domain_hi[0] - 1e-9, t->domain_hi[1] - 1e-9, t->domain_hi[2] - 1e-9};
+        c.hierarchy = AmrHierarchy::uniform(domain, h0, bs, 1);
+        auto& levels = c.hierarchy.levels();
+        levels.assign(t->level_count, {});
+        for (int l = 0; l < t->level_count; ++l)
+        {
+            const pcfd_level& src = t->levels[l];
+            AmrLevel& lev = levels[l];
+            lev.level = l;
+            lev.h = src.h;
+            lev.bricks.resize(src.brick_count);
+            for (int b = 0; b < src.brick_count; ++b)
+            {
+                BrickMetadata& m = lev.bricks[b];
+                m.level = l;
+                m.coord = {src.coord[3 * b], src.coord[3 * b + 1], src.coord[3 * b + 2]};
+                m.origin = {src.origin[3 * b], src.origin[3 * b + 1], src.origin[3 * b + 2]};
+                m.h = src.h;
+                for (int f = 0; f < 6; ++f) m.same_level_neighbor[f] = src.neighbors[6 * b + f];
+                if (src.children)
+                    for (int k = 0; k < 8; ++k) m.children[k] = src.children[8 * b + k];
+                m.flags = src.flags[b];
+                if (m.active()) ++lev.active_bricks;
+            }
+        }
+        CompositeAmrPressureSystem& s = c.system;
+        s.hierarchy = &c.hierarchy;
+        s.brick_size = bs;
+        s.storage_size = t->storage_size;
+        s.pressure_outlet_xmax = t->pressure_outlet_xmax != 0;
+        const int n = t->storage_size;
+        for (int l = 0; l < t->level_count; ++l) s.level_offset.push_back(t->levels[l].level_offset);
+        s.active.assign(t->active, t->active + n);
+        s.freestream_connected = t->freestream_connected ? std::vector<unsigned char>(t->freestream_connected, t->freestream_connected + n) : s.active;
+        s.cut_face_mask.assign(t->cut_face_mask, t->cut_face_mask + n);
+        s.volume.assign(t->volume, t->volume + n);
+        s.centroid.resize(n);
+        for (int q = 0; q < n; ++q) s.centroid[q] = {t->centroid[3 * q], t->centroid[3 * q + 1], t->centroid[3 * q + 2]};
+        s.preconditioner_aggregate.assign(t->preconditioner_aggregate, t->preconditioner_aggregate + n);
+        auto conn = [](const pcfd_connections& in, std::vector<CoarseFinePressureConnection>& out) {
+            out.resize(in.count);
+            for (int e = 0; e < in.count; ++e)
+            {
+                auto& o = out[e];
+                o.coarse_dof = in.coarse_dof[e]; o.fine_dof = in.fine_dof[e]; o.open_area = in.open_area[e];
+                o.centre_distance = in.centre_distance[e]; o.normal_distance = in.normal_distance[e];
+                o.axis = in.axis[e]; o.direction = in.direction[e];
+                o.face_centroid = {in.face_centroid[3 * e], in.face_centroid[3 * e + 1], in.face_centroid[3 * e + 2]};
+                o.orthogonal_gradient_factor = in.orthogonal_gradient_factor[e];
+                o.lower_gradient_node = in.lower_gradient_node[e]; o.upper_gradient_node = in.upper_gradient_node[e];
+                o.nonorthogonal_correction = {in.nonorthogonal_correction[3 * e], in.nonorthogonal_correction[3 * e + 1], in.nonorthogonal_correction[3 * e + 2]};
+                o.upper_gradient_weight = in.upper_gradient_weight[e];
+            }
+        };
+        conn(t->coarse_fine, s.coarse_fine);
+        conn(t->embedded, s.embedded);
+        s.regular_pressure_corrections.resize(t->regular.count);
+        for (int e = 0; e < t->regular.count; ++e)
+        {
+            auto& o = s.regular_pressure_corrections[e];
+            const pcfd_regular_corrections& r = t->regular;
+            o.lower_dof = r.lower_dof[e]; o.upper_dof = r.upper_dof[e]; o.level = r.level[e]; o.brick = r.brick[e];
+            o.i = r.ijk[3 * e]; o.j = r.ijk[3 * e + 1]; o.k = r.ijk[3 * e + 2]; o.axis = r.axis[e];
+            o.open_area = r.open_area[e]; o.two_point_delta = r.two_point_delta[e];
+            o.lower_gradient_node = r.lower_gradient_node[e]; o.upper_gradient_node = r.upper_gradient_node[e];
+            o.nonorthogonal_correction = {r.nonorthogonal_correction[3 * e], r.nonorthogonal_correction[3 * e + 1], r.nonorthogonal_correction[3 * e + 2]};
+            o.upper_gradient_weight = r.upper_gradient_weight[e];
+        }
+        const int nodes = t->gradient_node_count;
+        s.pressure_gradient_dof.assign(t->gradient_dof, t->gradient_dof + nodes);
+        s.pressure_gradient_offset.assign(t->gradient_offset, t->gradient_offset + (nodes ? nodes + 1 : 0));
+        const int nnz = nodes ? t->gradient_offset[nodes] : 0;
+        s.pressure_gradient_neighbour.assign(t->gradient_neighbour, t->gradient_neighbour + nnz);
+        s.pressure_gradient_weight.resize(nnz);
+        for (int q = 0; q < nnz; ++q) s.pressure_gradient_weight[q] = {t->gradient_weight[3 * q], t->gradient_weight[3 * q + 1], t->gradient_weight[3 * q + 2]};
+        s.pressure_gradient_rank.assign(nodes, 3);
+        s.pressure_gradient_ring.assign(nodes, 1);
+        for (int g = 0; g < t->gauge_count; ++g) s.gauges.push_back({t->gauge_dof[g], t->gauge_coefficient[g]});
+        for (int p = 0; p < t->patches.count; ++p)
+        {
+            CompositeSurfacePressurePatch o;
+            o.area = t->patches.area[p];
+            o.centroid = {t->patches.centroid[3 * p], t->patches.centroid[3 * p + 1], t->patches.centroid[3 * p + 2]};
+            o.normal = {t->patches.normal[3 * p], t->patches.normal[3 * p + 1], t->patches.normal[3 * p + 2]};
+            o.plus_dof = t->patches.plus_dof[p];
+            o.minus_dof = t->patches.minus_dof[p];
+            s.surface_patches.push_back(o);
+        }
+        for (int f = 0; f < t->boundary_faces.count; ++f)
+        {
+            CompositeBoundaryPressureFace o;
+            o.dof = t->boundary_faces.dof[f];
+            o.outward_area = {t->boundary_faces.outward_area[3 * f], t->boundary_faces.outward_area[3 * f + 1], t->boundary_faces.outward_area[3 * f + 2]};
+            o.centroid = {t->boundary_faces.centroid[3 * f], t->boundary_faces.centroid[3 * f + 1], t->boundary_faces.centroid[3 * f + 2]};
+            s.boundary_faces.push_back(o);
+        }
+        s.face_state_retained_dofs.assign(t->retained_dofs, t->retained_dofs + t->retained_count);
+        s.face_state_retained_small_root_count = s.face_state_retained_dofs.size();
+        export_case(c);
+        rc = owned.release();
+    });
+    return rc;
+}
+
+namespace
+{
+    struct RefDeviceCore
+    {
+        RefCase* c = nullptr;
+        ref_core_case cfg{};
+        std::unique_ptr<DeviceAmrFields> fields;
+        std::unique_ptr<DeviceCompositeAmrProjection> projection;
+        std::unique_ptr<DeviceCompositeCellMomentumTransport> momentum;
+        bool initialized = false;
+        double time = 0;
+    };
+    double ms_between(std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b)
+    {
+        return std::chrono::duration<double, std::milli>(b - a).count();
+    }
+}
+
+void* ref_device_core_create(void* case_handle, const ref_core_case* cfg, double min_volume_fraction)
+{
+    RefDeviceCore* out = nullptr;
+    guarded([&] {
+        auto core = std::make_unique<RefDeviceCore>();
+        core->c = static_cast<RefCase*>(case_handle);
+        core->cfg = *cfg;
+        RefCase& c = *core->c;
+        core->fields = std::make_unique<DeviceAmrFields>(c.hierarchy);
+        core->projection = std::make_unique<DeviceCompositeAmrProjection>(c.system, *core->fields);
+        core->momentum = std::make_unique<DeviceCompositeCellMomentumTransport>(c.system, *core->fields, min_volume_fraction);
+        out = core.release();
+    });
+    return out;
+}
+
+void ref_device_core_destroy(void* core) { delete static_cast<RefDeviceCore*>(core); }
+
+// ExternalAeroCore::initialize (external_aero_core.cpp:245-302) on the imported grid.
+int ref_device_core_initialize(void* handle, double* stats)
+{
+    return guarded([&] {
+        RefDeviceCore& k = *static_cast<RefDeviceCore*>(handle);
+        RefCase& c = *k.c;
+        const CompositeAmrPressureSystem& s = c.system;
+        const Real speed = Real(k.cfg.speed);
+        CompositeCellMomentumState state;
+        state.x.assign(s.storage_size, Real(0)); state.y.assign(s.storage_size, Real(0)); state.z.assign(s.storage_size, Real(0));
+        for (int q = 0; q < s.storage_size; ++q) if (s.active[q] && s.freestream_connected[q]) state.x[q] = speed;
+        AmrHostFields fields(c.hierarchy);
+        CompositeAmrFluxes fluxes;
+        reconstruct_composite_cell_fluxes_cpu(s, state, fields, fluxes);
+        const int bs = s.brick_size;
+        for (int l = 0; l < int(c.hierarchy.levels().size()); ++l)
+        {
+            const AmrLevel& level = c.hierarchy.levels()[l];
+            AmrHostLevelFields& values = fields.levels()[l];
+            for (int b = 0; b < int(level.bricks.size()); ++b)
+            {
+                const BrickMetadata& m = level.bricks[b];
+                if (!m.active()) continue;
+                for (int kk = 0; kk < bs; ++kk)
+                    for (int j = 0; j < bs; ++j)
+                    {
+                        if (m.flags & BRICK_XMIN) { const int d = s.dof(l, b, 0, j, kk); values.u[values.layout.u_index(b, 0, j, kk)] = s.active[d] && s.freestream_connected[d] ? speed : Real(0); }
+                        if (m.flags & BRICK_XMAX) { const int d = s.dof(l, b, bs - 1, j, kk); values.u[values.layout.u_index(b, bs, j, kk)] = s.active[d] && s.freestream_connected[d] ? speed : Real(0); }
+                    }
+            }
+        }
+        k.fields->upload(fields);
+        k.projection->upload_special_fluxes(fluxes);
+        k.momentum->upload_state(state);
+        k.momentum->reconstruct_fluxes(k.projection->coarse_fine_velocity_device(), k.projection->embedded_velocity_device());
+        k.fields->apply_external_aero_boundaries(speed);
+        const double maximum = std::max(1e-9, std::abs(k.cfg.speed)), dt = k.cfg.cfl * c.hierarchy.finest_cell_size() / maximum;
+        const auto t0 = std::chrono::steady_clock::now();
+        const AmrGpuSolveResult r = k.projection->project(Real(k.cfg.rho), Real(dt), k.cfg.projection_tolerance, k.cfg.projection_max_iterations, false);
+        if (r.converged) k.momentum->apply_projected_pressure_gradient(k.projection->pressure(), Real(dt), Real(k.cfg.rho));
+        const auto t1 = std::chrono::steady_clock::now();
+        k.initialized = r.converged;
+        stats[0] = dt; stats[1] = ms_between(t0, t1); stats[2] = stats[1]; stats[3] = r.iterations; stats[4] = r.converged; stats[5] = r.relative_residual;
+    });
+}
+
+// ExternalAeroCore::step (external_aero_core.cpp:304-328), conservative cell momentum, wall on.
+int ref_device_core_step(void* handle, double* stats)
+{
+    return guarded([&] {
+        RefDeviceCore& k = *static_cast<RefDeviceCore*>(handle);
+        if (!k.initialized) throw std::logic_error("reference device core needs a converged initialization");
+        RefCase& c = *k.c;
+        const auto t0 = std::chrono::steady_clock::now();
+        const double h = c.hierarchy.finest_cell_size();
+        const double rate = k.momentum->max_outflow_rate(k.projection->coarse_fine_velocity_device(), k.projection->embedded_velocity_device(), true);
+        (void)k.fields->max_abs_velocity();
+        (void)k.momentum->max_abs_velocity();
+        (void)k.projection->max_abs_special_velocity();
+        (void)k.projection->max_embedded_cfl_rate();
+        const double cfl_rate = std::max({1e-9, std::abs(k.cfg.speed) / h, rate}), dt_value = k.cfg.cfl / cfl_rate;
+        const Real dt = Real(dt_value), nu = Real(k.cfg.nu), cs = Real(k.cfg.smagorinsky_cs), speed = Real(k.cfg.speed), rho = Real(k.cfg.rho);
+        k.momentum->step(k.projection->coarse_fine_velocity_device(), k.projection->embedded_velocity_device(), dt, true, speed);
+        k.momentum->diffuse_smagorinsky(nu, cs, dt);
+        k.momentum->apply_smooth_fabric_wall_model(dt, nu);
+        k.momentum->reconstruct_fluxes(k.projection->coarse_fine_velocity_device(), k.projection->embedded_velocity_device());
+        k.fields->apply_external_aero_boundaries(speed);
+        const auto p0 = std::chrono::steady_clock::now();
+        const AmrGpuSolveResult r = k.projection->project(rho, dt, k.cfg.projection_tolerance, k.cfg.projection_max_iterations, true);
+        const auto p1 = std::chrono::steady_clock::now();
+        if (r.converged) { k.momentum->apply_projected_pressure_gradient(k.projection->pressure(), dt, rho); k.time += dt_value; }
+        cudaDeviceSynchronize();
+        const auto t1 = std::chrono::steady_clock::now();
+        stats[0] = dt_value; stats[1] = ms_between(t0, t1); stats[2] = ms_between(p0, p1); stats[3] = r.iterations; stats[4] = r.converged; stats[5] = r.relative_residual;
+    });
 }
 
 void* ref_core_create(void* case_handle, const ref_core_case* cfg)

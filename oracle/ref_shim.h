@@ -87,11 +87,24 @@ void* ref_case_from_mesh(const double* positions, int64_t vertices, const uint32
                          int32_t brick_size, double wing_refinement_distance, double surface_refinement_distance,
                          double wake_length, double wake_radius);
 
-/* The reference's own GPU path (ExternalAeroCore on the fixture), for the sm_100a baseline arm. */
 typedef struct ref_core_case {
     double speed, rho, nu, cfl, smagorinsky_cs, projection_tolerance;
     int32_t projection_max_iterations;
 } ref_core_case;
+
+/* Import a flat topology (e.g. one built by paracfd_b200's own preprocessing) into the
+ * reference's AmrHierarchy + CompositeAmrPressureSystem objects, so its host twins and device
+ * classes run on exactly that grid.  No mesh/atlas is attached. */
+void* ref_import_topology(const pcfd_topology* topology);
+/* The reference's device classes (DeviceAmrFields, DeviceCompositeAmrProjection,
+ * DeviceCompositeCellMomentumTransport) driven with ExternalAeroCore's initialize/step sequence
+ * (external_aero_core.cpp:245-328) on any case handle (fixture or imported). */
+void* ref_device_core_create(void* case_handle, const ref_core_case* config, double min_volume_fraction);
+void ref_device_core_destroy(void* core);
+int ref_device_core_initialize(void* core, double* stats6);
+int ref_device_core_step(void* core, double* stats6);
+
+/* The reference's own GPU path (ExternalAeroCore on the fixture), for the sm_100a baseline arm. */
 void* ref_core_create(void* case_handle, const ref_core_case* config);
 void ref_core_destroy(void* core);
 /* stats: [dt, gpu_step_ms, projection_ms, iterations, converged, residual] */
