@@ -170,6 +170,8 @@ typedef struct pcfd_options {
     int32_t device;                  /* CUDA device ordinal */
     void* stream;                    /* cudaStream_t or NULL for a library-owned stream */
     double momentum_min_volume_fraction; /* AmrConfig::min_volume_fraction (small-cell groups) */
+    int32_t disable_fused_smoother;  /* 1: run the preconditioner's fine level as separate
+                                        operator/vector launches (same sweeps, reference order) */
 } pcfd_options;
 
 /* AmrGpuSolveResult (amr_pressure.h:337-351), trimmed to what the solver reports. */
@@ -330,6 +332,15 @@ pcfd_status pcfd_core_initialize(pcfd_system* system, pcfd_step_stats* stats);
 /* One time step (ExternalAeroCore::step): CFL, transport, LES diffusion, wall, reconstruction,
  * boundaries, projection, pressure traction.  Time advances only when the solve converged. */
 pcfd_status pcfd_core_step(pcfd_system* system, pcfd_step_stats* stats);
+/* X-min inflow profile (generalises ExternalAeroCore's uniform u = speed on the XMIN faces,
+ * external_aero_core.cpp:290 / amr_advection.cu external-boundary kernel).  The layout is one
+ * normal velocity per boundary face: face (j, k) of the n-th non-covered brick carrying
+ * PCFD_BRICK_XMIN (all levels, coarsest first, brick order) sits at n*bs*bs + k*bs + j.
+ * pcfd_core_inflow_layout returns the face count and, if brick_slots is non-NULL, the global
+ * brick slot of each of those bricks ([face_count / bs^2]).  set_inflow with count 0 (and any
+ * pointer) returns to the uniform freestream; otherwise count must equal the face count. */
+pcfd_status pcfd_core_inflow_layout(pcfd_system* system, int64_t* face_count, int32_t* brick_slots);
+pcfd_status pcfd_core_set_inflow_host(pcfd_system* system, const float* normal_velocity, int64_t count);
 
 /* Integrated surface loads (AerodynamicLoads, src/core/aero_loads.h:33-53). */
 typedef struct pcfd_loads {
@@ -345,12 +356,28 @@ pcfd_status pcfd_core_loads(pcfd_system* system, double pressure_reference, cons
 
 /* ---- instrumentation ---------------------------------------------------------------------- */
 /* Average device time of one launch sequence of `which` (0 full apply, 1 orthogonal apply,
- * 2 preconditioner, 3 divergence, 4 flux correction, 5 FP64 dot), measured with CUDA events on
- * the system stream over `iterations` back-to-back repetitions on resident scratch vectors. */
+ * 2 preconditioner, 3 divergence, 4 flux correction, 5 FP64 dot, 6/7/8 preconditioner
+ * pre-smoothing / coarse correction / post-smoothing, 9 one GCRO column orthogonalisation
+ * against 3 recycled + 13 basis vectors), measured with CUDA events on the system stream over
+ * `iterations` back-to-back repetitions on resident scratch vectors. */
 pcfd_status pcfd_time_kernel(pcfd_system* system, int32_t which, int32_t iterations, double* ms_per_launch);
 /* Device-timeline markers on the system stream (slots 0..7) for whole-job timing. */
 pcfd_status pcfd_event_record(pcfd_system* system, int32_t slot);
 pcfd_status pcfd_event_elapsed(pcfd_system* system, int32_t start_slot, int32_t stop_slot, double* ms);
+/* Per-launch device time of one instrumented region inside the real time step: begin arms
+ * `capacity` CUDA event pairs recorded on the system stream around every launch of `region`;
+ * end waits for them, writes up to `capacity` per-launch times (ms) and the count, and disarms. */
+enum {
+    PCFD_PROFILE_STRUCTURED_APPLY = 0,   /* brick-tiled FP64 7-point operator kernel */
+    PCFD_PROFILE_PRECONDITIONER = 1      /* one whole multigrid preconditioner application */
+};
+/* 1 when the preconditioner's fine level runs as fused brick kernels (8^3 bricks whose
+ * level-0 aggregates follow the brick geometry), 0 when it runs as separate launches. */
+pcfd_status pcfd_preconditioner_fused(pcfd_system* system, int32_t* fused);
+/* Number of this library's kernels launched on the system's stream since creation. */
+pcfd_status pcfd_launch_count(pcfd_system* system, int64_t* launches);
+pcfd_status pcfd_profile_begin(pcfd_system* system, int32_t region, int32_t capacity);
+pcfd_status pcfd_profile_end(pcfd_system* system, double* ms_per_launch, int32_t capacity, int32_t* launches);
 
 #ifdef __cplusplus
 }

@@ -14,6 +14,8 @@ import numpy as np
 from . import capi
 from .capi import Options, SolveResult, Topology, check, ptr
 
+PROFILE_STRUCTURED_APPLY = 0
+PROFILE_PRECONDITIONER = 1
 MG_FP64, MG_FP32 = 0, 1
 
 
@@ -70,16 +72,18 @@ class CompositeSystem:
     """Resident topology + state on one GPU (one host thread at a time)."""
 
     def __init__(self, topology: Topology, mg_precision: int = MG_FP64, device: int = 0,
-                 momentum_min_volume_fraction: float = 0.0):
+                 momentum_min_volume_fraction: float = 0.0, fused_smoother: bool = True):
         self._lib = capi.load()
         self._topology = topology   # keep the caller's arrays alive during creation
-        opts = Options(mg_precision, device, None, momentum_min_volume_fraction)
+        opts = Options(mg_precision, device, None, momentum_min_volume_fraction, 0 if fused_smoother else 1)
         handle = C.c_void_p()
         check(self._lib.pcfd_system_create(C.byref(topology), C.byref(opts), C.byref(handle)))
         self.handle = handle
         sizes = [C.c_int64() for _ in range(5)]
         check(self._lib.pcfd_system_sizes(self.handle, *[C.byref(x) for x in sizes]))
         self.storage_size, self.bricks, self.faces, self.coarse_fine_count, self.embedded_count = (x.value for x in sizes)
+        per_brick = self.faces // max(self.bricks, 1)
+        self.brick_size = next((b for b in range(1, 65) if (b + 1) * b * b == per_brick), 0)
 
     def close(self):
         if getattr(self, "handle", None):
@@ -269,3 +273,44 @@ class CompositeSystem:
         ms = C.c_double()
         check(self._lib.pcfd_event_elapsed(self.handle, start, stop, C.byref(ms)))
         return ms.value
+
+    def inflow_layout(self) -> np.ndarray:
+        """Brick slots of the X-min inflow faces; face (j, k) of brick n is n*bs*bs + k*bs + j."""
+        count = C.c_int64()
+        check(self._lib.pcfd_core_inflow_layout(self.handle, C.byref(count), None))
+        slots = np.empty(count.value // (self.brick_size ** 2) if count.value else 0, np.int32)
+        check(self._lib.pcfd_core_inflow_layout(self.handle, C.byref(count), ptr(slots, C.c_int32)))
+        return slots
+
+    def set_inflow(self, normal_velocity) -> None:
+        """Per-face X-min inflow (float32, inflow_layout order); None restores the uniform freestream."""
+        if normal_velocity is None:
+            check(self._lib.pcfd_core_set_inflow_host(self.handle, None, 0))
+            return
+        check(self._lib.pcfd_core_set_inflow_host(self.handle, ptr(normal_velocity, C.c_float), normal_velocity.size))
+
+    def synchronize(self) -> None:
+        """Wait for all work queued on the system stream."""
+        check(self._lib.pcfd_system_synchronize(self.handle))
+
+    @property
+    def fused_preconditioner(self) -> bool:
+        flag = C.c_int32()
+        check(self._lib.pcfd_preconditioner_fused(self.handle, C.byref(flag)))
+        return bool(flag.value)
+
+    def launch_count(self) -> int:
+        """Kernels this system has launched on its stream so far."""
+        n = C.c_int64()
+        check(self._lib.pcfd_launch_count(self.handle, C.byref(n)))
+        return n.value
+
+    def profile_begin(self, region: int, capacity: int) -> None:
+        check(self._lib.pcfd_profile_begin(self.handle, region, capacity))
+
+    def profile_end(self, capacity: int) -> np.ndarray:
+        """Per-launch device milliseconds of the armed region since profile_begin."""
+        out = np.zeros(capacity, np.float64)
+        used = C.c_int32()
+        check(self._lib.pcfd_profile_end(self.handle, ptr(out, C.c_double), capacity, C.byref(used)))
+        return out[: min(used.value, capacity)]

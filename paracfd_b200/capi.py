@@ -14,7 +14,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIBRARY_PATH = os.path.join(_HERE, "libparacfd_b200.so")
 
-PCFD_OK = 0
+PCFD_OK, PCFD_INVALID_ARG, PCFD_NOT_CONVERGED = 0, 1, 3
 STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "CUDA_ERROR", 3: "NOT_CONVERGED",
                 4: "TOPOLOGY_UNRESOLVED", 5: "OUT_OF_MEMORY", 6: "TIMEOUT", 7: "INTERNAL"}
 
@@ -81,7 +81,7 @@ class Topology(C.Structure):
 
 class Options(C.Structure):
     _fields_ = [("mg_precision", C.c_int32), ("device", C.c_int32), ("stream", C.c_void_p),
-                ("momentum_min_volume_fraction", C.c_double)]
+                ("momentum_min_volume_fraction", C.c_double), ("disable_fused_smoother", C.c_int32)]
 
 
 class SolveResult(C.Structure):
@@ -198,6 +198,12 @@ SIGNATURES = {
     "pcfd_core_loads": (C.c_int, [C.c_void_p, C.c_double, _f64p, C.c_double, C.c_int32, C.POINTER(Loads)]),
     "pcfd_event_record": (C.c_int, [C.c_void_p, C.c_int32]),
     "pcfd_event_elapsed": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
+    "pcfd_core_inflow_layout": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
+    "pcfd_core_set_inflow_host": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int64]),
+    "pcfd_launch_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "pcfd_preconditioner_fused": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
+    "pcfd_profile_begin": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
+    "pcfd_profile_end": (C.c_int, [C.c_void_p, _f64p, C.c_int32, C.POINTER(C.c_int32)]),
     "pcfd_builder_last_error": (C.c_char_p, []),
 }
 

@@ -142,6 +142,7 @@ namespace pcfd
             s.bs3 = s.bs * s.bs * s.bs;
             s.levels = t.level_count;
             s.S = t.storage_size;
+            s.Sp = (s.S + 63) & ~63;
             s.outlet = t.pressure_outlet_xmax != 0;
             s.full_nonorthogonal = t.gradient_node_count > 0;
             // brick slots
@@ -176,11 +177,22 @@ namespace pcfd
             s.brick_nbr.upload(nbr);
             s.brick_flags.upload(flags);
             s.active_brick_list.upload(active_list);
+            std::vector<int> inflow_slot(size_t(s.B), -1);
+            int inflow_bricks = 0;
+            for (const int slot : active_list)
+                if (flags[slot] & PCFD_BRICK_XMIN) inflow_slot[slot] = inflow_bricks++;
+            s.inflow_faces = inflow_bricks * s.bs * s.bs;
+            s.inflow_slot_of_brick.upload(inflow_slot);
+            s.inflow.alloc(size_t(s.inflow_faces));
             s.d_level_h.upload(s.level_h);
             // per DOF
             s.h_active.assign(t.active, t.active + s.S);
             s.h_volume.assign(t.volume, t.volume + s.S);
-            s.active.upload(s.h_active);
+            {
+                std::vector<uint8_t> padded(s.h_active);
+                padded.resize(size_t(s.Sp), 0);
+                s.active.upload(padded);
+            }
             s.cut_face_mask.upload(std::vector<uint8_t>(t.cut_face_mask, t.cut_face_mask + s.S));
             s.volume.upload(s.h_volume);
             s.aggregate.upload(std::vector<int>(t.preconditioner_aggregate, t.preconditioner_aggregate + s.S));
@@ -188,20 +200,24 @@ namespace pcfd
             s.diagonal.upload(diag);
             build_operator(s, t);
             build_multigrid(s, t, diag);
+            if (!options || !options->disable_fused_smoother) build_fine_smoother(s, t, diag);
             // Krylov storage
             for (DBuf<double>* v : {&s.r, &s.z, &s.dvec, &s.Ad, &s.t, &s.correction, &s.defect, &s.scratch_p, &s.scratch_out,
                                      &s.integrated, &s.rhs, &s.pressure})
-                v->alloc(size_t(s.S));
+                v->alloc(size_t(s.Sp));
             if (s.full_nonorthogonal)
             {
-                s.gmres_v.alloc(size_t(System::gmres_restart + 1) * s.S);
-                s.gmres_z.alloc(size_t(System::gmres_restart) * s.S);
-                s.recycle_u.alloc(size_t(System::recycle_capacity) * s.S);
-                s.recycle_c.alloc(size_t(System::recycle_capacity) * s.S);
+                s.gmres_v.alloc(size_t(System::gmres_restart + 1) * s.Sp);
+                s.gmres_z.alloc(size_t(System::gmres_restart) * s.Sp);
+                s.recycle_u.alloc(size_t(System::recycle_capacity) * s.Sp);
+                s.recycle_c.alloc(size_t(System::recycle_capacity) * s.Sp);
             }
             s.dot_partial.alloc(4096);
             s.dot_result.alloc(16);
+            s.block_partial.alloc(size_t(592) * (kMaxSet + 1));
+            s.block_result.alloc(size_t(4) * (kMaxSet + 1));
             cuda_check(cudaMallocHost(&s.pinned, 16 * sizeof(double)), "pinned scalars");
+            cuda_check(cudaMallocHost(&s.pinned_block, size_t(4) * (kMaxSet + 1) * sizeof(double)), "pinned block scalars");
             // flow state
             s.u.alloc(size_t(s.faces)); s.v.alloc(size_t(s.faces)); s.w.alloc(size_t(s.faces));
             s.divergence.alloc(size_t(s.S));
@@ -239,9 +255,11 @@ namespace pcfd
     {
         for (cudaEvent_t& e : markers)
             if (e) cudaEventDestroy(e);
+        for (cudaEvent_t e : profile_events) cudaEventDestroy(e);
         destroy_loads(*this);
         delete momentum;
         if (pinned) cudaFreeHost(pinned);
+        if (pinned_block) cudaFreeHost(pinned_block);
         if (own_stream && stream) cudaStreamDestroy(stream);
     }
 }
@@ -608,6 +626,88 @@ pcfd_status pcfd_core_step(pcfd_system* system, pcfd_step_stats* stats)
     });
 }
 
+pcfd_status pcfd_core_inflow_layout(pcfd_system* system, int64_t* face_count, int32_t* brick_slots)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(face_count != nullptr, "null face count");
+        *face_count = s.inflow_faces;
+        if (brick_slots && s.inflow_faces)
+        {
+            std::vector<int> map(size_t(s.B));
+            cuda_check(cudaMemcpy(map.data(), s.inflow_slot_of_brick, map.size() * sizeof(int), cudaMemcpyDeviceToHost),
+                       "inflow layout");
+            for (int slot = 0; slot < s.B; ++slot)
+                if (map[slot] >= 0) brick_slots[map[slot]] = slot;
+        }
+    });
+}
+
+pcfd_status pcfd_core_set_inflow_host(pcfd_system* system, const float* normal_velocity, int64_t count)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        if (count == 0) { s.inflow_set = false; return; }
+        require(count == s.inflow_faces, "inflow count must equal the X-min boundary face count");
+        h2d(s, s.inflow.p, normal_velocity, size_t(count));
+        s.inflow_set = true;
+    });
+}
+
+pcfd_status pcfd_preconditioner_fused(pcfd_system* system, int32_t* fused)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(fused != nullptr, "null output");
+        *fused = s.fine.enabled ? 1 : 0;
+    });
+}
+
+pcfd_status pcfd_launch_count(pcfd_system* system, int64_t* launches)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(launches != nullptr, "null launch count");
+        *launches = s.launches;
+    });
+}
+
+pcfd_status pcfd_profile_begin(pcfd_system* system, int32_t region, int32_t capacity)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(region >= PCFD_PROFILE_STRUCTURED_APPLY && region <= PCFD_PROFILE_PRECONDITIONER, "unknown profile region");
+        require(capacity > 0 && capacity <= (1 << 16), "profile capacity must be 1..65536");
+        while (int(s.profile_events.size()) < 2 * capacity)
+        {
+            cudaEvent_t e;
+            cuda_check(cudaEventCreate(&e), "profile event");
+            s.profile_events.push_back(e);
+        }
+        s.profile_used = 0;
+        s.profile_region = region;
+    });
+}
+
+pcfd_status pcfd_profile_end(pcfd_system* system, double* ms_per_launch, int32_t capacity, int32_t* launches)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(launches != nullptr, "null launch count");
+        s.profile_region = -1;
+        const int used = s.profile_used;
+        *launches = used;
+        if (used) cuda_check(cudaEventSynchronize(s.profile_events[2 * used - 1]), "profile sync");
+        for (int q = 0; q < used && q < capacity && ms_per_launch; ++q)
+        {
+            float ms = 0;
+            cuda_check(cudaEventElapsedTime(&ms, s.profile_events[2 * q], s.profile_events[2 * q + 1]), "profile elapsed");
+            ms_per_launch[q] = ms;
+        }
+        s.profile_used = 0;
+    });
+}
+
 pcfd_status pcfd_event_record(pcfd_system* system, int32_t slot)
 {
     return guarded([&] {
@@ -673,6 +773,26 @@ pcfd_status pcfd_time_kernel(pcfd_system* system, int32_t which, int32_t iterati
             case 3: launch_integrated_flux(s); launch_normalize(s, 0.0, false); break;
             case 4: launch_correct_fluxes(s, 1.0, 1e-3); break;
             case 5: device_dot(s, s.scratch_p, s.scratch_out); break;
+            case 6:
+            case 7:
+            case 8: preconditioner_stage(s, which - 6, s.scratch_p, s.scratch_out); break;
+            case 9:
+            {
+                // one GCRO column orthogonalisation against 3 recycled + 13 basis vectors
+                require(s.full_nonorthogonal, "block orthogonalisation needs the GCRO storage");
+                VecSet Q, U;
+                for (int c = 0; c < System::recycle_capacity; ++c)
+                {
+                    Q.push(s.recycle_c.p + size_t(c) * s.Sp);
+                    U.push(s.recycle_u.p + size_t(c) * s.Sp);
+                }
+                for (int row = 0; row < 13; ++row) Q.push(s.gmres_v.p + size_t(row) * s.Sp);
+                double* h = s.block_result.p;
+                block_dot(s, Q, s.Ad, h);
+                block_update(s, Q, h, s.Ad, U, -1.0, s.gmres_z.p, 2, h + kMaxSet + 1);
+                block_update(s, Q, h + kMaxSet + 1, s.Ad, U, -1.0, s.gmres_z.p, 1, h + 2 * (kMaxSet + 1));
+                break;
+            }
             default: throw Error(PCFD_INVALID_ARG, "unknown kernel id");
             }
         };

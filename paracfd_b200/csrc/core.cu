@@ -70,14 +70,14 @@ namespace pcfd
         const float speed = float(c.speed);
         DBuf<uint8_t> connected;
         connected.upload(s.h_connected);
-        init_state_kernel<<<blocks_for(s.S), kThreads, 0, s.stream>>>(s.active, connected, s.S, speed, m.x, m.y, m.z, m.xn, m.yn, m.zn);
+        init_state_kernel<<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(s.active, connected, s.S, speed, m.x, m.y, m.z, m.xn, m.yn, m.zn);
         cuda_check(cudaMemsetAsync(s.u, 0, size_t(s.faces) * sizeof(float), s.stream), "clear faces");
         cuda_check(cudaMemsetAsync(s.v, 0, size_t(s.faces) * sizeof(float), s.stream), "clear faces");
         cuda_check(cudaMemsetAsync(s.w, 0, size_t(s.faces) * sizeof(float), s.stream), "clear faces");
         cuda_check(cudaMemsetAsync(s.special, 0, size_t(s.cf_count + s.eb_count) * sizeof(float), s.stream), "clear special");
         momentum_reconstruct_fluxes(s, m);
         if (s.active_bricks)
-            init_x_boundary_kernel<<<blocks_for(int64_t(s.active_bricks) * s.bs * s.bs), kThreads, 0, s.stream>>>(
+            init_x_boundary_kernel<<<blocks_for(int64_t(s.active_bricks) * s.bs * s.bs), kThreads, 0, launch_stream(s)>>>(
                 s.active_brick_list, s.active_bricks, s.bs, s.brick_flags, s.active, connected, speed, s.u);
         momentum_external_boundaries(s, speed);
         const double maximum = std::max(1e-9, std::abs(c.speed));

@@ -145,10 +145,10 @@ namespace pcfd
         Momentum& m = momentum_of(s);
         const IrregularOperator& o = s.irr;
         const int sides = viscous ? m.nW : 0;
-        loads_partial_kernel<<<kLoadBlocks, 256, 0, s.stream>>>(
+        loads_partial_kernel<<<kLoadBlocks, 256, 0, launch_stream(s)>>>(
             L.patches, L.area, L.centroid_p, L.normal, L.plus, L.minus, s.pressure32, L.pnode, o.grad_offset, o.grad_neighbour,
             o.grad_weight, L.dof_centroid, pref, origin[0], origin[1], origin[2], sides, m.w_force, L.side_patch, rho, L.partial);
-        loads_final_kernel<<<1, 256, 0, s.stream>>>(L.partial, kLoadBlocks, L.result);
+        loads_final_kernel<<<1, 256, 0, launch_stream(s)>>>(L.partial, kLoadBlocks, L.result);
         cuda_check(cudaMemcpyAsync(L.pinned, L.result, 12 * sizeof(double), cudaMemcpyDeviceToHost, s.stream), "loads readback");
         cuda_check(cudaStreamSynchronize(s.stream), "loads");
         for (int k = 0; k < 12; ++k) out[k] = L.pinned[k];

@@ -91,7 +91,16 @@ namespace pcfd
             return vb - 0.5f * (1.0f - fminf(1.0f, courant)) * minmod_cell(vb - va, vu - vb);
         }
 
-        __device__ inline float face_at(const float* u, const float* v, const float* w, int bs, int axis, int slot, int i, int j, int k)
+        // X-min inflow normal velocity of boundary face (j, k) of a brick: the per-face profile when one
+        // was set (pcfd_core_set_inflow_host), otherwise the uniform freestream.
+        __device__ inline float inflow_value(const int* slot_map, const float* inflow, int bs, int slot, int j, int k, float U)
+        {
+            if (!inflow) return U;
+            const int pos = slot_map[slot];
+            return pos >= 0 ? inflow[int64_t(pos) * bs * bs + k * bs + j] : U;
+        }
+
+        __device__ inline float face_at(const float* u,const float* v, const float* w, int bs, int axis, int slot, int i, int j, int k)
         {
             return axis == 0 ? u[u_face(bs, slot, i, j, k)] : (axis == 1 ? v[v_face(bs, slot, i, j, k)] : w[w_face(bs, slot, i, j, k)]);
         }
@@ -120,7 +129,7 @@ namespace pcfd
             const int* __restrict__ nbr, const uint32_t* __restrict__ flags, const double* __restrict__ level_h,
             const uint8_t* __restrict__ code, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w,
             const float* __restrict__ x, const float* __restrict__ y, const float* __restrict__ z, float dt, int external, float U,
-            float* __restrict__ xn, float* __restrict__ yn, float* __restrict__ zn, float* __restrict__ dx, float* __restrict__ dy,
+            const int* __restrict__ inflow_slot, const float* __restrict__ inflow, float* __restrict__ xn, float* __restrict__ yn, float* __restrict__ zn, float* __restrict__ dx, float* __restrict__ dy,
             float* __restrict__ dz)
         {
             const int64_t work = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -168,7 +177,8 @@ namespace pcfd
                 if (c.i == 0 && (fl & PCFD_BRICK_XMIN))
                 {
                     const float normal = u[u_face(bs, c.slot, 0, c.j, c.k)], swept = dt * area * normal;
-                    if (swept >= 0.0f) { D[0] += swept * U; D[1] += swept * 0.0f; D[2] += swept * 0.0f; }
+                    const float in = inflow_value(inflow_slot, inflow, bs, c.slot, c.j, c.k, U);
+                    if (swept >= 0.0f) { D[0] += swept * in; D[1] += swept * 0.0f; D[2] += swept * 0.0f; }
                     else { D[0] += swept * x[a]; D[1] += swept * y[a]; D[2] += swept * z[a]; }
                 }
                 if (c.i == bs - 1 && (fl & PCFD_BRICK_XMAX))
@@ -757,7 +767,7 @@ namespace pcfd
 
         // ---------------------------------------------------------------- boundaries
         __global__ void external_boundary_kernel(const int* __restrict__ brick_list, int nbricks, int bs, const uint32_t* __restrict__ flags,
-            float speed, float* u, float* v, float* w)
+            float speed, const int* __restrict__ inflow_slot, const float* __restrict__ inflow, float* u, float* v, float* w)
         {
             const int64_t work = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
             const int per = bs * bs;
@@ -766,7 +776,7 @@ namespace pcfd
             const int slot = brick_list[brick];
             const uint32_t fl = flags[slot];
             if (!(fl & (1u << face))) return;
-            if (face == 0) u[u_face(bs, slot, 0, a, b)] = speed;                       // X-min prescribed inflow
+            if (face == 0) u[u_face(bs, slot, 0, a, b)] = inflow_value(inflow_slot, inflow, bs, slot, a, b, speed);   // X-min inflow
             else if (face == 2 || face == 3) v[v_face(bs, slot, a, face == 3 ? bs : 0, b)] = 0.0f;   // Y free slip
             else if (face == 4 || face == 5) w[w_face(bs, slot, a, b, face == 5 ? bs : 0)] = 0.0f;   // Z free slip
         }
@@ -897,7 +907,7 @@ namespace pcfd
         void special_gradients(System& s, Momentum& m)
         {
             if (m.nS)
-                special_gradient_kernel<<<blocks_for(m.nS), kThreads, 0, s.stream>>>(m.nS, m.s_dof, m.s_offset, m.s_neighbor, m.s_weight,
+                special_gradient_kernel<<<blocks_for(m.nS), kThreads, 0, launch_stream(s)>>>(m.nS, m.s_dof, m.s_offset, m.s_neighbor, m.s_weight,
                                                                                    m.s_inverse, m.x, m.y, m.z, m.s_gradient);
         }
 
@@ -905,11 +915,11 @@ namespace pcfd
         {
             const CompactArgs k = compact_args(s, m);
             if (m.nD)
-                deferred_finish_kernel<<<blocks_for(m.nD), kThreads, 0, s.stream>>>(
+                deferred_finish_kernel<<<blocks_for(m.nD), kThreads, 0, launch_stream(s)>>>(
                     m.nD, m.d_dof, m.d_offset, m.d_edge, m.d_sign, m.d_group, s.structured, k, mode, dt, m.viscosity, s.u, s.v, s.w,
                     s.special, m.x, m.y, m.z, m.dx, m.dy, m.dz, m.xn, m.yn, m.zn, m.d_delta);
             if (m.nG)
-                group_apply_kernel<<<blocks_for(m.nG), kThreads, 0, s.stream>>>(m.nG, m.g_offset, m.g_member, m.g_volume, m.d_dof,
+                group_apply_kernel<<<blocks_for(m.nG), kThreads, 0, launch_stream(s)>>>(m.nG, m.g_offset, m.g_member, m.g_volume, m.d_dof,
                                                                                m.d_delta, m.x, m.y, m.z, m.xn, m.yn, m.zn);
             swap_state(m);
         }
@@ -919,9 +929,9 @@ namespace pcfd
     {
         special_gradients(s, m);
         if (s.active_bricks)
-            transport_struct_kernel<<<cell_blocks(s), kThreads, 0, s.stream>>>(
+            transport_struct_kernel<<<cell_blocks(s), kThreads, 0, launch_stream(s)>>>(
                 s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr, s.brick_flags, s.d_level_h, m.code, s.u, s.v,
-                s.w, m.x, m.y, m.z, dt, external_aero ? 1 : 0, freestream, m.xn, m.yn, m.zn, m.dx, m.dy, m.dz);
+                s.w, m.x, m.y, m.z, dt, external_aero ? 1 : 0, freestream, s.inflow_slot_of_brick, s.inflow_set ? s.inflow.p : nullptr, m.xn, m.yn, m.zn, m.dx, m.dy, m.dz);
         finish_buffered(s, m, 0, dt);
         cuda_check(cudaGetLastError(), "momentum transport");
     }
@@ -931,22 +941,22 @@ namespace pcfd
         if (nu == 0.0f && cs == 0.0f) { m.last_rate = 0; m.last_substeps = 1; return 0; }
         special_gradients(s, m);
         if (s.active_bricks)
-            viscosity_struct_kernel<<<cell_blocks(s), kThreads, 0, s.stream>>>(
+            viscosity_struct_kernel<<<cell_blocks(s), kThreads, 0, launch_stream(s)>>>(
                 s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr, s.d_level_h, m.code, m.special, m.volume32,
                 m.x, m.y, m.z, nu, cs, m.viscosity);
         if (m.nS)
-            viscosity_special_kernel<<<blocks_for(m.nS), kThreads, 0, s.stream>>>(m.nS, m.s_dof, m.s_gradient, m.volume32, nu, cs, m.viscosity);
+            viscosity_special_kernel<<<blocks_for(m.nS), kThreads, 0, launch_stream(s)>>>(m.nS, m.s_dof, m.s_gradient, m.volume32, nu, cs, m.viscosity);
         // spectral rate -> substeps (one scalar readback)
         const CompactArgs k = compact_args(s, m);
         const int cb = s.active_bricks ? cell_blocks(s) : 0, db = m.nD ? blocks_for(m.nD) : 0;
         require(cb + db <= int(m.reduce_partial.n), "reduction scratch too small");
         if (cb)
-            rate_struct_kernel<<<cb, 256, 0, s.stream>>>(s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr,
+            rate_struct_kernel<<<cb, 256, 0, launch_stream(s)>>>(s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr,
                                                         s.d_level_h, m.code, m.viscosity, m.dx, m.reduce_partial);
         if (db)
-            rate_deferred_kernel<<<db, 256, 0, s.stream>>>(m.nD, m.d_dof, m.d_offset, m.d_edge, s.structured, k, m.viscosity, m.dx,
+            rate_deferred_kernel<<<db, 256, 0, launch_stream(s)>>>(m.nD, m.d_dof, m.d_offset, m.d_edge, s.structured, k, m.viscosity, m.dx,
                                                           m.reduce_partial.p + cb);
-        max_final_kernel<<<1, 256, 0, s.stream>>>(m.reduce_partial, cb + db, m.reduce_result);
+        max_final_kernel<<<1, 256, 0, launch_stream(s)>>>(m.reduce_partial, cb + db, m.reduce_result);
         cuda_check(cudaMemcpyAsync(m.pinned, m.reduce_result, sizeof(float), cudaMemcpyDeviceToHost, s.stream), "rate readback");
         cuda_check(cudaStreamSynchronize(s.stream), "rate readback");
         m.last_rate = double(m.pinned[0]);
@@ -955,7 +965,7 @@ namespace pcfd
         for (int sub = 0; sub < m.last_substeps; ++sub)
         {
             if (s.active_bricks)
-                diffuse_struct_kernel<<<cell_blocks(s), kThreads, 0, s.stream>>>(
+                diffuse_struct_kernel<<<cell_blocks(s), kThreads, 0, launch_stream(s)>>>(
                     s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr, s.d_level_h, m.code, m.viscosity, m.x, m.y,
                     m.z, sub_dt, m.xn, m.yn, m.zn, m.dx, m.dy, m.dz);
             finish_buffered(s, m, 1, sub_dt);
@@ -968,15 +978,15 @@ namespace pcfd
     {
         if (!m.nW) return;
         if (m.nG)
-            save_deferred_kernel<<<blocks_for(m.nD), kThreads, 0, s.stream>>>(m.nD, m.d_dof, m.d_group, m.x, m.y, m.z, m.baseline_x,
+            save_deferred_kernel<<<blocks_for(m.nD), kThreads, 0, launch_stream(s)>>>(m.nD, m.d_dof, m.d_group, m.x, m.y, m.z, m.baseline_x,
                                                                              m.baseline_y, m.baseline_z);
-        wall_coefficient_kernel<<<blocks_for(m.nW), kThreads, 0, s.stream>>>(m.nW, m.w_dof, m.w_normal, m.w_area, m.w_distance, m.x,
+        wall_coefficient_kernel<<<blocks_for(m.nW), kThreads, 0, launch_stream(s)>>>(m.nW, m.w_dof, m.w_normal, m.w_area, m.w_distance, m.x,
                                                                            m.y, m.z, nu, m.w_k);
-        wall_apply_kernel<<<blocks_for(m.nWall), kThreads, 0, s.stream>>>(m.nWall, m.wall_dof, m.wall_offset, m.wall_side, m.w_normal,
+        wall_apply_kernel<<<blocks_for(m.nWall), kThreads, 0, launch_stream(s)>>>(m.nWall, m.wall_dof, m.wall_offset, m.wall_side, m.w_normal,
                                                                         m.w_k, m.volume32, dt, m.x, m.y, m.z);
-        wall_force_kernel<<<blocks_for(m.nW), kThreads, 0, s.stream>>>(m.nW, m.w_dof, m.w_normal, m.w_k, m.x, m.y, m.z, m.w_force);
+        wall_force_kernel<<<blocks_for(m.nW), kThreads, 0, launch_stream(s)>>>(m.nW, m.w_dof, m.w_normal, m.w_k, m.x, m.y, m.z, m.w_force);
         if (m.nG)
-            group_increment_kernel<<<blocks_for(m.nG), kThreads, 0, s.stream>>>(m.nG, m.g_offset, m.g_member, m.g_volume, m.d_dof,
+            group_increment_kernel<<<blocks_for(m.nG), kThreads, 0, launch_stream(s)>>>(m.nG, m.g_offset, m.g_member, m.g_volume, m.d_dof,
                                                                               m.volume32, m.baseline_x, m.baseline_y, m.baseline_z, 1,
                                                                               m.x, m.y, m.z);
         cuda_check(cudaGetLastError(), "smooth wall");
@@ -987,21 +997,21 @@ namespace pcfd
         const float scale = dt / rho;
         IrregularOperator& o = s.irr;
         if (o.gradient_nodes)
-            pressure_gradient32_kernel<<<blocks_for(o.gradient_nodes), kThreads, 0, s.stream>>>(
+            pressure_gradient32_kernel<<<blocks_for(o.gradient_nodes), kThreads, 0, launch_stream(s)>>>(
                 o.gradient_nodes, o.grad_dof, o.grad_offset, o.grad_neighbour, m.p_weight, s.pressure32, m.p_gradient);
         if (s.active_bricks)
-            impulse_struct_kernel<<<cell_blocks(s), kThreads, 0, s.stream>>>(
+            impulse_struct_kernel<<<cell_blocks(s), kThreads, 0, launch_stream(s)>>>(
                 s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr, s.brick_flags, s.d_level_h, m.code, s.pressure32,
                 scale, s.outlet ? 1 : 0, physical ? 1 : 0, m.x, m.y, m.z, m.xn, m.yn, m.zn, m.dx, m.dy, m.dz);
         const CompactArgs k = compact_args(s, m);
         if (m.nD)
-            impulse_deferred_kernel<<<blocks_for(m.nD), kThreads, 0, s.stream>>>(
+            impulse_deferred_kernel<<<blocks_for(m.nD), kThreads, 0, launch_stream(s)>>>(
                 m.nD, m.d_dof, m.d_offset, m.d_edge, m.d_sign, m.d_side_offset, m.d_side, m.d_boundary_offset, m.d_boundary,
                 s.structured, k, s.pressure32, m.p_gradient, m.w_pnode, m.w_coefficient, m.w_disp, m.b_coefficient, scale,
                 physical ? 1 : 0, m.x, m.y, m.z, m.dx, m.dy, m.dz, m.xn, m.yn, m.zn);
         swap_state(m);   // previous state (now xn) is the redistribution baseline
         if (m.nG)
-            group_increment_kernel<<<blocks_for(m.nG), kThreads, 0, s.stream>>>(m.nG, m.g_offset, m.g_member, m.g_volume, m.d_dof,
+            group_increment_kernel<<<blocks_for(m.nG), kThreads, 0, launch_stream(s)>>>(m.nG, m.g_offset, m.g_member, m.g_volume, m.d_dof,
                                                                               m.volume32, m.xn, m.yn, m.zn, 0, m.x, m.y, m.z);
         cuda_check(cudaGetLastError(), "pressure impulse");
     }
@@ -1010,10 +1020,10 @@ namespace pcfd
     {
         special_gradients(s, m);
         if (s.active_bricks)
-            reconstruct_struct_kernel<<<cell_blocks(s), kThreads, 0, s.stream>>>(s.active_brick_list, s.active_bricks, s.bs, s.brick_level,
+            reconstruct_struct_kernel<<<cell_blocks(s), kThreads, 0, launch_stream(s)>>>(s.active_brick_list, s.active_bricks, s.bs, s.brick_level,
                                                                                s.brick_nbr, s.d_level_h, m.code, m.x, m.y, m.z, s.u, s.v, s.w);
         if (m.nK)
-            reconstruct_compact_kernel<<<blocks_for(m.nK), kThreads, 0, s.stream>>>(m.nK, compact_args(s, m), m.x, m.y, m.z, s.u, s.v,
+            reconstruct_compact_kernel<<<blocks_for(m.nK), kThreads, 0, launch_stream(s)>>>(m.nK, compact_args(s, m), m.x, m.y, m.z, s.u, s.v,
                                                                                   s.w, s.special);
         cuda_check(cudaGetLastError(), "flux reconstruction");
     }
@@ -1021,8 +1031,9 @@ namespace pcfd
     void momentum_external_boundaries(System& s, float speed)
     {
         if (!s.active_bricks) return;
-        external_boundary_kernel<<<blocks_for(int64_t(s.active_bricks) * 6 * s.bs * s.bs), kThreads, 0, s.stream>>>(
-            s.active_brick_list, s.active_bricks, s.bs, s.brick_flags, speed, s.u, s.v, s.w);
+        external_boundary_kernel<<<blocks_for(int64_t(s.active_bricks) * 6 * s.bs * s.bs), kThreads, 0, launch_stream(s)>>>(
+            s.active_brick_list, s.active_bricks, s.bs, s.brick_flags, speed, s.inflow_slot_of_brick,
+            s.inflow_set ? s.inflow.p : nullptr, s.u, s.v, s.w);
         cuda_check(cudaGetLastError(), "external boundaries");
     }
 
@@ -1032,13 +1043,13 @@ namespace pcfd
         const int cb = s.active_bricks ? cell_blocks(s) : 0, db = m.nD ? blocks_for(m.nD) : 0;
         require(2 * (cb + db) <= int(m.reduce_partial.n), "reduction scratch too small");
         if (cb)
-            cfl_struct_kernel<<<cb, 256, 0, s.stream>>>(s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr,
+            cfl_struct_kernel<<<cb, 256, 0, launch_stream(s)>>>(s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr,
                                                        s.brick_flags, s.d_level_h, m.code, s.u, s.v, s.w, m.x, m.y, m.z,
                                                        external_aero ? 1 : 0, m.dx, m.reduce_partial);
         if (db)
-            cfl_deferred_kernel<<<db, 256, 0, s.stream>>>(m.nD, m.d_dof, m.d_offset, m.d_edge, m.d_sign, s.structured, k, s.u, s.v, s.w,
+            cfl_deferred_kernel<<<db, 256, 0, launch_stream(s)>>>(m.nD, m.d_dof, m.d_offset, m.d_edge, m.d_sign, s.structured, k, s.u, s.v, s.w,
                                                          s.special, m.x, m.y, m.z, m.dx, m.reduce_partial.p + 2 * cb);
-        cfl_final_kernel<<<1, 256, 0, s.stream>>>(m.reduce_partial, cb + db, s.special, s.cf_count + s.eb_count, m.reduce_result);
+        cfl_final_kernel<<<1, 256, 0, launch_stream(s)>>>(m.reduce_partial, cb + db, s.special, s.cf_count + s.eb_count, m.reduce_result);
         cuda_check(cudaMemcpyAsync(m.pinned, m.reduce_result, 4 * sizeof(float), cudaMemcpyDeviceToHost, s.stream), "cfl readback");
         cuda_check(cudaStreamSynchronize(s.stream), "cfl readback");
         for (int q = 0; q < 4; ++q) out[q] = m.pinned[q];

@@ -110,10 +110,38 @@ namespace pcfd
 
     struct Scalars;   // device scalar block for the Krylov recurrences
 
+    // Fused fine-level multigrid work for 8^3 bricks (smoother.cu).
+    struct FineSmoother
+    {
+        bool enabled = false;
+        DBuf<uint8_t> code;                     // [S] open faces (bits 0-5), outlet (6), deferred (7)
+        int deferred_count = 0;
+        DBuf<int> deferred_dof, deferred_incident, gauge_offset;
+        DBuf<double> gauge_coefficient;
+        DBuf<int> meta;                         // [active bricks][16] slot, level, level-0 cell, partial, neighbours
+        DBuf<double> partial, deferred_residual;
+        DBuf<int> gather_offset, gather_entry;  // base cell -> partials (>= 0) / deferred rows (< 0)
+        DBuf<double> t, z;                      // [S] deferred structured rows, ping-pong iterate
+    };
+
+    // Up to kMaxSet vectors of one system, passed by value to the fused block kernels (krylov.cu).
+    constexpr int kMaxSet = 32;   // >= GCRO restart (24) + recycled pairs (3) + 1
+    struct VecSet
+    {
+        const double* v[kMaxSet] = {};
+        int count = 0;
+        void push(const double* p) { v[count++] = p; }
+    };
+    struct Coefficients
+    {
+        double value[kMaxSet] = {};
+    };
+
     struct System
     {
         // sizes
         int bs = 0, bs3 = 0, levels = 0, S = 0, B = 0, structured = 0, active_bricks = 0;
+        int Sp = 0;   // S rounded up to 64: length/stride of internal DOF vectors (16-byte aligned slots)
         int64_t faces = 0;   // per component
         bool outlet = true, full_nonorthogonal = false;
         int mg_precision = PCFD_MG_FP64;
@@ -147,6 +175,7 @@ namespace pcfd
         DBuf<int> base_restrict_offset, base_restrict_dof;
         std::vector<MgLevel<double>> mg64;
         std::vector<MgLevel<float>> mg32;
+        FineSmoother fine;
         DBuf<float> diagonal32;
 
         // Krylov vectors
@@ -156,6 +185,9 @@ namespace pcfd
         static constexpr int gmres_restart = 24;
         static constexpr int recycle_capacity = 3;
         DBuf<double> dot_partial;               // reduction scratch
+        DBuf<double> block_partial;             // [592][kMaxSet + 1] block-kernel partial sums
+        DBuf<double> block_result;              // [4][kMaxSet + 1] device coefficients / norms
+        double* pinned_block = nullptr;         // pinned host copy of block_result
         DBuf<double> dot_result;                // device scalars
         double* pinned = nullptr;               // pinned host scalars
 
@@ -185,6 +217,16 @@ namespace pcfd
         struct Momentum* momentum = nullptr;
         void* loads = nullptr;                  // surface-load integration state (loads.cu)
         cudaEvent_t markers[8] = {};
+        int64_t launches = 0;                   // kernels launched on the system stream so far
+        // per-launch event pairs around one instrumented region (PCFD_PROFILE_*), for the roofline
+        int profile_region = -1;
+        std::vector<cudaEvent_t> profile_events;   // [2 * capacity]
+        int profile_used = 0;
+        // X-min inflow: one normal velocity per boundary face, or uniform freestream when empty
+        int inflow_faces = 0;
+        DBuf<int> inflow_slot_of_brick;           // [B] -> position among X-min bricks or -1
+        DBuf<float> inflow;                       // [inflow_faces]
+        bool inflow_set = false;
         std::vector<uint8_t> h_connected;       // freestream_connected
         std::vector<int> xface_dof;             // [bricks with XMIN/XMAX faces] helper for initialisation
         pcfd_case config{};
@@ -194,6 +236,30 @@ namespace pcfd
         ~System();
     };
 
+    // Every kernel launch takes its stream from here, so the system counts its own launches.
+    inline cudaStream_t launch_stream(System& s)
+    {
+        ++s.launches;
+        return s.stream;
+    }
+
+    // Records a start/stop event pair on the system stream around one launch of the region being
+    // profiled; a no-op for every other region or once the event capacity is used up.
+    struct ProfileScope
+    {
+        System& s;
+        bool on;
+        ProfileScope(System& sys, int region)
+            : s(sys), on(sys.profile_region == region && 2 * (sys.profile_used + 1) <= int(sys.profile_events.size()))
+        {
+            if (on) cuda_check(cudaEventRecord(s.profile_events[2 * s.profile_used], s.stream), "profile event");
+        }
+        ~ProfileScope()
+        {
+            if (on) cudaEventRecord(s.profile_events[2 * s.profile_used++ + 1], s.stream);
+        }
+    };
+
     // ---- kernels / launchers (pressure.cu) ----
     void launch_apply(System& s, const double* p, double* out, bool orthogonal_only);
     void launch_apply32(System& s, const float* p, float* out);
@@ -201,6 +267,13 @@ namespace pcfd
     void build_operator(System& s, const pcfd_topology& t);
     void build_multigrid(System& s, const pcfd_topology& t, const std::vector<double>& diagonal);
     void apply_preconditioner(System& s, const double* r, double* z);
+    // 0: pre-smoothing (first Jacobi sweep pair), 1: coarse-grid correction, 2: post-smoothing
+    void preconditioner_stage(System& s, int stage, const double* r, double* z);
+    // fused fine level (smoother.cu) around the coarse hierarchy below it (solver.cu)
+    void build_fine_smoother(System& s, const pcfd_topology& t, const std::vector<double>& diagonal);
+    void brick_apply(System& s, const double* p, double* out);   // code-byte structured operator
+    template <class T> void fine_preconditioner(System& s, const double* r, double* z, std::vector<MgLevel<T>>& levels);
+    template <class T> void multigrid_levels(System& s, std::vector<MgLevel<T>>& levels);
     pcfd_solve_result solve(System& s, double* x, const double* b, double tolerance, int max_iterations, bool warm);
     // vector helpers
     void vec_copy_active(System& s, const double* src, double* dst);
@@ -210,6 +283,14 @@ namespace pcfd
     void vec_zero(System& s, double* x);
     void vec_update_solution_residual(System& s, double* x, double* r, const double* d, const double* Ad, double alpha);
     void vec_update_direction(System& s, const double* z, double* d, double beta);
+
+    // ---- fused block vector kernels (krylov.cu); all active-masked, deterministic ----
+    void block_dot(System& s, const VecSet& Q, const double* w, double* out);   // out[0..|Q|) = Q^T w, out[|Q|] = w.w
+    // w -= Q h; y += sign * U h[0..|U|); mode 1: out[0] = w'.w'; mode 2: out = Q^T w' then w'.w'
+    void block_update(System& s, const VecSet& Q, const double* h, double* w, const VecSet& U, double sign, double* y, int mode,
+                      double* out);
+    void block_combine(System& s, const VecSet& Z, const Coefficients& c, double* y, bool accumulate);   // y (+)= Z c
+    void scale_by_inverse_norm(System& s, double* dst, const double* src, const double* norm2);        // dst = src / sqrt(n2)
 
     // ---- projection (projection.cu) ----
     void build_projection(System& s, const pcfd_topology& t);
@@ -235,6 +316,8 @@ namespace pcfd
     {
         return axis == 0 ? u_face(bs, slot, i, j, k) : (axis == 1 ? v_face(bs, slot, i, j, k) : w_face(bs, slot, i, j, k));
     }
+
+    inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
     constexpr int kThreads = 256;
     inline int blocks_for(int64_t n, int threads = kThreads) { return int((n + threads - 1) / threads); }

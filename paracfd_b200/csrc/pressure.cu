@@ -250,30 +250,32 @@ namespace pcfd
     {
         if (s.active_bricks)
         {
-            if (s.bs == 8)
-                structured_apply8_kernel<double><<<s.active_bricks, 256, 0, s.stream>>>(
+            ProfileScope scope(s, PCFD_PROFILE_STRUCTURED_APPLY);
+            if (s.fine.enabled && aligned16(p) && aligned16(out)) brick_apply(s, p, out);
+            else if (s.bs == 8)
+                structured_apply8_kernel<double><<<s.active_bricks, 256, 0, launch_stream(s)>>>(
                     s.active_brick_list, s.brick_level, s.brick_nbr, s.brick_flags, s.d_level_h, s.active,
                     s.cut_face_mask, p, out, s.outlet ? 1 : 0);
             else
-                structured_apply_generic_kernel<double><<<blocks_for(int64_t(s.active_bricks) * s.bs3), kThreads, 0, s.stream>>>(
+                structured_apply_generic_kernel<double><<<blocks_for(int64_t(s.active_bricks) * s.bs3), kThreads, 0, launch_stream(s)>>>(
                     s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr, s.brick_flags, s.d_level_h,
                     s.active, s.cut_face_mask, p, out, s.outlet ? 1 : 0);
         }
         if (s.S > s.structured)
-            zero_range_kernel<<<blocks_for(s.S - s.structured), kThreads, 0, s.stream>>>(out, s.structured, s.S);
+            zero_range_kernel<<<blocks_for(s.S - s.structured), kThreads, 0, launch_stream(s)>>>(out, s.structured, s.S);
         IrregularOperator& o = s.irr;
         if (o.incident_dofs)
-            irregular_orthogonal_gather_kernel<<<blocks_for(o.incident_dofs), kThreads, 0, s.stream>>>(
+            irregular_orthogonal_gather_kernel<<<blocks_for(o.incident_dofs), kThreads, 0, launch_stream(s)>>>(
                 o.incident_dof, o.incident_offset, o.incident_edge, o.incident_sign, o.incident_dofs, o.connection_count,
                 o.conn_lower, o.conn_upper, o.conn_coefficient, o.reg_lower, o.reg_upper, o.reg_coefficient, s.active, p, out);
         if (o.gauges)
-            gauge_apply_kernel<<<blocks_for(o.gauges), kThreads, 0, s.stream>>>(o.gauge_dof, o.gauge_coefficient, o.gauges, p, out);
+            gauge_apply_kernel<<<blocks_for(o.gauges), kThreads, 0, launch_stream(s)>>>(o.gauge_dof, o.gauge_coefficient, o.gauges, p, out);
         if (!orthogonal_only && o.gradient_nodes)
         {
-            reconstruct_gradient_kernel<<<blocks_for(o.gradient_nodes), kThreads, 0, s.stream>>>(
+            reconstruct_gradient_kernel<<<blocks_for(o.gradient_nodes), kThreads, 0, launch_stream(s)>>>(
                 o.grad_dof, o.grad_offset, o.grad_neighbour, o.grad_weight, p, o.gradient, o.gradient_nodes);
             if (o.incident_dofs)
-                irregular_nonorthogonal_gather_kernel<<<blocks_for(o.incident_dofs), kThreads, 0, s.stream>>>(
+                irregular_nonorthogonal_gather_kernel<<<blocks_for(o.incident_dofs), kThreads, 0, launch_stream(s)>>>(
                     o.incident_dof, o.incident_offset, o.incident_edge, o.incident_sign, o.incident_dofs, o.connection_count,
                     o.conn_lower, o.conn_upper, o.conn_lower_node, o.conn_upper_node, o.conn_correction, o.conn_upper_weight,
                     o.conn_area, o.reg_lower, o.reg_upper, o.reg_lower_node, o.reg_upper_node, o.reg_correction,
@@ -326,8 +328,8 @@ namespace pcfd
 
     double device_dot(System& s, const double* a, const double* b)
     {
-        dot_partial_kernel<<<kDotBlocks, 256, 0, s.stream>>>(a, b, s.active, s.S, s.dot_partial);
-        dot_final_kernel<<<1, 256, 0, s.stream>>>(s.dot_partial, kDotBlocks, s.dot_result);
+        dot_partial_kernel<<<kDotBlocks, 256, 0, launch_stream(s)>>>(a, b, s.active, s.S, s.dot_partial);
+        dot_final_kernel<<<1, 256, 0, launch_stream(s)>>>(s.dot_partial, kDotBlocks, s.dot_result);
         cuda_check(cudaMemcpyAsync(s.pinned, s.dot_result, sizeof(double), cudaMemcpyDeviceToHost, s.stream), "dot readback");
         cuda_check(cudaStreamSynchronize(s.stream), "dot synchronize");
         return s.pinned[0];
@@ -372,27 +374,27 @@ namespace pcfd
     }
     void vec_copy_active(System& s, const double* src, double* dst)
     {
-        copy_active_kernel<<<blocks_for(s.S), kThreads, 0, s.stream>>>(src, dst, s.active, s.S);
+        copy_active_kernel<<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(src, dst, s.active, s.S);
     }
     void vec_subtract(System& s, double* r, const double* v)
     {
-        subtract_kernel<<<blocks_for(s.S), kThreads, 0, s.stream>>>(r, v, s.active, s.S);
+        subtract_kernel<<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(r, v, s.active, s.S);
     }
     void vec_axpy_active(System& s, double* y, const double* x, double a)
     {
-        axpy_active_kernel<<<blocks_for(s.S), kThreads, 0, s.stream>>>(y, x, a, s.active, s.S);
+        axpy_active_kernel<<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(y, x, a, s.active, s.S);
     }
     void vec_scaled_copy_active(System& s, double* dst, const double* src, double a)
     {
-        scaled_copy_active_kernel<<<blocks_for(s.S), kThreads, 0, s.stream>>>(dst, src, a, s.active, s.S);
+        scaled_copy_active_kernel<<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(dst, src, a, s.active, s.S);
     }
     void vec_update_solution_residual(System& s, double* x, double* r, const double* d, const double* Ad, double alpha)
     {
-        update_solution_residual_kernel<<<blocks_for(s.S), kThreads, 0, s.stream>>>(x, r, d, Ad, alpha, s.active, s.S);
+        update_solution_residual_kernel<<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(x, r, d, Ad, alpha, s.active, s.S);
     }
     void vec_update_direction(System& s, const double* z, double* d, double beta)
     {
-        update_direction_kernel<<<blocks_for(s.S), kThreads, 0, s.stream>>>(z, d, beta, s.active, s.S);
+        update_direction_kernel<<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(z, d, beta, s.active, s.S);
     }
     void vec_zero(System& s, double* x)
     {

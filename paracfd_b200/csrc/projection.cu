@@ -381,13 +381,13 @@ namespace pcfd
     void launch_integrated_flux(System& s)
     {
         if (s.active_bricks)
-            structured_integrated_flux_kernel<<<blocks_for(int64_t(s.active_bricks) * s.bs3), kThreads, 0, s.stream>>>(
+            structured_integrated_flux_kernel<<<blocks_for(int64_t(s.active_bricks) * s.bs3), kThreads, 0, launch_stream(s)>>>(
                 s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr, s.brick_flags, s.d_level_h, s.active,
                 s.cut_face_mask, s.u, s.v, s.w, s.integrated);
         if (s.S > s.structured)
-            zero_tail_kernel<<<blocks_for(s.S - s.structured), kThreads, 0, s.stream>>>(s.integrated, s.structured, s.S);
+            zero_tail_kernel<<<blocks_for(s.S - s.structured), kThreads, 0, launch_stream(s)>>>(s.integrated, s.structured, s.S);
         if (s.special_incident_dofs)
-            special_integrated_flux_kernel<<<blocks_for(s.special_incident_dofs), kThreads, 0, s.stream>>>(
+            special_integrated_flux_kernel<<<blocks_for(s.special_incident_dofs), kThreads, 0, launch_stream(s)>>>(
                 s.special_incident_dof, s.special_incident_offset, s.special_incident_edge, s.special_incident_sign,
                 s.special_incident_dofs, s.special_area, s.special, s.integrated);
         cuda_check(cudaGetLastError(), "integrated flux");
@@ -395,7 +395,7 @@ namespace pcfd
 
     void launch_normalize(System& s, double rho_over_dt, bool with_rhs)
     {
-        normalize_kernel<<<blocks_for(s.S), kThreads, 0, s.stream>>>(s.integrated, s.volume, s.active, rho_over_dt, s.divergence,
+        normalize_kernel<<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(s.integrated, s.volume, s.active, rho_over_dt, s.divergence,
                                                                     with_rhs ? s.rhs.p : nullptr, s.S);
         cuda_check(cudaGetLastError(), "normalize divergence");
     }
@@ -404,25 +404,25 @@ namespace pcfd
     {
         const double scale = dt / rho;
         if (s.active_bricks)
-            structured_correction_kernel<<<blocks_for(int64_t(s.active_bricks) * s.bs3), kThreads, 0, s.stream>>>(
+            structured_correction_kernel<<<blocks_for(int64_t(s.active_bricks) * s.bs3), kThreads, 0, launch_stream(s)>>>(
                 s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr, s.brick_flags, s.d_level_h, s.active,
                 s.cut_face_mask, s.pressure, scale, s.outlet ? 1 : 0, s.u, s.v, s.w);
         IrregularOperator& o = s.irr;
         if (o.gradient_nodes)
-            gradient_kernel<<<blocks_for(o.gradient_nodes), kThreads, 0, s.stream>>>(o.grad_dof, o.grad_offset, o.grad_neighbour,
+            gradient_kernel<<<blocks_for(o.gradient_nodes), kThreads, 0, launch_stream(s)>>>(o.grad_dof, o.grad_offset, o.grad_neighbour,
                                                                                    o.grad_weight, s.pressure, o.gradient, o.gradient_nodes);
         if (o.regular_count)
-            regular_correction_kernel<<<blocks_for(o.regular_count), kThreads, 0, s.stream>>>(
+            regular_correction_kernel<<<blocks_for(o.regular_count), kThreads, 0, launch_stream(s)>>>(
                 s.reg_face, s.reg_mirror, s.reg_axis, o.reg_lower, o.reg_upper, o.reg_lower_node, o.reg_upper_node, o.reg_delta,
                 o.reg_correction, o.reg_upper_weight, o.gradient_nodes ? o.gradient.p : nullptr, s.pressure, scale, o.regular_count,
                 s.u, s.v, s.w);
         const int nc = s.cf_count + s.eb_count;
         if (nc)
-            special_correction_kernel<<<blocks_for(nc), kThreads, 0, s.stream>>>(
+            special_correction_kernel<<<blocks_for(nc), kThreads, 0, launch_stream(s)>>>(
                 s.special_lower, s.special_upper, s.special_factor, s.special_lower_node, s.special_upper_node, s.special_correction,
                 s.special_upper_weight, o.gradient_nodes ? o.gradient.p : nullptr, s.active, s.pressure, scale, nc, s.special);
         if (s.cf_groups)
-            coarse_fine_scatter_kernel<<<blocks_for(s.cf_groups), kThreads, 0, s.stream>>>(
+            coarse_fine_scatter_kernel<<<blocks_for(s.cf_groups), kThreads, 0, launch_stream(s)>>>(
                 s.cf_group_offset, s.cf_group_member, s.cf_group_face, s.cf_group_axis, s.cf_fine_face, s.cf_axis, s.special_area,
                 s.special, s.cf_groups, s.u, s.v, s.w);
         cuda_check(cudaGetLastError(), "correct fluxes");
@@ -430,7 +430,7 @@ namespace pcfd
 
     void launch_convert_pressure(System& s)
     {
-        convert_pressure_kernel<<<blocks_for(s.S), kThreads, 0, s.stream>>>(s.pressure, s.pressure32, s.S);
+        convert_pressure_kernel<<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(s.pressure, s.pressure32, s.S);
         cuda_check(cudaGetLastError(), "convert pressure");
     }
 }

@@ -1,0 +1,577 @@
+// smoother.cu -- fused fine-level work of the multigrid preconditioner for 8^3 bricks.
+//
+// The reference cycle (src/core/fluid/amr_pressure.cu:1103-1154) runs, per application,
+// z = w D^-1 r, then three times "t = A_orth z; z += w D^-1 (r - t)", restricts r - A_orth z to
+// the level-0 aggregates and prolongs the coarse correction back: ~10 full passes over the FP64
+// vectors plus a serial per-aggregate gather.  Here every fine-level stage is one brick-tiled
+// launch that reads z (tile + halo staged in shared memory), r and one code byte per DOF:
+//   sweep      z_new = z + w (r - A_struct z) / D          (ping-pong buffers)
+//   residual   per-brick partial sums of r - A_struct z for each level-0 cell the brick covers
+//   prolong    the coarse correction is added while the tile is staged (z + e[aggregate])
+// The code byte holds the six open-face bits (both cells active and the face not cut), the
+// X-max outlet bit and a "deferred" bit.  Deferred DOFs are those whose operator row has more
+// than the structured 7-point part -- compact coarse/fine, embedded or regular edges, gauges,
+// EB fragments, a diagonal that the code bits do not reproduce bit for bit -- and a small
+// per-DOF "finish" kernel completes them with the reference's irregular gather in the same
+// summation order.  Non-deferred rows use D = sum of h over the open faces (+ 2h outlet), which
+// equals the assembled diagonal bit for bit (checked at setup), so every sweep produces the
+// same bits as the unfused kernels; only the restriction sums in a different order.
+#include "pcfd_internal.h"
+
+#include <algorithm>
+#include <cmath>
+#include <unordered_map>
+
+namespace pcfd
+{
+    namespace
+    {
+        constexpr uint8_t kDeferred = 0x80, kOutlet = 0x40, kOpenMask = 0x3f;
+        constexpr int kBS = 8, kC3 = 512;
+
+        // Per active brick (indexed by position in the active list, so that one round trip
+        // fetches everything a CTA needs before its data loads): 64 bytes.
+        struct BrickMeta
+        {
+            int slot, level, base, partial;
+            int nbr[6];     // active same-level neighbour slot or -1
+            int nbase[6];   // level-0 cell of each neighbour's first cell
+        };
+
+        struct BrickHead
+        {
+            int slot, level, base, partial;
+        };
+
+        struct BrickView
+        {
+            const BrickMeta* meta;
+            const double* level_h;
+            const uint8_t* code;
+        };
+
+        // Shared tile of one brick plus its face halos: rows of 12 doubles so that interior rows
+        // start 16-byte aligned (x = -1 at offset 1, x = 0..7 at 2..9, x = 8 at 10).
+        constexpr int kP1 = 12, kP2 = 120, kTileSize = 10 * kP2;
+        __device__ inline int tix(int i, int j, int k) { return (k + 1) * kP2 + (j + 1) * kP1 + (i + 2); }
+
+        // base cell of cell (i,j,k) of a brick at level l whose (0,0,0) cell lies in base cell `b0`
+        __device__ inline int base_cell_of(int b0, int l, int i, int j, int k)
+        {
+            return b0 + ((k >> l) << 6) + ((j >> l) << 3) + (i >> l);
+        }
+
+        // Stage z (+ prolonged coarse correction) of one brick and its six face halos with one
+        // 16-byte interior load and one halo load per thread (256 threads), all independent.
+        template <class TC, bool kProlong>
+        __device__ inline void stage_tile(const BrickHead& m, const BrickMeta* __restrict__ gm, const double* __restrict__ z,
+                                          const TC* __restrict__ e, double* tile)
+        {
+            const int t = threadIdx.x;
+            const int l = m.level;
+            {
+                const int c = 2 * t, i = c & 7, j = (c >> 3) & 7, k = c >> 6;
+                double2 value = *reinterpret_cast<const double2*>(z + int64_t(m.slot) * kC3 + c);
+                if (kProlong)
+                {
+                    value.x += double(e[base_cell_of(m.base, l, i, j, k)]);
+                    value.y += double(e[base_cell_of(m.base, l, i + 1, j, k)]);
+                }
+                *reinterpret_cast<double2*>(tile + tix(i, j, k)) = value;
+            }
+            if (t < 128)
+            {
+                // -y, +y, -z, +z faces as pairs along x
+                const int face = 2 + (t >> 5), w = t & 31;
+                int i, j, k, hj, hk;
+                if (face < 4) { k = w >> 2; i = (w & 3) * 2; j = face == 2 ? kBS - 1 : 0; hj = face == 2 ? -1 : kBS; hk = k; }
+                else { i = (w * 2) & 7; j = (w * 2) >> 3; k = face == 4 ? kBS - 1 : 0; hj = j; hk = face == 4 ? -1 : kBS; }
+                const int n = gm->nbr[face];
+                double2 value = make_double2(0.0, 0.0);
+                if (n >= 0)
+                {
+                    value = *reinterpret_cast<const double2*>(z + int64_t(n) * kC3 + (k * kBS + j) * kBS + i);
+                    if (kProlong)
+                    {
+                        const int nb = gm->nbase[face];
+                        value.x += double(e[base_cell_of(nb, l, i, j, k)]);
+                        value.y += double(e[base_cell_of(nb, l, i + 1, j, k)]);
+                    }
+                }
+                *reinterpret_cast<double2*>(tile + tix(i, hj, hk)) = value;
+            }
+            else
+            {
+                // -x, +x faces, one value each
+                const int u = t - 128, face = u >> 6, j = u & 7, k = (u >> 3) & 7;
+                const int i = face == 0 ? kBS - 1 : 0, hi = face == 0 ? -1 : kBS;
+                const int n = gm->nbr[face];
+                double value = 0.0;
+                if (n >= 0)
+                {
+                    value = z[int64_t(n) * kC3 + (k * kBS + j) * kBS + i];
+                    if (kProlong) value += double(e[base_cell_of(gm->nbase[face], l, i, j, k)]);
+                }
+                tile[tix(hi, j, k)] = value;
+            }
+        }
+
+        // Structured 7-point row of cell s of the tile (order -x,+x,-y,+y,-z,+z, then outlet),
+        // and the matching diagonal; identical arithmetic to the unfused operator kernel.
+        __device__ inline void structured_row(const double* tile, int s, uint8_t code, double h, double& Az, double& D)
+        {
+            const double pa = tile[s];
+            Az = 0.0;
+            D = 0.0;
+            if (code & 1) { Az += h * (pa - tile[s - 1]); D += h; }
+            if (code & 2) { Az += h * (pa - tile[s + 1]); D += h; }
+            if (code & 4) { Az += h * (pa - tile[s - kP1]); D += h; }
+            if (code & 8) { Az += h * (pa - tile[s + kP1]); D += h; }
+            if (code & 16) { Az += h * (pa - tile[s - kP2]); D += h; }
+            if (code & 32) { Az += h * (pa - tile[s + kP2]); D += h; }
+            if (code & kOutlet) { Az += 2.0 * h * pa; D += 2.0 * h; }
+        }
+
+        // The scalar fields of the CTA's brick (every thread reads the same 16 bytes); neighbour
+        // fields are read from global memory where they are used.
+        __device__ inline BrickHead load_head(const BrickView& v)
+        {
+            const int4 h = *reinterpret_cast<const int4*>(v.meta + blockIdx.x);
+            return BrickHead{h.x, h.y, h.z, h.w};
+        }
+
+        // kMode 0: sweep (out = z_new; deferred rows store A_struct z in t)
+        //       1: residual restriction (partials; deferred rows store A_struct z in t)
+        // Thread t owns cells 2t and 2t+1 (same x row).
+        template <int kMode, class TC, bool kProlong>
+        __global__ void __launch_bounds__(256) brick_fine_kernel(BrickView v, const double* __restrict__ z, const double* __restrict__ r,
+            double* __restrict__ out, double* __restrict__ t, const TC* __restrict__ e, double* __restrict__ partial, double omega)
+        {
+            __shared__ __align__(16) double tile[kTileSize];
+            __shared__ double residual[kC3];
+            const BrickHead m = load_head(v);
+            const BrickMeta* gm = v.meta + blockIdx.x;
+            const int64_t base = int64_t(m.slot) * kC3;
+            const int c0 = 2 * threadIdx.x;
+            const uchar2 codes = *reinterpret_cast<const uchar2*>(v.code + base + c0);
+            const double2 rr = *reinterpret_cast<const double2*>(r + base + c0);
+            stage_tile<TC, kProlong>(m, gm, z, e, tile);
+            __syncthreads();
+            const int l = m.level;
+            const double h = v.level_h[l];
+            double result[2];
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+            {
+                const int c = c0 + q, i = c & 7, j = (c >> 3) & 7, k = c >> 6;
+                const int s = tix(i, j, k);
+                const uint8_t code = q ? codes.y : codes.x;
+                const double rc = q ? rr.y : rr.x;
+                double Az, D;
+                structured_row(tile, s, code, h, Az, D);
+                if (code & kDeferred) t[base + c] = Az;
+                if (kMode == 0) result[q] = code ? tile[s] + omega * (rc - Az) / D : 0.0;
+                else
+                {
+                    // level-0 cell ordering inside the brick: cells of one aggregate are contiguous
+                    const int n = l >= 3 ? 1 : (kBS >> l);
+                    const int group = l >= 3 ? 0 : ((k >> l) * n + (j >> l)) * n + (i >> l);
+                    const int size = l >= 3 ? kC3 : (1 << (3 * l));
+                    const int mask = (1 << l) - 1;
+                    const int within = l >= 3 ? c : ((((k & mask) << l) + (j & mask)) << l) + (i & mask);
+                    residual[group * size + within] = (code && !(code & kDeferred)) ? rc - Az : 0.0;
+                }
+            }
+            if (kMode == 0)
+            {
+                // deferred rows are written by the finish kernel; keep their slots untouched
+                if (!(codes.x & kDeferred) && !(codes.y & kDeferred))
+                    *reinterpret_cast<double2*>(out + base + c0) = make_double2(result[0], result[1]);
+                else
+                {
+                    if (!(codes.x & kDeferred)) out[base + c0] = result[0];
+                    if (!(codes.y & kDeferred)) out[base + c0 + 1] = result[1];
+                }
+            }
+            if (kMode == 1)
+            {
+                // deterministic pairwise tree inside each aggregate group
+                const int size = l >= 3 ? kC3 : (1 << (3 * l));
+                const int groups = kC3 / size;
+                __syncthreads();
+                for (int stride = size >> 1; stride > 0; stride >>= 1)
+                {
+                    for (int w = threadIdx.x; w < groups * stride; w += 256)
+                    {
+                        const int g = w / stride, p = w % stride;
+                        residual[g * size + p] += residual[g * size + p + stride];
+                    }
+                    __syncthreads();
+                }
+                for (int g = threadIdx.x; g < groups; g += 256) partial[m.partial + g] = residual[g * size];
+            }
+        }
+
+        // out = A_struct p over every cell of the active bricks (inactive cells 0); the compact
+        // edges, gauges and the WLS correction are added by the operator's other kernels.
+        __global__ void __launch_bounds__(256) brick_apply_kernel(BrickView v, const double* __restrict__ p, double* __restrict__ out)
+        {
+            __shared__ __align__(16) double tile[kTileSize];
+            const BrickHead m = load_head(v);
+            const BrickMeta* gm = v.meta + blockIdx.x;
+            const int64_t base = int64_t(m.slot) * kC3;
+            const int c0 = 2 * threadIdx.x;
+            const uchar2 codes = *reinterpret_cast<const uchar2*>(v.code + base + c0);
+            stage_tile<double, false>(m, gm, p, nullptr, tile);
+            __syncthreads();
+            const double h = v.level_h[m.level];
+            double Az[2], D;
+            const int i = c0 & 7, j = (c0 >> 3) & 7, k = c0 >> 6;
+            structured_row(tile, tix(i, j, k), codes.x, h, Az[0], D);
+            structured_row(tile, tix(i + 1, j, k), codes.y, h, Az[1], D);
+            *reinterpret_cast<double2*>(out + base + c0) = make_double2(Az[0], Az[1]);
+        }
+
+        // z = w r / D for every DOF (first sweep from zero); deferred rows read the assembled D.
+        __global__ void first_sweep_kernel(const uint8_t* __restrict__ code, const int* __restrict__ brick_level,
+                                           const double* __restrict__ level_h, const double* __restrict__ diag,
+                                           const uint8_t* __restrict__ active, const double* __restrict__ r,
+                                           double* __restrict__ z, int64_t structured, int64_t n, double omega)
+        {
+            const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+            if (q >= n) return;
+            const uint8_t c = code[q];
+            double D;
+            if (q >= structured || (c & kDeferred)) D = active[q] ? diag[q] : 0.0;
+            else
+            {
+                const double h = level_h[brick_level[q >> 9]];
+                D = 0.0;
+                for (int f = 0; f < 6; ++f)
+                    if (c & (1 << f)) D += h;
+                if (c & kOutlet) D += 2.0 * h;
+            }
+            z[q] = D > 0.0 ? omega * r[q] / D : 0.0;
+        }
+
+        // Completes deferred rows: A_orth z = t (structured part) + compact-edge gather + gauges,
+        // in the order of the unfused launch; kMode 0 writes z_new, 1 writes the row residual.
+        template <int kMode, class TC, bool kProlong>
+        __global__ void finish_deferred_kernel(int count, const int* __restrict__ dof, const int* __restrict__ incident,
+            const int* __restrict__ gauge_offset, const double* __restrict__ gauge_coefficient,
+            const int* __restrict__ incident_offset, const int* __restrict__ incident_edge, const int8_t* __restrict__ incident_sign,
+            int connection_count, const int* __restrict__ conn_lower, const int* __restrict__ conn_upper,
+            const double* __restrict__ conn_coefficient, const int* __restrict__ reg_lower, const int* __restrict__ reg_upper,
+            const double* __restrict__ reg_coefficient, const uint8_t* __restrict__ active, const double* __restrict__ diag,
+            const int* __restrict__ aggregate, int base_offset, int base_cells, const TC* __restrict__ e, int64_t structured,
+            const double* __restrict__ z, const double* __restrict__ r, const double* __restrict__ t, double* __restrict__ out,
+            double* __restrict__ residual, double omega)
+        {
+            const int d = blockIdx.x * blockDim.x + threadIdx.x;
+            if (d >= count) return;
+            auto value = [&](int q) {
+                double v = z[q];
+                if (kProlong && active[q])
+                {
+                    const int c = aggregate[q] - base_offset;
+                    if (c >= 0 && c < base_cells) v += double(e[c]);
+                }
+                return v;
+            };
+            const int a = dof[d];
+            double Az = a < structured ? t[a] : 0.0;
+            const int node = incident[d];
+            if (node >= 0)
+            {
+                double sum = 0.0;
+                for (int q = incident_offset[node]; q < incident_offset[node + 1]; ++q)
+                {
+                    const int edge = incident_edge[q];
+                    int lo, hi;
+                    double coefficient;
+                    if (edge < connection_count) { lo = conn_lower[edge]; hi = conn_upper[edge]; coefficient = conn_coefficient[edge]; }
+                    else { const int rr = edge - connection_count; lo = reg_lower[rr]; hi = reg_upper[rr]; coefficient = reg_coefficient[rr]; }
+                    if (active[lo] && active[hi]) sum += double(incident_sign[q]) * (coefficient * (value(lo) - value(hi)));
+                }
+                Az += sum;
+            }
+            const double za = value(a);
+            for (int g = gauge_offset[d]; g < gauge_offset[d + 1]; ++g) Az += gauge_coefficient[g] * za;
+            const double D = diag[a];
+            if (kMode == 0)
+            {
+                if (!active[a]) out[a] = 0.0;
+                else out[a] = D > 0.0 ? za + omega * (r[a] - Az) / D : za;
+            }
+            else residual[d] = active[a] ? r[a] - Az : 0.0;
+        }
+
+        // base-level right-hand side: brick partials (levels in order) then deferred-row residuals
+        template <class TC>
+        __global__ void gather_base_kernel(int cells, const int* __restrict__ offset, const int* __restrict__ entry,
+                                           const double* __restrict__ partial, const double* __restrict__ deferred, TC* __restrict__ rhs)
+        {
+            const int c = blockIdx.x * blockDim.x + threadIdx.x;
+            if (c >= cells) return;
+            double sum = 0.0;
+            for (int q = offset[c]; q < offset[c + 1]; ++q)
+            {
+                const int x = entry[q];
+                sum += x >= 0 ? partial[x] : deferred[-x - 1];
+            }
+            rhs[c] = TC(sum);
+        }
+    }
+
+    // ==================================================================================
+    // setup
+    // ==================================================================================
+    void build_fine_smoother(System& s, const pcfd_topology& t, const std::vector<double>& diag)
+    {
+        FineSmoother& f = s.fine;
+        f.enabled = false;
+        if (s.bs != kBS || s.mg64.empty()) return;
+        const int S = s.S, structured = s.structured;
+        std::vector<uint8_t> code(size_t(S), 0);
+        std::vector<int> slot_level(size_t(s.B));
+        std::vector<const pcfd_level*> slot_lev(size_t(s.B));
+        std::vector<int> slot_brick(size_t(s.B));
+        for (int l = 0, slot = 0; l < t.level_count; ++l)
+            for (int b = 0; b < t.levels[l].brick_count; ++b, ++slot)
+            {
+                slot_level[slot] = l;
+                slot_lev[slot] = &t.levels[l];
+                slot_brick[slot] = b;
+            }
+        // deferred rows: compact-edge incidence, gauges, fragments
+        std::vector<uint8_t> deferred(size_t(S), 0);
+        const IrregularOperator& o = s.irr;
+        std::vector<int> incident_dof(o.incident_dofs);
+        if (o.incident_dofs)
+            cuda_check(cudaMemcpy(incident_dof.data(), o.incident_dof.p, incident_dof.size() * sizeof(int), cudaMemcpyDeviceToHost),
+                       "incidence download");
+        for (int q : incident_dof) deferred[q] = 1;
+        for (int g = 0; g < t.gauge_count; ++g) deferred[t.gauge_dof[g]] = 1;
+        for (int q = structured; q < S; ++q) deferred[q] = t.active[q] ? 1 : 0;
+        // open faces per structured DOF, same rules as the unfused operator kernel
+        for (int slot = 0; slot < s.B; ++slot)
+        {
+            const pcfd_level& lev = *slot_lev[slot];
+            const int b = slot_brick[slot];
+            if (lev.flags[b] & PCFD_BRICK_COVERED) continue;
+            const int slot0 = slot - b;
+            const double h = lev.h;
+            for (int c = 0; c < kC3; ++c)
+            {
+                const int64_t a = int64_t(slot) * kC3 + c;
+                if (!t.active[a]) continue;
+                const int ijk[3] = {c & 7, (c >> 3) & 7, c >> 6};
+                uint8_t bits = 0;
+                for (int axis = 0; axis < 3; ++axis)
+                    for (int positive = 0; positive < 2; ++positive)
+                    {
+                        int q[3] = {ijk[0], ijk[1], ijk[2]};
+                        q[axis] += positive ? 1 : -1;
+                        int64_t nb = -1;
+                        if (q[axis] >= 0 && q[axis] < kBS) nb = int64_t(slot) * kC3 + (q[2] * kBS + q[1]) * kBS + q[0];
+                        else
+                        {
+                            const int n = lev.neighbors[b * 6 + 2 * axis + positive];
+                            if (n >= 0 && !(lev.flags[n] & PCFD_BRICK_COVERED))
+                            {
+                                q[axis] = positive ? 0 : kBS - 1;
+                                nb = int64_t(slot0 + n) * kC3 + (q[2] * kBS + q[1]) * kBS + q[0];
+                            }
+                        }
+                        const int64_t lower = positive ? a : nb;
+                        if (nb >= 0 && t.active[nb] && !(t.cut_face_mask[lower] & (1u << axis))) bits |= uint8_t(1u << (2 * axis + positive));
+                    }
+                if (s.outlet && (lev.flags[b] & PCFD_BRICK_XMAX) && ijk[0] == kBS - 1) bits |= kOutlet;
+                double D = 0.0;
+                for (int face = 0; face < 6; ++face)
+                    if (bits & (1 << face)) D += h;
+                if (bits & kOutlet) D += 2.0 * h;
+                if (!(D > 0.0) || D != diag[a]) deferred[a] = 1;
+                code[a] = bits;
+            }
+        }
+        for (int q = 0; q < S; ++q)
+            if (deferred[q] && t.active[q]) code[q] |= kDeferred;
+        // deferred list with its incidence row and gauge entries (gauge order kept per DOF)
+        std::unordered_map<int, int> incident_index;
+        for (int n = 0; n < o.incident_dofs; ++n) incident_index[incident_dof[n]] = n;
+        std::vector<int> ddof, dinc, goff(1, 0);
+        std::vector<double> gcoef;
+        std::vector<std::vector<double>> gauges_of;
+        std::unordered_map<int, std::vector<double>> gauge_map;
+        for (int g = 0; g < t.gauge_count; ++g) gauge_map[t.gauge_dof[g]].push_back(t.gauge_coefficient[g]);
+        std::vector<int> deferred_index(size_t(S), -1);
+        for (int q = 0; q < S; ++q)
+        {
+            if (!deferred[q]) continue;
+            deferred_index[q] = int(ddof.size());
+            ddof.push_back(q);
+            const auto it = incident_index.find(q);
+            dinc.push_back(it == incident_index.end() ? -1 : it->second);
+            const auto g = gauge_map.find(q);
+            if (g != gauge_map.end()) gcoef.insert(gcoef.end(), g->second.begin(), g->second.end());
+            goff.push_back(int(gcoef.size()));
+        }
+        // geometric level-0 cell of every brick; must reproduce the aggregate of every active DOF
+        const pcfd_level& base = t.levels[0];
+        std::unordered_map<int64_t, int> base_slot;
+        auto key = [](int64_t x, int64_t y, int64_t z) { return (x << 42) ^ (y << 21) ^ z; };
+        for (int b = 0; b < base.brick_count; ++b)
+            base_slot[key(base.coord[3 * b], base.coord[3 * b + 1], base.coord[3 * b + 2])] = b;
+        std::vector<int> brick_base(size_t(s.B), -1);
+        bool geometric = true;
+        for (int slot = 0; slot < s.B && geometric; ++slot)
+        {
+            const pcfd_level& lev = *slot_lev[slot];
+            const int b = slot_brick[slot], l = slot_level[slot];
+            if (lev.flags[b] & PCFD_BRICK_COVERED) continue;
+            int64_t g[3];
+            for (int a = 0; a < 3; ++a) g[a] = (int64_t(lev.coord[3 * b + a]) * kBS) >> l;   // level-0 cell of (0,0,0)
+            const auto it = base_slot.find(key(g[0] / kBS, g[1] / kBS, g[2] / kBS));
+            if (it == base_slot.end() || g[0] < 0 || g[1] < 0 || g[2] < 0) { geometric = false; break; }
+            brick_base[slot] = it->second * kC3 + int((g[2] % kBS) * 64 + (g[1] % kBS) * 8 + g[0] % kBS);
+            for (int c = 0; c < kC3; ++c)
+            {
+                const int64_t a = int64_t(slot) * kC3 + c;
+                if (!t.active[a]) continue;
+                const int expect = brick_base[slot] + (((c >> 6) >> l) << 6) + ((((c >> 3) & 7) >> l) << 3) + ((c & 7) >> l);
+                if (t.preconditioner_aggregate[a] - s.base_offset != expect) { geometric = false; break; }
+            }
+        }
+        if (!geometric) return;
+        // brick partial layout and the base-cell gather lists
+        std::vector<int> poff(size_t(s.B), -1);
+        std::vector<std::vector<int>> entries(size_t(s.base_cells));
+        int partials = 0;
+        for (int slot = 0; slot < s.B; ++slot)
+        {
+            const pcfd_level& lev = *slot_lev[slot];
+            const int b = slot_brick[slot], l = slot_level[slot];
+            if (lev.flags[b] & PCFD_BRICK_COVERED) continue;
+            const int n = l >= 3 ? 1 : (kBS >> l);
+            poff[slot] = partials;
+            for (int z = 0; z < n; ++z)
+                for (int y = 0; y < n; ++y)
+                    for (int x = 0; x < n; ++x)
+                        entries[size_t(brick_base[slot] + z * 64 + y * 8 + x)].push_back(partials + (z * n + y) * n + x);
+            partials += n * n * n;
+        }
+        for (size_t d = 0; d < ddof.size(); ++d)
+        {
+            const int q = ddof[d];
+            const int c = t.active[q] ? t.preconditioner_aggregate[q] - s.base_offset : -1;
+            if (c >= 0 && c < s.base_cells) entries[size_t(c)].push_back(-int(d) - 1);
+        }
+        std::vector<int> eoff(size_t(s.base_cells) + 1, 0), elist;
+        for (int c = 0; c < s.base_cells; ++c)
+        {
+            elist.insert(elist.end(), entries[c].begin(), entries[c].end());
+            eoff[c + 1] = int(elist.size());
+        }
+        f.code.upload(code);
+        f.deferred_count = int(ddof.size());
+        f.deferred_dof.upload(ddof);
+        f.deferred_incident.upload(dinc);
+        f.gauge_offset.upload(goff);
+        f.gauge_coefficient.upload(gcoef.empty() ? std::vector<double>(1, 0.0) : gcoef);
+        // per active brick, in active-list order: slot, level, base cell, partial offset,
+        // neighbour slots, neighbour base cells (BrickMeta)
+        std::vector<int> meta;
+        meta.reserve(size_t(s.active_bricks) * 16);
+        for (int slot = 0; slot < s.B; ++slot)
+        {
+            const pcfd_level& lev = *slot_lev[slot];
+            const int b = slot_brick[slot];
+            if (lev.flags[b] & PCFD_BRICK_COVERED) continue;
+            const int slot0 = slot - b;
+            int nbr[6];
+            for (int face = 0; face < 6; ++face)
+            {
+                const int n = lev.neighbors[b * 6 + face];
+                nbr[face] = n >= 0 && !(lev.flags[n] & PCFD_BRICK_COVERED) ? slot0 + n : -1;
+            }
+            meta.push_back(slot);
+            meta.push_back(slot_level[slot]);
+            meta.push_back(brick_base[slot]);
+            meta.push_back(poff[slot]);
+            for (int face = 0; face < 6; ++face) meta.push_back(nbr[face]);
+            for (int face = 0; face < 6; ++face) meta.push_back(nbr[face] >= 0 ? brick_base[nbr[face]] : -1);
+        }
+        if (meta.size() != size_t(s.active_bricks) * 16) return;
+        f.meta.upload(meta);
+        f.partial.alloc(size_t(std::max(1, partials)));
+        f.deferred_residual.alloc(size_t(std::max(1, f.deferred_count)));
+        f.gather_offset.upload(eoff);
+        f.gather_entry.upload(elist.empty() ? std::vector<int>(1, 0) : elist);
+        f.t.alloc(size_t(S));
+        f.z.alloc(size_t(S));
+        f.enabled = true;
+    }
+
+    // ==================================================================================
+    // launches
+    // ==================================================================================
+    namespace
+    {
+        BrickView view(System& s)
+        {
+            return BrickView{reinterpret_cast<const BrickMeta*>(s.fine.meta.p), s.d_level_h, s.fine.code};
+        }
+
+        template <int kMode, class TC, bool kProlong>
+        void finish(System& s, const double* z, const double* r, double* out, const TC* e)
+        {
+            FineSmoother& f = s.fine;
+            const IrregularOperator& o = s.irr;
+            if (!f.deferred_count) return;
+            finish_deferred_kernel<kMode, TC, kProlong><<<blocks_for(f.deferred_count), kThreads, 0, launch_stream(s)>>>(
+                f.deferred_count, f.deferred_dof, f.deferred_incident, f.gauge_offset, f.gauge_coefficient, o.incident_offset,
+                o.incident_edge, o.incident_sign, o.connection_count, o.conn_lower, o.conn_upper, o.conn_coefficient, o.reg_lower,
+                o.reg_upper, o.reg_coefficient, s.active, s.diagonal, s.aggregate, s.base_offset, s.base_cells, e, s.structured, z, r,
+                f.t, out, f.deferred_residual, 2.0 / 3.0);
+        }
+
+        template <class TC, bool kProlong>
+        void sweep(System& s, const double* z, const double* r, double* out, const TC* e)
+        {
+            FineSmoother& f = s.fine;
+            brick_fine_kernel<0, TC, kProlong><<<s.active_bricks, 256, 0, launch_stream(s)>>>(
+                view(s), z, r, out, f.t, e, nullptr, 2.0 / 3.0);
+            finish<0, TC, kProlong>(s, z, r, out, e);
+        }
+    }
+
+    void brick_apply(System& s, const double* p, double* out)
+    {
+        brick_apply_kernel<<<s.active_bricks, 256, 0, launch_stream(s)>>>(view(s), p, out);
+    }
+
+    template <class TC>
+    void fine_preconditioner(System& s, const double* r, double* z, std::vector<MgLevel<TC>>& levels)
+    {
+        FineSmoother& f = s.fine;
+        double* a = f.z.p;
+        first_sweep_kernel<<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(f.code, s.brick_level, s.d_level_h, s.diagonal,
+                                                                              s.active, r, a, s.structured, s.S, 2.0 / 3.0);
+        sweep<TC, false>(s, a, r, z, nullptr);
+        MgLevel<TC>& base = levels.front();
+        cuda_check(cudaMemsetAsync(base.x, 0, size_t(base.cells) * sizeof(TC), s.stream), "clear base correction");
+        brick_fine_kernel<1, TC, false><<<s.active_bricks, 256, 0, launch_stream(s)>>>(
+            view(s), z, r, nullptr, f.t, nullptr, f.partial, 2.0 / 3.0);
+        finish<1, TC, false>(s, z, r, nullptr, nullptr);
+        gather_base_kernel<TC><<<blocks_for(base.cells), kThreads, 0, launch_stream(s)>>>(base.cells, f.gather_offset, f.gather_entry,
+                                                                                         f.partial, f.deferred_residual, base.rhs);
+        multigrid_levels(s, levels);
+        sweep<TC, true>(s, z, r, a, base.x.p);
+        sweep<TC, false>(s, a, r, z, nullptr);
+        cuda_check(cudaGetLastError(), "fused preconditioner");
+    }
+
+    template void fine_preconditioner<double>(System&, const double*, double*, std::vector<MgLevel<double>>&);
+    template void fine_preconditioner<float>(System&, const double*, double*, std::vector<MgLevel<float>>&);
+}

@@ -375,7 +375,7 @@ namespace pcfd
             auto smooth = [&](int sweeps) {
                 for (int sweep = 0; sweep < sweeps; ++sweep)
                 {
-                    algebraic_jacobi_kernel<T><<<blocks_for(level.cells), kThreads, 0, s.stream>>>(
+                    algebraic_jacobi_kernel<T><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
                         level.rhs, level.x, level.temporary, level.row_offset, level.neighbour, level.coefficient,
                         level.diagonal, level.cells, omega);
                     std::swap(level.x.p, level.temporary.p);
@@ -384,21 +384,21 @@ namespace pcfd
             if (index + 1 == int(levels.size()))
             {
                 if (level.cells <= 4096)
-                    coarse_jacobi_kernel<T, 4><<<1, 1024, 0, s.stream>>>(level.rhs, level.x, level.temporary, level.row_offset,
+                    coarse_jacobi_kernel<T, 4><<<1, 1024, 0, launch_stream(s)>>>(level.rhs, level.x, level.temporary, level.row_offset,
                         level.neighbour, level.coefficient, level.diagonal, level.cells, omega, 96);
                 else
                     smooth(96);
                 return;
             }
             smooth(2);
-            algebraic_residual_kernel<T><<<blocks_for(level.cells), kThreads, 0, s.stream>>>(
+            algebraic_residual_kernel<T><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
                 level.rhs, level.x, level.residual, level.row_offset, level.neighbour, level.coefficient, level.diagonal, level.cells);
             MgLevel<T>& coarse = levels[index + 1];
-            restrict_gather_kernel<T><<<blocks_for(coarse.cells), kThreads, 0, s.stream>>>(
+            restrict_gather_kernel<T><<<blocks_for(coarse.cells), kThreads, 0, launch_stream(s)>>>(
                 level.restrict_offset, level.restrict_dof, level.residual, coarse.cells, coarse.rhs);
             cuda_check(cudaMemsetAsync(coarse.x, 0, size_t(coarse.cells) * sizeof(T), s.stream), "clear coarse correction");
             mg_level(s, levels, index + 1);
-            prolong_add_kernel<T><<<blocks_for(level.cells), kThreads, 0, s.stream>>>(level.aggregate, level.cells, coarse.x, level.x);
+            prolong_add_kernel<T><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(level.aggregate, level.cells, coarse.x, level.x);
             smooth(2);
         }
 
@@ -408,29 +408,51 @@ namespace pcfd
             MgLevel<T>& base = levels.front();
             cuda_check(cudaMemsetAsync(base.x, 0, size_t(base.cells) * sizeof(T), s.stream), "clear base correction");
             launch_apply(s, z, s.t, true);
-            restrict_difference_kernel<T><<<blocks_for(base.cells), kThreads, 0, s.stream>>>(
+            restrict_difference_kernel<T><<<blocks_for(base.cells), kThreads, 0, launch_stream(s)>>>(
                 s.base_restrict_offset, s.base_restrict_dof, r, s.t, base.cells, base.rhs);
             mg_level(s, levels, 0);
-            prolong_aggregate_kernel<T><<<blocks_for(s.S), kThreads, 0, s.stream>>>(s.aggregate, s.active, s.S, s.base_offset,
+            prolong_aggregate_kernel<T><<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(s.aggregate, s.active, s.S, s.base_offset,
                                                                                   s.base_cells, base.x, z);
         }
     }
 
-    void apply_preconditioner(System& s, const double* r, double* z)
+    void preconditioner_stage(System& s, int stage, const double* r, double* z)
     {
-        precondition_kernel<<<blocks_for(s.S), kThreads, 0, s.stream>>>(r, z, s.diagonal, s.active, s.S, kOmega);
-        launch_apply(s, z, s.t, true);
-        jacobi_correction_kernel<<<blocks_for(s.S), kThreads, 0, s.stream>>>(r, s.t, z, s.diagonal, s.active, s.S, kOmega);
-        if (!s.mg64.empty())
+        if (stage == 0)
+        {
+            precondition_kernel<<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(r, z, s.diagonal, s.active, s.S, kOmega);
+            launch_apply(s, z, s.t, true);
+            jacobi_correction_kernel<<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(r, s.t, z, s.diagonal, s.active, s.S, kOmega);
+        }
+        else if (stage == 1 && !s.mg64.empty())
         {
             if (s.mg_precision == PCFD_MG_FP32 && !s.mg32.empty()) coarse_correction(s, s.mg32, r, z);
             else coarse_correction(s, s.mg64, r, z);
         }
-        for (int sweep = 0; sweep < 2 && !s.mg64.empty(); ++sweep)
+        else if (stage == 2 && !s.mg64.empty())
+            for (int sweep = 0; sweep < 2; ++sweep)
+            {
+                launch_apply(s, z, s.t, true);
+                jacobi_correction_kernel<<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(r, s.t, z, s.diagonal, s.active, s.S, kOmega);
+            }
+    }
+
+    template <class T> void multigrid_levels(System& s, std::vector<MgLevel<T>>& levels) { mg_level(s, levels, 0); }
+    template void multigrid_levels<double>(System&, std::vector<MgLevel<double>>&);
+    template void multigrid_levels<float>(System&, std::vector<MgLevel<float>>&);
+
+    void apply_preconditioner(System& s, const double* r, double* z)
+    {
+        ProfileScope scope(s, PCFD_PROFILE_PRECONDITIONER);
+        if (s.fine.enabled && aligned16(r) && aligned16(z))
         {
-            launch_apply(s, z, s.t, true);
-            jacobi_correction_kernel<<<blocks_for(s.S), kThreads, 0, s.stream>>>(r, s.t, z, s.diagonal, s.active, s.S, kOmega);
+            if (s.mg_precision == PCFD_MG_FP32 && !s.mg32.empty()) fine_preconditioner(s, r, z, s.mg32);
+            else fine_preconditioner(s, r, z, s.mg64);
+            return;
         }
+        preconditioner_stage(s, 0, r, z);
+        preconditioner_stage(s, 1, r, z);
+        preconditioner_stage(s, 2, r, z);
         cuda_check(cudaGetLastError(), "preconditioner");
     }
 
@@ -517,6 +539,7 @@ namespace pcfd
         {
             pcfd_solve_result result{};
             const int n = s.S;
+            const size_t ld = size_t(s.Sp);   // stride of the multi-vector slots
             if (!warm)
             {
                 s.recycle_count = 0;
@@ -532,8 +555,26 @@ namespace pcfd
                 vec_subtract(s, s.defect, s.Ad);
                 return device_dot(s, s.defect, s.defect);
             };
-            auto ru = [&](int c) { return s.recycle_u.p + size_t(c) * n; };
-            auto rcv = [&](int c) { return s.recycle_c.p + size_t(c) * n; };
+            auto ru = [&](int c) { return s.recycle_u.p + size_t(c) * ld; };
+            auto rcv = [&](int c) { return s.recycle_c.p + size_t(c) * ld; };
+            // device coefficient blocks of the fused CGS2 passes and their pinned host copies
+            constexpr int kStride = kMaxSet + 1;
+            double* h1 = s.block_result.p;
+            double* h2 = h1 + kStride;
+            double* h3 = h2 + kStride;
+            const double* host_h1 = s.pinned_block;
+            const double* host_h2 = host_h1 + kStride;
+            const double* host_h3 = host_h2 + kStride;
+            auto read_block = [&](int blocks) {
+                cuda_check(cudaMemcpyAsync(s.pinned_block, s.block_result.p, size_t(blocks) * kStride * sizeof(double),
+                                           cudaMemcpyDeviceToHost, s.stream), "coefficient readback");
+                cuda_check(cudaStreamSynchronize(s.stream), "coefficient synchronize");
+            };
+            auto recycle_set = [&](double* base) {
+                VecSet set;
+                for (int c = 0; c < s.recycle_count; ++c) set.push(base + size_t(c) * ld);
+                return set;
+            };
             double residual2 = true_residual();
             result.relative_residual = std::sqrt(residual2 / rhs2);
             if (result.relative_residual <= tolerance) { result.converged = 1; return result; }
@@ -548,15 +589,15 @@ namespace pcfd
                 {
                     vec_copy_active(s, x, s.correction);
                     vec_copy_active(s, s.defect, s.t);
+                    // two projections of the defect off C, correction += U h (CGS2, one readback)
+                    const VecSet Cset = recycle_set(s.recycle_c.p), Uset = recycle_set(s.recycle_u.p);
+                    block_dot(s, Cset, s.defect, h1);
+                    block_update(s, Cset, h1, s.defect, Uset, 1.0, s.correction, 2, h2);
+                    block_update(s, Cset, h2, s.defect, Uset, 1.0, s.correction, 0, nullptr);
+                    read_block(2);
+                    for (int c = 0; c < attempted && valid; ++c)
+                        valid = finite_value(host_h1[c]) && finite_value(host_h2[c]);
                 }
-                for (int pass = 0; pass < 2 && valid; ++pass)
-                    for (int c = 0; c < s.recycle_count; ++c)
-                    {
-                        const double value = device_dot(s, rcv(c), s.defect);
-                        if (!finite_value(value)) { valid = false; break; }
-                        vec_axpy_active(s, s.correction, ru(c), value);
-                        vec_axpy_active(s, s.defect, rcv(c), -value);
-                    }
                 double gap2 = 0, true_recycled2 = before2;
                 if (attempted && valid)
                 {
@@ -599,38 +640,31 @@ namespace pcfd
                 int used = 0;
                 for (int col = 0; col < cycle; ++col)
                 {
-                    double* v = s.gmres_v.p + size_t(col) * n;
-                    double* zc = s.gmres_z.p + size_t(col) * n;
+                    double* v = s.gmres_v.p + size_t(col) * ld;
+                    double* zc = s.gmres_z.p + size_t(col) * ld;
                     apply_preconditioner(s, v, zc);
                     ++result.preconditioner_applications;
                     launch_apply(s, zc, s.Ad, false);
+                    // CGS2 against [C | V_0..V_col]; the U part of each coefficient block also updates z
+                    const int k = s.recycle_count, m = k + col + 1;
+                    VecSet Q = recycle_set(s.recycle_c.p), Uset = recycle_set(s.recycle_u.p);
+                    for (int row = 0; row <= col; ++row) Q.push(s.gmres_v.p + size_t(row) * ld);
+                    block_dot(s, Q, s.Ad, h1);
+                    block_update(s, Q, h1, s.Ad, Uset, -1.0, zc, 2, h2);
+                    block_update(s, Q, h2, s.Ad, Uset, -1.0, zc, 1, h3);
+                    scale_by_inverse_norm(s, s.gmres_v.p + size_t(col + 1) * ld, s.Ad, h3);
+                    read_block(3);
                     bool column_valid = true;
-                    for (int pass = 0; pass < 2 && column_valid; ++pass)
-                        for (int c = 0; c < s.recycle_count; ++c)
-                        {
-                            const double value = device_dot(s, rcv(c), s.Ad);
-                            if (!finite_value(value)) { column_valid = false; break; }
-                            vec_axpy_active(s, s.Ad, rcv(c), -value);
-                            vec_axpy_active(s, zc, ru(c), -value);
-                        }
+                    for (int j = 0; j < m && column_valid; ++j) column_valid = finite_value(host_h1[j]) && finite_value(host_h2[j]);
                     if (!column_valid) break;
-                    const double scale = std::sqrt(std::max(0.0, device_dot(s, s.Ad, s.Ad)));
+                    double c_part = 0;
+                    for (int c = 0; c < k; ++c) c_part += host_h1[c] * host_h1[c];
+                    const double scale = std::sqrt(std::max(0.0, host_h1[m] - c_part));
                     if (!(scale > 0) || !std::isfinite(scale)) break;
-                    for (int pass = 0; pass < 2 && column_valid; ++pass)
-                        for (int row = 0; row <= col; ++row)
-                        {
-                            double* basis = s.gmres_v.p + size_t(row) * n;
-                            const double value = device_dot(s, basis, s.Ad);
-                            if (!finite_value(value)) { column_valid = false; break; }
-                            H[size_t(row) * cycle + col] += value;
-                            vec_axpy_active(s, s.Ad, basis, -value);
-                        }
-                    if (!column_valid) break;
-                    double next_norm = std::sqrt(std::max(0.0, device_dot(s, s.Ad, s.Ad)));
+                    for (int row = 0; row <= col; ++row) H[size_t(row) * cycle + col] = host_h1[k + row] + host_h2[k + row];
+                    double next_norm = std::sqrt(std::max(0.0, host_h3[0]));
                     const double floor = 64 * std::numeric_limits<double>::epsilon() * scale;
-                    if (next_norm > floor && std::isfinite(1.0 / next_norm))
-                        vec_scaled_copy_active(s, s.gmres_v.p + size_t(col + 1) * n, s.Ad, 1.0 / next_norm);
-                    else next_norm = 0;
+                    if (!(next_norm > floor && std::isfinite(1.0 / next_norm))) next_norm = 0;
                     H[size_t(col + 1) * cycle + col] = next_norm;
                     for (int row = 0; row < col; ++row)
                     {
@@ -666,25 +700,34 @@ namespace pcfd
                     if (!std::isfinite(y[row])) { used = 0; break; }
                 }
                 if (used == 0) break;
-                vec_zero(s, s.correction);
-                for (int col = 0; col < used; ++col) vec_axpy_active(s, s.correction, s.gmres_z.p + size_t(col) * n, y[col]);
+                {
+                    VecSet Z;
+                    Coefficients coefficient;
+                    for (int col = 0; col < used; ++col)
+                    {
+                        Z.push(s.gmres_z.p + size_t(col) * ld);
+                        coefficient.value[col] = y[col];
+                    }
+                    block_combine(s, Z, coefficient, s.correction, false);
+                }
                 vec_axpy_active(s, x, s.correction, 1.0);
                 residual2 = true_residual();
                 result.relative_residual = std::sqrt(residual2 / rhs2);
                 if (!std::isfinite(result.relative_residual)) break;
                 // store a normalised (U, C = A U) pair when it adds a resolved direction
                 launch_apply(s, s.correction, s.Ad, false);
-                const double cand_before = std::sqrt(std::max(0.0, device_dot(s, s.Ad, s.Ad)));
+                {
+                    const VecSet Cset = recycle_set(s.recycle_c.p), Uset = recycle_set(s.recycle_u.p);
+                    block_dot(s, Cset, s.Ad, h1);
+                    block_update(s, Cset, h1, s.Ad, Uset, -1.0, s.correction, 2, h2);
+                    block_update(s, Cset, h2, s.Ad, Uset, -1.0, s.correction, 1, h3);
+                    read_block(3);
+                }
+                const int kc = s.recycle_count;
+                const double cand_before = std::sqrt(std::max(0.0, host_h1[kc]));
                 bool cand_valid = cand_before > 0 && std::isfinite(cand_before);
-                for (int pass = 0; pass < 2 && cand_valid; ++pass)
-                    for (int c = 0; c < s.recycle_count; ++c)
-                    {
-                        const double value = device_dot(s, rcv(c), s.Ad);
-                        if (!finite_value(value)) { cand_valid = false; break; }
-                        vec_axpy_active(s, s.Ad, rcv(c), -value);
-                        vec_axpy_active(s, s.correction, ru(c), -value);
-                    }
-                const double cand_after = cand_valid ? std::sqrt(std::max(0.0, device_dot(s, s.Ad, s.Ad))) : 0;
+                for (int c = 0; c < kc && cand_valid; ++c) cand_valid = finite_value(host_h1[c]) && finite_value(host_h2[c]);
+                const double cand_after = cand_valid ? std::sqrt(std::max(0.0, host_h3[0])) : 0;
                 cand_valid = cand_valid && std::isfinite(cand_after) && cand_after > 1e-12 * cand_before && std::isfinite(1.0 / cand_after);
                 if (cand_valid)
                 {
