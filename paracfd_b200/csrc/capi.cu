@@ -776,6 +776,10 @@ pcfd_status pcfd_time_kernel(pcfd_system* system, int32_t which, int32_t iterati
             case 6:
             case 7:
             case 8: preconditioner_stage(s, which - 6, s.scratch_p, s.scratch_out); break;
+            case 10:
+            case 11:
+            case 12:
+            case 13: fine_preconditioner_stage(s, which - 10, s.scratch_p, s.scratch_out); break;
             case 9:
             {
                 // one GCRO column orthogonalisation against 3 recycled + 13 basis vectors

@@ -272,6 +272,7 @@ namespace pcfd
     // fused fine level (smoother.cu) around the coarse hierarchy below it (solver.cu)
     void build_fine_smoother(System& s, const pcfd_topology& t, const std::vector<double>& diagonal);
     void brick_apply(System& s, const double* p, double* out);   // code-byte structured operator
+    void fine_preconditioner_stage(System& s, int stage, const double* r, double* z);
     template <class T> void fine_preconditioner(System& s, const double* r, double* z, std::vector<MgLevel<T>>& levels);
     template <class T> void multigrid_levels(System& s, std::vector<MgLevel<T>>& levels);
     pcfd_solve_result solve(System& s, double* x, const double* b, double tolerance, int max_iterations, bool warm);

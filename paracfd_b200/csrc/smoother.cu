@@ -572,6 +572,41 @@ namespace pcfd
         cuda_check(cudaGetLastError(), "fused preconditioner");
     }
 
+    // Stages of the fused cycle for component timing: 0 pre-smoothing, 1 residual restriction to
+    // the level-0 aggregates, 2 the aggregation hierarchy, 3 prolongation + post-smoothing.
+    void fine_preconditioner_stage(System& s, int stage, const double* r, double* z)
+    {
+        require(s.fine.enabled && !s.mg64.empty(), "fused preconditioner not enabled");
+        FineSmoother& f = s.fine;
+        std::vector<MgLevel<double>>& levels = s.mg64;
+        MgLevel<double>& base = levels.front();
+        double* a = f.z.p;
+        if (stage == 0)
+        {
+            first_sweep_kernel<<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(f.code, s.brick_level, s.d_level_h, s.diagonal,
+                                                                                  s.active, r, a, s.structured, s.S, 2.0 / 3.0);
+            sweep<double, false>(s, a, r, z, nullptr);
+        }
+        else if (stage == 1)
+        {
+            brick_fine_kernel<1, double, false><<<s.active_bricks, 256, 0, launch_stream(s)>>>(
+                view(s), z, r, nullptr, f.t, nullptr, f.partial, 2.0 / 3.0);
+            finish<1, double, false>(s, z, r, nullptr, nullptr);
+            gather_base_kernel<double><<<blocks_for(base.cells), kThreads, 0, launch_stream(s)>>>(
+                base.cells, f.gather_offset, f.gather_entry, f.partial, f.deferred_residual, base.rhs);
+        }
+        else if (stage == 2)
+        {
+            cuda_check(cudaMemsetAsync(base.x, 0, size_t(base.cells) * sizeof(double), s.stream), "clear base correction");
+            multigrid_levels(s, levels);
+        }
+        else
+        {
+            sweep<double, true>(s, z, r, a, base.x.p);
+            sweep<double, false>(s, a, r, z, nullptr);
+        }
+    }
+
     template void fine_preconditioner<double>(System&, const double*, double*, std::vector<MgLevel<double>>&);
     template void fine_preconditioner<float>(System&, const double*, double*, std::vector<MgLevel<float>>&);
 }
