@@ -267,6 +267,15 @@ pcfd_status pcfd_pressure_apply_host(pcfd_system* system, const double* p, doubl
                                      int32_t orthogonal);
 pcfd_status pcfd_pressure_apply_device(pcfd_system* system, const double* d_p, double* d_out,
                                        int32_t orthogonal);
+/* No reference counterpart.  The same operator as pcfd_pressure_apply_device, but the call
+ * allocates nothing: the WLS-gradient scratch is a static device array of at most 262,144
+ * gradient nodes (6 MiB), shared by all systems on the device; systems with more nodes get
+ * PCFD_INVALID_ARG for the full operator.  For callers that cannot allocate at call time
+ * (device memory reserved by another pool, allocator-free loops).  The first call on a device
+ * sets up the scratch address and should come before any stream capture; calls overlapping in
+ * time race on the scratch. */
+pcfd_status pcfd_pressure_apply_device_noalloc(pcfd_system* system, const double* d_p, double* d_out,
+                                               int32_t orthogonal);
 /* Jacobi diagonal used by the smoother (diagonal_cpu semantics). diag: [S]. */
 pcfd_status pcfd_pressure_diagonal_host(pcfd_system* system, double* diag);
 /* z = M^-1 r with the reference-structured V-cycle (FP64 or FP32 per options). [S]. */

@@ -161,6 +161,7 @@ SIGNATURES = {
     "pcfd_system_synchronize": (C.c_int, [C.c_void_p]),
     "pcfd_pressure_apply_host": (C.c_int, [C.c_void_p, _f64p, _f64p, C.c_int32]),
     "pcfd_pressure_apply_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]),
+    "pcfd_pressure_apply_device_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]),
     "pcfd_pressure_diagonal_host": (C.c_int, [C.c_void_p, _f64p]),
     "pcfd_pressure_precondition_host": (C.c_int, [C.c_void_p, _f64p, _f64p]),
     "pcfd_pressure_solve_host": (C.c_int, [C.c_void_p, _f64p, _f64p, C.c_double, C.c_int32,

@@ -328,6 +328,15 @@ pcfd_status pcfd_pressure_apply_device(pcfd_system* system, const double* d_p, d
     });
 }
 
+pcfd_status pcfd_pressure_apply_device_noalloc(pcfd_system* system, const double* d_p, double* d_out, int32_t orthogonal)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(d_p && d_out, "null device vector");
+        launch_apply_noalloc(s, d_p, d_out, orthogonal != 0);
+    });
+}
+
 pcfd_status pcfd_pressure_diagonal_host(pcfd_system* system, double* diag)
 {
     return guarded([&] {

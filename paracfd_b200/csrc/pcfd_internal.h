@@ -262,6 +262,8 @@ namespace pcfd
 
     // ---- kernels / launchers (pressure.cu) ----
     void launch_apply(System& s, const double* p, double* out, bool orthogonal_only);
+    // same operator with the WLS gradient scratch in a static device array (pressure.cu)
+    void launch_apply_noalloc(System& s, const double* p, double* out, bool orthogonal_only);
     void launch_apply32(System& s, const float* p, float* out);
     double device_dot(System& s, const double* a, const double* b);
     void build_operator(System& s, const pcfd_topology& t);

@@ -17,6 +17,7 @@
 #include <cstring>
 #include <limits>
 #include <numeric>
+#include <mutex>
 #include <unordered_map>
 
 namespace pcfd
@@ -499,5 +500,98 @@ namespace pcfd
             o.gauge_dof.upload(std::vector<int>(t.gauge_dof, t.gauge_dof + o.gauges));
             o.gauge_coefficient.upload(std::vector<double>(t.gauge_coefficient, t.gauge_coefficient + o.gauges));
         }
+    }
+
+    // ==================================================================================
+    // allocation-free operator apply
+    // ==================================================================================
+    // The full operator needs FP64 scratch for the WLS pressure gradient at every gradient node
+    // (3 doubles per node).  pcfd_pressure_apply_device takes it from the system; this variant
+    // takes it from a fixed static device array instead, so a call performs no device or pinned
+    // allocation of any kind and never touches the system's own scratch.  It serves callers that
+    // cannot allocate at call time -- hosts whose device memory is fully reserved by another
+    // pool, latency-bound loops that must not enter the allocator -- and a second user of one
+    // system that must not disturb the scratch an in-flight solve on that system is using.
+    //
+    // Limits and contract:
+    //   * at most kNoAllocGradientNodes WLS gradient nodes (262,144 nodes, 6 MiB of scratch);
+    //     larger systems are rejected with PCFD_INVALID_ARG before anything is launched;
+    //   * the first call on a device looks up the scratch address with the device current;
+    //     make that first call before any stream capture;
+    //   * the scratch is shared by every system on the device: calls that overlap in time (other
+    //     threads or other streams) race on it -- serialise them;
+    //   * no scratch entry needs to start at zero: the gradient kernel writes all 3 components
+    //     of every node before the gather reads them; the output is written exactly where
+    //     pcfd_pressure_apply_device writes it (every cell of the non-covered bricks and every
+    //     EB fragment).
+    namespace
+    {
+        constexpr int kNoAllocGradientNodes = 1 << 18;
+        static __device__ __align__(256) double g_noalloc_gradient[3 * kNoAllocGradientNodes];
+
+        constexpr int kNoAllocMaxDevices = 64;
+        std::mutex g_noalloc_mutex;
+        double* g_noalloc_scratch[kNoAllocMaxDevices] = {};
+
+        // One-time, per-device lookup of the static scratch with that device current.
+        double* noalloc_scratch(int device)
+        {
+            require(device >= 0 && device < kNoAllocMaxDevices, "device ordinal out of range");
+            std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+            if (!g_noalloc_scratch[device])
+            {
+                int current = 0;
+                cuda_check(cudaGetDevice(&current), "cudaGetDevice");
+                if (current != device) cuda_check(cudaSetDevice(device), "cudaSetDevice");
+                void* ptr = nullptr;
+                const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_gradient);
+                if (current != device) cudaSetDevice(current);
+                cuda_check(e, "cudaGetSymbolAddress(noalloc gradient scratch)");
+                g_noalloc_scratch[device] = static_cast<double*>(ptr);
+            }
+            return g_noalloc_scratch[device];
+        }
+    }
+
+    void launch_apply_noalloc(System& s, const double* p, double* out, bool orthogonal_only)
+    {
+        IrregularOperator& o = s.irr;
+        if (!orthogonal_only && o.gradient_nodes > kNoAllocGradientNodes)
+            throw Error(PCFD_INVALID_ARG, "pcfd_pressure_apply_device_noalloc: " + std::to_string(o.gradient_nodes) +
+                                              " WLS gradient nodes exceed the static scratch maximum of " +
+                                              std::to_string(kNoAllocGradientNodes));
+        double* gradient = noalloc_scratch(s.device);
+        if (s.active_bricks)
+        {
+            if (s.fine.enabled && aligned16(p) && aligned16(out)) brick_apply(s, p, out);
+            else if (s.bs == 8)
+                structured_apply8_kernel<double><<<s.active_bricks, 256, 0, launch_stream(s)>>>(
+                    s.active_brick_list, s.brick_level, s.brick_nbr, s.brick_flags, s.d_level_h, s.active,
+                    s.cut_face_mask, p, out, s.outlet ? 1 : 0);
+            else
+                structured_apply_generic_kernel<double><<<blocks_for(int64_t(s.active_bricks) * s.bs3), kThreads, 0, launch_stream(s)>>>(
+                    s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr, s.brick_flags, s.d_level_h,
+                    s.active, s.cut_face_mask, p, out, s.outlet ? 1 : 0);
+        }
+        if (s.S > s.structured)
+            zero_range_kernel<<<blocks_for(s.S - s.structured), kThreads, 0, launch_stream(s)>>>(out, s.structured, s.S);
+        if (o.incident_dofs)
+            irregular_orthogonal_gather_kernel<<<blocks_for(o.incident_dofs), kThreads, 0, launch_stream(s)>>>(
+                o.incident_dof, o.incident_offset, o.incident_edge, o.incident_sign, o.incident_dofs, o.connection_count,
+                o.conn_lower, o.conn_upper, o.conn_coefficient, o.reg_lower, o.reg_upper, o.reg_coefficient, s.active, p, out);
+        if (o.gauges)
+            gauge_apply_kernel<<<blocks_for(o.gauges), kThreads, 0, launch_stream(s)>>>(o.gauge_dof, o.gauge_coefficient, o.gauges, p, out);
+        if (!orthogonal_only && o.gradient_nodes)
+        {
+            reconstruct_gradient_kernel<<<blocks_for(o.gradient_nodes), kThreads, 0, launch_stream(s)>>>(
+                o.grad_dof, o.grad_offset, o.grad_neighbour, o.grad_weight, p, gradient, o.gradient_nodes);
+            if (o.incident_dofs)
+                irregular_nonorthogonal_gather_kernel<<<blocks_for(o.incident_dofs), kThreads, 0, launch_stream(s)>>>(
+                    o.incident_dof, o.incident_offset, o.incident_edge, o.incident_sign, o.incident_dofs, o.connection_count,
+                    o.conn_lower, o.conn_upper, o.conn_lower_node, o.conn_upper_node, o.conn_correction, o.conn_upper_weight,
+                    o.conn_area, o.reg_lower, o.reg_upper, o.reg_lower_node, o.reg_upper_node, o.reg_correction,
+                    o.reg_upper_weight, o.reg_area, gradient, s.active, out);
+        }
+        cuda_check(cudaGetLastError(), "launch allocation-free pressure operator");
     }
 }
