@@ -335,7 +335,8 @@ def run_ours(args, ranks: Ranks):
     # isolated per-component device times on the same resident system (not part of the timed region)
     components = {0: "apply_full", 1: "apply_orthogonal", 2: "preconditioner", 3: "divergence", 4: "flux_correction",
                   5: "dot", 6: "mg_presmooth", 7: "mg_coarse_correction", 8: "mg_postsmooth", 9: "gcro_column_orth_m16",
-                  10: "fused_presmooth", 11: "fused_restrict", 12: "mg_hierarchy", 13: "fused_prolong_postsmooth"}
+                  10: "fused_presmooth", 11: "fused_restrict", 12: "mg_hierarchy", 13: "fused_prolong_postsmooth",
+                  14: "gcro_column_orth_m8", 15: "gcro_column_orth_m27"}
     kernel_ms = {}
     for which, name in components.items():
         try:

@@ -790,20 +790,21 @@ pcfd_status pcfd_time_kernel(pcfd_system* system, int32_t which, int32_t iterati
             case 12:
             case 13: fine_preconditioner_stage(s, which - 10, s.scratch_p, s.scratch_out); break;
             case 9:
+            case 14:
+            case 15:
             {
-                // one GCRO column orthogonalisation against 3 recycled + 13 basis vectors
+                // one GCRO column orthogonalisation (CGS2, three passes) against 3 recycled + V
+                // basis vectors: 13 (m = 16), 5 (m = 8) or 24 (m = 27)
                 require(s.full_nonorthogonal, "block orthogonalisation needs the GCRO storage");
-                VecSet Q, U;
-                for (int c = 0; c < System::recycle_capacity; ++c)
-                {
-                    Q.push(s.recycle_c.p + size_t(c) * s.Sp);
-                    U.push(s.recycle_u.p + size_t(c) * s.Sp);
-                }
-                for (int row = 0; row < 13; ++row) Q.push(s.gmres_v.p + size_t(row) * s.Sp);
+                const int basis = which == 9 ? 13 : (which == 14 ? 5 : 24);
+                VecSet Q(s.Sp);
+                const VecSet none(s.Sp);
+                for (int c = 0; c < System::recycle_capacity; ++c) Q.push(s.recycle_c.p + size_t(c) * s.Sp);
+                for (int row = 0; row < basis; ++row) Q.push(s.gmres_v.p + size_t(row) * s.Sp);
                 double* h = s.block_result.p;
                 block_dot(s, Q, s.Ad, h);
-                block_update(s, Q, h, s.Ad, U, -1.0, s.gmres_z.p, 2, h + kMaxSet + 1);
-                block_update(s, Q, h + kMaxSet + 1, s.Ad, U, -1.0, s.gmres_z.p, 1, h + 2 * (kMaxSet + 1));
+                block_update(s, Q, h, s.Ad, none, -1.0, nullptr, 2, h + kMaxSet + 1);
+                block_update(s, Q, h + kMaxSet + 1, s.Ad, none, -1.0, nullptr, 1, h + 2 * (kMaxSet + 1));
                 break;
             }
             default: throw Error(PCFD_INVALID_ARG, "unknown kernel id");

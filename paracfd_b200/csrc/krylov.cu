@@ -18,9 +18,11 @@ namespace pcfd
 {
     namespace
     {
-        constexpr int kBlocks = 592;   // 4 CTAs per SM on 148 SMs
         constexpr int kThreadsBlock = 256;
         constexpr int kStride = kMaxSet + 1;
+        constexpr int kLanes = 4;                              // lanes per element pair
+        constexpr int kPairsPerWarp = 32 / kLanes;             // 8
+        constexpr int kPairsPerPass = kPairsPerWarp * (kThreadsBlock / 32);   // 64 pairs per CTA pass
 
         __device__ inline double warp_sum(double v)
         {
@@ -28,22 +30,61 @@ namespace pcfd
             return v;
         }
 
-        // Sums acc[0..count] over the block into partial[blockIdx.x * kStride + j].
-        template <int M>
-        __device__ inline void block_store(double (&acc)[M + 1], int count, double* partial)
+        // The DOF range swept by the block kernels: the non-covered bricks (one 512-entry brick
+        // per CTA iteration, 256 threads x one 16-byte pair) followed by the EB-fragment tail
+        // [structured, padded length) in 512-entry chunks.  Covered-brick slots hold no DOF and
+        // are skipped.  Every vector is 16-byte aligned; padding entries are inactive.
+        struct Sweep
         {
-            __shared__ double shared[kThreadsBlock / 32][M + 1];
-            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-            for (int j = 0; j <= M; ++j)
+            const int* bricks;
+            int64_t brick_count, items, structured, padded;
+            __device__ int64_t base(int64_t item) const
             {
-                const double v = warp_sum(acc[j]);
-                if (lane == 0) shared[warp][j] = v;
+                return item < brick_count ? int64_t(bricks[item]) * 512 : structured + (item - brick_count) * 512;
+            }
+        };
+
+        // ---- split-lane block kernels ----------------------------------------------------------
+        // Four lanes share one element pair (16 bytes of every vector): lane l handles pair
+        // (l & 7) of an 8-pair warp segment and vectors [V * (l >> 3), V * (l >> 3) + V), V = 1, 2,
+        // 4 or 8 for up to 4, 8, 16 or 32 vectors.  Each basis entry is loaded exactly once and a
+        // thread holds only V loads and V + 1 accumulators, so registers stay low and many warps
+        // keep loads in flight.  The four partial updates of an entry are combined as
+        // ((q0 + q1) + (q2 + q3)) on every lane, so the four lanes hold the same bits; the dot
+        // partials are reduced per quarter and then over the block in fixed order.
+        __device__ inline double quarter_total(double v)
+        {
+            const int pair = threadIdx.x & 7;
+            const double q0 = __shfl_sync(0xffffffffu, v, pair), q1 = __shfl_sync(0xffffffffu, v, pair + 8);
+            const double q2 = __shfl_sync(0xffffffffu, v, pair + 16), q3 = __shfl_sync(0xffffffffu, v, pair + 24);
+            return (q0 + q1) + (q2 + q3);
+        }
+        __device__ inline double segment_sum(double v)
+        {
+            for (int o = 4; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o, 8);
+            return v;
+        }
+
+        // sums acc[u] of vector V*quarter + u and the norm (kept by quarter 0) into partial[block][j]
+        template <int V>
+        __device__ inline void block_store(double (&acc)[V + 1], int count, double* partial)
+        {
+            __shared__ double shared[kThreadsBlock / 32][kMaxSet + 1];
+            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, quarter = lane >> 3;
+#pragma unroll
+            for (int u = 0; u <= V; ++u)
+            {
+                const double v = segment_sum(acc[u]);
+                if ((lane & 7) == 0)
+                {
+                    if (u < V) shared[warp][V * quarter + u] = v;
+                    else if (quarter == 0) shared[warp][kMaxSet] = v;
+                }
             }
             __syncthreads();
             if (threadIdx.x <= count)
             {
-                const int j = threadIdx.x == count ? M : threadIdx.x;   // the norm lives in slot M
+                const int j = threadIdx.x == count ? kMaxSet : threadIdx.x;
                 double v = 0.0;
 #pragma unroll
                 for (int w = 0; w < kThreadsBlock / 32; ++w) v += shared[w][j];
@@ -51,102 +92,98 @@ namespace pcfd
             }
         }
 
-        // Vectors are processed as pairs (16-byte loads): n2 = padded length / 2, every vector
-        // 16-byte aligned, padding entries inactive.
-        template <int M>
-        __global__ void __launch_bounds__(kThreadsBlock) block_dot_kernel(VecSet Q, const double* __restrict__ w,
-            const uint8_t* __restrict__ active, int64_t n2, double* __restrict__ partial)
+        // kMode -1: h = Q^T w and w.w (w unchanged)
+        //        0: w -= Q h, y += sign * U h[0..|U|)
+        //        1: as 0, then w.w
+        //        2: as 0, then Q^T w and w.w
+        template <int V, int kMode>
+        __global__ void __launch_bounds__(kThreadsBlock, V >= 8 ? 2 : 1) block_kernel(VecSet Q, const double* __restrict__ h, double* __restrict__ w,
+            VecSet U, double sign, double* __restrict__ y, const uint8_t* __restrict__ active, Sweep range, double* __restrict__ partial)
         {
-            double acc[M + 1];
+            __shared__ double coefficient[kMaxSet];
+            double acc[V + 1];
 #pragma unroll
-            for (int j = 0; j <= M; ++j) acc[j] = 0.0;
-            const int count = Q.count;
-            for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n2; q += int64_t(gridDim.x) * blockDim.x)
+            for (int u = 0; u <= V; ++u) acc[u] = 0.0;
+            const int count = Q.size(), ucount = U.size();
+            const int lane = threadIdx.x & 31, quarter = lane >> 3;
+            if (kMode >= 0)
             {
-                const uchar2 a = reinterpret_cast<const uchar2*>(active)[q];
-                double2 wq = reinterpret_cast<const double2*>(w)[q];
-#pragma unroll
-                for (int j = 0; j < M; ++j)
-                    if (j < count)
-                    {
-                        const double2 v = reinterpret_cast<const double2*>(Q.v[j])[q];
-                        acc[j] += a.x ? v.x * wq.x : 0.0;
-                        acc[j] += a.y ? v.y * wq.y : 0.0;
-                    }
-                acc[M] += a.x ? wq.x * wq.x : 0.0;
-                acc[M] += a.y ? wq.y * wq.y : 0.0;
+                if (threadIdx.x < kMaxSet) coefficient[threadIdx.x] = threadIdx.x < count ? h[threadIdx.x] : 0.0;
+                __syncthreads();
             }
-            block_store<M>(acc, count, partial);
-        }
-
-        // mode 0: update only; 1: + w'.w'; 2: + Q^T w' and w'.w'.  Inactive entries are left
-        // untouched and contribute nothing.
-        template <int M, int kMode>
-        __global__ void __launch_bounds__(kThreadsBlock) block_update_kernel(VecSet Q, const double* __restrict__ h, double* __restrict__ w,
-            VecSet U, double sign, double* __restrict__ y, const uint8_t* __restrict__ active, int64_t n2, double* __restrict__ partial)
-        {
-            __shared__ double coefficient[M];
-            double acc[M + 1];
-#pragma unroll
-            for (int j = 0; j <= M; ++j) acc[j] = 0.0;
-            const int count = Q.count, ucount = U.count;
-            if (threadIdx.x < M) coefficient[threadIdx.x] = threadIdx.x < count ? h[threadIdx.x] : 0.0;
-            __syncthreads();
-            for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n2; q += int64_t(gridDim.x) * blockDim.x)
+            const int seg_pair = ((threadIdx.x >> 5) * kPairsPerWarp) + (lane & 7);   // 0..63
+            for (int64_t item = blockIdx.x; item < range.items; item += gridDim.x)
             {
-                const uchar2 a = reinterpret_cast<const uchar2*>(active)[q];
-                // up to 16 basis pairs stay in registers for the dot pass; wider sets re-read
-                // them (the lines were just fetched, so the second read is served by L2)
-                constexpr int kKeep = M <= 16 ? M : 1;
-                double2 qv[kKeep];
-                const double2 w0 = reinterpret_cast<const double2*>(w)[q];
-                double2 wq = w0;
+                const int64_t base = range.base(item);
+#pragma unroll 1
+                for (int sub = 0; sub < 256 / kPairsPerPass; ++sub)
+                {
+                    // every lane runs the shuffles below; a pair past the end only loads nothing
+                    const int64_t e = base + 2 * (seg_pair + kPairsPerPass * sub);
+                    const bool valid = e < range.padded;
+                    const int64_t q = valid ? e >> 1 : 0;
+                    const uchar2 a = valid ? reinterpret_cast<const uchar2*>(active)[q] : make_uchar2(0, 0);
+                    const double2 w0 = valid ? reinterpret_cast<const double2*>(w)[q] : make_double2(0.0, 0.0);
+                    double2 v[V];
 #pragma unroll
-                for (int j = 0; j < M; ++j)
-                    if (j < count)
+                    for (int u = 0; u < V; ++u)
                     {
-                        const double2 v = reinterpret_cast<const double2*>(Q.v[j])[q];
-                        if (M <= 16) qv[j % kKeep] = v;
-                        wq.x -= coefficient[j] * v.x;
-                        wq.y -= coefficient[j] * v.y;
+                        const int j = V * quarter + u;
+                        v[u] = valid && j < count ? reinterpret_cast<const double2*>(Q.vec(j))[q] : make_double2(0.0, 0.0);
                     }
-                wq.x = a.x ? wq.x : w0.x;
-                wq.y = a.y ? wq.y : w0.y;
-                reinterpret_cast<double2*>(w)[q] = wq;
-                if (ucount)
-                {
-                    const double2 y0 = reinterpret_cast<const double2*>(y)[q];
-                    double2 yq = y0;
+                    double2 wq = w0;
+                    if (kMode >= 0)
+                    {
+                        double px = 0.0, py = 0.0;
 #pragma unroll
-                    for (int j = 0; j < M; ++j)
-                        if (j < ucount)
+                        for (int u = 0; u < V; ++u)
                         {
-                            const double2 u = reinterpret_cast<const double2*>(U.v[j])[q];
-                            yq.x += sign * coefficient[j] * u.x;
-                            yq.y += sign * coefficient[j] * u.y;
+                            px += coefficient[V * quarter + u] * v[u].x;
+                            py += coefficient[V * quarter + u] * v[u].y;
                         }
-                    yq.x = a.x ? yq.x : y0.x;
-                    yq.y = a.y ? yq.y : y0.y;
-                    reinterpret_cast<double2*>(y)[q] = yq;
-                }
-                if (kMode == 2)
-                {
+                        const double sx = quarter_total(px), sy = quarter_total(py);
+                        wq.x = a.x ? w0.x - sx : w0.x;
+                        wq.y = a.y ? w0.y - sy : w0.y;
+                        if (quarter == 0 && valid) reinterpret_cast<double2*>(w)[q] = wq;
+                        if (ucount)
+                        {
+                            double ux = 0.0, uy = 0.0;
 #pragma unroll
-                    for (int j = 0; j < M; ++j)
-                        if (j < count)
-                        {
-                            const double2 v = M <= 16 ? qv[j % kKeep] : reinterpret_cast<const double2*>(Q.v[j])[q];
-                            acc[j] += a.x ? v.x * wq.x : 0.0;
-                            acc[j] += a.y ? v.y * wq.y : 0.0;
+                            for (int u = 0; u < V; ++u)
+                            {
+                                const int j = V * quarter + u;
+                                if (valid && j < ucount)
+                                {
+                                    const double2 uv = reinterpret_cast<const double2*>(U.vec(j))[q];
+                                    ux += sign * coefficient[j] * uv.x;
+                                    uy += sign * coefficient[j] * uv.y;
+                                }
+                            }
+                            const double tx = quarter_total(ux), ty = quarter_total(uy);
+                            if (quarter == 0 && valid)
+                            {
+                                const double2 y0 = reinterpret_cast<const double2*>(y)[q];
+                                reinterpret_cast<double2*>(y)[q] = make_double2(a.x ? y0.x + tx : y0.x, a.y ? y0.y + ty : y0.y);
+                            }
                         }
-                }
-                if (kMode >= 1)
-                {
-                    acc[M] += a.x ? wq.x * wq.x : 0.0;
-                    acc[M] += a.y ? wq.y * wq.y : 0.0;
+                    }
+                    if (kMode == -1 || kMode == 2)
+                    {
+#pragma unroll
+                        for (int u = 0; u < V; ++u)
+                        {
+                            acc[u] += a.x ? v[u].x * wq.x : 0.0;
+                            acc[u] += a.y ? v[u].y * wq.y : 0.0;
+                        }
+                    }
+                    if (kMode != 0 && quarter == 0)
+                    {
+                        acc[V] += a.x ? wq.x * wq.x : 0.0;
+                        acc[V] += a.y ? wq.y * wq.y : 0.0;
+                    }
                 }
             }
-            if (kMode >= 1) block_store<M>(acc, kMode == 2 ? count : 0, partial);
+            if (kMode != 0) block_store<V>(acc, kMode == 1 ? 0 : count, partial);
         }
 
         // out[j] = sum over blocks of partial[b * kStride + j], j <= count (fixed order).
@@ -171,107 +208,122 @@ namespace pcfd
             }
         }
 
-        __global__ void combine_kernel(VecSet Z, Coefficients c, double* __restrict__ y, int accumulate,
-                                       const uint8_t* __restrict__ active, int64_t n)
+        // y (+)= Z c on the active entries of the swept range (inactive entries 0 when not
+        // accumulating); one CTA iteration per brick, one pair per thread.
+        __global__ void __launch_bounds__(256) combine_kernel(VecSet Z, Coefficients c, double* __restrict__ y, int accumulate,
+                                                               const uint8_t* __restrict__ active, Sweep range)
         {
-            const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-            if (q >= n) return;
-            if (!active[q]) { if (!accumulate) y[q] = 0.0; return; }
-            double v = accumulate ? y[q] : 0.0;
-            for (int j = 0; j < Z.count; ++j) v += c.value[j] * Z.v[j][q];
-            y[q] = v;
+            for (int64_t item = blockIdx.x; item < range.items; item += gridDim.x)
+            {
+                const int64_t e = range.base(item) + 2 * threadIdx.x;
+                if (e >= range.padded) continue;
+                const uchar2 a = reinterpret_cast<const uchar2*>(active)[e >> 1];
+                double2 v = accumulate ? reinterpret_cast<const double2*>(y)[e >> 1] : make_double2(0.0, 0.0);
+                for (int j = 0; j < Z.size(); ++j)
+                {
+                    const double2 z = reinterpret_cast<const double2*>(Z.vec(j))[e >> 1];
+                    v.x += c.value[j] * z.x;
+                    v.y += c.value[j] * z.y;
+                }
+                if (!a.x) v.x = accumulate ? y[e] : 0.0;
+                if (!a.y) v.y = accumulate ? y[e + 1] : 0.0;
+                reinterpret_cast<double2*>(y)[e >> 1] = v;
+            }
         }
 
-        __global__ void scale_by_inverse_norm_kernel(double* __restrict__ dst, const double* __restrict__ src,
-                                                     const double* __restrict__ norm2, const uint8_t* __restrict__ active, int64_t n)
+        __global__ void __launch_bounds__(256) scale_by_inverse_norm_kernel(double* __restrict__ dst, const double* __restrict__ src,
+            const double* __restrict__ norm2, const uint8_t* __restrict__ active, Sweep range)
         {
-            const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-            if (q >= n) return;
             const double a = 1.0 / sqrt(fmax(0.0, norm2[0]));
-            dst[q] = active[q] ? a * src[q] : 0.0;
+            for (int64_t item = blockIdx.x; item < range.items; item += gridDim.x)
+            {
+                const int64_t e = range.base(item) + 2 * threadIdx.x;
+                if (e >= range.padded) continue;
+                const uchar2 m = reinterpret_cast<const uchar2*>(active)[e >> 1];
+                const double2 v = reinterpret_cast<const double2*>(src)[e >> 1];
+                reinterpret_cast<double2*>(dst)[e >> 1] = make_double2(m.x ? a * v.x : 0.0, m.y ? a * v.y : 0.0);
+            }
         }
 
-        // Grid of a block kernel; it depends only on the device, so the reduction order is fixed.
-        template <class K> int resident_grid(K kernel)
+        Sweep sweep_range(const System& s)
         {
-            // 4 CTAs per SM: at the register budget of the widest instantiation two are resident at
-            // a time and the 16-byte loads keep enough bytes in flight either way.
-            (void)kernel;
-            int device = 0, sms = 0;
-            cuda_check(cudaGetDevice(&device), "device");
-            cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
-            return std::max(1, std::min(kBlocks, 4 * sms));
+            if (s.bs != 8) return Sweep{nullptr, 0, (int64_t(s.Sp) + 511) / 512, 0, s.Sp};   // contiguous chunks
+            const int64_t tail = (int64_t(s.Sp) - s.structured + 511) / 512;
+            return Sweep{s.active_brick_list, s.active_bricks, int64_t(s.active_bricks) + std::max<int64_t>(0, tail), s.structured,
+                         s.Sp};
         }
 
-        template <int M> int launch_dot(System& s, const VecSet& Q, const double* w)
+        // Grid of the block kernels; it depends only on the device, so the reduction order is fixed.
+        int block_grid()
         {
-            const int grid = resident_grid(block_dot_kernel<M>);
-            block_dot_kernel<M><<<grid, kThreadsBlock, 0, launch_stream(s)>>>(Q, w, s.active, s.Sp / 2, s.block_partial);
-            return grid;
+            static int sms = 0;
+            if (!sms)
+            {
+                int device = 0;
+                cuda_check(cudaGetDevice(&device), "device");
+                cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
+            }
+            return std::min(592, 4 * sms);
         }
-        template <int M, int kMode>
-        int launch_update(System& s, const VecSet& Q, const double* h, double* w, const VecSet& U, double sign, double* y)
-        {
-            const int grid = resident_grid(block_update_kernel<M, kMode>);
-            block_update_kernel<M, kMode><<<grid, kThreadsBlock, 0, launch_stream(s)>>>(Q, h, w, U, sign, y, s.active, s.Sp / 2,
-                                                                                        s.block_partial);
-            return grid;
-        }
+
         template <int kMode>
-        int dispatch_update(System& s, const VecSet& Q, const double* h, double* w, const VecSet& U, double sign, double* y)
+        int launch_block(System& s, const VecSet& Q, const double* h, double* w, const VecSet& U, double sign, double* y)
         {
-            const int m = std::max(Q.count, U.count);
-            if (m <= 4) return launch_update<4, kMode>(s, Q, h, w, U, sign, y);
-            if (m <= 8) return launch_update<8, kMode>(s, Q, h, w, U, sign, y);
-            if (m <= 16) return launch_update<16, kMode>(s, Q, h, w, U, sign, y);
-            return launch_update<32, kMode>(s, Q, h, w, U, sign, y);
+            const int grid = block_grid();
+            const int m = std::max(Q.size(), U.size());
+            auto go = [&](auto kernel) {
+                kernel<<<grid, kThreadsBlock, 0, launch_stream(s)>>>(Q, h, w, U, sign, y, s.active, sweep_range(s), s.block_partial);
+            };
+            if (m <= 4) go(block_kernel<1, kMode>);
+            else if (m <= 8) go(block_kernel<2, kMode>);
+            else if (m <= 16) go(block_kernel<4, kMode>);
+            else go(block_kernel<8, kMode>);
+            return grid;
         }
-    }
 
-    namespace
-    {
         void require_aligned(const VecSet& set, const char* what)
         {
-            for (int j = 0; j < set.count; ++j) require(aligned16(set.v[j]), what);
+            for (int g = 0; g < 2; ++g) require(!set.count[g] || aligned16(set.base[g]), what);
+            require(set.size() <= 1 || (set.stride * int64_t(sizeof(double))) % 16 == 0, what);
         }
     }
 
     void block_dot(System& s, const VecSet& Q, const double* w, double* out)
     {
-        require(Q.count >= 0 && Q.count <= kMaxSet, "block dot: too many vectors");
+        require(Q.size() >= 0 && Q.size() <= kMaxSet, "block dot: too many vectors");
         require(aligned16(w), "block dot: vector not 16-byte aligned");
         require_aligned(Q, "block dot: vector not 16-byte aligned");
-        int grid;
-        if (Q.count <= 4) grid = launch_dot<4>(s, Q, w);
-        else if (Q.count <= 8) grid = launch_dot<8>(s, Q, w);
-        else if (Q.count <= 16) grid = launch_dot<16>(s, Q, w);
-        else grid = launch_dot<32>(s, Q, w);
-        block_final_kernel<<<1, 256, 0, launch_stream(s)>>>(s.block_partial, grid, Q.count, out);
+        const VecSet none(Q.stride);
+        const int grid = launch_block<-1>(s, Q, nullptr, const_cast<double*>(w), none, 0.0, nullptr);
+        block_final_kernel<<<1, 256, 0, launch_stream(s)>>>(s.block_partial, grid, Q.size(), out);
     }
 
     void block_update(System& s, const VecSet& Q, const double* h, double* w, const VecSet& U, double sign, double* y, int mode,
                       double* out)
     {
-        require(Q.count <= kMaxSet && U.count <= Q.count, "block update: invalid vector sets");
-        require(aligned16(w) && (!U.count || aligned16(y)), "block update: vector not 16-byte aligned");
+        require(Q.size() <= kMaxSet && U.size() <= Q.size(), "block update: invalid vector sets");
+        require(aligned16(w) && (!U.size() || aligned16(y)), "block update: vector not 16-byte aligned");
         require_aligned(Q, "block update: vector not 16-byte aligned");
         require_aligned(U, "block update: vector not 16-byte aligned");
         int grid;
-        if (mode == 0) grid = dispatch_update<0>(s, Q, h, w, U, sign, y);
-        else if (mode == 1) grid = dispatch_update<1>(s, Q, h, w, U, sign, y);
-        else grid = dispatch_update<2>(s, Q, h, w, U, sign, y);
+        if (mode == 0) grid = launch_block<0>(s, Q, h, w, U, sign, y);
+        else if (mode == 1) grid = launch_block<1>(s, Q, h, w, U, sign, y);
+        else grid = launch_block<2>(s, Q, h, w, U, sign, y);
         if (mode >= 1)
-            block_final_kernel<<<1, 256, 0, launch_stream(s)>>>(s.block_partial, grid, mode == 2 ? Q.count : 0, out);
+            block_final_kernel<<<1, 256, 0, launch_stream(s)>>>(s.block_partial, grid, mode == 2 ? Q.size() : 0, out);
     }
 
     void block_combine(System& s, const VecSet& Z, const Coefficients& c, double* y, bool accumulate)
     {
-        require(Z.count <= kMaxSet, "block combine: too many vectors");
-        combine_kernel<<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(Z, c, y, accumulate ? 1 : 0, s.active, s.S);
+        require(Z.size() <= kMaxSet, "block combine: too many vectors");
+        require(aligned16(y), "block combine: vector not 16-byte aligned");
+        require_aligned(Z, "block combine: vector not 16-byte aligned");
+        combine_kernel<<<4 * 148, 256, 0, launch_stream(s)>>>(Z, c, y, accumulate ? 1 : 0, s.active, sweep_range(s));
     }
 
     void scale_by_inverse_norm(System& s, double* dst, const double* src, const double* norm2)
     {
-        scale_by_inverse_norm_kernel<<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(dst, src, norm2, s.active, s.S);
+        require(aligned16(dst) && aligned16(src), "scale: vector not 16-byte aligned");
+        scale_by_inverse_norm_kernel<<<4 * 148, 256, 0, launch_stream(s)>>>(dst, src, norm2, s.active, sweep_range(s));
     }
 }

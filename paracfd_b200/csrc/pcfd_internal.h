@@ -124,13 +124,31 @@ namespace pcfd
         DBuf<double> t, z;                      // [S] deferred structured rows, ping-pong iterate
     };
 
-    // Up to kMaxSet vectors of one system, passed by value to the fused block kernels (krylov.cu).
+    // Up to kMaxSet vectors of one system, passed by value to the fused block kernels (krylov.cu):
+    // at most two groups of consecutive slots of a multi-vector buffer (e.g. recycled C then the
+    // Krylov basis), so a kernel addresses vector j as base + j * stride instead of holding a
+    // pointer per vector in registers.
     constexpr int kMaxSet = 32;   // >= GCRO restart (24) + recycled pairs (3) + 1
     struct VecSet
     {
-        const double* v[kMaxSet] = {};
-        int count = 0;
-        void push(const double* p) { v[count++] = p; }
+        const double* base[2] = {nullptr, nullptr};
+        int count[2] = {0, 0};
+        int64_t stride = 0;
+        VecSet() = default;
+        explicit VecSet(int64_t slot_stride) : stride(slot_stride) {}
+        __host__ __device__ int size() const { return count[0] + count[1]; }
+        __host__ __device__ const double* vec(int j) const
+        {
+            return j < count[0] ? base[0] + j * stride : base[1] + (j - count[0]) * stride;
+        }
+        void push(const double* p)
+        {
+            if (!count[0]) { base[0] = p; count[0] = 1; }
+            else if (!count[1] && p == base[0] + count[0] * stride) ++count[0];
+            else if (!count[1]) { base[1] = p; count[1] = 1; }
+            else if (p == base[1] + count[1] * stride) ++count[1];
+            else throw Error(PCFD_INTERNAL, "vector set is not two strided groups");
+        }
     };
     struct Coefficients
     {

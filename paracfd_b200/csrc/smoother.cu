@@ -38,10 +38,6 @@ namespace pcfd
             int nbase[6];   // level-0 cell of each neighbour's first cell
         };
 
-        struct BrickHead
-        {
-            int slot, level, base, partial;
-        };
 
         struct BrickView
         {
@@ -61,61 +57,6 @@ namespace pcfd
             return b0 + ((k >> l) << 6) + ((j >> l) << 3) + (i >> l);
         }
 
-        // Stage z (+ prolonged coarse correction) of one brick and its six face halos with one
-        // 16-byte interior load and one halo load per thread (256 threads), all independent.
-        template <class TC, bool kProlong>
-        __device__ inline void stage_tile(const BrickHead& m, const BrickMeta* __restrict__ gm, const double* __restrict__ z,
-                                          const TC* __restrict__ e, double* tile)
-        {
-            const int t = threadIdx.x;
-            const int l = m.level;
-            {
-                const int c = 2 * t, i = c & 7, j = (c >> 3) & 7, k = c >> 6;
-                double2 value = *reinterpret_cast<const double2*>(z + int64_t(m.slot) * kC3 + c);
-                if (kProlong)
-                {
-                    value.x += double(e[base_cell_of(m.base, l, i, j, k)]);
-                    value.y += double(e[base_cell_of(m.base, l, i + 1, j, k)]);
-                }
-                *reinterpret_cast<double2*>(tile + tix(i, j, k)) = value;
-            }
-            if (t < 128)
-            {
-                // -y, +y, -z, +z faces as pairs along x
-                const int face = 2 + (t >> 5), w = t & 31;
-                int i, j, k, hj, hk;
-                if (face < 4) { k = w >> 2; i = (w & 3) * 2; j = face == 2 ? kBS - 1 : 0; hj = face == 2 ? -1 : kBS; hk = k; }
-                else { i = (w * 2) & 7; j = (w * 2) >> 3; k = face == 4 ? kBS - 1 : 0; hj = j; hk = face == 4 ? -1 : kBS; }
-                const int n = gm->nbr[face];
-                double2 value = make_double2(0.0, 0.0);
-                if (n >= 0)
-                {
-                    value = *reinterpret_cast<const double2*>(z + int64_t(n) * kC3 + (k * kBS + j) * kBS + i);
-                    if (kProlong)
-                    {
-                        const int nb = gm->nbase[face];
-                        value.x += double(e[base_cell_of(nb, l, i, j, k)]);
-                        value.y += double(e[base_cell_of(nb, l, i + 1, j, k)]);
-                    }
-                }
-                *reinterpret_cast<double2*>(tile + tix(i, hj, hk)) = value;
-            }
-            else
-            {
-                // -x, +x faces, one value each
-                const int u = t - 128, face = u >> 6, j = u & 7, k = (u >> 3) & 7;
-                const int i = face == 0 ? kBS - 1 : 0, hi = face == 0 ? -1 : kBS;
-                const int n = gm->nbr[face];
-                double value = 0.0;
-                if (n >= 0)
-                {
-                    value = z[int64_t(n) * kC3 + (k * kBS + j) * kBS + i];
-                    if (kProlong) value += double(e[base_cell_of(gm->nbase[face], l, i, j, k)]);
-                }
-                tile[tix(hi, j, k)] = value;
-            }
-        }
-
         // Structured 7-point row of cell s of the tile (order -x,+x,-y,+y,-z,+z, then outlet),
         // and the matching diagonal; identical arithmetic to the unfused operator kernel.
         __device__ inline void structured_row(const double* tile, int s, uint8_t code, double h, double& Az, double& D)
@@ -132,104 +73,182 @@ namespace pcfd
             if (code & kOutlet) { Az += 2.0 * h * pa; D += 2.0 * h; }
         }
 
-        // The scalar fields of the CTA's brick (every thread reads the same 16 bytes); neighbour
-        // fields are read from global memory where they are used.
-        __device__ inline BrickHead load_head(const BrickView& v)
+        // ---- persistent, double-buffered variant -------------------------------------------
+        // Each CTA walks bricks b, b + G, ... and stages brick n+1 (tile + halos, r, codes) with
+        // cp.async into the second shared buffer while it computes brick n, so every SM keeps two
+        // bricks' loads in flight per CTA; the metadata of brick n+2 is fetched during brick n.
+        __device__ inline unsigned smem_addr(const void* p) { return static_cast<unsigned>(__cvta_generic_to_shared(p)); }
+        __device__ inline void copy16(void* dst, const void* src, bool valid)
         {
-            const int4 h = *reinterpret_cast<const int4*>(v.meta + blockIdx.x);
-            return BrickHead{h.x, h.y, h.z, h.w};
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_addr(dst)), "l"(src), "r"(valid ? 16 : 0));
+        }
+        __device__ inline void copy8(void* dst, const void* src, bool valid)
+        {
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(smem_addr(dst)), "l"(src), "r"(valid ? 8 : 0));
+        }
+        __device__ inline void copy_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+        template <int N> __device__ inline void copy_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+        // What one thread needs of a brick: the head and the neighbour of the halo face it copies.
+        struct Ticket
+        {
+            int slot, level, base, partial, nbr, nbase;
+        };
+        __device__ inline int halo_face(int t) { return t < 128 ? 2 + (t >> 5) : ((t - 128) >> 6); }
+        __device__ inline Ticket load_ticket(const BrickMeta* meta, int64_t b)
+        {
+            const BrickMeta* m = meta + b;
+            const int4 h = *reinterpret_cast<const int4*>(m);
+            const int face = halo_face(threadIdx.x);
+            return Ticket{h.x, h.y, h.z, h.w, m->nbr[face], m->nbase[face]};
         }
 
-        // kMode 0: sweep (out = z_new; deferred rows store A_struct z in t)
-        //       1: residual restriction (partials; deferred rows store A_struct z in t)
-        // Thread t owns cells 2t and 2t+1 (same x row).
+        template <bool kWithR>
+        __device__ inline void issue_brick(const Ticket& k, const double* __restrict__ z, const double* __restrict__ r,
+                                           const uint8_t* __restrict__ code, double* tile, double* rbuf, uint8_t* cbuf)
+        {
+            const int t = threadIdx.x;
+            const int64_t base = int64_t(k.slot) * kC3;
+            {
+                const int c = 2 * t, i = c & 7, j = (c >> 3) & 7, kk = c >> 6;
+                copy16(tile + tix(i, j, kk), z + base + c, true);
+                if (kWithR) copy16(rbuf + c, r + base + c, true);
+            }
+            if (t < 32) copy16(cbuf + 16 * t, code + base + 16 * t, true);
+            const bool valid = k.nbr >= 0;
+            const int64_t nb = int64_t(valid ? k.nbr : k.slot) * kC3;   // any valid address when zero-filling
+            if (t < 128)
+            {
+                const int face = 2 + (t >> 5), w = t & 31;
+                int i, j, kk, hj, hk;
+                if (face < 4) { kk = w >> 2; i = (w & 3) * 2; j = face == 2 ? kBS - 1 : 0; hj = face == 2 ? -1 : kBS; hk = kk; }
+                else { i = (w * 2) & 7; j = (w * 2) >> 3; kk = face == 4 ? kBS - 1 : 0; hj = j; hk = face == 4 ? -1 : kBS; }
+                copy16(tile + tix(i, hj, hk), z + nb + (kk * kBS + j) * kBS + i, valid);
+            }
+            else
+            {
+                const int u = t - 128, face = u >> 6, j = u & 7, kk = (u >> 3) & 7;
+                const int i = face == 0 ? kBS - 1 : 0, hi = face == 0 ? -1 : kBS;
+                copy8(tile + tix(hi, j, kk), z + nb + (kk * kBS + j) * kBS + i, valid);
+            }
+        }
+
+        // adds the coarse correction to the tile entries this thread copied
+        template <class TC>
+        __device__ inline void prolong_own(const Ticket& k, const TC* __restrict__ e, double* tile)
+        {
+            const int t = threadIdx.x, l = k.level;
+            {
+                const int c = 2 * t, i = c & 7, j = (c >> 3) & 7, kk = c >> 6;
+                tile[tix(i, j, kk)] += double(e[base_cell_of(k.base, l, i, j, kk)]);
+                tile[tix(i + 1, j, kk)] += double(e[base_cell_of(k.base, l, i + 1, j, kk)]);
+            }
+            if (k.nbr < 0) return;
+            if (t < 128)
+            {
+                const int face = 2 + (t >> 5), w = t & 31;
+                int i, j, kk, hj, hk;
+                if (face < 4) { kk = w >> 2; i = (w & 3) * 2; j = face == 2 ? kBS - 1 : 0; hj = face == 2 ? -1 : kBS; hk = kk; }
+                else { i = (w * 2) & 7; j = (w * 2) >> 3; kk = face == 4 ? kBS - 1 : 0; hj = j; hk = face == 4 ? -1 : kBS; }
+                tile[tix(i, hj, hk)] += double(e[base_cell_of(k.nbase, l, i, j, kk)]);
+                tile[tix(i + 1, hj, hk)] += double(e[base_cell_of(k.nbase, l, i + 1, j, kk)]);
+            }
+            else
+            {
+                const int u = t - 128, face = u >> 6, j = u & 7, kk = (u >> 3) & 7;
+                const int i = face == 0 ? kBS - 1 : 0, hi = face == 0 ? -1 : kBS;
+                tile[tix(hi, j, kk)] += double(e[base_cell_of(k.nbase, l, i, j, kk)]);
+            }
+        }
+
+        // kMode 0: Jacobi sweep, 1: residual restriction, 2: structured apply (out = A_struct z)
         template <int kMode, class TC, bool kProlong>
-        __global__ void __launch_bounds__(256) brick_fine_kernel(BrickView v, const double* __restrict__ z, const double* __restrict__ r,
-            double* __restrict__ out, double* __restrict__ t, const TC* __restrict__ e, double* __restrict__ partial, double omega)
+        __global__ void __launch_bounds__(256) brick_pipe_kernel(BrickView v, int64_t bricks, const double* __restrict__ z,
+            const double* __restrict__ r, double* __restrict__ out, double* __restrict__ t, const TC* __restrict__ e,
+            double* __restrict__ partial, double omega)
         {
-            __shared__ __align__(16) double tile[kTileSize];
-            __shared__ double residual[kC3];
-            const BrickHead m = load_head(v);
-            const BrickMeta* gm = v.meta + blockIdx.x;
-            const int64_t base = int64_t(m.slot) * kC3;
-            const int c0 = 2 * threadIdx.x;
-            const uchar2 codes = *reinterpret_cast<const uchar2*>(v.code + base + c0);
-            const double2 rr = *reinterpret_cast<const double2*>(r + base + c0);
-            stage_tile<TC, kProlong>(m, gm, z, e, tile);
-            __syncthreads();
-            const int l = m.level;
-            const double h = v.level_h[l];
-            double result[2];
-#pragma unroll
-            for (int q = 0; q < 2; ++q)
+            constexpr bool kWithR = kMode != 2;
+            __shared__ __align__(16) double tile[2][kTileSize];
+            __shared__ __align__(16) double rbuf[kWithR ? 2 : 1][kC3];
+            __shared__ __align__(16) uint8_t cbuf[2][kC3];
+            __shared__ double residual[kMode == 1 ? kC3 : 1];
+            int64_t b = blockIdx.x;
+            if (b >= bricks) return;
+            const int64_t G = gridDim.x;
+            Ticket cur = load_ticket(v.meta, b);
+            issue_brick<kWithR>(cur, z, r, v.code, tile[0], rbuf[0], cbuf[0]);
+            copy_commit();
+            Ticket next = b + G < bricks ? load_ticket(v.meta, b + G) : cur;
+            for (int it = 0;; ++it)
             {
-                const int c = c0 + q, i = c & 7, j = (c >> 3) & 7, k = c >> 6;
-                const int s = tix(i, j, k);
-                const uint8_t code = q ? codes.y : codes.x;
-                const double rc = q ? rr.y : rr.x;
-                double Az, D;
-                structured_row(tile, s, code, h, Az, D);
-                if (code & kDeferred) t[base + c] = Az;
-                if (kMode == 0) result[q] = code ? tile[s] + omega * (rc - Az) / D : 0.0;
-                else
+                const int st = it & 1;
+                const bool has_next = b + G < bricks;
+                Ticket after = next;
+                if (has_next)
                 {
-                    // level-0 cell ordering inside the brick: cells of one aggregate are contiguous
-                    const int n = l >= 3 ? 1 : (kBS >> l);
-                    const int group = l >= 3 ? 0 : ((k >> l) * n + (j >> l)) * n + (i >> l);
-                    const int size = l >= 3 ? kC3 : (1 << (3 * l));
-                    const int mask = (1 << l) - 1;
-                    const int within = l >= 3 ? c : ((((k & mask) << l) + (j & mask)) << l) + (i & mask);
-                    residual[group * size + within] = (code && !(code & kDeferred)) ? rc - Az : 0.0;
+                    issue_brick<kWithR>(next, z, r, v.code, tile[st ^ 1], rbuf[kWithR ? (st ^ 1) : 0], cbuf[st ^ 1]);
+                    copy_commit();
+                    if (b + 2 * G < bricks) after = load_ticket(v.meta, b + 2 * G);
+                    copy_wait<1>();
                 }
-            }
-            if (kMode == 0)
-            {
-                // deferred rows are written by the finish kernel; keep their slots untouched
-                if (!(codes.x & kDeferred) && !(codes.y & kDeferred))
-                    *reinterpret_cast<double2*>(out + base + c0) = make_double2(result[0], result[1]);
-                else
-                {
-                    if (!(codes.x & kDeferred)) out[base + c0] = result[0];
-                    if (!(codes.y & kDeferred)) out[base + c0 + 1] = result[1];
-                }
-            }
-            if (kMode == 1)
-            {
-                // deterministic pairwise tree inside each aggregate group
-                const int size = l >= 3 ? kC3 : (1 << (3 * l));
-                const int groups = kC3 / size;
+                else copy_wait<0>();
+                if (kProlong) prolong_own<TC>(cur, e, tile[st]);
                 __syncthreads();
-                for (int stride = size >> 1; stride > 0; stride >>= 1)
+                // ---- compute brick `cur` from buffer st.  Thread t owns cells t and t + 256, so a
+                // warp reads consecutive doubles of the tile (no shared-memory bank replays).
+                const double* T = tile[st];
+                const int l = cur.level;
+                const double h = v.level_h[l];
+                const int64_t base = int64_t(cur.slot) * kC3;
+                const int n = l >= 3 ? 1 : (kBS >> l);
+                const int size = l >= 3 ? kC3 : (1 << (3 * l));
+                const int mask = (1 << l) - 1;
+#pragma unroll
+                for (int q = 0; q < 2; ++q)
                 {
-                    for (int w = threadIdx.x; w < groups * stride; w += 256)
+                    const int c = threadIdx.x + 256 * q, i = c & 7, j = (c >> 3) & 7, k = c >> 6;
+                    const int s = tix(i, j, k);
+                    const uint8_t code = cbuf[st][c];
+                    double Az, D;
+                    structured_row(T, s, code, h, Az, D);
+                    if (kMode == 2) out[base + c] = Az;
+                    else
                     {
-                        const int g = w / stride, p = w % stride;
-                        residual[g * size + p] += residual[g * size + p + stride];
+                        const double rc = rbuf[st][c];
+                        if (code & kDeferred) t[base + c] = Az;
+                        if (kMode == 0)
+                        {
+                            if (!(code & kDeferred)) out[base + c] = code ? T[s] + omega * (rc - Az) / D : 0.0;
+                        }
+                        else
+                        {
+                            const int group = l >= 3 ? 0 : ((k >> l) * n + (j >> l)) * n + (i >> l);
+                            const int within = l >= 3 ? c : ((((k & mask) << l) + (j & mask)) << l) + (i & mask);
+                            residual[group * size + within] = (code && !(code & kDeferred)) ? rc - Az : 0.0;
+                        }
                     }
-                    __syncthreads();
                 }
-                for (int g = threadIdx.x; g < groups; g += 256) partial[m.partial + g] = residual[g * size];
+                if (kMode == 1)
+                {
+                    const int groups = kC3 / size;
+                    __syncthreads();
+                    for (int stride = size >> 1; stride > 0; stride >>= 1)
+                    {
+                        for (int w = threadIdx.x; w < groups * stride; w += 256)
+                        {
+                            const int g = w / stride, p = w % stride;
+                            residual[g * size + p] += residual[g * size + p + stride];
+                        }
+                        __syncthreads();
+                    }
+                    for (int g = threadIdx.x; g < groups; g += 256) partial[cur.partial + g] = residual[g * size];
+                }
+                __syncthreads();   // buffer st and the residual scratch are refilled next
+                if (!has_next) break;
+                b += G;
+                cur = next;
+                next = after;
             }
-        }
-
-        // out = A_struct p over every cell of the active bricks (inactive cells 0); the compact
-        // edges, gauges and the WLS correction are added by the operator's other kernels.
-        __global__ void __launch_bounds__(256) brick_apply_kernel(BrickView v, const double* __restrict__ p, double* __restrict__ out)
-        {
-            __shared__ __align__(16) double tile[kTileSize];
-            const BrickHead m = load_head(v);
-            const BrickMeta* gm = v.meta + blockIdx.x;
-            const int64_t base = int64_t(m.slot) * kC3;
-            const int c0 = 2 * threadIdx.x;
-            const uchar2 codes = *reinterpret_cast<const uchar2*>(v.code + base + c0);
-            stage_tile<double, false>(m, gm, p, nullptr, tile);
-            __syncthreads();
-            const double h = v.level_h[m.level];
-            double Az[2], D;
-            const int i = c0 & 7, j = (c0 >> 3) & 7, k = c0 >> 6;
-            structured_row(tile, tix(i, j, k), codes.x, h, Az[0], D);
-            structured_row(tile, tix(i + 1, j, k), codes.y, h, Az[1], D);
-            *reinterpret_cast<double2*>(out + base + c0) = make_double2(Az[0], Az[1]);
         }
 
         // z = w r / D for every DOF (first sweep from zero); deferred rows read the assembled D.
@@ -536,19 +555,40 @@ namespace pcfd
                 f.t, out, f.deferred_residual, 2.0 / 3.0);
         }
 
+        int pipe_grid(const System& s)
+        {
+            static int sms = 0;
+            if (!sms)
+            {
+                int device = 0;
+                cuda_check(cudaGetDevice(&device), "device");
+                cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
+            }
+            return std::max(1, std::min(s.active_bricks, 4 * sms));
+        }
+
         template <class TC, bool kProlong>
         void sweep(System& s, const double* z, const double* r, double* out, const TC* e)
         {
             FineSmoother& f = s.fine;
-            brick_fine_kernel<0, TC, kProlong><<<s.active_bricks, 256, 0, launch_stream(s)>>>(
-                view(s), z, r, out, f.t, e, nullptr, 2.0 / 3.0);
+            brick_pipe_kernel<0, TC, kProlong><<<pipe_grid(s), 256, 0, launch_stream(s)>>>(
+                view(s), s.active_bricks, z, r, out, f.t, e, nullptr, 2.0 / 3.0);
             finish<0, TC, kProlong>(s, z, r, out, e);
+        }
+
+        template <class TC>
+        void restrict_residual(System& s, const double* z, const double* r)
+        {
+            FineSmoother& f = s.fine;
+            brick_pipe_kernel<1, TC, false><<<pipe_grid(s), 256, 0, launch_stream(s)>>>(
+                view(s), s.active_bricks, z, r, nullptr, f.t, nullptr, f.partial, 2.0 / 3.0);
         }
     }
 
     void brick_apply(System& s, const double* p, double* out)
     {
-        brick_apply_kernel<<<s.active_bricks, 256, 0, launch_stream(s)>>>(view(s), p, out);
+        brick_pipe_kernel<2, double, false><<<pipe_grid(s), 256, 0, launch_stream(s)>>>(
+            view(s), s.active_bricks, p, nullptr, out, nullptr, nullptr, nullptr, 0.0);
     }
 
     template <class TC>
@@ -561,8 +601,7 @@ namespace pcfd
         sweep<TC, false>(s, a, r, z, nullptr);
         MgLevel<TC>& base = levels.front();
         cuda_check(cudaMemsetAsync(base.x, 0, size_t(base.cells) * sizeof(TC), s.stream), "clear base correction");
-        brick_fine_kernel<1, TC, false><<<s.active_bricks, 256, 0, launch_stream(s)>>>(
-            view(s), z, r, nullptr, f.t, nullptr, f.partial, 2.0 / 3.0);
+        restrict_residual<TC>(s, z, r);
         finish<1, TC, false>(s, z, r, nullptr, nullptr);
         gather_base_kernel<TC><<<blocks_for(base.cells), kThreads, 0, launch_stream(s)>>>(base.cells, f.gather_offset, f.gather_entry,
                                                                                          f.partial, f.deferred_residual, base.rhs);
@@ -589,8 +628,7 @@ namespace pcfd
         }
         else if (stage == 1)
         {
-            brick_fine_kernel<1, double, false><<<s.active_bricks, 256, 0, launch_stream(s)>>>(
-                view(s), z, r, nullptr, f.t, nullptr, f.partial, 2.0 / 3.0);
+            restrict_residual<double>(s, z, r);
             finish<1, double, false>(s, z, r, nullptr, nullptr);
             gather_base_kernel<double><<<blocks_for(base.cells), kThreads, 0, launch_stream(s)>>>(
                 base.cells, f.gather_offset, f.gather_entry, f.partial, f.deferred_residual, base.rhs);

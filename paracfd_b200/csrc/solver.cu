@@ -571,7 +571,7 @@ namespace pcfd
                 cuda_check(cudaStreamSynchronize(s.stream), "coefficient synchronize");
             };
             auto recycle_set = [&](double* base) {
-                VecSet set;
+                VecSet set{int64_t(ld)};
                 for (int c = 0; c < s.recycle_count; ++c) set.push(base + size_t(c) * ld);
                 return set;
             };
@@ -635,6 +635,7 @@ namespace pcfd
                 if (!(beta > 0) || !std::isfinite(beta) || !std::isfinite(1.0 / beta)) break;
                 const int cycle = std::min(R, max_iterations - result.iterations);
                 std::vector<double> H(size_t(cycle + 1) * cycle, 0.0), cs(cycle), sn(cycle), g(cycle + 1, 0.0), y(cycle);
+                std::vector<double> zc_recycle(size_t(cycle) * System::recycle_capacity, 0.0);   // deferred U coefficients
                 g[0] = beta;
                 vec_scaled_copy_active(s, s.gmres_v, s.defect, 1.0 / beta);
                 int used = 0;
@@ -645,13 +646,16 @@ namespace pcfd
                     apply_preconditioner(s, v, zc);
                     ++result.preconditioner_applications;
                     launch_apply(s, zc, s.Ad, false);
-                    // CGS2 against [C | V_0..V_col]; the U part of each coefficient block also updates z
+                    // CGS2 against [C | V_0..V_col].  The matching z -= U h_C update is deferred: its
+                    // coefficients are kept per column and applied once when the cycle's
+                    // correction is formed (z only enters the solution through Z y).
                     const int k = s.recycle_count, m = k + col + 1;
-                    VecSet Q = recycle_set(s.recycle_c.p), Uset = recycle_set(s.recycle_u.p);
+                    VecSet Q = recycle_set(s.recycle_c.p);
+                    const VecSet none{int64_t(ld)};
                     for (int row = 0; row <= col; ++row) Q.push(s.gmres_v.p + size_t(row) * ld);
                     block_dot(s, Q, s.Ad, h1);
-                    block_update(s, Q, h1, s.Ad, Uset, -1.0, zc, 2, h2);
-                    block_update(s, Q, h2, s.Ad, Uset, -1.0, zc, 1, h3);
+                    block_update(s, Q, h1, s.Ad, none, -1.0, nullptr, 2, h2);
+                    block_update(s, Q, h2, s.Ad, none, -1.0, nullptr, 1, h3);
                     scale_by_inverse_norm(s, s.gmres_v.p + size_t(col + 1) * ld, s.Ad, h3);
                     read_block(3);
                     bool column_valid = true;
@@ -662,6 +666,7 @@ namespace pcfd
                     const double scale = std::sqrt(std::max(0.0, host_h1[m] - c_part));
                     if (!(scale > 0) || !std::isfinite(scale)) break;
                     for (int row = 0; row <= col; ++row) H[size_t(row) * cycle + col] = host_h1[k + row] + host_h2[k + row];
+                    for (int c = 0; c < k; ++c) zc_recycle[size_t(col) * System::recycle_capacity + c] = host_h1[c] + host_h2[c];
                     double next_norm = std::sqrt(std::max(0.0, host_h3[0]));
                     const double floor = 64 * std::numeric_limits<double>::epsilon() * scale;
                     if (!(next_norm > floor && std::isfinite(1.0 / next_norm))) next_norm = 0;
@@ -701,12 +706,20 @@ namespace pcfd
                 }
                 if (used == 0) break;
                 {
-                    VecSet Z;
+                    // correction = sum_j y_j (z_j - U c_j) = Z y - U (sum_j y_j c_j)
+                    VecSet Z{int64_t(ld)};
                     Coefficients coefficient;
                     for (int col = 0; col < used; ++col)
                     {
                         Z.push(s.gmres_z.p + size_t(col) * ld);
                         coefficient.value[col] = y[col];
+                    }
+                    for (int c = 0; c < s.recycle_count; ++c)
+                    {
+                        double sum = 0.0;
+                        for (int col = 0; col < used; ++col) sum += y[col] * zc_recycle[size_t(col) * System::recycle_capacity + c];
+                        Z.push(ru(c));
+                        coefficient.value[used + c] = -sum;
                     }
                     block_combine(s, Z, coefficient, s.correction, false);
                 }

@@ -3,8 +3,9 @@
 ``paraglider16m`` is the 4-level ~16 M leaf-cell paraglider case: elliptic planform, span 10 m,
 root chord 2.5 m, anhedral arc radius 6 m, NACA 4415, AoA 8 deg, surface points jittered by at
 most 1e-4 chord (seeded), freestream 11 m/s.  The outer surface is closed, so the 2 mm internal
-ribs of an inflated wing lie inside the solid and do not enter the flow grid.  ``paraglider1m``
-is the same wing on a coarser base grid (3 levels) for quick checks.
+ribs of an inflated wing lie inside the solid and do not enter the flow grid.  ``paraglider5m``
+(3 levels, 5.1 M cells) and ``paraglider1m`` (coarser base grid, 1.1 M cells) are the same wing
+on smaller grids for profiling captures and quick checks.
 """
 from __future__ import annotations
 
@@ -46,6 +47,7 @@ class Workload:
 
 WORKLOADS = {
     "paraglider16m": Workload("paraglider16m", (-5.0, -7.5, -8.5), (15.0, 7.5, 6.5), 0.125, 4),
+    "paraglider5m": Workload("paraglider5m", (-5.0, -7.5, -8.5), (15.0, 7.5, 6.5), 0.125, 3),
     "paraglider1m": Workload("paraglider1m", (-5.0, -7.5, -8.5), (15.0, 7.5, 6.5), 0.25, 3,
                              wing_refinement_distance=0.5, surface_refinement_distance=0.5),
 }
