@@ -190,14 +190,17 @@ def inflow_profile(speed: float, centres, step: int) -> np.ndarray:
 
 
 def ncu_traffic(workload: str) -> float | None:
-    """DRAM bytes per structured-operator launch from the committed ncu summary, if present."""
-    path = os.path.join(ROOT, "profiles", "structured_apply_traffic.json")
+    """DRAM bytes (read + write) per launch of the structured operator kernel, from the committed
+    ncu summary ``profiles/brick_apply_<workload>.md`` (line ``bytes_per_launch: N``), if present."""
+    path = os.path.join(ROOT, "profiles", f"brick_apply_{workload}.md")
     try:
         with open(path) as f:
-            data = json.load(f)
-        return float(data[workload]["bytes_per_launch"])
-    except (OSError, KeyError, ValueError):
-        return None
+            for line in f:
+                if line.strip().startswith("bytes_per_launch:"):
+                    return float(line.split(":", 1)[1].strip().split()[0])
+    except (OSError, ValueError):
+        pass
+    return None
 
 
 # ------------------------------------------------------------------------------------------ CPU sample
@@ -347,7 +350,7 @@ def run_ours(args, ranks: Ranks):
     n = ranks.world
     value = n * args.steps / (elapsed_ms * 1e-3)
     peak, peak_kind = measured_peak_gbs()
-    region_names = {0: "structured_apply8_kernel (FP64 7-point operator)", 1: "MG preconditioner application"}
+    region_names = {0: "brick_pipe_kernel<2> (FP64 structured 7-point operator)", 1: "MG preconditioner application"}
     roofline = None
     region_ms = round(float(np.mean(per_launch)), 4) if len(per_launch) else None
     if len(per_launch) and args.profile_region == 0:
@@ -375,6 +378,7 @@ def run_ours(args, ranks: Ranks):
         "e2e": {"value": round(n * args.steps / e2e_s, 4), "unit": "steps/s", "h2d_bytes_per_step": 4 * faces,
                 "d2h_bytes_per_step": 12 * 8},
         "gpu_launches": int(launches),
+        "launches_before_timed": int(launches0),
         "component_ms": kernel_ms,
         "roofline": roofline,
         "profiled_region": {"region": region_names.get(args.profile_region), "launches": int(len(per_launch)),

@@ -122,6 +122,7 @@ namespace pcfd
         DBuf<double> partial, deferred_residual;
         DBuf<int> gather_offset, gather_entry;  // base cell -> partials (>= 0) / deferred rows (< 0)
         DBuf<double> t, z;                      // [S] deferred structured rows, ping-pong iterate
+        DBuf<double> damping;                   // [levels][14] w / D of non-deferred rows
     };
 
     // Up to kMaxSet vectors of one system, passed by value to the fused block kernels (krylov.cu):

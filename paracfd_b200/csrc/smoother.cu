@@ -14,8 +14,9 @@
 // EB fragments, a diagonal that the code bits do not reproduce bit for bit -- and a small
 // per-DOF "finish" kernel completes them with the reference's irregular gather in the same
 // summation order.  Non-deferred rows use D = sum of h over the open faces (+ 2h outlet), which
-// equals the assembled diagonal bit for bit (checked at setup), so every sweep produces the
-// same bits as the unfused kernels; only the restriction sums in a different order.
+// equals the assembled diagonal bit for bit (checked at setup); their update is computed as
+// z + (r - Az) * (w / D) with w / D from a per-level table instead of a division, and the
+// restriction sums in a different (fixed) order -- the only departures from the unfused cycle.
 #include "pcfd_internal.h"
 
 #include <algorithm>
@@ -57,21 +58,26 @@ namespace pcfd
             return b0 + ((k >> l) << 6) + ((j >> l) << 3) + (i >> l);
         }
 
-        // Structured 7-point row of cell s of the tile (order -x,+x,-y,+y,-z,+z, then outlet),
-        // and the matching diagonal; identical arithmetic to the unfused operator kernel.
-        __device__ inline void structured_row(const double* tile, int s, uint8_t code, double h, double& Az, double& D)
+        // Structured 7-point row of cell s of the tile (order -x,+x,-y,+y,-z,+z, then outlet);
+        // identical arithmetic to the unfused operator kernel.
+        __device__ inline double structured_row(const double* tile, int s, uint8_t code, double h)
         {
             const double pa = tile[s];
-            Az = 0.0;
-            D = 0.0;
-            if (code & 1) { Az += h * (pa - tile[s - 1]); D += h; }
-            if (code & 2) { Az += h * (pa - tile[s + 1]); D += h; }
-            if (code & 4) { Az += h * (pa - tile[s - kP1]); D += h; }
-            if (code & 8) { Az += h * (pa - tile[s + kP1]); D += h; }
-            if (code & 16) { Az += h * (pa - tile[s - kP2]); D += h; }
-            if (code & 32) { Az += h * (pa - tile[s + kP2]); D += h; }
-            if (code & kOutlet) { Az += 2.0 * h * pa; D += 2.0 * h; }
+            double Az = 0.0;
+            if (code & 1) Az += h * (pa - tile[s - 1]);
+            if (code & 2) Az += h * (pa - tile[s + 1]);
+            if (code & 4) Az += h * (pa - tile[s - kP1]);
+            if (code & 8) Az += h * (pa - tile[s + kP1]);
+            if (code & 16) Az += h * (pa - tile[s - kP2]);
+            if (code & 32) Az += h * (pa - tile[s + kP2]);
+            if (code & kOutlet) Az += 2.0 * h * pa;
+            return Az;
         }
+
+        // Damping over the diagonal, w / D, of a non-deferred row: D is h per open face plus 2h
+        // for the outlet, so it is looked up by (open-face count, outlet) per level.
+        constexpr int kDiagonalKinds = 14;
+        __device__ inline int diagonal_kind(uint8_t code) { return __popc(code & kOpenMask) + 7 * ((code >> 6) & 1); }
 
         // ---- persistent, double-buffered variant -------------------------------------------
         // Each CTA walks bricks b, b + G, ... and stages brick n+1 (tile + halos, r, codes) with
@@ -165,7 +171,7 @@ namespace pcfd
         template <int kMode, class TC, bool kProlong>
         __global__ void __launch_bounds__(256) brick_pipe_kernel(BrickView v, int64_t bricks, const double* __restrict__ z,
             const double* __restrict__ r, double* __restrict__ out, double* __restrict__ t, const TC* __restrict__ e,
-            double* __restrict__ partial, double omega)
+            double* __restrict__ partial, const double* __restrict__ damping)
         {
             constexpr bool kWithR = kMode != 2;
             __shared__ __align__(16) double tile[2][kTileSize];
@@ -209,8 +215,7 @@ namespace pcfd
                     const int c = threadIdx.x + 256 * q, i = c & 7, j = (c >> 3) & 7, k = c >> 6;
                     const int s = tix(i, j, k);
                     const uint8_t code = cbuf[st][c];
-                    double Az, D;
-                    structured_row(T, s, code, h, Az, D);
+                    const double Az = structured_row(T, s, code, h);
                     if (kMode == 2) out[base + c] = Az;
                     else
                     {
@@ -218,7 +223,8 @@ namespace pcfd
                         if (code & kDeferred) t[base + c] = Az;
                         if (kMode == 0)
                         {
-                            if (!(code & kDeferred)) out[base + c] = code ? T[s] + omega * (rc - Az) / D : 0.0;
+                            if (!(code & kDeferred))
+                                out[base + c] = code ? T[s] + (rc - Az) * damping[l * kDiagonalKinds + diagonal_kind(code)] : 0.0;
                         }
                         else
                         {
@@ -230,18 +236,38 @@ namespace pcfd
                 }
                 if (kMode == 1)
                 {
-                    const int groups = kC3 / size;
+                    // fixed-order reduction of each aggregate group (groups are contiguous runs of
+                    // `size` entries): pair sums, then shuffles inside the group, then warps
                     __syncthreads();
-                    for (int stride = size >> 1; stride > 0; stride >>= 1)
+                    const int tt = threadIdx.x;
+                    if (size == 1)
                     {
-                        for (int w = threadIdx.x; w < groups * stride; w += 256)
-                        {
-                            const int g = w / stride, p = w % stride;
-                            residual[g * size + p] += residual[g * size + p + stride];
-                        }
-                        __syncthreads();
+                        partial[cur.partial + 2 * tt] = residual[2 * tt];
+                        partial[cur.partial + 2 * tt + 1] = residual[2 * tt + 1];
                     }
-                    for (int g = threadIdx.x; g < groups; g += 256) partial[cur.partial + g] = residual[g * size];
+                    else
+                    {
+                        double v = residual[2 * tt] + residual[2 * tt + 1];
+                        const int pairs = size >> 1;                         // pairs per group: 4, 32 or 256
+                        const int width = pairs < 32 ? pairs : 32;
+                        for (int o = width >> 1; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o, width);
+                        if (pairs <= 32)
+                        {
+                            if ((tt & (width - 1)) == 0) partial[cur.partial + tt / pairs] = v;
+                        }
+                        else
+                        {
+                            __syncthreads();                              // every pair read first
+                            if ((tt & 31) == 0) residual[tt >> 5] = v;
+                            __syncthreads();
+                            if (tt == 0)
+                            {
+                                double total = 0.0;
+                                for (int w = 0; w < 8; ++w) total += residual[w];
+                                partial[cur.partial] = total;
+                            }
+                        }
+                    }
                 }
                 __syncthreads();   // buffer st and the residual scratch are refilled next
                 if (!has_next) break;
@@ -253,24 +279,19 @@ namespace pcfd
 
         // z = w r / D for every DOF (first sweep from zero); deferred rows read the assembled D.
         __global__ void first_sweep_kernel(const uint8_t* __restrict__ code, const int* __restrict__ brick_level,
-                                           const double* __restrict__ level_h, const double* __restrict__ diag,
+                                           const double* __restrict__ damping, const double* __restrict__ diag,
                                            const uint8_t* __restrict__ active, const double* __restrict__ r,
                                            double* __restrict__ z, int64_t structured, int64_t n, double omega)
         {
             const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
             if (q >= n) return;
             const uint8_t c = code[q];
-            double D;
-            if (q >= structured || (c & kDeferred)) D = active[q] ? diag[q] : 0.0;
-            else
+            if (q >= structured || (c & kDeferred))
             {
-                const double h = level_h[brick_level[q >> 9]];
-                D = 0.0;
-                for (int f = 0; f < 6; ++f)
-                    if (c & (1 << f)) D += h;
-                if (c & kOutlet) D += 2.0 * h;
+                const double D = active[q] ? diag[q] : 0.0;
+                z[q] = D > 0.0 ? omega * r[q] / D : 0.0;
             }
-            z[q] = D > 0.0 ? omega * r[q] / D : 0.0;
+            else z[q] = c ? r[q] * damping[brick_level[q >> 9] * kDiagonalKinds + diagonal_kind(c)] : 0.0;
         }
 
         // Completes deferred rows: A_orth z = t (structured part) + compact-edge gather + gauges,
@@ -492,6 +513,18 @@ namespace pcfd
             elist.insert(elist.end(), entries[c].begin(), entries[c].end());
             eoff[c + 1] = int(elist.size());
         }
+        // w / D per level and (open faces, outlet), D summed exactly as in the code-bit check
+        std::vector<double> damping(size_t(s.levels) * kDiagonalKinds, 0.0);
+        for (int l = 0; l < s.levels; ++l)
+            for (int outlet = 0; outlet < 2; ++outlet)
+                for (int faces = 0; faces <= 6; ++faces)
+                {
+                    double D = 0.0;
+                    for (int q = 0; q < faces; ++q) D += s.level_h[l];
+                    if (outlet) D += 2.0 * s.level_h[l];
+                    damping[size_t(l) * kDiagonalKinds + faces + 7 * outlet] = D > 0.0 ? (2.0 / 3.0) / D : 0.0;
+                }
+        f.damping.upload(damping);
         f.code.upload(code);
         f.deferred_count = int(ddof.size());
         f.deferred_dof.upload(ddof);
@@ -572,7 +605,7 @@ namespace pcfd
         {
             FineSmoother& f = s.fine;
             brick_pipe_kernel<0, TC, kProlong><<<pipe_grid(s), 256, 0, launch_stream(s)>>>(
-                view(s), s.active_bricks, z, r, out, f.t, e, nullptr, 2.0 / 3.0);
+                view(s), s.active_bricks, z, r, out, f.t, e, nullptr, f.damping);
             finish<0, TC, kProlong>(s, z, r, out, e);
         }
 
@@ -581,14 +614,14 @@ namespace pcfd
         {
             FineSmoother& f = s.fine;
             brick_pipe_kernel<1, TC, false><<<pipe_grid(s), 256, 0, launch_stream(s)>>>(
-                view(s), s.active_bricks, z, r, nullptr, f.t, nullptr, f.partial, 2.0 / 3.0);
+                view(s), s.active_bricks, z, r, nullptr, f.t, nullptr, f.partial, f.damping);
         }
     }
 
     void brick_apply(System& s, const double* p, double* out)
     {
         brick_pipe_kernel<2, double, false><<<pipe_grid(s), 256, 0, launch_stream(s)>>>(
-            view(s), s.active_bricks, p, nullptr, out, nullptr, nullptr, nullptr, 0.0);
+            view(s), s.active_bricks, p, nullptr, out, nullptr, nullptr, nullptr, nullptr);
     }
 
     template <class TC>
@@ -596,7 +629,7 @@ namespace pcfd
     {
         FineSmoother& f = s.fine;
         double* a = f.z.p;
-        first_sweep_kernel<<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(f.code, s.brick_level, s.d_level_h, s.diagonal,
+        first_sweep_kernel<<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(f.code, s.brick_level, f.damping, s.diagonal,
                                                                               s.active, r, a, s.structured, s.S, 2.0 / 3.0);
         sweep<TC, false>(s, a, r, z, nullptr);
         MgLevel<TC>& base = levels.front();
@@ -622,7 +655,7 @@ namespace pcfd
         double* a = f.z.p;
         if (stage == 0)
         {
-            first_sweep_kernel<<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(f.code, s.brick_level, s.d_level_h, s.diagonal,
+            first_sweep_kernel<<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(f.code, s.brick_level, f.damping, s.diagonal,
                                                                                   s.active, r, a, s.structured, s.S, 2.0 / 3.0);
             sweep<double, false>(s, a, r, z, nullptr);
         }
