@@ -48,6 +48,8 @@ def parse_args():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", default="paraglider16m")
     ap.add_argument("--mg", choices=("fp64", "fp32"), default="fp64", help="multigrid preconditioner precision")
+    ap.add_argument("--mg-cycle", choices=("reference", "corrected"), default="reference",
+                    help="coarse-correction weighting of the multigrid cycle (pcfd_mg_cycle)")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU sample of the ours arm")
     ap.add_argument("--no-reference-gpu", action="store_true", help="reference arm: skip the sm_100a reference run")
     ap.add_argument("--profile-region", type=int, default=0, help="PCFD_PROFILE_* region timed per launch")
@@ -281,7 +283,8 @@ def run_ours(args, ranks: Ranks):
     spec = WORKLOADS[args.workload]
     built = spec.build()
     bricks = non_covered_bricks(built.topology)
-    system = CompositeSystem(built.topology, MG_FP32 if args.mg == "fp32" else MG_FP64, device=ranks.local)
+    system = CompositeSystem(built.topology, MG_FP32 if args.mg == "fp32" else MG_FP64, device=ranks.local,
+                             mg_cycle=1 if args.mg_cycle == "corrected" else 0)
     system.configure(speed=spec.speed, **spec.case)
     slots = system.inflow_layout()
     faces = len(slots) * spec.brick_size ** 2
@@ -368,7 +371,7 @@ def run_ours(args, ranks: Ranks):
         "ms_per_step": round(elapsed_ms / args.steps, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 state / f64 pressure", "data": "synthetic analytic geometry",
         "config": dict(spec.describe(), leaf_cells=built.leaf_cells, storage=built.storage_size,
-                       mg=args.mg, parallelism=f"replicas{n}", l2="inputs larger than L2"),
+                       mg=args.mg, mg_cycle=args.mg_cycle, parallelism=f"replicas{n}", l2="inputs larger than L2"),
         "projection_ms": round(statistics.mean(s["projection_ms"] for s in stats), 3),
         "iterations_per_step": round(statistics.mean(s["pressure"]["iterations"] for s in stats), 2),
         "final_residual_max": max(s["pressure"]["relative_residual"] for s in stats),
@@ -413,7 +416,8 @@ def run_kernel_only(args):
     from paracfd_b200.workloads import WORKLOADS
     spec = WORKLOADS[args.workload]
     built = spec.build()
-    system = CompositeSystem(built.topology, MG_FP32 if args.mg == "fp32" else MG_FP64)
+    system = CompositeSystem(built.topology, MG_FP32 if args.mg == "fp32" else MG_FP64,
+                             mg_cycle=1 if args.mg_cycle == "corrected" else 0)
     ms = system.time_kernel(args.kernel_only, args.kernel_iterations)
     line = {"kernel_only": args.kernel_only, "workload": args.workload, "ms_per_launch": ms,
             "iterations": args.kernel_iterations, "launches": system.launch_count()}

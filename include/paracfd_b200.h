@@ -172,7 +172,21 @@ typedef struct pcfd_options {
     double momentum_min_volume_fraction; /* AmrConfig::min_volume_fraction (small-cell groups) */
     int32_t disable_fused_smoother;  /* 1: run the preconditioner's fine level as separate
                                         operator/vector launches (same sweeps, reference order) */
+    int32_t mg_cycle;                /* pcfd_mg_cycle */
 } pcfd_options;
+
+/* Coarse-correction weighting of the multigrid cycle.  The aggregation coarse operators are
+ * Galerkin products with piecewise-constant transfer, which over-weight the coarse problem (by 2
+ * per 2x2x2 coarsening of a uniform Laplacian, 8^l for the reference's direct aggregation of a
+ * level-l cell into its level-0 cell); the corrected cycle scales the prolonged corrections by 2
+ * (fine <- level-0 aggregates) and 1.5 (between lattice levels).  Same smoother, transfers and
+ * coarse matrices.  On the 2- and 3-level wing grids (1-5 M cells) it cuts the cold-start
+ * iterations to 1e-8 by 25-40 %; on the 4-level 16 M-cell grid it does not help, so the
+ * reference cycle stays the default. */
+typedef enum pcfd_mg_cycle {
+    PCFD_MG_CYCLE_REFERENCE = 0,     /* the reference's cycle (amr_pressure.cu:1103-1154) */
+    PCFD_MG_CYCLE_CORRECTED = 1      /* over-corrected prolongation */
+} pcfd_mg_cycle;
 
 /* AmrGpuSolveResult (amr_pressure.h:337-351), trimmed to what the solver reports. */
 typedef struct pcfd_solve_result {

@@ -17,6 +17,7 @@ from .capi import Options, SolveResult, Topology, check, ptr
 PROFILE_STRUCTURED_APPLY = 0
 PROFILE_PRECONDITIONER = 1
 MG_FP64, MG_FP32 = 0, 1
+MG_CYCLE_REFERENCE, MG_CYCLE_CORRECTED = 0, 1
 
 
 class BuiltTopology:
@@ -72,10 +73,11 @@ class CompositeSystem:
     """Resident topology + state on one GPU (one host thread at a time)."""
 
     def __init__(self, topology: Topology, mg_precision: int = MG_FP64, device: int = 0,
-                 momentum_min_volume_fraction: float = 0.0, fused_smoother: bool = True):
+                 momentum_min_volume_fraction: float = 0.0, fused_smoother: bool = True,
+                 mg_cycle: int = 0):
         self._lib = capi.load()
         self._topology = topology   # keep the caller's arrays alive during creation
-        opts = Options(mg_precision, device, None, momentum_min_volume_fraction, 0 if fused_smoother else 1)
+        opts = Options(mg_precision, device, None, momentum_min_volume_fraction, 0 if fused_smoother else 1, mg_cycle)
         handle = C.c_void_p()
         check(self._lib.pcfd_system_create(C.byref(topology), C.byref(opts), C.byref(handle)))
         self.handle = handle

@@ -199,6 +199,12 @@ namespace pcfd
             const std::vector<double> diag = host_diagonal(t);
             s.diagonal.upload(diag);
             build_operator(s, t);
+            if (options && options->mg_cycle == PCFD_MG_CYCLE_CORRECTED)
+            {
+                s.mg_prolong_scale = 2.0;
+                s.mg_lattice_scale = 1.5;
+            }
+            else require(!options || options->mg_cycle == PCFD_MG_CYCLE_REFERENCE, "unknown multigrid cycle");
             build_multigrid(s, t, diag);
             if (!options || !options->disable_fused_smoother) build_fine_smoother(s, t, diag);
             // Krylov storage
@@ -256,6 +262,8 @@ namespace pcfd
         for (cudaEvent_t& e : markers)
             if (e) cudaEventDestroy(e);
         for (cudaEvent_t e : profile_events) cudaEventDestroy(e);
+        if (mg_graph64) cudaGraphExecDestroy(mg_graph64);
+        if (mg_graph32) cudaGraphExecDestroy(mg_graph32);
         destroy_loads(*this);
         delete momentum;
         if (pinned) cudaFreeHost(pinned);

@@ -123,6 +123,7 @@ namespace pcfd
         DBuf<int> gather_offset, gather_entry;  // base cell -> partials (>= 0) / deferred rows (< 0)
         DBuf<double> t, z;                      // [S] deferred structured rows, ping-pong iterate
         DBuf<double> damping;                   // [levels][14] w / D of non-deferred rows
+        DBuf<float> damping32, z32, z32b, r32, t32;   // FP32 multigrid: float fine-level buffers
     };
 
     // Up to kMaxSet vectors of one system, passed by value to the fused block kernels (krylov.cu):
@@ -164,6 +165,7 @@ namespace pcfd
         int64_t faces = 0;   // per component
         bool outlet = true, full_nonorthogonal = false;
         int mg_precision = PCFD_MG_FP64;
+        double mg_prolong_scale = 1.0, mg_lattice_scale = 1.0;   // coarse-correction weights (pcfd_mg_cycle)
         cudaStream_t stream = nullptr;
         bool own_stream = false;
         int device = 0;
@@ -195,6 +197,8 @@ namespace pcfd
         std::vector<MgLevel<double>> mg64;
         std::vector<MgLevel<float>> mg32;
         FineSmoother fine;
+        cudaGraphExec_t mg_graph64 = nullptr, mg_graph32 = nullptr;   // captured aggregation hierarchy
+        int64_t mg_graph64_launches = 0, mg_graph32_launches = 0;
         DBuf<float> diagonal32;
 
         // Krylov vectors

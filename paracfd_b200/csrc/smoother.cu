@@ -21,6 +21,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 #include <unordered_map>
 
 namespace pcfd
@@ -45,6 +46,7 @@ namespace pcfd
             const BrickMeta* meta;
             const double* level_h;
             const uint8_t* code;
+            double prolong;            // scale of the prolonged coarse correction
         };
 
         // Shared tile of one brick plus its face halos: rows of 12 doubles so that interior rows
@@ -60,17 +62,18 @@ namespace pcfd
 
         // Structured 7-point row of cell s of the tile (order -x,+x,-y,+y,-z,+z, then outlet);
         // identical arithmetic to the unfused operator kernel.
-        __device__ inline double structured_row(const double* tile, int s, uint8_t code, double h)
+        template <class T>
+        __device__ inline T structured_row(const T* tile, int s, uint8_t code, T h)
         {
-            const double pa = tile[s];
-            double Az = 0.0;
+            const T pa = tile[s];
+            T Az = T(0);
             if (code & 1) Az += h * (pa - tile[s - 1]);
             if (code & 2) Az += h * (pa - tile[s + 1]);
             if (code & 4) Az += h * (pa - tile[s - kP1]);
             if (code & 8) Az += h * (pa - tile[s + kP1]);
             if (code & 16) Az += h * (pa - tile[s - kP2]);
             if (code & 32) Az += h * (pa - tile[s + kP2]);
-            if (code & kOutlet) Az += 2.0 * h * pa;
+            if (code & kOutlet) Az += T(2) * h * pa;
             return Az;
         }
 
@@ -92,6 +95,21 @@ namespace pcfd
         {
             asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(smem_addr(dst)), "l"(src), "r"(valid ? 8 : 0));
         }
+        __device__ inline void copy4(void* dst, const void* src, bool valid)
+        {
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(smem_addr(dst)), "l"(src), "r"(valid ? 4 : 0));
+        }
+        // two consecutive values / one value of the field type
+        template <class T> __device__ inline void copy_pair(void* dst, const void* src, bool valid)
+        {
+            if (sizeof(T) == 8) copy16(dst, src, valid);
+            else copy8(dst, src, valid);
+        }
+        template <class T> __device__ inline void copy_one(void* dst, const void* src, bool valid)
+        {
+            if (sizeof(T) == 8) copy8(dst, src, valid);
+            else copy4(dst, src, valid);
+        }
         __device__ inline void copy_commit() { asm volatile("cp.async.commit_group;\n" ::); }
         template <int N> __device__ inline void copy_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
@@ -109,16 +127,16 @@ namespace pcfd
             return Ticket{h.x, h.y, h.z, h.w, m->nbr[face], m->nbase[face]};
         }
 
-        template <bool kWithR>
-        __device__ inline void issue_brick(const Ticket& k, const double* __restrict__ z, const double* __restrict__ r,
-                                           const uint8_t* __restrict__ code, double* tile, double* rbuf, uint8_t* cbuf)
+        template <class T, bool kWithR>
+        __device__ inline void issue_brick(const Ticket& k, const T* __restrict__ z, const T* __restrict__ r,
+                                           const uint8_t* __restrict__ code, T* tile, T* rbuf, uint8_t* cbuf)
         {
             const int t = threadIdx.x;
             const int64_t base = int64_t(k.slot) * kC3;
             {
                 const int c = 2 * t, i = c & 7, j = (c >> 3) & 7, kk = c >> 6;
-                copy16(tile + tix(i, j, kk), z + base + c, true);
-                if (kWithR) copy16(rbuf + c, r + base + c, true);
+                copy_pair<T>(tile + tix(i, j, kk), z + base + c, true);
+                if (kWithR) copy_pair<T>(rbuf + c, r + base + c, true);
             }
             if (t < 32) copy16(cbuf + 16 * t, code + base + 16 * t, true);
             const bool valid = k.nbr >= 0;
@@ -129,25 +147,25 @@ namespace pcfd
                 int i, j, kk, hj, hk;
                 if (face < 4) { kk = w >> 2; i = (w & 3) * 2; j = face == 2 ? kBS - 1 : 0; hj = face == 2 ? -1 : kBS; hk = kk; }
                 else { i = (w * 2) & 7; j = (w * 2) >> 3; kk = face == 4 ? kBS - 1 : 0; hj = j; hk = face == 4 ? -1 : kBS; }
-                copy16(tile + tix(i, hj, hk), z + nb + (kk * kBS + j) * kBS + i, valid);
+                copy_pair<T>(tile + tix(i, hj, hk), z + nb + (kk * kBS + j) * kBS + i, valid);
             }
             else
             {
                 const int u = t - 128, face = u >> 6, j = u & 7, kk = (u >> 3) & 7;
                 const int i = face == 0 ? kBS - 1 : 0, hi = face == 0 ? -1 : kBS;
-                copy8(tile + tix(hi, j, kk), z + nb + (kk * kBS + j) * kBS + i, valid);
+                copy_one<T>(tile + tix(hi, j, kk), z + nb + (kk * kBS + j) * kBS + i, valid);
             }
         }
 
         // adds the coarse correction to the tile entries this thread copied
-        template <class TC>
-        __device__ inline void prolong_own(const Ticket& k, const TC* __restrict__ e, double* tile)
+        template <class T, class TC>
+        __device__ inline void prolong_own(const Ticket& k, const TC* __restrict__ e, double scale, T* tile)
         {
             const int t = threadIdx.x, l = k.level;
             {
                 const int c = 2 * t, i = c & 7, j = (c >> 3) & 7, kk = c >> 6;
-                tile[tix(i, j, kk)] += double(e[base_cell_of(k.base, l, i, j, kk)]);
-                tile[tix(i + 1, j, kk)] += double(e[base_cell_of(k.base, l, i + 1, j, kk)]);
+                tile[tix(i, j, kk)] += T(scale * double(e[base_cell_of(k.base, l, i, j, kk)]));
+                tile[tix(i + 1, j, kk)] += T(scale * double(e[base_cell_of(k.base, l, i + 1, j, kk)]));
             }
             if (k.nbr < 0) return;
             if (t < 128)
@@ -156,33 +174,34 @@ namespace pcfd
                 int i, j, kk, hj, hk;
                 if (face < 4) { kk = w >> 2; i = (w & 3) * 2; j = face == 2 ? kBS - 1 : 0; hj = face == 2 ? -1 : kBS; hk = kk; }
                 else { i = (w * 2) & 7; j = (w * 2) >> 3; kk = face == 4 ? kBS - 1 : 0; hj = j; hk = face == 4 ? -1 : kBS; }
-                tile[tix(i, hj, hk)] += double(e[base_cell_of(k.nbase, l, i, j, kk)]);
-                tile[tix(i + 1, hj, hk)] += double(e[base_cell_of(k.nbase, l, i + 1, j, kk)]);
+                tile[tix(i, hj, hk)] += T(scale * double(e[base_cell_of(k.nbase, l, i, j, kk)]));
+                tile[tix(i + 1, hj, hk)] += T(scale * double(e[base_cell_of(k.nbase, l, i + 1, j, kk)]));
             }
             else
             {
                 const int u = t - 128, face = u >> 6, j = u & 7, kk = (u >> 3) & 7;
                 const int i = face == 0 ? kBS - 1 : 0, hi = face == 0 ? -1 : kBS;
-                tile[tix(hi, j, kk)] += double(e[base_cell_of(k.nbase, l, i, j, kk)]);
+                tile[tix(hi, j, kk)] += T(scale * double(e[base_cell_of(k.nbase, l, i, j, kk)]));
             }
         }
 
         // kMode 0: Jacobi sweep, 1: residual restriction, 2: structured apply (out = A_struct z)
-        template <int kMode, class TC, bool kProlong>
-        __global__ void __launch_bounds__(256) brick_pipe_kernel(BrickView v, int64_t bricks, const double* __restrict__ z,
-            const double* __restrict__ r, double* __restrict__ out, double* __restrict__ t, const TC* __restrict__ e,
-            double* __restrict__ partial, const double* __restrict__ damping)
+        // T: field type of z, r, t (double, or float for the FP32 multigrid); TO: output type.
+        template <int kMode, class T, class TO, class TC, bool kProlong>
+        __global__ void __launch_bounds__(256) brick_pipe_kernel(BrickView v, int64_t bricks, const T* __restrict__ z,
+            const T* __restrict__ r, TO* __restrict__ out, T* __restrict__ t, const TC* __restrict__ e,
+            double* __restrict__ partial, const T* __restrict__ damping)
         {
             constexpr bool kWithR = kMode != 2;
-            __shared__ __align__(16) double tile[2][kTileSize];
-            __shared__ __align__(16) double rbuf[kWithR ? 2 : 1][kC3];
+            __shared__ __align__(16) T tile[2][kTileSize];
+            __shared__ __align__(16) T rbuf[kWithR ? 2 : 1][kC3];
             __shared__ __align__(16) uint8_t cbuf[2][kC3];
             __shared__ double residual[kMode == 1 ? kC3 : 1];
             int64_t b = blockIdx.x;
             if (b >= bricks) return;
             const int64_t G = gridDim.x;
             Ticket cur = load_ticket(v.meta, b);
-            issue_brick<kWithR>(cur, z, r, v.code, tile[0], rbuf[0], cbuf[0]);
+            issue_brick<T, kWithR>(cur, z, r, v.code, tile[0], rbuf[0], cbuf[0]);
             copy_commit();
             Ticket next = b + G < bricks ? load_ticket(v.meta, b + G) : cur;
             for (int it = 0;; ++it)
@@ -192,19 +211,19 @@ namespace pcfd
                 Ticket after = next;
                 if (has_next)
                 {
-                    issue_brick<kWithR>(next, z, r, v.code, tile[st ^ 1], rbuf[kWithR ? (st ^ 1) : 0], cbuf[st ^ 1]);
+                    issue_brick<T, kWithR>(next, z, r, v.code, tile[st ^ 1], rbuf[kWithR ? (st ^ 1) : 0], cbuf[st ^ 1]);
                     copy_commit();
                     if (b + 2 * G < bricks) after = load_ticket(v.meta, b + 2 * G);
                     copy_wait<1>();
                 }
                 else copy_wait<0>();
-                if (kProlong) prolong_own<TC>(cur, e, tile[st]);
+                if (kProlong) prolong_own<T, TC>(cur, e, v.prolong, tile[st]);
                 __syncthreads();
                 // ---- compute brick `cur` from buffer st.  Thread t owns cells t and t + 256, so a
                 // warp reads consecutive doubles of the tile (no shared-memory bank replays).
-                const double* T = tile[st];
+                const T* F = tile[st];
                 const int l = cur.level;
-                const double h = v.level_h[l];
+                const T h = T(v.level_h[l]);
                 const int64_t base = int64_t(cur.slot) * kC3;
                 const int n = l >= 3 ? 1 : (kBS >> l);
                 const int size = l >= 3 ? kC3 : (1 << (3 * l));
@@ -215,22 +234,22 @@ namespace pcfd
                     const int c = threadIdx.x + 256 * q, i = c & 7, j = (c >> 3) & 7, k = c >> 6;
                     const int s = tix(i, j, k);
                     const uint8_t code = cbuf[st][c];
-                    const double Az = structured_row(T, s, code, h);
-                    if (kMode == 2) out[base + c] = Az;
+                    const T Az = structured_row<T>(F, s, code, h);
+                    if (kMode == 2) out[base + c] = TO(Az);
                     else
                     {
-                        const double rc = rbuf[st][c];
+                        const T rc = rbuf[st][c];
                         if (code & kDeferred) t[base + c] = Az;
                         if (kMode == 0)
                         {
                             if (!(code & kDeferred))
-                                out[base + c] = code ? T[s] + (rc - Az) * damping[l * kDiagonalKinds + diagonal_kind(code)] : 0.0;
+                                out[base + c] = code ? TO(F[s] + (rc - Az) * damping[l * kDiagonalKinds + diagonal_kind(code)]) : TO(0);
                         }
                         else
                         {
                             const int group = l >= 3 ? 0 : ((k >> l) * n + (j >> l)) * n + (i >> l);
                             const int within = l >= 3 ? c : ((((k & mask) << l) + (j & mask)) << l) + (i & mask);
-                            residual[group * size + within] = (code && !(code & kDeferred)) ? rc - Az : 0.0;
+                            residual[group * size + within] = (code && !(code & kDeferred)) ? double(rc - Az) : 0.0;
                         }
                     }
                 }
@@ -278,25 +297,28 @@ namespace pcfd
         }
 
         // z = w r / D for every DOF (first sweep from zero); deferred rows read the assembled D.
+        // (FP32 multigrid: also writes the float copy of r that the float sweeps read.)
+        template <class T>
         __global__ void first_sweep_kernel(const uint8_t* __restrict__ code, const int* __restrict__ brick_level,
-                                           const double* __restrict__ damping, const double* __restrict__ diag,
+                                           const T* __restrict__ damping, const double* __restrict__ diag,
                                            const uint8_t* __restrict__ active, const double* __restrict__ r,
-                                           double* __restrict__ z, int64_t structured, int64_t n, double omega)
+                                           T* __restrict__ z, T* __restrict__ r_copy, int64_t structured, int64_t n, double omega)
         {
             const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
             if (q >= n) return;
             const uint8_t c = code[q];
+            if (r_copy) r_copy[q] = T(r[q]);
             if (q >= structured || (c & kDeferred))
             {
                 const double D = active[q] ? diag[q] : 0.0;
-                z[q] = D > 0.0 ? omega * r[q] / D : 0.0;
+                z[q] = D > 0.0 ? T(omega * r[q] / D) : T(0);
             }
-            else z[q] = c ? r[q] * damping[brick_level[q >> 9] * kDiagonalKinds + diagonal_kind(c)] : 0.0;
+            else z[q] = c ? T(r[q]) * damping[brick_level[q >> 9] * kDiagonalKinds + diagonal_kind(c)] : T(0);
         }
 
         // Completes deferred rows: A_orth z = t (structured part) + compact-edge gather + gauges,
         // in the order of the unfused launch; kMode 0 writes z_new, 1 writes the row residual.
-        template <int kMode, class TC, bool kProlong>
+        template <int kMode, class T, class TO, class TC, bool kProlong>
         __global__ void finish_deferred_kernel(int count, const int* __restrict__ dof, const int* __restrict__ incident,
             const int* __restrict__ gauge_offset, const double* __restrict__ gauge_coefficient,
             const int* __restrict__ incident_offset, const int* __restrict__ incident_edge, const int8_t* __restrict__ incident_sign,
@@ -304,22 +326,22 @@ namespace pcfd
             const double* __restrict__ conn_coefficient, const int* __restrict__ reg_lower, const int* __restrict__ reg_upper,
             const double* __restrict__ reg_coefficient, const uint8_t* __restrict__ active, const double* __restrict__ diag,
             const int* __restrict__ aggregate, int base_offset, int base_cells, const TC* __restrict__ e, int64_t structured,
-            const double* __restrict__ z, const double* __restrict__ r, const double* __restrict__ t, double* __restrict__ out,
-            double* __restrict__ residual, double omega)
+            const T* __restrict__ z, const T* __restrict__ r, const T* __restrict__ t, TO* __restrict__ out,
+            double* __restrict__ residual, double omega, double scale)
         {
             const int d = blockIdx.x * blockDim.x + threadIdx.x;
             if (d >= count) return;
             auto value = [&](int q) {
-                double v = z[q];
+                double v = double(z[q]);
                 if (kProlong && active[q])
                 {
                     const int c = aggregate[q] - base_offset;
-                    if (c >= 0 && c < base_cells) v += double(e[c]);
+                    if (c >= 0 && c < base_cells) v += scale * double(e[c]);
                 }
                 return v;
             };
             const int a = dof[d];
-            double Az = a < structured ? t[a] : 0.0;
+            double Az = a < structured ? double(t[a]) : 0.0;
             const int node = incident[d];
             if (node >= 0)
             {
@@ -340,10 +362,10 @@ namespace pcfd
             const double D = diag[a];
             if (kMode == 0)
             {
-                if (!active[a]) out[a] = 0.0;
-                else out[a] = D > 0.0 ? za + omega * (r[a] - Az) / D : za;
+                if (!active[a]) out[a] = TO(0);
+                else out[a] = TO(D > 0.0 ? za + omega * (double(r[a]) - Az) / D : za);
             }
-            else residual[d] = active[a] ? r[a] - Az : 0.0;
+            else residual[d] = active[a] ? double(r[a]) - Az : 0.0;
         }
 
         // base-level right-hand side: brick partials (levels in order) then deferred-row residuals
@@ -525,6 +547,14 @@ namespace pcfd
                     damping[size_t(l) * kDiagonalKinds + faces + 7 * outlet] = D > 0.0 ? (2.0 / 3.0) / D : 0.0;
                 }
         f.damping.upload(damping);
+        if (s.mg_precision == PCFD_MG_FP32 && !s.mg32.empty())
+        {
+            f.damping32.upload(std::vector<float>(damping.begin(), damping.end()));
+            f.z32.alloc(size_t(S));
+            f.z32b.alloc(size_t(S));
+            f.r32.alloc(size_t(S));
+            f.t32.alloc(size_t(S));
+        }
         f.code.upload(code);
         f.deferred_count = int(ddof.size());
         f.deferred_dof.upload(ddof);
@@ -572,20 +602,20 @@ namespace pcfd
     {
         BrickView view(System& s)
         {
-            return BrickView{reinterpret_cast<const BrickMeta*>(s.fine.meta.p), s.d_level_h, s.fine.code};
+            return BrickView{reinterpret_cast<const BrickMeta*>(s.fine.meta.p), s.d_level_h, s.fine.code, s.mg_prolong_scale};
         }
 
-        template <int kMode, class TC, bool kProlong>
-        void finish(System& s, const double* z, const double* r, double* out, const TC* e)
+        template <int kMode, class T, class TO, class TC, bool kProlong>
+        void finish(System& s, const T* z, const T* r, TO* out, const TC* e, const T* t)
         {
             FineSmoother& f = s.fine;
             const IrregularOperator& o = s.irr;
             if (!f.deferred_count) return;
-            finish_deferred_kernel<kMode, TC, kProlong><<<blocks_for(f.deferred_count), kThreads, 0, launch_stream(s)>>>(
+            finish_deferred_kernel<kMode, T, TO, TC, kProlong><<<blocks_for(f.deferred_count), kThreads, 0, launch_stream(s)>>>(
                 f.deferred_count, f.deferred_dof, f.deferred_incident, f.gauge_offset, f.gauge_coefficient, o.incident_offset,
                 o.incident_edge, o.incident_sign, o.connection_count, o.conn_lower, o.conn_upper, o.conn_coefficient, o.reg_lower,
                 o.reg_upper, o.reg_coefficient, s.active, s.diagonal, s.aggregate, s.base_offset, s.base_cells, e, s.structured, z, r,
-                f.t, out, f.deferred_residual, 2.0 / 3.0);
+                t, out, f.deferred_residual, 2.0 / 3.0, s.mg_prolong_scale);
         }
 
         int pipe_grid(const System& s)
@@ -600,52 +630,89 @@ namespace pcfd
             return std::max(1, std::min(s.active_bricks, 4 * sms));
         }
 
-        template <class TC, bool kProlong>
-        void sweep(System& s, const double* z, const double* r, double* out, const TC* e)
+        // the working buffers of the fine level in field type T
+        template <class T> struct FineBuffers;
+        template <> struct FineBuffers<double>
         {
-            FineSmoother& f = s.fine;
-            brick_pipe_kernel<0, TC, kProlong><<<pipe_grid(s), 256, 0, launch_stream(s)>>>(
-                view(s), s.active_bricks, z, r, out, f.t, e, nullptr, f.damping);
-            finish<0, TC, kProlong>(s, z, r, out, e);
+            double *a, *t;
+            const double* damping;
+            explicit FineBuffers(FineSmoother& f) : a(f.z.p), t(f.t.p), damping(f.damping.p) {}
+        };
+        template <> struct FineBuffers<float>
+        {
+            float *a, *t;
+            const float* damping;
+            explicit FineBuffers(FineSmoother& f) : a(f.z32.p), t(f.t32.p), damping(f.damping32.p) {}
+        };
+
+        template <class T, class TO, class TC, bool kProlong>
+        void sweep(System& s, const T* z, const T* r, TO* out, const TC* e)
+        {
+            FineBuffers<T> w(s.fine);
+            brick_pipe_kernel<0, T, TO, TC, kProlong><<<pipe_grid(s), 256, 0, launch_stream(s)>>>(
+                view(s), s.active_bricks, z, r, out, w.t, e, nullptr, w.damping);
+            finish<0, T, TO, TC, kProlong>(s, z, r, out, e, w.t);
         }
 
-        template <class TC>
-        void restrict_residual(System& s, const double* z, const double* r)
+        template <class T>
+        void restrict_residual(System& s, const T* z, const T* r)
         {
             FineSmoother& f = s.fine;
-            brick_pipe_kernel<1, TC, false><<<pipe_grid(s), 256, 0, launch_stream(s)>>>(
-                view(s), s.active_bricks, z, r, nullptr, f.t, nullptr, f.partial, f.damping);
+            FineBuffers<T> w(f);
+            brick_pipe_kernel<1, T, T, double, false><<<pipe_grid(s), 256, 0, launch_stream(s)>>>(
+                view(s), s.active_bricks, z, r, nullptr, w.t, nullptr, f.partial, w.damping);
+            finish<1, T, T, double, false>(s, z, r, nullptr, nullptr, w.t);
         }
     }
 
     void brick_apply(System& s, const double* p, double* out)
     {
-        brick_pipe_kernel<2, double, false><<<pipe_grid(s), 256, 0, launch_stream(s)>>>(
+        brick_pipe_kernel<2, double, double, double, false><<<pipe_grid(s), 256, 0, launch_stream(s)>>>(
             view(s), s.active_bricks, p, nullptr, out, nullptr, nullptr, nullptr, nullptr);
     }
 
+    // One application of the reference cycle with its fine level fused.  FP64: z_a, z and r are
+    // the double vectors.  FP32 multigrid (the coarse levels in float): the fine sweeps run on
+    // float copies -- r is converted once by the first sweep, the iterate ping-pongs between two
+    // float buffers and only the last sweep writes the double result -- so the smoother moves
+    // 4-byte values; the outer Krylov vectors, dots and the operator stay FP64.
     template <class TC>
     void fine_preconditioner(System& s, const double* r, double* z, std::vector<MgLevel<TC>>& levels)
     {
         FineSmoother& f = s.fine;
-        double* a = f.z.p;
-        first_sweep_kernel<<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(f.code, s.brick_level, f.damping, s.diagonal,
-                                                                              s.active, r, a, s.structured, s.S, 2.0 / 3.0);
-        sweep<TC, false>(s, a, r, z, nullptr);
         MgLevel<TC>& base = levels.front();
-        cuda_check(cudaMemsetAsync(base.x, 0, size_t(base.cells) * sizeof(TC), s.stream), "clear base correction");
-        restrict_residual<TC>(s, z, r);
-        finish<1, TC, false>(s, z, r, nullptr, nullptr);
-        gather_base_kernel<TC><<<blocks_for(base.cells), kThreads, 0, launch_stream(s)>>>(base.cells, f.gather_offset, f.gather_entry,
-                                                                                         f.partial, f.deferred_residual, base.rhs);
-        multigrid_levels(s, levels);
-        sweep<TC, true>(s, z, r, a, base.x.p);
-        sweep<TC, false>(s, a, r, z, nullptr);
+        auto coarse = [&](auto* zz, auto* rr) {
+            cuda_check(cudaMemsetAsync(base.x, 0, size_t(base.cells) * sizeof(TC), s.stream), "clear base correction");
+            restrict_residual(s, zz, rr);
+            gather_base_kernel<TC><<<blocks_for(base.cells), kThreads, 0, launch_stream(s)>>>(
+                base.cells, f.gather_offset, f.gather_entry, f.partial, f.deferred_residual, base.rhs);
+            multigrid_levels(s, levels);
+        };
+        if (std::is_same<TC, float>::value && f.z32.n)
+        {
+            float *a = f.z32.p, *b = f.z32b.p, *r32 = f.r32.p;
+            first_sweep_kernel<float><<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(
+                f.code, s.brick_level, f.damping32.p, s.diagonal, s.active, r, a, r32, s.structured, s.S, 2.0 / 3.0);
+            sweep<float, float, TC, false>(s, a, r32, b, nullptr);
+            coarse(b, r32);
+            sweep<float, float, TC, true>(s, b, r32, a, base.x.p);
+            sweep<float, double, TC, false>(s, a, r32, z, nullptr);
+        }
+        else
+        {
+            double* a = f.z.p;
+            first_sweep_kernel<double><<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(
+                f.code, s.brick_level, f.damping.p, s.diagonal, s.active, r, a, nullptr, s.structured, s.S, 2.0 / 3.0);
+            sweep<double, double, TC, false>(s, a, r, z, nullptr);
+            coarse(z, r);
+            sweep<double, double, TC, true>(s, z, r, a, base.x.p);
+            sweep<double, double, TC, false>(s, a, r, z, nullptr);
+        }
         cuda_check(cudaGetLastError(), "fused preconditioner");
     }
 
-    // Stages of the fused cycle for component timing: 0 pre-smoothing, 1 residual restriction to
-    // the level-0 aggregates, 2 the aggregation hierarchy, 3 prolongation + post-smoothing.
+    // Stages of the fused FP64 cycle for component timing: 0 pre-smoothing, 1 residual restriction
+    // to the level-0 aggregates, 2 the aggregation hierarchy, 3 prolongation + post-smoothing.
     void fine_preconditioner_stage(System& s, int stage, const double* r, double* z)
     {
         require(s.fine.enabled && !s.mg64.empty(), "fused preconditioner not enabled");
@@ -655,14 +722,13 @@ namespace pcfd
         double* a = f.z.p;
         if (stage == 0)
         {
-            first_sweep_kernel<<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(f.code, s.brick_level, f.damping, s.diagonal,
-                                                                                  s.active, r, a, s.structured, s.S, 2.0 / 3.0);
-            sweep<double, false>(s, a, r, z, nullptr);
+            first_sweep_kernel<double><<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(
+                f.code, s.brick_level, f.damping.p, s.diagonal, s.active, r, a, nullptr, s.structured, s.S, 2.0 / 3.0);
+            sweep<double, double, double, false>(s, a, r, z, nullptr);
         }
         else if (stage == 1)
         {
             restrict_residual<double>(s, z, r);
-            finish<1, double, false>(s, z, r, nullptr, nullptr);
             gather_base_kernel<double><<<blocks_for(base.cells), kThreads, 0, launch_stream(s)>>>(
                 base.cells, f.gather_offset, f.gather_entry, f.partial, f.deferred_residual, base.rhs);
         }
@@ -673,8 +739,8 @@ namespace pcfd
         }
         else
         {
-            sweep<double, true>(s, z, r, a, base.x.p);
-            sweep<double, false>(s, a, r, z, nullptr);
+            sweep<double, double, double, true>(s, z, r, a, base.x.p);
+            sweep<double, double, double, false>(s, a, r, z, nullptr);
         }
     }
 

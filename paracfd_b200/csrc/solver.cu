@@ -17,6 +17,7 @@
 #include <array>
 #include <cmath>
 #include <limits>
+#include <type_traits>
 #include <unordered_map>
 
 namespace pcfd
@@ -327,19 +328,19 @@ namespace pcfd
             coarse_rhs[c] = T(sum);
         }
         template <class T>
-        __global__ void prolong_add_kernel(const int* aggregate, int cells, const T* coarse_x, T* fine_x)
+        __global__ void prolong_add_kernel(const int* aggregate, int cells, const T* coarse_x, T* fine_x, T scale)
         {
             const int q = blockIdx.x * blockDim.x + threadIdx.x;
-            if (q < cells && aggregate[q] >= 0) fine_x[q] += coarse_x[aggregate[q]];
+            if (q < cells && aggregate[q] >= 0) fine_x[q] += scale * coarse_x[aggregate[q]];
         }
         template <class T>
         __global__ void prolong_aggregate_kernel(const int* aggregate, const uint8_t* active, int64_t n, int base_offset,
-                                                 int base_cells, const T* coarse_x, double* out)
+                                                 int base_cells, const T* coarse_x, double* out, double scale)
         {
             const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
             if (q >= n || !active[q]) return;
             const int c = aggregate[q] - base_offset;
-            if (c >= 0 && c < base_cells) out[q] += double(coarse_x[c]);
+            if (c >= 0 && c < base_cells) out[q] += scale * double(coarse_x[c]);
         }
         // Coarsest-level Jacobi sweeps inside one CTA (cells <= blockDim.x * kPerThread).
         template <class T, int kPerThread>
@@ -398,7 +399,8 @@ namespace pcfd
                 level.restrict_offset, level.restrict_dof, level.residual, coarse.cells, coarse.rhs);
             cuda_check(cudaMemsetAsync(coarse.x, 0, size_t(coarse.cells) * sizeof(T), s.stream), "clear coarse correction");
             mg_level(s, levels, index + 1);
-            prolong_add_kernel<T><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(level.aggregate, level.cells, coarse.x, level.x);
+            prolong_add_kernel<T><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(level.aggregate, level.cells, coarse.x, level.x,
+                                                                                             T(s.mg_lattice_scale));
             smooth(2);
         }
 
@@ -412,7 +414,7 @@ namespace pcfd
                 s.base_restrict_offset, s.base_restrict_dof, r, s.t, base.cells, base.rhs);
             mg_level(s, levels, 0);
             prolong_aggregate_kernel<T><<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(s.aggregate, s.active, s.S, s.base_offset,
-                                                                                  s.base_cells, base.x, z);
+                                                                                  s.base_cells, base.x, z, s.mg_prolong_scale);
         }
     }
 
@@ -437,7 +439,45 @@ namespace pcfd
             }
     }
 
-    template <class T> void multigrid_levels(System& s, std::vector<MgLevel<T>>& levels) { mg_level(s, levels, 0); }
+    // The aggregation hierarchy below the fine level is the same fixed sequence of ~30 small
+    // launches on every application (levels of 2.3 M cells down to <= 512), so it is captured
+    // once into a CUDA graph on the system stream and replayed; the launch gaps of the coarse
+    // levels, not their bytes, dominate it.  Systems on the legacy default stream launch directly.
+    template <class T> void multigrid_levels(System& s, std::vector<MgLevel<T>>& levels)
+    {
+        const bool fp32 = std::is_same<T, float>::value;
+        cudaGraphExec_t& exec = fp32 ? s.mg_graph32 : s.mg_graph64;
+        int64_t& nodes = fp32 ? s.mg_graph32_launches : s.mg_graph64_launches;
+        if (!s.stream)
+        {
+            mg_level(s, levels, 0);
+            return;
+        }
+        if (!exec)
+        {
+            const int64_t before = s.launches;
+            cuda_check(cudaStreamBeginCapture(s.stream, cudaStreamCaptureModeThreadLocal), "begin hierarchy capture");
+            cudaGraph_t graph = nullptr;
+            try
+            {
+                mg_level(s, levels, 0);
+            }
+            catch (...)
+            {
+                cudaStreamEndCapture(s.stream, &graph);
+                if (graph) cudaGraphDestroy(graph);
+                throw;
+            }
+            cuda_check(cudaStreamEndCapture(s.stream, &graph), "end hierarchy capture");
+            const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphDestroy(graph);
+            cuda_check(e, "instantiate hierarchy graph");
+            nodes = s.launches - before;
+            s.launches = before;
+        }
+        cuda_check(cudaGraphLaunch(exec, s.stream), "launch hierarchy graph");
+        s.launches += nodes;
+    }
     template void multigrid_levels<double>(System&, std::vector<MgLevel<double>>&);
     template void multigrid_levels<float>(System&, std::vector<MgLevel<float>>&);
 

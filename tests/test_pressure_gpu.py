@@ -91,12 +91,12 @@ def test_flux_correction_matches_reference(case):
             assert rel(g[moved_by_twin], r[moved_by_twin]) <= 1e-6
 
 
-@pytest.mark.parametrize("precision", [MG_FP64, MG_FP32])
-def test_solve_reaches_tolerance_on_reference_operator(case, precision):
+@pytest.mark.parametrize("precision,cycle", [(MG_FP64, 0), (MG_FP32, 0), (MG_FP64, 1), (MG_FP32, 1)])
+def test_solve_reaches_tolerance_on_reference_operator(case, precision, cycle):
     rc, _ = case
     rng = np.random.default_rng(3)
     b = rng.standard_normal(rc.n) * rc.active
-    with CompositeSystem(rc.topology, mg_precision=precision) as s:
+    with CompositeSystem(rc.topology, mg_precision=precision, mg_cycle=cycle) as s:
         x, res = s.solve(b, 1e-8, 600)
     assert res["converged"], res
     true = np.linalg.norm((b - rc.apply(x))[rc.active.astype(bool)]) / np.linalg.norm(b)
@@ -122,3 +122,26 @@ def test_fused_preconditioner_matches_separate_launches_and_oracle(case):
     oracle.close()
     # repeated applications are identical (deterministic reductions, ping-pong buffers reset)
     assert np.array_equal(z, fused.precondition(r))
+
+
+def test_corrected_cycle_fused_matches_separate_launches(case):
+    """The over-corrected cycle scales the same prolongations in both implementations."""
+    rc, _ = case
+    r = np.random.default_rng(19).standard_normal(rc.n) * rc.active
+    with CompositeSystem(rc.topology, mg_cycle=1) as fused, CompositeSystem(rc.topology, mg_cycle=1,
+                                                                            fused_smoother=False) as plain:
+        assert fused.fused_preconditioner and not plain.fused_preconditioner
+        act = rc.active.astype(bool)
+        assert rel(fused.precondition(r), plain.precondition(r), act) <= 1e-12
+
+
+def test_fp32_fused_fine_level_matches_fp64_fine_level(case):
+    """FP32 multigrid: the fused cycle runs the fine sweeps on float copies; the separate-launch
+    cycle keeps the fine level in double.  They agree to float rounding."""
+    rc, _ = case
+    r = np.random.default_rng(29).standard_normal(rc.n) * rc.active
+    with CompositeSystem(rc.topology, mg_precision=MG_FP32) as fused, \
+            CompositeSystem(rc.topology, mg_precision=MG_FP32, fused_smoother=False) as plain:
+        assert fused.fused_preconditioner
+        act = rc.active.astype(bool)
+        assert rel(fused.precondition(r), plain.precondition(r), act) <= 1e-5
