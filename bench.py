@@ -48,7 +48,7 @@ def parse_args():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", default="paraglider16m")
     ap.add_argument("--mg", choices=("fp64", "fp32"), default="fp64", help="multigrid preconditioner precision")
-    ap.add_argument("--mg-cycle", choices=("reference", "corrected"), default="reference",
+    ap.add_argument("--mg-cycle", choices=("reference", "corrected", "composite"), default="composite",
                     help="coarse-correction weighting of the multigrid cycle (pcfd_mg_cycle)")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU sample of the ours arm")
     ap.add_argument("--no-reference-gpu", action="store_true", help="reference arm: skip the sm_100a reference run")
@@ -284,7 +284,7 @@ def run_ours(args, ranks: Ranks):
     built = spec.build()
     bricks = non_covered_bricks(built.topology)
     system = CompositeSystem(built.topology, MG_FP32 if args.mg == "fp32" else MG_FP64, device=ranks.local,
-                             mg_cycle=1 if args.mg_cycle == "corrected" else 0)
+                             mg_cycle={"reference": 0, "corrected": 1, "composite": 2}[args.mg_cycle])
     system.configure(speed=spec.speed, **spec.case)
     slots = system.inflow_layout()
     faces = len(slots) * spec.brick_size ** 2
@@ -417,7 +417,7 @@ def run_kernel_only(args):
     spec = WORKLOADS[args.workload]
     built = spec.build()
     system = CompositeSystem(built.topology, MG_FP32 if args.mg == "fp32" else MG_FP64,
-                             mg_cycle=1 if args.mg_cycle == "corrected" else 0)
+                             mg_cycle={"reference": 0, "corrected": 1, "composite": 2}[args.mg_cycle])
     ms = system.time_kernel(args.kernel_only, args.kernel_iterations)
     line = {"kernel_only": args.kernel_only, "workload": args.workload, "ms_per_launch": ms,
             "iterations": args.kernel_iterations, "launches": system.launch_count()}

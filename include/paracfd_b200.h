@@ -185,7 +185,14 @@ typedef struct pcfd_options {
  * reference cycle stays the default. */
 typedef enum pcfd_mg_cycle {
     PCFD_MG_CYCLE_REFERENCE = 0,     /* the reference's cycle (amr_pressure.cu:1103-1154) */
-    PCFD_MG_CYCLE_CORRECTED = 1      /* over-corrected prolongation */
+    PCFD_MG_CYCLE_CORRECTED = 1,     /* over-corrected prolongation */
+    PCFD_MG_CYCLE_COMPOSITE = 2      /* composite-grid stages between the fine level and the level-0
+                                        lattice (each coarsens the finest remaining AMR level 2x2x2,
+                                        Galerkin operators), prolongations weighted 2 (stages) and 1.3
+                                        (lattice): about half the iterations of the reference cycle on
+                                        the 4-level 16 M-cell wing grid.  Needs 8^3 bricks and the fused
+                                        fine level; with the FP32 multigrid the stages and the lattice
+                                        levels are float, the fine sweeps stay FP64. */
 } pcfd_mg_cycle;
 
 /* AmrGpuSolveResult (amr_pressure.h:337-351), trimmed to what the solver reports. */

@@ -17,7 +17,7 @@ from .capi import Options, SolveResult, Topology, check, ptr
 PROFILE_STRUCTURED_APPLY = 0
 PROFILE_PRECONDITIONER = 1
 MG_FP64, MG_FP32 = 0, 1
-MG_CYCLE_REFERENCE, MG_CYCLE_CORRECTED = 0, 1
+MG_CYCLE_REFERENCE, MG_CYCLE_CORRECTED, MG_CYCLE_COMPOSITE = 0, 1, 2
 
 
 class BuiltTopology:

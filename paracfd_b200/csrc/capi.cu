@@ -199,14 +199,20 @@ namespace pcfd
             const std::vector<double> diag = host_diagonal(t);
             s.diagonal.upload(diag);
             build_operator(s, t);
-            if (options && options->mg_cycle == PCFD_MG_CYCLE_CORRECTED)
-            {
-                s.mg_prolong_scale = 2.0;
-                s.mg_lattice_scale = 1.5;
-            }
-            else require(!options || options->mg_cycle == PCFD_MG_CYCLE_REFERENCE, "unknown multigrid cycle");
+            const int cycle = options ? options->mg_cycle : PCFD_MG_CYCLE_REFERENCE;
+            require(cycle >= PCFD_MG_CYCLE_REFERENCE && cycle <= PCFD_MG_CYCLE_COMPOSITE, "unknown multigrid cycle");
+            if (cycle == PCFD_MG_CYCLE_CORRECTED) { s.mg_prolong_scale = 2.0; s.mg_lattice_scale = 1.5; }
+            if (cycle == PCFD_MG_CYCLE_COMPOSITE) { s.mg_prolong_scale = 2.0; s.mg_lattice_scale = 1.3; }
             build_multigrid(s, t, diag);
+            for (MgLevel<double>& level : s.mg64) level.prolong = s.mg_lattice_scale;
+            for (MgLevel<float>& level : s.mg32) level.prolong = s.mg_lattice_scale;
             if (!options || !options->disable_fused_smoother) build_fine_smoother(s, t, diag);
+            if (cycle == PCFD_MG_CYCLE_COMPOSITE)
+            {
+                require(s.fine.enabled, "the composite cycle needs the fused fine level (8^3 bricks)");
+                s.composite_fp32 = s.mg_precision == PCFD_MG_FP32 && !s.mg32.empty();
+                build_composite(s, t);
+            }
             // Krylov storage
             for (DBuf<double>* v : {&s.r, &s.z, &s.dvec, &s.Ad, &s.t, &s.correction, &s.defect, &s.scratch_p, &s.scratch_out,
                                      &s.integrated, &s.rhs, &s.pressure})

@@ -106,6 +106,7 @@ namespace pcfd
         int cells = 0;
         DBuf<int> row_offset, neighbour, aggregate, restrict_offset, restrict_dof;
         DBuf<T> coefficient, diagonal, rhs, x, temporary, residual;
+        double prolong = 1.0;                   // weight of the next level's correction added here
     };
 
     struct Scalars;   // device scalar block for the Krylov recurrences
@@ -196,9 +197,17 @@ namespace pcfd
         DBuf<int> base_restrict_offset, base_restrict_dof;
         std::vector<MgLevel<double>> mg64;
         std::vector<MgLevel<float>> mg32;
+        // composite cycle (PCFD_MG_CYCLE_COMPOSITE): Galerkin levels of the AMR composite grid with
+        // the finest level coarsened 2x2x2 one level at a time, above the lattice hierarchy
+        bool composite = false;
+        std::vector<MgLevel<double>> inter64;
+        std::vector<MgLevel<float>> inter32;    // the same stages in float (FP32 multigrid)
+        DBuf<int> fine_map, fine_restrict_offset, fine_restrict_dof;   // fine DOF -> first coarse cell
+        DBuf<double> fine_residual;             // [S] r - A_orth z before the first restriction
         FineSmoother fine;
-        cudaGraphExec_t mg_graph64 = nullptr, mg_graph32 = nullptr;   // captured aggregation hierarchy
-        int64_t mg_graph64_launches = 0, mg_graph32_launches = 0;
+        cudaGraphExec_t mg_graph64 = nullptr, mg_graph32 = nullptr, mg_graph_composite = nullptr;   // captured hierarchies
+        int64_t mg_graph64_launches = 0, mg_graph32_launches = 0, mg_graph_composite_launches = 0;
+        bool composite_fp32 = false;            // composite stages + lattice in float
         DBuf<float> diagonal32;
 
         // Krylov vectors
@@ -300,6 +309,9 @@ namespace pcfd
     void fine_preconditioner_stage(System& s, int stage, const double* r, double* z);
     template <class T> void fine_preconditioner(System& s, const double* r, double* z, std::vector<MgLevel<T>>& levels);
     template <class T> void multigrid_levels(System& s, std::vector<MgLevel<T>>& levels);
+    void build_composite(System& s, const pcfd_topology& t);
+    void composite_levels(System& s);                 // V-cycle below the fine level, composite chain
+    void composite_preconditioner(System& s, const double* r, double* z);   // smoother.cu
     pcfd_solve_result solve(System& s, double* x, const double* b, double tolerance, int max_iterations, bool warm);
     // vector helpers
     void vec_copy_active(System& s, const double* src, double* dst);

@@ -47,6 +47,7 @@ namespace pcfd
             const double* level_h;
             const uint8_t* code;
             double prolong;            // scale of the prolonged coarse correction
+            const int* map;            // composite cycle: fine DOF -> first stage cell (mapped prolongation)
         };
 
         // Shared tile of one brick plus its face halos: rows of 12 doubles so that interior rows
@@ -157,37 +158,51 @@ namespace pcfd
             }
         }
 
-        // adds the coarse correction to the tile entries this thread copied
-        template <class T, class TC>
-        __device__ inline void prolong_own(const Ticket& k, const TC* __restrict__ e, double scale, T* tile)
+        // adds the coarse correction to the tile entries this thread copied; kMapped: through the
+        // fine -> stage-1 map of the composite cycle, else the geometric level-0 cell
+        template <class T, class TC, bool kMapped>
+        __device__ inline void prolong_own(const Ticket& k, const TC* __restrict__ e, double scale, const int* __restrict__ map, T* tile)
         {
             const int t = threadIdx.x, l = k.level;
+            auto add = [&](int s_tile, int64_t q, int b0, int i, int j, int kk) {
+                if (kMapped)
+                {
+                    const int c = map[q];
+                    if (c >= 0) tile[s_tile] += T(scale * double(e[c]));
+                }
+                else tile[s_tile] += T(scale * double(e[base_cell_of(b0, l, i, j, kk)]));
+            };
             {
                 const int c = 2 * t, i = c & 7, j = (c >> 3) & 7, kk = c >> 6;
-                tile[tix(i, j, kk)] += T(scale * double(e[base_cell_of(k.base, l, i, j, kk)]));
-                tile[tix(i + 1, j, kk)] += T(scale * double(e[base_cell_of(k.base, l, i + 1, j, kk)]));
+                const int64_t q = int64_t(k.slot) * kC3 + c;
+                add(tix(i, j, kk), q, k.base, i, j, kk);
+                add(tix(i + 1, j, kk), q + 1, k.base, i + 1, j, kk);
             }
             if (k.nbr < 0) return;
+            const int64_t nb = int64_t(k.nbr) * kC3;
             if (t < 128)
             {
                 const int face = 2 + (t >> 5), w = t & 31;
                 int i, j, kk, hj, hk;
                 if (face < 4) { kk = w >> 2; i = (w & 3) * 2; j = face == 2 ? kBS - 1 : 0; hj = face == 2 ? -1 : kBS; hk = kk; }
                 else { i = (w * 2) & 7; j = (w * 2) >> 3; kk = face == 4 ? kBS - 1 : 0; hj = j; hk = face == 4 ? -1 : kBS; }
-                tile[tix(i, hj, hk)] += T(scale * double(e[base_cell_of(k.nbase, l, i, j, kk)]));
-                tile[tix(i + 1, hj, hk)] += T(scale * double(e[base_cell_of(k.nbase, l, i + 1, j, kk)]));
+                const int64_t q = nb + (kk * kBS + j) * kBS + i;
+                add(tix(i, hj, hk), q, k.nbase, i, j, kk);
+                add(tix(i + 1, hj, hk), q + 1, k.nbase, i + 1, j, kk);
             }
             else
             {
                 const int u = t - 128, face = u >> 6, j = u & 7, kk = (u >> 3) & 7;
                 const int i = face == 0 ? kBS - 1 : 0, hi = face == 0 ? -1 : kBS;
-                tile[tix(hi, j, kk)] += T(scale * double(e[base_cell_of(k.nbase, l, i, j, kk)]));
+                add(tix(hi, j, kk), nb + (kk * kBS + j) * kBS + i, k.nbase, i, j, kk);
             }
         }
 
         // kMode 0: Jacobi sweep, 1: residual restriction, 2: structured apply (out = A_struct z)
         // T: field type of z, r, t (double, or float for the FP32 multigrid); TO: output type.
-        template <int kMode, class T, class TO, class TC, bool kProlong>
+        // kProlong: 0 none, 1 level-0 cell (reference cycle), 2 mapped (composite cycle);
+        // kMode 3: write the residual r - A_struct z (composite cycle's first restriction)
+        template <int kMode, class T, class TO, class TC, int kProlong>
         __global__ void __launch_bounds__(256) brick_pipe_kernel(BrickView v, int64_t bricks, const T* __restrict__ z,
             const T* __restrict__ r, TO* __restrict__ out, T* __restrict__ t, const TC* __restrict__ e,
             double* __restrict__ partial, const T* __restrict__ damping)
@@ -217,7 +232,7 @@ namespace pcfd
                     copy_wait<1>();
                 }
                 else copy_wait<0>();
-                if (kProlong) prolong_own<T, TC>(cur, e, v.prolong, tile[st]);
+                if (kProlong) prolong_own<T, TC, kProlong == 2>(cur, e, v.prolong, v.map, tile[st]);
                 __syncthreads();
                 // ---- compute brick `cur` from buffer st.  Thread t owns cells t and t + 256, so a
                 // warp reads consecutive doubles of the tile (no shared-memory bank replays).
@@ -244,6 +259,10 @@ namespace pcfd
                         {
                             if (!(code & kDeferred))
                                 out[base + c] = code ? TO(F[s] + (rc - Az) * damping[l * kDiagonalKinds + diagonal_kind(code)]) : TO(0);
+                        }
+                        else if (kMode == 3)
+                        {
+                            if (!(code & kDeferred)) out[base + c] = code ? TO(rc - Az) : TO(0);
                         }
                         else
                         {
@@ -318,7 +337,8 @@ namespace pcfd
 
         // Completes deferred rows: A_orth z = t (structured part) + compact-edge gather + gauges,
         // in the order of the unfused launch; kMode 0 writes z_new, 1 writes the row residual.
-        template <int kMode, class T, class TO, class TC, bool kProlong>
+        // kMode 0: z_new, 1: residual into the compact deferred list, 2: residual into out[a]
+        template <int kMode, class T, class TO, class TC, int kProlong>
         __global__ void finish_deferred_kernel(int count, const int* __restrict__ dof, const int* __restrict__ incident,
             const int* __restrict__ gauge_offset, const double* __restrict__ gauge_coefficient,
             const int* __restrict__ incident_offset, const int* __restrict__ incident_edge, const int8_t* __restrict__ incident_sign,
@@ -327,7 +347,7 @@ namespace pcfd
             const double* __restrict__ reg_coefficient, const uint8_t* __restrict__ active, const double* __restrict__ diag,
             const int* __restrict__ aggregate, int base_offset, int base_cells, const TC* __restrict__ e, int64_t structured,
             const T* __restrict__ z, const T* __restrict__ r, const T* __restrict__ t, TO* __restrict__ out,
-            double* __restrict__ residual, double omega, double scale)
+            double* __restrict__ residual, double omega, double scale, const int* __restrict__ map)
         {
             const int d = blockIdx.x * blockDim.x + threadIdx.x;
             if (d >= count) return;
@@ -335,8 +355,16 @@ namespace pcfd
                 double v = double(z[q]);
                 if (kProlong && active[q])
                 {
-                    const int c = aggregate[q] - base_offset;
-                    if (c >= 0 && c < base_cells) v += scale * double(e[c]);
+                    if (kProlong == 2)
+                    {
+                        const int c = map[q];
+                        if (c >= 0) v += scale * double(e[c]);
+                    }
+                    else
+                    {
+                        const int c = aggregate[q] - base_offset;
+                        if (c >= 0 && c < base_cells) v += scale * double(e[c]);
+                    }
                 }
                 return v;
             };
@@ -365,7 +393,8 @@ namespace pcfd
                 if (!active[a]) out[a] = TO(0);
                 else out[a] = TO(D > 0.0 ? za + omega * (double(r[a]) - Az) / D : za);
             }
-            else residual[d] = active[a] ? double(r[a]) - Az : 0.0;
+            else if (kMode == 1) residual[d] = active[a] ? double(r[a]) - Az : 0.0;
+            else out[a] = TO(active[a] ? double(r[a]) - Az : 0.0);
         }
 
         // base-level right-hand side: brick partials (levels in order) then deferred-row residuals
@@ -602,10 +631,11 @@ namespace pcfd
     {
         BrickView view(System& s)
         {
-            return BrickView{reinterpret_cast<const BrickMeta*>(s.fine.meta.p), s.d_level_h, s.fine.code, s.mg_prolong_scale};
+            return BrickView{reinterpret_cast<const BrickMeta*>(s.fine.meta.p), s.d_level_h, s.fine.code, s.mg_prolong_scale,
+                             s.fine_map.p};
         }
 
-        template <int kMode, class T, class TO, class TC, bool kProlong>
+        template <int kMode, class T, class TO, class TC, int kProlong>
         void finish(System& s, const T* z, const T* r, TO* out, const TC* e, const T* t)
         {
             FineSmoother& f = s.fine;
@@ -615,7 +645,7 @@ namespace pcfd
                 f.deferred_count, f.deferred_dof, f.deferred_incident, f.gauge_offset, f.gauge_coefficient, o.incident_offset,
                 o.incident_edge, o.incident_sign, o.connection_count, o.conn_lower, o.conn_upper, o.conn_coefficient, o.reg_lower,
                 o.reg_upper, o.reg_coefficient, s.active, s.diagonal, s.aggregate, s.base_offset, s.base_cells, e, s.structured, z, r,
-                t, out, f.deferred_residual, 2.0 / 3.0, s.mg_prolong_scale);
+                t, out, f.deferred_residual, 2.0 / 3.0, s.mg_prolong_scale, s.fine_map.p);
         }
 
         int pipe_grid(const System& s)
@@ -645,7 +675,7 @@ namespace pcfd
             explicit FineBuffers(FineSmoother& f) : a(f.z32.p), t(f.t32.p), damping(f.damping32.p) {}
         };
 
-        template <class T, class TO, class TC, bool kProlong>
+        template <class T, class TO, class TC, int kProlong>
         void sweep(System& s, const T* z, const T* r, TO* out, const TC* e)
         {
             FineBuffers<T> w(s.fine);
@@ -659,15 +689,15 @@ namespace pcfd
         {
             FineSmoother& f = s.fine;
             FineBuffers<T> w(f);
-            brick_pipe_kernel<1, T, T, double, false><<<pipe_grid(s), 256, 0, launch_stream(s)>>>(
+            brick_pipe_kernel<1, T, T, double, 0><<<pipe_grid(s), 256, 0, launch_stream(s)>>>(
                 view(s), s.active_bricks, z, r, nullptr, w.t, nullptr, f.partial, w.damping);
-            finish<1, T, T, double, false>(s, z, r, nullptr, nullptr, w.t);
+            finish<1, T, T, double, 0>(s, z, r, nullptr, nullptr, w.t);
         }
     }
 
     void brick_apply(System& s, const double* p, double* out)
     {
-        brick_pipe_kernel<2, double, double, double, false><<<pipe_grid(s), 256, 0, launch_stream(s)>>>(
+        brick_pipe_kernel<2, double, double, double, 0><<<pipe_grid(s), 256, 0, launch_stream(s)>>>(
             view(s), s.active_bricks, p, nullptr, out, nullptr, nullptr, nullptr, nullptr);
     }
 
@@ -693,22 +723,68 @@ namespace pcfd
             float *a = f.z32.p, *b = f.z32b.p, *r32 = f.r32.p;
             first_sweep_kernel<float><<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(
                 f.code, s.brick_level, f.damping32.p, s.diagonal, s.active, r, a, r32, s.structured, s.S, 2.0 / 3.0);
-            sweep<float, float, TC, false>(s, a, r32, b, nullptr);
+            sweep<float, float, TC, 0>(s, a, r32, b, nullptr);
             coarse(b, r32);
-            sweep<float, float, TC, true>(s, b, r32, a, base.x.p);
-            sweep<float, double, TC, false>(s, a, r32, z, nullptr);
+            sweep<float, float, TC, 1>(s, b, r32, a, base.x.p);
+            sweep<float, double, TC, 0>(s, a, r32, z, nullptr);
         }
         else
         {
             double* a = f.z.p;
             first_sweep_kernel<double><<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(
                 f.code, s.brick_level, f.damping.p, s.diagonal, s.active, r, a, nullptr, s.structured, s.S, 2.0 / 3.0);
-            sweep<double, double, TC, false>(s, a, r, z, nullptr);
+            sweep<double, double, TC, 0>(s, a, r, z, nullptr);
             coarse(z, r);
-            sweep<double, double, TC, true>(s, z, r, a, base.x.p);
-            sweep<double, double, TC, false>(s, a, r, z, nullptr);
+            sweep<double, double, TC, 1>(s, z, r, a, base.x.p);
+            sweep<double, double, TC, 0>(s, a, r, z, nullptr);
         }
         cuda_check(cudaGetLastError(), "fused preconditioner");
+    }
+
+    namespace
+    {
+        template <class TC>
+        __global__ void gather_first_kernel(int cells, const int* __restrict__ offset, const int* __restrict__ dof,
+                                            const double* __restrict__ residual, TC* __restrict__ rhs)
+        {
+            const int c = blockIdx.x * blockDim.x + threadIdx.x;
+            if (c >= cells) return;
+            double sum = 0.0;
+            for (int q = offset[c]; q < offset[c + 1]; ++q) sum += residual[dof[q]];
+            rhs[c] = TC(sum);
+        }
+
+        template <class TC>
+        void composite_cycle(System& s, const double* r, double* z, MgLevel<TC>& first)
+        {
+            FineSmoother& f = s.fine;
+            double* a = f.z.p;
+            first_sweep_kernel<double><<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(
+                f.code, s.brick_level, f.damping.p, s.diagonal, s.active, r, a, nullptr, s.structured, s.S, 2.0 / 3.0);
+            sweep<double, double, TC, 0>(s, a, r, z, nullptr);
+            double* res = s.fine_residual.p;
+            brick_pipe_kernel<3, double, double, TC, 0><<<pipe_grid(s), 256, 0, launch_stream(s)>>>(
+                view(s), s.active_bricks, z, r, res, f.t.p, nullptr, nullptr, f.damping.p);
+            finish<2, double, double, TC, 0>(s, z, r, res, static_cast<const TC*>(nullptr), f.t.p);
+            gather_first_kernel<TC><<<blocks_for(first.cells), kThreads, 0, launch_stream(s)>>>(
+                first.cells, s.fine_restrict_offset, s.fine_restrict_dof, res, first.rhs);
+            cuda_check(cudaMemsetAsync(first.x, 0, size_t(first.cells) * sizeof(TC), s.stream), "clear stage correction");
+            composite_levels(s);
+            sweep<double, double, TC, 2>(s, z, r, a, first.x.p);
+            sweep<double, double, TC, 0>(s, a, r, z, nullptr);
+            cuda_check(cudaGetLastError(), "composite preconditioner");
+        }
+    }
+
+    // The composite cycle: the fused FP64 fine sweeps of the reference cycle around the stage
+    // levels of the composite grid (solver.cu), in double or (FP32 multigrid) float.  Fine
+    // pre-smoothing as in the reference cycle, the residual written once and gathered into stage
+    // 1, the stage and lattice V-cycle, the weighted prolongation fused into the first post-sweep,
+    // one more post-sweep.
+    void composite_preconditioner(System& s, const double* r, double* z)
+    {
+        if (s.composite_fp32) composite_cycle<float>(s, r, z, s.inter32.empty() ? s.mg32.front() : s.inter32.front());
+        else composite_cycle<double>(s, r, z, s.inter64.empty() ? s.mg64.front() : s.inter64.front());
     }
 
     // Stages of the fused FP64 cycle for component timing: 0 pre-smoothing, 1 residual restriction
@@ -724,7 +800,7 @@ namespace pcfd
         {
             first_sweep_kernel<double><<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(
                 f.code, s.brick_level, f.damping.p, s.diagonal, s.active, r, a, nullptr, s.structured, s.S, 2.0 / 3.0);
-            sweep<double, double, double, false>(s, a, r, z, nullptr);
+            sweep<double, double, double, 0>(s, a, r, z, nullptr);
         }
         else if (stage == 1)
         {
@@ -739,8 +815,8 @@ namespace pcfd
         }
         else
         {
-            sweep<double, double, double, true>(s, z, r, a, base.x.p);
-            sweep<double, double, double, false>(s, a, r, z, nullptr);
+            sweep<double, double, double, 1>(s, z, r, a, base.x.p);
+            sweep<double, double, double, 0>(s, a, r, z, nullptr);
         }
     }
 

@@ -269,6 +269,246 @@ namespace pcfd
     }
 
     // ==================================================================================
+    // composite-grid levels (PCFD_MG_CYCLE_COMPOSITE)
+    // ==================================================================================
+    // The reference aggregates every DOF of a level-l brick straight into its level-0 cell (8^l
+    // fine cells per aggregate on the finest level), so the coarse space misses every scale
+    // between 2 h_l and h_0.  The composite cycle inserts the composite grids of the AMR
+    // hierarchy in between: stage k coarsens the cells of every level above L-k by 2x2x2 into
+    // their ancestors at level L-k and keeps the rest, so stage k is again a composite grid (the
+    // covered bricks of level L-k become its finest bricks) and stage L is the level-0 lattice of
+    // the reference hierarchy.  Stage operators are Galerkin products of the fine orthogonal
+    // operator with the piecewise-constant stage map; the prolongations are weighted (2 for the
+    // stages, as the 2x2x2 Galerkin coarse operator of a uniform Laplacian is twice the
+    // rediscretised one, and 1.3 on the lattice levels).
+    namespace
+    {
+        // the fine orthogonal operator's two-point couplings in the reference traversal order
+        template <class F> void fine_couplings(const pcfd_topology& t, F&& add)
+        {
+            const int bs = t.brick_size, c3 = bs * bs * bs;
+            for (int l = 0; l < t.level_count; ++l)
+            {
+                const pcfd_level& lev = t.levels[l];
+                for (int brick = 0; brick < lev.brick_count; ++brick)
+                {
+                    if (lev.flags[brick] & PCFD_BRICK_COVERED) continue;
+                    for (int c = 0; c < c3; ++c)
+                    {
+                        const int a = lev.level_offset + brick * c3 + c;
+                        if (!t.active[a]) continue;
+                        const int ijk[3] = {c % bs, (c / bs) % bs, c / (bs * bs)};
+                        for (int axis = 0; axis < 3; ++axis)
+                        {
+                            if (t.cut_face_mask[a] & (1u << axis)) continue;
+                            int q[3] = {ijk[0], ijk[1], ijk[2]}, b = -1;
+                            if (++q[axis] < bs) b = lev.level_offset + brick * c3 + (q[2] * bs + q[1]) * bs + q[0];
+                            else
+                            {
+                                const int nb = lev.neighbors[brick * 6 + 2 * axis + 1];
+                                if (nb >= 0 && !(lev.flags[nb] & PCFD_BRICK_COVERED))
+                                {
+                                    q[axis] = 0;
+                                    b = lev.level_offset + nb * c3 + (q[2] * bs + q[1]) * bs + q[0];
+                                }
+                            }
+                            add(a, b, lev.h);
+                        }
+                    }
+                }
+            }
+            for (int e = 0; e < t.coarse_fine.count; ++e)
+                add(t.coarse_fine.coarse_dof[e], t.coarse_fine.fine_dof[e], t.coarse_fine.open_area[e] * connection_factor(t.coarse_fine, e));
+            for (int e = 0; e < t.embedded.count; ++e)
+                add(t.embedded.coarse_dof[e], t.embedded.fine_dof[e], t.embedded.open_area[e] * connection_factor(t.embedded, e));
+            for (int e = 0; e < t.regular.count; ++e)
+                add(t.regular.lower_dof[e], t.regular.upper_dof[e], t.regular.open_area[e] * t.regular.two_point_delta[e]);
+        }
+    }
+
+    void build_composite(System& s, const pcfd_topology& t)
+    {
+        const int L = t.level_count - 1, bs = t.brick_size, c3 = bs * bs * bs, S = t.storage_size;
+        const int32_t* agg = t.preconditioner_aggregate;
+        // every active DOF: level and global cell coordinates at that level (fragments: their
+        // level-0 aggregate cell)
+        std::vector<int8_t> dof_level(size_t(S), -1);
+        std::vector<std::array<int64_t, 3>> gcoord(static_cast<size_t>(S));
+        const pcfd_level& base = t.levels[0];
+        for (int l = 0; l < t.level_count; ++l)
+        {
+            const pcfd_level& lev = t.levels[l];
+            for (int b = 0; b < lev.brick_count; ++b)
+            {
+                if (lev.flags[b] & PCFD_BRICK_COVERED) continue;
+                for (int c = 0; c < c3; ++c)
+                {
+                    const int q = lev.level_offset + b * c3 + c;
+                    if (!t.active[q]) continue;
+                    dof_level[q] = int8_t(l);
+                    gcoord[q] = {int64_t(lev.coord[3 * b]) * bs + c % bs, int64_t(lev.coord[3 * b + 1]) * bs + (c / bs) % bs,
+                            int64_t(lev.coord[3 * b + 2]) * bs + c / (bs * bs)};
+                }
+            }
+        }
+        for (int q = s.structured; q < S; ++q)
+        {
+            if (!t.active[q]) continue;
+            const int cell = agg[q] - s.base_offset;
+            if (cell < 0 || cell >= s.base_cells) continue;
+            const int brick = cell / c3, local = cell % c3;
+            dof_level[q] = 0;
+            gcoord[q] = {int64_t(base.coord[3 * brick]) * bs + local % bs, int64_t(base.coord[3 * brick + 1]) * bs + (local / bs) % bs,
+                    int64_t(base.coord[3 * brick + 2]) * bs + local / (bs * bs)};
+        }
+        auto key = [](int m, int64_t x, int64_t y, int64_t z) {
+            return (uint64_t(m) << 60) | (uint64_t(x & 0xfffff) << 40) | (uint64_t(y & 0xfffff) << 20) | uint64_t(z & 0xfffff);
+        };
+        // stage maps: map[k][q] for k = 1..L (stage L = the reference level-0 aggregate)
+        std::vector<std::vector<int>> map(size_t(L) + 1);
+        std::vector<int> stage_cells(size_t(L) + 1, 0);
+        for (int k = 1; k <= L; ++k)
+        {
+            std::vector<int>& m = map[k];
+            m.assign(size_t(S), -1);
+            if (k == L)
+            {
+                for (int q = 0; q < S; ++q)
+                    if (dof_level[q] >= 0) { const int cell = agg[q] - s.base_offset; if (cell >= 0 && cell < s.base_cells) m[q] = cell; }
+                stage_cells[k] = s.base_cells;
+                continue;
+            }
+            std::unordered_map<uint64_t, int> index;
+            index.reserve(size_t(S) / 2);
+            for (int q = 0; q < S; ++q)
+            {
+                const int l = dof_level[q];
+                if (l < 0) continue;
+                const int level = std::min(l, L - k), shift = l - level;
+                const uint64_t kq = key(level, gcoord[q][0] >> shift, gcoord[q][1] >> shift, gcoord[q][2] >> shift);
+                auto it = index.find(kq);
+                if (it == index.end()) it = index.emplace(kq, int(index.size())).first;
+                m[q] = it->second;
+            }
+            stage_cells[k] = int(index.size());
+        }
+        // Galerkin stage operators through map[k] (sort-based accumulation of the couplings)
+        struct Triple { uint64_t pair; double coefficient; };
+        std::vector<HostLevel> stages(size_t(std::max(0, L - 1)));
+        for (int k = 1; k < L; ++k)
+        {
+            const std::vector<int>& m = map[k];
+            HostLevel& level = stages[size_t(k - 1)];
+            level.cells = stage_cells[k];
+            level.diagonal.assign(size_t(level.cells), 0.0);
+            std::vector<Triple> triples;
+            triples.reserve(size_t(S) * 3 / 2);
+            fine_couplings(t, [&](int a, int b, double c) {
+                if (a < 0 || b < 0 || a == b || !t.active[a] || !t.active[b] || !(c > 0)) return;
+                int ca = m[a], cb = m[b];
+                if (ca < 0 || cb < 0 || ca == cb) return;
+                level.diagonal[ca] += c;
+                level.diagonal[cb] += c;
+                if (ca > cb) std::swap(ca, cb);
+                triples.push_back({(uint64_t(uint32_t(ca)) << 32) | uint32_t(cb), c});
+            });
+            for (int l = 0; l < t.level_count; ++l)
+            {
+                const pcfd_level& lev = t.levels[l];
+                if (!s.outlet) break;
+                for (int b = 0; b < lev.brick_count; ++b)
+                {
+                    if ((lev.flags[b] & PCFD_BRICK_COVERED) || !(lev.flags[b] & PCFD_BRICK_XMAX)) continue;
+                    for (int c = bs - 1; c < c3; c += bs)
+                    {
+                        const int q = lev.level_offset + b * c3 + c;
+                        if (t.active[q] && m[q] >= 0) level.diagonal[m[q]] += 2.0 * lev.h;
+                    }
+                }
+            }
+            for (int gg = 0; gg < t.gauge_count; ++gg)
+            {
+                const int q = t.gauge_dof[gg];
+                if (t.active[q] && m[q] >= 0) level.diagonal[m[q]] += t.gauge_coefficient[gg];
+            }
+            std::sort(triples.begin(), triples.end(), [](const Triple& x, const Triple& y) { return x.pair < y.pair; });
+            for (size_t e = 0; e < triples.size();)
+            {
+                size_t f = e;
+                double c = 0.0;
+                while (f < triples.size() && triples[f].pair == triples[e].pair) c += triples[f++].coefficient;
+                level.edges.push_back({int(triples[e].pair >> 32), int(triples[e].pair & 0xffffffffu), c});
+                e = f;
+            }
+        }
+        // stage k -> stage k + 1 aggregates (consistent for every DOF of a cell) and restriction CSR
+        for (int k = 1; k < L; ++k)
+        {
+            HostLevel& level = stages[size_t(k - 1)];
+            level.aggregate.assign(size_t(level.cells), -1);
+            for (int q = 0; q < S; ++q)
+            {
+                if (map[k][q] < 0) continue;
+                int& a = level.aggregate[map[k][q]];
+                if (a < 0) a = map[k + 1][q];
+                else if (a != map[k + 1][q]) throw Error(PCFD_INTERNAL, "composite stage maps are not nested");
+            }
+            const int next = stage_cells[k + 1];
+            level.restrict_offset.assign(size_t(next) + 1, 0);
+            for (int c = 0; c < level.cells; ++c) if (level.aggregate[c] >= 0) ++level.restrict_offset[level.aggregate[c] + 1];
+            for (int c = 0; c < next; ++c) level.restrict_offset[c + 1] += level.restrict_offset[c];
+            level.restrict_dof.resize(level.restrict_offset.back());
+            std::vector<int> cursor = level.restrict_offset;
+            for (int c = 0; c < level.cells; ++c) if (level.aggregate[c] >= 0) level.restrict_dof[cursor[level.aggregate[c]]++] = c;
+            finalize_level(level);
+        }
+        // fine -> stage 1 map and restriction CSR (DOF order kept); a single-level grid goes
+        // straight to the level-0 lattice
+        if (L < 1)
+        {
+            map.assign(2, std::vector<int>(size_t(S), -1));
+            for (int q = 0; q < S; ++q)
+                if (dof_level[q] >= 0) { const int cell = agg[q] - s.base_offset; if (cell >= 0 && cell < s.base_cells) map[1][q] = cell; }
+            stage_cells.assign(2, s.base_cells);
+        }
+        const std::vector<int>& first = map[1];
+        const int first_cells = stage_cells[1];
+        std::vector<int> roff(size_t(first_cells) + 1, 0), rdof;
+        for (int q = 0; q < S; ++q) if (first[q] >= 0) ++roff[first[q] + 1];
+        for (int c = 0; c < first_cells; ++c) roff[c + 1] += roff[c];
+        rdof.resize(roff.back());
+        {
+            std::vector<int> cursor = roff;
+            for (int q = 0; q < S; ++q) if (first[q] >= 0) rdof[cursor[first[q]]++] = q;
+        }
+        s.fine_map.upload(first);
+        s.fine_restrict_offset.upload(roff);
+        s.fine_restrict_dof.upload(rdof);
+        s.fine_residual.alloc(size_t(S));
+        s.inter64.clear();
+        s.inter32.clear();
+        if (s.composite_fp32)
+        {
+            s.inter32.resize(stages.size());
+            for (size_t k = 0; k < stages.size(); ++k)
+            {
+                upload_level(s.inter32[k], stages[k]);
+                s.inter32[k].prolong = 2.0;
+            }
+        }
+        else
+        {
+            s.inter64.resize(stages.size());
+            for (size_t k = 0; k < stages.size(); ++k)
+            {
+                upload_level(s.inter64[k], stages[k]);
+                s.inter64[k].prolong = 2.0;
+            }
+        }
+        s.composite = true;
+    }
+
+    // ==================================================================================
     // V-cycle kernels
     // ==================================================================================
     namespace
@@ -368,10 +608,13 @@ namespace pcfd
                 for (int q = threadIdx.x; q < cells; q += blockDim.x) x[q] = temporary[q];
         }
 
+        // One V-cycle from chain[index] down: 2 Jacobi sweeps, residual, restriction, the coarser
+        // levels, the weighted prolongation (chain[index]->prolong), 2 sweeps; the last level
+        // takes 96 sweeps (in one CTA when it fits).
         template <class T>
-        void mg_level(System& s, std::vector<MgLevel<T>>& levels, int index)
+        void mg_level(System& s, MgLevel<T>* const* chain, int count, int index)
         {
-            MgLevel<T>& level = levels[index];
+            MgLevel<T>& level = *chain[index];
             const T omega = T(kOmega);
             auto smooth = [&](int sweeps) {
                 for (int sweep = 0; sweep < sweeps; ++sweep)
@@ -382,7 +625,7 @@ namespace pcfd
                     std::swap(level.x.p, level.temporary.p);
                 }
             };
-            if (index + 1 == int(levels.size()))
+            if (index + 1 == count)
             {
                 if (level.cells <= 4096)
                     coarse_jacobi_kernel<T, 4><<<1, 1024, 0, launch_stream(s)>>>(level.rhs, level.x, level.temporary, level.row_offset,
@@ -394,14 +637,57 @@ namespace pcfd
             smooth(2);
             algebraic_residual_kernel<T><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
                 level.rhs, level.x, level.residual, level.row_offset, level.neighbour, level.coefficient, level.diagonal, level.cells);
-            MgLevel<T>& coarse = levels[index + 1];
+            MgLevel<T>& coarse = *chain[index + 1];
             restrict_gather_kernel<T><<<blocks_for(coarse.cells), kThreads, 0, launch_stream(s)>>>(
                 level.restrict_offset, level.restrict_dof, level.residual, coarse.cells, coarse.rhs);
             cuda_check(cudaMemsetAsync(coarse.x, 0, size_t(coarse.cells) * sizeof(T), s.stream), "clear coarse correction");
-            mg_level(s, levels, index + 1);
+            mg_level(s, chain, count, index + 1);
             prolong_add_kernel<T><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(level.aggregate, level.cells, coarse.x, level.x,
-                                                                                             T(s.mg_lattice_scale));
+                                                                                             T(level.prolong));
             smooth(2);
+        }
+
+        template <class T> void mg_level(System& s, std::vector<MgLevel<T>>& levels, int index)
+        {
+            std::vector<MgLevel<T>*> chain;
+            for (MgLevel<T>& level : levels) chain.push_back(&level);
+            mg_level(s, chain.data(), int(chain.size()), index);
+        }
+
+        // Runs mg_level over `chain` through a CUDA graph captured on first use (the chain and its
+        // buffers are fixed for the system's lifetime).
+        template <class T>
+        void run_captured(System& s, std::vector<MgLevel<T>*>& chain, cudaGraphExec_t& exec, int64_t& nodes)
+        {
+            if (!s.stream)
+            {
+                mg_level(s, chain.data(), int(chain.size()), 0);
+                return;
+            }
+            if (!exec)
+            {
+                const int64_t before = s.launches;
+                cuda_check(cudaStreamBeginCapture(s.stream, cudaStreamCaptureModeThreadLocal), "begin hierarchy capture");
+                cudaGraph_t graph = nullptr;
+                try
+                {
+                    mg_level(s, chain.data(), int(chain.size()), 0);
+                }
+                catch (...)
+                {
+                    cudaStreamEndCapture(s.stream, &graph);
+                    if (graph) cudaGraphDestroy(graph);
+                    throw;
+                }
+                cuda_check(cudaStreamEndCapture(s.stream, &graph), "end hierarchy capture");
+                const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+                cudaGraphDestroy(graph);
+                cuda_check(e, "instantiate hierarchy graph");
+                nodes = s.launches - before;
+                s.launches = before;
+            }
+            cuda_check(cudaGraphLaunch(exec, s.stream), "launch hierarchy graph");
+            s.launches += nodes;
         }
 
         template <class T>
@@ -446,44 +732,39 @@ namespace pcfd
     template <class T> void multigrid_levels(System& s, std::vector<MgLevel<T>>& levels)
     {
         const bool fp32 = std::is_same<T, float>::value;
-        cudaGraphExec_t& exec = fp32 ? s.mg_graph32 : s.mg_graph64;
-        int64_t& nodes = fp32 ? s.mg_graph32_launches : s.mg_graph64_launches;
-        if (!s.stream)
+        std::vector<MgLevel<T>*> chain;
+        for (MgLevel<T>& level : levels) chain.push_back(&level);
+        run_captured(s, chain, fp32 ? s.mg_graph32 : s.mg_graph64, fp32 ? s.mg_graph32_launches : s.mg_graph64_launches);
+    }
+
+    // composite chain: the stage levels, then the lattice hierarchy (FP64)
+    void composite_levels(System& s)
+    {
+        if (s.composite_fp32)
         {
-            mg_level(s, levels, 0);
+            std::vector<MgLevel<float>*> chain;
+            for (MgLevel<float>& level : s.inter32) chain.push_back(&level);
+            for (MgLevel<float>& level : s.mg32) chain.push_back(&level);
+            run_captured(s, chain, s.mg_graph_composite, s.mg_graph_composite_launches);
             return;
         }
-        if (!exec)
-        {
-            const int64_t before = s.launches;
-            cuda_check(cudaStreamBeginCapture(s.stream, cudaStreamCaptureModeThreadLocal), "begin hierarchy capture");
-            cudaGraph_t graph = nullptr;
-            try
-            {
-                mg_level(s, levels, 0);
-            }
-            catch (...)
-            {
-                cudaStreamEndCapture(s.stream, &graph);
-                if (graph) cudaGraphDestroy(graph);
-                throw;
-            }
-            cuda_check(cudaStreamEndCapture(s.stream, &graph), "end hierarchy capture");
-            const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
-            cudaGraphDestroy(graph);
-            cuda_check(e, "instantiate hierarchy graph");
-            nodes = s.launches - before;
-            s.launches = before;
-        }
-        cuda_check(cudaGraphLaunch(exec, s.stream), "launch hierarchy graph");
-        s.launches += nodes;
+        std::vector<MgLevel<double>*> chain;
+        for (MgLevel<double>& level : s.inter64) chain.push_back(&level);
+        for (MgLevel<double>& level : s.mg64) chain.push_back(&level);
+        run_captured(s, chain, s.mg_graph_composite, s.mg_graph_composite_launches);
     }
+
     template void multigrid_levels<double>(System&, std::vector<MgLevel<double>>&);
     template void multigrid_levels<float>(System&, std::vector<MgLevel<float>>&);
 
     void apply_preconditioner(System& s, const double* r, double* z)
     {
         ProfileScope scope(s, PCFD_PROFILE_PRECONDITIONER);
+        if (s.composite && s.fine.enabled && aligned16(r) && aligned16(z))
+        {
+            composite_preconditioner(s, r, z);
+            return;
+        }
         if (s.fine.enabled && aligned16(r) && aligned16(z))
         {
             if (s.mg_precision == PCFD_MG_FP32 && !s.mg32.empty()) fine_preconditioner(s, r, z, s.mg32);

@@ -145,3 +145,37 @@ def test_fp32_fused_fine_level_matches_fp64_fine_level(case):
         assert fused.fused_preconditioner
         act = rc.active.astype(bool)
         assert rel(fused.precondition(r), plain.precondition(r), act) <= 1e-5
+
+
+@pytest.mark.parametrize("precision", [MG_FP64, MG_FP32])
+def test_composite_cycle_solves_reference_fixtures(case, precision):
+    """Composite cycle on the reference fixtures (1 and 2 levels: no intermediate stage, the
+    weighted prolongations and the residual-gather restriction)."""
+    rc, _ = case
+    b = np.random.default_rng(31).standard_normal(rc.n) * rc.active
+    with CompositeSystem(rc.topology, mg_cycle=2, mg_precision=precision) as s:
+        x, res = s.solve(b, 1e-8, 600)
+    assert res["converged"], res
+    true = np.linalg.norm((b - rc.apply(x))[rc.active.astype(bool)]) / np.linalg.norm(b)
+    assert true <= 1e-8 * 1.01, (true, res)
+
+
+def test_composite_cycle_on_three_level_wing_halves_iterations():
+    """3-level wing grid (one intermediate composite stage): the composite cycle converges to
+    1e-8 on the oracle's operator in markedly fewer iterations than the reference cycle."""
+    from paracfd_b200.workloads import WORKLOADS
+    built = WORKLOADS["paraglider1m"].build()
+    oracle = port.PortSystem(built.topology)
+    act = built.active.astype(bool)
+    b = oracle.apply(np.where(act, np.random.default_rng(37).standard_normal(built.storage_size), 0.0))
+    its = {}
+    for cycle, precision in ((0, MG_FP64), (2, MG_FP64), (3, MG_FP32)):
+        with CompositeSystem(built.topology, mg_cycle=min(cycle, 2), mg_precision=precision) as s:
+            x, res = s.solve(b, 1e-8, 600)
+        assert res["converged"], (cycle, res)
+        true = np.linalg.norm((b - oracle.apply(x))[act]) / np.linalg.norm(b[act])
+        assert true <= 1e-8 * 1.01, (cycle, true)
+        its[cycle] = res["iterations"]
+    oracle.close()
+    built.close()
+    assert its[2] <= 0.8 * its[0] and its[3] <= 0.8 * its[0], its
