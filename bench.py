@@ -48,6 +48,7 @@ def parse_args():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", default="paraglider16m")
     ap.add_argument("--mg", choices=("fp64", "fp32"), default="fp64", help="multigrid preconditioner precision")
+    ap.add_argument("--restart", type=int, default=0, help="GCRO columns per cycle (0: the reference's 24)")
     ap.add_argument("--mg-cycle", choices=("reference", "corrected", "composite"), default="composite",
                     help="coarse-correction weighting of the multigrid cycle (pcfd_mg_cycle)")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU sample of the ours arm")
@@ -62,20 +63,24 @@ def parse_args():
 
 # ------------------------------------------------------------------------------------------ ranks
 class Ranks:
-    """One process per GPU; NCCL only for the barrier and the max over ranks."""
+    """One process per GPU; the collective (NCCL on GPUs, gloo for the CPU tests) only carries the
+    barrier and the max over ranks -- the replicas share no data."""
 
-    def __init__(self, collective: bool):
+    def __init__(self, collective: bool, backend: str = "nccl"):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.dist = None
+        self.device = "cpu"
         if self.world > 1 and collective:
             import datetime
 
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+                self.device = f"cuda:{self.local}"
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
             self.dist, self.torch = dist, torch
 
     def barrier(self):
@@ -85,13 +90,19 @@ class Ranks:
     def max(self, value: float) -> float:
         if not self.dist:
             return value
-        t = self.torch.tensor([value], dtype=self.torch.float64, device=f"cuda:{self.local}")
+        t = self.torch.tensor([value], dtype=self.torch.float64, device=self.device)
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return float(t.item())
 
     def close(self):
         if self.dist:
             self.dist.destroy_process_group()
+
+
+def replica_throughput(world: int, steps: int, slowest_ms: float) -> float:
+    """Whole-job steps/s of `world` independent replicas that each ran `steps` steps, timed by the
+    slowest rank (weak scaling: per-GPU work fixed)."""
+    return world * steps / (slowest_ms * 1e-3)
 
 
 # ------------------------------------------------------------------------------------------ clocks
@@ -284,7 +295,8 @@ def run_ours(args, ranks: Ranks):
     built = spec.build()
     bricks = non_covered_bricks(built.topology)
     system = CompositeSystem(built.topology, MG_FP32 if args.mg == "fp32" else MG_FP64, device=ranks.local,
-                             mg_cycle={"reference": 0, "corrected": 1, "composite": 2}[args.mg_cycle])
+                             mg_cycle={"reference": 0, "corrected": 1, "composite": 2}[args.mg_cycle],
+                             gmres_restart=args.restart)
     system.configure(speed=spec.speed, **spec.case)
     slots = system.inflow_layout()
     faces = len(slots) * spec.brick_size ** 2
@@ -351,7 +363,7 @@ def run_ours(args, ranks: Ranks):
             pass
 
     n = ranks.world
-    value = n * args.steps / (elapsed_ms * 1e-3)
+    value = replica_throughput(n, args.steps, elapsed_ms)
     peak, peak_kind = measured_peak_gbs()
     region_names = {0: "brick_pipe_kernel<2> (FP64 structured 7-point operator)", 1: "MG preconditioner application"}
     roofline = None
@@ -371,7 +383,8 @@ def run_ours(args, ranks: Ranks):
         "ms_per_step": round(elapsed_ms / args.steps, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 state / f64 pressure", "data": "synthetic analytic geometry",
         "config": dict(spec.describe(), leaf_cells=built.leaf_cells, storage=built.storage_size,
-                       mg=args.mg, mg_cycle=args.mg_cycle, parallelism=f"replicas{n}", l2="inputs larger than L2"),
+                       mg=args.mg, mg_cycle=args.mg_cycle, gcro_restart=args.restart or 24, parallelism=f"replicas{n}",
+                       l2="inputs larger than L2"),
         "projection_ms": round(statistics.mean(s["projection_ms"] for s in stats), 3),
         "iterations_per_step": round(statistics.mean(s["pressure"]["iterations"] for s in stats), 2),
         "final_residual_max": max(s["pressure"]["relative_residual"] for s in stats),
@@ -417,7 +430,8 @@ def run_kernel_only(args):
     spec = WORKLOADS[args.workload]
     built = spec.build()
     system = CompositeSystem(built.topology, MG_FP32 if args.mg == "fp32" else MG_FP64,
-                             mg_cycle={"reference": 0, "corrected": 1, "composite": 2}[args.mg_cycle])
+                             mg_cycle={"reference": 0, "corrected": 1, "composite": 2}[args.mg_cycle],
+                             gmres_restart=args.restart)
     ms = system.time_kernel(args.kernel_only, args.kernel_iterations)
     line = {"kernel_only": args.kernel_only, "workload": args.workload, "ms_per_launch": ms,
             "iterations": args.kernel_iterations, "launches": system.launch_count()}

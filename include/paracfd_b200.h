@@ -173,6 +173,7 @@ typedef struct pcfd_options {
     int32_t disable_fused_smoother;  /* 1: run the preconditioner's fine level as separate
                                         operator/vector launches (same sweeps, reference order) */
     int32_t mg_cycle;                /* pcfd_mg_cycle */
+    int32_t gmres_restart;           /* columns per GCRO/LGMRES cycle, 1..24; 0: the reference's 24 */
 } pcfd_options;
 
 /* Coarse-correction weighting of the multigrid cycle.  The aggregation coarse operators are

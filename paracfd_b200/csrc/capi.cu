@@ -199,6 +199,11 @@ namespace pcfd
             const std::vector<double> diag = host_diagonal(t);
             s.diagonal.upload(diag);
             build_operator(s, t);
+            if (options && options->gmres_restart)
+            {
+                require(options->gmres_restart > 0 && options->gmres_restart <= System::gmres_restart, "gmres_restart must be 0..24");
+                s.restart = options->gmres_restart;
+            }
             const int cycle = options ? options->mg_cycle : PCFD_MG_CYCLE_REFERENCE;
             require(cycle >= PCFD_MG_CYCLE_REFERENCE && cycle <= PCFD_MG_CYCLE_COMPOSITE, "unknown multigrid cycle");
             if (cycle == PCFD_MG_CYCLE_CORRECTED) { s.mg_prolong_scale = 2.0; s.mg_lattice_scale = 1.5; }

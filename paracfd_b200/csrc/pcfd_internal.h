@@ -214,7 +214,8 @@ namespace pcfd
         DBuf<double> r, z, dvec, Ad, t, correction, defect, scratch_p, scratch_out;
         DBuf<double> gmres_v, gmres_z, recycle_u, recycle_c;
         int recycle_count = 0;
-        static constexpr int gmres_restart = 24;
+        static constexpr int gmres_restart = 24;   // the reference's LGMRES(24) (storage and default)
+        int restart = gmres_restart;               // columns per cycle actually used (<= gmres_restart)
         static constexpr int recycle_capacity = 3;
         DBuf<double> dot_partial;               // reduction scratch
         DBuf<double> block_partial;             // [592][kMaxSet + 1] block-kernel partial sums

@@ -899,7 +899,7 @@ namespace pcfd
             double residual2 = true_residual();
             result.relative_residual = std::sqrt(residual2 / rhs2);
             if (result.relative_residual <= tolerance) { result.converged = 1; return result; }
-            const int R = System::gmres_restart;
+            const int R = s.restart;
             while (result.iterations < max_iterations)
             {
                 // minimise over the recycled space first; accept only if the true residual agrees
