@@ -51,6 +51,8 @@ def parse_args():
     ap.add_argument("--restart", type=int, default=0, help="GCRO columns per cycle (0: the reference's 24)")
     ap.add_argument("--mg-cycle", choices=("reference", "corrected", "composite"), default="composite",
                     help="coarse-correction weighting of the multigrid cycle (pcfd_mg_cycle)")
+    ap.add_argument("--stage-sweeps", type=int, default=0,
+                    help="composite cycle: Jacobi sweeps per stage before and after its correction (0: 4)")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU sample of the ours arm")
     ap.add_argument("--no-reference-gpu", action="store_true", help="reference arm: skip the sm_100a reference run")
     ap.add_argument("--profile-region", type=int, default=0, help="PCFD_PROFILE_* region timed per launch")
@@ -296,7 +298,7 @@ def run_ours(args, ranks: Ranks):
     bricks = non_covered_bricks(built.topology)
     system = CompositeSystem(built.topology, MG_FP32 if args.mg == "fp32" else MG_FP64, device=ranks.local,
                              mg_cycle={"reference": 0, "corrected": 1, "composite": 2}[args.mg_cycle],
-                             gmres_restart=args.restart)
+                             gmres_restart=args.restart, mg_stage_sweeps=args.stage_sweeps)
     system.configure(speed=spec.speed, **spec.case)
     slots = system.inflow_layout()
     faces = len(slots) * spec.brick_size ** 2
@@ -383,7 +385,8 @@ def run_ours(args, ranks: Ranks):
         "ms_per_step": round(elapsed_ms / args.steps, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 state / f64 pressure", "data": "synthetic analytic geometry",
         "config": dict(spec.describe(), leaf_cells=built.leaf_cells, storage=built.storage_size,
-                       mg=args.mg, mg_cycle=args.mg_cycle, gcro_restart=args.restart or 24, parallelism=f"replicas{n}",
+                       mg=args.mg, mg_cycle=args.mg_cycle, gcro_restart=args.restart or 24,
+                       stage_sweeps=args.stage_sweeps or 4, parallelism=f"replicas{n}",
                        l2="inputs larger than L2"),
         "projection_ms": round(statistics.mean(s["projection_ms"] for s in stats), 3),
         "iterations_per_step": round(statistics.mean(s["pressure"]["iterations"] for s in stats), 2),
@@ -431,7 +434,7 @@ def run_kernel_only(args):
     built = spec.build()
     system = CompositeSystem(built.topology, MG_FP32 if args.mg == "fp32" else MG_FP64,
                              mg_cycle={"reference": 0, "corrected": 1, "composite": 2}[args.mg_cycle],
-                             gmres_restart=args.restart)
+                             gmres_restart=args.restart, mg_stage_sweeps=args.stage_sweeps)
     ms = system.time_kernel(args.kernel_only, args.kernel_iterations)
     line = {"kernel_only": args.kernel_only, "workload": args.workload, "ms_per_launch": ms,
             "iterations": args.kernel_iterations, "launches": system.launch_count()}

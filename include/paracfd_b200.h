@@ -174,6 +174,8 @@ typedef struct pcfd_options {
                                         operator/vector launches (same sweeps, reference order) */
     int32_t mg_cycle;                /* pcfd_mg_cycle */
     int32_t gmres_restart;           /* columns per GCRO/LGMRES cycle, 1..24; 0: the reference's 24 */
+    int32_t mg_stage_sweeps;         /* composite cycle: Jacobi sweeps before and after each stage's
+                                        coarse correction, 1..16; 0: 4 */
 } pcfd_options;
 
 /* Coarse-correction weighting of the multigrid cycle.  The aggregation coarse operators are

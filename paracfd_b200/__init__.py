@@ -74,11 +74,11 @@ class CompositeSystem:
 
     def __init__(self, topology: Topology, mg_precision: int = MG_FP64, device: int = 0,
                  momentum_min_volume_fraction: float = 0.0, fused_smoother: bool = True,
-                 mg_cycle: int = 0, gmres_restart: int = 0):
+                 mg_cycle: int = 0, gmres_restart: int = 0, mg_stage_sweeps: int = 0):
         self._lib = capi.load()
         self._topology = topology   # keep the caller's arrays alive during creation
         opts = Options(mg_precision, device, None, momentum_min_volume_fraction, 0 if fused_smoother else 1, mg_cycle,
-                       gmres_restart)
+                       gmres_restart, mg_stage_sweeps)
         handle = C.c_void_p()
         check(self._lib.pcfd_system_create(C.byref(topology), C.byref(opts), C.byref(handle)))
         self.handle = handle

@@ -204,10 +204,15 @@ namespace pcfd
                 require(options->gmres_restart > 0 && options->gmres_restart <= System::gmres_restart, "gmres_restart must be 0..24");
                 s.restart = options->gmres_restart;
             }
+            if (options && options->mg_stage_sweeps)
+            {
+                require(options->mg_stage_sweeps > 0 && options->mg_stage_sweeps <= 16, "mg_stage_sweeps must be 0..16");
+                s.mg_stage_sweeps = options->mg_stage_sweeps;
+            }
             const int cycle = options ? options->mg_cycle : PCFD_MG_CYCLE_REFERENCE;
             require(cycle >= PCFD_MG_CYCLE_REFERENCE && cycle <= PCFD_MG_CYCLE_COMPOSITE, "unknown multigrid cycle");
             if (cycle == PCFD_MG_CYCLE_CORRECTED) { s.mg_prolong_scale = 2.0; s.mg_lattice_scale = 1.5; }
-            if (cycle == PCFD_MG_CYCLE_COMPOSITE) { s.mg_prolong_scale = 2.0; s.mg_lattice_scale = 1.3; }
+            if (cycle == PCFD_MG_CYCLE_COMPOSITE) s.mg_prolong_scale = 2.0;
             build_multigrid(s, t, diag);
             for (MgLevel<double>& level : s.mg64) level.prolong = s.mg_lattice_scale;
             for (MgLevel<float>& level : s.mg32) level.prolong = s.mg_lattice_scale;

@@ -107,6 +107,7 @@ namespace pcfd
         DBuf<int> row_offset, neighbour, aggregate, restrict_offset, restrict_dof;
         DBuf<T> coefficient, diagonal, rhs, x, temporary, residual;
         double prolong = 1.0;                   // weight of the next level's correction added here
+        int sweeps = 2;                         // Jacobi sweeps before and after the coarse correction
     };
 
     struct Scalars;   // device scalar block for the Krylov recurrences
@@ -167,6 +168,7 @@ namespace pcfd
         bool outlet = true, full_nonorthogonal = false;
         int mg_precision = PCFD_MG_FP64;
         double mg_prolong_scale = 1.0, mg_lattice_scale = 1.0;   // coarse-correction weights (pcfd_mg_cycle)
+        int mg_stage_sweeps = 4;                                 // composite-stage sweeps (pcfd_options)
         cudaStream_t stream = nullptr;
         bool own_stream = false;
         int device = 0;
@@ -197,8 +199,8 @@ namespace pcfd
         DBuf<int> base_restrict_offset, base_restrict_dof;
         std::vector<MgLevel<double>> mg64;
         std::vector<MgLevel<float>> mg32;
-        // composite cycle (PCFD_MG_CYCLE_COMPOSITE): Galerkin levels of the AMR composite grid with
-        // the finest level coarsened 2x2x2 one level at a time, above the lattice hierarchy
+        // composite cycle (PCFD_MG_CYCLE_COMPOSITE): Galerkin stages of the AMR composite grid, every
+        // level coarsened 2x2x2 per stage; the last stage is the coarsest
         bool composite = false;
         std::vector<MgLevel<double>> inter64;
         std::vector<MgLevel<float>> inter32;    // the same stages in float (FP32 multigrid)
@@ -207,7 +209,7 @@ namespace pcfd
         FineSmoother fine;
         cudaGraphExec_t mg_graph64 = nullptr, mg_graph32 = nullptr, mg_graph_composite = nullptr;   // captured hierarchies
         int64_t mg_graph64_launches = 0, mg_graph32_launches = 0, mg_graph_composite_launches = 0;
-        bool composite_fp32 = false;            // composite stages + lattice in float
+        bool composite_fp32 = false;            // composite stages in float
         DBuf<float> diagonal32;
 
         // Krylov vectors

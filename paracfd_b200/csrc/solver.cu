@@ -273,14 +273,14 @@ namespace pcfd
     // ==================================================================================
     // The reference aggregates every DOF of a level-l brick straight into its level-0 cell (8^l
     // fine cells per aggregate on the finest level), so the coarse space misses every scale
-    // between 2 h_l and h_0.  The composite cycle inserts the composite grids of the AMR
-    // hierarchy in between: stage k coarsens the cells of every level above L-k by 2x2x2 into
-    // their ancestors at level L-k and keeps the rest, so stage k is again a composite grid (the
-    // covered bricks of level L-k become its finest bricks) and stage L is the level-0 lattice of
-    // the reference hierarchy.  Stage operators are Galerkin products of the fine orthogonal
-    // operator with the piecewise-constant stage map; the prolongations are weighted (2 for the
-    // stages, as the 2x2x2 Galerkin coarse operator of a uniform Laplacian is twice the
-    // rediscretised one, and 1.3 on the lattice levels).
+    // between 2 h_l and h_0.  The composite cycle replaces that hierarchy with stages that
+    // coarsen every AMR level by 2x2x2 at once: stage k holds one cell per 2^k x 2^k x 2^k block
+    // of same-level cells (cells of different levels never merge; the levels stay coupled
+    // through the Galerkin coarse-fine couplings), down to 512 cells or fewer.  Stage operators
+    // are Galerkin products of the fine orthogonal operator with the piecewise-constant stage
+    // map; every prolongation is weighted 2, as the 2x2x2 Galerkin coarse operator of a uniform
+    // Laplacian is twice the rediscretised one.  Each stage takes mg_stage_sweeps damped-Jacobi
+    // sweeps before and after its coarse correction, the coarsest 96.
     namespace
     {
         // the fine orthogonal operator's two-point couplings in the reference traversal order
@@ -328,13 +328,11 @@ namespace pcfd
 
     void build_composite(System& s, const pcfd_topology& t)
     {
-        const int L = t.level_count - 1, bs = t.brick_size, c3 = bs * bs * bs, S = t.storage_size;
-        const int32_t* agg = t.preconditioner_aggregate;
-        // every active DOF: level and global cell coordinates at that level (fragments: their
-        // level-0 aggregate cell)
+        const int bs = t.brick_size, c3 = bs * bs * bs, S = t.storage_size;
+        // every active structured DOF: level and global cell coordinates at that level (the EB
+        // fragments stay out of the stages: the fine sweeps alone smooth them)
         std::vector<int8_t> dof_level(size_t(S), -1);
         std::vector<std::array<int64_t, 3>> gcoord(static_cast<size_t>(S));
-        const pcfd_level& base = t.levels[0];
         for (int l = 0; l < t.level_count; ++l)
         {
             const pcfd_level& lev = t.levels[l];
@@ -351,58 +349,47 @@ namespace pcfd
                 }
             }
         }
-        for (int q = s.structured; q < S; ++q)
-        {
-            if (!t.active[q]) continue;
-            const int cell = agg[q] - s.base_offset;
-            if (cell < 0 || cell >= s.base_cells) continue;
-            const int brick = cell / c3, local = cell % c3;
-            dof_level[q] = 0;
-            gcoord[q] = {int64_t(base.coord[3 * brick]) * bs + local % bs, int64_t(base.coord[3 * brick + 1]) * bs + (local / bs) % bs,
-                    int64_t(base.coord[3 * brick + 2]) * bs + local / (bs * bs)};
-        }
         auto key = [](int m, int64_t x, int64_t y, int64_t z) {
             return (uint64_t(m) << 60) | (uint64_t(x & 0xfffff) << 40) | (uint64_t(y & 0xfffff) << 20) | uint64_t(z & 0xfffff);
         };
-        // stage maps: map[k][q] for k = 1..L (stage L = the reference level-0 aggregate)
-        std::vector<std::vector<int>> map(size_t(L) + 1);
-        std::vector<int> stage_cells(size_t(L) + 1, 0);
-        for (int k = 1; k <= L; ++k)
+        // stage maps: stage k merges the level-l cells at global cell coordinates g into the cell
+        // (l, g >> k) of the same level, so the maps nest (stage k -> k + 1 halves every index);
+        // stages stop at 512 cells or when a coarsening no longer shrinks the grid
+        std::vector<std::vector<int>> map;
+        std::vector<int> stage_cells;
+        for (int k = 1; k <= 16; ++k)
         {
-            std::vector<int>& m = map[k];
-            m.assign(size_t(S), -1);
-            if (k == L)
-            {
-                for (int q = 0; q < S; ++q)
-                    if (dof_level[q] >= 0) { const int cell = agg[q] - s.base_offset; if (cell >= 0 && cell < s.base_cells) m[q] = cell; }
-                stage_cells[k] = s.base_cells;
-                continue;
-            }
+            std::vector<int> m(size_t(S), -1);
             std::unordered_map<uint64_t, int> index;
-            index.reserve(size_t(S) / 2);
+            index.reserve(stage_cells.empty() ? size_t(S) / 6 : size_t(stage_cells.back()) / 6 + 16);
             for (int q = 0; q < S; ++q)
             {
                 const int l = dof_level[q];
                 if (l < 0) continue;
-                const int level = std::min(l, L - k), shift = l - level;
-                const uint64_t kq = key(level, gcoord[q][0] >> shift, gcoord[q][1] >> shift, gcoord[q][2] >> shift);
+                const uint64_t kq = key(l, gcoord[q][0] >> k, gcoord[q][1] >> k, gcoord[q][2] >> k);
                 auto it = index.find(kq);
                 if (it == index.end()) it = index.emplace(kq, int(index.size())).first;
                 m[q] = it->second;
             }
-            stage_cells[k] = int(index.size());
+            const int cells = int(index.size());
+            if (cells == 0 || (!stage_cells.empty() && cells >= stage_cells.back())) break;
+            map.push_back(std::move(m));
+            stage_cells.push_back(cells);
+            if (cells <= 512) break;
         }
+        if (map.empty()) throw Error(PCFD_INTERNAL, "composite cycle: no active structured cells");
+        const int K = int(map.size());
         // Galerkin stage operators through map[k] (sort-based accumulation of the couplings)
         struct Triple { uint64_t pair; double coefficient; };
-        std::vector<HostLevel> stages(size_t(std::max(0, L - 1)));
-        for (int k = 1; k < L; ++k)
+        std::vector<HostLevel> stages(static_cast<size_t>(K));
+        for (int k = 0; k < K; ++k)
         {
             const std::vector<int>& m = map[k];
-            HostLevel& level = stages[size_t(k - 1)];
+            HostLevel& level = stages[size_t(k)];
             level.cells = stage_cells[k];
             level.diagonal.assign(size_t(level.cells), 0.0);
             std::vector<Triple> triples;
-            triples.reserve(size_t(S) * 3 / 2);
+            triples.reserve(k == 0 ? size_t(S) * 3 / 2 : size_t(stage_cells[0]) * 3);
             fine_couplings(t, [&](int a, int b, double c) {
                 if (a < 0 || b < 0 || a == b || !t.active[a] || !t.active[b] || !(c > 0)) return;
                 int ca = m[a], cb = m[b];
@@ -441,38 +428,34 @@ namespace pcfd
                 e = f;
             }
         }
-        // stage k -> stage k + 1 aggregates (consistent for every DOF of a cell) and restriction CSR
-        for (int k = 1; k < L; ++k)
+        // stage k -> stage k + 1 aggregates (consistent for every DOF of a cell) and restriction
+        // CSR; the last stage is the coarsest and keeps none
+        for (int k = 0; k < K; ++k)
         {
-            HostLevel& level = stages[size_t(k - 1)];
-            level.aggregate.assign(size_t(level.cells), -1);
-            for (int q = 0; q < S; ++q)
+            HostLevel& level = stages[size_t(k)];
+            if (k + 1 < K)
             {
-                if (map[k][q] < 0) continue;
-                int& a = level.aggregate[map[k][q]];
-                if (a < 0) a = map[k + 1][q];
-                else if (a != map[k + 1][q]) throw Error(PCFD_INTERNAL, "composite stage maps are not nested");
+                level.aggregate.assign(size_t(level.cells), -1);
+                for (int q = 0; q < S; ++q)
+                {
+                    if (map[k][q] < 0) continue;
+                    int& a = level.aggregate[map[k][q]];
+                    if (a < 0) a = map[k + 1][q];
+                    else if (a != map[k + 1][q]) throw Error(PCFD_INTERNAL, "composite stage maps are not nested");
+                }
+                const int next = stage_cells[k + 1];
+                level.restrict_offset.assign(size_t(next) + 1, 0);
+                for (int c = 0; c < level.cells; ++c) if (level.aggregate[c] >= 0) ++level.restrict_offset[level.aggregate[c] + 1];
+                for (int c = 0; c < next; ++c) level.restrict_offset[c + 1] += level.restrict_offset[c];
+                level.restrict_dof.resize(level.restrict_offset.back());
+                std::vector<int> cursor = level.restrict_offset;
+                for (int c = 0; c < level.cells; ++c) if (level.aggregate[c] >= 0) level.restrict_dof[cursor[level.aggregate[c]]++] = c;
             }
-            const int next = stage_cells[k + 1];
-            level.restrict_offset.assign(size_t(next) + 1, 0);
-            for (int c = 0; c < level.cells; ++c) if (level.aggregate[c] >= 0) ++level.restrict_offset[level.aggregate[c] + 1];
-            for (int c = 0; c < next; ++c) level.restrict_offset[c + 1] += level.restrict_offset[c];
-            level.restrict_dof.resize(level.restrict_offset.back());
-            std::vector<int> cursor = level.restrict_offset;
-            for (int c = 0; c < level.cells; ++c) if (level.aggregate[c] >= 0) level.restrict_dof[cursor[level.aggregate[c]]++] = c;
             finalize_level(level);
         }
-        // fine -> stage 1 map and restriction CSR (DOF order kept); a single-level grid goes
-        // straight to the level-0 lattice
-        if (L < 1)
-        {
-            map.assign(2, std::vector<int>(size_t(S), -1));
-            for (int q = 0; q < S; ++q)
-                if (dof_level[q] >= 0) { const int cell = agg[q] - s.base_offset; if (cell >= 0 && cell < s.base_cells) map[1][q] = cell; }
-            stage_cells.assign(2, s.base_cells);
-        }
-        const std::vector<int>& first = map[1];
-        const int first_cells = stage_cells[1];
+        // fine -> stage 1 map and restriction CSR (DOF order kept)
+        const std::vector<int>& first = map[0];
+        const int first_cells = stage_cells[0];
         std::vector<int> roff(size_t(first_cells) + 1, 0), rdof;
         for (int q = 0; q < S; ++q) if (first[q] >= 0) ++roff[first[q] + 1];
         for (int c = 0; c < first_cells; ++c) roff[c + 1] += roff[c];
@@ -494,6 +477,7 @@ namespace pcfd
             {
                 upload_level(s.inter32[k], stages[k]);
                 s.inter32[k].prolong = 2.0;
+                s.inter32[k].sweeps = s.mg_stage_sweeps;
             }
         }
         else
@@ -503,6 +487,7 @@ namespace pcfd
             {
                 upload_level(s.inter64[k], stages[k]);
                 s.inter64[k].prolong = 2.0;
+                s.inter64[k].sweeps = s.mg_stage_sweeps;
             }
         }
         s.composite = true;
@@ -608,9 +593,9 @@ namespace pcfd
                 for (int q = threadIdx.x; q < cells; q += blockDim.x) x[q] = temporary[q];
         }
 
-        // One V-cycle from chain[index] down: 2 Jacobi sweeps, residual, restriction, the coarser
-        // levels, the weighted prolongation (chain[index]->prolong), 2 sweeps; the last level
-        // takes 96 sweeps (in one CTA when it fits).
+        // One V-cycle from chain[index] down: level.sweeps Jacobi sweeps, residual, restriction,
+        // the coarser levels, the weighted prolongation (chain[index]->prolong), level.sweeps
+        // sweeps; the last level takes 96 sweeps (in one CTA when it fits).
         template <class T>
         void mg_level(System& s, MgLevel<T>* const* chain, int count, int index)
         {
@@ -634,7 +619,7 @@ namespace pcfd
                     smooth(96);
                 return;
             }
-            smooth(2);
+            smooth(level.sweeps);
             algebraic_residual_kernel<T><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
                 level.rhs, level.x, level.residual, level.row_offset, level.neighbour, level.coefficient, level.diagonal, level.cells);
             MgLevel<T>& coarse = *chain[index + 1];
@@ -644,7 +629,7 @@ namespace pcfd
             mg_level(s, chain, count, index + 1);
             prolong_add_kernel<T><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(level.aggregate, level.cells, coarse.x, level.x,
                                                                                              T(level.prolong));
-            smooth(2);
+            smooth(level.sweeps);
         }
 
         template <class T> void mg_level(System& s, std::vector<MgLevel<T>>& levels, int index)
@@ -737,20 +722,18 @@ namespace pcfd
         run_captured(s, chain, fp32 ? s.mg_graph32 : s.mg_graph64, fp32 ? s.mg_graph32_launches : s.mg_graph64_launches);
     }
 
-    // composite chain: the stage levels, then the lattice hierarchy (FP64)
+    // composite chain: the stage levels (FP32 or FP64), the last one the coarsest
     void composite_levels(System& s)
     {
         if (s.composite_fp32)
         {
             std::vector<MgLevel<float>*> chain;
             for (MgLevel<float>& level : s.inter32) chain.push_back(&level);
-            for (MgLevel<float>& level : s.mg32) chain.push_back(&level);
             run_captured(s, chain, s.mg_graph_composite, s.mg_graph_composite_launches);
             return;
         }
         std::vector<MgLevel<double>*> chain;
         for (MgLevel<double>& level : s.inter64) chain.push_back(&level);
-        for (MgLevel<double>& level : s.mg64) chain.push_back(&level);
         run_captured(s, chain, s.mg_graph_composite, s.mg_graph_composite_launches);
     }
 
