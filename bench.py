@@ -52,7 +52,7 @@ def parse_args():
     ap.add_argument("--mg-cycle", choices=("reference", "corrected", "composite"), default="composite",
                     help="coarse-correction weighting of the multigrid cycle (pcfd_mg_cycle)")
     ap.add_argument("--stage-sweeps", type=int, default=0,
-                    help="composite cycle: Jacobi sweeps per stage before and after its correction (0: 4)")
+                    help="composite cycle: Jacobi sweeps per stage before and after its correction (0: 6)")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU sample of the ours arm")
     ap.add_argument("--no-reference-gpu", action="store_true", help="reference arm: skip the sm_100a reference run")
     ap.add_argument("--profile-region", type=int, default=0, help="PCFD_PROFILE_* region timed per launch")
@@ -386,7 +386,7 @@ def run_ours(args, ranks: Ranks):
         "vs_baseline": None, "dtype": "f32 state / f64 pressure", "data": "synthetic analytic geometry",
         "config": dict(spec.describe(), leaf_cells=built.leaf_cells, storage=built.storage_size,
                        mg=args.mg, mg_cycle=args.mg_cycle, gcro_restart=args.restart or 24,
-                       stage_sweeps=args.stage_sweeps or 4, parallelism=f"replicas{n}",
+                       stage_sweeps=args.stage_sweeps or 6, parallelism=f"replicas{n}",
                        l2="inputs larger than L2"),
         "projection_ms": round(statistics.mean(s["projection_ms"] for s in stats), 3),
         "iterations_per_step": round(statistics.mean(s["pressure"]["iterations"] for s in stats), 2),

@@ -175,7 +175,7 @@ typedef struct pcfd_options {
     int32_t mg_cycle;                /* pcfd_mg_cycle */
     int32_t gmres_restart;           /* columns per GCRO/LGMRES cycle, 1..24; 0: the reference's 24 */
     int32_t mg_stage_sweeps;         /* composite cycle: Jacobi sweeps before and after each stage's
-                                        coarse correction, 1..16; 0: 4 */
+                                        coarse correction, 1..16; 0: 6 */
 } pcfd_options;
 
 /* Coarse-correction weighting of the multigrid cycle.  The aggregation coarse operators are
@@ -189,13 +189,13 @@ typedef struct pcfd_options {
 typedef enum pcfd_mg_cycle {
     PCFD_MG_CYCLE_REFERENCE = 0,     /* the reference's cycle (amr_pressure.cu:1103-1154) */
     PCFD_MG_CYCLE_CORRECTED = 1,     /* over-corrected prolongation */
-    PCFD_MG_CYCLE_COMPOSITE = 2      /* composite-grid stages between the fine level and the level-0
-                                        lattice (each coarsens the finest remaining AMR level 2x2x2,
-                                        Galerkin operators), prolongations weighted 2 (stages) and 1.3
-                                        (lattice): about half the iterations of the reference cycle on
-                                        the 4-level 16 M-cell wing grid.  Needs 8^3 bricks and the fused
-                                        fine level; with the FP32 multigrid the stages and the lattice
-                                        levels are float, the fine sweeps stay FP64. */
+    PCFD_MG_CYCLE_COMPOSITE = 2      /* composite-grid stages instead of the level-0 lattice: stage k
+                                        holds one cell per 2^k-wide block of same-level cells of every
+                                        AMR level (Galerkin operators, prolongations weighted 2,
+                                        mg_stage_sweeps sweeps per stage, down to 512 cells): 2.8x
+                                        fewer iterations than the reference cycle on the 4-level 16 M-cell
+                                        wing grid.  Needs 8^3 bricks and the fused fine level; with the
+                                        FP32 multigrid the stages are float, the fine sweeps stay FP64. */
 } pcfd_mg_cycle;
 
 /* AmrGpuSolveResult (amr_pressure.h:337-351), trimmed to what the solver reports. */
