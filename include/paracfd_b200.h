@@ -414,6 +414,43 @@ pcfd_status pcfd_launch_count(pcfd_system* system, int64_t* launches);
 pcfd_status pcfd_profile_begin(pcfd_system* system, int32_t region, int32_t capacity);
 pcfd_status pcfd_profile_end(pcfd_system* system, double* ms_per_launch, int32_t capacity, int32_t* launches);
 
+/* ---- learned preconditioner (no reference counterpart) ------------------------------
+ * A brick-local 3-D U-Net (8^3/4^3/2^3 levels, 16/32/64 channels, 3x3x3 BF16 tensor-core
+ * convolutions with FP32 accumulation, ReLU, 1x1x1 head) maps D^-1 r / s and the active mask
+ * of every non-covered brick to z / s (s = RMS of D^-1 r over the brick's active cells); the DOFs
+ * after the structured slots (EB fragments) take one damped Jacobi step.  It is trained on
+ * (r, multigrid preconditioner output) brick pairs that the solver harvests from its own
+ * preconditioner calls.  The definition is oracle/unet.py; parameters are FP32 in the flat order
+ * enc0, enc1, bottleneck, dec1 (up, skip), dec0 (up, skip) ([27][cout][cin] each), head [16]. */
+typedef enum pcfd_preconditioner {
+    PCFD_PRECONDITIONER_MULTIGRID = 0,   /* the multigrid V-cycle of pcfd_options (default) */
+    PCFD_PRECONDITIONER_LEARNED = 1,     /* the U-Net; solves run under flexible GCRO/LGMRES */
+    PCFD_PRECONDITIONER_JACOBI = 2       /* z = D^-1 r, the method without the network or the V-cycle */
+} pcfd_preconditioner;
+pcfd_status pcfd_set_preconditioner(pcfd_system* system, int32_t kind);
+pcfd_status pcfd_learned_parameter_count(int64_t* count);
+/* Replaces the FP32 master parameters (and resets the optimiser); count = parameter count.
+ * Before the first call a system uses He-normal weights from a fixed seed. */
+pcfd_status pcfd_learned_set_parameters(pcfd_system* system, const float* parameters, int64_t count);
+pcfd_status pcfd_learned_get_parameters(pcfd_system* system, float* parameters, int64_t count);
+/* From now on every multigrid preconditioner application stores bricks_per_pair randomly
+ * chosen bricks (input, mask, target) until capacity_pairs applications are stored. */
+pcfd_status pcfd_learned_harvest_begin(pcfd_system* system, int32_t capacity_pairs, int32_t bricks_per_pair,
+                                       uint64_t seed);
+/* Stops harvesting (the store is kept for training); samples = stored bricks. */
+pcfd_status pcfd_learned_harvest_stop(pcfd_system* system, int64_t* samples);
+/* `steps` Adam steps (cosine decay from learning_rate to a tenth) on random batches of the
+ * harvested bricks; final_loss = mean loss of the last min(steps, 50) steps. */
+pcfd_status pcfd_learned_train(pcfd_system* system, int32_t steps, int32_t batch, double learning_rate,
+                               uint64_t seed, double* final_loss);
+/* Forward and backward pass on host samples: inputs [samples][512][2] (D^-1 r / s, mask),
+ * targets [samples][512]; zhat [samples][512] = net output, loss, gradients [parameter count]
+ * (may be NULL).  For checking the kernels against the oracle. */
+pcfd_status pcfd_learned_evaluate_host(pcfd_system* system, int32_t samples, const float* inputs, const float* targets,
+                                       float* zhat, double* loss, float* gradients);
+/* z = learned preconditioner applied to r (device vectors [S]). */
+pcfd_status pcfd_learned_apply_device(pcfd_system* system, const double* d_r, double* d_z);
+
 #ifdef __cplusplus
 }
 #endif

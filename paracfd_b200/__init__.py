@@ -18,6 +18,13 @@ PROFILE_STRUCTURED_APPLY = 0
 PROFILE_PRECONDITIONER = 1
 MG_FP64, MG_FP32 = 0, 1
 MG_CYCLE_REFERENCE, MG_CYCLE_CORRECTED, MG_CYCLE_COMPOSITE = 0, 1, 2
+PRECONDITIONER_MULTIGRID, PRECONDITIONER_LEARNED, PRECONDITIONER_JACOBI = 0, 1, 2
+
+
+def learned_parameter_count() -> int:
+    n = C.c_int64()
+    check(capi.load().pcfd_learned_parameter_count(C.byref(n)))
+    return n.value
 
 
 class BuiltTopology:
@@ -136,6 +143,44 @@ class CompositeSystem:
         check(self._lib.pcfd_pressure_solve_host(self.handle, ptr(x, C.c_double), ptr(b, C.c_double), tolerance,
                                                  max_iterations, int(x0 is not None), C.byref(res)))
         return x, res.as_dict()
+
+    # ---- learned preconditioner ---------------------------------------------------------------
+    def set_preconditioner(self, kind: int):
+        check(self._lib.pcfd_set_preconditioner(self.handle, kind))
+
+    def learned_parameters(self) -> np.ndarray:
+        out = np.empty(learned_parameter_count(), np.float32)
+        check(self._lib.pcfd_learned_get_parameters(self.handle, ptr(out, C.c_float), len(out)))
+        return out
+
+    def set_learned_parameters(self, params):
+        params = np.ascontiguousarray(params, np.float32)
+        check(self._lib.pcfd_learned_set_parameters(self.handle, ptr(params, C.c_float), len(params)))
+
+    def harvest_begin(self, capacity_pairs: int, bricks_per_pair: int, seed: int = 1):
+        check(self._lib.pcfd_learned_harvest_begin(self.handle, capacity_pairs, bricks_per_pair, seed))
+
+    def harvest_stop(self) -> int:
+        n = C.c_int64()
+        check(self._lib.pcfd_learned_harvest_stop(self.handle, C.byref(n)))
+        return n.value
+
+    def train(self, steps: int, batch: int = 32, learning_rate: float = 1e-3, seed: int = 1) -> float:
+        loss = C.c_double()
+        check(self._lib.pcfd_learned_train(self.handle, steps, batch, learning_rate, seed, C.byref(loss)))
+        return loss.value
+
+    def learned_evaluate(self, inputs, targets, gradients: bool = True):
+        """inputs [n,512,2] (D^-1 r / s, mask), targets [n,512] -> (loss, zhat [n,512], grads or None)."""
+        inputs = np.ascontiguousarray(inputs, np.float32)
+        targets = np.ascontiguousarray(targets, np.float32)
+        n = inputs.shape[0]
+        zhat = np.empty((n, 512), np.float32)
+        grads = np.empty(learned_parameter_count(), np.float32) if gradients else None
+        loss = C.c_double()
+        check(self._lib.pcfd_learned_evaluate_host(self.handle, n, ptr(inputs, C.c_float), ptr(targets, C.c_float),
+                                                   ptr(zhat, C.c_float), C.byref(loss), ptr(grads, C.c_float)))
+        return loss.value, zhat, grads
 
     # ---- resident state ---------------------------------------------------------------------
     def set_faces(self, u, v, w):

@@ -207,6 +207,16 @@ SIGNATURES = {
     "pcfd_profile_begin": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     "pcfd_profile_end": (C.c_int, [C.c_void_p, _f64p, C.c_int32, C.POINTER(C.c_int32)]),
     "pcfd_builder_last_error": (C.c_char_p, []),
+    "pcfd_set_preconditioner": (C.c_int, [C.c_void_p, C.c_int32]),
+    "pcfd_learned_parameter_count": (C.c_int, [C.POINTER(C.c_int64)]),
+    "pcfd_learned_set_parameters": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int64]),
+    "pcfd_learned_get_parameters": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int64]),
+    "pcfd_learned_harvest_begin": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_uint64]),
+    "pcfd_learned_harvest_stop": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "pcfd_learned_train": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_uint64, C.POINTER(C.c_double)]),
+    "pcfd_learned_evaluate_host": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                             C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_float)]),
+    "pcfd_learned_apply_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
 }
 
 _lib = None

@@ -227,13 +227,7 @@ namespace pcfd
             for (DBuf<double>* v : {&s.r, &s.z, &s.dvec, &s.Ad, &s.t, &s.correction, &s.defect, &s.scratch_p, &s.scratch_out,
                                      &s.integrated, &s.rhs, &s.pressure})
                 v->alloc(size_t(s.Sp));
-            if (s.full_nonorthogonal)
-            {
-                s.gmres_v.alloc(size_t(System::gmres_restart + 1) * s.Sp);
-                s.gmres_z.alloc(size_t(System::gmres_restart) * s.Sp);
-                s.recycle_u.alloc(size_t(System::recycle_capacity) * s.Sp);
-                s.recycle_c.alloc(size_t(System::recycle_capacity) * s.Sp);
-            }
+            if (s.full_nonorthogonal) allocate_gcro(s);
             s.dot_partial.alloc(4096);
             s.dot_result.alloc(16);
             s.block_partial.alloc(size_t(592) * (kMaxSet + 1));
@@ -273,8 +267,20 @@ namespace pcfd
         void sync(System& s) { cuda_check(cudaStreamSynchronize(s.stream), "synchronize"); }
     }
 
+    // basis storage of the flexible GCRO/LGMRES solver
+    void allocate_gcro(System& s)
+    {
+        if (s.gmres_v.p) return;
+        s.gmres_v.alloc(size_t(System::gmres_restart + 1) * s.Sp);
+        s.gmres_z.alloc(size_t(System::gmres_restart) * s.Sp);
+        s.recycle_u.alloc(size_t(System::recycle_capacity) * s.Sp);
+        s.recycle_c.alloc(size_t(System::recycle_capacity) * s.Sp);
+    }
+
     System::~System()
     {
+        learned_destroy(*this);
+        if (mg_graph_composite) cudaGraphExecDestroy(mg_graph_composite);
         for (cudaEvent_t& e : markers)
             if (e) cudaEventDestroy(e);
         for (cudaEvent_t e : profile_events) cudaEventDestroy(e);
@@ -693,6 +699,85 @@ pcfd_status pcfd_preconditioner_fused(pcfd_system* system, int32_t* fused)
         System& s = sys(system);
         require(fused != nullptr, "null output");
         *fused = s.fine.enabled ? 1 : 0;
+    });
+}
+
+pcfd_status pcfd_set_preconditioner(pcfd_system* system, int32_t kind)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(kind >= PCFD_PRECONDITIONER_MULTIGRID && kind <= PCFD_PRECONDITIONER_JACOBI, "unknown preconditioner");
+        if (kind == PCFD_PRECONDITIONER_LEARNED) allocate_gcro(s);
+        s.preconditioner = kind;
+    });
+}
+
+pcfd_status pcfd_learned_parameter_count(int64_t* count)
+{
+    return guarded([&] {
+        require(count != nullptr, "null output");
+        *count = learned_parameter_count();
+    });
+}
+
+pcfd_status pcfd_learned_set_parameters(pcfd_system* system, const float* parameters, int64_t count)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(parameters != nullptr, "null parameters");
+        learned_set_parameters(s, parameters, count);
+    });
+}
+
+pcfd_status pcfd_learned_get_parameters(pcfd_system* system, float* parameters, int64_t count)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(parameters != nullptr, "null parameters");
+        learned_get_parameters(s, parameters, count);
+    });
+}
+
+pcfd_status pcfd_learned_harvest_begin(pcfd_system* system, int32_t capacity_pairs, int32_t bricks_per_pair, uint64_t seed)
+{
+    return guarded([&] { learned_harvest_begin(sys(system), capacity_pairs, bricks_per_pair, seed); });
+}
+
+pcfd_status pcfd_learned_harvest_stop(pcfd_system* system, int64_t* samples)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(samples != nullptr, "null output");
+        *samples = learned_harvest_stop(s);
+    });
+}
+
+pcfd_status pcfd_learned_train(pcfd_system* system, int32_t steps, int32_t batch, double learning_rate, uint64_t seed, double* final_loss)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        const double loss = learned_train(s, steps, batch, learning_rate, seed);
+        if (final_loss) *final_loss = loss;
+    });
+}
+
+pcfd_status pcfd_learned_evaluate_host(pcfd_system* system, int32_t samples, const float* inputs, const float* targets, float* zhat,
+                                       double* loss, float* gradients)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        const double l = learned_evaluate(s, samples, inputs, targets, zhat, gradients);
+        if (loss) *loss = l;
+    });
+}
+
+pcfd_status pcfd_learned_apply_device(pcfd_system* system, const double* d_r, double* d_z)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(d_r && d_z, "null vector");
+        learned_apply(s, d_r, d_z);
+        learned_check(s);
     });
 }
 

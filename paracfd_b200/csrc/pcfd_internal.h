@@ -248,6 +248,10 @@ namespace pcfd
         DBuf<int> cf_group_offset, cf_group_member;
         DBuf<double> cf_group_area;
 
+        // preconditioner of the Krylov solvers (pcfd_preconditioner) and the learned network state
+        int preconditioner = PCFD_PRECONDITIONER_MULTIGRID;
+        struct Learned* learned = nullptr;
+
         // cell-momentum transport and time-step orchestration
         struct Momentum* momentum = nullptr;
         void* loads = nullptr;                  // surface-load integration state (loads.cu)
@@ -316,6 +320,20 @@ namespace pcfd
     void composite_levels(System& s);                 // V-cycle below the fine level, composite chain
     void composite_preconditioner(System& s, const double* r, double* z);   // smoother.cu
     pcfd_solve_result solve(System& s, double* x, const double* b, double tolerance, int max_iterations, bool warm);
+    void allocate_gcro(System& s);   // GCRO/LGMRES basis storage (capi.cu), idempotent
+    // ---- learned preconditioner (learned.cu) ----
+    int64_t learned_parameter_count();
+    void learned_destroy(System& s);
+    void learned_set_parameters(System& s, const float* host, int64_t count);
+    void learned_get_parameters(System& s, float* host, int64_t count);
+    void learned_apply(System& s, const double* r, double* z);
+    void learned_check(System& s);   // throws PCFD_TIMEOUT when a tensor-core wait gave up
+    void learned_harvest_begin(System& s, int capacity_pairs, int per_pair, uint64_t seed);
+    int64_t learned_harvest_stop(System& s);
+    bool learned_harvesting(const System& s);
+    void learned_harvest(System& s, const double* r, const double* z);
+    double learned_train(System& s, int steps, int batch, double lr, uint64_t seed);
+    double learned_evaluate(System& s, int n, const float* x, const float* target, float* zhat, float* gradients);
     // vector helpers
     void vec_copy_active(System& s, const double* src, double* dst);
     void vec_subtract(System& s, double* residual, const double* value);   // r = active ? r - v : 0

@@ -740,24 +740,50 @@ namespace pcfd
     template void multigrid_levels<double>(System&, std::vector<MgLevel<double>>&);
     template void multigrid_levels<float>(System&, std::vector<MgLevel<float>>&);
 
+    namespace
+    {
+        __global__ void jacobi_precondition_kernel(const double* r, double* z, const double* diag, const uint8_t* active, int64_t n)
+        {
+            const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+            if (q < n) z[q] = active[q] && diag[q] > 0.0 ? r[q] / diag[q] : 0.0;
+        }
+
+        void multigrid_preconditioner(System& s, const double* r, double* z)
+        {
+            if (s.composite && s.fine.enabled && aligned16(r) && aligned16(z))
+            {
+                composite_preconditioner(s, r, z);
+                return;
+            }
+            if (s.fine.enabled && aligned16(r) && aligned16(z))
+            {
+                if (s.mg_precision == PCFD_MG_FP32 && !s.mg32.empty()) fine_preconditioner(s, r, z, s.mg32);
+                else fine_preconditioner(s, r, z, s.mg64);
+                return;
+            }
+            preconditioner_stage(s, 0, r, z);
+            preconditioner_stage(s, 1, r, z);
+            preconditioner_stage(s, 2, r, z);
+            cuda_check(cudaGetLastError(), "preconditioner");
+        }
+    }
+
     void apply_preconditioner(System& s, const double* r, double* z)
     {
         ProfileScope scope(s, PCFD_PROFILE_PRECONDITIONER);
-        if (s.composite && s.fine.enabled && aligned16(r) && aligned16(z))
+        if (s.preconditioner == PCFD_PRECONDITIONER_LEARNED)
         {
-            composite_preconditioner(s, r, z);
+            learned_apply(s, r, z);
             return;
         }
-        if (s.fine.enabled && aligned16(r) && aligned16(z))
+        if (s.preconditioner == PCFD_PRECONDITIONER_JACOBI)
         {
-            if (s.mg_precision == PCFD_MG_FP32 && !s.mg32.empty()) fine_preconditioner(s, r, z, s.mg32);
-            else fine_preconditioner(s, r, z, s.mg64);
+            jacobi_precondition_kernel<<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(r, z, s.diagonal, s.active, s.S);
             return;
         }
-        preconditioner_stage(s, 0, r, z);
-        preconditioner_stage(s, 1, r, z);
-        preconditioner_stage(s, 2, r, z);
-        cuda_check(cudaGetLastError(), "preconditioner");
+        multigrid_preconditioner(s, r, z);
+        // training pairs for the learned preconditioner: (r, one multigrid application)
+        if (learned_harvesting(s)) learned_harvest(s, r, z);
     }
 
     // ==================================================================================
@@ -1075,7 +1101,9 @@ namespace pcfd
 
     pcfd_solve_result solve(System& s, double* x, const double* b, double tolerance, int max_iterations, bool warm)
     {
-        if (!s.full_nonorthogonal)
+        // the learned preconditioner is not a fixed linear map: it always runs under the flexible
+        // GCRO/LGMRES recurrence
+        if (!s.full_nonorthogonal && s.preconditioner != PCFD_PRECONDITIONER_LEARNED)
         {
             // One continuous MG-PCG solve with a 5x iteration budget, then the final defect
             // (reference amr_pressure.cu:1361-1389).
@@ -1090,6 +1118,8 @@ namespace pcfd
             result.converged = std::isfinite(result.relative_residual) && result.relative_residual <= tolerance;
             return result;
         }
-        return solve_gcro(s, x, b, tolerance, max_iterations, warm);
+        pcfd_solve_result result = solve_gcro(s, x, b, tolerance, max_iterations, warm);
+        if (s.preconditioner == PCFD_PRECONDITIONER_LEARNED) learned_check(s);
+        return result;
     }
 }

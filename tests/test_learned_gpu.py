@@ -1,0 +1,121 @@
+"""Learned preconditioner on the GPU against the numpy oracle (oracle/unet.py): the tensor-core
+forward pass, the backward pass, and what the trained network gains inside the flexible solver."""
+import numpy as np
+import pytest
+
+from oracle import port, unet
+from paracfd_b200 import (PRECONDITIONER_JACOBI, PRECONDITIONER_LEARNED, PRECONDITIONER_MULTIGRID, BuiltTopology,
+                          CompositeSystem, learned_parameter_count)
+from paracfd_b200.geometry import extruded_wing, naca4_section, rotate_section
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def wing(gpu):
+    section = rotate_section(naca4_section(12, 48, 1.0), 4.0)
+    vertices, triangles = extruded_wing(section, -1.0, 1.0)
+    built = BuiltTopology(vertices, triangles, (-2.0, -2.0, -2.0), (4.0, 2.0, 2.0), 0.125, 2, 8,
+                          wing_refinement_distance=0.5, surface_refinement_distance=0.25, wake_length=1.0,
+                          wake_radius=0.5)
+    system = CompositeSystem(built.topology, device=0)
+    yield built, system
+    system.close()
+    built.close()
+
+
+def random_samples(n, seed):
+    """Oracle-prepared brick inputs: smooth-ish residuals, a few inactive cells, random targets."""
+    rng = np.random.default_rng(seed)
+    g = np.linspace(0, 1, 8)
+    z, y, x = np.meshgrid(g, g, g, indexing="ij")
+    r = np.stack([np.sin(3 * x + rng.uniform(0, 6)) * np.cos(2 * y + rng.uniform(0, 6)) + 0.3 * rng.standard_normal((8, 8, 8))
+                  for _ in range(n)]).reshape(n, 512)
+    dinv = rng.uniform(0.5, 2.0, (n, 512))
+    mask = (rng.random((n, 512)) > 0.08).astype(np.float64)
+    xin, _ = unet.prepare(r, dinv, mask)
+    target = rng.standard_normal((n, 512)) * 0.2 * mask
+    inputs = np.stack([xin[..., 0].reshape(n, 512), xin[..., 1].reshape(n, 512)], axis=-1)
+    return inputs.astype(np.float32), target.astype(np.float32), xin, mask
+
+
+def rel_l2(a, b):
+    a, b = np.asarray(a, np.float64).ravel(), np.asarray(b, np.float64).ravel()
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def test_parameter_count_matches_oracle():
+    assert learned_parameter_count() == unet.param_count()
+
+
+@pytest.mark.parametrize("n", [1, 37])
+def test_forward_matches_oracle(wing, n):
+    _, system = wing
+    params = unet.flatten(unet.init_params(3)).astype(np.float32)
+    system.set_learned_parameters(params)
+    inputs, target, xin, mask = random_samples(n, 100 + n)
+    loss, zhat, _ = system.learned_evaluate(inputs, target, gradients=False)
+    want, acts = unet.forward(unet.unflatten(params.astype(np.float64)), xin)
+    # BF16 activations: the only differences are FP32-vs-FP64 accumulation order before a BF16
+    # rounding (at most one BF16 ulp on a few activations); tolerance 1e-2 relative L2
+    assert rel_l2(zhat, want) <= 1e-2, rel_l2(zhat, want)
+    diff = (want - target) * mask
+    want_loss = (diff * diff).sum() / mask.sum()
+    assert abs(loss - want_loss) <= 2e-2 * want_loss
+
+
+def test_gradients_match_oracle(wing):
+    _, system = wing
+    params = unet.flatten(unet.init_params(5)).astype(np.float32)
+    system.set_learned_parameters(params)
+    n = 19
+    inputs, target, xin, mask = random_samples(n, 7)
+    loss, _, grads = system.learned_evaluate(inputs, target)
+    want_loss, want = unet.loss_and_grads(unet.unflatten(params.astype(np.float64)), xin, target.astype(np.float64), mask)
+    got = unet.unflatten(grads.astype(np.float64))
+    for name, _ in unet.param_shapes():
+        # BF16 pre-activation gradients in both; FP32 atomics vs FP64 sums: 3e-2 relative L2
+        assert rel_l2(got[name], want[name]) <= 3e-2, (name, rel_l2(got[name], want[name]))
+
+
+def harvest_and_train(system, built, steps=400, seed=3):
+    rng = np.random.default_rng(seed)
+    active = built.active.astype(bool)
+    oracle = port.PortSystem(built.topology)
+    system.set_preconditioner(PRECONDITIONER_MULTIGRID)
+    system.harvest_begin(capacity_pairs=4000, bricks_per_pair=16, seed=seed)
+    for _ in range(8):
+        b = oracle.apply(np.where(active, rng.standard_normal(built.storage_size), 0.0))
+        system.solve(b, 1e-8, 600)
+    samples = system.harvest_stop()
+    oracle.close()
+    assert samples > 1000
+    return samples, system.train(steps, batch=32, learning_rate=2e-3, seed=seed)
+
+
+def test_trained_network_gains_over_the_method_without_it(wing):
+    built, system = wing
+    rng = np.random.default_rng(99)
+    active = built.active.astype(bool)
+    oracle = port.PortSystem(built.topology)
+    b = oracle.apply(np.where(active, rng.standard_normal(built.storage_size), 0.0))
+
+    def run(kind):
+        system.set_preconditioner(kind)
+        x, info = system.solve(b, 1e-8, 2000)
+        residual = np.linalg.norm((b - oracle.apply(x))[active]) / np.linalg.norm(b[active])
+        return info, residual
+
+    jacobi, _ = run(PRECONDITIONER_JACOBI)
+    system.set_learned_parameters(unet.flatten(unet.init_params(11)).astype(np.float32))
+    untrained, _ = run(PRECONDITIONER_LEARNED)
+    samples, loss = harvest_and_train(system, built)
+    trained, residual = run(PRECONDITIONER_LEARNED)
+    multigrid, _ = run(PRECONDITIONER_MULTIGRID)
+    oracle.close()
+    system.set_preconditioner(PRECONDITIONER_MULTIGRID)
+    print(f"samples {samples} loss {loss:.3e}; iterations: jacobi {jacobi['iterations']} untrained "
+          f"{untrained['iterations']} trained {trained['iterations']} multigrid {multigrid['iterations']}")
+    assert trained["converged"] and residual <= 1e-7
+    assert trained["iterations"] < jacobi["iterations"]
+    assert trained["iterations"] < untrained["iterations"] or not untrained["converged"]
