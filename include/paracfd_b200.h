@@ -205,6 +205,9 @@ typedef struct pcfd_solve_result {
     int32_t converged;
     int32_t preconditioner_applications;
     int32_t recycle_rejections;
+    int32_t fallback_solves;     /* no reference counterpart: 1 when a solve under the learned
+                                    preconditioner did not converge and the multigrid solve from its
+                                    last iterate finished it (iterations count both) */
 } pcfd_solve_result;
 
 /* Physical case and solver settings used by the time step (ParagliderConfig's freestream and
@@ -424,19 +427,34 @@ pcfd_status pcfd_profile_end(pcfd_system* system, double* ms_per_launch, int32_t
  * enc0, enc1, bottleneck, dec1 (up, skip), dec0 (up, skip) ([27][cout][cin] each), head [16]. */
 typedef enum pcfd_preconditioner {
     PCFD_PRECONDITIONER_MULTIGRID = 0,   /* the multigrid V-cycle of pcfd_options (default) */
-    PCFD_PRECONDITIONER_LEARNED = 1,     /* the U-Net; solves run under flexible GCRO/LGMRES */
-    PCFD_PRECONDITIONER_JACOBI = 2       /* z = D^-1 r, the method without the network or the V-cycle */
+    PCFD_PRECONDITIONER_LEARNED = 1,     /* the U-Net, then one damped Jacobi sweep */
+    PCFD_PRECONDITIONER_JACOBI = 2,      /* z = D^-1 r: the method without the network or the V-cycle */
+    PCFD_PRECONDITIONER_LEARNED_MULTIGRID = 3 /* the composite cycle (PCFD_MG_CYCLE_COMPOSITE) with the
+                                            U-Net in place of its fine pre-sweeps */
 } pcfd_preconditioner;
+/* Solves under either learned kind run flexible GCRO/LGMRES; one that does not converge is
+ * finished by the multigrid solve from its last iterate (pcfd_solve_result.fallback_solves). */
 pcfd_status pcfd_set_preconditioner(pcfd_system* system, int32_t kind);
 pcfd_status pcfd_learned_parameter_count(int64_t* count);
 /* Replaces the FP32 master parameters (and resets the optimiser); count = parameter count.
  * Before the first call a system uses He-normal weights from a fixed seed. */
 pcfd_status pcfd_learned_set_parameters(pcfd_system* system, const float* parameters, int64_t count);
 pcfd_status pcfd_learned_get_parameters(pcfd_system* system, float* parameters, int64_t count);
-/* From now on every multigrid preconditioner application stores bricks_per_pair randomly
- * chosen bricks (input, mask, target) until capacity_pairs applications are stored. */
+/* Training target of a harvested brick: the multigrid preconditioner's output on it, or the
+ * solution of the brick's own diagonal block A_B z = r_B (conjugate gradients in the harvest
+ * kernel; the part of the correction a brick-local network can represent, since it depends on
+ * the brick's residual alone). */
+enum {
+    PCFD_LEARNED_TARGET_MULTIGRID = 0,
+    PCFD_LEARNED_TARGET_BRICK_SOLVE = 1
+};
+/* From now on every multigrid preconditioner application of this system stores bricks_per_pair
+ * randomly chosen bricks (input, mask, target) until capacity_pairs applications are stored.
+ * The store is one per process (on the first harvesting system's device) and shared by all
+ * systems, so pairs harvested on several grids accumulate; a call with another capacity,
+ * bricks_per_pair or target starts an empty store. */
 pcfd_status pcfd_learned_harvest_begin(pcfd_system* system, int32_t capacity_pairs, int32_t bricks_per_pair,
-                                       uint64_t seed);
+                                       uint64_t seed, int32_t target);
 /* Stops harvesting (the store is kept for training); samples = stored bricks. */
 pcfd_status pcfd_learned_harvest_stop(pcfd_system* system, int64_t* samples);
 /* `steps` Adam steps (cosine decay from learning_rate to a tenth) on random batches of the

@@ -18,7 +18,8 @@ PROFILE_STRUCTURED_APPLY = 0
 PROFILE_PRECONDITIONER = 1
 MG_FP64, MG_FP32 = 0, 1
 MG_CYCLE_REFERENCE, MG_CYCLE_CORRECTED, MG_CYCLE_COMPOSITE = 0, 1, 2
-PRECONDITIONER_MULTIGRID, PRECONDITIONER_LEARNED, PRECONDITIONER_JACOBI = 0, 1, 2
+PRECONDITIONER_MULTIGRID, PRECONDITIONER_LEARNED, PRECONDITIONER_JACOBI, PRECONDITIONER_LEARNED_MULTIGRID = 0, 1, 2, 3
+LEARNED_TARGET_MULTIGRID, LEARNED_TARGET_BRICK_SOLVE = 0, 1
 
 
 def learned_parameter_count() -> int:
@@ -157,8 +158,9 @@ class CompositeSystem:
         params = np.ascontiguousarray(params, np.float32)
         check(self._lib.pcfd_learned_set_parameters(self.handle, ptr(params, C.c_float), len(params)))
 
-    def harvest_begin(self, capacity_pairs: int, bricks_per_pair: int, seed: int = 1):
-        check(self._lib.pcfd_learned_harvest_begin(self.handle, capacity_pairs, bricks_per_pair, seed))
+    def harvest_begin(self, capacity_pairs: int, bricks_per_pair: int, seed: int = 1, target: int = 1):
+        """target: LEARNED_TARGET_BRICK_SOLVE (default) or LEARNED_TARGET_MULTIGRID."""
+        check(self._lib.pcfd_learned_harvest_begin(self.handle, capacity_pairs, bricks_per_pair, seed, target))
 
     def harvest_stop(self) -> int:
         n = C.c_int64()

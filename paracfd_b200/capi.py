@@ -88,13 +88,13 @@ class Options(C.Structure):
 class SolveResult(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("relative_residual", C.c_double),
                 ("converged", C.c_int32), ("preconditioner_applications", C.c_int32),
-                ("recycle_rejections", C.c_int32)]
+                ("recycle_rejections", C.c_int32), ("fallback_solves", C.c_int32)]
 
     def as_dict(self):
         return {"iterations": self.iterations, "relative_residual": self.relative_residual,
                 "converged": bool(self.converged),
                 "preconditioner_applications": self.preconditioner_applications,
-                "recycle_rejections": self.recycle_rejections}
+                "recycle_rejections": self.recycle_rejections, "fallback_solves": self.fallback_solves}
 
 
 class Case(C.Structure):
@@ -211,7 +211,7 @@ SIGNATURES = {
     "pcfd_learned_parameter_count": (C.c_int, [C.POINTER(C.c_int64)]),
     "pcfd_learned_set_parameters": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int64]),
     "pcfd_learned_get_parameters": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int64]),
-    "pcfd_learned_harvest_begin": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_uint64]),
+    "pcfd_learned_harvest_begin": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_uint64, C.c_int32]),
     "pcfd_learned_harvest_stop": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "pcfd_learned_train": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_uint64, C.POINTER(C.c_double)]),
     "pcfd_learned_evaluate_host": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_float),

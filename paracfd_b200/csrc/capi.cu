@@ -706,8 +706,10 @@ pcfd_status pcfd_set_preconditioner(pcfd_system* system, int32_t kind)
 {
     return guarded([&] {
         System& s = sys(system);
-        require(kind >= PCFD_PRECONDITIONER_MULTIGRID && kind <= PCFD_PRECONDITIONER_JACOBI, "unknown preconditioner");
-        if (kind == PCFD_PRECONDITIONER_LEARNED) allocate_gcro(s);
+        require(kind >= PCFD_PRECONDITIONER_MULTIGRID && kind <= PCFD_PRECONDITIONER_LEARNED_MULTIGRID, "unknown preconditioner");
+        require(kind != PCFD_PRECONDITIONER_LEARNED_MULTIGRID || (s.composite && s.fine.enabled),
+                "the learned multigrid preconditioner needs the composite cycle (PCFD_MG_CYCLE_COMPOSITE)");
+        if (kind == PCFD_PRECONDITIONER_LEARNED || kind == PCFD_PRECONDITIONER_LEARNED_MULTIGRID) allocate_gcro(s);
         s.preconditioner = kind;
     });
 }
@@ -738,9 +740,10 @@ pcfd_status pcfd_learned_get_parameters(pcfd_system* system, float* parameters, 
     });
 }
 
-pcfd_status pcfd_learned_harvest_begin(pcfd_system* system, int32_t capacity_pairs, int32_t bricks_per_pair, uint64_t seed)
+pcfd_status pcfd_learned_harvest_begin(pcfd_system* system, int32_t capacity_pairs, int32_t bricks_per_pair, uint64_t seed,
+                                       int32_t target)
 {
-    return guarded([&] { learned_harvest_begin(sys(system), capacity_pairs, bricks_per_pair, seed); });
+    return guarded([&] { learned_harvest_begin(sys(system), capacity_pairs, bricks_per_pair, seed, target); });
 }
 
 pcfd_status pcfd_learned_harvest_stop(pcfd_system* system, int64_t* samples)

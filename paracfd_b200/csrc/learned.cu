@@ -453,11 +453,78 @@ namespace pcfd
             if (q < end) z[q] = active[q] && diag[q] > 0 ? (2.0 / 3.0) * r[q] / diag[q] : 0.0;
         }
 
+        // 256-thread block sum
+        __device__ inline double block_sum(double v, double* red)
+        {
+            for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            __syncthreads();
+            if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+            __syncthreads();
+            double t = 0;
+            for (int w = 0; w < 8; ++w) t += red[w];
+            return t;
+        }
+
+        // x = A_B^-1 b on one brick by conjugate gradients in shared memory: A_B is the operator's
+        // diagonal block of the brick (the full diagonal D, minus h for every open face to a cell of
+        // the same brick); 2 cells per thread, to 1e-8 relative or 400 iterations
+        __device__ void brick_solve(const double* b, double* x, const uint8_t* code, const double* D, double h, double* ps, double* red)
+        {
+            double r[2], p[2], Ap[2];
+            for (int k = 0; k < 2; ++k)
+            {
+                const int v = threadIdx.x + 256 * k;
+                x[v] = 0;
+                r[k] = b[v];
+                p[k] = r[k];
+                ps[v] = p[k];
+            }
+            double rr = block_sum(r[0] * r[0] + r[1] * r[1], red);
+            const double stop = 1e-16 * rr;
+            for (int it = 0; it < 400 && rr > stop; ++it)
+            {
+                __syncthreads();
+                for (int k = 0; k < 2; ++k)
+                {
+                    const int v = threadIdx.x + 256 * k;
+                    const int c[3] = {v & 7, (v >> 3) & 7, v >> 6};
+                    double a = D[v] * ps[v];
+                    for (int axis = 0; axis < 3; ++axis)
+                        for (int pos = 0; pos < 2; ++pos)
+                        {
+                            const int q = c[axis] + (pos ? 1 : -1);
+                            if (q < 0 || q > 7 || !(code[v] & (1u << (2 * axis + pos)))) continue;
+                            a -= h * ps[v + (pos ? 1 : -1) * (axis == 0 ? 1 : axis == 1 ? 8 : 64)];
+                        }
+                    Ap[k] = D[v] > 0 ? a : 0.0;
+                }
+                const double pAp = block_sum(p[0] * Ap[0] + p[1] * Ap[1], red);
+                if (!(pAp > 0)) break;
+                const double alpha = rr / pAp;
+                for (int k = 0; k < 2; ++k)
+                {
+                    x[threadIdx.x + 256 * k] += alpha * p[k];
+                    r[k] -= alpha * Ap[k];
+                }
+                const double next = block_sum(r[0] * r[0] + r[1] * r[1], red);
+                const double beta = next / rr;
+                rr = next;
+                __syncthreads();
+                for (int k = 0; k < 2; ++k)
+                {
+                    p[k] = r[k] + beta * p[k];
+                    ps[threadIdx.x + 256 * k] = p[k];
+                }
+            }
+            __syncthreads();
+        }
+
         // harvest: brick k of preconditioner call `pair` -> store slot; input D^-1 r / s, mask,
-        // target z / s
+        // target z / s with z the multigrid output (local = 0) or the brick-local solve (local = 1)
         __global__ void harvest_kernel(const int* slots, int bricks, int64_t pair, int per_pair, uint64_t seed, int64_t capacity,
                                        const double* r, const double* z, const double* diag, const uint8_t* active, bf16* hx,
-                                       uint8_t* hm, float* ht)
+                                       uint8_t* hm, float* ht, int local, const uint8_t* code, const int* brick_level,
+                                       const double* level_h)
         {
             const int k = blockIdx.x;
             const int64_t sample = pair * per_pair + k;
@@ -482,19 +549,46 @@ namespace pcfd
             for (int w = 0; w < 8; ++w) { tss += red[0][w]; tcnt += red[1][w]; }
             double s = std::sqrt(tss / fmax(tcnt, 1.0));
             if (!(s > 0)) s = 1.0;
+            __shared__ double bs[512], xs[512], ps[512], Ds[512], red2[8];
+            __shared__ uint8_t cs[512];
+            if (local)
+            {
+                for (int j = 0; j < 2; ++j)
+                {
+                    const int v = threadIdx.x + 256 * j;
+                    const int64_t qq = q0 + v;
+                    const bool on = active[qq] && diag[qq] > 0;
+                    bs[v] = on ? r[qq] : 0.0;
+                    Ds[v] = on ? diag[qq] : 0.0;
+                    cs[v] = on ? code[qq] : 0;
+                }
+                __syncthreads();
+                brick_solve(bs, xs, cs, Ds, level_h[brick_level[slots[b]]], ps, red2);
+            }
             for (int j = 0; j < 2; ++j)
             {
                 const int v = threadIdx.x + 256 * j;
                 const int64_t qq = q0 + v;
                 hx[sample * 512 + v] = __float2bfloat16_rn(float(q[j] / s));
                 hm[sample * 512 + v] = active[qq] ? 1 : 0;
-                ht[sample * 512 + v] = active[qq] ? float(z[qq] / s) : 0.0f;
+                const double target = local ? xs[v] : z[qq];
+                ht[sample * 512 + v] = active[qq] ? float(target / s) : 0.0f;
             }
         }
 
-        // training batch: x0 [batch][512][16], target, mask; count += active cells
-        __global__ void gather_batch_kernel(const int* index, int batch, const bf16* hx, const uint8_t* hm, const float* ht, bf16* x0,
-                                            float* target, uint8_t* mask, float* count)
+        // sum of squared targets and active count over the harvest store
+        __global__ void target_moment_kernel(int64_t n, const uint8_t* hm, const float* ht, double* out)
+        {
+            double ss = 0, cnt = 0;
+            for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+                if (hm[i]) { ss += double(ht[i]) * ht[i]; cnt += 1; }
+            for (int o = 16; o; o >>= 1) { ss += __shfl_xor_sync(0xffffffffu, ss, o); cnt += __shfl_xor_sync(0xffffffffu, cnt, o); }
+            if ((threadIdx.x & 31) == 0) { atomicAdd(&out[0], ss); atomicAdd(&out[1], cnt); }
+        }
+
+        // training batch: x0 [batch][512][16], target * target_scale, mask; count += active cells
+        __global__ void gather_batch_kernel(const int* index, int batch, const bf16* hx, const uint8_t* hm, const float* ht, float target_scale,
+                                            bf16* x0, float* target, uint8_t* mask, float* count)
         {
             const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
             if (i >= int64_t(batch) * 512) return;
@@ -504,7 +598,7 @@ namespace pcfd
             uint4* o = reinterpret_cast<uint4*>(x0 + i * 16);
             o[0] = pack8(f);
             o[1] = pack8(zero);
-            target[i] = ht[src];
+            target[i] = ht[src] * target_scale;
             mask[i] = hm[src];
             if (hm[src]) atomicAdd(count, 1.0f);
         }
@@ -689,15 +783,29 @@ namespace pcfd
         DBuf<int> batch_index;
         DBuf<float> scalars;        // [0] count, [1] loss
         DBuf<int> error;
-        // harvest store
         bool harvesting = false;
-        int per_pair = 0;
-        int64_t store_capacity = 0, pairs = 0;
-        uint64_t seed = 0;
-        DBuf<bf16> hx;
-        DBuf<uint8_t> hm;
-        DBuf<float> ht;
     };
+
+    namespace
+    {
+        // Harvested training bricks.  One store per process (the device of the first system that
+        // harvests), shared by every system, so pairs from several grids accumulate.
+        struct Store
+        {
+            int device = -1, per_pair = 0, local = 1;
+            int64_t capacity = 0, pairs = 0;
+            uint64_t seed = 0;
+            DBuf<bf16> hx;          // [capacity][512] D^-1 r / s
+            DBuf<uint8_t> hm;       // [capacity][512] active mask
+            DBuf<float> ht;         // [capacity][512] z / s
+            int64_t samples() const { return std::min(pairs * per_pair, capacity); }
+        };
+        Store& store()
+        {
+            static Store* st = new Store();   // never destroyed: the CUDA context may be gone at exit
+            return *st;
+        }
+    }
 
     namespace
     {
@@ -755,12 +863,12 @@ namespace pcfd
             p.y = y;
             p.error = L.error;
             const size_t smem = conv_smem<N>(cout);
-            static bool configured[3] = {false, false, false};
+            static size_t configured[3] = {0, 0, 0};
             const int slot = N == 8 ? 0 : N == 4 ? 1 : 2;
-            if (!configured[slot])
+            if (smem > configured[slot])
             {
-                cuda_check(cudaFuncSetAttribute(conv_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024), "conv smem");
-                configured[slot] = true;
+                cuda_check(cudaFuncSetAttribute(conv_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)), "conv smem");
+                configured[slot] = smem;
             }
             const int groups = (samples + Geometry<N>::NB - 1) / Geometry<N>::NB;
             const int per_sm = smem > 114 * 1024 ? 1 : smem > 76 * 1024 ? 2 : 3;
@@ -773,14 +881,14 @@ namespace pcfd
         {
             constexpr int P = (N + 2) * (N + 2) * (N + 2), V = N * N * N;
             const size_t smem = size_t(P) * src.channels * 2 + size_t(V) * cout * 2;
-            static bool configured[3] = {false, false, false};
+            require(smem <= 200 * 1024, "learned: weight-gradient staging");
+            static size_t configured[3] = {0, 0, 0};
             const int slot = N == 8 ? 0 : N == 4 ? 1 : 2;
-            if (!configured[slot])
+            if (smem > configured[slot])
             {
-                cuda_check(cudaFuncSetAttribute(weight_grad_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024), "wgrad smem");
-                configured[slot] = true;
+                cuda_check(cudaFuncSetAttribute(weight_grad_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)), "wgrad smem");
+                configured[slot] = smem;
             }
-            require(smem <= 227 * 1024, "learned: weight-gradient staging");
             const int entries = 27 * (cout / 4) * (src.channels / 4);
             const int chunk = 8;
             dim3 grid((entries + 255) / 256, (samples + chunk - 1) / chunk);
@@ -926,45 +1034,63 @@ namespace pcfd
         if (s.learned) check_error(s, *s.learned);
     }
 
-    void learned_harvest_begin(System& s, int capacity_pairs, int per_pair, uint64_t seed)
+    void learned_harvest_begin(System& s, int capacity_pairs, int per_pair, uint64_t seed, int target)
     {
         require(capacity_pairs > 0 && per_pair > 0 && per_pair <= 4096, "learned: harvest sizes");
+        require(target == PCFD_LEARNED_TARGET_MULTIGRID || target == PCFD_LEARNED_TARGET_BRICK_SOLVE, "learned: harvest target");
+        require(target == PCFD_LEARNED_TARGET_MULTIGRID || s.fine.enabled, "learned: the brick-solve target needs 8^3 bricks");
         Learned& L = state(s);
+        Store& st = store();
+        require(st.device < 0 || st.device == s.device, "learned: the harvest store lives on another device");
         const int64_t capacity = int64_t(capacity_pairs) * per_pair;
-        if (capacity != L.store_capacity)
+        if (capacity != st.capacity || per_pair != st.per_pair || target != st.local)
         {
-            L.hx.alloc(size_t(capacity) * 512);
-            L.hm.alloc(size_t(capacity) * 512);
-            L.ht.alloc(size_t(capacity) * 512);
-            L.store_capacity = capacity;
-            L.pairs = 0;
+            cuda_check(cudaStreamSynchronize(s.stream), "harvest store");
+            st.hx.alloc(size_t(capacity) * 512);
+            st.hm.alloc(size_t(capacity) * 512);
+            st.ht.alloc(size_t(capacity) * 512);
+            st.capacity = capacity;
+            st.per_pair = per_pair;
+            st.pairs = 0;
+            st.device = s.device;
+            st.local = target;
         }
-        L.per_pair = per_pair;
-        L.seed = seed;
+        st.seed = seed;
         L.harvesting = true;
     }
 
     int64_t learned_harvest_stop(System& s)
     {
-        if (!s.learned) return 0;
-        Learned& L = *s.learned;
-        L.harvesting = false;
-        return std::min(L.pairs * L.per_pair, L.store_capacity);
+        if (s.learned) s.learned->harvesting = false;
+        return store().samples();
     }
 
     bool learned_harvesting(const System& s) { return s.learned && s.learned->harvesting; }
 
     void learned_harvest(System& s, const double* r, const double* z)
     {
-        Learned& L = *s.learned;
-        if (!s.active_bricks || L.pairs * L.per_pair >= L.store_capacity) return;
-        harvest_kernel<<<L.per_pair, 256, 0, launch_stream(s)>>>(s.active_brick_list, s.active_bricks, L.pairs, L.per_pair, L.seed,
-                                                                 L.store_capacity, r, z, s.diagonal, s.active, L.hx, L.hm, L.ht);
-        ++L.pairs;
+        Store& st = store();
+        if (!s.active_bricks || st.pairs * st.per_pair >= st.capacity) return;
+        harvest_kernel<<<st.per_pair, 256, 0, launch_stream(s)>>>(s.active_brick_list, s.active_bricks, st.pairs, st.per_pair,
+                                                                  st.seed, st.capacity, r, z, s.diagonal, s.active, st.hx, st.hm, st.ht,
+                                                                  st.local, s.fine.code, s.brick_level, s.d_level_h);
+        ++st.pairs;
     }
 
     namespace
     {
+        // head master weights *= factor (and the BF16 copies)
+        void scale_head(System& s, Learned& L, double factor)
+        {
+            float h[kHead];
+            cuda_check(cudaMemcpyAsync(h, L.master.p + kWeights, sizeof(h), cudaMemcpyDeviceToHost, s.stream), "head");
+            cuda_check(cudaStreamSynchronize(s.stream), "head");
+            for (float& v : h) v = float(v * factor);
+            cuda_check(cudaMemcpyAsync(L.master.p + kWeights, h, sizeof(h), cudaMemcpyHostToDevice, s.stream), "head");
+            cuda_check(cudaStreamSynchronize(s.stream), "head");
+            convert(s, L);
+        }
+
         // one optimiser step on L.x0 / target / mask for `batch` samples; returns nothing (loss on device)
         void train_step(System& s, Learned& L, int batch, float lr)
         {
@@ -985,9 +1111,27 @@ namespace pcfd
         require(steps >= 0 && batch > 0 && lr > 0, "learned: training arguments");
         Learned& L = state(s);
         if (!L.has_weights) default_parameters(s, L);
-        const int64_t samples = std::min(L.pairs * L.per_pair, L.store_capacity);
-        require(samples > 0, "learned: no harvested samples to train on");
+        Store& st = store();
+        const int64_t samples = st.samples();
+        require(samples > 0 && st.device == s.device, "learned: no harvested samples on this device to train on");
         ensure_capacity(L, batch);
+        // Targets (multigrid corrections over D^-1 r / s) are 10^2..10^4 in size: train against
+        // targets divided by their RMS tau over the store, with the head divided by tau, and fold
+        // tau back into the head afterwards (the head is linear, so the trained map is unchanged).
+        double tau = 1.0;
+        {
+            DBuf<double> moment;
+            moment.alloc(2);
+            target_moment_kernel<<<4 * sm_count(s), 256, 0, launch_stream(s)>>>(samples * 512, st.hm, st.ht, moment);
+            double h[2] = {0, 0};
+            cuda_check(cudaMemcpyAsync(h, moment.p, sizeof(h), cudaMemcpyDeviceToHost, s.stream), "target moment");
+            cuda_check(cudaStreamSynchronize(s.stream), "target moment");
+            if (h[1] > 0 && h[0] > 0) tau = std::sqrt(h[0] / h[1]);
+        }
+        scale_head(s, L, 1.0 / tau);
+        cuda_check(cudaMemsetAsync(L.adam_m, 0, size_t(kParams) * sizeof(float), s.stream), "reset adam");
+        cuda_check(cudaMemsetAsync(L.adam_v, 0, size_t(kParams) * sizeof(float), s.stream), "reset adam");
+        L.adam_step = 0;
         std::mt19937_64 rng(seed);
         std::vector<int> index(static_cast<size_t>(batch));
         std::vector<float> losses;
@@ -1002,8 +1146,9 @@ namespace pcfd
                 cuda_check(cudaMemcpyAsync(L.batch_index, index.data(), index.size() * sizeof(int), cudaMemcpyHostToDevice, s.stream),
                            "batch indices");
                 cuda_check(cudaMemsetAsync(L.scalars, 0, sizeof(float), s.stream), "zero count");
-                gather_batch_kernel<<<blocks_for(int64_t(batch) * 512), kThreads, 0, launch_stream(s)>>>(L.batch_index, batch, L.hx, L.hm, L.ht,
-                                                                                                        L.x0, L.target, L.mask, L.scalars);
+                gather_batch_kernel<<<blocks_for(int64_t(batch) * 512), kThreads, 0, launch_stream(s)>>>(L.batch_index, batch, st.hx, st.hm,
+                                                                                                        st.ht, float(1.0 / tau), L.x0, L.target,
+                                                                                                        L.mask, L.scalars);
                 // cosine decay to 10 % of the initial rate
                 const double frac = steps > 1 ? double(step) / double(steps - 1) : 0.0;
                 const float rate = float(lr * (0.1 + 0.45 * (1.0 + std::cos(M_PI * frac))));
@@ -1015,6 +1160,7 @@ namespace pcfd
                 if ((step & 63) == 63) cuda_check(cudaStreamSynchronize(s.stream), "train sync");
             }
             check_error(s, L);
+            scale_head(s, L, tau);
         }
         catch (...)
         {
@@ -1055,8 +1201,8 @@ namespace pcfd
         for (int i = 0; i < n; ++i) index[size_t(i)] = i;
         cuda_check(cudaMemcpyAsync(L.batch_index, index.data(), index.size() * sizeof(int), cudaMemcpyHostToDevice, s.stream), "indices");
         cuda_check(cudaMemsetAsync(L.scalars, 0, sizeof(float), s.stream), "zero count");
-        gather_batch_kernel<<<blocks_for(int64_t(n) * 512), kThreads, 0, launch_stream(s)>>>(L.batch_index, n, dx, dm, dt, L.x0, L.target,
-                                                                                            L.mask, L.scalars);
+        gather_batch_kernel<<<blocks_for(int64_t(n) * 512), kThreads, 0, launch_stream(s)>>>(L.batch_index, n, dx, dm, dt, 1.0f, L.x0,
+                                                                                            L.target, L.mask, L.scalars);
         forward(s, L, n);
         backward(s, L, n);
         float loss = 0;

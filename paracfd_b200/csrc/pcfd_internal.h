@@ -319,6 +319,7 @@ namespace pcfd
     void build_composite(System& s, const pcfd_topology& t);
     void composite_levels(System& s);                 // V-cycle below the fine level, composite chain
     void composite_preconditioner(System& s, const double* r, double* z);   // smoother.cu
+    void learned_preconditioner(System& s, const double* r, double* z, bool coarse);   // smoother.cu
     pcfd_solve_result solve(System& s, double* x, const double* b, double tolerance, int max_iterations, bool warm);
     void allocate_gcro(System& s);   // GCRO/LGMRES basis storage (capi.cu), idempotent
     // ---- learned preconditioner (learned.cu) ----
@@ -328,7 +329,7 @@ namespace pcfd
     void learned_get_parameters(System& s, float* host, int64_t count);
     void learned_apply(System& s, const double* r, double* z);
     void learned_check(System& s);   // throws PCFD_TIMEOUT when a tensor-core wait gave up
-    void learned_harvest_begin(System& s, int capacity_pairs, int per_pair, uint64_t seed);
+    void learned_harvest_begin(System& s, int capacity_pairs, int per_pair, uint64_t seed, int target);
     int64_t learned_harvest_stop(System& s);
     bool learned_harvesting(const System& s);
     void learned_harvest(System& s, const double* r, const double* z);

@@ -754,6 +754,10 @@ namespace pcfd
             rhs[c] = TC(sum);
         }
 
+        // residual of the pre-smoothed z, its gather into stage 1, the stage V-cycle, the weighted
+        // prolongation fused into the first post-sweep, one more post-sweep
+        template <class TC> void composite_tail(System& s, const double* r, double* z, MgLevel<TC>& first);
+
         template <class TC>
         void composite_cycle(System& s, const double* r, double* z, MgLevel<TC>& first)
         {
@@ -762,6 +766,34 @@ namespace pcfd
             first_sweep_kernel<double><<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(
                 f.code, s.brick_level, f.damping.p, s.diagonal, s.active, r, a, nullptr, s.structured, s.S, 2.0 / 3.0);
             sweep<double, double, TC, 0>(s, a, r, z, nullptr);
+            composite_tail<TC>(s, r, z, first);
+        }
+    }
+
+    // The learned preconditioner around the fused fine level: a = net(r), then one damped Jacobi
+    // sweep (PCFD_PRECONDITIONER_LEARNED), or the composite cycle's residual, stage correction and
+    // post-sweeps with the network in place of the fine pre-sweeps
+    // (PCFD_PRECONDITIONER_LEARNED_MULTIGRID).
+    void learned_preconditioner(System& s, const double* r, double* z, bool coarse)
+    {
+        if (!coarse)
+        {
+            learned_apply(s, r, s.fine.z.p);
+            sweep<double, double, double, 0>(s, s.fine.z.p, r, z, nullptr);
+            return;
+        }
+        require(s.composite, "the learned multigrid preconditioner needs the composite cycle");
+        learned_apply(s, r, z);
+        if (s.composite_fp32) composite_tail<float>(s, r, z, s.inter32.front());
+        else composite_tail<double>(s, r, z, s.inter64.front());
+    }
+
+    namespace
+    {
+        template <class TC> void composite_tail(System& s, const double* r, double* z, MgLevel<TC>& first)
+        {
+            FineSmoother& f = s.fine;
+            double* a = f.z.p;
             double* res = s.fine_residual.p;
             brick_pipe_kernel<3, double, double, TC, 0><<<pipe_grid(s), 256, 0, launch_stream(s)>>>(
                 view(s), s.active_bricks, z, r, res, f.t.p, nullptr, nullptr, f.damping.p);

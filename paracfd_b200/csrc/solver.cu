@@ -771,9 +771,11 @@ namespace pcfd
     void apply_preconditioner(System& s, const double* r, double* z)
     {
         ProfileScope scope(s, PCFD_PROFILE_PRECONDITIONER);
-        if (s.preconditioner == PCFD_PRECONDITIONER_LEARNED)
+        if (s.preconditioner == PCFD_PRECONDITIONER_LEARNED || s.preconditioner == PCFD_PRECONDITIONER_LEARNED_MULTIGRID)
         {
-            learned_apply(s, r, z);
+            const bool coarse = s.preconditioner == PCFD_PRECONDITIONER_LEARNED_MULTIGRID;
+            if (s.fine.enabled && aligned16(r) && aligned16(z) && (!coarse || s.composite)) learned_preconditioner(s, r, z, coarse);
+            else learned_apply(s, r, z);
             return;
         }
         if (s.preconditioner == PCFD_PRECONDITIONER_JACOBI)
@@ -1102,8 +1104,32 @@ namespace pcfd
     pcfd_solve_result solve(System& s, double* x, const double* b, double tolerance, int max_iterations, bool warm)
     {
         // the learned preconditioner is not a fixed linear map: it always runs under the flexible
-        // GCRO/LGMRES recurrence
-        if (!s.full_nonorthogonal && s.preconditioner != PCFD_PRECONDITIONER_LEARNED)
+        // GCRO/LGMRES recurrence, with the multigrid solve from its last iterate as the fallback
+        const bool learned = s.preconditioner == PCFD_PRECONDITIONER_LEARNED || s.preconditioner == PCFD_PRECONDITIONER_LEARNED_MULTIGRID;
+        if (learned)
+        {
+            pcfd_solve_result result = solve_gcro(s, x, b, tolerance, max_iterations, warm);
+            learned_check(s);
+            if (result.converged) return result;
+            const int kind = s.preconditioner;
+            s.preconditioner = PCFD_PRECONDITIONER_MULTIGRID;
+            pcfd_solve_result fallback{};
+            try
+            {
+                fallback = solve(s, x, b, tolerance, max_iterations, true);
+            }
+            catch (...)
+            {
+                s.preconditioner = kind;
+                throw;
+            }
+            s.preconditioner = kind;
+            fallback.iterations += result.iterations;
+            fallback.preconditioner_applications += result.preconditioner_applications;
+            fallback.fallback_solves = 1;
+            return fallback;
+        }
+        if (!s.full_nonorthogonal)
         {
             // One continuous MG-PCG solve with a 5x iteration budget, then the final defect
             // (reference amr_pressure.cu:1361-1389).
@@ -1118,8 +1144,6 @@ namespace pcfd
             result.converged = std::isfinite(result.relative_residual) && result.relative_residual <= tolerance;
             return result;
         }
-        pcfd_solve_result result = solve_gcro(s, x, b, tolerance, max_iterations, warm);
-        if (s.preconditioner == PCFD_PRECONDITIONER_LEARNED) learned_check(s);
-        return result;
+        return solve_gcro(s, x, b, tolerance, max_iterations, warm);
     }
 }

@@ -4,8 +4,9 @@ import numpy as np
 import pytest
 
 from oracle import port, unet
-from paracfd_b200 import (PRECONDITIONER_JACOBI, PRECONDITIONER_LEARNED, PRECONDITIONER_MULTIGRID, BuiltTopology,
-                          CompositeSystem, learned_parameter_count)
+from paracfd_b200 import (LEARNED_TARGET_BRICK_SOLVE, MG_CYCLE_COMPOSITE, PRECONDITIONER_JACOBI, PRECONDITIONER_LEARNED,
+                          PRECONDITIONER_LEARNED_MULTIGRID, PRECONDITIONER_MULTIGRID, BuiltTopology, CompositeSystem,
+                          learned_parameter_count)
 from paracfd_b200.geometry import extruded_wing, naca4_section, rotate_section
 
 pytestmark = pytest.mark.gpu
@@ -18,7 +19,7 @@ def wing(gpu):
     built = BuiltTopology(vertices, triangles, (-2.0, -2.0, -2.0), (4.0, 2.0, 2.0), 0.125, 2, 8,
                           wing_refinement_distance=0.5, surface_refinement_distance=0.25, wake_length=1.0,
                           wake_radius=0.5)
-    system = CompositeSystem(built.topology, device=0)
+    system = CompositeSystem(built.topology, device=0, mg_cycle=MG_CYCLE_COMPOSITE)
     yield built, system
     system.close()
     built.close()
@@ -78,19 +79,20 @@ def test_gradients_match_oracle(wing):
         assert rel_l2(got[name], want[name]) <= 3e-2, (name, rel_l2(got[name], want[name]))
 
 
-def harvest_and_train(system, built, steps=400, seed=3):
+def harvest_and_train(system, built, steps=500, seed=3):
+    """Brick-solve targets harvested from 12 multigrid solves, then `steps` Adam steps."""
     rng = np.random.default_rng(seed)
     active = built.active.astype(bool)
     oracle = port.PortSystem(built.topology)
     system.set_preconditioner(PRECONDITIONER_MULTIGRID)
-    system.harvest_begin(capacity_pairs=4000, bricks_per_pair=16, seed=seed)
-    for _ in range(8):
+    system.harvest_begin(capacity_pairs=4000, bricks_per_pair=32, seed=seed, target=LEARNED_TARGET_BRICK_SOLVE)
+    for _ in range(12):
         b = oracle.apply(np.where(active, rng.standard_normal(built.storage_size), 0.0))
         system.solve(b, 1e-8, 600)
     samples = system.harvest_stop()
     oracle.close()
-    assert samples > 1000
-    return samples, system.train(steps, batch=32, learning_rate=2e-3, seed=seed)
+    assert samples > 2000
+    return samples, system.train(steps, batch=64, learning_rate=2e-3, seed=seed)
 
 
 def test_trained_network_gains_over_the_method_without_it(wing):
@@ -102,20 +104,44 @@ def test_trained_network_gains_over_the_method_without_it(wing):
 
     def run(kind):
         system.set_preconditioner(kind)
-        x, info = system.solve(b, 1e-8, 2000)
+        x, info = system.solve(b, 1e-8, 1500)
         residual = np.linalg.norm((b - oracle.apply(x))[active]) / np.linalg.norm(b[active])
         return info, residual
 
     jacobi, _ = run(PRECONDITIONER_JACOBI)
+    multigrid, _ = run(PRECONDITIONER_MULTIGRID)
     system.set_learned_parameters(unet.flatten(unet.init_params(11)).astype(np.float32))
     untrained, _ = run(PRECONDITIONER_LEARNED)
     samples, loss = harvest_and_train(system, built)
     trained, residual = run(PRECONDITIONER_LEARNED)
-    multigrid, _ = run(PRECONDITIONER_MULTIGRID)
+    trained_mg, residual_mg = run(PRECONDITIONER_LEARNED_MULTIGRID)
     oracle.close()
     system.set_preconditioner(PRECONDITIONER_MULTIGRID)
     print(f"samples {samples} loss {loss:.3e}; iterations: jacobi {jacobi['iterations']} untrained "
-          f"{untrained['iterations']} trained {trained['iterations']} multigrid {multigrid['iterations']}")
-    assert trained["converged"] and residual <= 1e-7
-    assert trained["iterations"] < jacobi["iterations"]
-    assert trained["iterations"] < untrained["iterations"] or not untrained["converged"]
+          f"{untrained['iterations']} trained {trained['iterations']} multigrid {multigrid['iterations']} "
+          f"learned multigrid {trained_mg['iterations']}")
+    # the normalised loss: the fraction of the brick-solve variance the network leaves unexplained
+    assert loss < 0.1
+    for info, res in ((trained, residual), (trained_mg, residual_mg)):
+        assert info["converged"] and not info["fallback_solves"] and res <= 1e-7
+    # what the trained network gains: against the same flexible solve with a Jacobi step alone, and
+    # against the untrained network (measured 102 vs 499 and 789)
+    assert trained["iterations"] * 2 < jacobi["iterations"]
+    assert trained["iterations"] * 2 < untrained["iterations"]
+    # in place of the composite cycle's fine pre-sweeps it keeps the multigrid iteration count
+    # within a few (measured 13 vs 12)
+    assert trained_mg["iterations"] <= multigrid["iterations"] + 4
+
+
+def test_fallback_finishes_an_unconverged_learned_solve(wing):
+    built, system = wing
+    rng = np.random.default_rng(5)
+    active = built.active.astype(bool)
+    oracle = port.PortSystem(built.topology)
+    b = oracle.apply(np.where(active, rng.standard_normal(built.storage_size), 0.0))
+    system.set_preconditioner(PRECONDITIONER_LEARNED)
+    x, info = system.solve(b, 1e-8, 3)   # 3 learned iterations cannot reach 1e-8
+    residual = np.linalg.norm((b - oracle.apply(x))[active]) / np.linalg.norm(b[active])
+    oracle.close()
+    system.set_preconditioner(PRECONDITIONER_MULTIGRID)
+    assert info["fallback_solves"] == 1 and info["converged"] and residual <= 1e-7
