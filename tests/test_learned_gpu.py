@@ -140,7 +140,7 @@ def test_fallback_finishes_an_unconverged_learned_solve(wing):
     oracle = port.PortSystem(built.topology)
     b = oracle.apply(np.where(active, rng.standard_normal(built.storage_size), 0.0))
     system.set_preconditioner(PRECONDITIONER_LEARNED)
-    x, info = system.solve(b, 1e-8, 3)   # 3 learned iterations cannot reach 1e-8
+    x, info = system.solve(b, 1e-8, 16)   # the learned form needs ~100 iterations, multigrid ~12
     residual = np.linalg.norm((b - oracle.apply(x))[active]) / np.linalg.norm(b[active])
     oracle.close()
     system.set_preconditioner(PRECONDITIONER_MULTIGRID)
