@@ -60,6 +60,12 @@ def parse_args():
                     help="build the workload, time one pcfd_time_kernel component (a few launches) and exit; "
                          "the small command an ncu capture of that component runs")
     ap.add_argument("--kernel-iterations", type=int, default=1)
+    ap.add_argument("--learned", action="store_true",
+                    help="the learned-preconditioner measurement: harvest brick pairs from seeded naca0012_slab / "
+                         "naca4412_wing runs, train, then time projections to 1e-8 with the learned forms against "
+                         "the multigrid on the same right-hand sides of the naca4412_wing case")
+    ap.add_argument("--train-steps", type=int, default=3000)
+    ap.add_argument("--harvest-runs", type=int, default=4, help="seeded harvest runs (alternating the two cases)")
     return ap.parse_args()
 
 
@@ -520,11 +526,122 @@ def run_reference(args, ranks: Ranks):
     return line
 
 
+# Network FLOPs per brick as the oracle defines it (oracle/unet.py LAYERS): 2*27*Cin*Cout per
+# output voxel of every convolution, plus the 16-wide head.
+LEARNED_FLOPS_PER_BRICK = 2 * 27 * (16 * 16 * 512 + 16 * 32 * 64 + 32 * 64 * 8 + 96 * 32 * 64 + 48 * 16 * 512) + 2 * 16 * 512
+
+
+def measured_peak_tflops() -> tuple[float, str]:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 1590.0, "fallback"
+
+
+def run_learned(args, ranks: Ranks):
+    """Projection time to 1e-8 under the learned preconditioner forms against the multigrid one,
+    on the same right-hand sides (state snapshots of the naca4412_wing run)."""
+    from paracfd_b200 import (LEARNED_TARGET_BRICK_SOLVE, MG_CYCLE_COMPOSITE, PRECONDITIONER_LEARNED,
+                              PRECONDITIONER_LEARNED_MULTIGRID, PRECONDITIONER_MULTIGRID, CompositeSystem)
+    from paracfd_b200.workloads import WORKLOADS, with_aoa
+
+    rng = np.random.default_rng(20261203)
+    harvest = []
+    t0 = time.time()
+    pairs_per_run = 4000 // max(args.harvest_runs, 1)
+    for k in range(args.harvest_runs):
+        name = ("naca0012_slab", "naca4412_wing")[k % 2]
+        spec = with_aoa(name, float(rng.uniform(0.0, 10.0)))
+        built = spec.build()
+        with CompositeSystem(built.topology, device=ranks.local, mg_cycle=MG_CYCLE_COMPOSITE) as system:
+            system.configure(speed=spec.speed, **spec.case)
+            system.initialize()
+            system.harvest_begin(capacity_pairs=4000, bricks_per_pair=32, seed=1000 + k, target=LEARNED_TARGET_BRICK_SOLVE)
+            before = system.harvest_stop()
+            system.harvest_begin(capacity_pairs=4000, bricks_per_pair=32, seed=1000 + k, target=LEARNED_TARGET_BRICK_SOLVE)
+            steps = 0
+            while steps < 400:
+                system.step()
+                steps += 1
+                if system.harvest_stop() - before >= pairs_per_run * 32:
+                    break
+                system.harvest_begin(capacity_pairs=4000, bricks_per_pair=32, seed=1000 + k, target=LEARNED_TARGET_BRICK_SOLVE)
+            samples = system.harvest_stop()
+        harvest.append({"case": name, "aoa": round(spec.aoa, 3), "steps": steps, "samples": samples - before})
+        built.close()
+    harvest_s = time.time() - t0
+
+    spec = WORKLOADS["naca4412_wing"]
+    built = spec.build()
+    system = CompositeSystem(built.topology, device=ranks.local, mg_cycle=MG_CYCLE_COMPOSITE)
+    system.configure(speed=spec.speed, **spec.case)
+    system.initialize()
+    t0 = time.time()
+    loss = system.train(args.train_steps, batch=64, learning_rate=2e-3, seed=7)
+    system.synchronize()
+    train_s = time.time() - t0
+    forward_ms = system.time_kernel(16, 10)
+    bricks = non_covered_bricks(built.topology)
+    peak, peak_kind = measured_peak_tflops()
+    achieved = LEARNED_FLOPS_PER_BRICK * bricks / (forward_ms * 1e-3) / 1e12
+
+    rho = spec.case["rho"]
+    kinds = {"multigrid": PRECONDITIONER_MULTIGRID, "learned_multigrid": PRECONDITIONER_LEARNED_MULTIGRID,
+             "learned": PRECONDITIONER_LEARNED}
+    results = {k: {"ms": [], "iterations": [], "residual": [], "fallbacks": 0} for k in kinds}
+    for step in range(args.warmup + args.steps):
+        stats = system.step()
+        if step < args.warmup:
+            continue
+        dt = stats["dt"]
+        faces, special, pressure = system.get_faces(), system.get_special(), system.get_pressure()
+        for name, kind in kinds.items():
+            system.set_faces(*faces)
+            system.set_special(*special)
+            system.set_pressure(pressure)
+            system.set_preconditioner(kind)
+            system.event_record(0)
+            res = system.project(rho, dt, 1e-8, 600, warm_start=True)
+            system.event_record(1)
+            r = results[name]
+            r["ms"].append(system.event_elapsed(0, 1))
+            r["iterations"].append(res["iterations"])
+            r["residual"].append(res["relative_residual"])
+            r["fallbacks"] += res["fallback_solves"]
+        system.set_faces(*faces)
+        system.set_special(*special)
+        system.set_pressure(pressure)
+        system.set_preconditioner(PRECONDITIONER_MULTIGRID)
+    summary = {k: {"projection_ms": round(statistics.mean(v["ms"]), 3), "iterations": round(statistics.mean(v["iterations"]), 2),
+                   "final_residual_max": max(v["residual"]), "fallbacks": v["fallbacks"]} for k, v in results.items()}
+    mg_ms = summary["multigrid"]["projection_ms"]
+    line = {
+        "metric": "projection time to 1e-8 relative residual, learned (NN) vs multigrid preconditioner",
+        "value": summary["learned_multigrid"]["projection_ms"], "unit": "ms", "higher_is_better": False,
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "vs_multigrid": round(mg_ms / summary["learned_multigrid"]["projection_ms"], 3),
+        "dtype": "bf16 network / f64 Krylov", "data": "synthetic analytic geometry",
+        "config": dict(spec.describe(), leaf_cells=built.leaf_cells, bricks=bricks, mg_cycle="composite",
+                       harvest_target="brick solve", train_steps=args.train_steps, batch=64),
+        "preconditioners": summary,
+        "harvest": harvest, "harvest_s": round(harvest_s, 1), "train_s": round(train_s, 1), "train_loss": loss,
+        "network": {"forward_ms": round(forward_ms, 3), "flops_per_brick": LEARNED_FLOPS_PER_BRICK,
+                    "roofline": {"bound": "tensor", "achieved": round(achieved, 1), "peak": peak, "unit": "TFLOP/s",
+                                 "frac": round(achieved / peak, 4), "peak_kind": peak_kind}},
+    }
+    system.close()
+    built.close()
+    return line
+
+
 def main():
     args = parse_args()
     ranks = Ranks(collective=args.impl == "ours")
     try:
-        if args.kernel_only is not None:
+        if args.learned:
+            line = run_learned(args, ranks) if ranks.rank == 0 else None
+        elif args.kernel_only is not None:
             line = run_kernel_only(args)
         elif args.impl == "reference":
             line = run_reference(args, ranks)

@@ -396,7 +396,7 @@ pcfd_status pcfd_core_loads(pcfd_system* system, double pressure_reference, cons
  * pre-smoothing / coarse correction / post-smoothing of the separate-launch cycle, 9/14/15 one
  * GCRO column orthogonalisation against 3 recycled + 13/5/24 basis vectors, 10/11/12/13 the
  * fused cycle's pre-smoothing / restriction / aggregation hierarchy / prolongation +
- * post-smoothing), measured with CUDA events on the system stream over
+ * post-smoothing, 16 the learned network on every brick), measured with CUDA events on the system stream over
  * `iterations` back-to-back repetitions on resident scratch vectors. */
 pcfd_status pcfd_time_kernel(pcfd_system* system, int32_t which, int32_t iterations, double* ms_per_launch);
 /* Device-timeline markers on the system stream (slots 0..7) for whole-job timing. */

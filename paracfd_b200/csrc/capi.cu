@@ -919,6 +919,7 @@ pcfd_status pcfd_time_kernel(pcfd_system* system, int32_t which, int32_t iterati
                 block_update(s, Q, h + kMaxSet + 1, s.Ad, none, -1.0, nullptr, 1, h + 2 * (kMaxSet + 1));
                 break;
             }
+            case 16: learned_apply(s, s.scratch_p, s.scratch_out); break;
             default: throw Error(PCFD_INVALID_ARG, "unknown kernel id");
             }
         };
