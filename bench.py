@@ -53,6 +53,8 @@ def parse_args():
                     help="coarse-correction weighting of the multigrid cycle (pcfd_mg_cycle)")
     ap.add_argument("--stage-sweeps", type=int, default=0,
                     help="composite cycle: Jacobi sweeps per stage before and after its correction (0: 6)")
+    ap.add_argument("--block-iterations", type=int, default=0,
+                    help="composite cycle: Chebyshev iterations of the brick block pre-smoother (0: Jacobi pre-sweeps)")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU sample of the ours arm")
     ap.add_argument("--no-reference-gpu", action="store_true", help="reference arm: skip the sm_100a reference run")
     ap.add_argument("--profile-region", type=int, default=0, help="PCFD_PROFILE_* region timed per launch")
@@ -65,6 +67,7 @@ def parse_args():
                          "naca4412_wing runs, train, then time projections to 1e-8 with the learned forms against "
                          "the multigrid on the same right-hand sides of the naca4412_wing case")
     ap.add_argument("--train-steps", type=int, default=3000)
+    ap.add_argument("--no-learned", action="store_true", help="skip the short learned-preconditioner comparison")
     ap.add_argument("--harvest-runs", type=int, default=4, help="seeded harvest runs (alternating the two cases)")
     return ap.parse_args()
 
@@ -304,7 +307,8 @@ def run_ours(args, ranks: Ranks):
     bricks = non_covered_bricks(built.topology)
     system = CompositeSystem(built.topology, MG_FP32 if args.mg == "fp32" else MG_FP64, device=ranks.local,
                              mg_cycle={"reference": 0, "corrected": 1, "composite": 2}[args.mg_cycle],
-                             gmres_restart=args.restart, mg_stage_sweeps=args.stage_sweeps)
+                             gmres_restart=args.restart, mg_stage_sweeps=args.stage_sweeps,
+                             mg_block_iterations=args.block_iterations)
     system.configure(speed=spec.speed, **spec.case)
     slots = system.inflow_layout()
     faces = len(slots) * spec.brick_size ** 2
@@ -392,7 +396,7 @@ def run_ours(args, ranks: Ranks):
         "vs_baseline": None, "dtype": "f32 state / f64 pressure", "data": "synthetic analytic geometry",
         "config": dict(spec.describe(), leaf_cells=built.leaf_cells, storage=built.storage_size,
                        mg=args.mg, mg_cycle=args.mg_cycle, gcro_restart=args.restart or 24,
-                       stage_sweeps=args.stage_sweeps or 6, parallelism=f"replicas{n}",
+                       stage_sweeps=args.stage_sweeps or 6, block_iterations=args.block_iterations, parallelism=f"replicas{n}",
                        l2="inputs larger than L2"),
         "projection_ms": round(statistics.mean(s["projection_ms"] for s in stats), 3),
         "iterations_per_step": round(statistics.mean(s["pressure"]["iterations"] for s in stats), 2),
@@ -430,6 +434,13 @@ def run_ours(args, ranks: Ranks):
             line["cpu_baseline"] = {"value": None, "error": str(exc)[:200]}
     system.close()
     built.close()
+    if ranks.rank == 0 and n == 1 and not args.no_learned:
+        # the learned-preconditioner comparison (a short --learned run) beside the headline
+        try:
+            short = argparse.Namespace(**{**vars(args), "harvest_runs": 2, "train_steps": 1500, "steps": 2, "warmup": 2})
+            line["learned"] = run_learned(short, ranks)
+        except Exception as exc:
+            line["learned"] = {"error": str(exc)[:200]}
     return line
 
 
@@ -440,7 +451,8 @@ def run_kernel_only(args):
     built = spec.build()
     system = CompositeSystem(built.topology, MG_FP32 if args.mg == "fp32" else MG_FP64,
                              mg_cycle={"reference": 0, "corrected": 1, "composite": 2}[args.mg_cycle],
-                             gmres_restart=args.restart, mg_stage_sweeps=args.stage_sweeps)
+                             gmres_restart=args.restart, mg_stage_sweeps=args.stage_sweeps,
+                             mg_block_iterations=args.block_iterations)
     ms = system.time_kernel(args.kernel_only, args.kernel_iterations)
     line = {"kernel_only": args.kernel_only, "workload": args.workload, "ms_per_launch": ms,
             "iterations": args.kernel_iterations, "launches": system.launch_count()}
@@ -586,33 +598,26 @@ def run_learned(args, ranks: Ranks):
     peak, peak_kind = measured_peak_tflops()
     achieved = LEARNED_FLOPS_PER_BRICK * bricks / (forward_ms * 1e-3) / 1e12
 
-    rho = spec.case["rho"]
     kinds = {"multigrid": PRECONDITIONER_MULTIGRID, "learned_multigrid": PRECONDITIONER_LEARNED_MULTIGRID,
              "learned": PRECONDITIONER_LEARNED}
     results = {k: {"ms": [], "iterations": [], "residual": [], "fallbacks": 0} for k in kinds}
+    system.keep_projection_start(True)
     for step in range(args.warmup + args.steps):
-        stats = system.step()
+        system.step()
         if step < args.warmup:
             continue
-        dt = stats["dt"]
-        faces, special, pressure = system.get_faces(), system.get_special(), system.get_pressure()
+        # the step's own projection solved again from its saved start (same right-hand side, warm
+        # start and recycled subspace) under each preconditioner
         for name, kind in kinds.items():
-            system.set_faces(*faces)
-            system.set_special(*special)
-            system.set_pressure(pressure)
             system.set_preconditioner(kind)
-            system.event_record(0)
-            res = system.project(rho, dt, 1e-8, 600, warm_start=True)
-            system.event_record(1)
+            ms, res = system.resolve_projection(1e-8, 600)
             r = results[name]
-            r["ms"].append(system.event_elapsed(0, 1))
+            r["ms"].append(ms)
             r["iterations"].append(res["iterations"])
             r["residual"].append(res["relative_residual"])
             r["fallbacks"] += res["fallback_solves"]
-        system.set_faces(*faces)
-        system.set_special(*special)
-        system.set_pressure(pressure)
         system.set_preconditioner(PRECONDITIONER_MULTIGRID)
+        system.resolve_projection(1e-8, 600)   # leave the multigrid solve's pressure and subspace
     summary = {k: {"projection_ms": round(statistics.mean(v["ms"]), 3), "iterations": round(statistics.mean(v["iterations"]), 2),
                    "final_residual_max": max(v["residual"]), "fallbacks": v["fallbacks"]} for k, v in results.items()}
     mg_ms = summary["multigrid"]["projection_ms"]

@@ -176,6 +176,9 @@ typedef struct pcfd_options {
     int32_t gmres_restart;           /* columns per GCRO/LGMRES cycle, 1..24; 0: the reference's 24 */
     int32_t mg_stage_sweeps;         /* composite cycle: Jacobi sweeps before and after each stage's
                                         coarse correction, 1..16; 0: 6 */
+    int32_t mg_block_iterations;     /* composite cycle: 0 = the reference's two Jacobi pre-sweeps on
+                                        the fine level; k = 1..64: instead, k Chebyshev iterations of
+                                        each brick's own diagonal block solve in shared memory */
 } pcfd_options;
 
 /* Coarse-correction weighting of the multigrid cycle.  The aggregation coarse operators are
@@ -335,6 +338,15 @@ pcfd_status pcfd_projection_correct(pcfd_system* system, double rho, double dt);
 /* build rhs -> solve -> (if converged) shadow, correct, divergence. */
 pcfd_status pcfd_projection_project(pcfd_system* system, double rho, double dt, double tolerance,
                                     int32_t max_iterations, int32_t warm_start,
+                                    pcfd_solve_result* result);
+
+/* No reference counterpart.  keep != 0: every projection saves its solver start (warm-start
+ * pressure, recycled GCRO subspace) on the device; resolve solves the last projection's system
+ * again from that start with the current preconditioner and returns its device time (CUDA
+ * events on the system stream) -- the same right-hand side and start for every preconditioner
+ * being compared. */
+pcfd_status pcfd_projection_keep_start(pcfd_system* system, int32_t keep);
+pcfd_status pcfd_projection_resolve(pcfd_system* system, double tolerance, int32_t max_iterations, double* ms,
                                     pcfd_solve_result* result);
 
 /* ---- cell momentum (DeviceCompositeCellMomentumTransport, amr_advection.h:269-405) ---------- */

@@ -82,11 +82,11 @@ class CompositeSystem:
 
     def __init__(self, topology: Topology, mg_precision: int = MG_FP64, device: int = 0,
                  momentum_min_volume_fraction: float = 0.0, fused_smoother: bool = True,
-                 mg_cycle: int = 0, gmres_restart: int = 0, mg_stage_sweeps: int = 0):
+                 mg_cycle: int = 0, gmres_restart: int = 0, mg_stage_sweeps: int = 0, mg_block_iterations: int = 0):
         self._lib = capi.load()
         self._topology = topology   # keep the caller's arrays alive during creation
         opts = Options(mg_precision, device, None, momentum_min_volume_fraction, 0 if fused_smoother else 1, mg_cycle,
-                       gmres_restart, mg_stage_sweeps)
+                       gmres_restart, mg_stage_sweeps, mg_block_iterations)
         handle = C.c_void_p()
         check(self._lib.pcfd_system_create(C.byref(topology), C.byref(opts), C.byref(handle)))
         self.handle = handle
@@ -144,6 +144,18 @@ class CompositeSystem:
         check(self._lib.pcfd_pressure_solve_host(self.handle, ptr(x, C.c_double), ptr(b, C.c_double), tolerance,
                                                  max_iterations, int(x0 is not None), C.byref(res)))
         return x, res.as_dict()
+
+    def keep_projection_start(self, keep: bool = True):
+        check(self._lib.pcfd_projection_keep_start(self.handle, int(keep)))
+
+    def resolve_projection(self, tolerance: float, max_iterations: int):
+        """The last projection solved again from its saved start: (device ms, solve result)."""
+        ms = C.c_double()
+        res = SolveResult()
+        status = self._lib.pcfd_projection_resolve(self.handle, tolerance, max_iterations, C.byref(ms), C.byref(res))
+        if status not in (capi.PCFD_OK, capi.PCFD_NOT_CONVERGED):
+            check(status)
+        return ms.value, res.as_dict()
 
     # ---- learned preconditioner ---------------------------------------------------------------
     def set_preconditioner(self, kind: int):

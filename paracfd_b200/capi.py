@@ -82,7 +82,8 @@ class Topology(C.Structure):
 class Options(C.Structure):
     _fields_ = [("mg_precision", C.c_int32), ("device", C.c_int32), ("stream", C.c_void_p),
                 ("momentum_min_volume_fraction", C.c_double), ("disable_fused_smoother", C.c_int32),
-                ("mg_cycle", C.c_int32), ("gmres_restart", C.c_int32), ("mg_stage_sweeps", C.c_int32)]
+                ("mg_cycle", C.c_int32), ("gmres_restart", C.c_int32), ("mg_stage_sweeps", C.c_int32),
+                ("mg_block_iterations", C.c_int32)]
 
 
 class SolveResult(C.Structure):
@@ -208,6 +209,9 @@ SIGNATURES = {
     "pcfd_profile_end": (C.c_int, [C.c_void_p, _f64p, C.c_int32, C.POINTER(C.c_int32)]),
     "pcfd_builder_last_error": (C.c_char_p, []),
     "pcfd_set_preconditioner": (C.c_int, [C.c_void_p, C.c_int32]),
+    "pcfd_projection_keep_start": (C.c_int, [C.c_void_p, C.c_int32]),
+    "pcfd_projection_resolve": (C.c_int, [C.c_void_p, C.c_double, C.c_int32, C.POINTER(C.c_double),
+                                          C.POINTER(SolveResult)]),
     "pcfd_learned_parameter_count": (C.c_int, [C.POINTER(C.c_int64)]),
     "pcfd_learned_set_parameters": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int64]),
     "pcfd_learned_get_parameters": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int64]),

@@ -209,6 +209,11 @@ namespace pcfd
                 require(options->mg_stage_sweeps > 0 && options->mg_stage_sweeps <= 16, "mg_stage_sweeps must be 0..16");
                 s.mg_stage_sweeps = options->mg_stage_sweeps;
             }
+            if (options && options->mg_block_iterations)
+            {
+                require(options->mg_block_iterations > 0 && options->mg_block_iterations <= 64, "mg_block_iterations must be 0..64");
+                s.mg_block_iterations = options->mg_block_iterations;
+            }
             const int cycle = options ? options->mg_cycle : PCFD_MG_CYCLE_REFERENCE;
             require(cycle >= PCFD_MG_CYCLE_REFERENCE && cycle <= PCFD_MG_CYCLE_COMPOSITE, "unknown multigrid cycle");
             if (cycle == PCFD_MG_CYCLE_CORRECTED) { s.mg_prolong_scale = 2.0; s.mg_lattice_scale = 1.5; }
@@ -699,6 +704,32 @@ pcfd_status pcfd_preconditioner_fused(pcfd_system* system, int32_t* fused)
         System& s = sys(system);
         require(fused != nullptr, "null output");
         *fused = s.fine.enabled ? 1 : 0;
+    });
+}
+
+pcfd_status pcfd_projection_keep_start(pcfd_system* system, int32_t keep)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        if (keep && !s.start_pressure.p)
+        {
+            s.start_pressure.alloc(size_t(s.Sp));
+            s.start_recycle_u.alloc(size_t(System::recycle_capacity) * s.Sp);
+            s.start_recycle_c.alloc(size_t(System::recycle_capacity) * s.Sp);
+        }
+        s.keep_projection_start = keep != 0;
+        s.start_saved = false;
+    });
+}
+
+pcfd_status pcfd_projection_resolve(pcfd_system* system, double tolerance, int32_t max_iterations, double* ms,
+                                    pcfd_solve_result* result)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(tolerance > 0 && max_iterations >= 0 && ms, "invalid resolve request");
+        const pcfd_solve_result r = resolve_projection(s, tolerance, max_iterations, ms);
+        if (result) *result = r;
     });
 }
 

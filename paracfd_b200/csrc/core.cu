@@ -41,6 +41,49 @@ namespace pcfd
         }
     }
 
+    // the solver's starting state of a projection: warm-start pressure and recycled subspace
+    void save_projection_start(System& s, bool warm)
+    {
+        const size_t n = size_t(s.Sp) * sizeof(double);
+        s.start_saved = true;
+        s.start_warm = warm;
+        cuda_check(cudaMemcpyAsync(s.start_pressure, s.pressure, n, cudaMemcpyDeviceToDevice, s.stream), "save start");
+        s.start_recycle_count = s.recycle_count;
+        if (s.recycle_count)
+        {
+            cuda_check(cudaMemcpyAsync(s.start_recycle_u, s.recycle_u, n * s.recycle_count, cudaMemcpyDeviceToDevice, s.stream), "save U");
+            cuda_check(cudaMemcpyAsync(s.start_recycle_c, s.recycle_c, n * s.recycle_count, cudaMemcpyDeviceToDevice, s.stream), "save C");
+        }
+    }
+
+    // solves the last projection's system again from its saved start with the current
+    // preconditioner; the pressure and recycled subspace end as that solve leaves them
+    pcfd_solve_result resolve_projection(System& s, double tolerance, int max_iterations, double* ms)
+    {
+        require(s.keep_projection_start && s.start_saved, "no saved projection start");
+        const size_t n = size_t(s.Sp) * sizeof(double);
+        cuda_check(cudaMemcpyAsync(s.pressure, s.start_pressure, n, cudaMemcpyDeviceToDevice, s.stream), "restore start");
+        s.recycle_count = s.start_recycle_count;
+        if (s.recycle_count)
+        {
+            cuda_check(cudaMemcpyAsync(s.recycle_u, s.start_recycle_u, n * s.recycle_count, cudaMemcpyDeviceToDevice, s.stream), "restore U");
+            cuda_check(cudaMemcpyAsync(s.recycle_c, s.start_recycle_c, n * s.recycle_count, cudaMemcpyDeviceToDevice, s.stream), "restore C");
+        }
+        cudaEvent_t start, stop;
+        cuda_check(cudaEventCreate(&start), "event");
+        cuda_check(cudaEventCreate(&stop), "event");
+        cuda_check(cudaEventRecord(start, s.stream), "event");
+        const pcfd_solve_result r = solve(s, s.pressure, s.rhs, tolerance, max_iterations, s.start_warm);
+        cuda_check(cudaEventRecord(stop, s.stream), "event");
+        cuda_check(cudaEventSynchronize(stop), "event");
+        float t = 0;
+        cuda_check(cudaEventElapsedTime(&t, start, stop), "event");
+        cudaEventDestroy(start);
+        cudaEventDestroy(stop);
+        *ms = t;
+        return r;
+    }
+
     Momentum& momentum_of(System& s)
     {
         require(s.momentum && s.momentum->ready, "cell-momentum topology was not built");
@@ -51,6 +94,7 @@ namespace pcfd
     {
         launch_integrated_flux(s);
         launch_normalize(s, rho / dt, true);
+        if (s.keep_projection_start) save_projection_start(s, warm);
         const pcfd_solve_result r = solve(s, s.pressure, s.rhs, tolerance, max_iterations, warm);
         if (r.converged)
         {

@@ -169,6 +169,7 @@ namespace pcfd
         int mg_precision = PCFD_MG_FP64;
         double mg_prolong_scale = 1.0, mg_lattice_scale = 1.0;   // coarse-correction weights (pcfd_mg_cycle)
         int mg_stage_sweeps = 6;                                 // composite-stage sweeps (pcfd_options)
+        int mg_block_iterations = 0;                             // composite cycle: brick block pre-smoother (pcfd_options)
         cudaStream_t stream = nullptr;
         bool own_stream = false;
         int device = 0;
@@ -248,6 +249,11 @@ namespace pcfd
         DBuf<int> cf_group_offset, cf_group_member;
         DBuf<double> cf_group_area;
 
+        // saved solver start of the last projection (pcfd_projection_keep_start / resolve)
+        bool keep_projection_start = false, start_saved = false, start_warm = false;
+        int start_recycle_count = 0;
+        DBuf<double> start_pressure, start_recycle_u, start_recycle_c;
+
         // preconditioner of the Krylov solvers (pcfd_preconditioner) and the learned network state
         int preconditioner = PCFD_PRECONDITIONER_MULTIGRID;
         struct Learned* learned = nullptr;
@@ -322,6 +328,7 @@ namespace pcfd
     void learned_preconditioner(System& s, const double* r, double* z, bool coarse);   // smoother.cu
     pcfd_solve_result solve(System& s, double* x, const double* b, double tolerance, int max_iterations, bool warm);
     void allocate_gcro(System& s);   // GCRO/LGMRES basis storage (capi.cu), idempotent
+    pcfd_solve_result resolve_projection(System& s, double tolerance, int max_iterations, double* ms);   // core.cu
     // ---- learned preconditioner (learned.cu) ----
     int64_t learned_parameter_count();
     void learned_destroy(System& s);

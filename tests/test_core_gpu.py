@@ -46,3 +46,18 @@ def test_initialize_and_steps_track_reference(pair):
         # both solve to 1e-8; FP32 transport with different summation order, FP32 (reference)
         # vs FP64 (here) operator coefficients: states agree to 1e-4 of the freestream
         assert err <= 1e-4, (step, err)
+
+
+def test_resolve_repeats_the_step_projection(pair):
+    """The saved projection start reproduces the step's own solve: same iterations, same pressure."""
+    rc, s, _ = pair
+    s.keep_projection_start(True)
+    stats = s.step()
+    p_step = s.get_pressure()
+    ms, res = s.resolve_projection(1e-8, 600)
+    s.keep_projection_start(False)
+    assert ms > 0 and res["converged"]
+    assert res["iterations"] == stats["pressure"]["iterations"]
+    act = rc.active.astype(bool)
+    p = s.get_pressure()
+    assert np.abs(p - p_step)[act].max() <= 1e-12 * max(np.abs(p_step[act]).max(), 1e-300)
