@@ -175,7 +175,7 @@ typedef struct pcfd_options {
     int32_t mg_cycle;                /* pcfd_mg_cycle */
     int32_t gmres_restart;           /* columns per GCRO/LGMRES cycle, 1..24; 0: the reference's 24 */
     int32_t mg_stage_sweeps;         /* composite cycle: Jacobi sweeps before and after each stage's
-                                        coarse correction, 1..16; 0: 6 */
+                                        coarse correction, 1..16; 0: 8 */
     int32_t mg_block_iterations;     /* composite cycle: 0 = the reference's two Jacobi pre-sweeps on
                                         the fine level; k = 1..64: instead, k Chebyshev iterations of
                                         each brick's own diagonal block solve in shared memory */

@@ -266,6 +266,23 @@ namespace pcfd
             return pack8(acc);
         }
 
+        // address of the 8 channels [c0, c0 + 8) of voxel (x,y,z) of sample b for a SAME or UP source
+        template <int N> __device__ inline const bf16* source_address(const ConvSource& s, int64_t b, int x, int y, int z, int c0)
+        {
+            const int C = s.channels;
+            if (s.mode == SAME) return s.x + ((b * N + z) * N + y) * int64_t(N) * C + int64_t(x) * C + c0;
+            constexpr int M = N / 2;
+            return s.x + ((b * M + z / 2) * M + y / 2) * int64_t(M) * C + int64_t(x / 2) * C + c0;
+        }
+        __device__ inline void cp_async16(void* dst, const void* src)
+        {
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+        }
+        __device__ inline void cp_async_wait_all()
+        {
+            asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+        }
+
         // One CTA of 128 threads per group of Geometry<N>::NB bricks (persistent over groups).
         // Shared memory: A [2][NPOS][16 B] | B [27][2][cout][16 B] | barrier | TMEM address.
         template <int N>
@@ -304,18 +321,39 @@ namespace pcfd
                     const ConvSource& s = p.src[si];
                     for (int c0 = 0; c0 < s.channels; c0 += 16)
                     {
-                        // stage 16 channels of the group's bricks and the matching weights
-                        for (int i = tid; i < nb * V * 2; i += 128)
+                        // stage 16 channels of the group's bricks and the matching weights: copies
+                        // straight to shared memory (cp.async) for plain and upsampled sources, a
+                        // register average for pooled ones (two voxels in flight per thread)
+                        const int items = nb * V * 2;
+                        if (s.mode != POOL)
                         {
-                            const int half = i & 1, v = (i >> 1) % V, b = (i >> 1) / V;
-                            const int x = v % N, y = (v / N) % N, z = v / (N * N);
-                            A[half * Gm::NPOS + padded<N>(b, x, y, z)] = load_source<N>(s, b0 + b, x, y, z, c0 + 8 * half);
+                            for (int i = tid; i < items; i += 128)
+                            {
+                                const int half = i & 1, v = (i >> 1) % V, b = (i >> 1) / V;
+                                const int x = v % N, y = (v / N) % N, z = v / (N * N);
+                                cp_async16(&A[half * Gm::NPOS + padded<N>(b, x, y, z)], source_address<N>(s, b0 + b, x, y, z, c0 + 8 * half));
+                            }
+                        }
+                        else
+                        {
+                            for (int i = tid; i < items; i += 256)
+                            {
+                                const int j = i + 128;
+                                uint4 u0, u1 = make_uint4(0, 0, 0, 0);
+                                const int h0 = i & 1, v0 = (i >> 1) % V, bb0 = (i >> 1) / V;
+                                u0 = load_source<N>(s, b0 + bb0, v0 % N, (v0 / N) % N, v0 / (N * N), c0 + 8 * h0);
+                                const int h1 = j & 1, v1 = (j >> 1) % V, bb1 = (j >> 1) / V;
+                                if (j < items) u1 = load_source<N>(s, b0 + bb1, v1 % N, (v1 / N) % N, v1 / (N * N), c0 + 8 * h1);
+                                A[h0 * Gm::NPOS + padded<N>(bb0, v0 % N, (v0 / N) % N, v0 / (N * N))] = u0;
+                                if (j < items) A[h1 * Gm::NPOS + padded<N>(bb1, v1 % N, (v1 / N) % N, v1 / (N * N))] = u1;
+                            }
                         }
                         for (int i = tid; i < 27 * 2 * cout; i += 128)
                         {
                             const int co = i % cout, half = (i / cout) & 1, tap = i / (2 * cout);
-                            Bw[i] = *reinterpret_cast<const uint4*>(s.w + (int64_t(tap) * cout + co) * s.channels + c0 + 8 * half);
+                            cp_async16(&Bw[i], s.w + (int64_t(tap) * cout + co) * s.channels + c0 + 8 * half);
                         }
+                        cp_async_wait_all();
                         fence_async_shared();
                         __syncthreads();
                         if (tid == 0)
