@@ -14,6 +14,7 @@
 // in a third.  No atomics: results are deterministic run to run.  The state is double-buffered.
 #include "momentum.h"
 
+#include <algorithm>
 #include <cmath>
 
 namespace pcfd
@@ -870,19 +871,31 @@ namespace pcfd
             if (threadIdx.x == 0) { block_partial[2 * blockIdx.x] = vmax; block_partial[2 * blockIdx.x + 1] = rmax; }
         }
 
+        // grid-wide maxima of the per-block partials and of |special|; out (zeroed before) holds the
+        // non-negative maxima as float bit patterns, whose unsigned order is their float order
         __global__ void __launch_bounds__(256) cfl_final_kernel(const float* __restrict__ partial, int count, const float* __restrict__ special,
-            int nspecial, float* __restrict__ out)
+            int nspecial, unsigned int* __restrict__ out)
         {
             __shared__ float shared[8];
             float vm = 0.0f, rm = 0.0f, sm = 0.0f;
-            for (int q = threadIdx.x; q < count; q += blockDim.x) { vm = fmaxf(vm, partial[2 * q]); rm = fmaxf(rm, partial[2 * q + 1]); }
-            for (int q = threadIdx.x; q < nspecial; q += blockDim.x) sm = fmaxf(sm, fabsf(special[q]));
+            const int stride = gridDim.x * blockDim.x;
+            for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < count; q += stride)
+            {
+                vm = fmaxf(vm, partial[2 * q]);
+                rm = fmaxf(rm, partial[2 * q + 1]);
+            }
+            for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nspecial; q += stride) sm = fmaxf(sm, fabsf(special[q]));
             vm = block_max(vm, shared);
             __syncthreads();
             rm = block_max(rm, shared);
             __syncthreads();
             sm = block_max(sm, shared);
-            if (threadIdx.x == 0) { out[0] = vm; out[1] = rm; out[2] = sm; out[3] = 0.0f; }
+            if (threadIdx.x == 0)
+            {
+                atomicMax(&out[0], __float_as_uint(vm));
+                atomicMax(&out[1], __float_as_uint(rm));
+                atomicMax(&out[2], __float_as_uint(sm));
+            }
         }
 
         CompactArgs compact_args(System& s, Momentum& m)
@@ -1049,7 +1062,13 @@ namespace pcfd
         if (db)
             cfl_deferred_kernel<<<db, 256, 0, launch_stream(s)>>>(m.nD, m.d_dof, m.d_offset, m.d_edge, m.d_sign, s.structured, k, s.u, s.v, s.w,
                                                          s.special, m.x, m.y, m.z, m.dx, m.reduce_partial.p + 2 * cb);
-        cfl_final_kernel<<<1, 256, 0, launch_stream(s)>>>(m.reduce_partial, cb + db, s.special, s.cf_count + s.eb_count, m.reduce_result);
+        cuda_check(cudaMemsetAsync(m.reduce_result, 0, 4 * sizeof(float), s.stream), "cfl maxima");
+        {
+            const int work = std::max(cb + db, s.cf_count + s.eb_count);
+            const int grid = std::max(1, std::min(592, blocks_for(work)));
+            cfl_final_kernel<<<grid, 256, 0, launch_stream(s)>>>(m.reduce_partial, cb + db, s.special, s.cf_count + s.eb_count,
+                                                                 reinterpret_cast<unsigned int*>(m.reduce_result.p));
+        }
         cuda_check(cudaMemcpyAsync(m.pinned, m.reduce_result, 4 * sizeof(float), cudaMemcpyDeviceToHost, s.stream), "cfl readback");
         cuda_check(cudaStreamSynchronize(s.stream), "cfl readback");
         for (int q = 0; q < 4; ++q) out[q] = m.pinned[q];

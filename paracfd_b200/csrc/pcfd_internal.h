@@ -125,7 +125,7 @@ namespace pcfd
         DBuf<int> gather_offset, gather_entry;  // base cell -> partials (>= 0) / deferred rows (< 0)
         DBuf<double> t, z;                      // [S] deferred structured rows, ping-pong iterate
         DBuf<double> damping;                   // [levels][14] w / D of non-deferred rows
-        DBuf<float> damping32, z32, z32b, r32, t32;   // FP32 multigrid: float fine-level buffers
+        DBuf<float> damping32, z32, z32b, r32, t32, res32;   // FP32 multigrid: float fine-level buffers
     };
 
     // Up to kMaxSet vectors of one system, passed by value to the fused block kernels (krylov.cu):

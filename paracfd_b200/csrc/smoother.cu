@@ -652,6 +652,7 @@ namespace pcfd
             f.z32b.alloc(size_t(S));
             f.r32.alloc(size_t(S));
             f.t32.alloc(size_t(S));
+            f.res32.alloc(size_t(S));
         }
         f.code.upload(code);
         f.deferred_count = int(ddof.size());
@@ -812,9 +813,9 @@ namespace pcfd
 
     namespace
     {
-        template <class TC>
+        template <class TC, class TR>
         __global__ void gather_first_kernel(int cells, const int* __restrict__ offset, const int* __restrict__ dof,
-                                            const double* __restrict__ residual, TC* __restrict__ rhs)
+                                            const TR* __restrict__ residual, TC* __restrict__ rhs)
         {
             const int c = blockIdx.x * blockDim.x + threadIdx.x;
             if (c >= cells) return;
@@ -881,12 +882,35 @@ namespace pcfd
             brick_pipe_kernel<3, double, double, TC, 0><<<pipe_grid(s), 256, 0, launch_stream(s)>>>(
                 view(s), s.active_bricks, z, r, res, f.t.p, nullptr, nullptr, f.damping.p);
             finish<2, double, double, TC, 0>(s, z, r, res, static_cast<const TC*>(nullptr), f.t.p);
-            gather_first_kernel<TC><<<blocks_for(first.cells), kThreads, 0, launch_stream(s)>>>(
+            gather_first_kernel<TC, double><<<blocks_for(first.cells), kThreads, 0, launch_stream(s)>>>(
                 first.cells, s.fine_restrict_offset, s.fine_restrict_dof, res, first.rhs);
             cuda_check(cudaMemsetAsync(first.x, 0, size_t(first.cells) * sizeof(TC), s.stream), "clear stage correction");
             composite_levels(s);
             sweep<double, double, TC, 2>(s, z, r, a, first.x.p);
             sweep<double, double, TC, 0>(s, a, r, z, nullptr);
+            cuda_check(cudaGetLastError(), "composite preconditioner");
+        }
+
+        // the composite cycle with the FP32 multigrid: the fine sweeps on float copies as in the
+        // reference cycle's FP32 path (r converted once by the first sweep, the iterate
+        // ping-ponging between two float buffers, the residual gathered from floats, only the last
+        // sweep writing the double result)
+        void composite_cycle_fp32(System& s, const double* r, double* z, MgLevel<float>& first)
+        {
+            FineSmoother& f = s.fine;
+            float *a = f.z32.p, *b = f.z32b.p, *r32 = f.r32.p, *res = f.res32.p;
+            first_sweep_kernel<float><<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(
+                f.code, s.brick_level, f.damping32.p, s.diagonal, s.active, r, a, r32, s.structured, s.S, 2.0 / 3.0);
+            sweep<float, float, float, 0>(s, a, r32, b, nullptr);
+            brick_pipe_kernel<3, float, float, float, 0><<<pipe_grid(s), 256, 0, launch_stream(s)>>>(
+                view(s), s.active_bricks, b, r32, res, f.t32.p, nullptr, nullptr, f.damping32.p);
+            finish<2, float, float, float, 0>(s, b, r32, res, static_cast<const float*>(nullptr), f.t32.p);
+            gather_first_kernel<float, float><<<blocks_for(first.cells), kThreads, 0, launch_stream(s)>>>(
+                first.cells, s.fine_restrict_offset, s.fine_restrict_dof, res, first.rhs);
+            cuda_check(cudaMemsetAsync(first.x, 0, size_t(first.cells) * sizeof(float), s.stream), "clear stage correction");
+            composite_levels(s);
+            sweep<float, float, float, 2>(s, b, r32, a, first.x.p);
+            sweep<float, double, float, 0>(s, a, r32, z, nullptr);
             cuda_check(cudaGetLastError(), "composite preconditioner");
         }
     }
@@ -898,7 +922,8 @@ namespace pcfd
     // one more post-sweep.
     void composite_preconditioner(System& s, const double* r, double* z)
     {
-        if (s.composite_fp32) composite_cycle<float>(s, r, z, s.inter32.empty() ? s.mg32.front() : s.inter32.front());
+        if (s.composite_fp32 && s.fine.res32.n && !s.mg_block_iterations) composite_cycle_fp32(s, r, z, s.inter32.front());
+        else if (s.composite_fp32) composite_cycle<float>(s, r, z, s.inter32.empty() ? s.mg32.front() : s.inter32.front());
         else composite_cycle<double>(s, r, z, s.inter64.empty() ? s.mg64.front() : s.inter64.front());
     }
 
