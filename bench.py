@@ -54,6 +54,10 @@ def parse_args():
                     help="coarse-correction weighting of the multigrid cycle (pcfd_mg_cycle)")
     ap.add_argument("--stage-sweeps", type=int, default=0,
                     help="composite cycle: Jacobi sweeps per stage before and after its correction (0: 8)")
+    ap.add_argument("--chebyshev", type=int, default=0,
+                    help="composite stages: 0 = damped Jacobi, r >= 2 = Chebyshev smoothing on [2/r, 2]")
+    ap.add_argument("--fine-chebyshev", type=int, default=0,
+                    help="composite fine sweeps: 0 = damped Jacobi, r >= 2 = Chebyshev-Richardson steps on [2/r, 2]")
     ap.add_argument("--block-iterations", type=int, default=0,
                     help="composite cycle: Chebyshev iterations of the brick block pre-smoother (0: Jacobi pre-sweeps)")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU sample of the ours arm")
@@ -309,7 +313,8 @@ def run_ours(args, ranks: Ranks):
     system = CompositeSystem(built.topology, MG_FP32 if args.mg == "fp32" else MG_FP64, device=ranks.local,
                              mg_cycle={"reference": 0, "corrected": 1, "composite": 2}[args.mg_cycle],
                              gmres_restart=args.restart, mg_stage_sweeps=args.stage_sweeps,
-                             mg_block_iterations=args.block_iterations)
+                             mg_block_iterations=args.block_iterations, mg_stage_chebyshev=args.chebyshev,
+                             mg_fine_chebyshev=args.fine_chebyshev)
     system.configure(speed=spec.speed, **spec.case)
     slots = system.inflow_layout()
     faces = len(slots) * spec.brick_size ** 2
@@ -397,7 +402,10 @@ def run_ours(args, ranks: Ranks):
         "vs_baseline": None, "dtype": "f32 state / f64 pressure", "data": "synthetic analytic geometry",
         "config": dict(spec.describe(), leaf_cells=built.leaf_cells, storage=built.storage_size,
                        mg=args.mg, mg_cycle=args.mg_cycle, gcro_restart=args.restart or 24,
-                       stage_sweeps=args.stage_sweeps or 8, block_iterations=args.block_iterations, parallelism=f"replicas{n}",
+                       stage_sweeps=args.stage_sweeps or 8, block_iterations=args.block_iterations,
+                       stage_smoother=f"chebyshev 2/{args.chebyshev}" if args.chebyshev else "jacobi",
+                       fine_smoother=f"chebyshev-richardson 2/{args.fine_chebyshev}" if args.fine_chebyshev else "jacobi",
+                       parallelism=f"replicas{n}",
                        l2="inputs larger than L2"),
         "projection_ms": round(statistics.mean(s["projection_ms"] for s in stats), 3),
         "iterations_per_step": round(statistics.mean(s["pressure"]["iterations"] for s in stats), 2),
@@ -453,7 +461,8 @@ def run_kernel_only(args):
     system = CompositeSystem(built.topology, MG_FP32 if args.mg == "fp32" else MG_FP64,
                              mg_cycle={"reference": 0, "corrected": 1, "composite": 2}[args.mg_cycle],
                              gmres_restart=args.restart, mg_stage_sweeps=args.stage_sweeps,
-                             mg_block_iterations=args.block_iterations)
+                             mg_block_iterations=args.block_iterations, mg_stage_chebyshev=args.chebyshev,
+                             mg_fine_chebyshev=args.fine_chebyshev)
     ms = system.time_kernel(args.kernel_only, args.kernel_iterations)
     line = {"kernel_only": args.kernel_only, "workload": args.workload, "ms_per_launch": ms,
             "iterations": args.kernel_iterations, "launches": system.launch_count()}

@@ -179,6 +179,11 @@ typedef struct pcfd_options {
     int32_t mg_block_iterations;     /* composite cycle: 0 = the reference's two Jacobi pre-sweeps on
                                         the fine level; k = 1..64: instead, k Chebyshev iterations of
                                         each brick's own diagonal block solve in shared memory */
+    int32_t mg_stage_chebyshev;      /* composite stages: 0 = damped Jacobi (w = 2/3); r = 2..1000:
+                                        Chebyshev polynomial smoothing of D^-1 A on [2 / r, 2] */
+    int32_t mg_fine_chebyshev;       /* composite cycle's fine sweeps: 0 = damped Jacobi (w = 2/3);
+                                        r = 2..1000: the two pre- and two post-sweeps take the
+                                        Chebyshev-Richardson step sizes of [2 / r, 2] */
 } pcfd_options;
 
 /* Coarse-correction weighting of the multigrid cycle.  The aggregation coarse operators are

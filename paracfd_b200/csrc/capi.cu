@@ -209,6 +209,16 @@ namespace pcfd
                 require(options->mg_stage_sweeps > 0 && options->mg_stage_sweeps <= 16, "mg_stage_sweeps must be 0..16");
                 s.mg_stage_sweeps = options->mg_stage_sweeps;
             }
+            if (options && options->mg_stage_chebyshev)
+            {
+                require(options->mg_stage_chebyshev >= 2 && options->mg_stage_chebyshev <= 1000, "mg_stage_chebyshev must be 0 or 2..1000");
+                s.mg_stage_chebyshev = options->mg_stage_chebyshev;
+            }
+            if (options && options->mg_fine_chebyshev)
+            {
+                require(options->mg_fine_chebyshev >= 2 && options->mg_fine_chebyshev <= 1000, "mg_fine_chebyshev must be 0 or 2..1000");
+                s.mg_fine_chebyshev = options->mg_fine_chebyshev;
+            }
             if (options && options->mg_block_iterations)
             {
                 require(options->mg_block_iterations > 0 && options->mg_block_iterations <= 64, "mg_block_iterations must be 0..64");

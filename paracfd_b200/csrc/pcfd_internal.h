@@ -107,7 +107,8 @@ namespace pcfd
         DBuf<int> row_offset, neighbour, aggregate, restrict_offset, restrict_dof;
         DBuf<T> coefficient, diagonal, rhs, x, temporary, residual;
         double prolong = 1.0;                   // weight of the next level's correction added here
-        int sweeps = 2;                         // Jacobi sweeps before and after the coarse correction
+        int sweeps = 2;                         // smoothing steps before and after the coarse correction
+        int chebyshev = 0;                      // 0: damped Jacobi; r >= 2: Chebyshev on [2 / r, 2]
     };
 
     struct Scalars;   // device scalar block for the Krylov recurrences
@@ -126,6 +127,10 @@ namespace pcfd
         DBuf<double> t, z;                      // [S] deferred structured rows, ping-pong iterate
         DBuf<double> damping;                   // [levels][14] w / D of non-deferred rows
         DBuf<float> damping32, z32, z32b, r32, t32, res32;   // FP32 multigrid: float fine-level buffers
+        DBuf<double> cheb_damping;              // [4][damping] Chebyshev-Richardson w / D per sweep (or empty)
+        DBuf<float> cheb_damping32;
+        size_t cheb_stride = 0;
+        double cheb_omega[4] = {};
     };
 
     // Up to kMaxSet vectors of one system, passed by value to the fused block kernels (krylov.cu):
@@ -170,6 +175,8 @@ namespace pcfd
         double mg_prolong_scale = 1.0, mg_lattice_scale = 1.0;   // coarse-correction weights (pcfd_mg_cycle)
         int mg_stage_sweeps = 8;                                 // composite-stage sweeps (pcfd_options)
         int mg_block_iterations = 0;                             // composite cycle: brick block pre-smoother (pcfd_options)
+        int mg_stage_chebyshev = 0;                              // composite stages: Chebyshev ratio (pcfd_options)
+        int mg_fine_chebyshev = 0;                               // composite fine sweeps: Chebyshev-Richardson ratio
         cudaStream_t stream = nullptr;
         bool own_stream = false;
         int device = 0;

@@ -654,6 +654,23 @@ namespace pcfd
             f.t32.alloc(size_t(S));
             f.res32.alloc(size_t(S));
         }
+        if (s.mg_fine_chebyshev >= 2)
+        {
+            // Chebyshev-Richardson schedule for the two pre- and the two post-sweeps: the step sizes
+            // are the inverse roots of the degree-2 Chebyshev polynomial on [2 / ratio, 2], smaller
+            // step first; each step's w / D table is the w = 2/3 table rescaled
+            const double hi = 2.0, lo = hi / s.mg_fine_chebyshev, theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo);
+            const double steps[2] = {1.0 / (theta + delta * std::sqrt(0.5)), 1.0 / (theta - delta * std::sqrt(0.5))};
+            f.cheb_stride = damping.size();
+            std::vector<double> table(4 * damping.size());
+            for (int slot = 0; slot < 4; ++slot)
+            {
+                f.cheb_omega[slot] = steps[slot & 1];
+                for (size_t i = 0; i < damping.size(); ++i) table[slot * damping.size() + i] = damping[i] * (steps[slot & 1] / (2.0 / 3.0));
+            }
+            f.cheb_damping.upload(table);
+            if (s.mg_precision == PCFD_MG_FP32 && !s.mg32.empty()) f.cheb_damping32.upload(std::vector<float>(table.begin(), table.end()));
+        }
         f.code.upload(code);
         f.deferred_count = int(ddof.size());
         f.deferred_dof.upload(ddof);
@@ -706,7 +723,7 @@ namespace pcfd
         }
 
         template <int kMode, class T, class TO, class TC, int kProlong>
-        void finish(System& s, const T* z, const T* r, TO* out, const TC* e, const T* t)
+        void finish(System& s, const T* z, const T* r, TO* out, const TC* e, const T* t, double omega = 2.0 / 3.0)
         {
             FineSmoother& f = s.fine;
             const IrregularOperator& o = s.irr;
@@ -715,7 +732,7 @@ namespace pcfd
                 f.deferred_count, f.deferred_dof, f.deferred_incident, f.gauge_offset, f.gauge_coefficient, o.incident_offset,
                 o.incident_edge, o.incident_sign, o.connection_count, o.conn_lower, o.conn_upper, o.conn_coefficient, o.reg_lower,
                 o.reg_upper, o.reg_coefficient, s.active, s.diagonal, s.aggregate, s.base_offset, s.base_cells, e, s.structured, z, r,
-                t, out, f.deferred_residual, 2.0 / 3.0, s.mg_prolong_scale, s.fine_map.p);
+                t, out, f.deferred_residual, omega, s.mg_prolong_scale, s.fine_map.p);
         }
 
         int pipe_grid(const System& s)
@@ -735,23 +752,37 @@ namespace pcfd
         template <> struct FineBuffers<double>
         {
             double *a, *t;
-            const double* damping;
-            explicit FineBuffers(FineSmoother& f) : a(f.z.p), t(f.t.p), damping(f.damping.p) {}
+            const double *damping, *chebyshev;
+            explicit FineBuffers(FineSmoother& f) : a(f.z.p), t(f.t.p), damping(f.damping.p), chebyshev(f.cheb_damping.p) {}
         };
         template <> struct FineBuffers<float>
         {
             float *a, *t;
-            const float* damping;
-            explicit FineBuffers(FineSmoother& f) : a(f.z32.p), t(f.t32.p), damping(f.damping32.p) {}
+            const float *damping, *chebyshev;
+            explicit FineBuffers(FineSmoother& f) : a(f.z32.p), t(f.t32.p), damping(f.damping32.p), chebyshev(f.cheb_damping32.p) {}
         };
 
+        // one fine sweep z + w (r - A z) / D; slot >= 0 selects the w of that step of the
+        // Chebyshev-Richardson schedule (mg_fine_chebyshev), otherwise w = 2/3
         template <class T, class TO, class TC, int kProlong>
-        void sweep(System& s, const T* z, const T* r, TO* out, const TC* e)
+        void sweep(System& s, const T* z, const T* r, TO* out, const TC* e, int slot = -1)
         {
             FineBuffers<T> w(s.fine);
+            const bool cheb = slot >= 0 && w.chebyshev;
+            const T* damping = cheb ? w.chebyshev + size_t(slot) * s.fine.cheb_stride : w.damping;
             brick_pipe_kernel<0, T, TO, TC, kProlong><<<pipe_grid(s), 256, 0, launch_stream(s)>>>(
-                view(s), s.active_bricks, z, r, out, w.t, e, nullptr, w.damping);
-            finish<0, T, TO, TC, kProlong>(s, z, r, out, e, w.t);
+                view(s), s.active_bricks, z, r, out, w.t, e, nullptr, damping);
+            finish<0, T, TO, TC, kProlong>(s, z, r, out, e, w.t, cheb ? s.fine.cheb_omega[slot] : 2.0 / 3.0);
+        }
+        // the first pre-sweep from z = 0 (slot 0 of the schedule when it is on)
+        template <class T> void first_sweep(System& s, const double* r, T* z, T* r_copy)
+        {
+            FineSmoother& f = s.fine;
+            FineBuffers<T> w(f);
+            const bool cheb = w.chebyshev != nullptr;
+            first_sweep_kernel<T><<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(
+                f.code, s.brick_level, cheb ? w.chebyshev : w.damping, s.diagonal, s.active, r, z, r_copy, s.structured, s.S,
+                cheb ? f.cheb_omega[0] : 2.0 / 3.0);
         }
 
         template <class T>
@@ -847,9 +878,8 @@ namespace pcfd
                 return;
             }
             double* a = f.z.p;
-            first_sweep_kernel<double><<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(
-                f.code, s.brick_level, f.damping.p, s.diagonal, s.active, r, a, nullptr, s.structured, s.S, 2.0 / 3.0);
-            sweep<double, double, TC, 0>(s, a, r, z, nullptr);
+            first_sweep<double>(s, r, a, nullptr);
+            sweep<double, double, TC, 0>(s, a, r, z, nullptr, 1);
             composite_tail<TC>(s, r, z, first);
         }
     }
@@ -886,8 +916,8 @@ namespace pcfd
                 first.cells, s.fine_restrict_offset, s.fine_restrict_dof, res, first.rhs);
             cuda_check(cudaMemsetAsync(first.x, 0, size_t(first.cells) * sizeof(TC), s.stream), "clear stage correction");
             composite_levels(s);
-            sweep<double, double, TC, 2>(s, z, r, a, first.x.p);
-            sweep<double, double, TC, 0>(s, a, r, z, nullptr);
+            sweep<double, double, TC, 2>(s, z, r, a, first.x.p, 2);
+            sweep<double, double, TC, 0>(s, a, r, z, nullptr, 3);
             cuda_check(cudaGetLastError(), "composite preconditioner");
         }
 
@@ -899,9 +929,8 @@ namespace pcfd
         {
             FineSmoother& f = s.fine;
             float *a = f.z32.p, *b = f.z32b.p, *r32 = f.r32.p, *res = f.res32.p;
-            first_sweep_kernel<float><<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(
-                f.code, s.brick_level, f.damping32.p, s.diagonal, s.active, r, a, r32, s.structured, s.S, 2.0 / 3.0);
-            sweep<float, float, float, 0>(s, a, r32, b, nullptr);
+            first_sweep<float>(s, r, a, r32);
+            sweep<float, float, float, 0>(s, a, r32, b, nullptr, 1);
             brick_pipe_kernel<3, float, float, float, 0><<<pipe_grid(s), 256, 0, launch_stream(s)>>>(
                 view(s), s.active_bricks, b, r32, res, f.t32.p, nullptr, nullptr, f.damping32.p);
             finish<2, float, float, float, 0>(s, b, r32, res, static_cast<const float*>(nullptr), f.t32.p);
@@ -909,8 +938,8 @@ namespace pcfd
                 first.cells, s.fine_restrict_offset, s.fine_restrict_dof, res, first.rhs);
             cuda_check(cudaMemsetAsync(first.x, 0, size_t(first.cells) * sizeof(float), s.stream), "clear stage correction");
             composite_levels(s);
-            sweep<float, float, float, 2>(s, b, r32, a, first.x.p);
-            sweep<float, double, float, 0>(s, a, r32, z, nullptr);
+            sweep<float, float, float, 2>(s, b, r32, a, first.x.p, 2);
+            sweep<float, double, float, 0>(s, a, r32, z, nullptr, 3);
             cuda_check(cudaGetLastError(), "composite preconditioner");
         }
     }

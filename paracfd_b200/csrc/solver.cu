@@ -478,6 +478,7 @@ namespace pcfd
                 upload_level(s.inter32[k], stages[k]);
                 s.inter32[k].prolong = 2.0;
                 s.inter32[k].sweeps = s.mg_stage_sweeps;
+                s.inter32[k].chebyshev = s.mg_stage_chebyshev;
             }
         }
         else
@@ -488,6 +489,7 @@ namespace pcfd
                 upload_level(s.inter64[k], stages[k]);
                 s.inter64[k].prolong = 2.0;
                 s.inter64[k].sweeps = s.mg_stage_sweeps;
+                s.inter64[k].chebyshev = s.mg_stage_chebyshev;
             }
         }
         s.composite = true;
@@ -531,6 +533,22 @@ namespace pcfd
             double Ax = double(diag[q]) * double(x[q]);
             for (int e = row_offset[q]; e < row_offset[q + 1]; ++e) Ax -= double(coefficient[e]) * double(x[neighbour[e]]);
             next[q] = x[q] + omega * T((double(rhs[q]) - Ax) / double(diag[q]));
+        }
+        // One Chebyshev step of a CSR level, fused: r = rhs - A x, d = c1 d + c2 D^-1 r (first step:
+        // d = c2 D^-1 r), next = x + d
+        template <class T>
+        __global__ void algebraic_chebyshev_kernel(const T* rhs, const T* x, T* next, T* d, const int* row_offset, const int* neighbour,
+                                                   const T* coefficient, const T* diag, int cells, T c1, T c2, int first)
+        {
+            const int q = blockIdx.x * blockDim.x + threadIdx.x;
+            if (q >= cells) return;
+            if (!(diag[q] > T(0))) { next[q] = T(0); d[q] = T(0); return; }
+            double Ax = double(diag[q]) * double(x[q]);
+            for (int e = row_offset[q]; e < row_offset[q + 1]; ++e) Ax -= double(coefficient[e]) * double(x[neighbour[e]]);
+            const T step = c2 * T((double(rhs[q]) - Ax) / double(diag[q]));
+            const T dn = first ? step : c1 * d[q] + step;
+            d[q] = dn;
+            next[q] = x[q] + dn;
         }
         template <class T>
         __global__ void algebraic_residual_kernel(const T* rhs, const T* x, T* residual, const int* row_offset, const int* neighbour,
@@ -602,6 +620,30 @@ namespace pcfd
             MgLevel<T>& level = *chain[index];
             const T omega = T(kOmega);
             auto smooth = [&](int sweeps) {
+                if (level.chebyshev >= 2)
+                {
+                    // Chebyshev polynomial smoothing on [2 / ratio, 2] (D^-1 A of a diagonally dominant
+                    // Galerkin level has its spectrum in (0, 2]); the direction lives in level.residual
+                    const double hi = 2.0, lo = hi / level.chebyshev;
+                    const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
+                    double rho = 1.0 / sigma;
+                    for (int sweep = 0; sweep < sweeps; ++sweep)
+                    {
+                        double c1 = 0.0, c2 = 1.0 / theta;
+                        if (sweep)
+                        {
+                            const double next = 1.0 / (2.0 * sigma - rho);
+                            c1 = next * rho;
+                            c2 = 2.0 * next / delta;
+                            rho = next;
+                        }
+                        algebraic_chebyshev_kernel<T><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
+                            level.rhs, level.x, level.temporary, level.residual, level.row_offset, level.neighbour, level.coefficient,
+                            level.diagonal, level.cells, T(c1), T(c2), sweep == 0 ? 1 : 0);
+                        std::swap(level.x.p, level.temporary.p);
+                    }
+                    return;
+                }
                 for (int sweep = 0; sweep < sweeps; ++sweep)
                 {
                     algebraic_jacobi_kernel<T><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
