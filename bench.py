@@ -73,6 +73,10 @@ def parse_args():
                          "the multigrid on the same right-hand sides of the naca4412_wing case")
     ap.add_argument("--train-steps", type=int, default=3000)
     ap.add_argument("--no-learned", action="store_true", help="skip the short learned-preconditioner comparison")
+    ap.add_argument("--sweep", action="store_true",
+                    help="batched angle sweep: 16 naca4412_wing instances (AoA -4..11 deg, seeded refinement bands) in "
+                         "4 batches of 4, each batch stepped sequentially and then concurrently (one host thread and "
+                         "stream per instance); reports instance-steps/s of both")
     ap.add_argument("--harvest-runs", type=int, default=4, help="seeded harvest runs (alternating the two cases)")
     return ap.parse_args()
 
@@ -650,12 +654,79 @@ def run_learned(args, ranks: Ranks):
     return line
 
 
+def run_sweep(args, ranks: Ranks):
+    """BASELINE config 5 on one GPU: the angle-of-attack sweep as batches of concurrent instances."""
+    import dataclasses
+    from concurrent.futures import ThreadPoolExecutor
+
+    from paracfd_b200 import MG_CYCLE_COMPOSITE, MG_FP32, CompositeSystem
+    from paracfd_b200.workloads import WORKLOADS
+
+    rng = np.random.default_rng(20261203)
+    base = WORKLOADS["naca4412_wing"]
+    specs = [dataclasses.replace(base, name=f"naca4412_aoa{a}", aoa=float(a),
+                                 surface_refinement_distance=round(float(rng.uniform(0.03, 0.12)), 4),
+                                 wing_refinement_distance=round(float(rng.uniform(0.2, 0.6)), 4))
+             for a in range(-4, 12)]
+    batches = []
+    for first in range(0, len(specs), 4):
+        batch = specs[first:first + 4]
+        builts = [sp.build() for sp in batch]
+        systems = [CompositeSystem(b.topology, MG_FP32, device=ranks.local, mg_cycle=MG_CYCLE_COMPOSITE,
+                                   mg_stage_sweeps=args.stage_sweeps, mg_stage_chebyshev=args.chebyshev,
+                                   mg_fine_chebyshev=args.fine_chebyshev) for b in builts]
+        for sp, sy in zip(batch, systems):
+            sy.configure(speed=sp.speed, **sp.case)
+            sy.initialize()
+            for _ in range(args.warmup):
+                sy.step()
+            sy.synchronize()
+
+        def run(sy):
+            its = 0
+            for _ in range(args.steps):
+                its += sy.step()["pressure"]["iterations"]
+            sy.synchronize()
+            return its
+
+        sequential = []
+        for sy in systems:
+            t0 = time.perf_counter()
+            run(sy)
+            sequential.append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(max_workers=len(systems)) as pool:
+            iterations = list(pool.map(run, systems))
+        concurrent = time.perf_counter() - t0
+        batches.append({"aoa": [sp.aoa for sp in batch], "leaf_cells": [b.leaf_cells for b in builts],
+                        "sequential_s": round(sum(sequential), 3), "concurrent_s": round(concurrent, 3),
+                        "iterations_per_step": [round(i / args.steps, 2) for i in iterations]})
+        for sy in systems:
+            sy.close()
+        for b in builts:
+            b.close()
+    instance_steps = len(specs) * args.steps
+    seq = sum(b["sequential_s"] for b in batches)
+    conc = sum(b["concurrent_s"] for b in batches)
+    return {
+        "metric": "batched angle sweep: instance-steps/s over 16 naca4412_wing instances (4 batches of 4)",
+        "value": round(instance_steps / conc, 3), "unit": "instance-steps/s", "higher_is_better": True, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "sequential": round(instance_steps / seq, 3),
+        "speedup_vs_sequential": round(seq / conc, 3), "timing": "host wall clock around synchronised step loops",
+        "config": {"workload": "naca4412_wing sweep", "aoa": [-4, 11], "seed": 20261203, "mg": "fp32",
+                   "leaf_cells_per_batch": [sum(b["leaf_cells"]) for b in batches]},
+        "batches": batches,
+    }
+
+
 def main():
     args = parse_args()
     ranks = Ranks(collective=args.impl == "ours")
     try:
         if args.learned:
             line = run_learned(args, ranks) if ranks.rank == 0 else None
+        elif args.sweep:
+            line = run_sweep(args, ranks) if ranks.rank == 0 else None
         elif args.kernel_only is not None:
             line = run_kernel_only(args)
         elif args.impl == "reference":
