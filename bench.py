@@ -53,11 +53,11 @@ def parse_args():
     ap.add_argument("--mg-cycle", choices=("reference", "corrected", "composite"), default="composite",
                     help="coarse-correction weighting of the multigrid cycle (pcfd_mg_cycle)")
     ap.add_argument("--stage-sweeps", type=int, default=0,
-                    help="composite cycle: Jacobi sweeps per stage before and after its correction (0: 8)")
+                    help="composite cycle: smoothing steps per stage before and after its correction (0: 6)")
     ap.add_argument("--chebyshev", type=int, default=0,
-                    help="composite stages: 0 = damped Jacobi, r >= 2 = Chebyshev smoothing on [2/r, 2]")
+                    help="composite stages: r >= 2 = Chebyshev smoothing on [2/r, 2], 1 = damped Jacobi, 0: r = 30")
     ap.add_argument("--fine-chebyshev", type=int, default=0,
-                    help="composite fine sweeps: 0 = damped Jacobi, r >= 2 = Chebyshev-Richardson steps on [2/r, 2]")
+                    help="composite fine sweeps: r >= 2 = Chebyshev-Richardson steps on [2/r, 2], 1 = damped Jacobi, 0: r = 10")
     ap.add_argument("--block-iterations", type=int, default=0,
                     help="composite cycle: Chebyshev iterations of the brick block pre-smoother (0: Jacobi pre-sweeps)")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU sample of the ours arm")
@@ -406,9 +406,9 @@ def run_ours(args, ranks: Ranks):
         "vs_baseline": None, "dtype": "f32 state / f64 pressure", "data": "synthetic analytic geometry",
         "config": dict(spec.describe(), leaf_cells=built.leaf_cells, storage=built.storage_size,
                        mg=args.mg, mg_cycle=args.mg_cycle, gcro_restart=args.restart or 24,
-                       stage_sweeps=args.stage_sweeps or 8, block_iterations=args.block_iterations,
-                       stage_smoother=f"chebyshev 2/{args.chebyshev}" if args.chebyshev else "jacobi",
-                       fine_smoother=f"chebyshev-richardson 2/{args.fine_chebyshev}" if args.fine_chebyshev else "jacobi",
+                       stage_sweeps=args.stage_sweeps or 6, block_iterations=args.block_iterations,
+                       stage_smoother="jacobi" if args.chebyshev == 1 else f"chebyshev 2/{args.chebyshev or 30}",
+                       fine_smoother="jacobi" if args.fine_chebyshev == 1 else f"chebyshev-richardson 2/{args.fine_chebyshev or 10}",
                        parallelism=f"replicas{n}",
                        l2="inputs larger than L2"),
         "projection_ms": round(statistics.mean(s["projection_ms"] for s in stats), 3),

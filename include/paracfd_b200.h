@@ -174,16 +174,16 @@ typedef struct pcfd_options {
                                         operator/vector launches (same sweeps, reference order) */
     int32_t mg_cycle;                /* pcfd_mg_cycle */
     int32_t gmres_restart;           /* columns per GCRO/LGMRES cycle, 1..24; 0: the reference's 24 */
-    int32_t mg_stage_sweeps;         /* composite cycle: Jacobi sweeps before and after each stage's
-                                        coarse correction, 1..16; 0: 8 */
+    int32_t mg_stage_sweeps;         /* composite cycle: smoothing steps before and after each stage's
+                                        coarse correction, 1..16; 0: 6 */
     int32_t mg_block_iterations;     /* composite cycle: 0 = the reference's two Jacobi pre-sweeps on
                                         the fine level; k = 1..64: instead, k Chebyshev iterations of
                                         each brick's own diagonal block solve in shared memory */
-    int32_t mg_stage_chebyshev;      /* composite stages: 0 = damped Jacobi (w = 2/3); r = 2..1000:
-                                        Chebyshev polynomial smoothing of D^-1 A on [2 / r, 2] */
-    int32_t mg_fine_chebyshev;       /* composite cycle's fine sweeps: 0 = damped Jacobi (w = 2/3);
-                                        r = 2..1000: the two pre- and two post-sweeps take the
-                                        Chebyshev-Richardson step sizes of [2 / r, 2] */
+    int32_t mg_stage_chebyshev;      /* composite stages: r = 2..1000: Chebyshev polynomial smoothing of
+                                        D^-1 A on [2 / r, 2]; 1 = damped Jacobi (w = 2/3); 0: r = 30 */
+    int32_t mg_fine_chebyshev;       /* composite cycle's fine sweeps: r = 2..1000: the two pre- and two
+                                        post-sweeps take the Chebyshev-Richardson step sizes of
+                                        [2 / r, 2]; 1 = damped Jacobi (w = 2/3); 0: r = 10 */
 } pcfd_options;
 
 /* Coarse-correction weighting of the multigrid cycle.  The aggregation coarse operators are

@@ -211,13 +211,13 @@ namespace pcfd
             }
             if (options && options->mg_stage_chebyshev)
             {
-                require(options->mg_stage_chebyshev >= 2 && options->mg_stage_chebyshev <= 1000, "mg_stage_chebyshev must be 0 or 2..1000");
-                s.mg_stage_chebyshev = options->mg_stage_chebyshev;
+                require(options->mg_stage_chebyshev >= 1 && options->mg_stage_chebyshev <= 1000, "mg_stage_chebyshev must be 0..1000");
+                s.mg_stage_chebyshev = options->mg_stage_chebyshev == 1 ? 0 : options->mg_stage_chebyshev;
             }
             if (options && options->mg_fine_chebyshev)
             {
-                require(options->mg_fine_chebyshev >= 2 && options->mg_fine_chebyshev <= 1000, "mg_fine_chebyshev must be 0 or 2..1000");
-                s.mg_fine_chebyshev = options->mg_fine_chebyshev;
+                require(options->mg_fine_chebyshev >= 1 && options->mg_fine_chebyshev <= 1000, "mg_fine_chebyshev must be 0..1000");
+                s.mg_fine_chebyshev = options->mg_fine_chebyshev == 1 ? 0 : options->mg_fine_chebyshev;
             }
             if (options && options->mg_block_iterations)
             {

@@ -173,10 +173,10 @@ namespace pcfd
         bool outlet = true, full_nonorthogonal = false;
         int mg_precision = PCFD_MG_FP64;
         double mg_prolong_scale = 1.0, mg_lattice_scale = 1.0;   // coarse-correction weights (pcfd_mg_cycle)
-        int mg_stage_sweeps = 8;                                 // composite-stage sweeps (pcfd_options)
+        int mg_stage_sweeps = 6;                                 // composite-stage sweeps (pcfd_options)
         int mg_block_iterations = 0;                             // composite cycle: brick block pre-smoother (pcfd_options)
-        int mg_stage_chebyshev = 0;                              // composite stages: Chebyshev ratio (pcfd_options)
-        int mg_fine_chebyshev = 0;                               // composite fine sweeps: Chebyshev-Richardson ratio
+        int mg_stage_chebyshev = 30;                             // composite stages: Chebyshev ratio, 0 = Jacobi (pcfd_options)
+        int mg_fine_chebyshev = 10;                              // composite fine sweeps: Chebyshev-Richardson ratio, 0 = Jacobi
         cudaStream_t stream = nullptr;
         bool own_stream = false;
         int device = 0;
