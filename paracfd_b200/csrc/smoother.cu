@@ -857,7 +857,7 @@ namespace pcfd
 
         // residual of the pre-smoothed z, its gather into stage 1, the stage V-cycle, the weighted
         // prolongation fused into the first post-sweep, one more post-sweep
-        template <class TC> void composite_tail(System& s, const double* r, double* z, MgLevel<TC>& first);
+        template <class TC> void composite_tail(System& s, const double* r, double* z, MgLevel<TC>& first, bool schedule = true);
 
         template <class TC>
         void composite_cycle(System& s, const double* r, double* z, MgLevel<TC>& first)
@@ -898,13 +898,15 @@ namespace pcfd
         }
         require(s.composite, "the learned multigrid preconditioner needs the composite cycle");
         learned_apply(s, r, z);
-        if (s.composite_fp32) composite_tail<float>(s, r, z, s.inter32.front());
-        else composite_tail<double>(s, r, z, s.inter64.front());
+        if (s.composite_fp32) composite_tail<float>(s, r, z, s.inter32.front(), false);
+        else composite_tail<double>(s, r, z, s.inter64.front(), false);
     }
 
     namespace
     {
-        template <class TC> void composite_tail(System& s, const double* r, double* z, MgLevel<TC>& first)
+        // schedule: the post-sweeps take the Chebyshev-Richardson steps of the fine schedule (the
+        // second half of a pre/post pair), otherwise w = 2/3
+        template <class TC> void composite_tail(System& s, const double* r, double* z, MgLevel<TC>& first, bool schedule)
         {
             FineSmoother& f = s.fine;
             double* a = f.z.p;
@@ -916,8 +918,8 @@ namespace pcfd
                 first.cells, s.fine_restrict_offset, s.fine_restrict_dof, res, first.rhs);
             cuda_check(cudaMemsetAsync(first.x, 0, size_t(first.cells) * sizeof(TC), s.stream), "clear stage correction");
             composite_levels(s);
-            sweep<double, double, TC, 2>(s, z, r, a, first.x.p, 2);
-            sweep<double, double, TC, 0>(s, a, r, z, nullptr, 3);
+            sweep<double, double, TC, 2>(s, z, r, a, first.x.p, schedule ? 2 : -1);
+            sweep<double, double, TC, 0>(s, a, r, z, nullptr, schedule ? 3 : -1);
             cuda_check(cudaGetLastError(), "composite preconditioner");
         }
 
