@@ -898,8 +898,8 @@ namespace pcfd
         }
         require(s.composite, "the learned multigrid preconditioner needs the composite cycle");
         learned_apply(s, r, z);
-        if (s.composite_fp32) composite_tail<float>(s, r, z, s.inter32.front(), false);
-        else composite_tail<double>(s, r, z, s.inter64.front(), false);
+        if (s.composite_fp32) composite_tail<float>(s, r, z, s.inter32.front());
+        else composite_tail<double>(s, r, z, s.inter64.front());
     }
 
     namespace
