@@ -184,6 +184,10 @@ typedef struct pcfd_options {
     int32_t mg_fine_chebyshev;       /* composite cycle's fine sweeps: r = 2..1000: the two pre- and two
                                         post-sweeps take the Chebyshev-Richardson step sizes of
                                         [2 / r, 2]; 1 = damped Jacobi (w = 2/3); 0: r = 10 */
+    int32_t gmres_delayed;           /* 1: GCRO/LGMRES columns orthogonalised by delayed CGS2 (one dot
+                                        and one update pass over the basis per column; the previous
+                                        basis vector reorthogonalised in the same passes); 0: CGS2
+                                        (three passes) */
 } pcfd_options;
 
 /* Coarse-correction weighting of the multigrid cycle.  The aggregation coarse operators are

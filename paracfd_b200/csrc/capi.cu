@@ -209,6 +209,11 @@ namespace pcfd
                 require(options->mg_stage_sweeps > 0 && options->mg_stage_sweeps <= 16, "mg_stage_sweeps must be 0..16");
                 s.mg_stage_sweeps = options->mg_stage_sweeps;
             }
+            if (options && options->gmres_delayed)
+            {
+                require(options->gmres_delayed == 1, "gmres_delayed must be 0 or 1");
+                s.delayed_orthogonalisation = true;
+            }
             if (options && options->mg_stage_chebyshev)
             {
                 require(options->mg_stage_chebyshev >= 1 && options->mg_stage_chebyshev <= 1000, "mg_stage_chebyshev must be 0..1000");
@@ -249,6 +254,9 @@ namespace pcfd
             s.block_result.alloc(size_t(4) * (kMaxSet + 1));
             cuda_check(cudaMallocHost(&s.pinned, 16 * sizeof(double)), "pinned scalars");
             cuda_check(cudaMallocHost(&s.pinned_block, size_t(4) * (kMaxSet + 1) * sizeof(double)), "pinned block scalars");
+            s.dcgs_partial.alloc(size_t(592) * (2 * kMaxSet + 4));
+            s.dcgs_result.alloc(size_t(kDcgsCoefficients));
+            cuda_check(cudaMallocHost(&s.pinned_dcgs, size_t(kDcgsCoefficients) * sizeof(double)), "pinned orthogonalisation scalars");
             // flow state
             s.u.alloc(size_t(s.faces)); s.v.alloc(size_t(s.faces)); s.w.alloc(size_t(s.faces));
             s.divergence.alloc(size_t(s.S));
@@ -305,6 +313,7 @@ namespace pcfd
         delete momentum;
         if (pinned) cudaFreeHost(pinned);
         if (pinned_block) cudaFreeHost(pinned_block);
+        if (pinned_dcgs) cudaFreeHost(pinned_dcgs);
         if (own_stream && stream) cudaStreamDestroy(stream);
     }
 }

@@ -245,6 +245,185 @@ namespace pcfd
             }
         }
 
+        // ---- delayed CGS2 (one dot pass and one update pass per Krylov column) -------------------
+        // Pass 1 for Q = [C | V_0..V_{j-1}] (final), v = V_j (projected once) and w = A z_j:
+        // s = Q^T v, t = Q^T w, v.v, v.w, w.w -> partial[block][2 * kMaxSet + 3].
+        constexpr int kDcgsStride = 2 * kMaxSet + 4;
+        template <int V>
+        __global__ void __launch_bounds__(kThreadsBlock, V >= 8 ? 2 : 1) dcgs_dot_kernel(VecSet Q, const double* __restrict__ vv,
+            const double* __restrict__ w, const uint8_t* __restrict__ active, Sweep range, double* __restrict__ partial)
+        {
+            __shared__ double shared[kThreadsBlock / 32][kDcgsStride];
+            double as[V], at[V], vv2 = 0.0, vw = 0.0, ww = 0.0;
+#pragma unroll
+            for (int u = 0; u < V; ++u) { as[u] = 0.0; at[u] = 0.0; }
+            const int count = Q.size();
+            const int lane = threadIdx.x & 31, quarter = lane >> 3, warp = threadIdx.x >> 5;
+            const int seg_pair = (warp * kPairsPerWarp) + (lane & 7);
+            for (int64_t item = blockIdx.x; item < range.items; item += gridDim.x)
+            {
+                const int64_t base = range.base(item);
+#pragma unroll 1
+                for (int sub = 0; sub < 256 / kPairsPerPass; ++sub)
+                {
+                    const int64_t e = base + 2 * (seg_pair + kPairsPerPass * sub);
+                    const bool valid = e < range.padded;
+                    const int64_t q = valid ? e >> 1 : 0;
+                    const uchar2 a = valid ? reinterpret_cast<const uchar2*>(active)[q] : make_uchar2(0, 0);
+                    const double2 v0 = valid ? reinterpret_cast<const double2*>(vv)[q] : make_double2(0.0, 0.0);
+                    const double2 w0 = valid ? reinterpret_cast<const double2*>(w)[q] : make_double2(0.0, 0.0);
+#pragma unroll
+                    for (int u = 0; u < V; ++u)
+                    {
+                        const int j = V * quarter + u;
+                        const double2 b = valid && j < count ? reinterpret_cast<const double2*>(Q.vec(j))[q] : make_double2(0.0, 0.0);
+                        as[u] += (a.x ? b.x * v0.x : 0.0) + (a.y ? b.y * v0.y : 0.0);
+                        at[u] += (a.x ? b.x * w0.x : 0.0) + (a.y ? b.y * w0.y : 0.0);
+                    }
+                    if (quarter == 0)
+                    {
+                        vv2 += (a.x ? v0.x * v0.x : 0.0) + (a.y ? v0.y * v0.y : 0.0);
+                        vw += (a.x ? v0.x * w0.x : 0.0) + (a.y ? v0.y * w0.y : 0.0);
+                        ww += (a.x ? w0.x * w0.x : 0.0) + (a.y ? w0.y * w0.y : 0.0);
+                    }
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < V; ++u)
+            {
+                const double x = segment_sum(as[u]), y = segment_sum(at[u]);
+                if ((lane & 7) == 0)
+                {
+                    shared[warp][V * quarter + u] = x;
+                    shared[warp][kMaxSet + V * quarter + u] = y;
+                }
+            }
+            const double a1 = segment_sum(vv2), a2 = segment_sum(vw), a3 = segment_sum(ww);
+            if (lane == 0)
+            {
+                shared[warp][2 * kMaxSet] = a1;
+                shared[warp][2 * kMaxSet + 1] = a2;
+                shared[warp][2 * kMaxSet + 2] = a3;
+            }
+            __syncthreads();
+            for (int j = threadIdx.x; j < kDcgsStride - 1; j += blockDim.x)
+            {
+                const bool used = j < count || (j >= kMaxSet && j < kMaxSet + count) || j >= 2 * kMaxSet;
+                double v = 0.0;
+                if (used)
+#pragma unroll
+                    for (int wp = 0; wp < kThreadsBlock / 32; ++wp) v += shared[wp][j];
+                partial[int64_t(blockIdx.x) * kDcgsStride + j] = v;
+            }
+        }
+
+        // Sums the pass-1 partials (fixed order) and forms the update coefficients:
+        //   r = |v - Q s| = sqrt(v.v - s.s), c = (v.w - s.t) / r, rho^2 = w.w - t.t - c^2,
+        //   v_new = v / r - Q (s / r),  w_new = w - (c / r) v - Q (t - (c / r) s),  next = w_new / rho.
+        // out: [0, 32) s, [32, 64) t, [64, 96) s / r, [96, 128) t - (c / r) s, then v.v, v.w, w.w,
+        // r, c, rho, 1 / r, c / r, 1 / rho (rho and r are 0 when their squares are not positive).
+        __global__ void __launch_bounds__(256) dcgs_final_kernel(const double* __restrict__ partial, int blocks, int count,
+                                                                 double* __restrict__ out)
+        {
+            __shared__ double shared[8];
+            __shared__ double total[kDcgsStride];
+            for (int j = 0; j < 2 * kMaxSet + 3; ++j)
+            {
+                const bool used = j < count || (j >= kMaxSet && j < kMaxSet + count) || j >= 2 * kMaxSet;
+                if (!used)
+                {
+                    if (threadIdx.x == 0) total[j] = 0.0;
+                    continue;
+                }
+                double v = 0.0;
+                for (int b = threadIdx.x; b < blocks; b += blockDim.x) v += partial[int64_t(b) * kDcgsStride + j];
+                v = warp_sum(v);
+                if ((threadIdx.x & 31) == 0) shared[threadIdx.x >> 5] = v;
+                __syncthreads();
+                if (threadIdx.x == 0)
+                {
+                    double t = 0.0;
+                    for (int w = 0; w < 8; ++w) t += shared[w];
+                    total[j] = t;
+                }
+                __syncthreads();
+            }
+            if (threadIdx.x != 0) return;
+            double ss = 0.0, st = 0.0, tt = 0.0;
+            for (int l = 0; l < count; ++l)
+            {
+                ss += total[l] * total[l];
+                st += total[l] * total[kMaxSet + l];
+                tt += total[kMaxSet + l] * total[kMaxSet + l];
+            }
+            const double vv = total[2 * kMaxSet], vw = total[2 * kMaxSet + 1], ww = total[2 * kMaxSet + 2];
+            const double r2 = vv - ss, r = r2 > 0.0 ? sqrt(r2) : 0.0;
+            const double c = r > 0.0 ? (vw - st) / r : 0.0;
+            const double rho2 = ww - tt - c * c, rho = rho2 > 0.0 ? sqrt(rho2) : 0.0;
+            const double inv_r = r > 0.0 ? 1.0 / r : 0.0, c_r = c * inv_r;
+            for (int l = 0; l < kMaxSet; ++l)
+            {
+                const bool in = l < count;
+                out[l] = in ? total[l] : 0.0;
+                out[kMaxSet + l] = in ? total[kMaxSet + l] : 0.0;
+                out[2 * kMaxSet + l] = in ? total[l] * inv_r : 0.0;
+                out[3 * kMaxSet + l] = in ? total[kMaxSet + l] - c_r * total[l] : 0.0;
+            }
+            double* sc = out + 4 * kMaxSet;
+            sc[0] = vv; sc[1] = vw; sc[2] = ww; sc[3] = r; sc[4] = c; sc[5] = rho; sc[6] = inv_r; sc[7] = c_r;
+            sc[8] = rho > 0.0 ? 1.0 / rho : 0.0;
+        }
+
+        // Pass 2: v <- v / r - Q (s / r) in place, next = (w - (c / r) v_old - Q (t - (c / r) s)) / rho.
+        template <int V>
+        __global__ void __launch_bounds__(kThreadsBlock, V >= 8 ? 2 : 1) dcgs_update_kernel(VecSet Q, const double* __restrict__ coefficient,
+            double* __restrict__ vv, const double* __restrict__ w, double* __restrict__ next, const uint8_t* __restrict__ active, Sweep range)
+        {
+            __shared__ double cv[kMaxSet], cw[kMaxSet];
+            if (threadIdx.x < kMaxSet)
+            {
+                cv[threadIdx.x] = coefficient[2 * kMaxSet + threadIdx.x];
+                cw[threadIdx.x] = coefficient[3 * kMaxSet + threadIdx.x];
+            }
+            __syncthreads();
+            const double inv_r = coefficient[4 * kMaxSet + 6], c_r = coefficient[4 * kMaxSet + 7], inv_rho = coefficient[4 * kMaxSet + 8];
+            const int count = Q.size();
+            const int lane = threadIdx.x & 31, quarter = lane >> 3;
+            const int seg_pair = ((threadIdx.x >> 5) * kPairsPerWarp) + (lane & 7);
+            for (int64_t item = blockIdx.x; item < range.items; item += gridDim.x)
+            {
+                const int64_t base = range.base(item);
+#pragma unroll 1
+                for (int sub = 0; sub < 256 / kPairsPerPass; ++sub)
+                {
+                    const int64_t e = base + 2 * (seg_pair + kPairsPerPass * sub);
+                    const bool valid = e < range.padded;
+                    const int64_t q = valid ? e >> 1 : 0;
+                    const uchar2 a = valid ? reinterpret_cast<const uchar2*>(active)[q] : make_uchar2(0, 0);
+                    const double2 v0 = valid ? reinterpret_cast<const double2*>(vv)[q] : make_double2(0.0, 0.0);
+                    const double2 w0 = valid ? reinterpret_cast<const double2*>(w)[q] : make_double2(0.0, 0.0);
+                    double vx = 0.0, vy = 0.0, wx = 0.0, wy = 0.0;
+#pragma unroll
+                    for (int u = 0; u < V; ++u)
+                    {
+                        const int j = V * quarter + u;
+                        const double2 b = valid && j < count ? reinterpret_cast<const double2*>(Q.vec(j))[q] : make_double2(0.0, 0.0);
+                        vx += cv[j] * b.x; vy += cv[j] * b.y;
+                        wx += cw[j] * b.x; wy += cw[j] * b.y;
+                    }
+                    const double svx = quarter_total(vx), svy = quarter_total(vy), swx = quarter_total(wx), swy = quarter_total(wy);
+                    if (quarter == 0 && valid)
+                    {
+                        const double2 vn = make_double2(a.x ? inv_r * v0.x - svx : 0.0, a.y ? inv_r * v0.y - svy : 0.0);
+                        const double2 nx = make_double2(a.x ? inv_rho * (w0.x - c_r * v0.x - swx) : 0.0,
+                                                        a.y ? inv_rho * (w0.y - c_r * v0.y - swy) : 0.0);
+                        reinterpret_cast<double2*>(vv)[q] = vn;
+                        reinterpret_cast<double2*>(next)[q] = nx;
+                    }
+                }
+            }
+        }
+
         Sweep sweep_range(const System& s)
         {
             if (s.bs != 8) return Sweep{nullptr, 0, (int64_t(s.Sp) + 511) / 512, 0, s.Sp};   // contiguous chunks
@@ -311,6 +490,27 @@ namespace pcfd
         else grid = launch_block<2>(s, Q, h, w, U, sign, y);
         if (mode >= 1)
             block_final_kernel<<<1, 256, 0, launch_stream(s)>>>(s.block_partial, grid, mode == 2 ? Q.size() : 0, out);
+    }
+
+    void dcgs_pass(System& s, const VecSet& Q, double* v, const double* w, double* next, double* coefficient)
+    {
+        require(Q.size() <= kMaxSet, "delayed CGS2: too many vectors");
+        require(aligned16(v) && aligned16(w) && aligned16(next), "delayed CGS2: vector not 16-byte aligned");
+        require_aligned(Q, "delayed CGS2: vector not 16-byte aligned");
+        const int grid = block_grid();
+        const int m = Q.size();
+        const Sweep range = sweep_range(s);
+        auto dot = [&](auto kernel) { kernel<<<grid, kThreadsBlock, 0, launch_stream(s)>>>(Q, v, w, s.active, range, s.dcgs_partial); };
+        if (m <= 4) dot(dcgs_dot_kernel<1>);
+        else if (m <= 8) dot(dcgs_dot_kernel<2>);
+        else if (m <= 16) dot(dcgs_dot_kernel<4>);
+        else dot(dcgs_dot_kernel<8>);
+        dcgs_final_kernel<<<1, 256, 0, launch_stream(s)>>>(s.dcgs_partial, grid, m, coefficient);
+        auto update = [&](auto kernel) { kernel<<<grid, kThreadsBlock, 0, launch_stream(s)>>>(Q, coefficient, v, w, next, s.active, range); };
+        if (m <= 4) update(dcgs_update_kernel<1>);
+        else if (m <= 8) update(dcgs_update_kernel<2>);
+        else if (m <= 16) update(dcgs_update_kernel<4>);
+        else update(dcgs_update_kernel<8>);
     }
 
     void block_combine(System& s, const VecSet& Z, const Coefficients& c, double* y, bool accumulate)

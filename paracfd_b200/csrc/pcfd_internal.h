@@ -230,6 +230,9 @@ namespace pcfd
         DBuf<double> dot_partial;               // reduction scratch
         DBuf<double> block_partial;             // [592][kMaxSet + 1] block-kernel partial sums
         DBuf<double> block_result;              // [4][kMaxSet + 1] device coefficients / norms
+        DBuf<double> dcgs_partial, dcgs_result; // delayed CGS2 partials [592][2 kMaxSet + 4] and coefficients
+        double* pinned_dcgs = nullptr;          // pinned host copy of dcgs_result
+        bool delayed_orthogonalisation = false; // pcfd_options.gmres_delayed
         double* pinned_block = nullptr;         // pinned host copy of block_result
         DBuf<double> dot_result;                // device scalars
         double* pinned = nullptr;               // pinned host scalars
@@ -365,6 +368,10 @@ namespace pcfd
                       double* out);
     void block_combine(System& s, const VecSet& Z, const Coefficients& c, double* y, bool accumulate);   // y (+)= Z c
     void scale_by_inverse_norm(System& s, double* dst, const double* src, const double* norm2);        // dst = src / sqrt(n2)
+    // delayed CGS2 column step: reorthogonalise v against Q in place and write the next basis vector
+    // from w; coefficient[0..4*kMaxSet+9) as dcgs_final_kernel documents (krylov.cu)
+    void dcgs_pass(System& s, const VecSet& Q, double* v, const double* w, double* next, double* coefficient);
+    constexpr int kDcgsCoefficients = 4 * kMaxSet + 9;
 
     // ---- projection (projection.cu) ----
     void build_projection(System& s, const pcfd_topology& t);

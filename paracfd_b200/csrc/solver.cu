@@ -1013,72 +1013,170 @@ namespace pcfd
                 g[0] = beta;
                 vec_scaled_copy_active(s, s.gmres_v, s.defect, 1.0 / beta);
                 int used = 0;
-                for (int col = 0; col < cycle; ++col)
+                if (s.delayed_orthogonalisation)
                 {
-                    double* v = s.gmres_v.p + size_t(col) * ld;
-                    double* zc = s.gmres_z.p + size_t(col) * ld;
-                    apply_preconditioner(s, v, zc);
-                    ++result.preconditioner_applications;
-                    launch_apply(s, zc, s.Ad, false);
-                    // CGS2 against [C | V_0..V_col].  The matching z -= U h_C update is deferred: its
-                    // coefficients are kept per column and applied once when the cycle's
-                    // correction is formed (z only enters the solution through Z y).
-                    const int k = s.recycle_count, m = k + col + 1;
-                    VecSet Q = recycle_set(s.recycle_c.p);
-                    const VecSet none{int64_t(ld)};
-                    for (int row = 0; row <= col; ++row) Q.push(s.gmres_v.p + size_t(row) * ld);
-                    block_dot(s, Q, s.Ad, h1);
-                    block_update(s, Q, h1, s.Ad, none, -1.0, nullptr, 2, h2);
-                    block_update(s, Q, h2, s.Ad, none, -1.0, nullptr, 1, h3);
-                    scale_by_inverse_norm(s, s.gmres_v.p + size_t(col + 1) * ld, s.Ad, h3);
-                    read_block(3);
-                    bool column_valid = true;
-                    for (int j = 0; j < m && column_valid; ++j) column_valid = finite_value(host_h1[j]) && finite_value(host_h2[j]);
-                    if (!column_valid) break;
-                    double c_part = 0;
-                    for (int c = 0; c < k; ++c) c_part += host_h1[c] * host_h1[c];
-                    const double scale = std::sqrt(std::max(0.0, host_h1[m] - c_part));
-                    if (!(scale > 0) || !std::isfinite(scale)) break;
-                    for (int row = 0; row <= col; ++row) H[size_t(row) * cycle + col] = host_h1[k + row] + host_h2[k + row];
-                    for (int c = 0; c < k; ++c) zc_recycle[size_t(col) * System::recycle_capacity + c] = host_h1[c] + host_h2[c];
-                    double next_norm = std::sqrt(std::max(0.0, host_h3[0]));
-                    const double floor = 64 * std::numeric_limits<double>::epsilon() * scale;
-                    if (!(next_norm > floor && std::isfinite(1.0 / next_norm))) next_norm = 0;
-                    H[size_t(col + 1) * cycle + col] = next_norm;
-                    for (int row = 0; row < col; ++row)
+                    // Delayed CGS2: column col's single pass pair reorthogonalises V_col (projected
+                    // once in the previous column) and projects w = A z_col once; the previous
+                    // column's Hessenberg entries and deferred C coefficients are corrected here by
+                    // V_col's reorthogonalisation coefficients.  H is kept unrotated and the small
+                    // least-squares problem is solved from scratch per column.
+                    std::vector<double> Hu(size_t(cycle + 1) * cycle, 0.0);
+                    const int cap = System::recycle_capacity;
+                    double prev_rho = 0.0;
+                    auto least_squares = [&](int cols, bool solve) {
+                        std::vector<double> Rm(Hu.begin(), Hu.begin() + size_t(cols + 1) * cycle), gg(size_t(cols) + 1, 0.0);
+                        std::vector<double> c_(static_cast<size_t>(cols)), s_(static_cast<size_t>(cols));
+                        gg[0] = beta;
+                        for (int j = 0; j < cols; ++j)
+                        {
+                            for (int i = 0; i < j; ++i)
+                            {
+                                double& a = Rm[size_t(i) * cycle + j];
+                                double& bb = Rm[size_t(i + 1) * cycle + j];
+                                const double rot = c_[i] * a + s_[i] * bb;
+                                bb = -s_[i] * a + c_[i] * bb;
+                                a = rot;
+                            }
+                            double& d = Rm[size_t(j) * cycle + j];
+                            double& below = Rm[size_t(j + 1) * cycle + j];
+                            const double norm = std::hypot(d, below);
+                            if (!(norm > 0) || !std::isfinite(norm)) return std::numeric_limits<double>::quiet_NaN();
+                            c_[j] = d / norm;
+                            s_[j] = below / norm;
+                            d = norm;
+                            below = 0;
+                            const double old = gg[j];
+                            gg[j] = c_[j] * old;
+                            gg[j + 1] = -s_[j] * old;
+                        }
+                        if (solve)
+                            for (int row = cols - 1; row >= 0; --row)
+                            {
+                                double value = gg[row];
+                                for (int col = row + 1; col < cols; ++col) value -= Rm[size_t(row) * cycle + col] * y[col];
+                                y[row] = value / Rm[size_t(row) * cycle + row];
+                                if (!std::isfinite(y[row])) return std::numeric_limits<double>::quiet_NaN();
+                            }
+                        return std::abs(gg[cols]);
+                    };
+                    for (int col = 0; col < cycle; ++col)
                     {
-                        double& a = H[size_t(row) * cycle + col];
-                        double& bb = H[size_t(row + 1) * cycle + col];
-                        const double rot = cs[row] * a + sn[row] * bb;
-                        bb = -sn[row] * a + cs[row] * bb;
-                        a = rot;
+                        double* v = s.gmres_v.p + size_t(col) * ld;
+                        double* zc = s.gmres_z.p + size_t(col) * ld;
+                        apply_preconditioner(s, v, zc);
+                        ++result.preconditioner_applications;
+                        launch_apply(s, zc, s.Ad, false);
+                        const int k = s.recycle_count, m = k + col;
+                        VecSet Q = recycle_set(s.recycle_c.p);
+                        for (int row = 0; row < col; ++row) Q.push(s.gmres_v.p + size_t(row) * ld);
+                        dcgs_pass(s, Q, v, s.Ad, s.gmres_v.p + size_t(col + 1) * ld, s.dcgs_result);
+                        cuda_check(cudaMemcpyAsync(s.pinned_dcgs, s.dcgs_result.p, size_t(kDcgsCoefficients) * sizeof(double),
+                                                   cudaMemcpyDeviceToHost, s.stream), "coefficient readback");
+                        cuda_check(cudaStreamSynchronize(s.stream), "coefficient synchronize");
+                        const double* cf = s.pinned_dcgs;
+                        const double* sc = cf + 4 * kMaxSet;
+                        const double r = sc[3], c = sc[4], rho = sc[5];
+                        bool ok = std::isfinite(r) && std::isfinite(c) && std::isfinite(rho);
+                        for (int l = 0; l < m && ok; ++l) ok = std::isfinite(cf[l]) && std::isfinite(cf[kMaxSet + l]);
+                        if (!ok) break;
+                        if (col > 0)
+                        {
+                            for (int i = 0; i < col; ++i) Hu[size_t(i) * cycle + col - 1] += prev_rho * cf[k + i];
+                            for (int cc = 0; cc < k; ++cc) zc_recycle[size_t(col - 1) * cap + cc] += prev_rho * cf[cc];
+                            Hu[size_t(col) * cycle + col - 1] = prev_rho * r;
+                        }
+                        // V_col inside the span of the earlier vectors: the previous column closed
+                        // the Krylov space, and this column is not used
+                        if (!(r > 64 * std::numeric_limits<double>::epsilon() * std::sqrt(std::max(sc[0], 0.0))))
+                        {
+                            if (col > 0) Hu[size_t(col) * cycle + col - 1] = 0.0;
+                            break;
+                        }
+                        for (int i = 0; i < col; ++i) Hu[size_t(i) * cycle + col] = cf[kMaxSet + k + i];
+                        Hu[size_t(col) * cycle + col] = c;
+                        double next_norm = rho;
+                        if (!(next_norm > 64 * std::numeric_limits<double>::epsilon() * std::sqrt(std::max(sc[2], 0.0)))) next_norm = 0;
+                        Hu[size_t(col + 1) * cycle + col] = next_norm;
+                        for (int cc = 0; cc < k; ++cc) zc_recycle[size_t(col) * cap + cc] = cf[kMaxSet + cc];
+                        used = col + 1;
+                        ++result.iterations;
+                        const double estimate = least_squares(used, false);
+                        if (!std::isfinite(estimate)) { --used; --result.iterations; break; }
+                        if (estimate / std::sqrt(rhs2) <= tolerance || next_norm == 0) break;
+                        prev_rho = rho;
                     }
-                    double& diag = H[size_t(col) * cycle + col];
-                    double& below = H[size_t(col + 1) * cycle + col];
-                    const double norm = std::hypot(diag, below);
-                    if (!(norm > 0) || !std::isfinite(norm)) break;
-                    cs[col] = diag / norm;
-                    sn[col] = below / norm;
-                    diag = norm;
-                    below = 0;
-                    const double old = g[col];
-                    g[col] = cs[col] * old;
-                    g[col + 1] = -sn[col] * old;
-                    used = col + 1;
-                    ++result.iterations;
-                    if (std::abs(g[col + 1]) / std::sqrt(rhs2) <= tolerance || next_norm == 0) break;
+                    if (used == 0) break;
+                    if (!std::isfinite(least_squares(used, true))) break;
                 }
-                if (used == 0) break;
-                for (int row = used - 1; row >= 0; --row)
+                else
                 {
-                    double value = g[row];
-                    for (int col = row + 1; col < used; ++col) value -= H[size_t(row) * cycle + col] * y[col];
-                    const double d = H[size_t(row) * cycle + row];
-                    if (!(std::abs(d) > 0) || !std::isfinite(d)) { used = 0; break; }
-                    y[row] = value / d;
-                    if (!std::isfinite(y[row])) { used = 0; break; }
+                    for (int col = 0; col < cycle; ++col)
+                    {
+                        double* v = s.gmres_v.p + size_t(col) * ld;
+                        double* zc = s.gmres_z.p + size_t(col) * ld;
+                        apply_preconditioner(s, v, zc);
+                        ++result.preconditioner_applications;
+                        launch_apply(s, zc, s.Ad, false);
+                        // CGS2 against [C | V_0..V_col].  The matching z -= U h_C update is deferred: its
+                        // coefficients are kept per column and applied once when the cycle's
+                        // correction is formed (z only enters the solution through Z y).
+                        const int k = s.recycle_count, m = k + col + 1;
+                        VecSet Q = recycle_set(s.recycle_c.p);
+                        const VecSet none{int64_t(ld)};
+                        for (int row = 0; row <= col; ++row) Q.push(s.gmres_v.p + size_t(row) * ld);
+                        block_dot(s, Q, s.Ad, h1);
+                        block_update(s, Q, h1, s.Ad, none, -1.0, nullptr, 2, h2);
+                        block_update(s, Q, h2, s.Ad, none, -1.0, nullptr, 1, h3);
+                        scale_by_inverse_norm(s, s.gmres_v.p + size_t(col + 1) * ld, s.Ad, h3);
+                        read_block(3);
+                        bool column_valid = true;
+                        for (int j = 0; j < m && column_valid; ++j) column_valid = finite_value(host_h1[j]) && finite_value(host_h2[j]);
+                        if (!column_valid) break;
+                        double c_part = 0;
+                        for (int c = 0; c < k; ++c) c_part += host_h1[c] * host_h1[c];
+                        const double scale = std::sqrt(std::max(0.0, host_h1[m] - c_part));
+                        if (!(scale > 0) || !std::isfinite(scale)) break;
+                        for (int row = 0; row <= col; ++row) H[size_t(row) * cycle + col] = host_h1[k + row] + host_h2[k + row];
+                        for (int c = 0; c < k; ++c) zc_recycle[size_t(col) * System::recycle_capacity + c] = host_h1[c] + host_h2[c];
+                        double next_norm = std::sqrt(std::max(0.0, host_h3[0]));
+                        const double floor = 64 * std::numeric_limits<double>::epsilon() * scale;
+                        if (!(next_norm > floor && std::isfinite(1.0 / next_norm))) next_norm = 0;
+                        H[size_t(col + 1) * cycle + col] = next_norm;
+                        for (int row = 0; row < col; ++row)
+                        {
+                            double& a = H[size_t(row) * cycle + col];
+                            double& bb = H[size_t(row + 1) * cycle + col];
+                            const double rot = cs[row] * a + sn[row] * bb;
+                            bb = -sn[row] * a + cs[row] * bb;
+                            a = rot;
+                        }
+                        double& diag = H[size_t(col) * cycle + col];
+                        double& below = H[size_t(col + 1) * cycle + col];
+                        const double norm = std::hypot(diag, below);
+                        if (!(norm > 0) || !std::isfinite(norm)) break;
+                        cs[col] = diag / norm;
+                        sn[col] = below / norm;
+                        diag = norm;
+                        below = 0;
+                        const double old = g[col];
+                        g[col] = cs[col] * old;
+                        g[col + 1] = -sn[col] * old;
+                        used = col + 1;
+                        ++result.iterations;
+                        if (std::abs(g[col + 1]) / std::sqrt(rhs2) <= tolerance || next_norm == 0) break;
+                    }
+                    if (used == 0) break;
+                    for (int row = used - 1; row >= 0; --row)
+                    {
+                        double value = g[row];
+                        for (int col = row + 1; col < used; ++col) value -= H[size_t(row) * cycle + col] * y[col];
+                        const double d = H[size_t(row) * cycle + row];
+                        if (!(std::abs(d) > 0) || !std::isfinite(d)) { used = 0; break; }
+                        y[row] = value / d;
+                        if (!std::isfinite(y[row])) { used = 0; break; }
+                    }
+                    if (used == 0) break;
                 }
-                if (used == 0) break;
                 {
                     // correction = sum_j y_j (z_j - U c_j) = Z y - U (sum_j y_j c_j)
                     VecSet Z{int64_t(ld)};
