@@ -106,6 +106,7 @@ namespace pcfd
         int cells = 0;
         DBuf<int> row_offset, neighbour, aggregate, restrict_offset, restrict_dof;
         DBuf<T> coefficient, diagonal, rhs, x, temporary, residual;
+        DBuf<T> inverse;                        // coarsest composite stage: explicit inverse [cells][cells] or empty
         double prolong = 1.0;                   // weight of the next level's correction added here
         int sweeps = 2;                         // smoothing steps before and after the coarse correction
         int chebyshev = 0;                      // 0: damped Jacobi; r >= 2: Chebyshev on [2 / r, 2]

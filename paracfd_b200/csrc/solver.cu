@@ -326,6 +326,75 @@ namespace pcfd
         }
     }
 
+    namespace
+    {
+        // Explicit inverse of a coarsest level of at most 512 cells (Gauss-Jordan with partial
+        // pivoting in FP64) over its cells with a positive diagonal; rows and columns of the other
+        // cells stay zero, as the Jacobi sweeps leave them.  Empty when the level is larger or the
+        // matrix is numerically singular (the 96 Jacobi sweeps are used then).
+        std::vector<double> dense_inverse(const HostLevel& level)
+        {
+            const int n = level.cells;
+            if (n <= 0 || n > 512) return {};
+            std::vector<int> live;
+            std::vector<int> index(size_t(n), -1);
+            for (int q = 0; q < n; ++q)
+                if (level.diagonal[q] > 0) { index[q] = int(live.size()); live.push_back(q); }
+            const int m = int(live.size());
+            if (!m) return {};
+            std::vector<double> a(size_t(m) * m, 0.0), inv(size_t(m) * m, 0.0);
+            double scale = 0.0;
+            for (int i = 0; i < m; ++i)
+            {
+                a[size_t(i) * m + i] = level.diagonal[live[i]];
+                inv[size_t(i) * m + i] = 1.0;
+                scale = std::max(scale, std::abs(level.diagonal[live[i]]));
+            }
+            for (const HostEdge& e : level.edges)
+            {
+                const int i = index[e.a], j = index[e.b];
+                if (i < 0 || j < 0) continue;
+                a[size_t(i) * m + j] -= e.coefficient;
+                a[size_t(j) * m + i] -= e.coefficient;
+            }
+            for (int c = 0; c < m; ++c)
+            {
+                int p = c;
+                for (int r = c + 1; r < m; ++r)
+                    if (std::abs(a[size_t(r) * m + c]) > std::abs(a[size_t(p) * m + c])) p = r;
+                if (!(std::abs(a[size_t(p) * m + c]) > 1e-12 * scale)) return {};
+                if (p != c)
+                    for (int j = 0; j < m; ++j)
+                    {
+                        std::swap(a[size_t(p) * m + j], a[size_t(c) * m + j]);
+                        std::swap(inv[size_t(p) * m + j], inv[size_t(c) * m + j]);
+                    }
+                const double d = 1.0 / a[size_t(c) * m + c];
+                for (int j = 0; j < m; ++j) { a[size_t(c) * m + j] *= d; inv[size_t(c) * m + j] *= d; }
+                for (int r = 0; r < m; ++r)
+                {
+                    if (r == c) continue;
+                    const double f = a[size_t(r) * m + c];
+                    if (f == 0.0) continue;
+                    for (int j = 0; j < m; ++j)
+                    {
+                        a[size_t(r) * m + j] -= f * a[size_t(c) * m + j];
+                        inv[size_t(r) * m + j] -= f * inv[size_t(c) * m + j];
+                    }
+                }
+            }
+            std::vector<double> out(size_t(n) * n, 0.0);
+            for (int i = 0; i < m; ++i)
+                for (int j = 0; j < m; ++j)
+                {
+                    const double v = inv[size_t(i) * m + j];
+                    if (!std::isfinite(v)) return {};
+                    out[size_t(live[i]) * n + live[j]] = v;
+                }
+            return out;
+        }
+    }
+
     void build_composite(System& s, const pcfd_topology& t)
     {
         const int bs = t.brick_size, c3 = bs * bs * bs, S = t.storage_size;
@@ -470,6 +539,7 @@ namespace pcfd
         s.fine_residual.alloc(size_t(S));
         s.inter64.clear();
         s.inter32.clear();
+        const std::vector<double> inverse = dense_inverse(stages.back());
         if (s.composite_fp32)
         {
             s.inter32.resize(stages.size());
@@ -480,6 +550,7 @@ namespace pcfd
                 s.inter32[k].sweeps = s.mg_stage_sweeps;
                 s.inter32[k].chebyshev = s.mg_stage_chebyshev;
             }
+            if (!inverse.empty()) s.inter32.back().inverse.upload(std::vector<float>(inverse.begin(), inverse.end()));
         }
         else
         {
@@ -491,6 +562,7 @@ namespace pcfd
                 s.inter64[k].sweeps = s.mg_stage_sweeps;
                 s.inter64[k].chebyshev = s.mg_stage_chebyshev;
             }
+            if (!inverse.empty()) s.inter64.back().inverse.upload(inverse);
         }
         s.composite = true;
     }
@@ -534,6 +606,18 @@ namespace pcfd
             for (int e = row_offset[q]; e < row_offset[q + 1]; ++e) Ax -= double(coefficient[e]) * double(x[neighbour[e]]);
             next[q] = x[q] + omega * T((double(rhs[q]) - Ax) / double(diag[q]));
         }
+        // x = inverse * rhs on a coarsest level (one warp per row, FP64 accumulation)
+        template <class T>
+        __global__ void dense_apply_kernel(const T* __restrict__ inverse, const T* __restrict__ rhs, T* __restrict__ x, int n)
+        {
+            const int row = int((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+            if (row >= n) return;
+            double acc = 0.0;
+            for (int j = lane; j < n; j += 32) acc += double(inverse[int64_t(row) * n + j]) * double(rhs[j]);
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+            if (lane == 0) x[row] = T(acc);
+        }
+
         // One Chebyshev step of a CSR level, fused: r = rhs - A x, d = c1 d + c2 D^-1 r (first step:
         // d = c2 D^-1 r), next = x + d
         template <class T>
@@ -654,7 +738,10 @@ namespace pcfd
             };
             if (index + 1 == count)
             {
-                if (level.cells <= 4096)
+                if (level.inverse.p)
+                    dense_apply_kernel<T><<<blocks_for(int64_t(level.cells) * 32), kThreads, 0, launch_stream(s)>>>(level.inverse, level.rhs,
+                                                                                                              level.x, level.cells);
+                else if (level.cells <= 4096)
                     coarse_jacobi_kernel<T, 4><<<1, 1024, 0, launch_stream(s)>>>(level.rhs, level.x, level.temporary, level.row_offset,
                         level.neighbour, level.coefficient, level.diagonal, level.cells, omega, 96);
                 else
