@@ -60,6 +60,7 @@ def parse_args():
                     help="composite fine sweeps: r >= 2 = Chebyshev-Richardson steps on [2/r, 2], 1 = damped Jacobi, 0: r = 10")
     ap.add_argument("--delayed", type=int, default=1, choices=(0, 1),
                     help="1: GCRO columns orthogonalised by delayed CGS2 (two passes instead of three); 0: CGS2")
+    ap.add_argument("--recycle", type=int, default=0, help="GCRO recycled pairs: 1..3, -1 none, 0: 3")
     ap.add_argument("--block-iterations", type=int, default=0,
                     help="composite cycle: Chebyshev iterations of the brick block pre-smoother (0: Jacobi pre-sweeps)")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU sample of the ours arm")
@@ -320,7 +321,8 @@ def run_ours(args, ranks: Ranks):
                              mg_cycle={"reference": 0, "corrected": 1, "composite": 2}[args.mg_cycle],
                              gmres_restart=args.restart, mg_stage_sweeps=args.stage_sweeps,
                              mg_block_iterations=args.block_iterations, mg_stage_chebyshev=args.chebyshev,
-                             mg_fine_chebyshev=args.fine_chebyshev, gmres_delayed=args.delayed)
+                             mg_fine_chebyshev=args.fine_chebyshev, gmres_delayed=args.delayed,
+                             gmres_recycle=args.recycle)
     system.configure(speed=spec.speed, **spec.case)
     slots = system.inflow_layout()
     faces = len(slots) * spec.brick_size ** 2
@@ -412,6 +414,7 @@ def run_ours(args, ranks: Ranks):
                        stage_smoother="jacobi" if args.chebyshev == 1 else f"chebyshev 2/{args.chebyshev or 30}",
                        fine_smoother="jacobi" if args.fine_chebyshev == 1 else f"chebyshev-richardson 2/{args.fine_chebyshev or 10}",
                        orthogonalisation="delayed CGS2" if args.delayed else "CGS2",
+                       recycled_pairs=3 if args.recycle == 0 else max(args.recycle, 0),
                        parallelism=f"replicas{n}",
                        l2="inputs larger than L2"),
         "projection_ms": round(statistics.mean(s["projection_ms"] for s in stats), 3),
@@ -469,7 +472,8 @@ def run_kernel_only(args):
                              mg_cycle={"reference": 0, "corrected": 1, "composite": 2}[args.mg_cycle],
                              gmres_restart=args.restart, mg_stage_sweeps=args.stage_sweeps,
                              mg_block_iterations=args.block_iterations, mg_stage_chebyshev=args.chebyshev,
-                             mg_fine_chebyshev=args.fine_chebyshev, gmres_delayed=args.delayed)
+                             mg_fine_chebyshev=args.fine_chebyshev, gmres_delayed=args.delayed,
+                             gmres_recycle=args.recycle)
     ms = system.time_kernel(args.kernel_only, args.kernel_iterations)
     line = {"kernel_only": args.kernel_only, "workload": args.workload, "ms_per_launch": ms,
             "iterations": args.kernel_iterations, "launches": system.launch_count()}
@@ -677,7 +681,8 @@ def run_sweep(args, ranks: Ranks):
         builts = [sp.build() for sp in batch]
         systems = [CompositeSystem(b.topology, MG_FP32, device=ranks.local, mg_cycle=MG_CYCLE_COMPOSITE,
                                    mg_stage_sweeps=args.stage_sweeps, mg_stage_chebyshev=args.chebyshev,
-                                   mg_fine_chebyshev=args.fine_chebyshev, gmres_delayed=args.delayed) for b in builts]
+                                   mg_fine_chebyshev=args.fine_chebyshev, gmres_delayed=args.delayed,
+                             gmres_recycle=args.recycle) for b in builts]
         for sp, sy in zip(batch, systems):
             sy.configure(speed=sp.speed, **sp.case)
             sy.initialize()

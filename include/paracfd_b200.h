@@ -188,6 +188,8 @@ typedef struct pcfd_options {
                                         and one update pass over the basis per column; the previous
                                         basis vector reorthogonalised in the same passes); 0: CGS2
                                         (three passes) */
+    int32_t gmres_recycle;           /* recycled (U, C = A U) pairs kept between solves: 1..3; -1: none;
+                                        0: the reference's 3 */
 } pcfd_options;
 
 /* Coarse-correction weighting of the multigrid cycle.  The aggregation coarse operators are

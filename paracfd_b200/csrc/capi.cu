@@ -209,6 +209,11 @@ namespace pcfd
                 require(options->mg_stage_sweeps > 0 && options->mg_stage_sweeps <= 16, "mg_stage_sweeps must be 0..16");
                 s.mg_stage_sweeps = options->mg_stage_sweeps;
             }
+            if (options && options->gmres_recycle)
+            {
+                require(options->gmres_recycle >= -1 && options->gmres_recycle <= System::recycle_capacity, "gmres_recycle must be -1..3");
+                s.recycle_limit = options->gmres_recycle < 0 ? 0 : options->gmres_recycle;
+            }
             if (options && options->gmres_delayed)
             {
                 require(options->gmres_delayed == 1, "gmres_delayed must be 0 or 1");

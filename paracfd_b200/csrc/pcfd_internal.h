@@ -228,6 +228,7 @@ namespace pcfd
         static constexpr int gmres_restart = 24;   // the reference's LGMRES(24) (storage and default)
         int restart = gmres_restart;               // columns per cycle actually used (<= gmres_restart)
         static constexpr int recycle_capacity = 3;
+        int recycle_limit = recycle_capacity;      // recycled pairs kept between solves (pcfd_options)
         DBuf<double> dot_partial;               // reduction scratch
         DBuf<double> block_partial;             // [592][kMaxSet + 1] block-kernel partial sums
         DBuf<double> block_result;              // [4][kMaxSet + 1] device coefficients / norms

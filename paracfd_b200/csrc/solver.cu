@@ -1286,6 +1286,11 @@ namespace pcfd
                 residual2 = true_residual();
                 result.relative_residual = std::sqrt(residual2 / rhs2);
                 if (!std::isfinite(result.relative_residual)) break;
+                if (s.recycle_limit <= 0)
+                {
+                    if (result.relative_residual <= tolerance) { result.converged = 1; break; }
+                    continue;
+                }
                 // store a normalised (U, C = A U) pair when it adds a resolved direction
                 launch_apply(s, s.correction, s.Ad, false);
                 {
@@ -1303,9 +1308,9 @@ namespace pcfd
                 cand_valid = cand_valid && std::isfinite(cand_after) && cand_after > 1e-12 * cand_before && std::isfinite(1.0 / cand_after);
                 if (cand_valid)
                 {
-                    if (s.recycle_count == System::recycle_capacity)
+                    if (s.recycle_count >= s.recycle_limit)
                     {
-                        for (int c = 1; c < System::recycle_capacity; ++c)
+                        for (int c = 1; c < s.recycle_count; ++c)
                         {
                             cuda_check(cudaMemcpyAsync(ru(c - 1), ru(c), size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, s.stream), "shift recycle");
                             cuda_check(cudaMemcpyAsync(rcv(c - 1), rcv(c), size_t(n) * sizeof(double), cudaMemcpyDeviceToDevice, s.stream), "shift recycle");
