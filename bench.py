@@ -60,7 +60,8 @@ def parse_args():
                     help="composite fine sweeps: r >= 2 = Chebyshev-Richardson steps on [2/r, 2], 1 = damped Jacobi, 0: r = 10")
     ap.add_argument("--delayed", type=int, default=1, choices=(0, 1),
                     help="1: GCRO columns orthogonalised by delayed CGS2 (two passes instead of three); 0: CGS2")
-    ap.add_argument("--recycle", type=int, default=0, help="GCRO recycled pairs: 1..3, -1 none, 0: 3")
+    ap.add_argument("--recycle", type=int, default=-1,
+                    help="GCRO recycled pairs kept between solves: 1..3, -1 none (default), 0: the reference's 3")
     ap.add_argument("--block-iterations", type=int, default=0,
                     help="composite cycle: Chebyshev iterations of the brick block pre-smoother (0: Jacobi pre-sweeps)")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU sample of the ours arm")
