@@ -261,7 +261,8 @@ namespace pcfd
             cuda_check(cudaMallocHost(&s.pinned_block, size_t(4) * (kMaxSet + 1) * sizeof(double)), "pinned block scalars");
             s.dcgs_partial.alloc(size_t(592) * (2 * kMaxSet + 4));
             s.dcgs_result.alloc(size_t(kDcgsCoefficients));
-            cuda_check(cudaMallocHost(&s.pinned_dcgs, size_t(kDcgsCoefficients) * sizeof(double)), "pinned orthogonalisation scalars");
+            cuda_check(cudaMallocHost(&s.pinned_dcgs, size_t(2) * kDcgsCoefficients * sizeof(double)), "pinned orthogonalisation scalars");
+            for (cudaEvent_t& e : s.dcgs_ready) cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "column event");
             // flow state
             s.u.alloc(size_t(s.faces)); s.v.alloc(size_t(s.faces)); s.w.alloc(size_t(s.faces));
             s.divergence.alloc(size_t(s.S));
@@ -319,6 +320,8 @@ namespace pcfd
         if (pinned) cudaFreeHost(pinned);
         if (pinned_block) cudaFreeHost(pinned_block);
         if (pinned_dcgs) cudaFreeHost(pinned_dcgs);
+        for (cudaEvent_t e : dcgs_ready)
+            if (e) cudaEventDestroy(e);
         if (own_stream && stream) cudaStreamDestroy(stream);
     }
 }

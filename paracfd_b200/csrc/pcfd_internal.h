@@ -233,7 +233,8 @@ namespace pcfd
         DBuf<double> block_partial;             // [592][kMaxSet + 1] block-kernel partial sums
         DBuf<double> block_result;              // [4][kMaxSet + 1] device coefficients / norms
         DBuf<double> dcgs_partial, dcgs_result; // delayed CGS2 partials [592][2 kMaxSet + 4] and coefficients
-        double* pinned_dcgs = nullptr;          // pinned host copy of dcgs_result
+        double* pinned_dcgs = nullptr;          // pinned host copies of dcgs_result, two columns
+        cudaEvent_t dcgs_ready[2] = {};         // readback of column j lands in slot j & 1
         bool delayed_orthogonalisation = false; // pcfd_options.gmres_delayed
         double* pinned_block = nullptr;         // pinned host copy of block_result
         DBuf<double> dot_result;                // device scalars

@@ -1146,21 +1146,33 @@ namespace pcfd
                             }
                         return std::abs(gg[cols]);
                     };
-                    for (int col = 0; col < cycle; ++col)
-                    {
+                    // Column col's work (preconditioner, operator, both passes, coefficient readback)
+                    // is enqueued as one unit; while the residual estimate is still far above the
+                    // tolerance, column col + 1 is enqueued before the host waits for column col.
+                    const int k = s.recycle_count;
+                    auto enqueue = [&](int col) {
                         double* v = s.gmres_v.p + size_t(col) * ld;
                         double* zc = s.gmres_z.p + size_t(col) * ld;
                         apply_preconditioner(s, v, zc);
-                        ++result.preconditioner_applications;
                         launch_apply(s, zc, s.Ad, false);
-                        const int k = s.recycle_count, m = k + col;
                         VecSet Q = recycle_set(s.recycle_c.p);
                         for (int row = 0; row < col; ++row) Q.push(s.gmres_v.p + size_t(row) * ld);
                         dcgs_pass(s, Q, v, s.Ad, s.gmres_v.p + size_t(col + 1) * ld, s.dcgs_result);
-                        cuda_check(cudaMemcpyAsync(s.pinned_dcgs, s.dcgs_result.p, size_t(kDcgsCoefficients) * sizeof(double),
-                                                   cudaMemcpyDeviceToHost, s.stream), "coefficient readback");
-                        cuda_check(cudaStreamSynchronize(s.stream), "coefficient synchronize");
-                        const double* cf = s.pinned_dcgs;
+                        cuda_check(cudaMemcpyAsync(s.pinned_dcgs + size_t(col & 1) * kDcgsCoefficients, s.dcgs_result.p,
+                                                   size_t(kDcgsCoefficients) * sizeof(double), cudaMemcpyDeviceToHost, s.stream),
+                                   "coefficient readback");
+                        cuda_check(cudaEventRecord(s.dcgs_ready[col & 1], s.stream), "coefficient event");
+                    };
+                    double previous_estimate = beta;
+                    enqueue(0);
+                    for (int col = 0; col < cycle; ++col)
+                    {
+                        const bool speculate = col + 1 < cycle && previous_estimate > 30.0 * tolerance * std::sqrt(rhs2);
+                        if (speculate) enqueue(col + 1);
+                        cuda_check(cudaEventSynchronize(s.dcgs_ready[col & 1]), "coefficient synchronize");
+                        ++result.preconditioner_applications;
+                        const int m = k + col;
+                        const double* cf = s.pinned_dcgs + size_t(col & 1) * kDcgsCoefficients;
                         const double* sc = cf + 4 * kMaxSet;
                         const double r = sc[3], c = sc[4], rho = sc[5];
                         bool ok = std::isfinite(r) && std::isfinite(c) && std::isfinite(rho);
@@ -1190,8 +1202,12 @@ namespace pcfd
                         const double estimate = least_squares(used, false);
                         if (!std::isfinite(estimate)) { --used; --result.iterations; break; }
                         if (estimate / std::sqrt(rhs2) <= tolerance || next_norm == 0) break;
+                        if (!speculate && col + 1 < cycle) enqueue(col + 1);
+                        previous_estimate = estimate;
                         prev_rho = rho;
                     }
+                    // a column enqueued ahead and not used has finished before the correction is formed
+                    cuda_check(cudaStreamSynchronize(s.stream), "column pipeline");
                     if (used == 0) break;
                     if (!std::isfinite(least_squares(used, true))) break;
                 }
