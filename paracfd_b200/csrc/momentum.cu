@@ -32,8 +32,9 @@ namespace pcfd
                                            const double* level_h, CellCtx& c)
         {
             const int c3 = bs * bs * bs;
-            c.slot = brick_list[work / c3];
-            const int local = int(work % c3);
+            // DOF counts fit in 32 bits (pcfd_topology indexes them with int): 32-bit division
+            c.slot = brick_list[int(work) / c3];
+            const int local = int(work) % c3;
             c.i = local % bs; c.j = (local / bs) % bs; c.k = local / (bs * bs);
             c.dof = int64_t(c.slot) * c3 + local;
             c.h = float(level_h[brick_level[c.slot]]);

@@ -113,7 +113,7 @@ namespace pcfd
             const int c3 = bs * bs * bs;
             const int64_t work = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
             if (work >= int64_t(brick_count) * c3) return;
-            const int slot = brick_list[work / c3], local = int(work % c3);
+            const int slot = brick_list[int(work) / c3], local = int(work) % c3;
             const int i = local % bs, j = (local / bs) % bs, k = local / (bs * bs);
             const int64_t a = int64_t(slot) * c3 + local;
             if (!active[a]) { out[a] = T(0); return; }

@@ -36,7 +36,7 @@ namespace pcfd
             const int c3 = bs * bs * bs;
             const int64_t work = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
             if (work >= int64_t(brick_count) * c3) return;
-            const int slot = brick_list[work / c3], local = int(work % c3);
+            const int slot = brick_list[int(work) / c3], local = int(work) % c3;
             const int i = local % bs, j = (local / bs) % bs, k = local / (bs * bs);
             const int64_t a = int64_t(slot) * c3 + local;
             if (!active[a]) { integrated[a] = 0.0; return; }
@@ -77,6 +77,86 @@ namespace pcfd
             if ((flags[slot] & PCFD_BRICK_XMIN) && i == 0) net -= double(u[u_face(bs, slot, 0, j, k)]) * area;
             if ((flags[slot] & PCFD_BRICK_XMAX) && i == bs - 1) net += double(u[u_face(bs, slot, bs, j, k)]) * area;
             integrated[a] = net;
+        }
+
+        // The same integrated flux for 8^3 bricks, one CTA per non-covered brick (two cells per
+        // thread): the brick's active and cut bytes and its neighbour slots staged in shared
+        // memory, 32-bit index arithmetic, and the per-cell terms added in the order above, so the
+        // result is bit-identical.
+        __global__ void __launch_bounds__(256) brick_integrated_flux_kernel(const int* __restrict__ brick_list,
+            const int* __restrict__ brick_level, const int* __restrict__ nbr, const uint32_t* __restrict__ flags,
+            const double* __restrict__ level_h, const uint8_t* __restrict__ active, const uint8_t* __restrict__ cut,
+            const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w, double* __restrict__ integrated)
+        {
+            constexpr int bs = 8, c3 = 512;
+            __shared__ uint8_t act[c3], cm[c3];
+            __shared__ int nb[6];
+            const int slot = brick_list[blockIdx.x];
+            const int64_t first = int64_t(slot) * c3;
+            if (threadIdx.x < 6) nb[threadIdx.x] = nbr[slot * 6 + threadIdx.x];
+            for (int c = threadIdx.x; c < c3; c += 256)
+            {
+                act[c] = active[first + c];
+                cm[c] = cut[first + c];
+            }
+            __syncthreads();
+            const double h = level_h[brick_level[slot]], area = h * h;
+            const uint32_t fl = flags[slot];
+            const float* comp[3] = {u, v, w};
+            for (int half = 0; half < 2; ++half)
+            {
+                const int local = threadIdx.x + 256 * half;
+                const int i = local & 7, j = (local >> 3) & 7, k = local >> 6;
+                const int64_t a = first + local;
+                if (!act[local]) { integrated[a] = 0.0; continue; }
+                const int ijk[3] = {i, j, k};
+                const int stride[3] = {1, 8, 64};
+                double net = 0.0;
+                for (int axis = 0; axis < 3; ++axis)
+                {
+                    // + face (a -> upper)
+                    bool upper_active = false;
+                    if (ijk[axis] < bs - 1) upper_active = act[local + stride[axis]];
+                    else if (nb[2 * axis + 1] >= 0) upper_active = active[int64_t(nb[2 * axis + 1]) * c3 + local - (bs - 1) * stride[axis]];
+                    if (upper_active && !(cm[local] & (1u << axis)))
+                    {
+                        int f[3] = {i, j, k};
+                        ++f[axis];
+                        net += double(comp[axis][axis == 0 ? u_face(bs, slot, f[0], f[1], f[2])
+                                                           : (axis == 1 ? v_face(bs, slot, f[0], f[1], f[2]) : w_face(bs, slot, f[0], f[1], f[2]))]) * area;
+                    }
+                    // - face (lower -> a), read from the lower cell's brick
+                    int lower_slot = -1, lower_local = 0;
+                    bool lower_active = false;
+                    uint8_t lower_cut = 0;
+                    if (ijk[axis] > 0)
+                    {
+                        lower_slot = slot;
+                        lower_local = local - stride[axis];
+                        lower_active = act[lower_local];
+                        lower_cut = cm[lower_local];
+                    }
+                    else if (nb[2 * axis] >= 0)
+                    {
+                        lower_slot = nb[2 * axis];
+                        lower_local = local + (bs - 1) * stride[axis];
+                        const int64_t lq = int64_t(lower_slot) * c3 + lower_local;
+                        lower_active = active[lq];
+                        lower_cut = cut[lq];
+                    }
+                    if (lower_slot >= 0 && lower_active && !(lower_cut & (1u << axis)))
+                    {
+                        int f[3] = {lower_local & 7, (lower_local >> 3) & 7, lower_local >> 6};
+                        ++f[axis];
+                        net -= double(comp[axis][axis == 0 ? u_face(bs, lower_slot, f[0], f[1], f[2])
+                                                           : (axis == 1 ? v_face(bs, lower_slot, f[0], f[1], f[2])
+                                                                        : w_face(bs, lower_slot, f[0], f[1], f[2]))]) * area;
+                    }
+                }
+                if ((fl & PCFD_BRICK_XMIN) && i == 0) net -= double(u[u_face(bs, slot, 0, j, k)]) * area;
+                if ((fl & PCFD_BRICK_XMAX) && i == bs - 1) net += double(u[u_face(bs, slot, bs, j, k)]) * area;
+                integrated[a] = net;
+            }
         }
 
         __global__ void zero_tail_kernel(double* x, int64_t begin, int64_t end)
@@ -127,7 +207,7 @@ namespace pcfd
             const int c3 = bs * bs * bs;
             const int64_t work = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
             if (work >= int64_t(brick_count) * c3) return;
-            const int slot = brick_list[work / c3], local = int(work % c3);
+            const int slot = brick_list[int(work) / c3], local = int(work) % c3;
             const int i = local % bs, j = (local / bs) % bs, k = local / (bs * bs);
             const int64_t a = int64_t(slot) * c3 + local;
             if (!active[a]) return;
@@ -381,9 +461,16 @@ namespace pcfd
     void launch_integrated_flux(System& s)
     {
         if (s.active_bricks)
-            structured_integrated_flux_kernel<<<blocks_for(int64_t(s.active_bricks) * s.bs3), kThreads, 0, launch_stream(s)>>>(
-                s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr, s.brick_flags, s.d_level_h, s.active,
-                s.cut_face_mask, s.u, s.v, s.w, s.integrated);
+        {
+            if (s.bs == 8)
+                brick_integrated_flux_kernel<<<s.active_bricks, 256, 0, launch_stream(s)>>>(
+                    s.active_brick_list, s.brick_level, s.brick_nbr, s.brick_flags, s.d_level_h, s.active, s.cut_face_mask, s.u, s.v,
+                    s.w, s.integrated);
+            else
+                structured_integrated_flux_kernel<<<blocks_for(int64_t(s.active_bricks) * s.bs3), kThreads, 0, launch_stream(s)>>>(
+                    s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr, s.brick_flags, s.d_level_h, s.active,
+                    s.cut_face_mask, s.u, s.v, s.w, s.integrated);
+        }
         if (s.S > s.structured)
             zero_tail_kernel<<<blocks_for(s.S - s.structured), kThreads, 0, launch_stream(s)>>>(s.integrated, s.structured, s.S);
         if (s.special_incident_dofs)
