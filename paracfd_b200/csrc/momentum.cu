@@ -127,13 +127,15 @@ namespace pcfd
         }
 
         // ---------------------------------------------------------------- transport
-        __global__ void transport_struct_kernel(const int* __restrict__ brick_list, int nbricks, int bs, const int* __restrict__ brick_level,
+        template <int kBS>
+        __global__ void transport_struct_kernel(const int* __restrict__ brick_list, int nbricks, int bs_arg, const int* __restrict__ brick_level,
             const int* __restrict__ nbr, const uint32_t* __restrict__ flags, const double* __restrict__ level_h,
             const uint8_t* __restrict__ code, const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w,
             const float* __restrict__ x, const float* __restrict__ y, const float* __restrict__ z, float dt, int external, float U,
             const int* __restrict__ inflow_slot, const float* __restrict__ inflow, float* __restrict__ xn, float* __restrict__ yn, float* __restrict__ zn, float* __restrict__ dx, float* __restrict__ dy,
             float* __restrict__ dz)
         {
+            const int bs = kBS ? kBS : bs_arg;   // 8^3 bricks: index math folded at compile time
             const int64_t work = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
             if (work >= int64_t(nbricks) * bs * bs * bs) return;
             CellCtx c;
@@ -354,11 +356,13 @@ namespace pcfd
             return 2.0f * (sxx * sxx + syy * syy + szz * szz + 2.0f * (sxy * sxy + sxz * sxz + syz * syz));
         }
 
-        __global__ void viscosity_struct_kernel(const int* __restrict__ brick_list, int nbricks, int bs, const int* __restrict__ brick_level,
+        template <int kBS>
+        __global__ void viscosity_struct_kernel(const int* __restrict__ brick_list, int nbricks, int bs_arg, const int* __restrict__ brick_level,
             const int* __restrict__ nbr, const double* __restrict__ level_h, const uint8_t* __restrict__ code,
             const uint8_t* __restrict__ special, const float* __restrict__ volume, const float* __restrict__ x,
             const float* __restrict__ y, const float* __restrict__ z, float nu, float cs, float* __restrict__ viscosity)
         {
+            const int bs = kBS ? kBS : bs_arg;   // 8^3 bricks: index math folded at compile time
             const int64_t work = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
             if (work >= int64_t(nbricks) * bs * bs * bs) return;
             CellCtx c;
@@ -410,11 +414,13 @@ namespace pcfd
             return v;
         }
 
-        __global__ void __launch_bounds__(256) rate_struct_kernel(const int* __restrict__ brick_list, int nbricks, int bs,
+        template <int kBS>
+        __global__ void __launch_bounds__(256) rate_struct_kernel(const int* __restrict__ brick_list, int nbricks, int bs_arg,
             const int* __restrict__ brick_level, const int* __restrict__ nbr, const double* __restrict__ level_h,
             const uint8_t* __restrict__ code, const float* __restrict__ viscosity, float* __restrict__ partial_rate,
             float* __restrict__ block_partial)
         {
+            const int bs = kBS ? kBS : bs_arg;   // 8^3 bricks: index math folded at compile time
             __shared__ float shared[8];
             const int64_t work = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
             float local_max = 0.0f;
@@ -477,12 +483,14 @@ namespace pcfd
             if (threadIdx.x == 0) *out = v;
         }
 
-        __global__ void diffuse_struct_kernel(const int* __restrict__ brick_list, int nbricks, int bs, const int* __restrict__ brick_level,
+        template <int kBS>
+        __global__ void diffuse_struct_kernel(const int* __restrict__ brick_list, int nbricks, int bs_arg, const int* __restrict__ brick_level,
             const int* __restrict__ nbr, const double* __restrict__ level_h, const uint8_t* __restrict__ code,
             const float* __restrict__ viscosity, const float* __restrict__ x, const float* __restrict__ y, const float* __restrict__ z,
             float dt, float* __restrict__ xn, float* __restrict__ yn, float* __restrict__ zn, float* __restrict__ dx,
             float* __restrict__ dy, float* __restrict__ dz)
         {
+            const int bs = kBS ? kBS : bs_arg;   // 8^3 bricks: index math folded at compile time
             const int64_t work = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
             if (work >= int64_t(nbricks) * bs * bs * bs) return;
             CellCtx c;
@@ -618,12 +626,14 @@ namespace pcfd
             gradient[3 * node] = gx; gradient[3 * node + 1] = gy; gradient[3 * node + 2] = gz;
         }
 
-        __global__ void impulse_struct_kernel(const int* __restrict__ brick_list, int nbricks, int bs, const int* __restrict__ brick_level,
+        template <int kBS>
+        __global__ void impulse_struct_kernel(const int* __restrict__ brick_list, int nbricks, int bs_arg, const int* __restrict__ brick_level,
             const int* __restrict__ nbr, const uint32_t* __restrict__ flags, const double* __restrict__ level_h,
             const uint8_t* __restrict__ code, const float* __restrict__ p, float scale, int outlet, int physical,
             const float* __restrict__ x, const float* __restrict__ y, const float* __restrict__ z, float* __restrict__ xn,
             float* __restrict__ yn, float* __restrict__ zn, float* __restrict__ dx, float* __restrict__ dy, float* __restrict__ dz)
         {
+            const int bs = kBS ? kBS : bs_arg;   // 8^3 bricks: index math folded at compile time
             const int64_t work = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
             if (work >= int64_t(nbricks) * bs * bs * bs) return;
             CellCtx c;
@@ -707,10 +717,12 @@ namespace pcfd
         }
 
         // ---------------------------------------------------------------- reconstruction
-        __global__ void reconstruct_struct_kernel(const int* __restrict__ brick_list, int nbricks, int bs, const int* __restrict__ brick_level,
+        template <int kBS>
+        __global__ void reconstruct_struct_kernel(const int* __restrict__ brick_list, int nbricks, int bs_arg, const int* __restrict__ brick_level,
             const int* __restrict__ nbr, const double* __restrict__ level_h, const uint8_t* __restrict__ code,
             const float* __restrict__ x, const float* __restrict__ y, const float* __restrict__ z, float* u, float* v, float* w)
         {
+            const int bs = kBS ? kBS : bs_arg;   // 8^3 bricks: index math folded at compile time
             const int64_t work = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
             if (work >= int64_t(nbricks) * bs * bs * bs) return;
             CellCtx c;
@@ -784,12 +796,14 @@ namespace pcfd
         }
 
         // ---------------------------------------------------------------- CFL reductions
-        __global__ void __launch_bounds__(256) cfl_struct_kernel(const int* __restrict__ brick_list, int nbricks, int bs,
+        template <int kBS>
+        __global__ void __launch_bounds__(256) cfl_struct_kernel(const int* __restrict__ brick_list, int nbricks, int bs_arg,
             const int* __restrict__ brick_level, const int* __restrict__ nbr, const uint32_t* __restrict__ flags,
             const double* __restrict__ level_h, const uint8_t* __restrict__ code, const float* __restrict__ u,
             const float* __restrict__ v, const float* __restrict__ w, const float* __restrict__ x, const float* __restrict__ y,
             const float* __restrict__ z, int external, float* __restrict__ partial_outflow, float* __restrict__ block_partial)
         {
+            const int bs = kBS ? kBS : bs_arg;   // 8^3 bricks: index math folded at compile time
             __shared__ float shared[8];
             const int64_t work = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
             float vmax = 0.0f, rmax = 0.0f;
@@ -943,7 +957,7 @@ namespace pcfd
     {
         special_gradients(s, m);
         if (s.active_bricks)
-            transport_struct_kernel<<<cell_blocks(s), kThreads, 0, launch_stream(s)>>>(
+            (s.bs == 8 ? transport_struct_kernel<8> : transport_struct_kernel<0>)<<<cell_blocks(s), kThreads, 0, launch_stream(s)>>>(
                 s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr, s.brick_flags, s.d_level_h, m.code, s.u, s.v,
                 s.w, m.x, m.y, m.z, dt, external_aero ? 1 : 0, freestream, s.inflow_slot_of_brick, s.inflow_set ? s.inflow.p : nullptr, m.xn, m.yn, m.zn, m.dx, m.dy, m.dz);
         finish_buffered(s, m, 0, dt);
@@ -955,7 +969,7 @@ namespace pcfd
         if (nu == 0.0f && cs == 0.0f) { m.last_rate = 0; m.last_substeps = 1; return 0; }
         special_gradients(s, m);
         if (s.active_bricks)
-            viscosity_struct_kernel<<<cell_blocks(s), kThreads, 0, launch_stream(s)>>>(
+            (s.bs == 8 ? viscosity_struct_kernel<8> : viscosity_struct_kernel<0>)<<<cell_blocks(s), kThreads, 0, launch_stream(s)>>>(
                 s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr, s.d_level_h, m.code, m.special, m.volume32,
                 m.x, m.y, m.z, nu, cs, m.viscosity);
         if (m.nS)
@@ -965,7 +979,7 @@ namespace pcfd
         const int cb = s.active_bricks ? cell_blocks(s) : 0, db = m.nD ? blocks_for(m.nD) : 0;
         require(cb + db <= int(m.reduce_partial.n), "reduction scratch too small");
         if (cb)
-            rate_struct_kernel<<<cb, 256, 0, launch_stream(s)>>>(s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr,
+            (s.bs == 8 ? rate_struct_kernel<8> : rate_struct_kernel<0>)<<<cb, 256, 0, launch_stream(s)>>>(s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr,
                                                         s.d_level_h, m.code, m.viscosity, m.dx, m.reduce_partial);
         if (db)
             rate_deferred_kernel<<<db, 256, 0, launch_stream(s)>>>(m.nD, m.d_dof, m.d_offset, m.d_edge, s.structured, k, m.viscosity, m.dx,
@@ -979,7 +993,7 @@ namespace pcfd
         for (int sub = 0; sub < m.last_substeps; ++sub)
         {
             if (s.active_bricks)
-                diffuse_struct_kernel<<<cell_blocks(s), kThreads, 0, launch_stream(s)>>>(
+                (s.bs == 8 ? diffuse_struct_kernel<8> : diffuse_struct_kernel<0>)<<<cell_blocks(s), kThreads, 0, launch_stream(s)>>>(
                     s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr, s.d_level_h, m.code, m.viscosity, m.x, m.y,
                     m.z, sub_dt, m.xn, m.yn, m.zn, m.dx, m.dy, m.dz);
             finish_buffered(s, m, 1, sub_dt);
@@ -1014,7 +1028,7 @@ namespace pcfd
             pressure_gradient32_kernel<<<blocks_for(o.gradient_nodes), kThreads, 0, launch_stream(s)>>>(
                 o.gradient_nodes, o.grad_dof, o.grad_offset, o.grad_neighbour, m.p_weight, s.pressure32, m.p_gradient);
         if (s.active_bricks)
-            impulse_struct_kernel<<<cell_blocks(s), kThreads, 0, launch_stream(s)>>>(
+            (s.bs == 8 ? impulse_struct_kernel<8> : impulse_struct_kernel<0>)<<<cell_blocks(s), kThreads, 0, launch_stream(s)>>>(
                 s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr, s.brick_flags, s.d_level_h, m.code, s.pressure32,
                 scale, s.outlet ? 1 : 0, physical ? 1 : 0, m.x, m.y, m.z, m.xn, m.yn, m.zn, m.dx, m.dy, m.dz);
         const CompactArgs k = compact_args(s, m);
@@ -1034,7 +1048,7 @@ namespace pcfd
     {
         special_gradients(s, m);
         if (s.active_bricks)
-            reconstruct_struct_kernel<<<cell_blocks(s), kThreads, 0, launch_stream(s)>>>(s.active_brick_list, s.active_bricks, s.bs, s.brick_level,
+            (s.bs == 8 ? reconstruct_struct_kernel<8> : reconstruct_struct_kernel<0>)<<<cell_blocks(s), kThreads, 0, launch_stream(s)>>>(s.active_brick_list, s.active_bricks, s.bs, s.brick_level,
                                                                                s.brick_nbr, s.d_level_h, m.code, m.x, m.y, m.z, s.u, s.v, s.w);
         if (m.nK)
             reconstruct_compact_kernel<<<blocks_for(m.nK), kThreads, 0, launch_stream(s)>>>(m.nK, compact_args(s, m), m.x, m.y, m.z, s.u, s.v,
@@ -1057,7 +1071,7 @@ namespace pcfd
         const int cb = s.active_bricks ? cell_blocks(s) : 0, db = m.nD ? blocks_for(m.nD) : 0;
         require(2 * (cb + db) <= int(m.reduce_partial.n), "reduction scratch too small");
         if (cb)
-            cfl_struct_kernel<<<cb, 256, 0, launch_stream(s)>>>(s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr,
+            (s.bs == 8 ? cfl_struct_kernel<8> : cfl_struct_kernel<0>)<<<cb, 256, 0, launch_stream(s)>>>(s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr,
                                                        s.brick_flags, s.d_level_h, m.code, s.u, s.v, s.w, m.x, m.y, m.z,
                                                        external_aero ? 1 : 0, m.dx, m.reduce_partial);
         if (db)
