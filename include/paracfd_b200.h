@@ -206,9 +206,9 @@ typedef enum pcfd_mg_cycle {
     PCFD_MG_CYCLE_COMPOSITE = 2      /* composite-grid stages instead of the level-0 lattice: stage k
                                         holds one cell per 2^k-wide block of same-level cells of every
                                         AMR level (Galerkin operators, prolongations weighted 2,
-                                        mg_stage_sweeps sweeps per stage, down to 512 cells): 2.8x
-                                        fewer iterations than the reference cycle on the 4-level 16 M-cell
-                                        wing grid.  Needs 8^3 bricks and the fused fine level; with the
+                                        mg_stage_sweeps Chebyshev steps per stage, an explicit inverse
+                                        on the last stage of at most 512 cells): 3.8x fewer iterations
+                                        than the reference cycle on the 4-level 16 M-cell wing grid.  Needs 8^3 bricks and the fused fine level; with the
                                         FP32 multigrid the stages are float, the fine sweeps stay FP64. */
 } pcfd_mg_cycle;
 
