@@ -208,8 +208,10 @@ typedef enum pcfd_mg_cycle {
                                         AMR level (Galerkin operators, prolongations weighted 2,
                                         mg_stage_sweeps Chebyshev steps per stage, an explicit inverse
                                         on the last stage of at most 512 cells): 3.8x fewer iterations
-                                        than the reference cycle on the 4-level 16 M-cell wing grid.  Needs 8^3 bricks and the fused fine level; with the
-                                        FP32 multigrid the stages are float, the fine sweeps stay FP64. */
+                                        than the reference cycle on the 4-level 16 M-cell wing grid.
+                                        Needs 8^3 bricks and the fused fine level; with the FP32
+                                        multigrid the stages and the fine sweeps are float, the Krylov
+                                        vectors and the operator stay FP64. */
 } pcfd_mg_cycle;
 
 /* AmrGpuSolveResult (amr_pressure.h:337-351), trimmed to what the solver reports. */
