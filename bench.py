@@ -18,6 +18,16 @@ Arms
              (oracle/_ref: its CPU twins of every operator, timed at full size) with the
              projection from the FP64 OpenMP restatement of its solver; see cpu_step_sample.
 Multi-GPU: independent replicas, one per rank (the path has no exchange step).
+
+Solver defaults of the ours arm: the composite multigrid cycle in FP32 (Chebyshev stage
+smoothing, Chebyshev-Richardson fine steps, exact coarsest stage), flexible GMRES with delayed
+CGS2 and no recycled subspace; --mg-cycle reference --mg fp64 --delayed 0 --recycle 0 selects the
+reference's solver configuration.  The line also carries a short learned-preconditioner
+comparison (skip with --no-learned).  Other modes:
+  --learned     the learned-preconditioner measurement (harvest, train, re-solve each step's
+                projection under each preconditioner)
+  --sweep       the batched angle sweep (16 wing instances, 4 concurrent batches)
+  --kernel-only the small per-component command that ncu captures
 """
 from __future__ import annotations
 
