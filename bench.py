@@ -70,6 +70,8 @@ def parse_args():
                     help="composite fine sweeps: r >= 2 = Chebyshev-Richardson steps on [2/r, 2], 1 = damped Jacobi, 0: r = 10")
     ap.add_argument("--delayed", type=int, default=1, choices=(0, 1),
                     help="1: GCRO columns orthogonalised by delayed CGS2 (two passes instead of three); 0: CGS2")
+    ap.add_argument("--stage-fp16", type=int, default=0, choices=(0, 1),
+                    help="1: FP16 storage of the composite stages' coefficients (FP32 multigrid)")
     ap.add_argument("--recycle", type=int, default=-1,
                     help="GCRO recycled pairs kept between solves: 1..3, -1 none (default), 0: the reference's 3")
     ap.add_argument("--block-iterations", type=int, default=0,
@@ -333,7 +335,7 @@ def run_ours(args, ranks: Ranks):
                              gmres_restart=args.restart, mg_stage_sweeps=args.stage_sweeps,
                              mg_block_iterations=args.block_iterations, mg_stage_chebyshev=args.chebyshev,
                              mg_fine_chebyshev=args.fine_chebyshev, gmres_delayed=args.delayed,
-                             gmres_recycle=args.recycle)
+                             gmres_recycle=args.recycle, mg_stage_fp16=args.stage_fp16)
     system.configure(speed=spec.speed, **spec.case)
     slots = system.inflow_layout()
     faces = len(slots) * spec.brick_size ** 2
@@ -426,6 +428,7 @@ def run_ours(args, ranks: Ranks):
                        fine_smoother="jacobi" if args.fine_chebyshev == 1 else f"chebyshev-richardson 2/{args.fine_chebyshev or 10}",
                        orthogonalisation="delayed CGS2" if args.delayed else "CGS2",
                        recycled_pairs=3 if args.recycle == 0 else max(args.recycle, 0),
+                       stage_coefficients="fp16" if args.stage_fp16 else args.mg,
                        parallelism=f"replicas{n}",
                        l2="inputs larger than L2"),
         "projection_ms": round(statistics.mean(s["projection_ms"] for s in stats), 3),
@@ -484,7 +487,7 @@ def run_kernel_only(args):
                              gmres_restart=args.restart, mg_stage_sweeps=args.stage_sweeps,
                              mg_block_iterations=args.block_iterations, mg_stage_chebyshev=args.chebyshev,
                              mg_fine_chebyshev=args.fine_chebyshev, gmres_delayed=args.delayed,
-                             gmres_recycle=args.recycle)
+                             gmres_recycle=args.recycle, mg_stage_fp16=args.stage_fp16)
     ms = system.time_kernel(args.kernel_only, args.kernel_iterations)
     line = {"kernel_only": args.kernel_only, "workload": args.workload, "ms_per_launch": ms,
             "iterations": args.kernel_iterations, "launches": system.launch_count()}
@@ -693,7 +696,7 @@ def run_sweep(args, ranks: Ranks):
         systems = [CompositeSystem(b.topology, MG_FP32, device=ranks.local, mg_cycle=MG_CYCLE_COMPOSITE,
                                    mg_stage_sweeps=args.stage_sweeps, mg_stage_chebyshev=args.chebyshev,
                                    mg_fine_chebyshev=args.fine_chebyshev, gmres_delayed=args.delayed,
-                             gmres_recycle=args.recycle) for b in builts]
+                             gmres_recycle=args.recycle, mg_stage_fp16=args.stage_fp16) for b in builts]
         for sp, sy in zip(batch, systems):
             sy.configure(speed=sp.speed, **sp.case)
             sy.initialize()

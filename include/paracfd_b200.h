@@ -190,6 +190,10 @@ typedef struct pcfd_options {
                                         (three passes) */
     int32_t gmres_recycle;           /* recycled (U, C = A U) pairs kept between solves: 1..3; -1: none;
                                         0: the reference's 3 */
+    int32_t mg_stage_fp16;           /* 1: with the composite cycle and the FP32 multigrid, the stage
+                                        matrices (all but the coarsest) store their off-diagonal
+                                        coefficients in FP16; vectors, diagonals and sums stay FP32 or
+                                        wider.  0: FP32 */
 } pcfd_options;
 
 /* Coarse-correction weighting of the multigrid cycle.  The aggregation coarse operators are

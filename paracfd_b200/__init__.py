@@ -84,12 +84,12 @@ class CompositeSystem:
                  momentum_min_volume_fraction: float = 0.0, fused_smoother: bool = True,
                  mg_cycle: int = 0, gmres_restart: int = 0, mg_stage_sweeps: int = 0, mg_block_iterations: int = 0,
                  mg_stage_chebyshev: int = 0, mg_fine_chebyshev: int = 0, gmres_delayed: int = 0,
-                 gmres_recycle: int = 0):
+                 gmres_recycle: int = 0, mg_stage_fp16: int = 0):
         self._lib = capi.load()
         self._topology = topology   # keep the caller's arrays alive during creation
         opts = Options(mg_precision, device, None, momentum_min_volume_fraction, 0 if fused_smoother else 1, mg_cycle,
                        gmres_restart, mg_stage_sweeps, mg_block_iterations, mg_stage_chebyshev, mg_fine_chebyshev,
-                       gmres_delayed, gmres_recycle)
+                       gmres_delayed, gmres_recycle, mg_stage_fp16)
         handle = C.c_void_p()
         check(self._lib.pcfd_system_create(C.byref(topology), C.byref(opts), C.byref(handle)))
         self.handle = handle

@@ -84,7 +84,7 @@ class Options(C.Structure):
                 ("momentum_min_volume_fraction", C.c_double), ("disable_fused_smoother", C.c_int32),
                 ("mg_cycle", C.c_int32), ("gmres_restart", C.c_int32), ("mg_stage_sweeps", C.c_int32),
                 ("mg_block_iterations", C.c_int32), ("mg_stage_chebyshev", C.c_int32), ("mg_fine_chebyshev", C.c_int32),
-                ("gmres_delayed", C.c_int32), ("gmres_recycle", C.c_int32)]
+                ("gmres_delayed", C.c_int32), ("gmres_recycle", C.c_int32), ("mg_stage_fp16", C.c_int32)]
 
 
 class SolveResult(C.Structure):

@@ -209,6 +209,11 @@ namespace pcfd
                 require(options->mg_stage_sweeps > 0 && options->mg_stage_sweeps <= 16, "mg_stage_sweeps must be 0..16");
                 s.mg_stage_sweeps = options->mg_stage_sweeps;
             }
+            if (options && options->mg_stage_fp16)
+            {
+                require(options->mg_stage_fp16 == 1, "mg_stage_fp16 must be 0 or 1");
+                s.mg_stage_fp16 = 1;
+            }
             if (options && options->gmres_recycle)
             {
                 require(options->gmres_recycle >= -1 && options->gmres_recycle <= System::recycle_capacity, "gmres_recycle must be -1..3");

@@ -107,6 +107,7 @@ namespace pcfd
         DBuf<int> row_offset, neighbour, aggregate, restrict_offset, restrict_dof;
         DBuf<T> coefficient, diagonal, rhs, x, temporary, residual;
         DBuf<T> inverse;                        // coarsest composite stage: explicit inverse [cells][cells] or empty
+        DBuf<uint16_t> coefficient16;           // FP16 copy of the coefficients the kernels read instead (or empty)
         double prolong = 1.0;                   // weight of the next level's correction added here
         int sweeps = 2;                         // smoothing steps before and after the coarse correction
         int chebyshev = 0;                      // 0: damped Jacobi; r >= 2: Chebyshev on [2 / r, 2]
@@ -177,6 +178,7 @@ namespace pcfd
         int mg_stage_sweeps = 6;                                 // composite-stage sweeps (pcfd_options)
         int mg_block_iterations = 0;                             // composite cycle: brick block pre-smoother (pcfd_options)
         int mg_stage_chebyshev = 30;                             // composite stages: Chebyshev ratio, 0 = Jacobi (pcfd_options)
+        int mg_stage_fp16 = 0;                                   // composite stages: FP16 coefficients (pcfd_options)
         int mg_fine_chebyshev = 10;                              // composite fine sweeps: Chebyshev-Richardson ratio, 0 = Jacobi
         cudaStream_t stream = nullptr;
         bool own_stream = false;

@@ -13,6 +13,10 @@
 // when WLS non-orthogonal corrections are present.
 #include "pcfd_internal.h"
 
+#include <cuda_fp16.h>
+
+#include <cstring>
+
 #include <algorithm>
 #include <array>
 #include <cmath>
@@ -551,6 +555,18 @@ namespace pcfd
                 s.inter32[k].chebyshev = s.mg_stage_chebyshev;
             }
             if (!inverse.empty()) s.inter32.back().inverse.upload(std::vector<float>(inverse.begin(), inverse.end()));
+            if (s.mg_stage_fp16)
+                // FP16 storage of the stage coefficients (the coarsest keeps FP32 for its own sweeps)
+                for (size_t k = 0; k + 1 < stages.size(); ++k)
+                {
+                    std::vector<uint16_t> bits(stages[k].coefficient.size());
+                    for (size_t e = 0; e < bits.size(); ++e)
+                    {
+                        const __half hv = __float2half_rn(float(stages[k].coefficient[e]));
+                        std::memcpy(&bits[e], &hv, sizeof(uint16_t));
+                    }
+                    s.inter32[k].coefficient16.upload(bits);
+                }
         }
         else
         {
@@ -595,15 +611,20 @@ namespace pcfd
             for (int q = offset[c]; q < offset[c + 1]; ++q) sum += r[dof[q]] - Ax[dof[q]];
             coarse_rhs[c] = T(sum);
         }
-        template <class T>
+        // CSR coefficients as stored: FP64, FP32 or (mg_stage_fp16) FP16
+        __device__ inline double coefficient_value(double c) { return c; }
+        __device__ inline double coefficient_value(float c) { return double(c); }
+        __device__ inline double coefficient_value(__half c) { return double(__half2float(c)); }
+
+        template <class T, class TK = T>
         __global__ void algebraic_jacobi_kernel(const T* rhs, const T* x, T* next, const int* row_offset, const int* neighbour,
-                                                const T* coefficient, const T* diag, int cells, T omega)
+                                                const TK* coefficient, const T* diag, int cells, T omega)
         {
             const int q = blockIdx.x * blockDim.x + threadIdx.x;
             if (q >= cells) return;
             if (!(diag[q] > T(0))) { next[q] = T(0); return; }
             double Ax = double(diag[q]) * double(x[q]);
-            for (int e = row_offset[q]; e < row_offset[q + 1]; ++e) Ax -= double(coefficient[e]) * double(x[neighbour[e]]);
+            for (int e = row_offset[q]; e < row_offset[q + 1]; ++e) Ax -= coefficient_value(coefficient[e]) * double(x[neighbour[e]]);
             next[q] = x[q] + omega * T((double(rhs[q]) - Ax) / double(diag[q]));
         }
         // x = inverse * rhs on a coarsest level (one warp per row, FP64 accumulation)
@@ -620,29 +641,29 @@ namespace pcfd
 
         // One Chebyshev step of a CSR level, fused: r = rhs - A x, d = c1 d + c2 D^-1 r (first step:
         // d = c2 D^-1 r), next = x + d
-        template <class T>
+        template <class T, class TK = T>
         __global__ void algebraic_chebyshev_kernel(const T* rhs, const T* x, T* next, T* d, const int* row_offset, const int* neighbour,
-                                                   const T* coefficient, const T* diag, int cells, T c1, T c2, int first)
+                                                   const TK* coefficient, const T* diag, int cells, T c1, T c2, int first)
         {
             const int q = blockIdx.x * blockDim.x + threadIdx.x;
             if (q >= cells) return;
             if (!(diag[q] > T(0))) { next[q] = T(0); d[q] = T(0); return; }
             double Ax = double(diag[q]) * double(x[q]);
-            for (int e = row_offset[q]; e < row_offset[q + 1]; ++e) Ax -= double(coefficient[e]) * double(x[neighbour[e]]);
+            for (int e = row_offset[q]; e < row_offset[q + 1]; ++e) Ax -= coefficient_value(coefficient[e]) * double(x[neighbour[e]]);
             const T step = c2 * T((double(rhs[q]) - Ax) / double(diag[q]));
             const T dn = first ? step : c1 * d[q] + step;
             d[q] = dn;
             next[q] = x[q] + dn;
         }
-        template <class T>
+        template <class T, class TK = T>
         __global__ void algebraic_residual_kernel(const T* rhs, const T* x, T* residual, const int* row_offset, const int* neighbour,
-                                                  const T* coefficient, const T* diag, int cells)
+                                                  const TK* coefficient, const T* diag, int cells)
         {
             const int q = blockIdx.x * blockDim.x + threadIdx.x;
             if (q >= cells) return;
             if (!(diag[q] > T(0))) { residual[q] = T(0); return; }
             double Ax = double(diag[q]) * double(x[q]);
-            for (int e = row_offset[q]; e < row_offset[q + 1]; ++e) Ax -= double(coefficient[e]) * double(x[neighbour[e]]);
+            for (int e = row_offset[q]; e < row_offset[q + 1]; ++e) Ax -= coefficient_value(coefficient[e]) * double(x[neighbour[e]]);
             residual[q] = T(double(rhs[q]) - Ax);
         }
         template <class T>
@@ -721,18 +742,29 @@ namespace pcfd
                             c2 = 2.0 * next / delta;
                             rho = next;
                         }
-                        algebraic_chebyshev_kernel<T><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
-                            level.rhs, level.x, level.temporary, level.residual, level.row_offset, level.neighbour, level.coefficient,
-                            level.diagonal, level.cells, T(c1), T(c2), sweep == 0 ? 1 : 0);
+                        if (level.coefficient16.p)
+                            algebraic_chebyshev_kernel<T, __half><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
+                                level.rhs, level.x, level.temporary, level.residual, level.row_offset, level.neighbour,
+                                reinterpret_cast<const __half*>(level.coefficient16.p), level.diagonal, level.cells, T(c1), T(c2),
+                                sweep == 0 ? 1 : 0);
+                        else
+                            algebraic_chebyshev_kernel<T, T><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
+                                level.rhs, level.x, level.temporary, level.residual, level.row_offset, level.neighbour, level.coefficient,
+                                level.diagonal, level.cells, T(c1), T(c2), sweep == 0 ? 1 : 0);
                         std::swap(level.x.p, level.temporary.p);
                     }
                     return;
                 }
                 for (int sweep = 0; sweep < sweeps; ++sweep)
                 {
-                    algebraic_jacobi_kernel<T><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
-                        level.rhs, level.x, level.temporary, level.row_offset, level.neighbour, level.coefficient,
-                        level.diagonal, level.cells, omega);
+                    if (level.coefficient16.p)
+                        algebraic_jacobi_kernel<T, __half><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
+                            level.rhs, level.x, level.temporary, level.row_offset, level.neighbour,
+                            reinterpret_cast<const __half*>(level.coefficient16.p), level.diagonal, level.cells, omega);
+                    else
+                        algebraic_jacobi_kernel<T, T><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
+                            level.rhs, level.x, level.temporary, level.row_offset, level.neighbour, level.coefficient,
+                            level.diagonal, level.cells, omega);
                     std::swap(level.x.p, level.temporary.p);
                 }
             };
@@ -749,8 +781,13 @@ namespace pcfd
                 return;
             }
             smooth(level.sweeps);
-            algebraic_residual_kernel<T><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
-                level.rhs, level.x, level.residual, level.row_offset, level.neighbour, level.coefficient, level.diagonal, level.cells);
+            if (level.coefficient16.p)
+                algebraic_residual_kernel<T, __half><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
+                    level.rhs, level.x, level.residual, level.row_offset, level.neighbour,
+                    reinterpret_cast<const __half*>(level.coefficient16.p), level.diagonal, level.cells);
+            else
+                algebraic_residual_kernel<T, T><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
+                    level.rhs, level.x, level.residual, level.row_offset, level.neighbour, level.coefficient, level.diagonal, level.cells);
             MgLevel<T>& coarse = *chain[index + 1];
             restrict_gather_kernel<T><<<blocks_for(coarse.cells), kThreads, 0, launch_stream(s)>>>(
                 level.restrict_offset, level.restrict_dof, level.residual, coarse.cells, coarse.rhs);

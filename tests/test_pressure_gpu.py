@@ -124,6 +124,20 @@ def test_delayed_orthogonalisation_reaches_tolerance(case, cycle):
     assert out[1] <= out[0] + 2, out
 
 
+def test_fp16_stage_coefficients_reach_tolerance(case):
+    """The composite stages with FP16 coefficients (FP32 multigrid) still precondition a solve
+    to the FP64 true residual of the reference operator."""
+    rc, _ = case
+    rng = np.random.default_rng(8)
+    b = rng.standard_normal(rc.n) * rc.active
+    act = rc.active.astype(bool)
+    with CompositeSystem(rc.topology, mg_precision=MG_FP32, mg_cycle=2, mg_stage_fp16=1) as s:
+        x, res = s.solve(b, 1e-8, 600)
+    assert res["converged"], res
+    true = np.linalg.norm((b - rc.apply(x))[act]) / np.linalg.norm(b)
+    assert true <= 1e-8 * 1.01, (true, res)
+
+
 def test_fused_preconditioner_matches_separate_launches_and_oracle(case):
     """The brick-fused fine level runs the same Jacobi sweeps; only the aggregate restriction
     sums in another order, so the result agrees with the separate-launch path and with the CPU
