@@ -19,10 +19,10 @@ Arms
              projection from the FP64 OpenMP restatement of its solver; see cpu_step_sample.
 Multi-GPU: independent replicas, one per rank (the path has no exchange step).
 
-Solver defaults of the ours arm: the composite multigrid cycle in FP32 (Chebyshev stage
-smoothing, Chebyshev-Richardson fine steps, exact coarsest stage), flexible GMRES with delayed
-CGS2 and no recycled subspace; --mg-cycle reference --mg fp64 --delayed 0 --recycle 0 selects the
-reference's solver configuration.  The line also carries a short learned-preconditioner
+Solver defaults of the ours arm: the composite multigrid cycle in FP32 with FP16 stage
+coefficients (Chebyshev stage smoothing, Chebyshev-Richardson fine steps, exact coarsest stage),
+flexible GMRES with delayed CGS2 and no recycled subspace; --mg-cycle reference --mg fp64
+--delayed 0 --recycle 0 selects the reference's solver configuration.  The line also carries a short learned-preconditioner
 comparison (skip with --no-learned).  Other modes:
   --learned     the learned-preconditioner measurement (harvest, train, re-solve each step's
                 projection under each preconditioner)
@@ -70,8 +70,8 @@ def parse_args():
                     help="composite fine sweeps: r >= 2 = Chebyshev-Richardson steps on [2/r, 2], 1 = damped Jacobi, 0: r = 10")
     ap.add_argument("--delayed", type=int, default=1, choices=(0, 1),
                     help="1: GCRO columns orthogonalised by delayed CGS2 (two passes instead of three); 0: CGS2")
-    ap.add_argument("--stage-fp16", type=int, default=0, choices=(0, 1),
-                    help="1: FP16 storage of the composite stages' coefficients (FP32 multigrid)")
+    ap.add_argument("--stage-fp16", type=int, default=1, choices=(0, 1),
+                    help="1: FP16 storage of the composite stages' coefficients (FP32 multigrid); 0: FP32")
     ap.add_argument("--recycle", type=int, default=-1,
                     help="GCRO recycled pairs kept between solves: 1..3, -1 none (default), 0: the reference's 3")
     ap.add_argument("--block-iterations", type=int, default=0,
