@@ -677,18 +677,12 @@ def run_learned(args, ranks: Ranks):
 
 def run_sweep(args, ranks: Ranks):
     """BASELINE config 5 on one GPU: the angle-of-attack sweep as batches of concurrent instances."""
-    import dataclasses
     from concurrent.futures import ThreadPoolExecutor
 
     from paracfd_b200 import MG_CYCLE_COMPOSITE, MG_FP32, CompositeSystem
-    from paracfd_b200.workloads import WORKLOADS
+    from paracfd_b200.workloads import sweep_instances
 
-    rng = np.random.default_rng(20261203)
-    base = WORKLOADS["naca4412_wing"]
-    specs = [dataclasses.replace(base, name=f"naca4412_aoa{a}", aoa=float(a),
-                                 surface_refinement_distance=round(float(rng.uniform(0.03, 0.12)), 4),
-                                 wing_refinement_distance=round(float(rng.uniform(0.2, 0.6)), 4))
-             for a in range(-4, 12)]
+    specs = sweep_instances()
     batches = []
     for first in range(0, len(specs), 4):
         batch = specs[first:first + 4]

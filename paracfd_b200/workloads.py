@@ -79,6 +79,22 @@ WORKLOADS = {
 }
 
 
+def sweep_instances(seed: int = 20261203) -> list:
+    """The batched angle sweep: 16 naca4412_wing instances at AoA -4..11 deg (1 deg steps), each
+    with its surface and wing refinement bands drawn from a seeded uniform distribution
+    (U[0.03, 0.12] m and U[0.2, 0.6] m), so brick counts vary unevenly between instances."""
+    import dataclasses
+
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    base = WORKLOADS["naca4412_wing"]
+    return [dataclasses.replace(base, name=f"naca4412_aoa{a}", aoa=float(a),
+                                surface_refinement_distance=round(float(rng.uniform(0.03, 0.12)), 4),
+                                wing_refinement_distance=round(float(rng.uniform(0.2, 0.6)), 4))
+            for a in range(-4, 12)]
+
+
 def with_aoa(name: str, aoa: float) -> Workload:
     """The named workload at another angle of attack (the learned preconditioner's harvest runs)."""
     from dataclasses import replace
