@@ -51,6 +51,12 @@ struct po_system
     std::vector<double> r, z, d, Ad, tv, corrv, defect;
     std::vector<double> V, Z, RU, RC;     // GCRO bases
     int recycle = 0;
+    // composite cycle (po_set_composite): stages, fine -> stage-1 map, coarsest inverse
+    bool composite = false;
+    int stage_steps = 6, stage_ratio = 30, fine_ratio = 10;
+    std::vector<MgLevel> stages;
+    std::vector<int> fine_map, fine_roff, fine_rdof;
+    std::vector<double> coarse_inverse, fine_res, stage_d;
 };
 
 namespace
@@ -366,8 +372,300 @@ namespace
         jacobi(L, 2);
     }
 
+    // ---- composite cycle (paracfd_b200 solver.cu build_composite, smoother.cu composite_cycle) ----
+    // Stage k merges the level-l structured cells at global cell coordinates g into (l, g >> k);
+    // Galerkin operators of the fine orthogonal couplings (+ outlet and gauge diagonal terms);
+    // stages down to 512 cells; the coarsest solved with its explicit inverse.
+    void build_composite(po_system& s)
+    {
+        const pcfd_topology& t = s.t;
+        const int bs = s.bs, c3 = s.c3, S = s.S;
+        std::vector<int> dof_level(S, -1);
+        std::vector<std::array<int64_t, 3>> g(S);
+        for (int l = 0; l < t.level_count; ++l)
+        {
+            const pcfd_level& lev = t.levels[l];
+            for (int b = 0; b < lev.brick_count; ++b)
+            {
+                if (lev.flags[b] & COVERED) continue;
+                for (int c = 0; c < c3; ++c)
+                {
+                    const int q = lev.level_offset + b * c3 + c;
+                    if (!t.active[q]) continue;
+                    dof_level[q] = l;
+                    g[q] = {int64_t(lev.coord[3 * b]) * bs + c % bs, int64_t(lev.coord[3 * b + 1]) * bs + (c / bs) % bs,
+                            int64_t(lev.coord[3 * b + 2]) * bs + c / (bs * bs)};
+                }
+            }
+        }
+        auto key = [](int m, int64_t x, int64_t y, int64_t z) {
+            return (uint64_t(m) << 60) | (uint64_t(x & 0xfffff) << 40) | (uint64_t(y & 0xfffff) << 20) | uint64_t(z & 0xfffff);
+        };
+        std::vector<std::vector<int>> maps;
+        std::vector<int> cells;
+        for (int k = 1; k <= 16; ++k)
+        {
+            std::vector<int> m(S, -1);
+            std::unordered_map<uint64_t, int> index;
+            for (int q = 0; q < S; ++q)
+            {
+                if (dof_level[q] < 0) continue;
+                const uint64_t kq = key(dof_level[q], g[q][0] >> k, g[q][1] >> k, g[q][2] >> k);
+                auto it = index.find(kq);
+                if (it == index.end()) it = index.emplace(kq, int(index.size())).first;
+                m[q] = it->second;
+            }
+            const int n = int(index.size());
+            if (n == 0 || (!cells.empty() && n >= cells.back())) break;
+            maps.push_back(std::move(m));
+            cells.push_back(n);
+            if (n <= 512) break;
+        }
+        s.stages.assign(maps.size(), MgLevel());
+        for (size_t k = 0; k < maps.size(); ++k)
+        {
+            const std::vector<int>& m = maps[k];
+            MgLevel& L = s.stages[k];
+            L.cells = cells[k];
+            L.diag.assign(L.cells, 0.0);
+            std::unordered_map<uint64_t, double> w;
+            auto add = [&](int a, int b, double c) {
+                if (a < 0 || b < 0 || a == b || !t.active[a] || !t.active[b] || !(c > 0)) return;
+                int ca = m[a], cb = m[b];
+                if (ca < 0 || cb < 0 || ca == cb) return;
+                L.diag[ca] += c;
+                L.diag[cb] += c;
+                if (ca > cb) std::swap(ca, cb);
+                w[(uint64_t(uint32_t(ca)) << 32) | uint32_t(cb)] += c;
+            };
+            for (int l = 0; l < t.level_count; ++l)
+            {
+                const pcfd_level& lev = t.levels[l];
+                for (int brick = 0; brick < lev.brick_count; ++brick)
+                {
+                    if (lev.flags[brick] & COVERED) continue;
+                    for (int c = 0; c < c3; ++c)
+                    {
+                        const int a = lev.level_offset + brick * c3 + c;
+                        if (!t.active[a]) continue;
+                        const int ijk[3] = {c % bs, (c / bs) % bs, c / (bs * bs)};
+                        for (int axis = 0; axis < 3; ++axis)
+                        {
+                            if (t.cut_face_mask[a] & (1u << axis)) continue;
+                            int q[3] = {ijk[0], ijk[1], ijk[2]}, b = -1;
+                            if (++q[axis] < bs) b = lev.level_offset + brick * c3 + (q[2] * bs + q[1]) * bs + q[0];
+                            else
+                            {
+                                const int nb = lev.neighbors[brick * 6 + 2 * axis + 1];
+                                if (nb >= 0 && !(lev.flags[nb] & COVERED)) { q[axis] = 0; b = lev.level_offset + nb * c3 + (q[2] * bs + q[1]) * bs + q[0]; }
+                            }
+                            add(a, b, lev.h);
+                        }
+                        if (t.pressure_outlet_xmax && (lev.flags[brick] & XMAX) && ijk[0] == bs - 1 && m[a] >= 0) L.diag[m[a]] += 2.0 * lev.h;
+                    }
+                }
+            }
+            for (int e = 0; e < t.coarse_fine.count; ++e) add(t.coarse_fine.coarse_dof[e], t.coarse_fine.fine_dof[e], t.coarse_fine.open_area[e] * factor_of(t.coarse_fine, e));
+            for (int e = 0; e < t.embedded.count; ++e) add(t.embedded.coarse_dof[e], t.embedded.fine_dof[e], t.embedded.open_area[e] * factor_of(t.embedded, e));
+            for (int e = 0; e < t.regular.count; ++e) add(t.regular.lower_dof[e], t.regular.upper_dof[e], t.regular.open_area[e] * t.regular.two_point_delta[e]);
+            for (int gg = 0; gg < t.gauge_count; ++gg)
+            {
+                const int q = t.gauge_dof[gg];
+                if (t.active[q] && m[q] >= 0) L.diag[m[q]] += t.gauge_coefficient[gg];
+            }
+            for (const auto& it : w) L.edges.push_back({int(it.first >> 32), int(it.first & 0xffffffffu), it.second});
+            std::sort(L.edges.begin(), L.edges.end(), [](const Edge& x, const Edge& y) { return x.a < y.a || (x.a == y.a && x.b < y.b); });
+        }
+        for (size_t k = 0; k < s.stages.size(); ++k)
+        {
+            MgLevel& L = s.stages[k];
+            if (k + 1 < s.stages.size())
+            {
+                L.aggregate.assign(L.cells, -1);
+                for (int q = 0; q < S; ++q) if (maps[k][q] >= 0) L.aggregate[maps[k][q]] = maps[k + 1][q];
+                const int next = cells[k + 1];
+                L.roff.assign(size_t(next) + 1, 0);
+                for (int c = 0; c < L.cells; ++c) if (L.aggregate[c] >= 0) ++L.roff[L.aggregate[c] + 1];
+                for (int c = 0; c < next; ++c) L.roff[c + 1] += L.roff[c];
+                L.rdof.resize(L.roff.back());
+                std::vector<int> cur = L.roff;
+                for (int c = 0; c < L.cells; ++c) if (L.aggregate[c] >= 0) L.rdof[cur[L.aggregate[c]]++] = c;
+            }
+            finalize(L);
+        }
+        s.fine_map = maps.front();
+        const int n1 = cells.front();
+        s.fine_roff.assign(size_t(n1) + 1, 0);
+        for (int q = 0; q < S; ++q) if (s.fine_map[q] >= 0) ++s.fine_roff[s.fine_map[q] + 1];
+        for (int c = 0; c < n1; ++c) s.fine_roff[c + 1] += s.fine_roff[c];
+        s.fine_rdof.resize(s.fine_roff.back());
+        {
+            std::vector<int> cur = s.fine_roff;
+            for (int q = 0; q < S; ++q) if (s.fine_map[q] >= 0) s.fine_rdof[cur[s.fine_map[q]]++] = q;
+        }
+        // explicit inverse of the coarsest stage over its cells with a positive diagonal
+        s.coarse_inverse.clear();
+        const MgLevel& C = s.stages.back();
+        if (C.cells <= 512)
+        {
+            const int n = C.cells;
+            std::vector<int> live, idx(n, -1);
+            for (int q = 0; q < n; ++q) if (C.diag[q] > 0) { idx[q] = int(live.size()); live.push_back(q); }
+            const int m = int(live.size());
+            std::vector<double> a(size_t(m) * m, 0.0), inv(size_t(m) * m, 0.0);
+            double scale = 0;
+            for (int i = 0; i < m; ++i) { a[size_t(i) * m + i] = C.diag[live[i]]; inv[size_t(i) * m + i] = 1; scale = std::max(scale, C.diag[live[i]]); }
+            for (const Edge& e : C.edges)
+            {
+                const int i = idx[e.a], j = idx[e.b];
+                if (i < 0 || j < 0) continue;
+                a[size_t(i) * m + j] -= e.c;
+                a[size_t(j) * m + i] -= e.c;
+            }
+            bool ok = m > 0;
+            for (int c = 0; c < m && ok; ++c)
+            {
+                int p = c;
+                for (int r = c + 1; r < m; ++r) if (std::abs(a[size_t(r) * m + c]) > std::abs(a[size_t(p) * m + c])) p = r;
+                if (!(std::abs(a[size_t(p) * m + c]) > 1e-12 * scale)) { ok = false; break; }
+                if (p != c)
+                    for (int j = 0; j < m; ++j) { std::swap(a[size_t(p) * m + j], a[size_t(c) * m + j]); std::swap(inv[size_t(p) * m + j], inv[size_t(c) * m + j]); }
+                const double d = 1.0 / a[size_t(c) * m + c];
+                for (int j = 0; j < m; ++j) { a[size_t(c) * m + j] *= d; inv[size_t(c) * m + j] *= d; }
+                for (int r = 0; r < m; ++r)
+                {
+                    if (r == c) continue;
+                    const double f = a[size_t(r) * m + c];
+                    if (f == 0.0) continue;
+                    for (int j = 0; j < m; ++j) { a[size_t(r) * m + j] -= f * a[size_t(c) * m + j]; inv[size_t(r) * m + j] -= f * inv[size_t(c) * m + j]; }
+                }
+            }
+            if (ok)
+            {
+                s.coarse_inverse.assign(size_t(n) * n, 0.0);
+                for (int i = 0; i < m; ++i)
+                    for (int j = 0; j < m; ++j) s.coarse_inverse[size_t(live[i]) * n + live[j]] = inv[size_t(i) * m + j];
+            }
+        }
+        s.fine_res.assign(S, 0.0);
+        s.composite = true;
+    }
+
+    // stage smoothing: damped Jacobi (ratio < 2) or Chebyshev of D^-1 A on [2 / ratio, 2]
+    void stage_smooth(po_system& s, MgLevel& L, int steps)
+    {
+        if (s.stage_ratio < 2) { jacobi(L, steps); return; }
+        const double hi = 2.0, lo = hi / s.stage_ratio, theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
+        double rho = 1.0 / sigma;
+        s.stage_d.assign(L.cells, 0.0);
+        for (int k = 0; k < steps; ++k)
+        {
+            double c1 = 0.0, c2 = 1.0 / theta;
+            if (k)
+            {
+                const double next = 1.0 / (2.0 * sigma - rho);
+                c1 = next * rho;
+                c2 = 2.0 * next / delta;
+                rho = next;
+            }
+#pragma omp parallel for schedule(static)
+            for (int q = 0; q < L.cells; ++q)
+            {
+                if (!(L.diag[q] > 0)) { L.tmp[q] = 0; s.stage_d[q] = 0; continue; }
+                double Ax = L.diag[q] * L.x[q];
+                for (int e = L.row[q]; e < L.row[q + 1]; ++e) Ax -= L.coef[e] * L.x[L.nbr[e]];
+                const double step = c2 * ((L.rhs[q] - Ax) / L.diag[q]);
+                const double dn = k ? c1 * s.stage_d[q] + step : step;
+                s.stage_d[q] = dn;
+                L.tmp[q] = L.x[q] + dn;
+            }
+            std::swap(L.x, L.tmp);
+        }
+    }
+
+    void stage_cycle(po_system& s, int index)
+    {
+        MgLevel& L = s.stages[index];
+        if (index + 1 == int(s.stages.size()))
+        {
+            if (!s.coarse_inverse.empty())
+            {
+                const int n = L.cells;
+#pragma omp parallel for schedule(static)
+                for (int i = 0; i < n; ++i)
+                {
+                    double v = 0;
+                    for (int j = 0; j < n; ++j) v += s.coarse_inverse[size_t(i) * n + j] * L.rhs[j];
+                    L.x[i] = v;
+                }
+            }
+            else jacobi(L, 96);
+            return;
+        }
+        stage_smooth(s, L, s.stage_steps);
+#pragma omp parallel for schedule(static)
+        for (int q = 0; q < L.cells; ++q)
+        {
+            if (!(L.diag[q] > 0)) { L.res[q] = 0; continue; }
+            double Ax = L.diag[q] * L.x[q];
+            for (int e = L.row[q]; e < L.row[q + 1]; ++e) Ax -= L.coef[e] * L.x[L.nbr[e]];
+            L.res[q] = L.rhs[q] - Ax;
+        }
+        MgLevel& C = s.stages[index + 1];
+#pragma omp parallel for schedule(static)
+        for (int c = 0; c < C.cells; ++c)
+        {
+            double v = 0;
+            for (int q = L.roff[c]; q < L.roff[c + 1]; ++q) v += L.res[L.rdof[q]];
+            C.rhs[c] = v;
+        }
+        std::fill(C.x.begin(), C.x.end(), 0.0);
+        stage_cycle(s, index + 1);
+#pragma omp parallel for schedule(static)
+        for (int q = 0; q < L.cells; ++q) if (L.aggregate[q] >= 0) L.x[q] += 2.0 * C.x[L.aggregate[q]];
+        stage_smooth(s, L, s.stage_steps);
+    }
+
+    // fine sweeps with the Chebyshev-Richardson step sizes of [2 / fine_ratio, 2] (or w = 2/3),
+    // two before and two after the stage correction, which is prolonged with weight 2
+    void precondition_composite(po_system& s, const double* r, double* z)
+    {
+        const uint8_t* act = s.t.active;
+        double w[4] = {2.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0};
+        if (s.fine_ratio >= 2)
+        {
+            const double hi = 2.0, lo = hi / s.fine_ratio, theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo);
+            const double steps[2] = {1.0 / (theta + delta * std::sqrt(0.5)), 1.0 / (theta - delta * std::sqrt(0.5))};
+            for (int k = 0; k < 4; ++k) w[k] = steps[k & 1];
+        }
+        auto sweep = [&](double omega) {
+            apply(s, z, s.tv.data(), true);
+#pragma omp parallel for schedule(static)
+            for (int q = 0; q < s.S; ++q) if (act[q] && s.diagonal[q] > 0) z[q] += omega * (r[q] - s.tv[q]) / s.diagonal[q];
+        };
+#pragma omp parallel for schedule(static)
+        for (int q = 0; q < s.S; ++q) z[q] = act[q] && s.diagonal[q] > 0 ? w[0] * r[q] / s.diagonal[q] : 0.0;
+        sweep(w[1]);
+        apply(s, z, s.tv.data(), true);
+        MgLevel& first = s.stages.front();
+#pragma omp parallel for schedule(static)
+        for (int c = 0; c < first.cells; ++c)
+        {
+            double v = 0;
+            for (int q = s.fine_roff[c]; q < s.fine_roff[c + 1]; ++q) v += r[s.fine_rdof[q]] - s.tv[s.fine_rdof[q]];
+            first.rhs[c] = v;
+        }
+        std::fill(first.x.begin(), first.x.end(), 0.0);
+        stage_cycle(s, 0);
+#pragma omp parallel for schedule(static)
+        for (int q = 0; q < s.S; ++q) if (act[q] && s.fine_map[q] >= 0) z[q] += 2.0 * first.x[s.fine_map[q]];
+        sweep(w[2]);
+        sweep(w[3]);
+    }
+
     void precondition(po_system& s, const double* r, double* z)
     {
+        if (s.composite) { precondition_composite(s, r, z); return; }
         const double omega = 2.0 / 3.0;
         const uint8_t* act = s.t.active;
         auto jcorr = [&]() {
@@ -760,6 +1058,14 @@ void po_destroy(po_system* s) { delete s; }
 void po_apply(po_system* s, const double* p, double* out, int orthogonal) { apply(*s, p, out, orthogonal != 0); }
 void po_diagonal(po_system* s, double* d) { std::copy(s->diagonal.begin(), s->diagonal.end(), d); }
 void po_precondition(po_system* s, const double* r, double* z) { precondition(*s, r, z); }
+
+void po_set_composite(po_system* s, int steps, int stage_ratio, int fine_ratio)
+{
+    s->stage_steps = steps > 0 ? steps : 6;
+    s->stage_ratio = stage_ratio;
+    s->fine_ratio = fine_ratio;
+    build_composite(*s);
+}
 
 int po_solve(po_system* s, double* x, const double* b, double tol, int maxit, int warm, double* out)
 {

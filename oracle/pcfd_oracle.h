@@ -25,6 +25,11 @@ int po_threads(void);
 void po_apply(po_system* s, const double* p, double* out, int orthogonal);
 void po_diagonal(po_system* s, double* diagonal);
 void po_precondition(po_system* s, const double* r, double* z);
+/* From now on po_precondition / po_solve use the composite cycle of paracfd_b200 (its
+ * PCFD_MG_CYCLE_COMPOSITE in FP64): `steps` smoothing steps per stage (0: 6), Chebyshev stage
+ * smoothing on [2 / stage_ratio, 2] (< 2: damped Jacobi), fine Chebyshev-Richardson steps on
+ * [2 / fine_ratio, 2] (< 2: w = 2/3), an explicit inverse on a coarsest stage of <= 512 cells. */
+void po_set_composite(po_system* s, int steps, int stage_ratio, int fine_ratio);
 /* returns converged; out[0] relative residual, out[1] iterations, out[2] preconditioner applications */
 int po_solve(po_system* s, double* x, const double* b, double tolerance, int max_iterations, int warm_start,
              double* out3);

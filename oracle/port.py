@@ -33,6 +33,7 @@ def lib():
         L.po_apply.argtypes = [vp, f64p, f64p, C.c_int]
         L.po_diagonal.argtypes = [vp, f64p]
         L.po_precondition.argtypes = [vp, f64p, f64p]
+        L.po_set_composite.argtypes = [vp, C.c_int, C.c_int, C.c_int]
         L.po_solve.restype = C.c_int
         L.po_solve.argtypes = [vp, f64p, f64p, C.c_double, C.c_int, C.c_int, f64p]
         L.po_divergence.argtypes = [vp, f32p, f32p, f32p, f32p, f64p, f64p]
@@ -71,6 +72,10 @@ class PortSystem:
         out = np.zeros(self.n)
         lib().po_diagonal(self.handle, ptr(out, C.c_double))
         return out
+
+    def set_composite(self, steps: int = 6, stage_ratio: int = 30, fine_ratio: int = 10):
+        """Switch to the composite cycle (FP64 restatement of paracfd_b200's)."""
+        lib().po_set_composite(self.handle, steps, stage_ratio, fine_ratio)
 
     def precondition(self, r):
         out = np.zeros(self.n)
