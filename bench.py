@@ -2,9 +2,14 @@
 """Time-step throughput of the ParaCFD per-timestep solver path on B200.
 
 Workload: the 4-level ~16 M leaf-cell paraglider case (``paraglider16m``, FP32 flow state, FP64
-pressure, projection to 1e-8 relative residual, surface loads integrated every step).  A step
-is one ``pcfd_core_step`` (CFL -> MUSCL transport -> Smagorinsky diffusion -> smooth wall ->
-flux reconstruction -> boundaries -> projection -> pressure traction) plus ``pcfd_core_loads``.
+pressure, projection to 1e-8 relative residual, surface loads integrated every step) on its
+cut-cell grid.  The grid (brick hierarchy, cut-cell embedded-boundary atlas, composite pressure
+system) is the reference's own host preprocessing of the closed wing surface, compiled from its
+sources (oracle/_ref); it reaches this library through ``pcfd_topology``, the drop-in boundary,
+before any timed region.  ``--grid staircase`` uses this library's own solid-cell builder
+(``pcfd_topology_build``) instead.  A step is one ``pcfd_core_step`` (CFL -> MUSCL transport ->
+Smagorinsky diffusion -> smooth wall -> flux reconstruction -> boundaries -> projection ->
+pressure traction) plus ``pcfd_core_loads``.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -13,17 +18,23 @@ Arms
              system stream, max over ranks); e2e = steps/s over K more steps through the public
              API with host buffers: per step the X-min inflow profile is copied from pinned host
              memory and the loads are read back.  Every resident vector (19 M-DOF FP64 pressure
-             vectors, 0.2 GB each) is larger than the 126 MB L2.
-  reference  the reference's own host implementation of the step on this machine's cores
-             (oracle/_ref: its CPU twins of every operator, timed at full size) with the
-             projection from the FP64 OpenMP restatement of its solver; see cpu_step_sample.
+             vectors, 0.16 GB each) is larger than the 126 MB L2.
+  reference  whole time steps of the reference's host implementation on this machine's cores:
+             its CPU twins of every operator (oracle/_ref, single-threaded as written) in
+             ExternalAeroCore::step's order, with the projection solved to 1e-8 by the FP64
+             OpenMP restatement of its solver (the reference has no CPU solver).  A CPU step of
+             the 16 M-cell grid takes minutes, so each timed step is a whole step of the same
+             wing on the 1.1 M-cell grid (paraglider1m) and the value is scaled to 16 M cells by
+             the cell count (see CpuStepper).  Beside it, the reference's own sm_100a build
+             (its device classes in ExternalAeroCore's step sequence) runs K whole steps of the
+             full workload: ``reference_sm100a``.  This arm never loads libparacfd_b200.so.
 Multi-GPU: independent replicas, one per rank (the path has no exchange step).
 
 Solver defaults of the ours arm: the composite multigrid cycle in FP32 with FP16 stage
 coefficients (Chebyshev stage smoothing, Chebyshev-Richardson fine steps, exact coarsest stage),
 flexible GMRES with delayed CGS2 and no recycled subspace; --mg-cycle reference --mg fp64
---delayed 0 --recycle 0 selects the reference's solver configuration.  The line also carries a short learned-preconditioner
-comparison (skip with --no-learned).  Other modes:
+--delayed 0 --recycle 0 selects the reference's solver configuration.  The line also carries a
+short learned-preconditioner comparison (skip with --no-learned).  Other modes:
   --learned     the learned-preconditioner measurement (harvest, train, re-solve each step's
                 projection under each preconditioner)
   --sweep       the batched angle sweep (16 wing instances, 4 concurrent batches)
@@ -37,6 +48,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -57,6 +69,9 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", default="paraglider16m")
+    ap.add_argument("--grid", choices=("cutcell", "staircase"), default="cutcell",
+                    help="cutcell: the reference's own preprocessing of the surface (brick hierarchy, cut-cell EB "
+                         "atlas, composite system); staircase: this library's solid-cell builder")
     ap.add_argument("--mg", choices=("fp64", "fp32"), default="fp32",
                     help="multigrid preconditioner precision (the composite stages; fine sweeps and Krylov stay FP64)")
     ap.add_argument("--restart", type=int, default=0, help="GCRO columns per cycle (0: the reference's 24)")
@@ -148,7 +163,7 @@ class ClockSampler:
     def __init__(self, device: int, path: str | None = None):
         self.device = device
         self.proc = None
-        self.path = path or os.path.join(ROOT, "gpurun_out", f"clocks_rank{device}.csv")
+        self.path = path or os.path.join(tempfile.gettempdir(), f"pcfd_clocks_{os.getpid()}_{device}.csv")
 
     def __enter__(self):
         try:
@@ -170,6 +185,15 @@ class ClockSampler:
             self.file.close()
 
     def summary(self) -> dict:
+        out = self._read()
+        if self.proc:
+            try:
+                os.remove(self.path)
+            except OSError:
+                pass
+        return out
+
+    def _read(self) -> dict:
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         visible = os.environ.get("CUDA_VISIBLE_DEVICES")
@@ -238,108 +262,233 @@ def inflow_profile(speed: float, centres, step: int) -> np.ndarray:
     return (speed * (1.0 + 0.02 * np.sin(0.6 * y + 0.4 * z + 0.1 * step))).astype(np.float32)
 
 
-def ncu_traffic(workload: str) -> float | None:
-    """DRAM bytes (read + write) per launch of the structured operator kernel, from the committed
-    ncu summary ``profiles/brick_apply_<workload>.md`` (line ``bytes_per_launch: N``), if present."""
-    path = os.path.join(ROOT, "profiles", f"brick_apply_{workload}.md")
-    try:
-        with open(path) as f:
-            for line in f:
-                if line.strip().startswith("bytes_per_launch:"):
-                    return float(line.split(":", 1)[1].strip().split()[0])
-    except (OSError, ValueError):
-        pass
-    return None
+# DRAM bytes (read + write) per launch of the roofline kernel, from one ncu capture of
+# `bench.py --kernel-only <k> --workload <w>` (--metrics dram__bytes_read.sum,dram__bytes_write.sum,
+# one pass); keyed by (workload, grid, kernel-only component).  A bench run cannot measure DRAM
+# traffic itself; absent entries report null.
+DRAM_BYTES_PER_LAUNCH: dict = {}
 
 
-# ------------------------------------------------------------------------------------------ CPU sample
-class CpuReference:
-    """The reference's host implementation of one time step on the full workload.
+# ------------------------------------------------------------------------------------------ grids
+class Grid:
+    """A workload's grid: the topology view handed to the library plus what the line reports.
 
-    Every operator of the step is the reference's own CPU twin (oracle/_ref, single-threaded as
-    the reference wrote it): outflow-rate reduction, MUSCL transport, Smagorinsky diffusion,
-    smooth wall, flux reconstruction, projection RHS, flux correction, pressure traction and
-    surface loads.  The reference has no CPU pressure solver; the projection is the FP64 OpenMP
-    restatement of its solver (oracle/pcfd_oracle.cpp).  Stages run on fixed inputs derived
-    from the freestream initial state (their cost does not depend on the values).
-    """
+    ``cutcell`` is the reference's own preprocessing of the workload's closed surface (brick
+    hierarchy, cut-cell embedded-boundary atlas, composite pressure system; oracle/_ref), the
+    input the drop-in boundary receives from the reference's caller.  ``staircase`` is this
+    library's own solid-cell builder (pcfd_topology_build)."""
 
-    STAGES = ("outflow_rate", "transport", "diffusion", "wall", "reconstruct", "rhs", "correct", "impulse", "loads")
-
-    def __init__(self, topology, spec):
-        from oracle import port, ref
+    def __init__(self, spec, kind: str = "cutcell"):
+        self.kind = kind
         self.spec = spec
-        self.rc = rc = ref.import_topology(topology)
-        self.ps = port.PortSystem(topology)
+        if kind == "cutcell":
+            from oracle import ref
+            self.holder = ref.workload_case(spec)
+            self.topology = self.holder.topology
+            s = self.holder.summary
+            self.storage_size = int(s["storage"])
+            bs3 = spec.brick_size ** 3
+            structured = sum(self.topology.levels[l].brick_count for l in range(self.topology.level_count)) * bs3
+            active = self.holder.active.astype(bool)
+            self.leaf_cells = int(active[:structured].sum())
+            self.counts = {"grid": "cut-cell (reference preprocessing)", "eb_fragments": int(self.storage_size - structured),
+                           "active_dofs": int(s["active"]), "coarse_fine_edges": int(s["coarse_fine"]),
+                           "embedded_edges": int(s["embedded"]), "wls_gradient_nodes": int(s["gradient_nodes"]),
+                           "surface_patches": int(s["patches"])}
+            self.min_volume_fraction = spec.min_volume_fraction
+        else:
+            self.holder = spec.build()
+            self.topology = self.holder.topology
+            self.storage_size = self.holder.storage_size
+            self.leaf_cells = self.holder.leaf_cells
+            self.counts = {"grid": "staircase (pcfd_topology_build)"}
+            self.min_volume_fraction = 0.0
+
+    def close(self):
+        if self.holder is not None:
+            self.holder.close()
+            self.holder = None
+
+
+# ------------------------------------------------------------------------------------------ CPU steps
+# Whole CPU steps of a 16 M-cell grid take minutes each, so the CPU timings run whole steps of the
+# same wing on a smaller grid of the same family and scale by the DOF count.
+CPU_SAMPLE = {"paraglider16m": "paraglider1m", "paraglider5m": "paraglider1m"}
+
+
+class CpuStepper:
+    """Whole time steps of the reference's host implementation on one grid.
+
+    ExternalAeroCore::step's sequence (external_aero_core.cpp:304-328) with the reference's own CPU
+    twins (oracle/_ref, single-threaded as written): outflow-rate CFL reduction, MUSCL transport,
+    Smagorinsky diffusion, smooth wall, cell-to-face reconstruction, the external boundaries of
+    amr_fields.cu:86-118 (X-min inflow, Y/Z free slip; restated below on the compact faces),
+    projection RHS, the pressure solve, flux correction, pressure traction, surface loads.  The
+    reference has no CPU pressure solver: the solve to the case tolerance is the FP64 OpenMP
+    restatement of its own solver (reference multigrid cycle, flexible GCRO; oracle/pcfd_oracle.cpp),
+    warm-started from the previous pressure like the reference's.  ``initialize`` follows
+    ExternalAeroCore::initialize (external_aero_core.cpp:245-302)."""
+
+    def __init__(self, grid: Grid):
+        from oracle import port
+        self.grid, self.spec = grid, grid.spec
+        self.rc = grid.holder
+        self.ps = port.PortSystem(grid.topology)
         self.threads = port.threads()
-        n = rc.n
-        active = rc.active.astype(bool)
-        connected = np.ctypeslib.as_array(topology.freestream_connected, shape=(n,)).astype(bool)
-        x = np.where(active & connected, spec.speed, 0.0).astype(np.float32)
-        self.state = (x, np.zeros(n, np.float32), np.zeros(n, np.float32))
-        zeros = np.zeros(rc.faces, np.float32)
-        self.faces = rc.reconstruct(self.state, zeros, zeros, zeros)
-        rate = rc.outflow_rate(*self.faces, True)
-        h = topology.levels[topology.level_count - 1].h
-        self.dt = spec.case["cfl"] / max(1e-9, spec.speed / h, rate)
-        self.rhs = rc.rhs(*self.faces, spec.case["rho"], self.dt)
-        self.pressure = np.zeros(n)
-        self.per_iteration_s = None
-        self.solver_iterations = None
+        t = grid.topology
+        self.bs = bs = t.brick_size
+        self.h = t.levels[t.level_count - 1].h
+        flags = np.concatenate([np.ctypeslib.as_array(t.levels[l].flags, shape=(t.levels[l].brick_count,))
+                                for l in range(t.level_count)])
+        from paracfd_b200 import capi
+        live = (flags & capi.BRICK_COVERED) == 0
+        per = (bs + 1) * bs * bs
+        a, b = np.meshgrid(np.arange(bs), np.arange(bs), indexing="ij")
+        a, b = a.ravel(), b.ravel()
+
+        def faces(mask, index):
+            slots = np.nonzero(live & ((flags & mask) != 0))[0]
+            return (slots[:, None] * per + index[None, :]).ravel()
+        # compact layouts: u (k*bs+j)*(bs+1)+i, v (k*(bs+1)+j)*bs+i, w (k*bs+j)*bs+i
+        self.xmin = faces(capi.BRICK_XMIN, (b * bs + a) * (bs + 1))
+        self.ywall = np.concatenate([faces(capi.BRICK_YMIN, (b * (bs + 1)) * bs + a),
+                                     faces(capi.BRICK_YMAX, (b * (bs + 1) + bs) * bs + a)])
+        self.zwall = np.concatenate([faces(capi.BRICK_ZMIN, a * bs + b),
+                                     faces(capi.BRICK_ZMAX, bs * bs * bs + a * bs + b)])
+        self.n = self.rc.n
+        self.pressure = np.zeros(self.n)
+        self.faces = None
+        self.state = None
 
     def close(self):
         self.ps.close()
-        self.rc.close()
 
-    def time_solver(self, max_iterations: int) -> dict:
-        """Restated FP64 solve of the step's RHS from zero, capped at ``max_iterations``."""
-        case = self.spec.case
-        t0 = time.perf_counter()
-        self.pressure, info = self.ps.solve(self.rhs, case["projection_tolerance"], max_iterations)
-        elapsed = time.perf_counter() - t0
-        self.per_iteration_s = elapsed / max(1, info["iterations"])
-        self.solver_iterations = info["iterations"]
-        return dict(info, seconds=elapsed)
+    def boundaries(self, faces):
+        u, v, w, cf, eb = faces
+        u[self.xmin] = self.spec.speed
+        v[self.ywall] = 0.0
+        w[self.zwall] = 0.0
+        return u, v, w, cf, eb
 
-    def stage(self, name: str) -> float:
-        rc, case, (u, v, w, cf, eb), st = self.rc, self.spec.case, self.faces, self.state
-        nu, rho, dt = case["nu"], case["rho"], self.dt
-        calls = {
-            "outflow_rate": lambda: rc.outflow_rate(u, v, w, cf, eb, True),
-            "transport": lambda: rc.transport(u, v, w, cf, eb, dt, st, True, self.spec.speed),
-            "diffusion": lambda: rc.diffuse_smagorinsky(st, nu, case["smagorinsky_cs"], dt),
-            "wall": lambda: rc.wall(st, nu, dt, rho),
-            "reconstruct": lambda: rc.reconstruct(st, u, v, w),
-            "rhs": lambda: rc.rhs(u, v, w, cf, eb, rho, dt),
-            "correct": lambda: rc.correct_fluxes(self.pressure, rho, dt, u, v, w, cf, eb),
-            "impulse": lambda: rc.impulse(self.pressure, dt, rho, st, True),
-            "loads": lambda: rc.pressure_loads(self.pressure),
-        }
+    def initialize(self) -> dict:
+        rc, spec, case = self.rc, self.spec, self.spec.case
+        t = self.grid.topology
+        active = rc.active.astype(bool)
+        connected = np.ctypeslib.as_array(t.freestream_connected, shape=(self.n,)).astype(bool)
+        x = np.where(active & connected, spec.speed, 0.0).astype(np.float32)
+        self.state = (x, np.zeros(self.n, np.float32), np.zeros(self.n, np.float32))
+        zeros = np.zeros(rc.faces, np.float32)
+        self.faces = self.boundaries(rc.reconstruct(self.state, zeros, zeros, zeros))
+        dt = case["cfl"] * self.h / max(1e-9, abs(spec.speed))
+        return self._project(dt, warm=False)
+
+    def _project(self, dt: float, warm: bool) -> dict:
+        rc, case = self.rc, self.spec.case
+        rhs = rc.rhs(*self.faces, case["rho"], dt)
+        p, info = self.ps.solve(rhs, case["projection_tolerance"], case["projection_max_iterations"],
+                                x0=self.pressure if warm else None)
+        self.pressure = p
+        self.faces = rc.correct_fluxes(p, case["rho"], dt, *self.faces)
+        if info["converged"]:
+            self.state = rc.impulse(p, dt, case["rho"], self.state, True)
+        return dict(info, dt=dt)
+
+    def step(self) -> dict:
+        rc, spec, case = self.rc, self.spec, self.spec.case
+        rate = rc.outflow_rate(*self.faces, True)
+        dt = case["cfl"] / max(1e-9, abs(spec.speed) / self.h, rate)
+        self.state = rc.transport(*self.faces, dt, self.state, True, spec.speed)
+        self.state = rc.diffuse_smagorinsky(self.state, case["nu"], case["smagorinsky_cs"], dt)
+        self.state, _ = rc.wall(self.state, case["nu"], dt, case["rho"])
+        self.faces = self.boundaries(rc.reconstruct(self.state, *self.faces[:3]))
+        info = self._project(dt, warm=True)
+        info["loads"] = rc.pressure_loads(self.pressure)
+        return info
+
+
+def cpu_steps(spec, warmup: int, steps: int) -> dict:
+    """Times whole CPU steps (CpuStepper) on the workload's CPU sample grid; the value is scaled to
+    the workload's DOF count.  Returns the cpu_baseline fields."""
+    from paracfd_b200.workloads import WORKLOADS
+    sample_name = CPU_SAMPLE.get(spec.name, spec.name)
+    sample = Grid(WORKLOADS[sample_name], "cutcell")
+    stepper = CpuStepper(sample)
+    t0 = time.perf_counter()
+    init = stepper.initialize()
+    init_s = time.perf_counter() - t0
+    for _ in range(warmup):
+        stepper.step()
+    times, iterations, converged = [], [], 0
+    for _ in range(steps):
         t0 = time.perf_counter()
-        calls[name]()
-        return time.perf_counter() - t0
+        info = stepper.step()
+        times.append(time.perf_counter() - t0)
+        iterations.append(info["iterations"])
+        converged += int(info["converged"])
+    stepper.close()
+    sample_dofs = sample.storage_size
+    sample.close()
+    return {"sample_workload": sample_name, "sample_storage": sample_dofs, "step_s": times,
+            "iterations": iterations, "converged_steps": converged, "init_s": init_s,
+            "init_iterations": init["iterations"], "threads": stepper.threads}
 
 
 # ------------------------------------------------------------------------------------------ arms
-def run_ours(args, ranks: Ranks):
-    import ctypes as C
-
+def make_system(args, grid: Grid, device: int):
     from paracfd_b200 import MG_FP32, MG_FP64, CompositeSystem
+    return CompositeSystem(grid.topology, MG_FP32 if args.mg == "fp32" else MG_FP64, device=device,
+                           momentum_min_volume_fraction=grid.min_volume_fraction,
+                           mg_cycle={"reference": 0, "corrected": 1, "composite": 2}[args.mg_cycle],
+                           gmres_restart=args.restart, mg_stage_sweeps=args.stage_sweeps,
+                           mg_block_iterations=args.block_iterations, mg_stage_chebyshev=args.chebyshev,
+                           mg_fine_chebyshev=args.fine_chebyshev, gmres_delayed=args.delayed,
+                           gmres_recycle=args.recycle, mg_stage_fp16=args.stage_fp16)
+
+
+def line_config(args, grid: Grid, n: int) -> dict:
+    """The config object both arms print (same workload, same grid)."""
+    spec = grid.spec
+    return dict(spec.describe(), leaf_cells=grid.leaf_cells, storage=grid.storage_size, **grid.counts,
+                mg=args.mg, mg_cycle=args.mg_cycle, gcro_restart=args.restart or 24,
+                stage_sweeps=args.stage_sweeps or 6, block_iterations=args.block_iterations,
+                stage_smoother="jacobi" if args.chebyshev == 1 else f"chebyshev 2/{args.chebyshev or 30}",
+                fine_smoother="jacobi" if args.fine_chebyshev == 1 else f"chebyshev-richardson 2/{args.fine_chebyshev or 10}",
+                orthogonalisation="delayed CGS2" if args.delayed else "CGS2",
+                recycled_pairs=3 if args.recycle == 0 else max(args.recycle, 0),
+                stage_coefficients="fp16" if args.stage_fp16 else args.mg,
+                parallelism=f"replicas{n}", l2="inputs larger than L2")
+
+
+METRIC = "AMR steps/s at 16M cells (projection to 1e-8, loads every step)"
+
+
+def cpu_baseline_fields(spec, grid: Grid, timing: dict) -> dict:
+    """cpu_baseline of a cpu_steps() timing: steps/s scaled from the sample grid to the workload."""
+    mean_s = statistics.mean(timing["step_s"])
+    scale = grid.storage_size / timing["sample_storage"]
+    return {
+        "value": round(1.0 / (mean_s * scale), 6), "unit": "steps/s", "cores": timing["threads"], "kind": "reference",
+        "sample": (f"{len(timing['step_s'])} whole CPU time steps (after the initial projection and the warm-up "
+                   f"steps) of the same wing on the {timing['sample_workload']} cut-cell grid "
+                   f"({timing['sample_storage']} DOFs): the reference's CPU twins of every stage (1 thread) and "
+                   f"its solver restated in FP64 OpenMP ({timing['threads']} threads) to the case tolerance; "
+                   f"mean {mean_s:.3f} s per step scaled by the DOF ratio {scale:.2f} to this grid (the "
+                   f"solver's iteration count grows with the grid, so the scaled CPU figure is optimistic)"),
+        "sample_step_s": round(mean_s, 4), "sample_iterations_per_step": round(statistics.mean(timing["iterations"]), 2),
+        "sample_converged_steps": timing["converged_steps"]}
+
+
+def run_ours(args, ranks: Ranks):
     from paracfd_b200.workloads import WORKLOADS
 
     spec = WORKLOADS[args.workload]
-    built = spec.build()
-    bricks = non_covered_bricks(built.topology)
-    system = CompositeSystem(built.topology, MG_FP32 if args.mg == "fp32" else MG_FP64, device=ranks.local,
-                             mg_cycle={"reference": 0, "corrected": 1, "composite": 2}[args.mg_cycle],
-                             gmres_restart=args.restart, mg_stage_sweeps=args.stage_sweeps,
-                             mg_block_iterations=args.block_iterations, mg_stage_chebyshev=args.chebyshev,
-                             mg_fine_chebyshev=args.fine_chebyshev, gmres_delayed=args.delayed,
-                             gmres_recycle=args.recycle, mg_stage_fp16=args.stage_fp16)
+    grid = Grid(spec, args.grid)
+    bricks = non_covered_bricks(grid.topology)
+    system = make_system(args, grid, ranks.local)
     system.configure(speed=spec.speed, **spec.case)
     slots = system.inflow_layout()
     faces = len(slots) * spec.brick_size ** 2
-    centres = inflow_face_centres(built.topology, slots)
+    centres = inflow_face_centres(grid.topology, slots)
     system.set_inflow(inflow_profile(spec.speed, centres, 0))
     init = system.initialize()
     stats = []
@@ -411,26 +560,17 @@ def run_ours(args, ranks: Ranks):
         avg_ms = float(np.mean(per_launch))
         algorithmic = A_P_BYTES_PER_DOF * bricks * spec.brick_size ** 3
         achieved = algorithmic / (avg_ms * 1e-3) / 1e9
-        traffic = ncu_traffic(args.workload)
+        traffic = DRAM_BYTES_PER_LAUNCH.get((args.workload, args.grid, 1))
         roofline = {"bound": "hbm", "kernel": region_names[0], "achieved": round(achieved, 1), "peak": peak,
                     "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                     "traffic": traffic, "algorithmic_bytes_per_launch": algorithmic,
                     "launches_timed": int(len(per_launch)), "avg_launch_us": round(avg_ms * 1e3, 2)}
     line = {
-        "metric": "AMR steps/s at 16M cells (projection to 1e-8, loads every step)",
+        "metric": METRIC,
         "value": round(value, 4), "unit": "steps/s", "n_gpus": n, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(elapsed_ms / args.steps, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 state / f64 pressure", "data": "synthetic analytic geometry",
-        "config": dict(spec.describe(), leaf_cells=built.leaf_cells, storage=built.storage_size,
-                       mg=args.mg, mg_cycle=args.mg_cycle, gcro_restart=args.restart or 24,
-                       stage_sweeps=args.stage_sweeps or 6, block_iterations=args.block_iterations,
-                       stage_smoother="jacobi" if args.chebyshev == 1 else f"chebyshev 2/{args.chebyshev or 30}",
-                       fine_smoother="jacobi" if args.fine_chebyshev == 1 else f"chebyshev-richardson 2/{args.fine_chebyshev or 10}",
-                       orthogonalisation="delayed CGS2" if args.delayed else "CGS2",
-                       recycled_pairs=3 if args.recycle == 0 else max(args.recycle, 0),
-                       stage_coefficients="fp16" if args.stage_fp16 else args.mg,
-                       parallelism=f"replicas{n}",
-                       l2="inputs larger than L2"),
+        "config": line_config(args, grid, n),
         "projection_ms": round(statistics.mean(s["projection_ms"] for s in stats), 3),
         "iterations_per_step": round(statistics.mean(s["pressure"]["iterations"] for s in stats), 2),
         "final_residual_max": max(s["pressure"]["relative_residual"] for s in stats),
@@ -447,26 +587,13 @@ def run_ours(args, ranks: Ranks):
                             "avg_ms": region_ms},
         "cpu_baseline": None,
     }
+    system.close()
     if ranks.rank == 0 and n == 1 and not args.no_cpu_baseline:
         try:
-            cpu = CpuReference(built.topology, spec)
-            stages = {name: cpu.stage(name) for name in CpuReference.STAGES}
-            cpu.time_solver(2)
-            iters = max(1, int(round(line["iterations_per_step"])))
-            stages["projection_solve"] = cpu.per_iteration_s * iters
-            cpu.close()
-            step_s = sum(stages.values())
-            line["cpu_baseline"] = {
-                "value": round(1.0 / step_s, 6), "unit": "steps/s", "cores": cpu.threads, "kind": "reference",
-                "sample": (f"one full-size step: each operator once through the reference CPU twins (1 thread); "
-                           f"solve = FP64 OpenMP restated solver ({cpu.threads} threads), time of its first 2 "
-                           f"Krylov iterations per iteration x {iters} (this run's GPU count; early iterations are "
-                           f"the cheapest, so the CPU figure is optimistic)"),
-                "stages_s": {k: round(t, 4) for k, t in stages.items()}}
+            line["cpu_baseline"] = cpu_baseline_fields(spec, grid, cpu_steps(spec, 1, 3))
         except Exception as exc:   # the CPU sample must not hide the GPU result
             line["cpu_baseline"] = {"value": None, "error": str(exc)[:200]}
-    system.close()
-    built.close()
+    grid.close()
     if ranks.rank == 0 and n == 1 and not args.no_learned:
         # the learned-preconditioner comparison (a short --learned run) beside the headline
         try:
@@ -478,98 +605,77 @@ def run_ours(args, ranks: Ranks):
 
 
 def run_kernel_only(args):
-    from paracfd_b200 import MG_FP32, MG_FP64, CompositeSystem
     from paracfd_b200.workloads import WORKLOADS
     spec = WORKLOADS[args.workload]
-    built = spec.build()
-    system = CompositeSystem(built.topology, MG_FP32 if args.mg == "fp32" else MG_FP64,
-                             mg_cycle={"reference": 0, "corrected": 1, "composite": 2}[args.mg_cycle],
-                             gmres_restart=args.restart, mg_stage_sweeps=args.stage_sweeps,
-                             mg_block_iterations=args.block_iterations, mg_stage_chebyshev=args.chebyshev,
-                             mg_fine_chebyshev=args.fine_chebyshev, gmres_delayed=args.delayed,
-                             gmres_recycle=args.recycle, mg_stage_fp16=args.stage_fp16)
+    grid = Grid(spec, args.grid)
+    system = make_system(args, grid, 0)
     ms = system.time_kernel(args.kernel_only, args.kernel_iterations)
-    line = {"kernel_only": args.kernel_only, "workload": args.workload, "ms_per_launch": ms,
+    line = {"kernel_only": args.kernel_only, "workload": args.workload, "grid": args.grid, "ms_per_launch": ms,
             "iterations": args.kernel_iterations, "launches": system.launch_count()}
     system.close()
-    built.close()
+    grid.close()
     return line
 
 
 def run_reference(args, ranks: Ranks):
-    """The reference's CPU implementation of the step on this machine's cores.
-
-    Setup (untimed): the reference imports the topology; its solver restatement solves the first
-    step's RHS to 1e-8 once, which gives the per-iteration cost and, without a GPU, the iteration
-    count.  With a GPU, the reference's own sm_100a device classes run the same workload
-    (ExternalAeroCore's step sequence) and their mean iterations per step are used, and reported
-    beside.  Each timed step then times one stage of the step in rotation (all stages are covered
-    after len(STAGES) steps; any left over are timed after the loop), so a run stays within a few
-    minutes; value = 1 / (sum of the mean stage times + per-iteration time x iterations).
-    """
+    """The reference arm: whole CPU time steps of the reference's host implementation (CpuStepper
+    on the workload's CPU sample grid, scaled to the workload), and whole steps of the reference's
+    own sm_100a build on the full workload.  Loads only oracle/_ref libraries."""
     from paracfd_b200.workloads import WORKLOADS
-    spec = WORKLOADS[args.workload]
     if ranks.rank != 0:
         return None
-    built = spec.build()
+    spec = WORKLOADS[args.workload]
+    if args.grid != "cutcell":
+        raise SystemExit("the reference arm runs on the reference's own cut-cell grid (--grid cutcell)")
+    grid = Grid(spec, "cutcell")
     case = spec.case
     gpu = None
-    iterations = None
     if not args.no_reference_gpu:
         try:
             from oracle import ref
-            rc = ref.import_topology(built.topology)
-            core = ref.RefDeviceCore(rc, spec.speed, case["rho"], case["nu"], case["cfl"], case["smagorinsky_cs"],
-                                     case["projection_tolerance"], case["projection_max_iterations"], 0.0)
-            core.initialize()
+            core = ref.RefDeviceCore(grid.holder, spec.speed, case["rho"], case["nu"], case["cfl"], case["smagorinsky_cs"],
+                                     case["projection_tolerance"], case["projection_max_iterations"],
+                                     grid.min_volume_fraction)
+            init = core.initialize()
             for _ in range(args.warmup):
                 core.step()
+            t0 = time.perf_counter()
             st = [core.step() for _ in range(args.steps)]
+            wall_s = time.perf_counter() - t0
             core.close()
-            rc.close()
             step_ms = statistics.mean(s["gpu_step_ms"] for s in st)
-            iterations = max(1, int(round(statistics.mean(s["iterations"] for s in st))))
-            gpu = {"steps_per_s": round(1000.0 / step_ms, 4), "step_ms": round(step_ms, 3),
+            gpu = {"steps_per_s": round(args.steps / wall_s, 4), "ms_per_step": round(1e3 * wall_s / args.steps, 3),
+                   "gpu_step_ms": round(step_ms, 3), "steps": args.steps, "warmup": args.warmup,
                    "projection_ms": round(statistics.mean(s["projection_ms"] for s in st), 3),
-                   "iterations_per_step": iterations, "converged_steps": sum(bool(s["converged"]) for s in st),
-                   "timing": "reference ExternalAeroStepStats host clock around its synchronous stages",
-                   "build": "reference sources compiled for sm_100a (oracle/_ref)"}
+                   "iterations_per_step": round(statistics.mean(s["iterations"] for s in st), 2),
+                   "converged_steps": sum(bool(s["converged"]) for s in st),
+                   "init_iterations": init["iterations"],
+                   "timing": "host clock around K whole synchronous steps (the reference synchronises every stage)",
+                   "build": "reference sources compiled for sm_100a (oracle/_ref): its DeviceAmrFields, "
+                            "DeviceCompositeAmrProjection and DeviceCompositeCellMomentumTransport in "
+                            "ExternalAeroCore::step's sequence"}
         except Exception as exc:
             gpu = {"unavailable": str(exc)[:200]}
-    cpu = CpuReference(built.topology, spec)
-    solve = cpu.time_solver(case["projection_max_iterations"])
-    if iterations is None:
-        iterations = max(1, solve["iterations"])
-    names = CpuReference.STAGES
-    for q in range(args.warmup):
-        cpu.stage(names[q % len(names)])
-    times = {name: [] for name in names}
-    for q in range(args.steps):
-        name = names[q % len(names)]
-        times[name].append(cpu.stage(name))
-    for name in names:
-        if not times[name]:
-            times[name].append(cpu.stage(name))
-    cpu.close()
-    stages = {name: statistics.mean(t) for name, t in times.items()}
-    stages["projection_solve"] = cpu.per_iteration_s * iterations
-    step_s = sum(stages.values())
-    value = 1.0 / step_s
-    sample = (f"per step one stage of the reference CPU twins (1 thread) at full size, in rotation; solve = FP64 "
-              f"OpenMP restated solver ({cpu.threads} threads): {solve['iterations']} iterations to "
-              f"{solve['relative_residual']:.2e} in {solve['seconds']:.1f} s, per-iteration time x {iterations} iterations")
+    t0 = time.perf_counter()
+    timing = cpu_steps(spec, args.warmup, args.steps)
+    cpu_wall = time.perf_counter() - t0
+    cpu = cpu_baseline_fields(spec, grid, timing)
+    sample_ms = 1e3 * statistics.mean(timing["step_s"])
     line = {
-        "metric": "AMR steps/s at 16M cells (projection to 1e-8, loads every step)", "impl": "reference",
-        "value": round(value, 6), "unit": "steps/s", "n_gpus": ranks.world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(step_s * 1e3, 1), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "metric": METRIC, "impl": "reference",
+        "value": cpu["value"], "unit": "steps/s", "n_gpus": ranks.world, "steps": args.steps, "warmup": args.warmup,
+        # each timed step is a whole step of the sample grid: ms_per_step x steps is the timed CPU region
+        "ms_per_step": round(sample_ms, 1),
+        "full_grid_ms_per_step_equivalent": round(1e3 / cpu["value"], 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 state / f64 pressure", "data": "synthetic analytic geometry",
-        "config": dict(spec.describe(), leaf_cells=built.leaf_cells, storage=built.storage_size),
-        "cpu_baseline": {"value": round(value, 6), "unit": "steps/s", "cores": cpu.threads, "kind": "reference",
-                         "sample": sample, "stages_s": {k: round(t, 4) for k, t in stages.items()}},
-        "e2e": {"value": round(value, 6), "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "config": line_config(args, grid, ranks.world),
+        "cpu_baseline": cpu,
+        "cpu_wall_s": round(cpu_wall, 1),
+        "e2e": {"value": cpu["value"], "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "reference_sm100a": gpu,
     }
-    built.close()
+    grid.close()
     return line
 
 
@@ -600,8 +706,9 @@ def run_learned(args, ranks: Ranks):
     for k in range(args.harvest_runs):
         name = ("naca0012_slab", "naca4412_wing")[k % 2]
         spec = with_aoa(name, float(rng.uniform(0.0, 10.0)))
-        built = spec.build()
-        with CompositeSystem(built.topology, device=ranks.local, mg_cycle=MG_CYCLE_COMPOSITE) as system:
+        built = Grid(spec, args.grid)
+        with CompositeSystem(built.topology, device=ranks.local, mg_cycle=MG_CYCLE_COMPOSITE,
+                             momentum_min_volume_fraction=built.min_volume_fraction) as system:
             system.configure(speed=spec.speed, **spec.case)
             system.initialize()
             system.harvest_begin(capacity_pairs=4000, bricks_per_pair=32, seed=1000 + k, target=LEARNED_TARGET_BRICK_SOLVE)
@@ -620,8 +727,9 @@ def run_learned(args, ranks: Ranks):
     harvest_s = time.time() - t0
 
     spec = WORKLOADS["naca4412_wing"]
-    built = spec.build()
-    system = CompositeSystem(built.topology, device=ranks.local, mg_cycle=MG_CYCLE_COMPOSITE)
+    built = Grid(spec, args.grid)
+    system = CompositeSystem(built.topology, device=ranks.local, mg_cycle=MG_CYCLE_COMPOSITE,
+                             momentum_min_volume_fraction=built.min_volume_fraction)
     system.configure(speed=spec.speed, **spec.case)
     system.initialize()
     t0 = time.time()
@@ -662,7 +770,7 @@ def run_learned(args, ranks: Ranks):
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "vs_multigrid": round(mg_ms / summary["learned_multigrid"]["projection_ms"], 3),
         "dtype": "bf16 network / f64 Krylov", "data": "synthetic analytic geometry",
-        "config": dict(spec.describe(), leaf_cells=built.leaf_cells, bricks=bricks, mg_cycle="composite",
+        "config": dict(spec.describe(), leaf_cells=built.leaf_cells, **built.counts, bricks=bricks, mg_cycle="composite",
                        harvest_target="brick solve", train_steps=args.train_steps, batch=64),
         "preconditioners": summary,
         "harvest": harvest, "harvest_s": round(harvest_s, 1), "train_s": round(train_s, 1), "train_loss": loss,
@@ -686,8 +794,9 @@ def run_sweep(args, ranks: Ranks):
     batches = []
     for first in range(0, len(specs), 4):
         batch = specs[first:first + 4]
-        builts = [sp.build() for sp in batch]
+        builts = [Grid(sp, args.grid) for sp in batch]
         systems = [CompositeSystem(b.topology, MG_FP32, device=ranks.local, mg_cycle=MG_CYCLE_COMPOSITE,
+                                   momentum_min_volume_fraction=b.min_volume_fraction,
                                    mg_stage_sweeps=args.stage_sweeps, mg_stage_chebyshev=args.chebyshev,
                                    mg_fine_chebyshev=args.fine_chebyshev, gmres_delayed=args.delayed,
                              gmres_recycle=args.recycle, mg_stage_fp16=args.stage_fp16) for b in builts]

@@ -88,6 +88,10 @@ def lib():
         L.ref_case_from_mesh.restype = vp
         L.ref_case_from_mesh.argtypes = [f64p, C.c_int64, C.POINTER(C.c_uint32), C.c_int64, f64p, f64p, C.c_double,
                                          C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double]
+        L.ref_case_from_mesh_eb.restype = vp
+        L.ref_case_from_mesh_eb.argtypes = [f64p, C.c_int64, C.POINTER(C.c_uint32), C.c_int64, f64p, f64p, C.c_double,
+                                            C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double,
+                                            C.c_double]
         _lib = L
     return _lib
 
@@ -337,6 +341,36 @@ def case_from_mesh(vertices, triangles, domain_lo, domain_hi, base_cell_size, ma
     if not handle:
         raise RuntimeError("reference mesh case failed: " + lib().ref_last_error().decode(errors="replace"))
     return RefCase(None, handle=handle)
+
+
+def cut_cell_case_from_mesh(vertices, triangles, domain_lo, domain_hi, base_cell_size, max_levels, brick_size=8,
+                            wing_refinement_distance=1.0, surface_refinement_distance=0.35, wake_length=8.0,
+                            wake_radius=2.0, min_volume_fraction=0.25) -> RefCase:
+    """Reference hierarchy + cut-cell embedded-boundary atlas + composite system for a closed
+    triangle shell (the shell's own discrete inside test is the solid)."""
+    v = np.ascontiguousarray(vertices, np.float64)
+    t = np.ascontiguousarray(triangles, np.uint32)
+    lo = np.ascontiguousarray(domain_lo, np.float64)
+    hi = np.ascontiguousarray(domain_hi, np.float64)
+    handle = lib().ref_case_from_mesh_eb(ptr(v, C.c_double), len(v), ptr(t, C.c_uint32), len(t), ptr(lo, C.c_double),
+                                         ptr(hi, C.c_double), base_cell_size, max_levels, brick_size,
+                                         wing_refinement_distance, surface_refinement_distance, wake_length,
+                                         wake_radius, min_volume_fraction)
+    if not handle:
+        raise RuntimeError("reference cut-cell case failed: " + lib().ref_last_error().decode(errors="replace"))
+    return RefCase(None, handle=handle)
+
+
+def workload_case(spec) -> RefCase:
+    """A named workload's grid built by the reference's own preprocessing: its brick hierarchy
+    (AmrHierarchy::build_static over the workload's domain), the cut-cell embedded-boundary atlas
+    of the workload's closed surface and the composite pressure system, as ExternalAeroCore's
+    constructor builds them (external_aero_core.cpp:77-103, 199-200)."""
+    vertices, triangles = spec.surface()
+    return cut_cell_case_from_mesh(vertices, triangles, spec.domain_lo, spec.domain_hi, spec.base_cell_size,
+                                   spec.max_levels, spec.brick_size, spec.wing_refinement_distance,
+                                   spec.surface_refinement_distance, spec.wake_length, spec.wake_radius,
+                                   spec.min_volume_fraction)
 
 
 def box_case(**kw) -> RefCase:

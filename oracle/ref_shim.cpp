@@ -889,12 +889,48 @@ int ref_pressure_loads(void* handle, const double* pressure, double pref, const 
     });
 }
 
-void* ref_case_from_mesh(const double* positions, int64_t vertices, const uint32_t* indices, int64_t triangles,
-                         const double* lo, const double* hi, double h, int32_t levels, int32_t bs, double wing_distance,
-                         double surface_distance, double wake_length, double wake_radius)
+}  // extern "C"
+
+namespace
 {
-    RefCase* rc = nullptr;
-    guarded([&] {
+    // Closed-solid classification by the reference's own discrete test on the same triangle
+    // shell (TriangleBvh::classify_closed_point, three-ray parity with a solid-angle fallback).
+    // The reference's STEP solid answers classify_discrete_points exactly this way
+    // (occt_closed_solid.cpp:46-58), and the cut-cell builder only asks that question
+    // (solid_embedded_boundary.cpp:831, 1062; amr_eb.cpp:109).
+    class DiscreteMeshSolid final : public ClosedSolidGeometry
+    {
+        const TriangleBvh* bvh_;
+        Aabb3d bounds_;
+
+    public:
+        DiscreteMeshSolid(const TriMesh& mesh, const TriangleBvh* bvh) : bvh_(bvh)
+        {
+            for (std::size_t q = 0; q < mesh.vertex_count(); ++q)
+            {
+                const auto p = mesh.vertex_position_double(q);
+                bounds_.expand(Vec3d{p[0], p[1], p[2]});
+            }
+        }
+        const Aabb3d& bounds() const override { return bounds_; }
+        void classify_points(const Vec3d* points, std::size_t count, double tolerance,
+                             ClosedSolidPointLocation* locations) const override
+        {
+            for (std::size_t q = 0; q < count; ++q)
+            {
+                const auto location = bvh_->classify_closed_point(points[q], tolerance);
+                locations[q] = location == ClosedMeshPointLocation::inside ? ClosedSolidPointLocation::inside
+                             : (location == ClosedMeshPointLocation::outside ? ClosedSolidPointLocation::outside
+                                                                             : ClosedSolidPointLocation::boundary);
+            }
+        }
+    };
+
+    RefCase* case_from_mesh(const double* positions, int64_t vertices, const uint32_t* indices, int64_t triangles,
+                            const double* lo, const double* hi, double h, int32_t levels, int32_t bs,
+                            double wing_distance, double surface_distance, double wake_length, double wake_radius,
+                            bool cut_cells, double min_volume_fraction)
+    {
         auto owned = std::make_unique<RefCase>();
         RefCase& c = *owned;
         TriMesh mesh;
@@ -924,14 +960,71 @@ void* ref_case_from_mesh(const double* positions, int64_t vertices, const uint32
         c.config.amr.surface_refinement_distance = surface_distance;
         c.config.amr.wake_length = wake_length;
         c.config.amr.wake_radius = wake_radius;
+        c.config.amr.min_volume_fraction = min_volume_fraction;
         Aabb3d domain;
         domain.lo = {lo[0], lo[1], lo[2]};
         domain.hi = {hi[0], hi[1], hi[2]};
         c.hierarchy = AmrHierarchy::build_static(domain, c.wing, *c.bvh, c.config.amr, false);
-        c.system = build_composite_amr_pressure_system(c.hierarchy, true);
+        if (cut_cells)
+        {
+            // external_aero_core.cpp:97-103: the constructor's atlas options.
+            c.solid = std::make_shared<DiscreteMeshSolid>(c.wing, c.bvh.get());
+            EmbeddedBoundaryBuildOptions eb;
+            eb.min_volume_fraction = c.config.amr.min_volume_fraction;
+            eb.retain_signed_bracketed_small_roots_for_face_state = true;
+            eb.min_aperture_area_fraction = c.config.amr.min_aperture_area_fraction;
+            eb.closed_solid = c.solid;
+            c.atlas = build_amr_embedded_boundary_atlas(c.hierarchy, c.wing, *c.bvh, eb);
+            if (!c.atlas.ready_for_flow())
+            {
+                std::string why;
+                int shown = 0;
+                for (const auto& level : c.atlas.levels)
+                    for (const auto& problem : level.topology.unresolved)
+                        if (shown++ < 3)
+                        {
+                            const Vec3d at = level.topology.grid.cell_centroid(problem.parent_cell);
+                            why += "; level " + std::to_string(level.level) + " at (" + std::to_string(at.x) + "," +
+                                   std::to_string(at.y) + "," + std::to_string(at.z) + "): " + problem.reason;
+                        }
+                throw std::runtime_error("reference EB atlas has " + std::to_string(c.atlas.unresolved_count()) +
+                                         " unresolved cells" + why);
+            }
+            CompositeAmrPressureBuildOptions options;
+            options.pressure_outlet_xmax = true;
+            c.system = build_composite_amr_pressure_system(c.hierarchy, c.atlas, options);
+        }
+        else
+            c.system = build_composite_amr_pressure_system(c.hierarchy, true);
         c.system.hierarchy = &c.hierarchy;
         export_case(c);
-        rc = owned.release();
+        return owned.release();
+    }
+}
+
+extern "C" {
+
+void* ref_case_from_mesh(const double* positions, int64_t vertices, const uint32_t* indices, int64_t triangles,
+                         const double* lo, const double* hi, double h, int32_t levels, int32_t bs, double wing_distance,
+                         double surface_distance, double wake_length, double wake_radius)
+{
+    RefCase* rc = nullptr;
+    guarded([&] {
+        rc = case_from_mesh(positions, vertices, indices, triangles, lo, hi, h, levels, bs, wing_distance,
+                            surface_distance, wake_length, wake_radius, false, 0.25);
+    });
+    return rc;
+}
+
+void* ref_case_from_mesh_eb(const double* positions, int64_t vertices, const uint32_t* indices, int64_t triangles,
+                            const double* lo, const double* hi, double h, int32_t levels, int32_t bs,
+                            double wing_distance, double surface_distance, double wake_length, double wake_radius,
+                            double min_volume_fraction)
+{
+    RefCase* rc = nullptr;
+    guarded([&] {
+        rc = case_from_mesh(positions, vertices, indices, triangles, lo, hi, h, levels, bs, wing_distance,
+                            surface_distance, wake_length, wake_radius, true, min_volume_fraction);
     });
     return rc;
 }

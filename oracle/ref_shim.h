@@ -87,6 +87,16 @@ void* ref_case_from_mesh(const double* positions, int64_t vertices, const uint32
                          int32_t brick_size, double wing_refinement_distance, double surface_refinement_distance,
                          double wake_length, double wake_radius);
 
+/* The same with the reference's cut-cell embedded boundary: the closed mesh is the solid (its
+ * discrete inside test), then build_amr_embedded_boundary_atlas and the atlas overload of
+ * build_composite_amr_pressure_system, with ExternalAeroCore's atlas options
+ * (external_aero_core.cpp:97-103). */
+void* ref_case_from_mesh_eb(const double* positions, int64_t vertices, const uint32_t* indices, int64_t triangles,
+                            const double* domain_lo, const double* domain_hi, double base_cell_size,
+                            int32_t max_levels, int32_t brick_size, double wing_refinement_distance,
+                            double surface_refinement_distance, double wake_length, double wake_radius,
+                            double min_volume_fraction);
+
 typedef struct ref_core_case {
     double speed, rho, nu, cfl, smagorinsky_cs, projection_tolerance;
     int32_t projection_max_iterations;

@@ -73,7 +73,8 @@ def extruded_wing(section: np.ndarray, y0: float, y1: float, offset=(0.0, 0.0, 0
         vertices.append(np.array([[centre[0], y0, centre[1]], [centre[0], y1, centre[1]]]))
         for q in range(n):
             a, b = q, (q + 1) % n
-            tris += [(c0, b, a), (c0 + 1, n + a, n + b)]
+            # the section runs counter-clockwise in (x, z): (centre, a, b) faces -Y, (centre, b, a) +Y
+            tris += [(c0, a, b), (c0 + 1, n + b, n + a)]
     v = np.concatenate(vertices) + np.asarray(offset)
     t = _orient_outward(v, np.array(tris, np.int64))
     return v.astype(np.float64), t.astype(np.uint32)
@@ -81,17 +82,22 @@ def extruded_wing(section: np.ndarray, y0: float, y1: float, offset=(0.0, 0.0, 0
 
 def paraglider_wing(span: float = 10.0, root_chord: float = 2.5, arc_radius: float = 6.0, digits: int = 4415,
                     aoa_deg: float = 8.0, stations: int = 96, points_per_side: int = 48, jitter: float = 1e-4,
-                    seed: int = 20261203):
+                    seed: int = 20261203, tip_chord: float = 0.02, tip_clustering: bool = False,
+                    flat_tips: bool = True):
     """Elliptic planform c(eta) = c0 sqrt(1 - eta^2) on a circular anhedral arc of the given
     radius (projected span ``span``), NACA section, tips closed at a small residual chord.
-    Surface points are displaced by a seeded uniform jitter of at most ``jitter * root_chord``."""
+    Surface points are displaced by a seeded uniform jitter of at most ``jitter * root_chord``.
+    With ``flat_tips`` the two tip sections and their cap centres keep their exact positions, so
+    each closed tip is one plane: a jittered cap folds at the 1e-4 chord scale, and the cut-cell
+    builder then finds isolated fluid slivers (~1e-12 m^3) whose pressure-gradient stencils have
+    rank 1, which the composite system rejects."""
     section = rotate_section(naca4_section(digits, points_per_side, 1.0), aoa_deg, pivot=(0.25, 0.0))
     half = 0.5 * span
     theta_max = np.arcsin(min(1.0, half / arc_radius))
-    eta = np.sin(np.linspace(-np.pi / 2, np.pi / 2, stations))          # clustered at the tips
+    eta = np.sin(np.linspace(-np.pi / 2, np.pi / 2, stations)) if tip_clustering else np.linspace(-1.0, 1.0, stations)
     theta = eta * theta_max
     chord = root_chord * np.sqrt(np.maximum(1.0 - eta ** 2, 0.0))
-    chord = np.maximum(chord, 0.02 * root_chord)
+    chord = np.maximum(chord, tip_chord * root_chord)
     n = len(section)
     rings = []
     for k in range(stations):
@@ -114,8 +120,12 @@ def paraglider_wing(span: float = 10.0, root_chord: float = 2.5, arc_radius: flo
     last = (stations - 1) * n
     for q in range(n):
         a, b = q, (q + 1) % n
-        tris += [(c0, b, a), (c0 + 1, last + a, last + b)]
+        tris += [(c0, a, b), (c0 + 1, last + b, last + a)]
     rng = np.random.default_rng(seed)
-    v = v + rng.uniform(-jitter * root_chord, jitter * root_chord, size=v.shape)
+    offset = rng.uniform(-jitter * root_chord, jitter * root_chord, size=v.shape)
+    if flat_tips:
+        offset[:n] = 0.0
+        offset[last:] = 0.0
+    v = v + offset
     t = _orient_outward(v, np.array(tris, np.int64))
     return v.astype(np.float64), t.astype(np.uint32)

@@ -35,6 +35,7 @@ class Workload:
     wake_length: float = 5.0
     wake_radius: float = 1.5
     speed: float = 11.0
+    min_volume_fraction: float = 0.25
     geometry: str = "paraglider"
     aoa: float = 8.0
     case: dict = field(default_factory=lambda: dict(rho=1.225, nu=1.5e-5, cfl=0.5, smagorinsky_cs=0.10,

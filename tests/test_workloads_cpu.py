@@ -37,3 +37,30 @@ def test_sweep_instances_are_seeded_and_batches_fit_8_to_20_million_cells():
     batches = [sum(cells[i:i + 4]) for i in range(0, 16, 4)]
     assert all(8e6 <= b <= 20e6 for b in batches), batches
     assert np.std(cells) > 0                         # uneven brick counts between instances
+
+
+def test_cut_cell_grids_come_from_the_reference_preprocessing():
+    """The bench grids: the reference's own hierarchy + cut-cell atlas + composite system of the
+    workload surfaces, with no unresolved cell (the closed paraglider shell's planar tips keep its
+    composite system valid)."""
+    from oracle import ref
+    for name, levels in (("naca0012_slab", 1), ("paraglider1m", 3)):
+        case = ref.workload_case(WORKLOADS[name])
+        try:
+            s = case.summary
+            assert s["levels"] == levels and s["unresolved"] == 0
+            assert s["embedded"] > 0 and s["gradient_nodes"] > 0 and s["patches"] > 0
+            assert s["storage"] > case.structured                       # EB fragments follow the bricks
+        finally:
+            case.close()
+
+
+def test_paraglider_shell_is_closed_and_outward():
+    from paracfd_b200.workloads import WORKLOADS as W
+    v, t = W["paraglider16m"].surface()
+    edges = np.concatenate([t[:, [0, 1]], t[:, [1, 2]], t[:, [2, 0]]]).astype(np.int64)
+    directed = set(map(tuple, edges))
+    assert len(directed) == len(edges)                                    # each directed edge once
+    assert all((b, a) in directed for a, b in directed)                   # and its reverse: closed, consistent
+    p0, p1, p2 = (v[t[:, q]] for q in range(3))
+    assert np.einsum("ij,ij->i", p0, np.cross(p1, p2)).sum() > 0          # outward (positive volume)
