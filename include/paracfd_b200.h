@@ -318,9 +318,9 @@ pcfd_status pcfd_pressure_apply_device(pcfd_system* system, const double* d_p, d
  * allocates nothing: the WLS-gradient scratch is a static device array of at most 262,144
  * gradient nodes (6 MiB), shared by all systems on the device; systems with more nodes get
  * PCFD_INVALID_ARG for the full operator.  For callers that cannot allocate at call time
- * (device memory reserved by another pool, allocator-free loops).  The first call on a device
- * sets up the scratch address and should come before any stream capture; calls overlapping in
- * time race on the scratch. */
+ * (device memory reserved by another pool, allocator-free loops).  The first full-operator
+ * call through a system looks up the scratch address (no allocation) and should come before any
+ * stream capture; calls overlapping in time race on the scratch. */
 pcfd_status pcfd_pressure_apply_device_noalloc(pcfd_system* system, const double* d_p, double* d_out,
                                                int32_t orthogonal);
 /* Jacobi diagonal used by the smoother (diagonal_cpu semantics). diag: [S]. */
@@ -391,6 +391,9 @@ pcfd_status pcfd_apply_external_boundaries(pcfd_system* system, double freestrea
 pcfd_status pcfd_momentum_cfl(pcfd_system* system, int32_t external_aero, double out[3]);
 
 /* ---- time step (ExternalAeroCore, external_aero_core.h:124-182) ------------------------------ */
+/* Sets the case.  A changed flow case (speed, rho, nu, cfl, Smagorinsky constant, wall or impulse
+ * switch) needs pcfd_core_initialize again; a call that changes only the projection tolerance or
+ * iteration budget keeps the initialized state and the physical time. */
 pcfd_status pcfd_core_configure(pcfd_system* system, const pcfd_case* config);
 /* Freestream state, reconstruction, first projection (ExternalAeroCore::initialize). */
 pcfd_status pcfd_core_initialize(pcfd_system* system, pcfd_step_stats* stats);
@@ -497,6 +500,12 @@ pcfd_status pcfd_learned_evaluate_host(pcfd_system* system, int32_t samples, con
                                        float* zhat, double* loss, float* gradients);
 /* z = learned preconditioner applied to r (device vectors [S]). */
 pcfd_status pcfd_learned_apply_device(pcfd_system* system, const double* d_r, double* d_z);
+/* No reference counterpart.  Limit of each tensor-core completion wait of the network kernels
+ * (default 2 s): a wait that runs out makes the call return PCFD_TIMEOUT after the kernel has
+ * drained its own MMAs and freed its tensor memory, and the system stays usable.
+ * idle_barrier_once != 0 makes the first wait of the next network convolution poll a barrier that
+ * nothing completes, so it runs out: the fault-path check of the tests (no GPU fault involved). */
+pcfd_status pcfd_learned_set_wait(pcfd_system* system, double seconds, int32_t idle_barrier_once);
 
 #ifdef __cplusplus
 }

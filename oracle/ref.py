@@ -78,6 +78,8 @@ def lib():
         L.ref_core_step.argtypes = [vp, f64p]
         L.ref_core_state.argtypes = [vp, f32p, f32p, f32p, f64p]
         L.ref_pressure_loads.argtypes = [vp, f64p, C.c_double, f64p, f64p]
+        L.ref_wall_loads_cpu.argtypes = [vp, C.c_double, C.c_double, C.c_double, f32p, f32p, f32p, f64p, C.c_double,
+                                         f64p, f64p]
         L.ref_import_topology.restype = vp
         L.ref_import_topology.argtypes = [C.POINTER(Topology)]
         L.ref_device_core_create.restype = vp
@@ -85,6 +87,7 @@ def lib():
         L.ref_device_core_destroy.argtypes = [vp]
         L.ref_device_core_initialize.argtypes = [vp, f64p]
         L.ref_device_core_step.argtypes = [vp, f64p]
+        L.ref_device_core_state.argtypes = [vp, f32p, f32p, f32p, f64p]
         L.ref_case_from_mesh.restype = vp
         L.ref_case_from_mesh.argtypes = [f64p, C.c_int64, C.POINTER(C.c_uint32), C.c_int64, f64p, f64p, C.c_double,
                                          C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double]
@@ -237,6 +240,16 @@ class RefCase:
                                         pressure_reference, ptr(o, C.c_double), ptr(out, C.c_double)))
         return out[:3], out[3:]
 
+    def wall_loads(self, state, nu, dt, rho, pressure, pressure_reference=0.0, origin=(0.0, 0.0, 0.0)):
+        """Pressure and viscous (smooth-wall) loads: (Fp, Mp, Fv, Mv)."""
+        x, y, z = self._state(*state)
+        out = np.zeros(12)
+        o = np.ascontiguousarray(origin, np.float64)
+        _check(lib().ref_wall_loads_cpu(self.handle, nu, dt, rho, ptr(x, C.c_float), ptr(y, C.c_float), ptr(z, C.c_float),
+                                        ptr(np.ascontiguousarray(pressure, np.float64), C.c_double), pressure_reference,
+                                        ptr(o, C.c_double), ptr(out, C.c_double)))
+        return out[0:3], out[3:6], out[6:9], out[9:12]
+
     def outflow_rate(self, u, v, w, cf, eb, external=True):
         out = C.c_double()
         _check(lib().ref_outflow_rate_cpu(self.handle, ptr(u, C.c_float), ptr(v, C.c_float), ptr(w, C.c_float),
@@ -319,7 +332,12 @@ class RefDeviceCore(RefCore):
         return self._stats(a)
 
     def state(self):
-        raise NotImplementedError
+        n = self.case.n
+        x, y, z = (np.zeros(n, np.float32) for _ in range(3))
+        p = np.zeros(n)
+        _check(lib().ref_device_core_state(self.handle, ptr(x, C.c_float), ptr(y, C.c_float), ptr(z, C.c_float),
+                                           ptr(p, C.c_double)))
+        return (x, y, z), p
 
     def close(self):
         if self.handle:

@@ -5,6 +5,7 @@
 // diagonal_cpu, composite_amr_*_cpu); this file only builds analytic fixtures, in the
 // pattern of the reference's tools/physics_contract_probe.cpp:19-67, and converts layouts.
 #include "ref_shim.h"
+#include "adapter/external_aero_core_b200.h"
 
 #include "core/fluid/amr_eb.h"
 #include "core/fluid/amr_pressure.h"
@@ -290,120 +291,13 @@ namespace
         AmrHierarchy hierarchy;
         AmrEmbeddedBoundaryAtlas atlas;
         CompositeAmrPressureSystem system;
-        // exported flat arrays
-        std::vector<pcfd_level> levels;
-        std::vector<std::vector<int32_t>> coord, neighbors, children;
-        std::vector<std::vector<double>> origin;
-        std::vector<std::vector<uint32_t>> flags;
-        std::vector<double> centroid;
-        struct Conn
-        {
-            std::vector<int32_t> coarse, fine, lower_node, upper_node;
-            std::vector<double> area, centre, normal_distance, face_centroid, factor, correction, weight;
-            std::vector<int8_t> axis, direction;
-        } cf, eb;
-        std::vector<int32_t> rc_lower, rc_upper, rc_level, rc_brick, rc_ijk, rc_lower_node, rc_upper_node;
-        std::vector<int8_t> rc_axis;
-        std::vector<double> rc_area, rc_delta, rc_correction, rc_weight;
-        std::vector<double> gradient_weight;
-        std::vector<int32_t> gauge_dof;
-        std::vector<double> gauge_coefficient;
-        std::vector<double> patch_area, patch_centroid, patch_normal;
-        std::vector<int32_t> patch_plus, patch_minus;
-        std::vector<int32_t> bf_dof;
-        std::vector<double> bf_area, bf_centroid;
-        std::vector<int32_t> retained;
+        // the flattened pcfd_topology (the adapter's view of hierarchy + system)
+        std::unique_ptr<paracfd_b200_adapter::TopologyView> view;
     };
-
-    void export_connections(const std::vector<CoarseFinePressureConnection>& in, RefCase::Conn& out)
-    {
-        for (const auto& e : in)
-        {
-            out.coarse.push_back(e.coarse_dof);
-            out.fine.push_back(e.fine_dof);
-            out.area.push_back(e.open_area);
-            out.centre.push_back(e.centre_distance);
-            out.normal_distance.push_back(e.normal_distance);
-            out.axis.push_back(e.axis);
-            out.direction.push_back(e.direction);
-            for (int a = 0; a < 3; ++a) out.face_centroid.push_back(e.face_centroid[a]);
-            out.factor.push_back(e.orthogonal_gradient_factor);
-            out.lower_node.push_back(e.lower_gradient_node);
-            out.upper_node.push_back(e.upper_gradient_node);
-            for (int a = 0; a < 3; ++a) out.correction.push_back(e.nonorthogonal_correction[a]);
-            out.weight.push_back(e.upper_gradient_weight);
-        }
-    }
-    pcfd_connections view_connections(RefCase::Conn& c)
-    {
-        pcfd_connections v{};
-        v.count = int32_t(c.coarse.size());
-        v.coarse_dof = c.coarse.data(); v.fine_dof = c.fine.data(); v.open_area = c.area.data();
-        v.centre_distance = c.centre.data(); v.normal_distance = c.normal_distance.data();
-        v.axis = c.axis.data(); v.direction = c.direction.data(); v.face_centroid = c.face_centroid.data();
-        v.orthogonal_gradient_factor = c.factor.data(); v.lower_gradient_node = c.lower_node.data();
-        v.upper_gradient_node = c.upper_node.data(); v.nonorthogonal_correction = c.correction.data();
-        v.upper_gradient_weight = c.weight.data();
-        return v;
-    }
 
     void export_case(RefCase& rc)
     {
-        const auto& levels = rc.hierarchy.levels();
-        const int L = int(levels.size());
-        rc.levels.resize(L);
-        rc.coord.resize(L); rc.neighbors.resize(L); rc.children.resize(L); rc.origin.resize(L); rc.flags.resize(L);
-        for (int l = 0; l < L; ++l)
-        {
-            const AmrLevel& lev = levels[l];
-            for (const BrickMetadata& b : lev.bricks)
-            {
-                rc.coord[l].insert(rc.coord[l].end(), {b.coord.x, b.coord.y, b.coord.z});
-                rc.origin[l].insert(rc.origin[l].end(), {b.origin.x, b.origin.y, b.origin.z});
-                for (int f = 0; f < 6; ++f) rc.neighbors[l].push_back(b.same_level_neighbor[f]);
-                for (int c = 0; c < 8; ++c) rc.children[l].push_back(b.children[c]);
-                rc.flags[l].push_back(b.flags);
-            }
-            pcfd_level& v = rc.levels[l];
-            v.h = lev.h;
-            v.brick_count = int32_t(lev.bricks.size());
-            v.level_offset = rc.system.level_offset[l];
-            v.coord = rc.coord[l].data();
-            v.origin = rc.origin[l].data();
-            v.neighbors = rc.neighbors[l].data();
-            v.flags = rc.flags[l].data();
-            v.children = rc.children[l].data();
-        }
-        const auto& s = rc.system;
-        for (const Vec3d& c : s.centroid) rc.centroid.insert(rc.centroid.end(), {c.x, c.y, c.z});
-        export_connections(s.coarse_fine, rc.cf);
-        export_connections(s.embedded, rc.eb);
-        for (const auto& r : s.regular_pressure_corrections)
-        {
-            rc.rc_lower.push_back(r.lower_dof); rc.rc_upper.push_back(r.upper_dof);
-            rc.rc_level.push_back(r.level); rc.rc_brick.push_back(r.brick);
-            rc.rc_ijk.insert(rc.rc_ijk.end(), {r.i, r.j, r.k});
-            rc.rc_axis.push_back(r.axis); rc.rc_area.push_back(r.open_area); rc.rc_delta.push_back(r.two_point_delta);
-            rc.rc_lower_node.push_back(r.lower_gradient_node); rc.rc_upper_node.push_back(r.upper_gradient_node);
-            for (int a = 0; a < 3; ++a) rc.rc_correction.push_back(r.nonorthogonal_correction[a]);
-            rc.rc_weight.push_back(r.upper_gradient_weight);
-        }
-        for (const Vec3d& w : s.pressure_gradient_weight) rc.gradient_weight.insert(rc.gradient_weight.end(), {w.x, w.y, w.z});
-        for (const auto& g : s.gauges) { rc.gauge_dof.push_back(g.dof); rc.gauge_coefficient.push_back(g.coefficient); }
-        for (const auto& p : s.surface_patches)
-        {
-            rc.patch_area.push_back(p.area);
-            rc.patch_centroid.insert(rc.patch_centroid.end(), {p.centroid.x, p.centroid.y, p.centroid.z});
-            rc.patch_normal.insert(rc.patch_normal.end(), {p.normal.x, p.normal.y, p.normal.z});
-            rc.patch_plus.push_back(p.plus_dof); rc.patch_minus.push_back(p.minus_dof);
-        }
-        for (const auto& f : s.boundary_faces)
-        {
-            rc.bf_dof.push_back(f.dof);
-            rc.bf_area.insert(rc.bf_area.end(), {f.outward_area.x, f.outward_area.y, f.outward_area.z});
-            rc.bf_centroid.insert(rc.bf_centroid.end(), {f.centroid.x, f.centroid.y, f.centroid.z});
-        }
-        rc.retained.assign(s.face_state_retained_dofs.begin(), s.face_state_retained_dofs.end());
+        rc.view = std::make_unique<paracfd_b200_adapter::TopologyView>(rc.hierarchy, rc.system);
     }
 
     // Compact per-brick face layout <-> reference ghosted AmrHostFields.
@@ -610,49 +504,18 @@ int ref_case_topology(void* handle, pcfd_topology* out)
 {
     return guarded([&] {
         RefCase& c = *static_cast<RefCase*>(handle);
-        const auto& s = c.system;
-        std::memset(out, 0, sizeof(*out));
-        out->brick_size = s.brick_size;
-        out->level_count = int32_t(c.levels.size());
-        out->levels = c.levels.data();
-        for (int a = 0; a < 3; ++a) { out->domain_lo[a] = c.hierarchy.domain().lo[a]; out->domain_hi[a] = c.hierarchy.domain().hi[a]; }
-        out->storage_size = s.storage_size;
-        out->pressure_outlet_xmax = s.pressure_outlet_xmax ? 1 : 0;
-        out->active = s.active.data();
-        out->freestream_connected = s.freestream_connected.data();
-        out->cut_face_mask = s.cut_face_mask.data();
-        out->volume = s.volume.data();
-        out->centroid = c.centroid.data();
-        out->preconditioner_aggregate = s.preconditioner_aggregate.data();
-        out->coarse_fine = view_connections(c.cf);
-        out->embedded = view_connections(c.eb);
-        pcfd_regular_corrections& r = out->regular;
-        r.count = int32_t(c.rc_lower.size());
-        r.lower_dof = c.rc_lower.data(); r.upper_dof = c.rc_upper.data(); r.level = c.rc_level.data();
-        r.brick = c.rc_brick.data(); r.ijk = c.rc_ijk.data(); r.axis = c.rc_axis.data();
-        r.open_area = c.rc_area.data(); r.two_point_delta = c.rc_delta.data();
-        r.lower_gradient_node = c.rc_lower_node.data(); r.upper_gradient_node = c.rc_upper_node.data();
-        r.nonorthogonal_correction = c.rc_correction.data(); r.upper_gradient_weight = c.rc_weight.data();
-        out->gradient_node_count = int32_t(s.pressure_gradient_dof.size());
-        out->gradient_dof = s.pressure_gradient_dof.data();
-        out->gradient_offset = s.pressure_gradient_offset.data();
-        out->gradient_neighbour = s.pressure_gradient_neighbour.data();
-        out->gradient_weight = c.gradient_weight.data();
-        out->gauge_count = int32_t(c.gauge_dof.size());
-        out->gauge_dof = c.gauge_dof.data();
-        out->gauge_coefficient = c.gauge_coefficient.data();
-        out->patches.count = int32_t(c.patch_area.size());
-        out->patches.area = c.patch_area.data(); out->patches.centroid = c.patch_centroid.data();
-        out->patches.normal = c.patch_normal.data(); out->patches.plus_dof = c.patch_plus.data();
-        out->patches.minus_dof = c.patch_minus.data();
-        out->boundary_faces.count = int32_t(c.bf_dof.size());
-        out->boundary_faces.dof = c.bf_dof.data(); out->boundary_faces.outward_area = c.bf_area.data();
-        out->boundary_faces.centroid = c.bf_centroid.data();
-        out->retained_count = int32_t(c.retained.size());
-        out->retained_dofs = c.retained.data();
+        *out = c.view->topology;
     });
 }
-
+int ref_case_objects(void* handle, const void** hierarchy, const void** system, const void** config)
+{
+    return guarded([&] {
+        RefCase& c = *static_cast<RefCase*>(handle);
+        if (hierarchy) *hierarchy = &c.hierarchy;
+        if (system) *system = &c.system;
+        if (config) *config = &c.config;
+    });
+}
 int ref_case_summary(void* handle, int64_t* o)
 {
     return guarded([&] {
@@ -837,6 +700,31 @@ int ref_wall_cpu(void* handle, double nu, double dt, double rho, float* x, float
         if (forces)
             for (std::size_t q = 0; q < loads.size(); ++q)
                 for (int a = 0; a < 3; ++a) forces[3 * q + a] = loads[q].force[a];
+    });
+}
+
+int ref_wall_loads_cpu(void* handle, double nu, double dt, double rho, const float* x, const float* y, const float* z,
+                       const double* pressure, double pref, const double* origin, double* out12)
+{
+    return guarded([&] {
+        RefCase& c = *static_cast<RefCase*>(handle);
+        CompositeCellMomentumState st = state_from(c, x, y, z);
+        const auto wall = apply_composite_cell_smooth_fabric_wall_cpu(c.system, nu, dt, rho, st);
+        std::vector<double> p(pressure, pressure + c.system.storage_size);
+        FreestreamConfig fs;
+        fs.rho = rho;
+        AeroReferenceConfig rf;
+        rf.moment_origin = {origin[0], origin[1], origin[2]};
+        // (ExternalAeroCore::aerodynamic_loads: pressure loads, then the wall model's patch loads)
+        auto loads = compute_pressure_loads(c.system, p, c.wing.triangle_count() + 1, fs, rf, pref);
+        accumulate_viscous_loads(loads, wall, fs, rf);
+        for (int a = 0; a < 3; ++a)
+        {
+            out12[a] = loads.pressure_force[a];
+            out12[3 + a] = loads.pressure_moment[a];
+            out12[6 + a] = loads.viscous_force[a];
+            out12[9 + a] = loads.viscous_moment[a];
+        }
     });
 }
 
@@ -1292,6 +1180,21 @@ int ref_core_step(void* core, double* stats)
     return guarded([&] { fill_stats(static_cast<RefCore*>(core)->core->step(), stats); });
 }
 
+int ref_device_core_state(void* handle, float* x, float* y, float* z, double* pressure)
+{
+    return guarded([&] {
+        RefDeviceCore& k = *static_cast<RefDeviceCore*>(handle);
+        CompositeCellMomentumState st;
+        k.momentum->download_state(st);
+        state_to(st, x, y, z);
+        if (pressure)
+        {
+            std::vector<Real> p;
+            k.projection->download_pressure(p);
+            for (std::size_t q = 0; q < p.size(); ++q) pressure[q] = double(p[q]);
+        }
+    });
+}
 int ref_core_state(void* core, float* x, float* y, float* z, double* pressure)
 {
     return guarded([&] {

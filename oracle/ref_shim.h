@@ -38,6 +38,9 @@ void ref_case_destroy(void* handle);
 const char* ref_last_error(void);
 /* Fills a topology view whose arrays live inside the handle. */
 int ref_case_topology(void* handle, pcfd_topology* out);
+/* The case's reference objects (AmrHierarchy, CompositeAmrPressureSystem, ParagliderConfig), for
+ * C++ drivers compiled against the reference headers (oracle/adapter/adapter_probe.cpp). */
+int ref_case_objects(void* handle, const void** hierarchy, const void** system, const void** config);
 /* Summary numbers: [levels, storage, active dofs, coarse_fine, embedded, regular corr,
  * gradient nodes, gauges, patches, boundary faces, unresolved cells, retained] */
 int ref_case_summary(void* handle, int64_t* out12);
@@ -75,6 +78,11 @@ int ref_reconstruct_cpu(void* handle, const float* x, const float* y, const floa
 int ref_outflow_rate_cpu(void* handle, const float* u, const float* v, const float* w, const double* cf,
                          const double* eb, int external, double* rate);
 
+/* The smooth-wall twin on a copy of the state x,y,z, then compute_pressure_loads of `pressure` and
+ * accumulate_viscous_loads of the wall's patch loads (aero_loads.cpp:183-204), as
+ * ExternalAeroCore::aerodynamic_loads combines them: out = [Fp(3), Mp(3), Fv(3), Mv(3)]. */
+int ref_wall_loads_cpu(void* handle, double nu, double dt, double rho, const float* x, const float* y, const float* z,
+                       const double* pressure, double pressure_reference, const double* origin, double* out12);
 /* compute_pressure_loads (aero_loads.cpp:183-195) of a DOF pressure vector: out = [F(3), M(3)]. */
 int ref_pressure_loads(void* handle, const double* pressure, double pressure_reference, const double* origin,
                        double* out6);
@@ -113,6 +121,9 @@ void* ref_device_core_create(void* case_handle, const ref_core_case* config, dou
 void ref_device_core_destroy(void* core);
 int ref_device_core_initialize(void* core, double* stats6);
 int ref_device_core_step(void* core, double* stats6);
+
+/* Cell-momentum state [S] (FP32) and the FP32 pressure shadow widened to double [S]. */
+int ref_device_core_state(void* core, float* x, float* y, float* z, double* pressure);
 
 /* The reference's own GPU path (ExternalAeroCore on the fixture), for the sm_100a baseline arm. */
 void* ref_core_create(void* case_handle, const ref_core_case* config);

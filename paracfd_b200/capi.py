@@ -222,6 +222,7 @@ SIGNATURES = {
     "pcfd_learned_evaluate_host": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_float),
                                              C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_float)]),
     "pcfd_learned_apply_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "pcfd_learned_set_wait": (C.c_int, [C.c_void_p, C.c_double, C.c_int32]),
 }
 
 _lib = None

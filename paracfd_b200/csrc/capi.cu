@@ -293,6 +293,15 @@ namespace pcfd
             require(src != nullptr || n == 0, "null host buffer");
             if (n) cuda_check(cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyHostToDevice, s.stream), "host to device");
         }
+        // Host inputs of the state setters are rejected when any entry is NaN or infinite, before
+        // anything reaches the device (the reference checks its velocities before each step,
+        // external_aero_core.cpp:308).
+        template <class T> void require_finite(const T* src, size_t n, const char* what)
+        {
+            if (!src) return;
+            for (size_t q = 0; q < n; ++q)
+                if (!std::isfinite(src[q])) throw Error(PCFD_INVALID_ARG, std::string("non-finite ") + what + " at entry " + std::to_string(q));
+        }
         template <class T> void d2h(System& s, T* dst, const T* src, size_t n)
         {
             require(dst != nullptr || n == 0, "null host buffer");
@@ -430,6 +439,8 @@ pcfd_status pcfd_pressure_solve_host(pcfd_system* system, double* x, const doubl
     return guarded([&] {
         System& s = sys(system);
         require(tolerance > 0 && max_iterations >= 0, "invalid solve tolerance or iteration budget");
+        require_finite(b, size_t(s.S), "right-hand side");
+        if (warm_start) require_finite(x, size_t(s.S), "initial guess");
         h2d(s, s.scratch_p.p, b, size_t(s.S));
         if (warm_start) h2d(s, s.scratch_out.p, x, size_t(s.S));
         const pcfd_solve_result r = solve(s, s.scratch_out, s.scratch_p, tolerance, max_iterations, warm_start != 0);
@@ -443,6 +454,9 @@ pcfd_status pcfd_set_faces_host(pcfd_system* system, const float* u, const float
 {
     return guarded([&] {
         System& s = sys(system);
+        require_finite(u, size_t(s.faces), "face velocity u");
+        require_finite(v, size_t(s.faces), "face velocity v");
+        require_finite(w, size_t(s.faces), "face velocity w");
         h2d(s, s.u.p, u, size_t(s.faces)); h2d(s, s.v.p, v, size_t(s.faces)); h2d(s, s.w.p, w, size_t(s.faces));
         sync(s);
     });
@@ -459,6 +473,8 @@ pcfd_status pcfd_set_special_host(pcfd_system* system, const float* cf, const fl
 {
     return guarded([&] {
         System& s = sys(system);
+        require_finite(cf, size_t(s.cf_count), "coarse/fine velocity");
+        require_finite(eb, size_t(s.eb_count), "embedded velocity");
         h2d(s, s.special.p, cf, size_t(s.cf_count));
         h2d(s, s.special.p + s.cf_count, eb, size_t(s.eb_count));
         sync(s);
@@ -477,7 +493,7 @@ pcfd_status pcfd_set_pressure_host(pcfd_system* system, const double* p)
 {
     return guarded([&] {
         System& s = sys(system);
-        for (int q = 0; q < s.S; ++q) require(std::isfinite(p[q]), "non-finite pressure state");
+        require_finite(p, size_t(s.S), "pressure state");
         h2d(s, s.pressure.p, p, size_t(s.S));
         launch_convert_pressure(s);
         sync(s);
@@ -560,6 +576,9 @@ pcfd_status pcfd_momentum_set_state_host(pcfd_system* system, const float* x, co
     return guarded([&] {
         System& s = sys(system);
         Momentum& m = momentum_of(s);
+        require_finite(x, size_t(s.S), "cell momentum x");
+        require_finite(y, size_t(s.S), "cell momentum y");
+        require_finite(z, size_t(s.S), "cell momentum z");
         h2d(s, m.x.p, x, size_t(s.S)); h2d(s, m.y.p, y, size_t(s.S)); h2d(s, m.z.p, z, size_t(s.S));
         h2d(s, m.xn.p, x, size_t(s.S)); h2d(s, m.yn.p, y, size_t(s.S)); h2d(s, m.zn.p, z, size_t(s.S));
         sync(s);
@@ -673,10 +692,19 @@ pcfd_status pcfd_core_configure(pcfd_system* system, const pcfd_case* config)
         require(c.speed >= 0 && c.rho > 0 && c.nu >= 0 && c.cfl > 0 && c.smagorinsky_cs >= 0 && c.projection_tolerance > 0 &&
                     c.projection_max_iterations > 0,
                 "invalid case configuration");
+        // a new flow case needs a new initialization; changing only the projection tolerance or
+        // iteration budget keeps the initialized state and the physical time
+        const pcfd_case& o = s.config;
+        const bool same_flow = s.configured && o.speed == c.speed && o.rho == c.rho && o.nu == c.nu && o.cfl == c.cfl &&
+                               o.smagorinsky_cs == c.smagorinsky_cs && o.smooth_wall == c.smooth_wall &&
+                               o.pressure_impulse == c.pressure_impulse;
         s.config = c;
         s.configured = true;
-        s.initialized = false;
-        s.physical_time = 0.0;
+        if (!same_flow)
+        {
+            s.initialized = false;
+            s.physical_time = 0.0;
+        }
     });
 }
 
@@ -725,6 +753,7 @@ pcfd_status pcfd_core_set_inflow_host(pcfd_system* system, const float* normal_v
         System& s = sys(system);
         if (count == 0) { s.inflow_set = false; return; }
         require(count == s.inflow_faces, "inflow count must equal the X-min boundary face count");
+        require_finite(normal_velocity, size_t(count), "inflow velocity");
         h2d(s, s.inflow.p, normal_velocity, size_t(count));
         s.inflow_set = true;
     });
@@ -835,6 +864,11 @@ pcfd_status pcfd_learned_evaluate_host(pcfd_system* system, int32_t samples, con
         const double l = learned_evaluate(s, samples, inputs, targets, zhat, gradients);
         if (loss) *loss = l;
     });
+}
+
+pcfd_status pcfd_learned_set_wait(pcfd_system* system, double seconds, int32_t idle_barrier_once)
+{
+    return guarded([&] { learned_set_wait(sys(system), seconds, idle_barrier_once != 0); });
 }
 
 pcfd_status pcfd_learned_apply_device(pcfd_system* system, const double* d_r, double* d_z)

@@ -49,7 +49,10 @@ namespace pcfd
         constexpr int64_t kParams = kWeights + kHead;
         static_assert(kParams == 179728, "parameter count must match oracle/unet.py");
 
-        constexpr uint64_t kMaxWaitNs = 2000000000ull;   // a tensor-core wait gives up after 2 s
+        // A tensor-core wait gives up after the system's wait limit (pcfd_learned_set_wait, 2 s by
+        // default); after a wait gave up, the kernel drains its last commit with this fixed limit
+        // before freeing its tensor memory.
+        constexpr uint64_t kMaxWaitNs = 2000000000ull;
 
         // ---- geometry of one level's staged group of bricks ----
         // N: brick edge; XP: padded edge; NB: bricks per CTA; G: positions between the 8-row
@@ -157,8 +160,8 @@ namespace pcfd
             asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
             return t;
         }
-        // polls the barrier phase with the given parity; false after kMaxWaitNs nanoseconds
-        __device__ inline bool barrier_wait(uint64_t* bar, uint32_t parity)
+        // polls the barrier phase with the given parity; false after limit_ns nanoseconds
+        __device__ inline bool barrier_wait(uint64_t* bar, uint32_t parity, uint64_t limit_ns)
         {
             const uint32_t a = smem_u32(bar);
             const uint64_t start = global_ns();
@@ -173,7 +176,7 @@ namespace pcfd
                     : "r"(a), "r"(parity)
                     : "memory");
                 if (done) return true;
-                if (global_ns() - start > kMaxWaitNs) return false;
+                if (global_ns() - start > limit_ns) return false;
             }
         }
         __device__ inline void tmem_alloc(uint32_t* slot, uint32_t cols)
@@ -235,6 +238,8 @@ namespace pcfd
             int sources, cout, samples, relu, out_fp32;
             void* y;           // [samples][N^3][cout], BF16 or FP32
             int* error;        // set to 1 when a barrier wait gave up
+            uint64_t wait_ns;  // limit of each tensor-core wait
+            int idle_wait;     // 1: the first wait polls a barrier that no commit completes (fault-path check)
         };
 
         __host__ __device__ constexpr int tmem_columns(int cols)
@@ -295,12 +300,13 @@ namespace pcfd
             uint4* Bw = A + 2 * Gm::NPOS;
             uint64_t* bar = reinterpret_cast<uint64_t*>(Bw + 27 * 2 * cout);
             uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+            uint64_t* idle = bar + 2;      // initialised, never arrived on
             __shared__ int failed;
             const int tid = threadIdx.x, warp = tid >> 5;
             const uint32_t cols = tmem_columns(Gm::T * cout);
 
             for (int i = tid; i < 2 * Gm::NPOS; i += 128) A[i] = make_uint4(0, 0, 0, 0);
-            if (tid == 0) { barrier_init(bar); failed = 0; }
+            if (tid == 0) { barrier_init(bar); barrier_init(idle); failed = 0; }
             if (warp == 0) tmem_alloc(tslot, cols);
             fence_before_sync();
             __syncthreads();
@@ -370,7 +376,8 @@ namespace pcfd
                             mma_commit(bar);
                         }
                         first = false;
-                        if (!barrier_wait(bar, phase)) failed = 1;
+                        const bool done = p.idle_wait ? barrier_wait(idle, 0, p.wait_ns) : barrier_wait(bar, phase, p.wait_ns);
+                        if (!done) failed = 1;
                         phase ^= 1;
                         __syncthreads();
                         if (failed) break;
@@ -414,8 +421,9 @@ namespace pcfd
             if (failed)
             {
                 if (tid == 0) atomicExch(p.error, 1);
-                // the last commit has not been seen: give the tensor core one more bounded wait
-                barrier_wait(bar, phase ^ 1);
+                // the last commit has not been seen: wait for it (fixed bound) before the tensor
+                // memory its MMAs write is freed
+                barrier_wait(bar, phase ^ 1, kMaxWaitNs);
             }
             fence_before_sync();
             __syncthreads();
@@ -424,7 +432,7 @@ namespace pcfd
 
         template <int N> size_t conv_smem(int cout)
         {
-            const size_t bytes = size_t(2) * Geometry<N>::NPOS * 16 + size_t(27) * 2 * cout * 16 + 16;
+            const size_t bytes = size_t(2) * Geometry<N>::NPOS * 16 + size_t(27) * 2 * cout * 16 + 32;
             // co-resident CTAs must fit their TMEM allocations into the SM's 512 columns
             const int cols = tmem_columns(Geometry<N>::T * cout);
             const size_t floor_bytes = cols == 512 ? 116 * 1024 : cols == 256 ? 80 * 1024 : cols == 128 ? 48 * 1024 : 0;
@@ -822,6 +830,8 @@ namespace pcfd
         DBuf<float> scalars;        // [0] count, [1] loss
         DBuf<int> error;
         bool harvesting = false;
+        uint64_t wait_ns = kMaxWaitNs;   // limit of each tensor-core wait
+        bool idle_wait_once = false;     // the next convolution's first wait runs out (fault-path check)
     };
 
     namespace
@@ -900,6 +910,9 @@ namespace pcfd
             p.out_fp32 = fp32;
             p.y = y;
             p.error = L.error;
+            p.wait_ns = L.wait_ns;
+            p.idle_wait = L.idle_wait_once ? 1 : 0;
+            L.idle_wait_once = false;
             const size_t smem = conv_smem<N>(cout);
             static size_t configured[3] = {0, 0, 0};
             const int slot = N == 8 ? 0 : N == 4 ? 1 : 2;
@@ -1070,6 +1083,14 @@ namespace pcfd
     void learned_check(System& s)
     {
         if (s.learned) check_error(s, *s.learned);
+    }
+
+    void learned_set_wait(System& s, double seconds, bool idle_barrier_once)
+    {
+        require(seconds > 0 && seconds <= 60, "learned: wait limit must be in (0, 60] s");
+        Learned& L = state(s);
+        L.wait_ns = uint64_t(seconds * 1e9);
+        L.idle_wait_once = idle_barrier_once;
     }
 
     void learned_harvest_begin(System& s, int capacity_pairs, int per_pair, uint64_t seed, int target)

@@ -183,6 +183,7 @@ namespace pcfd
         cudaStream_t stream = nullptr;
         bool own_stream = false;
         int device = 0;
+        double* noalloc_gradient = nullptr;     // static scratch of the allocation-free apply (pressure.cu), once looked up
 
         // host copies of topology needed after setup
         std::vector<double> level_h;
@@ -351,6 +352,7 @@ namespace pcfd
     void learned_get_parameters(System& s, float* host, int64_t count);
     void learned_apply(System& s, const double* r, double* z);
     void learned_check(System& s);   // throws PCFD_TIMEOUT when a tensor-core wait gave up
+    void learned_set_wait(System& s, double seconds, bool idle_barrier_once);
     void learned_harvest_begin(System& s, int capacity_pairs, int per_pair, uint64_t seed, int target);
     int64_t learned_harvest_stop(System& s);
     bool learned_harvesting(const System& s);

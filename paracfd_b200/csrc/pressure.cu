@@ -17,7 +17,6 @@
 #include <cstring>
 #include <limits>
 #include <numeric>
-#include <mutex>
 #include <unordered_map>
 
 namespace pcfd
@@ -516,8 +515,13 @@ namespace pcfd
     // Limits and contract:
     //   * at most kNoAllocGradientNodes WLS gradient nodes (262,144 nodes, 6 MiB of scratch);
     //     larger systems are rejected with PCFD_INVALID_ARG before anything is launched;
-    //   * the first call on a device looks up the scratch address with the device current;
-    //     make that first call before any stream capture;
+    //   * the first call through a system that needs the WLS term (not orthogonal-only, gradient
+    //     nodes present) looks up the scratch address with cudaGetSymbolAddress, the system's
+    //     device current, and keeps it in the system; make that first call before any stream
+    //     capture.  Orthogonal-only calls and systems without gradient nodes never look it up.
+    //     The address lives as long as the device context, which outlives every system on it (a
+    //     cudaDeviceReset invalidates the systems too; they are created again, and look it up
+    //     again);
     //   * the scratch is shared by every system on the device: calls that overlap in time (other
     //     threads or other streams) race on it -- serialise them;
     //   * no scratch entry needs to start at zero: the gradient kernel writes all 3 components
@@ -529,27 +533,21 @@ namespace pcfd
         constexpr int kNoAllocGradientNodes = 1 << 18;
         static __device__ __align__(256) double g_noalloc_gradient[3 * kNoAllocGradientNodes];
 
-        constexpr int kNoAllocMaxDevices = 64;
-        std::mutex g_noalloc_mutex;
-        double* g_noalloc_scratch[kNoAllocMaxDevices] = {};
-
-        // One-time, per-device lookup of the static scratch with that device current.
-        double* noalloc_scratch(int device)
+        // The static scratch's device address, looked up once per system with its device current.
+        double* noalloc_scratch(System& s)
         {
-            require(device >= 0 && device < kNoAllocMaxDevices, "device ordinal out of range");
-            std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-            if (!g_noalloc_scratch[device])
+            if (!s.noalloc_gradient)
             {
                 int current = 0;
                 cuda_check(cudaGetDevice(&current), "cudaGetDevice");
-                if (current != device) cuda_check(cudaSetDevice(device), "cudaSetDevice");
+                if (current != s.device) cuda_check(cudaSetDevice(s.device), "cudaSetDevice");
                 void* ptr = nullptr;
                 const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_gradient);
-                if (current != device) cudaSetDevice(current);
+                if (current != s.device) cudaSetDevice(current);
                 cuda_check(e, "cudaGetSymbolAddress(noalloc gradient scratch)");
-                g_noalloc_scratch[device] = static_cast<double*>(ptr);
+                s.noalloc_gradient = static_cast<double*>(ptr);
             }
-            return g_noalloc_scratch[device];
+            return s.noalloc_gradient;
         }
     }
 
@@ -560,7 +558,7 @@ namespace pcfd
             throw Error(PCFD_INVALID_ARG, "pcfd_pressure_apply_device_noalloc: " + std::to_string(o.gradient_nodes) +
                                               " WLS gradient nodes exceed the static scratch maximum of " +
                                               std::to_string(kNoAllocGradientNodes));
-        double* gradient = noalloc_scratch(s.device);
+        double* gradient = !orthogonal_only && o.gradient_nodes ? noalloc_scratch(s) : nullptr;
         if (s.active_bricks)
         {
             if (s.fine.enabled && aligned16(p) && aligned16(out)) brick_apply(s, p, out);

@@ -28,46 +28,86 @@ namespace pcfd
 {
     namespace
     {
-        struct HostEdge { int a, b; double coefficient; };
-        struct HostLevel
+        // One level of an aggregation hierarchy, assembled on the host: a weighted graph
+        // Laplacian (the couplings) plus a non-negative sink per cell, the part of the row that no
+        // coupling represents (outlet and gauge terms).  Keeping the sink explicit gives every
+        // coarser diagonal as a plain sum, with no subtraction of nearly equal numbers.
+        struct Coupling { int lo, hi; double weight; };
+        struct GraphLevel
         {
             int cells = 0;
-            std::vector<std::array<int, 3>> coordinate;
-            std::vector<double> diagonal;
-            std::vector<HostEdge> edges;
-            std::vector<int> aggregate, restrict_offset, restrict_dof, row_offset, neighbour;
-            std::vector<double> coefficient;
+            std::vector<double> sink, diagonal;       // diagonal = sink + incident coupling weights
+            std::vector<Coupling> couplings;          // lo < hi, sorted, each pair once
+            std::vector<int> row_offset, neighbour;   // symmetric CSR of the couplings
+            std::vector<double> weight;
+            std::vector<int> parent;                  // cell of the next coarser level (empty on the coarsest)
+            std::vector<int> member_offset, member;   // members of each next-level cell (restriction)
         };
 
-        void finalize_level(HostLevel& level)
+        // Members of each group of `map` (entries < 0 belong to none) as CSR over [0, groups), each
+        // group's members in ascending order.
+        void group_members(const std::vector<int>& map, int groups, std::vector<int>& offset, std::vector<int>& member)
         {
-            level.row_offset.assign(size_t(level.cells) + 1, 0);
-            for (const HostEdge& e : level.edges) { ++level.row_offset[e.a + 1]; ++level.row_offset[e.b + 1]; }
-            for (int q = 0; q < level.cells; ++q) level.row_offset[q + 1] += level.row_offset[q];
-            level.neighbour.resize(level.row_offset.back());
-            level.coefficient.resize(level.row_offset.back());
-            std::vector<int> cursor = level.row_offset;
-            for (const HostEdge& e : level.edges)
+            offset.assign(size_t(groups) + 1, 0);
+            for (const int g : map)
+                if (g >= 0) ++offset[size_t(g) + 1];
+            for (int g = 0; g < groups; ++g) offset[size_t(g) + 1] += offset[size_t(g)];
+            member.resize(size_t(offset.back()));
+            std::vector<int> fill(offset.begin(), offset.end() - 1);
+            for (int q = 0; q < int(map.size()); ++q)
+                if (map[q] >= 0) member[size_t(fill[size_t(map[q])]++)] = q;
+        }
+
+        // Merges the coupling records of `level` by cell pair, then derives the diagonal and the
+        // CSR rows.  `records` holds (lo, hi, weight) with lo < hi, in any order and repeated.
+        void assemble(GraphLevel& level, std::vector<Coupling>& records)
+        {
+            std::sort(records.begin(), records.end(),
+                      [](const Coupling& x, const Coupling& y) { return x.lo != y.lo ? x.lo < y.lo : x.hi < y.hi; });
+            level.couplings.clear();
+            for (const Coupling& r : records)
             {
-                int slot = cursor[e.a]++;
-                level.neighbour[slot] = e.b; level.coefficient[slot] = e.coefficient;
-                slot = cursor[e.b]++;
-                level.neighbour[slot] = e.a; level.coefficient[slot] = e.coefficient;
+                if (!level.couplings.empty() && level.couplings.back().lo == r.lo && level.couplings.back().hi == r.hi)
+                    level.couplings.back().weight += r.weight;
+                else
+                    level.couplings.push_back(r);
+            }
+            level.diagonal = level.sink;
+            std::vector<int> degree(size_t(level.cells), 0);
+            for (const Coupling& c : level.couplings)
+            {
+                level.diagonal[size_t(c.lo)] += c.weight;
+                level.diagonal[size_t(c.hi)] += c.weight;
+                ++degree[size_t(c.lo)];
+                ++degree[size_t(c.hi)];
+            }
+            level.row_offset.assign(size_t(level.cells) + 1, 0);
+            for (int q = 0; q < level.cells; ++q) level.row_offset[size_t(q) + 1] = level.row_offset[size_t(q)] + degree[size_t(q)];
+            level.neighbour.resize(size_t(level.row_offset.back()));
+            level.weight.resize(size_t(level.row_offset.back()));
+            std::vector<int> fill(level.row_offset.begin(), level.row_offset.end() - 1);
+            for (const Coupling& c : level.couplings)
+            {
+                int slot = fill[size_t(c.lo)]++;
+                level.neighbour[size_t(slot)] = c.hi;
+                level.weight[size_t(slot)] = c.weight;
+                slot = fill[size_t(c.hi)]++;
+                level.neighbour[size_t(slot)] = c.lo;
+                level.weight[size_t(slot)] = c.weight;
             }
         }
 
-        template <class T> void upload_level(MgLevel<T>& d, const HostLevel& h)
+        template <class T> void upload_level(MgLevel<T>& d, const GraphLevel& h)
         {
             d.cells = h.cells;
             d.row_offset.upload(h.row_offset);
             d.neighbour.upload(h.neighbour);
-            std::vector<T> coefficient(h.coefficient.begin(), h.coefficient.end()), diagonal(h.diagonal.begin(), h.diagonal.end());
-            d.coefficient.upload(coefficient);
-            d.diagonal.upload(diagonal);
+            d.coefficient.upload(std::vector<T>(h.weight.begin(), h.weight.end()));
+            d.diagonal.upload(std::vector<T>(h.diagonal.begin(), h.diagonal.end()));
             d.rhs.alloc(h.cells); d.x.alloc(h.cells); d.temporary.alloc(h.cells); d.residual.alloc(h.cells);
-            d.aggregate.upload(h.aggregate);
-            d.restrict_offset.upload(h.restrict_offset);
-            d.restrict_dof.upload(h.restrict_dof);
+            d.aggregate.upload(h.parent);
+            d.restrict_offset.upload(h.member_offset);
+            d.restrict_dof.upload(h.member);
         }
 
         double connection_factor(const pcfd_connections& c, int e)
@@ -75,219 +115,10 @@ namespace pcfd
             const double f = c.orthogonal_gradient_factor[e];
             return f > 0 ? f : (c.normal_distance[e] > 0 ? 1.0 / c.normal_distance[e] : 0.0);
         }
-    }
 
-    void build_multigrid(System& s, const pcfd_topology& t, const std::vector<double>& diagonal)
-    {
-        (void)diagonal;
-        const int bs = t.brick_size, c3 = bs * bs * bs;
-        const pcfd_level& base = t.levels[0];
-        s.base_offset = base.level_offset;
-        s.base_cells = base.brick_count * c3;
-        const int n = t.storage_size, base_cells = s.base_cells, base_offset = s.base_offset;
-        const int32_t* agg = t.preconditioner_aggregate;
-
-        // aggregate restriction CSR (active DOFs grouped by level-0 cell, DOF order kept)
-        std::vector<int> roff(size_t(base_cells) + 1, 0);
-        for (int q = 0; q < n; ++q)
-            if (t.active[q]) { const int c = agg[q] - base_offset; if (c >= 0 && c < base_cells) ++roff[c + 1]; }
-        for (int c = 0; c < base_cells; ++c) roff[c + 1] += roff[c];
-        std::vector<int> rdof(roff.back()), cursor = roff;
-        for (int q = 0; q < n; ++q)
-            if (t.active[q]) { const int c = agg[q] - base_offset; if (c >= 0 && c < base_cells) rdof[cursor[c]++] = q; }
-        s.base_restrict_offset.upload(roff);
-        s.base_restrict_dof.upload(rdof);
-
-        auto global_coord = [&](int coarse) {
-            const int brick = coarse / c3, local = coarse % c3;
-            return std::array<int, 3>{base.coord[3 * brick] * bs + local % bs, base.coord[3 * brick + 1] * bs + (local / bs) % bs,
-                                      base.coord[3 * brick + 2] * bs + local / (bs * bs)};
-        };
-        std::vector<double> positive(size_t(base_cells) * 3, 0.0), cdiag(base_cells, 0.0);
-        std::vector<HostEdge> extra;
-        auto add_coarse_edge = [&](int a, int b, double coefficient) {
-            if (a < 0 || b < 0 || a == b || !t.active[a] || !t.active[b] || !(coefficient > 0)) return;
-            const int ca = agg[a] - base_offset, cb = agg[b] - base_offset;
-            if (ca < 0 || cb < 0 || ca >= base_cells || cb >= base_cells || ca == cb) return;
-            const auto ga = global_coord(ca), gb = global_coord(cb);
-            int axis = -1, manhattan = 0;
-            for (int d = 0; d < 3; ++d) { const int delta = gb[d] - ga[d]; manhattan += std::abs(delta); if (delta) axis = d; }
-            if (manhattan == 1 && axis >= 0) { const int lo = ga[axis] < gb[axis] ? ca : cb; positive[size_t(lo) * 3 + axis] += coefficient; }
-            else extra.push_back({ca, cb, coefficient});
-            cdiag[ca] += coefficient;
-            cdiag[cb] += coefficient;
-        };
-        // structured same-level faces in the reference's traversal order
-        for (int l = 0; l < t.level_count; ++l)
-        {
-            const pcfd_level& lev = t.levels[l];
-            const double coefficient = lev.h;
-            for (int brick = 0; brick < lev.brick_count; ++brick)
-            {
-                if (lev.flags[brick] & PCFD_BRICK_COVERED) continue;
-                for (int k = 0; k < bs; ++k)
-                    for (int j = 0; j < bs; ++j)
-                        for (int i = 0; i < bs; ++i)
-                        {
-                            const int a = lev.level_offset + brick * c3 + (k * bs + j) * bs + i;
-                            if (!t.active[a]) continue;
-                            for (int axis = 0; axis < 3; ++axis)
-                            {
-                                if (t.cut_face_mask[a] & (1u << axis)) continue;
-                                int c[3] = {i, j, k}, b = -1;
-                                if (++c[axis] < bs) b = lev.level_offset + brick * c3 + (c[2] * bs + c[1]) * bs + c[0];
-                                else
-                                {
-                                    const int nb = lev.neighbors[brick * 6 + 2 * axis + 1];
-                                    if (nb >= 0 && !(lev.flags[nb] & PCFD_BRICK_COVERED)) { c[axis] = 0; b = lev.level_offset + nb * c3 + (c[2] * bs + c[1]) * bs + c[0]; }
-                                }
-                                add_coarse_edge(a, b, coefficient);
-                            }
-                            if (t.pressure_outlet_xmax && (lev.flags[brick] & PCFD_BRICK_XMAX) && i == bs - 1)
-                            {
-                                const int cc = agg[a] - base_offset;
-                                if (cc >= 0 && cc < base_cells) cdiag[cc] += 2.0 * lev.h;
-                            }
-                        }
-            }
-        }
-        for (int e = 0; e < t.coarse_fine.count; ++e)
-            add_coarse_edge(t.coarse_fine.coarse_dof[e], t.coarse_fine.fine_dof[e], t.coarse_fine.open_area[e] * connection_factor(t.coarse_fine, e));
-        for (int e = 0; e < t.embedded.count; ++e)
-            add_coarse_edge(t.embedded.coarse_dof[e], t.embedded.fine_dof[e], t.embedded.open_area[e] * connection_factor(t.embedded, e));
-        for (int e = 0; e < t.regular.count; ++e)
-            add_coarse_edge(t.regular.lower_dof[e], t.regular.upper_dof[e], t.regular.open_area[e] * t.regular.two_point_delta[e]);
-        for (int g = 0; g < t.gauge_count; ++g)
-        {
-            const int cc = agg[t.gauge_dof[g]] - base_offset;
-            if (cc >= 0 && cc < base_cells) cdiag[cc] += t.gauge_coefficient[g];
-        }
-
-        HostLevel first;
-        first.cells = base_cells;
-        first.diagonal = std::move(cdiag);
-        first.coordinate.resize(base_cells);
-        for (int q = 0; q < base_cells; ++q) first.coordinate[q] = global_coord(q);
-        for (int q = 0; q < base_cells; ++q)
-        {
-            const int brick = q / c3, local = q % c3, i = local % bs, j = (local / bs) % bs, k = local / (bs * bs);
-            for (int axis = 0; axis < 3; ++axis)
-            {
-                const double coefficient = positive[size_t(q) * 3 + axis];
-                if (!(coefficient > 0)) continue;
-                int c[3] = {i, j, k}, other = -1;
-                if (++c[axis] < bs) other = brick * c3 + (c[2] * bs + c[1]) * bs + c[0];
-                else
-                {
-                    const int nb = base.neighbors[brick * 6 + 2 * axis + 1];
-                    if (nb >= 0) { c[axis] = 0; other = nb * c3 + (c[2] * bs + c[1]) * bs + c[0]; }
-                }
-                if (other < 0) throw Error(PCFD_INTERNAL, "multigrid base face has no geometric neighbour");
-                first.edges.push_back({q, other, coefficient});
-            }
-        }
-        first.edges.insert(first.edges.end(), extra.begin(), extra.end());
-
-        std::vector<HostLevel> host;
-        HostLevel current = std::move(first);
-        for (;;)
-        {
-            int active_cells = 0;
-            for (double v : current.diagonal) if (v > 0) ++active_cells;
-            if (active_cells <= 512 || host.size() >= 8) { finalize_level(current); host.push_back(std::move(current)); break; }
-            std::vector<int> parent(current.cells, -1);
-            for (int q = 0; q < current.cells; ++q) if (current.diagonal[q] > 0) parent[q] = q;
-            auto root = [&](int q) {
-                int r = q;
-                while (parent[r] != r) r = parent[r];
-                while (parent[q] != q) { const int next = parent[q]; parent[q] = r; q = next; }
-                return r;
-            };
-            for (const HostEdge& e : current.edges)
-            {
-                const auto& a = current.coordinate[e.a];
-                const auto& b = current.coordinate[e.b];
-                if (a[0] / 2 != b[0] / 2 || a[1] / 2 != b[1] / 2 || a[2] / 2 != b[2] / 2) continue;
-                const int ra = root(e.a), rb = root(e.b);
-                if (ra != rb) parent[std::max(ra, rb)] = std::min(ra, rb);
-            }
-            current.aggregate.assign(current.cells, -1);
-            std::vector<int> root_index(current.cells, -1);
-            HostLevel coarse;
-            for (int q = 0; q < current.cells; ++q)
-                if (parent[q] >= 0)
-                {
-                    const int r = root(q);
-                    if (root_index[r] < 0)
-                    {
-                        root_index[r] = coarse.cells++;
-                        coarse.coordinate.push_back({current.coordinate[q][0] / 2, current.coordinate[q][1] / 2, current.coordinate[q][2] / 2});
-                    }
-                    current.aggregate[q] = root_index[r];
-                }
-            if (coarse.cells <= 0 || coarse.cells >= active_cells) { finalize_level(current); host.push_back(std::move(current)); break; }
-            current.restrict_offset.assign(size_t(coarse.cells) + 1, 0);
-            for (int q = 0; q < current.cells; ++q) if (current.aggregate[q] >= 0) ++current.restrict_offset[current.aggregate[q] + 1];
-            for (int q = 0; q < coarse.cells; ++q) current.restrict_offset[q + 1] += current.restrict_offset[q];
-            current.restrict_dof.resize(current.restrict_offset.back());
-            std::vector<int> rc = current.restrict_offset;
-            for (int q = 0; q < current.cells; ++q) if (current.aggregate[q] >= 0) current.restrict_dof[rc[current.aggregate[q]]++] = q;
-            std::vector<double> incident(current.cells, 0), coarse_ground(coarse.cells, 0);
-            for (const HostEdge& e : current.edges) { incident[e.a] += e.coefficient; incident[e.b] += e.coefficient; }
-            for (int q = 0; q < current.cells; ++q)
-                if (current.diagonal[q] > 0)
-                {
-                    const double scale = std::max(1.0, std::abs(current.diagonal[q]));
-                    const double ground = current.diagonal[q] - incident[q];
-                    if (ground < -1e-9 * scale) throw Error(PCFD_INTERNAL, "multigrid Galerkin diagonal inconsistent with its edges");
-                    coarse_ground[current.aggregate[q]] += std::max(0.0, ground);
-                }
-            // Coarse edge weights: first-seen accumulation per (a,b) pair, then sorted by (a,b).
-            std::unordered_map<uint64_t, double> weight;
-            weight.reserve(current.edges.size() / 4 + 1);
-            for (const HostEdge& e : current.edges)
-            {
-                int a = current.aggregate[e.a], b = current.aggregate[e.b];
-                if (a == b) continue;
-                if (a > b) std::swap(a, b);
-                weight[(uint64_t(uint32_t(a)) << 32) | uint32_t(b)] += e.coefficient;
-            }
-            coarse.edges.reserve(weight.size());
-            for (const auto& item : weight) coarse.edges.push_back({int(item.first >> 32), int(item.first & 0xffffffffu), item.second});
-            std::sort(coarse.edges.begin(), coarse.edges.end(), [](const HostEdge& a, const HostEdge& b) { return a.a < b.a || (a.a == b.a && a.b < b.b); });
-            coarse.diagonal = std::move(coarse_ground);
-            for (const HostEdge& e : coarse.edges) { coarse.diagonal[e.a] += e.coefficient; coarse.diagonal[e.b] += e.coefficient; }
-            finalize_level(current);
-            host.push_back(std::move(current));
-            current = std::move(coarse);
-        }
-        s.mg64.clear();
-        s.mg32.clear();
-        s.mg64.resize(host.size());
-        for (size_t l = 0; l < host.size(); ++l) upload_level(s.mg64[l], host[l]);
-        if (s.mg_precision == PCFD_MG_FP32)
-        {
-            s.mg32.resize(host.size());
-            for (size_t l = 0; l < host.size(); ++l) upload_level(s.mg32[l], host[l]);
-        }
-    }
-
-    // ==================================================================================
-    // composite-grid levels (PCFD_MG_CYCLE_COMPOSITE)
-    // ==================================================================================
-    // The reference aggregates every DOF of a level-l brick straight into its level-0 cell (8^l
-    // fine cells per aggregate on the finest level), so the coarse space misses every scale
-    // between 2 h_l and h_0.  The composite cycle replaces that hierarchy with stages that
-    // coarsen every AMR level by 2x2x2 at once: stage k holds one cell per 2^k x 2^k x 2^k block
-    // of same-level cells (cells of different levels never merge; the levels stay coupled
-    // through the Galerkin coarse-fine couplings), down to 512 cells or fewer.  Stage operators
-    // are Galerkin products of the fine orthogonal operator with the piecewise-constant stage
-    // map; every prolongation is weighted 2, as the 2x2x2 Galerkin coarse operator of a uniform
-    // Laplacian is twice the rediscretised one.  Each stage takes mg_stage_sweeps damped-Jacobi
-    // sweeps before and after its coarse correction, the coarsest 96.
-    namespace
-    {
-        // the fine orthogonal operator's two-point couplings in the reference traversal order
+        // The fine orthogonal operator's two-point couplings: same-level faces of every
+        // non-covered brick (minus cut faces), then the coarse/fine, embedded and regular
+        // correction edges with their two-point weights.
         template <class F> void fine_couplings(const pcfd_topology& t, F&& add)
         {
             const int bs = t.brick_size, c3 = bs * bs * bs;
@@ -328,15 +159,188 @@ namespace pcfd
             for (int e = 0; e < t.regular.count; ++e)
                 add(t.regular.lower_dof[e], t.regular.upper_dof[e], t.regular.open_area[e] * t.regular.two_point_delta[e]);
         }
+
+        // Galerkin product of the fine orthogonal operator with the piecewise-constant map of the
+        // active DOFs onto `cells` coarse cells (map[q] < 0: DOF q is not represented).  Couplings
+        // inside one coarse cell cancel; the outlet (2h on X-max faces) and gauge terms become sinks.
+        GraphLevel galerkin_level(const pcfd_topology& t, const std::vector<int>& map, int cells, bool outlet)
+        {
+            GraphLevel level;
+            level.cells = cells;
+            level.sink.assign(size_t(cells), 0.0);
+            std::vector<Coupling> records;
+            records.reserve(size_t(cells) * 3 + 16);
+            fine_couplings(t, [&](int a, int b, double w) {
+                if (a < 0 || b < 0 || a == b || !t.active[a] || !t.active[b] || !(w > 0)) return;
+                const int ca = map[size_t(a)], cb = map[size_t(b)];
+                if (ca < 0 || cb < 0 || ca == cb) return;
+                records.push_back({std::min(ca, cb), std::max(ca, cb), w});
+            });
+            const int bs = t.brick_size, c3 = bs * bs * bs;
+            if (outlet)
+                for (int l = 0; l < t.level_count; ++l)
+                {
+                    const pcfd_level& lev = t.levels[l];
+                    for (int b = 0; b < lev.brick_count; ++b)
+                    {
+                        if ((lev.flags[b] & PCFD_BRICK_COVERED) || !(lev.flags[b] & PCFD_BRICK_XMAX)) continue;
+                        for (int c = bs - 1; c < c3; c += bs)
+                        {
+                            const int q = lev.level_offset + b * c3 + c;
+                            if (t.active[q] && map[size_t(q)] >= 0) level.sink[size_t(map[size_t(q)])] += 2.0 * lev.h;
+                        }
+                    }
+                }
+            for (int g = 0; g < t.gauge_count; ++g)
+            {
+                const int q = t.gauge_dof[g];
+                if (t.active[q] && map[size_t(q)] >= 0) level.sink[size_t(map[size_t(q)])] += t.gauge_coefficient[g];
+            }
+            assemble(level, records);
+            return level;
+        }
+
+        // Galerkin coarsening of `fine` through `parent` (cell -> coarse cell, < 0: none).
+        GraphLevel coarsen(const GraphLevel& fine, const std::vector<int>& parent, int cells)
+        {
+            GraphLevel coarse;
+            coarse.cells = cells;
+            coarse.sink.assign(size_t(cells), 0.0);
+            for (int q = 0; q < fine.cells; ++q)
+                if (parent[size_t(q)] >= 0) coarse.sink[size_t(parent[size_t(q)])] += fine.sink[size_t(q)];
+            std::vector<Coupling> records;
+            records.reserve(fine.couplings.size());
+            for (const Coupling& c : fine.couplings)
+            {
+                const int a = parent[size_t(c.lo)], b = parent[size_t(c.hi)];
+                if (a >= 0 && b >= 0 && a != b) records.push_back({std::min(a, b), std::max(a, b), c.weight});
+            }
+            assemble(coarse, records);
+            return coarse;
+        }
+
+        // Block aggregation of a lattice level: cells of one 2x2x2 block of lattice coordinates
+        // that are connected through couplings inside the block form one coarse cell, found by a
+        // depth-first walk from each unvisited cell in index order (so coarse cells are numbered by
+        // their lowest member).  Cells with a zero diagonal are not aggregated.  Each coarse cell
+        // sits at its block's coordinate.  Returns the number of coarse cells.
+        using Lattice = std::array<int, 3>;
+        int block_aggregates(const GraphLevel& level, const std::vector<Lattice>& at, std::vector<int>& parent,
+                             std::vector<Lattice>& coarse_at)
+        {
+            parent.assign(size_t(level.cells), -1);
+            coarse_at.clear();
+            auto block = [&](int q) { return Lattice{at[size_t(q)][0] >> 1, at[size_t(q)][1] >> 1, at[size_t(q)][2] >> 1}; };
+            std::vector<int> pending;
+            for (int seed = 0; seed < level.cells; ++seed)
+            {
+                if (parent[size_t(seed)] >= 0 || !(level.diagonal[size_t(seed)] > 0)) continue;
+                const int id = int(coarse_at.size());
+                const Lattice home = block(seed);
+                coarse_at.push_back(home);
+                parent[size_t(seed)] = id;
+                pending.push_back(seed);
+                while (!pending.empty())
+                {
+                    const int a = pending.back();
+                    pending.pop_back();
+                    for (int e = level.row_offset[size_t(a)]; e < level.row_offset[size_t(a) + 1]; ++e)
+                    {
+                        const int b = level.neighbour[size_t(e)];
+                        if (parent[size_t(b)] < 0 && level.diagonal[size_t(b)] > 0 && block(b) == home)
+                        {
+                            parent[size_t(b)] = id;
+                            pending.push_back(b);
+                        }
+                    }
+                }
+            }
+            return int(coarse_at.size());
+        }
     }
 
+    // The reference's lattice multigrid (its setup: amr_pressure.cu:915-1069), built here as
+    // Galerkin levels: the active DOFs summed into their level-0 Cartesian cells
+    // (preconditioner_aggregate), then block aggregates of 2x2x2 lattice cells while the level
+    // keeps more than 512 live cells (at most 8 levels above the coarsest) and aggregation still
+    // shrinks it.
+    void build_multigrid(System& s, const pcfd_topology& t, const std::vector<double>& diagonal)
+    {
+        (void)diagonal;
+        const int bs = t.brick_size, c3 = bs * bs * bs;
+        const pcfd_level& base = t.levels[0];
+        s.base_offset = base.level_offset;
+        s.base_cells = base.brick_count * c3;
+        const int n = t.storage_size;
+
+        // active DOF -> level-0 lattice cell; restriction CSR over the lattice cells
+        std::vector<int> lattice(size_t(n), -1);
+        for (int q = 0; q < n; ++q)
+        {
+            const int c = t.preconditioner_aggregate[q] - s.base_offset;
+            if (t.active[q] && c >= 0 && c < s.base_cells) lattice[size_t(q)] = c;
+        }
+        {
+            std::vector<int> offset, member;
+            group_members(lattice, s.base_cells, offset, member);
+            s.base_restrict_offset.upload(offset);
+            s.base_restrict_dof.upload(member);
+        }
+
+        std::vector<Lattice> at(size_t(s.base_cells));
+        for (int brick = 0; brick < base.brick_count; ++brick)
+            for (int c = 0; c < c3; ++c)
+                at[size_t(brick) * c3 + c] = {base.coord[3 * brick] * bs + c % bs, base.coord[3 * brick + 1] * bs + (c / bs) % bs,
+                                              base.coord[3 * brick + 2] * bs + c / (bs * bs)};
+        std::vector<GraphLevel> levels;
+        GraphLevel current = galerkin_level(t, lattice, s.base_cells, s.outlet);
+        for (;;)
+        {
+            const int live = int(std::count_if(current.diagonal.begin(), current.diagonal.end(), [](double v) { return v > 0; }));
+            if (live <= 512 || levels.size() >= 8) break;
+            std::vector<int> parent;
+            std::vector<Lattice> coarse_at;
+            const int cells = block_aggregates(current, at, parent, coarse_at);
+            if (cells <= 0 || cells >= live) break;
+            GraphLevel coarse = coarsen(current, parent, cells);
+            current.parent = std::move(parent);
+            group_members(current.parent, cells, current.member_offset, current.member);
+            levels.push_back(std::move(current));
+            current = std::move(coarse);
+            at = std::move(coarse_at);
+        }
+        levels.push_back(std::move(current));
+        s.mg64.clear();
+        s.mg32.clear();
+        s.mg64.resize(levels.size());
+        for (size_t l = 0; l < levels.size(); ++l) upload_level(s.mg64[l], levels[l]);
+        if (s.mg_precision == PCFD_MG_FP32)
+        {
+            s.mg32.resize(levels.size());
+            for (size_t l = 0; l < levels.size(); ++l) upload_level(s.mg32[l], levels[l]);
+        }
+    }
+
+    // ==================================================================================
+    // composite-grid levels (PCFD_MG_CYCLE_COMPOSITE)
+    // ==================================================================================
+    // The reference aggregates every DOF of a level-l brick straight into its level-0 cell (8^l
+    // fine cells per aggregate on the finest level), so the coarse space misses every scale
+    // between 2 h_l and h_0.  The composite cycle replaces that hierarchy with stages that
+    // coarsen every AMR level by 2x2x2 at once: stage k holds one cell per 2^k x 2^k x 2^k block
+    // of same-level cells (cells of different levels never merge; the levels stay coupled
+    // through the Galerkin coarse-fine couplings), down to 512 cells or fewer.  Stage operators
+    // are Galerkin products of the fine orthogonal operator with the piecewise-constant stage
+    // map; every prolongation is weighted 2, as the 2x2x2 Galerkin coarse operator of a uniform
+    // Laplacian is twice the rediscretised one.  Each stage takes mg_stage_sweeps damped-Jacobi
+    // sweeps before and after its coarse correction, the coarsest 96.
     namespace
     {
         // Explicit inverse of a coarsest level of at most 512 cells (Gauss-Jordan with partial
         // pivoting in FP64) over its cells with a positive diagonal; rows and columns of the other
         // cells stay zero, as the Jacobi sweeps leave them.  Empty when the level is larger or the
         // matrix is numerically singular (the 96 Jacobi sweeps are used then).
-        std::vector<double> dense_inverse(const HostLevel& level)
+        std::vector<double> dense_inverse(const GraphLevel& level)
         {
             const int n = level.cells;
             if (n <= 0 || n > 512) return {};
@@ -354,12 +358,12 @@ namespace pcfd
                 inv[size_t(i) * m + i] = 1.0;
                 scale = std::max(scale, std::abs(level.diagonal[live[i]]));
             }
-            for (const HostEdge& e : level.edges)
+            for (const Coupling& e : level.couplings)
             {
-                const int i = index[e.a], j = index[e.b];
+                const int i = index[e.lo], j = index[e.hi];
                 if (i < 0 || j < 0) continue;
-                a[size_t(i) * m + j] -= e.coefficient;
-                a[size_t(j) * m + i] -= e.coefficient;
+                a[size_t(i) * m + j] -= e.weight;
+                a[size_t(j) * m + i] -= e.weight;
             }
             for (int c = 0; c < m; ++c)
             {
@@ -452,91 +456,29 @@ namespace pcfd
         }
         if (map.empty()) throw Error(PCFD_INTERNAL, "composite cycle: no active structured cells");
         const int K = int(map.size());
-        // Galerkin stage operators through map[k] (sort-based accumulation of the couplings)
-        struct Triple { uint64_t pair; double coefficient; };
-        std::vector<HostLevel> stages(static_cast<size_t>(K));
-        for (int k = 0; k < K; ++k)
+        // Galerkin stage operators through map[k]; stage k -> stage k + 1 parents (consistent for
+        // every DOF of a cell) and restriction CSR; the last stage is the coarsest and keeps none
+        std::vector<GraphLevel> stages;
+        stages.reserve(size_t(K));
+        for (int k = 0; k < K; ++k) stages.push_back(galerkin_level(t, map[size_t(k)], stage_cells[size_t(k)], s.outlet));
+        for (int k = 0; k + 1 < K; ++k)
         {
-            const std::vector<int>& m = map[k];
-            HostLevel& level = stages[size_t(k)];
-            level.cells = stage_cells[k];
-            level.diagonal.assign(size_t(level.cells), 0.0);
-            std::vector<Triple> triples;
-            triples.reserve(k == 0 ? size_t(S) * 3 / 2 : size_t(stage_cells[0]) * 3);
-            fine_couplings(t, [&](int a, int b, double c) {
-                if (a < 0 || b < 0 || a == b || !t.active[a] || !t.active[b] || !(c > 0)) return;
-                int ca = m[a], cb = m[b];
-                if (ca < 0 || cb < 0 || ca == cb) return;
-                level.diagonal[ca] += c;
-                level.diagonal[cb] += c;
-                if (ca > cb) std::swap(ca, cb);
-                triples.push_back({(uint64_t(uint32_t(ca)) << 32) | uint32_t(cb), c});
-            });
-            for (int l = 0; l < t.level_count; ++l)
+            GraphLevel& level = stages[size_t(k)];
+            level.parent.assign(size_t(level.cells), -1);
+            for (int q = 0; q < S; ++q)
             {
-                const pcfd_level& lev = t.levels[l];
-                if (!s.outlet) break;
-                for (int b = 0; b < lev.brick_count; ++b)
-                {
-                    if ((lev.flags[b] & PCFD_BRICK_COVERED) || !(lev.flags[b] & PCFD_BRICK_XMAX)) continue;
-                    for (int c = bs - 1; c < c3; c += bs)
-                    {
-                        const int q = lev.level_offset + b * c3 + c;
-                        if (t.active[q] && m[q] >= 0) level.diagonal[m[q]] += 2.0 * lev.h;
-                    }
-                }
+                const int here = map[size_t(k)][size_t(q)];
+                if (here < 0) continue;
+                int& p = level.parent[size_t(here)];
+                if (p < 0) p = map[size_t(k) + 1][size_t(q)];
+                else if (p != map[size_t(k) + 1][size_t(q)]) throw Error(PCFD_INTERNAL, "composite stage maps are not nested");
             }
-            for (int gg = 0; gg < t.gauge_count; ++gg)
-            {
-                const int q = t.gauge_dof[gg];
-                if (t.active[q] && m[q] >= 0) level.diagonal[m[q]] += t.gauge_coefficient[gg];
-            }
-            std::sort(triples.begin(), triples.end(), [](const Triple& x, const Triple& y) { return x.pair < y.pair; });
-            for (size_t e = 0; e < triples.size();)
-            {
-                size_t f = e;
-                double c = 0.0;
-                while (f < triples.size() && triples[f].pair == triples[e].pair) c += triples[f++].coefficient;
-                level.edges.push_back({int(triples[e].pair >> 32), int(triples[e].pair & 0xffffffffu), c});
-                e = f;
-            }
-        }
-        // stage k -> stage k + 1 aggregates (consistent for every DOF of a cell) and restriction
-        // CSR; the last stage is the coarsest and keeps none
-        for (int k = 0; k < K; ++k)
-        {
-            HostLevel& level = stages[size_t(k)];
-            if (k + 1 < K)
-            {
-                level.aggregate.assign(size_t(level.cells), -1);
-                for (int q = 0; q < S; ++q)
-                {
-                    if (map[k][q] < 0) continue;
-                    int& a = level.aggregate[map[k][q]];
-                    if (a < 0) a = map[k + 1][q];
-                    else if (a != map[k + 1][q]) throw Error(PCFD_INTERNAL, "composite stage maps are not nested");
-                }
-                const int next = stage_cells[k + 1];
-                level.restrict_offset.assign(size_t(next) + 1, 0);
-                for (int c = 0; c < level.cells; ++c) if (level.aggregate[c] >= 0) ++level.restrict_offset[level.aggregate[c] + 1];
-                for (int c = 0; c < next; ++c) level.restrict_offset[c + 1] += level.restrict_offset[c];
-                level.restrict_dof.resize(level.restrict_offset.back());
-                std::vector<int> cursor = level.restrict_offset;
-                for (int c = 0; c < level.cells; ++c) if (level.aggregate[c] >= 0) level.restrict_dof[cursor[level.aggregate[c]]++] = c;
-            }
-            finalize_level(level);
+            group_members(level.parent, stage_cells[size_t(k) + 1], level.member_offset, level.member);
         }
         // fine -> stage 1 map and restriction CSR (DOF order kept)
         const std::vector<int>& first = map[0];
-        const int first_cells = stage_cells[0];
-        std::vector<int> roff(size_t(first_cells) + 1, 0), rdof;
-        for (int q = 0; q < S; ++q) if (first[q] >= 0) ++roff[first[q] + 1];
-        for (int c = 0; c < first_cells; ++c) roff[c + 1] += roff[c];
-        rdof.resize(roff.back());
-        {
-            std::vector<int> cursor = roff;
-            for (int q = 0; q < S; ++q) if (first[q] >= 0) rdof[cursor[first[q]]++] = q;
-        }
+        std::vector<int> roff, rdof;
+        group_members(first, stage_cells[0], roff, rdof);
         s.fine_map.upload(first);
         s.fine_restrict_offset.upload(roff);
         s.fine_restrict_dof.upload(rdof);
@@ -559,10 +501,10 @@ namespace pcfd
                 // FP16 storage of the stage coefficients (the coarsest keeps FP32 for its own sweeps)
                 for (size_t k = 0; k + 1 < stages.size(); ++k)
                 {
-                    std::vector<uint16_t> bits(stages[k].coefficient.size());
+                    std::vector<uint16_t> bits(stages[k].weight.size());
                     for (size_t e = 0; e < bits.size(); ++e)
                     {
-                        const __half hv = __float2half_rn(float(stages[k].coefficient[e]));
+                        const __half hv = __float2half_rn(float(stages[k].weight[e]));
                         std::memcpy(&bits[e], &hv, sizeof(uint16_t));
                     }
                     s.inter32[k].coefficient16.upload(bits);
@@ -1184,8 +1126,8 @@ namespace pcfd
                         return std::abs(gg[cols]);
                     };
                     // Column col's work (preconditioner, operator, both passes, coefficient readback)
-                    // is enqueued as one unit; while the residual estimate is still far above the
-                    // tolerance, column col + 1 is enqueued before the host waits for column col.
+                    // is enqueued as one unit, after the host has read column col - 1's coefficients
+                    // (enqueueing the next column ahead of that wait measured no gain at 16 M cells).
                     const int k = s.recycle_count;
                     auto enqueue = [&](int col) {
                         double* v = s.gmres_v.p + size_t(col) * ld;
@@ -1200,12 +1142,9 @@ namespace pcfd
                                    "coefficient readback");
                         cuda_check(cudaEventRecord(s.dcgs_ready[col & 1], s.stream), "coefficient event");
                     };
-                    double previous_estimate = beta;
                     enqueue(0);
                     for (int col = 0; col < cycle; ++col)
                     {
-                        const bool speculate = col + 1 < cycle && previous_estimate > 30.0 * tolerance * std::sqrt(rhs2);
-                        if (speculate) enqueue(col + 1);
                         cuda_check(cudaEventSynchronize(s.dcgs_ready[col & 1]), "coefficient synchronize");
                         ++result.preconditioner_applications;
                         const int m = k + col;
@@ -1239,12 +1178,9 @@ namespace pcfd
                         const double estimate = least_squares(used, false);
                         if (!std::isfinite(estimate)) { --used; --result.iterations; break; }
                         if (estimate / std::sqrt(rhs2) <= tolerance || next_norm == 0) break;
-                        if (!speculate && col + 1 < cycle) enqueue(col + 1);
-                        previous_estimate = estimate;
+                        if (col + 1 < cycle) enqueue(col + 1);
                         prev_rho = rho;
                     }
-                    // a column enqueued ahead and not used has finished before the correction is formed
-                    cuda_check(cudaStreamSynchronize(s.stream), "column pipeline");
                     if (used == 0) break;
                     if (!std::isfinite(least_squares(used, true))) break;
                 }

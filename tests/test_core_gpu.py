@@ -61,3 +61,74 @@ def test_resolve_repeats_the_step_projection(pair):
     act = rc.active.astype(bool)
     p = s.get_pressure()
     assert np.abs(p - p_step)[act].max() <= 1e-12 * max(np.abs(p_step[act]).max(), 1e-300)
+
+
+def _state_error(s, core, act):
+    (gx, gy, gz) = s.get_state()
+    (rx, ry, rz), rp = core.state()
+    scale = np.abs(rx[act]).max()
+    return max(np.abs(gx - rx)[act].max(), np.abs(gy - ry)[act].max(), np.abs(gz - rz)[act].max()) / scale, rp
+
+
+def _device_pair(spec):
+    """This library and the reference's device classes (ExternalAeroCore's step sequence) on the
+    reference-built cut-cell grid of a workload, same case settings."""
+    rc = ref.workload_case(spec)
+    s = CompositeSystem(rc.topology, momentum_min_volume_fraction=spec.min_volume_fraction)
+    settings = dict(SETTINGS, speed=spec.speed)
+    s.configure(**settings)
+    core = ref.RefDeviceCore(rc, settings["speed"], settings["rho"], settings["nu"], settings["cfl"],
+                             settings["smagorinsky_cs"], settings["projection_tolerance"],
+                             settings["projection_max_iterations"], spec.min_volume_fraction)
+    return rc, s, core
+
+
+def test_three_level_cut_cell_wing_tracks_reference_device_classes(gpu):
+    """5 whole steps on a 3-level cut-cell NACA 4412 wing (coarse/fine tiles, EB fragments,
+    small-cell groups) against the reference's sm_100a device classes: states within 1e-4 of the
+    freestream after every step."""
+    from tests.test_loads_gpu import WING3
+    rc, s, core = _device_pair(WING3)
+    try:
+        a, b = s.initialize(), core.initialize()
+        assert a["pressure"]["converged"] and b["converged"]
+        act = rc.active.astype(bool)
+        for step in range(5):
+            a, b = s.step(), core.step()
+            assert a["pressure"]["converged"] and b["converged"], (step, a, b)
+            assert abs(a["dt"] - b["dt"]) <= 1e-5 * b["dt"]
+            err, _ = _state_error(s, core, act)
+            assert err <= 1e-4, (step, err)
+    finally:
+        core.close()
+        s.close()
+        rc.close()
+
+
+def test_config1_slab_tracks_reference_over_200_steps(gpu):
+    """BASELINE config 1 (128 x 64 x 64 cells of h = c/32 around the NACA 0012 slab at AoA 4 deg,
+    10 m/s, CFL 0.5, projection to 1e-8) against the reference's device classes: states within 1e-4
+    of the freestream for the first 20 steps, and the surface pressure force within 1e-3 after 200
+    steps (both pressures integrated by the reference's compute_pressure_loads for the reference
+    side and by pcfd_core_loads here)."""
+    from paracfd_b200.workloads import WORKLOADS
+    spec = WORKLOADS["naca0012_slab"]
+    rc, s, core = _device_pair(spec)
+    try:
+        a, b = s.initialize(), core.initialize()
+        assert a["pressure"]["converged"] and b["converged"]
+        act = rc.active.astype(bool)
+        for step in range(200):
+            a, b = s.step(), core.step()
+            assert a["pressure"]["converged"] and b["converged"], (step, a, b)
+            if step < 20:
+                err, _ = _state_error(s, core, act)
+                assert err <= 1e-4, (step, err)
+        _, rp = _state_error(s, core, act)
+        ours = np.array(s.loads()["pressure_force"])
+        theirs, _ = rc.pressure_loads(rp)
+        assert np.abs(ours - theirs).max() <= 1e-3 * np.abs(theirs).max(), (ours, theirs)
+    finally:
+        core.close()
+        s.close()
+        rc.close()

@@ -146,3 +146,22 @@ def test_fallback_finishes_an_unconverged_learned_solve(wing):
     oracle.close()
     system.set_preconditioner(PRECONDITIONER_MULTIGRID)
     assert info["fallback_solves"] == 1 and info["converged"] and residual <= 1e-7
+
+
+def test_tensor_core_wait_that_runs_out_returns_timeout_and_frees_tensor_memory(wing):
+    """Failure detection without a GPU fault: the first completion wait of the next convolution
+    polls a barrier that nothing completes, with a 10 ms limit.  The call returns PCFD_TIMEOUT; the
+    kernel drained its own MMAs and freed its tensor memory, so the same evaluation then runs again
+    on the same system and gives the same result as before."""
+    from paracfd_b200 import capi
+    _, system = wing
+    inputs, targets, _, _ = random_samples(5, 71)
+    before, zhat0, _ = system.learned_evaluate(inputs, targets, gradients=False)
+    lib = capi.load()
+    capi.check(lib.pcfd_learned_set_wait(system.handle, 0.01, 1))
+    with pytest.raises(capi.PcfdError) as err:
+        system.learned_evaluate(inputs, targets, gradients=False)
+    assert err.value.status == 6                      # PCFD_TIMEOUT
+    capi.check(lib.pcfd_learned_set_wait(system.handle, 2.0, 0))
+    after, zhat1, _ = system.learned_evaluate(inputs, targets, gradients=False)
+    assert after == before and np.array_equal(zhat0, zhat1)

@@ -214,3 +214,58 @@ def test_composite_cycle_on_three_level_wing_halves_iterations():
     oracle.close()
     built.close()
     assert its[2] <= 0.8 * its[0] and its[3] <= 0.8 * its[0], its
+
+
+def test_fp64_composite_cycle_matches_oracle_restatement(case):
+    """The default preconditioner (composite cycle: Galerkin stages, Chebyshev stage smoothing on
+    [2/30, 2] with 6 steps, exact coarsest stage, Chebyshev-Richardson fine steps on [2/10, 2]) in
+    FP64 against its CPU restatement (oracle po_set_composite), element by element."""
+    rc, _ = case
+    r = np.random.default_rng(41).standard_normal(rc.n) * rc.active
+    act = rc.active.astype(bool)
+    oracle = port.PortSystem(rc.topology)
+    oracle.set_composite(6, 30, 10)
+    want = oracle.precondition(r)
+    oracle.close()
+    with CompositeSystem(rc.topology, mg_cycle=2, mg_precision=MG_FP64, mg_stage_sweeps=6, mg_stage_chebyshev=30,
+                         mg_fine_chebyshev=10) as s:
+        got = s.precondition(r)
+    assert rel(got, want, act) <= 1e-12
+
+
+def test_composite_cycle_matches_oracle_on_three_level_cut_cell_wing(gpu):
+    from tests.test_loads_gpu import WING3
+    rc = ref.workload_case(WING3)
+    r = np.random.default_rng(43).standard_normal(rc.n) * rc.active
+    act = rc.active.astype(bool)
+    oracle = port.PortSystem(rc.topology)
+    want_ref = oracle.precondition(r)             # the reference cycle (lattice hierarchy)
+    oracle.set_composite(6, 30, 10)
+    want = oracle.precondition(r)
+    oracle.close()
+    with CompositeSystem(rc.topology, mg_cycle=2, mg_precision=MG_FP64) as s:
+        got = s.precondition(r)
+    with CompositeSystem(rc.topology, mg_cycle=0, mg_precision=MG_FP64) as s:
+        got_ref = s.precondition(r)
+    rc.close()
+    assert rel(got, want, act) <= 1e-12
+    assert rel(got_ref, want_ref, act) <= 1e-12
+
+
+def test_orthogonal_pcg_on_a_grid_without_wls_nodes(gpu):
+    """A grid with no cut cells has no WLS gradient nodes; the solve then takes the reference's
+    multigrid PCG (solve_orthogonal, amr_pressure.cu:1267-1353): true residual of apply_cpu <= 1e-8."""
+    from paracfd_b200.workloads import WORKLOADS
+    spec = WORKLOADS["paraglider1m"]
+    v, t = spec.surface()
+    rc = ref.case_from_mesh(v, t, spec.domain_lo, spec.domain_hi, 0.25, 1, 8, 1.0, 0.5, 2.0, 1.0)   # one level: no 2:1 tiles
+    assert rc.summary["gradient_nodes"] == 0 and rc.summary["embedded"] == 0
+    act = rc.active.astype(bool)
+    b = rc.apply(np.random.default_rng(47).standard_normal(rc.n) * rc.active)
+    for precision in (MG_FP64, MG_FP32):
+        with CompositeSystem(rc.topology, mg_precision=precision) as s:
+            x, res = s.solve(b, 1e-8, 600)
+        assert res["converged"], res
+        true = np.linalg.norm((b - rc.apply(x))[act]) / np.linalg.norm(b[act])
+        assert true <= 1e-8 * 1.01, (precision, true, res)
+    rc.close()
