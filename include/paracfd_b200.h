@@ -422,6 +422,34 @@ typedef struct pcfd_loads {
 pcfd_status pcfd_core_loads(pcfd_system* system, double pressure_reference, const double moment_origin[3],
                             double reference_area, int32_t include_viscous, pcfd_loads* out);
 
+/* ExternalAeroConservationStats (external_aero_core.h:84-92). */
+typedef struct pcfd_conservation_stats {
+    double max_abs_divergence;             /* 1/s */
+    double volume_weighted_rms_divergence; /* 1/s */
+    double worst_control_volume;           /* m^3 at max_abs_divergence (first DOF on ties) */
+    double max_integrated_flux_error;      /* m^3/s, one control volume */
+    double absolute_integrated_flux_error; /* sum |divergence * volume|, m^3/s */
+    double net_integrated_flux_error;      /* sum divergence * volume, m^3/s */
+} pcfd_conservation_stats;
+/* ExternalAeroCore::conservation_stats (external_aero_core.cpp:347-356) of the resident divergence
+ * (left by the last projection, or by pcfd_projection_divergence_host): device FP64 reductions,
+ * six doubles read back. */
+pcfd_status pcfd_core_conservation_stats(pcfd_system* system, pcfd_conservation_stats* out);
+
+/* ---- point location and headless slices ---------------------------------------------------- */
+/* DeviceAmrLocator::locate_points (amr_fields.cu:131-168, 244-249): for each point of d_points
+ * [count][3] (FP32, device) the finest non-covered brick containing it, d_locations [count][5] =
+ * level, brick (index within its level), i, j, k (device); level = brick = -1 for a point outside
+ * every brick.  Same FP32 arithmetic as the reference, so the same answer at brick and cell edges. */
+pcfd_status pcfd_locate_points_device(pcfd_system* system, const float* d_points, int32_t count, int32_t* d_locations);
+/* Headless slice of the resident state (in place of the reference GUI's OpenGL slice,
+ * src/gui/slice_field.cu:147-261): nu x nv samples at origin + (a + 1/2)/nu edge_u + (b + 1/2)/nv
+ * edge_v, point located as above, each the value of the finest active cell containing it (NaN
+ * where none).  field: 0 |cell velocity|, 1/2/3 cell velocity x/y/z, 4 pressure (FP32 shadow).
+ * out [nv][nu] (host). */
+pcfd_status pcfd_sample_slice_host(pcfd_system* system, const double origin[3], const double edge_u[3],
+                                   const double edge_v[3], int32_t nu, int32_t nv, int32_t field, float* out);
+
 /* ---- instrumentation ---------------------------------------------------------------------- */
 /* Average device time of one launch sequence of `which` (0 full apply, 1 orthogonal apply,
  * 2 preconditioner, 3 divergence, 4 flux correction, 5 FP64 dot, 6/7/8 preconditioner

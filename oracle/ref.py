@@ -78,6 +78,7 @@ def lib():
         L.ref_core_step.argtypes = [vp, f64p]
         L.ref_core_state.argtypes = [vp, f32p, f32p, f32p, f64p]
         L.ref_pressure_loads.argtypes = [vp, f64p, C.c_double, f64p, f64p]
+        L.ref_locate_points.argtypes = [vp, f32p, C.c_int64, C.POINTER(C.c_int32)]
         L.ref_wall_loads_cpu.argtypes = [vp, C.c_double, C.c_double, C.c_double, f32p, f32p, f32p, f64p, C.c_double,
                                          f64p, f64p]
         L.ref_import_topology.restype = vp
@@ -249,6 +250,13 @@ class RefCase:
                                         ptr(np.ascontiguousarray(pressure, np.float64), C.c_double), pressure_reference,
                                         ptr(o, C.c_double), ptr(out, C.c_double)))
         return out[0:3], out[3:6], out[6:9], out[9:12]
+
+    def locate_points(self, points) -> np.ndarray:
+        """The reference's DeviceAmrLocator (GPU): [n, 5] level, brick, i, j, k."""
+        pts = np.ascontiguousarray(points, np.float32)
+        out = np.zeros((len(pts), 5), np.int32)
+        _check(lib().ref_locate_points(self.handle, ptr(pts, C.c_float), len(pts), ptr(out, C.c_int32)))
+        return out
 
     def outflow_rate(self, u, v, w, cf, eb, external=True):
         out = C.c_double()

@@ -8,6 +8,7 @@
 #include "adapter/external_aero_core_b200.h"
 
 #include "core/fluid/amr_eb.h"
+#include "core/fluid/amr_fields.h"
 #include "core/fluid/amr_pressure.h"
 #include "core/fluid/amr_advection.h"
 #include "core/fluid/external_aero_core.h"
@@ -514,6 +515,32 @@ int ref_case_objects(void* handle, const void** hierarchy, const void** system, 
         if (hierarchy) *hierarchy = &c.hierarchy;
         if (system) *system = &c.system;
         if (config) *config = &c.config;
+    });
+}
+int ref_locate_points(void* handle, const float* points, int64_t count, int32_t* out5)
+{
+    return guarded([&] {
+        RefCase& c = *static_cast<RefCase*>(handle);
+        if (count <= 0) return;
+        DeviceAmrLocator locator(c.hierarchy);
+        GpuAmrPoint* d_points = nullptr;
+        GpuBrickLocation* d_out = nullptr;
+        auto ok = [](cudaError_t e, const char* what) { if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e)); };
+        ok(cudaMalloc(&d_points, size_t(count) * sizeof(GpuAmrPoint)), "points");
+        ok(cudaMalloc(&d_out, size_t(count) * sizeof(GpuBrickLocation)), "locations");
+        std::vector<GpuAmrPoint> host(static_cast<size_t>(count));
+        for (int64_t q = 0; q < count; ++q) host[size_t(q)] = {points[3 * q], points[3 * q + 1], points[3 * q + 2]};
+        ok(cudaMemcpy(d_points, host.data(), host.size() * sizeof(GpuAmrPoint), cudaMemcpyHostToDevice), "upload points");
+        locator.locate_points(d_points, d_out, int(count));
+        std::vector<GpuBrickLocation> result(static_cast<size_t>(count));
+        ok(cudaMemcpy(result.data(), d_out, result.size() * sizeof(GpuBrickLocation), cudaMemcpyDeviceToHost), "download locations");
+        cudaFree(d_points);
+        cudaFree(d_out);
+        for (int64_t q = 0; q < count; ++q)
+        {
+            const GpuBrickLocation& r = result[size_t(q)];
+            out5[5 * q] = r.level; out5[5 * q + 1] = r.brick; out5[5 * q + 2] = r.i; out5[5 * q + 3] = r.j; out5[5 * q + 4] = r.k;
+        }
     });
 }
 int ref_case_summary(void* handle, int64_t* o)

@@ -41,6 +41,9 @@ int ref_case_topology(void* handle, pcfd_topology* out);
 /* The case's reference objects (AmrHierarchy, CompositeAmrPressureSystem, ParagliderConfig), for
  * C++ drivers compiled against the reference headers (oracle/adapter/adapter_probe.cpp). */
 int ref_case_objects(void* handle, const void** hierarchy, const void** system, const void** config);
+/* The reference's DeviceAmrLocator::locate_points (its GPU code) on the case's hierarchy:
+ * points [count][3] (host), out5 [count][5] = level, brick, i, j, k (host).  Needs a GPU. */
+int ref_locate_points(void* handle, const float* points, int64_t count, int32_t* out5);
 /* Summary numbers: [levels, storage, active dofs, coarse_fine, embedded, regular corr,
  * gradient nodes, gauges, patches, boundary faces, unresolved cells, retained] */
 int ref_case_summary(void* handle, int64_t* out12);

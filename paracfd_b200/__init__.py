@@ -331,6 +331,20 @@ class CompositeSystem:
                                         int(include_viscous), C.byref(out)))
         return out.as_dict()
 
+    def conservation_stats(self) -> dict:
+        """ExternalAeroCore::conservation_stats of the resident divergence."""
+        out = capi.ConservationStats()
+        check(self._lib.pcfd_core_conservation_stats(self.handle, C.byref(out)))
+        return out.as_dict()
+
+    def sample_slice(self, origin, edge_u, edge_v, nu: int, nv: int, field: int = 0) -> np.ndarray:
+        """Headless slice [nv, nu] of the resident state (field 0 |v|, 1..3 v_x..v_z, 4 pressure)."""
+        o, u, v = (np.ascontiguousarray(a, np.float64) for a in (origin, edge_u, edge_v))
+        out = np.empty((nv, nu), np.float32)
+        check(self._lib.pcfd_sample_slice_host(self.handle, ptr(o, C.c_double), ptr(u, C.c_double), ptr(v, C.c_double), nu, nv,
+                                               field, ptr(out, C.c_float)))
+        return out
+
     def event_record(self, slot: int):
         check(self._lib.pcfd_event_record(self.handle, slot))
 

@@ -133,6 +133,15 @@ class Loads(C.Structure):
         return out
 
 
+class ConservationStats(C.Structure):
+    _fields_ = [("max_abs_divergence", C.c_double), ("volume_weighted_rms_divergence", C.c_double),
+                ("worst_control_volume", C.c_double), ("max_integrated_flux_error", C.c_double),
+                ("absolute_integrated_flux_error", C.c_double), ("net_integrated_flux_error", C.c_double)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 class Mesh(C.Structure):
     _fields_ = [("vertex_count", C.c_int64), ("positions", _f64p), ("triangle_count", C.c_int64),
                 ("indices", _u32p)]
@@ -223,6 +232,10 @@ SIGNATURES = {
                                              C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_float)]),
     "pcfd_learned_apply_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "pcfd_learned_set_wait": (C.c_int, [C.c_void_p, C.c_double, C.c_int32]),
+    "pcfd_core_conservation_stats": (C.c_int, [C.c_void_p, C.POINTER(ConservationStats)]),
+    "pcfd_locate_points_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+    "pcfd_sample_slice_host": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                         C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_float)]),
 }
 
 _lib = None

@@ -279,6 +279,7 @@ namespace pcfd
             s.momentum = new Momentum();
             build_momentum(s, *s.momentum, t, options ? options->momentum_min_volume_fraction : 0.0);
             build_loads(s, t);
+            build_locator(s, t);
             cuda_check(cudaDeviceSynchronize(), "system setup");
         }
 
@@ -330,6 +331,7 @@ namespace pcfd
         if (mg_graph64) cudaGraphExecDestroy(mg_graph64);
         if (mg_graph32) cudaGraphExecDestroy(mg_graph32);
         destroy_loads(*this);
+        destroy_locator(*this);
         delete momentum;
         if (pinned) cudaFreeHost(pinned);
         if (pinned_block) cudaFreeHost(pinned_block);
@@ -727,6 +729,46 @@ pcfd_status pcfd_core_step(pcfd_system* system, pcfd_step_stats* stats)
         core_step(s, local);
         if (stats) *stats = local;
         if (!local.pressure.converged) throw Error(PCFD_NOT_CONVERGED, "pressure solve did not converge; time not advanced");
+    });
+}
+
+pcfd_status pcfd_core_conservation_stats(pcfd_system* system, pcfd_conservation_stats* out)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(out != nullptr, "null output");
+        double v[6];
+        conservation_stats(s, v);
+        out->max_abs_divergence = v[0];
+        out->volume_weighted_rms_divergence = v[1];
+        out->worst_control_volume = v[2];
+        out->max_integrated_flux_error = v[3];
+        out->absolute_integrated_flux_error = v[4];
+        out->net_integrated_flux_error = v[5];
+    });
+}
+
+pcfd_status pcfd_locate_points_device(pcfd_system* system, const float* d_points, int32_t count, int32_t* d_locations)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(count >= 0 && (count == 0 || (d_points && d_locations)), "null points or locations");
+        locate_points(s, d_points, count, d_locations);
+    });
+}
+
+pcfd_status pcfd_sample_slice_host(pcfd_system* system, const double origin[3], const double edge_u[3], const double edge_v[3],
+                                   int32_t nu, int32_t nv, int32_t field, float* out)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(origin && edge_u && edge_v && out, "null slice argument");
+        require(nu > 0 && nv > 0, "slice: nu, nv must be positive");
+        const size_t n = size_t(nu) * size_t(nv);
+        if (s.slice_buffer.n < n) s.slice_buffer.alloc(n);
+        sample_slice(s, origin, edge_u, edge_v, nu, nv, field, s.slice_buffer.p);
+        d2h(s, out, s.slice_buffer.p, n);
+        sync(s);
     });
 }
 

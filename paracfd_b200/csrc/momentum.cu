@@ -198,6 +198,142 @@ namespace pcfd
             xn[a] = x[a] + D[0] * inverse; yn[a] = y[a] + D[1] * inverse; zn[a] = z[a] + D[2] * inverse;
         }
 
+        // ---------------------------------------------------------------- transport, 8^3 bricks
+        // One CTA per active brick.  The brick's momentum and codes plus a two-cell halo along each
+        // axis (from the same-level face neighbours; absent neighbours read as inactive) are staged
+        // in shared memory as a 12^3 tile (cells -2..9).  Each of the brick's 3 x 9 x 64 faces then
+        // evaluates its MUSCL flux once with the per-cell kernel's expression (regular_face_flux), so
+        // a face shared with the neighbouring brick gets the bit-identical flux there; each cell sums
+        // its six faces in the per-cell kernel's order.  The normal velocity of a face is read from the
+        // brick of the face's lower cell, as the per-cell kernel reads it.
+        constexpr int kTile = 12;
+        __device__ inline int tile_index(int i, int j, int k) { return ((k + 2) * kTile + (j + 2)) * kTile + (i + 2); }
+
+        __global__ void __launch_bounds__(256) transport_brick_kernel(const int* __restrict__ brick_list,
+            const int* __restrict__ brick_level, const int* __restrict__ nbr, const uint32_t* __restrict__ flags,
+            const double* __restrict__ level_h, const uint8_t* __restrict__ code, const float* __restrict__ u,
+            const float* __restrict__ v, const float* __restrict__ w, const float* __restrict__ x, const float* __restrict__ y,
+            const float* __restrict__ z, float dt, int external, float U, const int* __restrict__ inflow_slot,
+            const float* __restrict__ inflow, float* __restrict__ xn, float* __restrict__ yn, float* __restrict__ zn,
+            float* __restrict__ dx, float* __restrict__ dy, float* __restrict__ dz)
+        {
+            constexpr int bs = 8, c3 = 512, T3 = kTile * kTile * kTile, F = 9 * 64;
+            __shared__ float sv[3][T3];
+            __shared__ uint8_t sc[T3];
+            __shared__ float flux[3][F][3];            // [axis][face][component]
+            __shared__ int neighbour[6];
+            const int slot = brick_list[blockIdx.x], tid = threadIdx.x;
+            if (tid < 6) neighbour[tid] = nbr[slot * 6 + tid];
+            for (int q = tid; q < T3; q += 256) sc[q] = 0;
+            __syncthreads();
+            const int64_t base = int64_t(slot) * c3;
+            for (int q = tid; q < c3; q += 256)
+            {
+                const int t = tile_index(q & 7, (q >> 3) & 7, q >> 6);
+                sv[0][t] = x[base + q]; sv[1][t] = y[base + q]; sv[2][t] = z[base + q]; sc[t] = code[base + q];
+            }
+            // halos: direction d = 2 axis + (side > 0), two layers of 64 cells each
+            for (int q = tid; q < 6 * 128; q += 256)
+            {
+                const int d = q >> 7, layer = (q >> 6) & 1, a = q & 7, b = (q >> 3) & 7, axis = d >> 1;
+                const int ns = neighbour[d];
+                if (ns < 0) continue;
+                const int src = (d & 1) ? layer : bs - 1 - layer, dst = (d & 1) ? bs + layer : -1 - layer;
+                int si[3], ti[3];
+                // the two transverse coordinates of the halo cell, in axis order
+                const int t0 = axis == 0 ? 1 : 0, t1 = axis == 2 ? 1 : 2;
+                si[axis] = src; ti[axis] = dst;
+                si[t0] = ti[t0] = a; si[t1] = ti[t1] = b;
+                const int64_t g = int64_t(ns) * c3 + (si[2] * bs + si[1]) * bs + si[0];
+                const int t = tile_index(ti[0], ti[1], ti[2]);
+                sv[0][t] = x[g]; sv[1][t] = y[g]; sv[2][t] = z[g]; sc[t] = code[g];
+            }
+            __syncthreads();
+            const float h = float(level_h[brick_level[slot]]);
+            // face fluxes: face p (0..8) along `axis` lies between tile cells p - 1 (lower) and p
+            for (int q = tid; q < 3 * F; q += 256)
+            {
+                const int axis = q / F, f = q % F, p = f % 9, a = (f / 9) & 7, b = f / 72;
+                int lo[3];
+                const int t0 = axis == 0 ? 1 : 0, t1 = axis == 2 ? 1 : 2;
+                lo[axis] = p - 1; lo[t0] = a; lo[t1] = b;
+                int step[3] = {0, 0, 0};
+                step[axis] = 1;
+                const int stride = step[0] + kTile * (step[1] + kTile * step[2]);
+                const int ta = tile_index(lo[0], lo[1], lo[2]), tb = ta + stride;
+                const uint8_t ca = sc[ta], cb = sc[tb];
+                float* out = flux[axis][f];
+                if (!(ca & CODE_ACTIVE) || !(cb & CODE_ACTIVE) || !face_open(ca, axis)) { out[0] = out[1] = out[2] = 0.0f; continue; }
+                // the face's normal velocity, stored in the brick of its lower cell
+                int fs = slot, fi[3] = {lo[0], lo[1], lo[2]};
+                if (p == 0) { fs = neighbour[2 * axis]; fi[axis] = bs - 1; }
+                ++fi[axis];
+                const float normal = axis == 0 ? u[u_face(bs, fs, fi[0], fi[1], fi[2])]
+                                   : (axis == 1 ? v[v_face(bs, fs, fi[0], fi[1], fi[2])] : w[w_face(bs, fs, fi[0], fi[1], fi[2])]);
+                const int tl = ta - stride, tu = tb + stride;
+                const bool has_l = (sc[tl] & CODE_ACTIVE) && face_open(sc[tl], axis);
+                const bool has_u = (sc[tu] & CODE_ACTIVE) && face_open(cb, axis);
+                const float swept = dt * h * h * normal, courant = fabsf(normal) * dt / h;
+                for (int c = 0; c < 3; ++c)
+                {
+                    const float va = sv[c][ta], vb = sv[c][tb];
+                    const float vl = has_l ? sv[c][tl] : 0.0f, vu = has_u ? sv[c][tu] : 0.0f;
+                    out[c] = swept * muscl_value(va, vb, vl, vu, has_l, has_u, swept, courant);
+                }
+            }
+            __syncthreads();
+            const double hd = level_h[brick_level[slot]];
+            const float inverse = 1.0f / float(hd * hd * hd);
+            const uint32_t fl = flags[slot];
+            for (int q = tid; q < c3; q += 256)
+            {
+                const int i = q & 7, j = (q >> 3) & 7, k = q >> 6, t = tile_index(i, j, k);
+                const int64_t a = base + q;
+                const uint8_t ca = sc[t];
+                if (!(ca & CODE_ACTIVE)) { xn[a] = sv[0][t]; yn[a] = sv[1][t]; zn[a] = sv[2][t]; continue; }
+                float D[3] = {0.0f, 0.0f, 0.0f};
+                const int ijk[3] = {i, j, k};
+                for (int axis = 0; axis < 3; ++axis)
+                {
+                    const int t0 = axis == 0 ? 1 : 0, t1 = axis == 2 ? 1 : 2;
+                    int step[3] = {0, 0, 0};
+                    step[axis] = 1;
+                    const int stride = step[0] + kTile * (step[1] + kTile * step[2]);
+                    const int fplus = (ijk[axis] + 1) + 9 * (ijk[t0] + 8 * ijk[t1]), fminus = fplus - 1;
+                    const uint8_t cp = sc[t + stride], cm = sc[t - stride];
+                    if ((cp & CODE_ACTIVE) && face_open(ca, axis))
+                    {
+                        const float* f = flux[axis][fplus];
+                        D[0] -= f[0]; D[1] -= f[1]; D[2] -= f[2];
+                    }
+                    if ((cm & CODE_ACTIVE) && face_open(cm, axis))
+                    {
+                        const float* f = flux[axis][fminus];
+                        D[0] += f[0]; D[1] += f[1]; D[2] += f[2];
+                    }
+                }
+                if (external)
+                {
+                    const float area = h * h;
+                    if (i == 0 && (fl & PCFD_BRICK_XMIN))
+                    {
+                        const float normal = u[u_face(bs, slot, 0, j, k)], swept = dt * area * normal;
+                        const float in = inflow_value(inflow_slot, inflow, bs, slot, j, k, U);
+                        if (swept >= 0.0f) { D[0] += swept * in; D[1] += swept * 0.0f; D[2] += swept * 0.0f; }
+                        else { D[0] += swept * sv[0][t]; D[1] += swept * sv[1][t]; D[2] += swept * sv[2][t]; }
+                    }
+                    if (i == bs - 1 && (fl & PCFD_BRICK_XMAX))
+                    {
+                        const float normal = u[u_face(bs, slot, bs, j, k)], swept = dt * area * normal;
+                        if (swept >= 0.0f) { D[0] += -swept * sv[0][t]; D[1] += -swept * sv[1][t]; D[2] += -swept * sv[2][t]; }
+                        else D[0] += -swept * U;
+                    }
+                }
+                if (ca & CODE_DEFERRED) { dx[a] = D[0]; dy[a] = D[1]; dz[a] = D[2]; continue; }
+                xn[a] = sv[0][t] + D[0] * inverse; yn[a] = sv[1][t] + D[1] * inverse; zn[a] = sv[2][t] + D[2] * inverse;
+            }
+        }
+
         __device__ inline float edge_velocity(int e, const int* source, const int8_t* axis, const int64_t* face, const float* u,
                                               const float* v, const float* w, const float* special)
         {
@@ -626,6 +762,311 @@ namespace pcfd
             gradient[3 * node] = gx; gradient[3 * node + 1] = gy; gradient[3 * node + 2] = gz;
         }
 
+        // ---------------------------------------------------------------- 8^3 brick forms
+        // One CTA per active brick: the brick's codes and the per-cell values an operator reads,
+        // with the facing layer of each same-level neighbour (absent neighbours: code 0, inactive),
+        // are staged once into a 10^3 shared tile (cells -1..8); the per-cell expressions then read
+        // neighbours from shared memory instead of chasing the neighbour table per access.  Same
+        // arithmetic, same order as the per-cell kernels above.
+        constexpr int kHalo = 10, kHalo3 = 1000;
+        __device__ inline int halo_index(int i, int j, int k) { return ((k + 1) * kHalo + (j + 1)) * kHalo + (i + 1); }
+        __device__ inline int halo_stride(int axis) { return axis == 0 ? 1 : (axis == 1 ? kHalo : kHalo * kHalo); }
+
+        template <int NF> struct HaloSources { const float* p[NF > 0 ? NF : 1]; };
+
+        template <int NF>
+        __device__ inline void stage_halo(int slot, const int* __restrict__ nbr, const uint8_t* __restrict__ code,
+                                          HaloSources<NF> src, float (*tile)[kHalo3], uint8_t* tcode, int* neighbour)
+        {
+            const int tid = threadIdx.x;
+            if (tid < 6) neighbour[tid] = nbr[slot * 6 + tid];
+            for (int q = tid; q < kHalo3; q += blockDim.x) tcode[q] = 0;
+            __syncthreads();
+            const int64_t base = int64_t(slot) * 512;
+            for (int q = tid; q < 512; q += blockDim.x)
+            {
+                const int t = halo_index(q & 7, (q >> 3) & 7, q >> 6);
+                tcode[t] = code[base + q];
+                for (int f = 0; f < NF; ++f) tile[f][t] = src.p[f][base + q];
+            }
+            for (int q = tid; q < 6 * 64; q += blockDim.x)
+            {
+                const int d = q >> 6, a = q & 7, b = (q >> 3) & 7, axis = d >> 1;
+                const int ns = neighbour[d];
+                if (ns < 0) continue;
+                const int t0 = axis == 0 ? 1 : 0, t1 = axis == 2 ? 1 : 2;
+                int si[3], ti[3];
+                si[axis] = (d & 1) ? 0 : 7;
+                ti[axis] = (d & 1) ? 8 : -1;
+                si[t0] = ti[t0] = a;
+                si[t1] = ti[t1] = b;
+                const int64_t g = int64_t(ns) * 512 + (si[2] * 8 + si[1]) * 8 + si[0];
+                const int t = halo_index(ti[0], ti[1], ti[2]);
+                tcode[t] = code[g];
+                for (int f = 0; f < NF; ++f) tile[f][t] = src.p[f][g];
+            }
+            __syncthreads();
+        }
+
+        __global__ void __launch_bounds__(256) diffuse_brick_kernel(const int* __restrict__ brick_list,
+            const int* __restrict__ brick_level, const int* __restrict__ nbr, const double* __restrict__ level_h,
+            const uint8_t* __restrict__ code, const float* __restrict__ viscosity, const float* __restrict__ x,
+            const float* __restrict__ y, const float* __restrict__ z, float dt, float* __restrict__ xn, float* __restrict__ yn,
+            float* __restrict__ zn, float* __restrict__ dx, float* __restrict__ dy, float* __restrict__ dz)
+        {
+            __shared__ float tile[4][kHalo3];      // x, y, z, viscosity
+            __shared__ uint8_t tcode[kHalo3];
+            __shared__ int neighbour[6];
+            const int slot = brick_list[blockIdx.x];
+            stage_halo<4>(slot, nbr, code, HaloSources<4>{{x, y, z, viscosity}}, tile, tcode, neighbour);
+            const double hd = level_h[brick_level[slot]];
+            const float h = float(hd), inverse = 1.0f / float(hd * hd * hd);
+            const int64_t base = int64_t(slot) * 512;
+            for (int q = threadIdx.x; q < 512; q += blockDim.x)
+            {
+                const int t = halo_index(q & 7, (q >> 3) & 7, q >> 6);
+                const int64_t a = base + q;
+                const uint8_t ca = tcode[t];
+                if (!(ca & CODE_ACTIVE)) { xn[a] = tile[0][t]; yn[a] = tile[1][t]; zn[a] = tile[2][t]; continue; }
+                float D[3] = {0.0f, 0.0f, 0.0f};
+                for (int axis = 0; axis < 3; ++axis)
+                {
+                    const int s = halo_stride(axis), b = t + s, p = t - s;
+                    if ((tcode[b] & CODE_ACTIVE) && face_open(ca, axis))
+                    {
+                        const float scale = dt * h * 0.5f * (tile[3][t] + tile[3][b]);
+                        D[0] += scale * (tile[0][b] - tile[0][t]); D[1] += scale * (tile[1][b] - tile[1][t]);
+                        D[2] += scale * (tile[2][b] - tile[2][t]);
+                    }
+                    if ((tcode[p] & CODE_ACTIVE) && face_open(tcode[p], axis))
+                    {
+                        const float scale = dt * h * 0.5f * (tile[3][p] + tile[3][t]);
+                        D[0] -= scale * (tile[0][t] - tile[0][p]); D[1] -= scale * (tile[1][t] - tile[1][p]);
+                        D[2] -= scale * (tile[2][t] - tile[2][p]);
+                    }
+                }
+                if (ca & CODE_DEFERRED) { dx[a] = D[0]; dy[a] = D[1]; dz[a] = D[2]; continue; }
+                xn[a] = tile[0][t] + D[0] * inverse; yn[a] = tile[1][t] + D[1] * inverse; zn[a] = tile[2][t] + D[2] * inverse;
+            }
+        }
+
+        __global__ void __launch_bounds__(256) viscosity_brick_kernel(const int* __restrict__ brick_list,
+            const int* __restrict__ brick_level, const int* __restrict__ nbr, const double* __restrict__ level_h,
+            const uint8_t* __restrict__ code, const uint8_t* __restrict__ special, const float* __restrict__ volume,
+            const float* __restrict__ x, const float* __restrict__ y, const float* __restrict__ z, float nu, float cs,
+            float* __restrict__ viscosity)
+        {
+            __shared__ float tile[3][kHalo3];
+            __shared__ uint8_t tcode[kHalo3];
+            __shared__ int neighbour[6];
+            const int slot = brick_list[blockIdx.x];
+            stage_halo<3>(slot, nbr, code, HaloSources<3>{{x, y, z}}, tile, tcode, neighbour);
+            const float h = float(level_h[brick_level[slot]]);
+            const int64_t base = int64_t(slot) * 512;
+            for (int q = threadIdx.x; q < 512; q += blockDim.x)
+            {
+                const int t = halo_index(q & 7, (q >> 3) & 7, q >> 6);
+                const int64_t a = base + q;
+                const uint8_t ca = tcode[t];
+                if (!(ca & CODE_ACTIVE)) continue;
+                float value = nu;
+                if (!special[a] && cs != 0.0f)
+                {
+                    float g[9];
+                    for (int axis = 0; axis < 3; ++axis)
+                    {
+                        const int s = halo_stride(axis), lo = t - s, hi = t + s;
+                        // open_neighbor: the neighbour is active and the face between them is open
+                        const bool has_lo = (tcode[lo] & CODE_ACTIVE) && face_open(tcode[lo], axis);
+                        const bool has_hi = (tcode[hi] & CODE_ACTIVE) && face_open(ca, axis);
+                        for (int comp = 0; comp < 3; ++comp)
+                        {
+                            const float cur = tile[comp][t];
+                            float gv;
+                            if (has_lo && has_hi) gv = (tile[comp][hi] - tile[comp][lo]) / (2.0f * h);
+                            else if (has_hi) gv = (tile[comp][hi] - cur) / h;
+                            else if (has_lo) gv = (cur - tile[comp][lo]) / h;
+                            else gv = 0.0f;
+                            g[comp * 3 + axis] = gv;
+                        }
+                    }
+                    const float strain = sqrtf(fmaxf(0.0f, strain_rate(g))), length = cs * cbrtf(volume[a]);
+                    value += length * length * strain;
+                }
+                viscosity[a] = value;
+            }
+        }
+
+        __global__ void __launch_bounds__(256) rate_brick_kernel(const int* __restrict__ brick_list,
+            const int* __restrict__ brick_level, const int* __restrict__ nbr, const double* __restrict__ level_h,
+            const uint8_t* __restrict__ code, const float* __restrict__ viscosity, float* __restrict__ partial_rate,
+            float* __restrict__ block_partial)
+        {
+            __shared__ float tile[1][kHalo3];
+            __shared__ uint8_t tcode[kHalo3];
+            __shared__ int neighbour[6];
+            __shared__ float shared[8];
+            const int slot = brick_list[blockIdx.x];
+            stage_halo<1>(slot, nbr, code, HaloSources<1>{{viscosity}}, tile, tcode, neighbour);
+            const double hd = level_h[brick_level[slot]];
+            const float h = float(hd);
+            const int64_t base = int64_t(slot) * 512;
+            float local_max = 0.0f;
+            for (int q = threadIdx.x; q < 512; q += blockDim.x)
+            {
+                const int t = halo_index(q & 7, (q >> 3) & 7, q >> 6);
+                const uint8_t ca = tcode[t];
+                if (!(ca & CODE_ACTIVE)) continue;
+                float rate = 0.0f;
+                for (int axis = 0; axis < 3; ++axis)
+                {
+                    const int s = halo_stride(axis), b = t + s, p = t - s;
+                    if ((tcode[b] & CODE_ACTIVE) && face_open(ca, axis)) rate += h * 0.5f * (tile[0][t] + tile[0][b]);
+                    if ((tcode[p] & CODE_ACTIVE) && face_open(tcode[p], axis)) rate += h * 0.5f * (tile[0][p] + tile[0][t]);
+                }
+                if (ca & CODE_DEFERRED) partial_rate[base + q] = rate;
+                else local_max = fmaxf(local_max, rate / float(hd * hd * hd));
+            }
+            local_max = block_max(local_max, shared);
+            if (threadIdx.x == 0) block_partial[blockIdx.x] = local_max;
+        }
+
+        __global__ void __launch_bounds__(256) impulse_brick_kernel(const int* __restrict__ brick_list,
+            const int* __restrict__ brick_level, const int* __restrict__ nbr, const uint32_t* __restrict__ flags,
+            const double* __restrict__ level_h, const uint8_t* __restrict__ code, const float* __restrict__ p, float scale,
+            int outlet, int physical, const float* __restrict__ x, const float* __restrict__ y, const float* __restrict__ z,
+            float* __restrict__ xn, float* __restrict__ yn, float* __restrict__ zn, float* __restrict__ dx, float* __restrict__ dy,
+            float* __restrict__ dz)
+        {
+            __shared__ float tile[1][kHalo3];
+            __shared__ uint8_t tcode[kHalo3];
+            __shared__ int neighbour[6];
+            const int slot = brick_list[blockIdx.x];
+            stage_halo<1>(slot, nbr, code, HaloSources<1>{{p}}, tile, tcode, neighbour);
+            const double hd = level_h[brick_level[slot]];
+            const float h = float(hd), area = h * h, inverse = 1.0f / float(hd * hd * hd);
+            const uint32_t fl = flags[slot];
+            const int64_t base = int64_t(slot) * 512;
+            for (int q = threadIdx.x; q < 512; q += blockDim.x)
+            {
+                const int i = q & 7, j = (q >> 3) & 7, k = q >> 6, t = halo_index(i, j, k);
+                const int64_t a = base + q;
+                const uint8_t ca = tcode[t];
+                if (!(ca & CODE_ACTIVE)) { xn[a] = x[a]; yn[a] = y[a]; zn[a] = z[a]; continue; }
+                float D[3] = {0.0f, 0.0f, 0.0f};
+                for (int axis = 0; axis < 3; ++axis)
+                {
+                    const int s = halo_stride(axis), b = t + s, m = t - s;
+                    if ((tcode[b] & CODE_ACTIVE) && face_open(ca, axis)) D[axis] -= scale * area * 0.5f * (tile[0][t] + tile[0][b]);
+                    if ((tcode[m] & CODE_ACTIVE) && face_open(tcode[m], axis)) D[axis] += scale * area * 0.5f * (tile[0][m] + tile[0][t]);
+                }
+                if (physical)
+                {
+                    const float boundary = scale * area * tile[0][t];
+                    if (i == 0 && (fl & PCFD_BRICK_XMIN)) D[0] += boundary;
+                    if (i == 7 && (fl & PCFD_BRICK_XMAX) && !outlet) D[0] -= boundary;
+                    if (j == 0 && (fl & PCFD_BRICK_YMIN)) D[1] += boundary;
+                    if (j == 7 && (fl & PCFD_BRICK_YMAX)) D[1] -= boundary;
+                    if (k == 0 && (fl & PCFD_BRICK_ZMIN)) D[2] += boundary;
+                    if (k == 7 && (fl & PCFD_BRICK_ZMAX)) D[2] -= boundary;
+                }
+                if (ca & CODE_DEFERRED) { dx[a] = D[0]; dy[a] = D[1]; dz[a] = D[2]; continue; }
+                xn[a] = x[a] + D[0] * inverse; yn[a] = y[a] + D[1] * inverse; zn[a] = z[a] + D[2] * inverse;
+            }
+        }
+
+        __global__ void __launch_bounds__(256) reconstruct_brick_kernel(const int* __restrict__ brick_list,
+            const int* __restrict__ nbr, const uint8_t* __restrict__ code, const float* __restrict__ x, const float* __restrict__ y,
+            const float* __restrict__ z, float* u, float* v, float* w)
+        {
+            __shared__ float tile[3][kHalo3];
+            __shared__ uint8_t tcode[kHalo3];
+            __shared__ int neighbour[6];
+            const int slot = brick_list[blockIdx.x];
+            stage_halo<3>(slot, nbr, code, HaloSources<3>{{x, y, z}}, tile, tcode, neighbour);
+            for (int q = threadIdx.x; q < 512; q += blockDim.x)
+            {
+                const int ijk[3] = {q & 7, (q >> 3) & 7, q >> 6};
+                const int t = halo_index(ijk[0], ijk[1], ijk[2]);
+                const uint8_t ca = tcode[t];
+                if (!(ca & CODE_ACTIVE)) continue;
+                for (int axis = 0; axis < 3; ++axis)
+                {
+                    const int b = t + halo_stride(axis);
+                    if (!(tcode[b] & CODE_ACTIVE) || !face_open(ca, axis)) continue;
+                    const float value = 0.5f * (tile[axis][t] + tile[axis][b]);
+                    int f[3] = {ijk[0], ijk[1], ijk[2]};
+                    ++f[axis];
+                    float* faces = axis == 0 ? u : (axis == 1 ? v : w);
+                    faces[axis_face(8, axis, slot, f[0], f[1], f[2])] = value;
+                    if (ijk[axis] == 7)
+                    {
+                        // the shared face is stored in the neighbour brick too (its face 0)
+                        int m[3] = {ijk[0], ijk[1], ijk[2]};
+                        m[axis] = 0;
+                        faces[axis_face(8, axis, neighbour[2 * axis + 1], m[0], m[1], m[2])] = value;
+                    }
+                }
+            }
+        }
+
+        __global__ void __launch_bounds__(256) cfl_brick_kernel(const int* __restrict__ brick_list,
+            const int* __restrict__ brick_level, const int* __restrict__ nbr, const uint32_t* __restrict__ flags,
+            const double* __restrict__ level_h, const uint8_t* __restrict__ code, const float* __restrict__ u,
+            const float* __restrict__ v, const float* __restrict__ w, const float* __restrict__ x, const float* __restrict__ y,
+            const float* __restrict__ z, int external, float* __restrict__ partial_outflow, float* __restrict__ block_partial)
+        {
+            __shared__ uint8_t tcode[kHalo3];
+            __shared__ int neighbour[6];
+            __shared__ float shared[8];
+            const int slot = brick_list[blockIdx.x];
+            stage_halo<0>(slot, nbr, code, HaloSources<0>{{nullptr}}, nullptr, tcode, neighbour);
+            const double hd = level_h[brick_level[slot]];
+            const float h = float(hd), area = h * h;
+            const uint32_t fl = flags[slot];
+            const int64_t base = int64_t(slot) * 512;
+            float vmax = 0.0f, rmax = 0.0f;
+            for (int q = threadIdx.x; q < 512; q += blockDim.x)
+            {
+                const int ijk[3] = {q & 7, (q >> 3) & 7, q >> 6};
+                const int t = halo_index(ijk[0], ijk[1], ijk[2]);
+                const int64_t a = base + q;
+                const uint8_t ca = tcode[t];
+                if (!(ca & CODE_ACTIVE)) continue;
+                vmax = fmaxf(vmax, fmaxf(fabsf(x[a]), fmaxf(fabsf(y[a]), fabsf(z[a]))));
+                float out = 0.0f;
+                for (int axis = 0; axis < 3; ++axis)
+                {
+                    const int s = halo_stride(axis), b = t + s, p = t - s;
+                    if ((tcode[b] & CODE_ACTIVE) && face_open(ca, axis))
+                    {
+                        int f[3] = {ijk[0], ijk[1], ijk[2]};
+                        ++f[axis];
+                        out += fmaxf(area * face_at(u, v, w, 8, axis, slot, f[0], f[1], f[2]), 0.0f);
+                    }
+                    if ((tcode[p] & CODE_ACTIVE) && face_open(tcode[p], axis))
+                    {
+                        // the lower neighbour's +axis face (in its own brick)
+                        int f[3] = {ijk[0], ijk[1], ijk[2]};
+                        const int sp = f[axis] == 0 ? neighbour[2 * axis] : slot;
+                        f[axis] = f[axis] == 0 ? 8 : f[axis];
+                        out += fmaxf(-(area * face_at(u, v, w, 8, axis, sp, f[0], f[1], f[2])), 0.0f);
+                    }
+                }
+                if (external)
+                {
+                    if (ijk[0] == 0 && (fl & PCFD_BRICK_XMIN)) out += fmaxf(-area * u[u_face(8, slot, 0, ijk[1], ijk[2])], 0.0f);
+                    if (ijk[0] == 7 && (fl & PCFD_BRICK_XMAX)) out += fmaxf(area * u[u_face(8, slot, 8, ijk[1], ijk[2])], 0.0f);
+                }
+                if (ca & CODE_DEFERRED) partial_outflow[a] = out;
+                else rmax = fmaxf(rmax, out / float(hd * hd * hd));
+            }
+            vmax = block_max(vmax, shared);
+            __syncthreads();
+            rmax = block_max(rmax, shared);
+            if (threadIdx.x == 0) { block_partial[2 * blockIdx.x] = vmax; block_partial[2 * blockIdx.x + 1] = rmax; }
+        }
+
         template <int kBS>
         __global__ void impulse_struct_kernel(const int* __restrict__ brick_list, int nbricks, int bs_arg, const int* __restrict__ brick_level,
             const int* __restrict__ nbr, const uint32_t* __restrict__ flags, const double* __restrict__ level_h,
@@ -956,8 +1397,13 @@ namespace pcfd
     void momentum_transport(System& s, Momentum& m, float dt, float freestream, bool external_aero)
     {
         special_gradients(s, m);
-        if (s.active_bricks)
-            (s.bs == 8 ? transport_struct_kernel<8> : transport_struct_kernel<0>)<<<cell_blocks(s), kThreads, 0, launch_stream(s)>>>(
+        if (s.active_bricks && s.bs == 8)
+            transport_brick_kernel<<<s.active_bricks, 256, 0, launch_stream(s)>>>(
+                s.active_brick_list, s.brick_level, s.brick_nbr, s.brick_flags, s.d_level_h, m.code, s.u, s.v, s.w, m.x, m.y, m.z, dt,
+                external_aero ? 1 : 0, freestream, s.inflow_slot_of_brick, s.inflow_set ? s.inflow.p : nullptr, m.xn, m.yn, m.zn, m.dx,
+                m.dy, m.dz);
+        else if (s.active_bricks)
+            transport_struct_kernel<0><<<cell_blocks(s), kThreads, 0, launch_stream(s)>>>(
                 s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr, s.brick_flags, s.d_level_h, m.code, s.u, s.v,
                 s.w, m.x, m.y, m.z, dt, external_aero ? 1 : 0, freestream, s.inflow_slot_of_brick, s.inflow_set ? s.inflow.p : nullptr, m.xn, m.yn, m.zn, m.dx, m.dy, m.dz);
         finish_buffered(s, m, 0, dt);
@@ -968,18 +1414,26 @@ namespace pcfd
     {
         if (nu == 0.0f && cs == 0.0f) { m.last_rate = 0; m.last_substeps = 1; return 0; }
         special_gradients(s, m);
-        if (s.active_bricks)
-            (s.bs == 8 ? viscosity_struct_kernel<8> : viscosity_struct_kernel<0>)<<<cell_blocks(s), kThreads, 0, launch_stream(s)>>>(
+        const bool bricks8 = s.active_bricks && s.bs == 8;
+        if (bricks8)
+            viscosity_brick_kernel<<<s.active_bricks, 256, 0, launch_stream(s)>>>(
+                s.active_brick_list, s.brick_level, s.brick_nbr, s.d_level_h, m.code, m.special, m.volume32, m.x, m.y, m.z, nu, cs,
+                m.viscosity);
+        else if (s.active_bricks)
+            viscosity_struct_kernel<0><<<cell_blocks(s), kThreads, 0, launch_stream(s)>>>(
                 s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr, s.d_level_h, m.code, m.special, m.volume32,
                 m.x, m.y, m.z, nu, cs, m.viscosity);
         if (m.nS)
             viscosity_special_kernel<<<blocks_for(m.nS), kThreads, 0, launch_stream(s)>>>(m.nS, m.s_dof, m.s_gradient, m.volume32, nu, cs, m.viscosity);
         // spectral rate -> substeps (one scalar readback)
         const CompactArgs k = compact_args(s, m);
-        const int cb = s.active_bricks ? cell_blocks(s) : 0, db = m.nD ? blocks_for(m.nD) : 0;
+        const int cb = s.active_bricks ? (bricks8 ? s.active_bricks : cell_blocks(s)) : 0, db = m.nD ? blocks_for(m.nD) : 0;
         require(cb + db <= int(m.reduce_partial.n), "reduction scratch too small");
-        if (cb)
-            (s.bs == 8 ? rate_struct_kernel<8> : rate_struct_kernel<0>)<<<cb, 256, 0, launch_stream(s)>>>(s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr,
+        if (bricks8)
+            rate_brick_kernel<<<cb, 256, 0, launch_stream(s)>>>(s.active_brick_list, s.brick_level, s.brick_nbr, s.d_level_h, m.code,
+                                                               m.viscosity, m.dx, m.reduce_partial);
+        else if (cb)
+            rate_struct_kernel<0><<<cb, 256, 0, launch_stream(s)>>>(s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr,
                                                         s.d_level_h, m.code, m.viscosity, m.dx, m.reduce_partial);
         if (db)
             rate_deferred_kernel<<<db, 256, 0, launch_stream(s)>>>(m.nD, m.d_dof, m.d_offset, m.d_edge, s.structured, k, m.viscosity, m.dx,
@@ -992,8 +1446,12 @@ namespace pcfd
         const float sub_dt = dt / float(m.last_substeps);
         for (int sub = 0; sub < m.last_substeps; ++sub)
         {
-            if (s.active_bricks)
-                (s.bs == 8 ? diffuse_struct_kernel<8> : diffuse_struct_kernel<0>)<<<cell_blocks(s), kThreads, 0, launch_stream(s)>>>(
+            if (bricks8)
+                diffuse_brick_kernel<<<s.active_bricks, 256, 0, launch_stream(s)>>>(
+                    s.active_brick_list, s.brick_level, s.brick_nbr, s.d_level_h, m.code, m.viscosity, m.x, m.y, m.z, sub_dt, m.xn,
+                    m.yn, m.zn, m.dx, m.dy, m.dz);
+            else if (s.active_bricks)
+                diffuse_struct_kernel<0><<<cell_blocks(s), kThreads, 0, launch_stream(s)>>>(
                     s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr, s.d_level_h, m.code, m.viscosity, m.x, m.y,
                     m.z, sub_dt, m.xn, m.yn, m.zn, m.dx, m.dy, m.dz);
             finish_buffered(s, m, 1, sub_dt);
@@ -1027,8 +1485,12 @@ namespace pcfd
         if (o.gradient_nodes)
             pressure_gradient32_kernel<<<blocks_for(o.gradient_nodes), kThreads, 0, launch_stream(s)>>>(
                 o.gradient_nodes, o.grad_dof, o.grad_offset, o.grad_neighbour, m.p_weight, s.pressure32, m.p_gradient);
-        if (s.active_bricks)
-            (s.bs == 8 ? impulse_struct_kernel<8> : impulse_struct_kernel<0>)<<<cell_blocks(s), kThreads, 0, launch_stream(s)>>>(
+        if (s.active_bricks && s.bs == 8)
+            impulse_brick_kernel<<<s.active_bricks, 256, 0, launch_stream(s)>>>(
+                s.active_brick_list, s.brick_level, s.brick_nbr, s.brick_flags, s.d_level_h, m.code, s.pressure32, scale,
+                s.outlet ? 1 : 0, physical ? 1 : 0, m.x, m.y, m.z, m.xn, m.yn, m.zn, m.dx, m.dy, m.dz);
+        else if (s.active_bricks)
+            impulse_struct_kernel<0><<<cell_blocks(s), kThreads, 0, launch_stream(s)>>>(
                 s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr, s.brick_flags, s.d_level_h, m.code, s.pressure32,
                 scale, s.outlet ? 1 : 0, physical ? 1 : 0, m.x, m.y, m.z, m.xn, m.yn, m.zn, m.dx, m.dy, m.dz);
         const CompactArgs k = compact_args(s, m);
@@ -1047,8 +1509,11 @@ namespace pcfd
     void momentum_reconstruct_fluxes(System& s, Momentum& m)
     {
         special_gradients(s, m);
-        if (s.active_bricks)
-            (s.bs == 8 ? reconstruct_struct_kernel<8> : reconstruct_struct_kernel<0>)<<<cell_blocks(s), kThreads, 0, launch_stream(s)>>>(s.active_brick_list, s.active_bricks, s.bs, s.brick_level,
+        if (s.active_bricks && s.bs == 8)
+            reconstruct_brick_kernel<<<s.active_bricks, 256, 0, launch_stream(s)>>>(s.active_brick_list, s.brick_nbr, m.code, m.x, m.y,
+                                                                                   m.z, s.u, s.v, s.w);
+        else if (s.active_bricks)
+            reconstruct_struct_kernel<0><<<cell_blocks(s), kThreads, 0, launch_stream(s)>>>(s.active_brick_list, s.active_bricks, s.bs, s.brick_level,
                                                                                s.brick_nbr, s.d_level_h, m.code, m.x, m.y, m.z, s.u, s.v, s.w);
         if (m.nK)
             reconstruct_compact_kernel<<<blocks_for(m.nK), kThreads, 0, launch_stream(s)>>>(m.nK, compact_args(s, m), m.x, m.y, m.z, s.u, s.v,
@@ -1068,10 +1533,15 @@ namespace pcfd
     void momentum_cfl(System& s, Momentum& m, bool external_aero, float out[4])
     {
         const CompactArgs k = compact_args(s, m);
-        const int cb = s.active_bricks ? cell_blocks(s) : 0, db = m.nD ? blocks_for(m.nD) : 0;
+        const bool bricks8 = s.active_bricks && s.bs == 8;
+        const int cb = s.active_bricks ? (bricks8 ? s.active_bricks : cell_blocks(s)) : 0, db = m.nD ? blocks_for(m.nD) : 0;
         require(2 * (cb + db) <= int(m.reduce_partial.n), "reduction scratch too small");
-        if (cb)
-            (s.bs == 8 ? cfl_struct_kernel<8> : cfl_struct_kernel<0>)<<<cb, 256, 0, launch_stream(s)>>>(s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr,
+        if (bricks8)
+            cfl_brick_kernel<<<cb, 256, 0, launch_stream(s)>>>(s.active_brick_list, s.brick_level, s.brick_nbr, s.brick_flags,
+                                                              s.d_level_h, m.code, s.u, s.v, s.w, m.x, m.y, m.z,
+                                                              external_aero ? 1 : 0, m.dx, m.reduce_partial);
+        else if (cb)
+            cfl_struct_kernel<0><<<cb, 256, 0, launch_stream(s)>>>(s.active_brick_list, s.active_bricks, s.bs, s.brick_level, s.brick_nbr,
                                                        s.brick_flags, s.d_level_h, m.code, s.u, s.v, s.w, m.x, m.y, m.z,
                                                        external_aero ? 1 : 0, m.dx, m.reduce_partial);
         if (db)

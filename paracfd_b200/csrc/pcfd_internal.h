@@ -253,6 +253,8 @@ namespace pcfd
         DBuf<int8_t> special_incident_sign;
         DBuf<double> integrated;                // [S]
         DBuf<float> divergence;                 // [S]
+        DBuf<double> conservation_scratch;      // conservation statistics: block partials and result
+        DBuf<int64_t> conservation_index;
         DBuf<double> rhs, pressure;             // [S]
         DBuf<float> pressure32;                 // [S]
         // regular correction face addresses (face array index, mirror or -1)
@@ -277,6 +279,8 @@ namespace pcfd
         // cell-momentum transport and time-step orchestration
         struct Momentum* momentum = nullptr;
         void* loads = nullptr;                  // surface-load integration state (loads.cu)
+        void* locator = nullptr;                // point location / slice sampling state (locator.cu)
+        DBuf<float> slice_buffer;               // device output of pcfd_sample_slice_host
         cudaEvent_t markers[8] = {};
         int64_t launches = 0;                   // kernels launched on the system stream so far
         // per-launch event pairs around one instrumented region (PCFD_PROFILE_*), for the roofline
@@ -386,6 +390,13 @@ namespace pcfd
     void launch_normalize(System& s, double rho_over_dt, bool with_rhs);
     void launch_correct_fluxes(System& s, double rho, double dt);
     void launch_convert_pressure(System& s);
+    void conservation_stats(System& s, double out[6]);
+    // point location and slice sampling (locator.cu)
+    void build_locator(System& s, const pcfd_topology& t);
+    void destroy_locator(System& s);
+    void locate_points(System& s, const float* d_points, int count, int* d_out);
+    void sample_slice(System& s, const double origin[3], const double edge_u[3], const double edge_v[3], int nu, int nv,
+                      int field, float* d_out);   // [max |div|, rms, worst V, max |div V|, sum |div V|, sum div V]
 
     // face array index helpers (compact per-brick layout)
     __host__ __device__ inline int64_t u_face(int bs, int64_t slot, int i, int j, int k)

@@ -517,6 +517,125 @@ namespace pcfd
         cuda_check(cudaGetLastError(), "correct fluxes");
     }
 
+    // ==================================================================================
+    // conservation statistics of the resident divergence (ExternalAeroCore::conservation_stats,
+    // external_aero_core.cpp:347-356): over active DOFs with positive volume, the largest
+    // |divergence| and its control volume (first DOF on ties), the largest |divergence * V|,
+    // sum |divergence * V|, sum divergence * V and the volume-weighted RMS divergence.  FP64 sums
+    // over a fixed grid with fixed-order trees: deterministic run to run.
+    // ==================================================================================
+    namespace
+    {
+        constexpr int kStatBlocks = 592, kStatThreads = 256, kStatSums = 5;
+        struct StatMax { double value; int64_t index; };
+        __device__ inline StatMax better(StatMax a, StatMax b)
+        {
+            if (b.value > a.value || (b.value == a.value && b.index >= 0 && (a.index < 0 || b.index < a.index))) return b;
+            return a;
+        }
+
+        // sums: [max |div V|, sum |div V|, sum div V, sum div^2 V, sum V]
+        __global__ void __launch_bounds__(kStatThreads) conservation_partial_kernel(const float* __restrict__ divergence,
+            const double* __restrict__ volume, const uint8_t* __restrict__ active, int64_t n, double* __restrict__ partial,
+            double* __restrict__ partial_max, int64_t* __restrict__ partial_index)
+        {
+            __shared__ double sums[kStatSums][kStatThreads];
+            __shared__ StatMax best[kStatThreads];
+            double s[kStatSums] = {0, 0, 0, 0, 0};
+            StatMax m{0.0, -1};
+            for (int64_t q = int64_t(blockIdx.x) * kStatThreads + threadIdx.x; q < n; q += int64_t(gridDim.x) * kStatThreads)
+            {
+                if (!active[q] || !(volume[q] > 0.0)) continue;
+                const double value = double(divergence[q]), v = volume[q], integrated = value * v;
+                m = better(m, StatMax{fabs(value), q});
+                s[0] = fmax(s[0], fabs(integrated));
+                s[1] += fabs(integrated);
+                s[2] += integrated;
+                s[3] += value * value * v;
+                s[4] += v;
+            }
+            for (int k = 0; k < kStatSums; ++k) sums[k][threadIdx.x] = s[k];
+            best[threadIdx.x] = m;
+            __syncthreads();
+            for (int stride = kStatThreads / 2; stride > 0; stride >>= 1)
+            {
+                if (threadIdx.x < stride)
+                {
+                    sums[0][threadIdx.x] = fmax(sums[0][threadIdx.x], sums[0][threadIdx.x + stride]);
+                    for (int k = 1; k < kStatSums; ++k) sums[k][threadIdx.x] += sums[k][threadIdx.x + stride];
+                    best[threadIdx.x] = better(best[threadIdx.x], best[threadIdx.x + stride]);
+                }
+                __syncthreads();
+            }
+            if (threadIdx.x == 0)
+            {
+                for (int k = 0; k < kStatSums; ++k) partial[blockIdx.x * kStatSums + k] = sums[k][0];
+                partial_max[blockIdx.x] = best[0].value;
+                partial_index[blockIdx.x] = best[0].index;
+            }
+        }
+
+        // out: [max |div|, rms, worst volume, max |div V|, sum |div V|, sum div V]
+        __global__ void __launch_bounds__(kStatThreads) conservation_final_kernel(const double* __restrict__ partial,
+            const double* __restrict__ partial_max, const int64_t* __restrict__ partial_index, int blocks,
+            const double* __restrict__ volume, double* __restrict__ out)
+        {
+            __shared__ double sums[kStatSums][kStatThreads];
+            __shared__ StatMax best[kStatThreads];
+            double s[kStatSums] = {0, 0, 0, 0, 0};
+            StatMax m{0.0, -1};
+            for (int b = threadIdx.x; b < blocks; b += kStatThreads)
+            {
+                s[0] = fmax(s[0], partial[b * kStatSums]);
+                for (int k = 1; k < kStatSums; ++k) s[k] += partial[b * kStatSums + k];
+                m = better(m, StatMax{partial_max[b], partial_index[b]});
+            }
+            for (int k = 0; k < kStatSums; ++k) sums[k][threadIdx.x] = s[k];
+            best[threadIdx.x] = m;
+            __syncthreads();
+            for (int stride = kStatThreads / 2; stride > 0; stride >>= 1)
+            {
+                if (threadIdx.x < stride)
+                {
+                    sums[0][threadIdx.x] = fmax(sums[0][threadIdx.x], sums[0][threadIdx.x + stride]);
+                    for (int k = 1; k < kStatSums; ++k) sums[k][threadIdx.x] += sums[k][threadIdx.x + stride];
+                    best[threadIdx.x] = better(best[threadIdx.x], best[threadIdx.x + stride]);
+                }
+                __syncthreads();
+            }
+            if (threadIdx.x == 0)
+            {
+                out[0] = best[0].value;
+                out[1] = sums[4][0] > 0.0 ? sqrt(sums[3][0] / sums[4][0]) : 0.0;
+                out[2] = best[0].index >= 0 ? volume[best[0].index] : 0.0;
+                out[3] = sums[0][0];
+                out[4] = sums[1][0];
+                out[5] = sums[2][0];
+            }
+        }
+    }
+
+    void conservation_stats(System& s, double out[6])
+    {
+        DBuf<double>& scratch = s.conservation_scratch;
+        DBuf<int64_t>& where = s.conservation_index;
+        if (!scratch.p)
+        {
+            scratch.alloc(size_t(kStatBlocks) * (kStatSums + 1) + 8);
+            where.alloc(size_t(kStatBlocks));
+        }
+        const int grid = std::max(1, std::min(kStatBlocks, int((int64_t(s.S) + kStatThreads - 1) / kStatThreads)));
+        double* partial = scratch.p;
+        double* partial_max = partial + size_t(kStatBlocks) * kStatSums;
+        double* result = partial_max + kStatBlocks;
+        conservation_partial_kernel<<<grid, kStatThreads, 0, launch_stream(s)>>>(s.divergence, s.volume, s.active, s.S, partial,
+                                                                                 partial_max, where);
+        conservation_final_kernel<<<1, kStatThreads, 0, launch_stream(s)>>>(partial, partial_max, where, grid, s.volume, result);
+        cuda_check(cudaGetLastError(), "conservation statistics");
+        cuda_check(cudaMemcpyAsync(out, result, 6 * sizeof(double), cudaMemcpyDeviceToHost, s.stream), "conservation readback");
+        cuda_check(cudaStreamSynchronize(s.stream), "conservation readback");
+    }
+
     void launch_convert_pressure(System& s)
     {
         convert_pressure_kernel<<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(s.pressure, s.pressure32, s.S);

@@ -63,3 +63,39 @@ def test_pressure_and_viscous_loads_match_reference(case):
     assert np.abs(np.array(got["viscous_force"]) - fv).max() <= 1e-4 * max(np.abs(fv).max(), 1e-30)
     assert np.abs(np.array(got["viscous_moment"]) - mv).max() <= 1e-4 * max(np.abs(mv).max(), 1e-30)
     assert np.allclose(got["total_force"], np.array(got["pressure_force"]) + np.array(got["viscous_force"]), rtol=1e-12)
+
+
+def _reference_conservation(divergence, volume, active):
+    """ExternalAeroCore::conservation_stats (external_aero_core.cpp:347-356), restated in numpy."""
+    ok = active.astype(bool) & (volume > 0)
+    d = np.asarray(divergence, np.float64)[ok]
+    v = volume[ok]
+    a = np.abs(d)
+    first = int(np.argmax(a))            # first DOF on ties, as the reference's strict '>' scan
+    integrated = d * v
+    return {"max_abs_divergence": a[first], "worst_control_volume": v[first],
+            "max_integrated_flux_error": np.abs(integrated).max(), "absolute_integrated_flux_error": np.abs(integrated).sum(),
+            "net_integrated_flux_error": integrated.sum(),
+            "volume_weighted_rms_divergence": np.sqrt((d * d * v).sum() / v.sum())}
+
+
+def test_conservation_stats_match_reference(case):
+    rc, s = case
+    state = smooth_state(rc, 9)
+    s.set_state(*state)
+    s.reconstruct_fluxes()
+    u, v, w = s.get_faces()
+    cf, eb = s.get_special()
+    ours_div = s.divergence()
+    got = s.conservation_stats()
+    volume = np.ctypeslib.as_array(rc.topology.volume, shape=(rc.n,))
+    # the device reductions restate the reference's loop on the same FP32 divergence
+    want = _reference_conservation(ours_div, volume, rc.active)
+    for key, value in want.items():
+        assert abs(got[key] - value) <= 1e-12 * max(abs(value), 1e-300) + 1e-300, (key, got[key], value)
+    # and on the reference twin's divergence (composite_amr_divergence_cpu, rounded to FP32 like the
+    # reference's device field) the statistics agree to FP32 rounding
+    twin = _reference_conservation(rc.divergence(u, v, w, cf.astype(np.float64), eb.astype(np.float64)).astype(np.float32),
+                                   volume, rc.active)
+    for key in ("max_abs_divergence", "volume_weighted_rms_divergence", "absolute_integrated_flux_error"):
+        assert abs(got[key] - twin[key]) <= 1e-5 * max(abs(twin[key]), 1e-30), (key, got[key], twin[key])
