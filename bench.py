@@ -104,6 +104,8 @@ def parse_args():
                          "the multigrid on the same right-hand sides of the naca4412_wing case")
     ap.add_argument("--train-steps", type=int, default=3000)
     ap.add_argument("--no-learned", action="store_true", help="skip the short learned-preconditioner comparison")
+    ap.add_argument("--no-sweep-summary", action="store_true", help="skip the one-batch angle-sweep summary")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default brick-pipeline launch shape")
     ap.add_argument("--sweep", action="store_true",
                     help="batched angle sweep: 16 naca4412_wing instances (AoA -4..11 deg, seeded refinement bands) in "
                          "4 batches of 4, each batch stepped sequentially and then concurrently (one host thread and "
@@ -486,6 +488,7 @@ def run_ours(args, ranks: Ranks):
     bricks = non_covered_bricks(grid.topology)
     system = make_system(args, grid, ranks.local)
     system.configure(speed=spec.speed, **spec.case)
+    tune = system.autotune(5) if not args.no_autotune else None
     slots = system.inflow_layout()
     faces = len(slots) * spec.brick_size ** 2
     centres = inflow_face_centres(grid.topology, slots)
@@ -586,6 +589,7 @@ def run_ours(args, ranks: Ranks):
         "profiled_region": {"region": region_names.get(args.profile_region), "launches": int(len(per_launch)),
                             "avg_ms": region_ms},
         "cpu_baseline": None,
+        "autotune": tune,
     }
     system.close()
     if ranks.rank == 0 and n == 1 and not args.no_cpu_baseline:
@@ -594,6 +598,13 @@ def run_ours(args, ranks: Ranks):
         except Exception as exc:   # the CPU sample must not hide the GPU result
             line["cpu_baseline"] = {"value": None, "error": str(exc)[:200]}
     grid.close()
+    if ranks.rank == 0 and n == 1 and not args.no_sweep_summary:
+        # one batch of the angle sweep (4 instances) beside the headline
+        try:
+            short = argparse.Namespace(**{**vars(args), "steps": 3, "warmup": 1})
+            line["sweep"] = run_sweep(short, ranks, batches=1)
+        except Exception as exc:
+            line["sweep"] = {"error": str(exc)[:200]}
     if ranks.rank == 0 and n == 1 and not args.no_learned:
         # the learned-preconditioner comparison (a short --learned run) beside the headline
         try:
@@ -783,14 +794,15 @@ def run_learned(args, ranks: Ranks):
     return line
 
 
-def run_sweep(args, ranks: Ranks):
-    """BASELINE config 5 on one GPU: the angle-of-attack sweep as batches of concurrent instances."""
+def run_sweep(args, ranks: Ranks, batches: int = 4):
+    """BASELINE config 5 on one GPU: the angle-of-attack sweep as batches of concurrent instances
+    (the first `batches` of the 4 batches of 4)."""
     from concurrent.futures import ThreadPoolExecutor
 
     from paracfd_b200 import MG_CYCLE_COMPOSITE, MG_FP32, CompositeSystem
     from paracfd_b200.workloads import sweep_instances
 
-    specs = sweep_instances()
+    specs = sweep_instances()[:4 * batches]
     batches = []
     for first in range(0, len(specs), 4):
         batch = specs[first:first + 4]
@@ -800,8 +812,10 @@ def run_sweep(args, ranks: Ranks):
                                    mg_stage_sweeps=args.stage_sweeps, mg_stage_chebyshev=args.chebyshev,
                                    mg_fine_chebyshev=args.fine_chebyshev, gmres_delayed=args.delayed,
                              gmres_recycle=args.recycle, mg_stage_fp16=args.stage_fp16) for b in builts]
+        tuned = []
         for sp, sy in zip(batch, systems):
             sy.configure(speed=sp.speed, **sp.case)
+            tuned.append(sy.autotune(3)["chosen"] if not args.no_autotune else None)
             sy.initialize()
             for _ in range(args.warmup):
                 sy.step()
@@ -825,7 +839,8 @@ def run_sweep(args, ranks: Ranks):
         concurrent = time.perf_counter() - t0
         batches.append({"aoa": [sp.aoa for sp in batch], "leaf_cells": [b.leaf_cells for b in builts],
                         "sequential_s": round(sum(sequential), 3), "concurrent_s": round(concurrent, 3),
-                        "iterations_per_step": [round(i / args.steps, 2) for i in iterations]})
+                        "iterations_per_step": [round(i / args.steps, 2) for i in iterations],
+                        "autotuned_ctas_per_sm": tuned})
         for sy in systems:
             sy.close()
         for b in builts:
@@ -834,7 +849,8 @@ def run_sweep(args, ranks: Ranks):
     seq = sum(b["sequential_s"] for b in batches)
     conc = sum(b["concurrent_s"] for b in batches)
     return {
-        "metric": "batched angle sweep: instance-steps/s over 16 naca4412_wing instances (4 batches of 4)",
+        "metric": f"batched angle sweep: instance-steps/s over {len(specs)} naca4412_wing instances "
+                  f"({len(batches)} batch{'es' if len(batches) > 1 else ''} of 4)",
         "value": round(instance_steps / conc, 3), "unit": "instance-steps/s", "higher_is_better": True, "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "sequential": round(instance_steps / seq, 3),
         "speedup_vs_sequential": round(seq / conc, 3), "timing": "host wall clock around synchronised step loops",

@@ -436,6 +436,20 @@ typedef struct pcfd_conservation_stats {
  * six doubles read back. */
 pcfd_status pcfd_core_conservation_stats(pcfd_system* system, pcfd_conservation_stats* out);
 
+/* ---- launch-shape autotuner ---------------------------------------------------------------- */
+/* No reference counterpart.  Times each candidate persistent-grid size of the brick pipeline (the
+ * fused fine-level multigrid and structured-operator kernels: 1 .. the occupancy limit, at most 8
+ * resident CTAs per SM) on this system's bricks -- the FP64 structured operator plus one fine sweep,
+ * CUDA events over `iterations` launches -- and keeps the fastest for the system's later launches. */
+typedef struct pcfd_autotune_report {
+    int32_t candidates;
+    int32_t ctas_per_sm[8];
+    double apply_ms[8];
+    double sweep_ms[8];
+    int32_t chosen;                  /* resident CTAs per SM now used */
+} pcfd_autotune_report;
+pcfd_status pcfd_autotune(pcfd_system* system, int32_t iterations, pcfd_autotune_report* report);
+
 /* ---- point location and headless slices ---------------------------------------------------- */
 /* DeviceAmrLocator::locate_points (amr_fields.cu:131-168, 244-249): for each point of d_points
  * [count][3] (FP32, device) the finest non-covered brick containing it, d_locations [count][5] =

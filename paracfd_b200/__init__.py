@@ -337,6 +337,12 @@ class CompositeSystem:
         check(self._lib.pcfd_core_conservation_stats(self.handle, C.byref(out)))
         return out.as_dict()
 
+    def autotune(self, iterations: int = 10) -> dict:
+        """Picks the brick pipeline's resident CTAs per SM by timing (pcfd_autotune)."""
+        out = capi.AutotuneReport()
+        check(self._lib.pcfd_autotune(self.handle, iterations, C.byref(out)))
+        return out.as_dict()
+
     def sample_slice(self, origin, edge_u, edge_v, nu: int, nv: int, field: int = 0) -> np.ndarray:
         """Headless slice [nv, nu] of the resident state (field 0 |v|, 1..3 v_x..v_z, 4 pressure)."""
         o, u, v = (np.ascontiguousarray(a, np.float64) for a in (origin, edge_u, edge_v))

@@ -142,6 +142,16 @@ class ConservationStats(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class AutotuneReport(C.Structure):
+    _fields_ = [("candidates", C.c_int32), ("ctas_per_sm", C.c_int32 * 8), ("apply_ms", C.c_double * 8),
+                ("sweep_ms", C.c_double * 8), ("chosen", C.c_int32)]
+
+    def as_dict(self):
+        n = self.candidates
+        return {"ctas_per_sm": list(self.ctas_per_sm[:n]), "apply_ms": [round(v, 5) for v in self.apply_ms[:n]],
+                "sweep_ms": [round(v, 5) for v in self.sweep_ms[:n]], "chosen": self.chosen}
+
+
 class Mesh(C.Structure):
     _fields_ = [("vertex_count", C.c_int64), ("positions", _f64p), ("triangle_count", C.c_int64),
                 ("indices", _u32p)]
@@ -233,6 +243,7 @@ SIGNATURES = {
     "pcfd_learned_apply_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "pcfd_learned_set_wait": (C.c_int, [C.c_void_p, C.c_double, C.c_int32]),
     "pcfd_core_conservation_stats": (C.c_int, [C.c_void_p, C.POINTER(ConservationStats)]),
+    "pcfd_autotune": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(AutotuneReport)]),
     "pcfd_locate_points_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     "pcfd_sample_slice_host": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
                                          C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_float)]),

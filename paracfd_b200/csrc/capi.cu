@@ -748,6 +748,18 @@ pcfd_status pcfd_core_conservation_stats(pcfd_system* system, pcfd_conservation_
     });
 }
 
+pcfd_status pcfd_autotune(pcfd_system* system, int32_t iterations, pcfd_autotune_report* report)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(iterations > 0 && iterations <= 1000, "autotune: 1..1000 iterations");
+        pcfd_autotune_report r{};
+        r.candidates = autotune_pipe(s, iterations, r.ctas_per_sm, r.apply_ms, r.sweep_ms);
+        r.chosen = s.pipe_ctas_per_sm;
+        if (report) *report = r;
+    });
+}
+
 pcfd_status pcfd_locate_points_device(pcfd_system* system, const float* d_points, int32_t count, int32_t* d_locations)
 {
     return guarded([&] {

@@ -183,6 +183,7 @@ namespace pcfd
         cudaStream_t stream = nullptr;
         bool own_stream = false;
         int device = 0;
+        int pipe_ctas_per_sm = 4;               // resident CTAs per SM of the brick pipeline (autotune_pipe)
         double* noalloc_gradient = nullptr;     // static scratch of the allocation-free apply (pressure.cu), once looked up
 
         // host copies of topology needed after setup
@@ -391,6 +392,7 @@ namespace pcfd
     void launch_correct_fluxes(System& s, double rho, double dt);
     void launch_convert_pressure(System& s);
     void conservation_stats(System& s, double out[6]);
+    int autotune_pipe(System& s, int iterations, int* ctas, double* apply_ms, double* sweep_ms);   // smoother.cu
     // point location and slice sampling (locator.cu)
     void build_locator(System& s, const pcfd_topology& t);
     void destroy_locator(System& s);

@@ -744,7 +744,7 @@ namespace pcfd
                 cuda_check(cudaGetDevice(&device), "device");
                 cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
             }
-            return std::max(1, std::min(s.active_bricks, 4 * sms));
+            return std::max(1, std::min(s.active_bricks, s.pipe_ctas_per_sm * sms));
         }
 
         // the working buffers of the fine level in field type T
@@ -989,6 +989,57 @@ namespace pcfd
             sweep<double, double, double, 1>(s, z, r, a, base.x.p);
             sweep<double, double, double, 0>(s, a, r, z, nullptr);
         }
+    }
+
+    // Autotuner of the brick pipeline's persistent grid: each candidate number of resident CTAs
+    // per SM (1 up to what the kernel's registers and shared memory allow, at most 8) is timed on
+    // this system's own bricks -- the structured FP64 operator and one fine-level sweep of the
+    // multigrid in its precision, CUDA events over `iterations` launches on resident scratch
+    // vectors -- and the fastest sum is kept.  Returns the number of candidates written.
+    int autotune_pipe(System& s, int iterations, int* ctas, double* apply_ms, double* sweep_ms)
+    {
+        require(s.fine.enabled, "autotune: the brick pipeline needs 8^3 bricks");
+        int fit = 0;
+        cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, brick_pipe_kernel<2, double, double, double, 0>, 256, 0),
+                   "pipeline occupancy");
+        int fit32 = fit;
+        cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit32, brick_pipe_kernel<0, float, float, float, 0>, 256, 0),
+                   "pipeline occupancy");
+        const int top = std::max(1, std::min({8, fit, fit32}));
+        const bool fp32 = s.composite_fp32 && s.fine.res32.n;
+        cudaEvent_t e0, e1;
+        cuda_check(cudaEventCreate(&e0), "event");
+        cuda_check(cudaEventCreate(&e1), "event");
+        auto time = [&](auto&& body) {
+            body();
+            cuda_check(cudaEventRecord(e0, s.stream), "event");
+            for (int q = 0; q < iterations; ++q) body();
+            cuda_check(cudaEventRecord(e1, s.stream), "event");
+            cuda_check(cudaEventSynchronize(e1), "event");
+            float ms = 0;
+            cuda_check(cudaEventElapsedTime(&ms, e0, e1), "event");
+            return double(ms) / iterations;
+        };
+        int best = s.pipe_ctas_per_sm;
+        double best_ms = 1e300;
+        int n = 0;
+        for (int c = 1; c <= top; ++c)
+        {
+            s.pipe_ctas_per_sm = c;
+            apply_ms[n] = time([&] { brick_apply(s, s.scratch_p, s.scratch_out); });
+            sweep_ms[n] = fp32 ? time([&] {
+                FineSmoother& f = s.fine;
+                sweep<float, float, float, 0>(s, f.z32.p, f.r32.p, f.z32b.p, nullptr);
+            })
+                               : time([&] { sweep<double, double, double, 0>(s, s.fine.z.p, s.scratch_p, s.scratch_out, nullptr); });
+            ctas[n] = c;
+            if (apply_ms[n] + sweep_ms[n] < best_ms) { best_ms = apply_ms[n] + sweep_ms[n]; best = c; }
+            ++n;
+        }
+        s.pipe_ctas_per_sm = best;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return n;
     }
 
     template void fine_preconditioner<double>(System&, const double*, double*, std::vector<MgLevel<double>>&);
