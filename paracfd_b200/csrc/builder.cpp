@@ -15,6 +15,7 @@
 // ring by ring until full rank.  The solid is represented on the Cartesian cells (a cell whose
 // centre lies inside the closed surface is solid; every fluid/solid face becomes a wall patch),
 // which stands in for the reference's exact polyhedral cut-cell builder.
+#include "pseudoinverse3.h"
 #include "../../include/paracfd_b200.h"
 
 #include <algorithm>
@@ -391,55 +392,6 @@ namespace pcfd_builder
     };
     struct Patch { double area; V3 centroid, normal; int plus, minus; };
 
-    // Cyclic Jacobi eigen-decomposition of a symmetric 3x3 matrix -> pseudoinverse, rank.
-    int pseudoinverse3(const double* input, double* inverse, int sweeps, double cutoff)
-    {
-        double a[9], v[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
-        std::copy(input, input + 9, a);
-        for (int sweep = 0; sweep < sweeps; ++sweep)
-        {
-            bool rotated = false;
-            for (int pair = 0; pair < 3; ++pair)
-            {
-                const int p = pair == 2 ? 1 : 0, q = pair == 0 ? 1 : 2;
-                const double apq = a[p * 3 + q], scale = std::max({std::abs(a[p * 3 + p]), std::abs(a[q * 3 + q]), 1e-300});
-                if (std::abs(apq) <= 1e-14 * scale) continue;
-                rotated = true;
-                const double phi = 0.5 * std::atan2(2 * apq, a[q * 3 + q] - a[p * 3 + p]);
-                const double c = std::cos(phi), s = std::sin(phi), app = a[p * 3 + p], aqq = a[q * 3 + q];
-                for (int k = 0; k < 3; ++k)
-                    if (k != p && k != q)
-                    {
-                        const double akp = a[k * 3 + p], akq = a[k * 3 + q];
-                        a[k * 3 + p] = a[p * 3 + k] = c * akp - s * akq;
-                        a[k * 3 + q] = a[q * 3 + k] = s * akp + c * akq;
-                    }
-                a[p * 3 + p] = c * c * app - 2 * s * c * apq + s * s * aqq;
-                a[q * 3 + q] = s * s * app + 2 * s * c * apq + c * c * aqq;
-                a[p * 3 + q] = a[q * 3 + p] = 0;
-                for (int k = 0; k < 3; ++k)
-                {
-                    const double vkp = v[k * 3 + p], vkq = v[k * 3 + q];
-                    v[k * 3 + p] = c * vkp - s * vkq;
-                    v[k * 3 + q] = s * vkp + c * vkq;
-                }
-            }
-            if (!rotated) break;
-        }
-        std::fill(inverse, inverse + 9, 0.0);
-        const double maximum = std::max({std::abs(a[0]), std::abs(a[4]), std::abs(a[8])}), threshold = maximum * cutoff;
-        int rank = 0;
-        for (int mode = 0; mode < 3; ++mode)
-        {
-            const double lambda = a[mode * 3 + mode];
-            if (!(lambda > threshold)) continue;
-            ++rank;
-            for (int r = 0; r < 3; ++r)
-                for (int c = 0; c < 3; ++c) inverse[r * 3 + c] += v[r * 3 + mode] * v[c * 3 + mode] / lambda;
-        }
-        return rank;
-    }
-
     struct System
     {
         const Hierarchy* H = nullptr;
@@ -764,7 +716,7 @@ namespace pcfd_builder
                     for (int c = 0; c < 3; ++c) m[r * 3 + c] += q.weight * d[r] * d[c];
             }
             double local[9];
-            return pseudoinverse3(m, inverse ? inverse : local, 20, 1e-4);
+            return pcfd::pseudoinverse3(m, inverse ? inverse : local, 20, 1e-4);
         };
         auto extend = [&](const std::vector<int>& deficient) {
             struct Src { int node; double path_area; };

@@ -14,6 +14,7 @@
 //  * small-cell redistribution groups (amr_advection.cu:1108-1178);
 //  * smooth-wall patch sides and boundary pressure faces (amr_advection.cu:1186-1208).
 // Everything is indexed for deterministic per-DOF gathers on the device (no atomics).
+#include "pseudoinverse3.h"
 #include "momentum.h"
 
 #include <algorithm>
@@ -33,57 +34,6 @@ namespace pcfd
         inline V3 sub(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
         inline double dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
         inline double comp(V3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
-
-        // Cyclic Jacobi eigen-decomposition of a symmetric 3x3 matrix, then the pseudoinverse that
-        // keeps modes with eigenvalue > relative_cutoff * max|eigenvalue|.  Returns the rank.
-        int symmetric_pseudoinverse(const double* input, double* inverse, double relative_cutoff)
-        {
-            double a[9], v[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
-            std::copy(input, input + 9, a);
-            for (int sweep = 0; sweep < 16; ++sweep)
-            {
-                bool rotated = false;
-                for (int pair = 0; pair < 3; ++pair)
-                {
-                    const int p = pair == 2 ? 1 : 0, q = pair == 0 ? 1 : 2;
-                    const double apq = a[p * 3 + q];
-                    const double scale = std::max({std::abs(a[p * 3 + p]), std::abs(a[q * 3 + q]), 1e-300});
-                    if (std::abs(apq) <= 1e-14 * scale) continue;
-                    rotated = true;
-                    const double phi = 0.5 * std::atan2(2 * apq, a[q * 3 + q] - a[p * 3 + p]);
-                    const double c = std::cos(phi), s = std::sin(phi), app = a[p * 3 + p], aqq = a[q * 3 + q];
-                    for (int k = 0; k < 3; ++k)
-                    {
-                        if (k == p || k == q) continue;
-                        const double akp = a[k * 3 + p], akq = a[k * 3 + q];
-                        a[k * 3 + p] = a[p * 3 + k] = c * akp - s * akq;
-                        a[k * 3 + q] = a[q * 3 + k] = s * akp + c * akq;
-                    }
-                    a[p * 3 + p] = c * c * app - 2 * s * c * apq + s * s * aqq;
-                    a[q * 3 + q] = s * s * app + 2 * s * c * apq + c * c * aqq;
-                    a[p * 3 + q] = a[q * 3 + p] = 0;
-                    for (int k = 0; k < 3; ++k)
-                    {
-                        const double vkp = v[k * 3 + p], vkq = v[k * 3 + q];
-                        v[k * 3 + p] = c * vkp - s * vkq;
-                        v[k * 3 + q] = s * vkp + c * vkq;
-                    }
-                }
-                if (!rotated) break;
-            }
-            std::fill(inverse, inverse + 9, 0.0);
-            const double maximum = std::max({std::abs(a[0]), std::abs(a[4]), std::abs(a[8])});
-            int rank = 0;
-            for (int mode = 0; mode < 3; ++mode)
-            {
-                const double lambda = a[mode * 3 + mode];
-                if (!(lambda > maximum * relative_cutoff)) continue;
-                ++rank;
-                for (int r = 0; r < 3; ++r)
-                    for (int c = 0; c < 3; ++c) inverse[r * 3 + c] += v[r * 3 + mode] * v[c * 3 + mode] / lambda;
-            }
-            return rank;
-        }
 
         double interpolation_weight(V3 lower, V3 upper, V3 face, int axis)
         {
@@ -258,7 +208,7 @@ namespace pcfd
         }
         for (const Edge& e : edges) add_conn(e.a, e.b, e.area);
         std::vector<double> inverse(size_t(nS) * 9);
-        for (int sp = 0; sp < nS; ++sp) symmetric_pseudoinverse(&normal[size_t(sp) * 9], &inverse[size_t(sp) * 9], 1e-4);
+        for (int sp = 0; sp < nS; ++sp) pseudoinverse3(&normal[size_t(sp) * 9], &inverse[size_t(sp) * 9], 16, 1e-4);
         // Nodes with a checked pressure WLS stencil reuse it (identity inverse, WLS weights).
         std::vector<int> pnode(S, -1);
         for (int n = 0; n < t.gradient_node_count; ++n) pnode[t.gradient_dof[n]] = n;
