@@ -398,6 +398,41 @@ namespace
                 }
             }
         }
+        {
+            // EB fragments (DOFs after the structured slots) join the cell that contains their
+            // centroid: the finest non-covered brick there, the cell index clamped to the brick
+            std::vector<std::unordered_map<uint64_t, int>> lookup(t.level_count);
+            auto ck = [](int64_t x, int64_t y, int64_t z) { return (uint64_t(x & 0xfffff) << 40) | (uint64_t(y & 0xfffff) << 20) | uint64_t(z & 0xfffff); };
+            for (int l = 0; l < t.level_count; ++l)
+                for (int b = 0; b < t.levels[l].brick_count; ++b)
+                    lookup[l][ck(t.levels[l].coord[3 * b], t.levels[l].coord[3 * b + 1], t.levels[l].coord[3 * b + 2])] = b;
+            int placed = 0, total = 0;
+            for (int q = s.B * c3; q < S; ++q)
+            {
+                if (!t.active[q]) continue;
+                ++total;
+                const double* c = t.centroid + 3 * size_t(q);
+                for (int l = t.level_count - 1; l >= 0; --l)
+                {
+                    const pcfd_level& lev = t.levels[l];
+                    const double w = bs * lev.h;
+                    int64_t bc[3];
+                    for (int a = 0; a < 3; ++a) bc[a] = int64_t(std::floor((c[a] - t.domain_lo[a]) / w));
+                    auto it = lookup[l].find(ck(bc[0], bc[1], bc[2]));
+                    if (it == lookup[l].end() || (lev.flags[it->second] & COVERED)) continue;
+                    const int b = it->second;
+                    int64_t gc[3];
+                    for (int a = 0; a < 3; ++a)
+                        gc[a] = int64_t(lev.coord[3 * b + a]) * bs +
+                                std::min<int64_t>(bs - 1, std::max<int64_t>(0, int64_t(std::floor((c[a] - lev.origin[3 * b + a]) / lev.h))));
+                    dof_level[q] = l;
+                    g[q] = {gc[0], gc[1], gc[2]};
+                    ++placed;
+                    break;
+                }
+            }
+            (void)placed; (void)total;
+        }
         auto key = [](int m, int64_t x, int64_t y, int64_t z) {
             return (uint64_t(m) << 60) | (uint64_t(x & 0xfffff) << 40) | (uint64_t(y & 0xfffff) << 20) | uint64_t(z & 0xfffff);
         };

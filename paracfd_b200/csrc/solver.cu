@@ -406,8 +406,7 @@ namespace pcfd
     void build_composite(System& s, const pcfd_topology& t)
     {
         const int bs = t.brick_size, c3 = bs * bs * bs, S = t.storage_size;
-        // every active structured DOF: level and global cell coordinates at that level (the EB
-        // fragments stay out of the stages: the fine sweeps alone smooth them)
+        // every active structured DOF: level and global cell coordinates at that level
         std::vector<int8_t> dof_level(size_t(S), -1);
         std::vector<std::array<int64_t, 3>> gcoord(static_cast<size_t>(S));
         for (int l = 0; l < t.level_count; ++l)
@@ -423,6 +422,43 @@ namespace pcfd
                     dof_level[q] = int8_t(l);
                     gcoord[q] = {int64_t(lev.coord[3 * b]) * bs + c % bs, int64_t(lev.coord[3 * b + 1]) * bs + (c / bs) % bs,
                             int64_t(lev.coord[3 * b + 2]) * bs + c / (bs * bs)};
+                }
+            }
+        }
+        // EB fragments (DOFs after the structured slots) join the stages through the cell that
+        // contains their centroid (a fragment is a piece of its cut cell, and a cell box is convex,
+        // so the centroid lies in that cell): the finest non-covered brick at the centroid, the
+        // cell index inside it clamped to the brick.  Without them the stages carry no coarse
+        // correction for the cut cells, and on cut-cell grids the cycle loses its coarse space
+        // exactly where the solution varies most.
+        {
+            const auto brick_key = [](int64_t x, int64_t y, int64_t z) {
+                return (uint64_t(x & 0x1fffff) << 42) | (uint64_t(y & 0x1fffff) << 21) | uint64_t(z & 0x1fffff);
+            };
+            std::vector<std::unordered_map<uint64_t, int>> bricks(static_cast<size_t>(t.level_count));
+            for (int l = 0; l < t.level_count; ++l)
+                for (int b = 0; b < t.levels[l].brick_count; ++b)
+                    bricks[size_t(l)][brick_key(t.levels[l].coord[3 * b], t.levels[l].coord[3 * b + 1], t.levels[l].coord[3 * b + 2])] = b;
+            for (int q = s.structured; q < S; ++q)
+            {
+                if (!t.active[q]) continue;
+                const double* c = t.centroid + 3 * size_t(q);
+                for (int l = t.level_count - 1; l >= 0; --l)
+                {
+                    const pcfd_level& lev = t.levels[l];
+                    const double width = bs * lev.h;
+                    int64_t at[3];
+                    for (int a = 0; a < 3; ++a) at[a] = int64_t(std::floor((c[a] - t.domain_lo[a]) / width));
+                    const auto it = bricks[size_t(l)].find(brick_key(at[0], at[1], at[2]));
+                    if (it == bricks[size_t(l)].end() || (lev.flags[it->second] & PCFD_BRICK_COVERED)) continue;
+                    const int b = it->second;
+                    std::array<int64_t, 3> cell;
+                    for (int a = 0; a < 3; ++a)
+                        cell[size_t(a)] = int64_t(lev.coord[3 * b + a]) * bs +
+                                          std::min<int64_t>(bs - 1, std::max<int64_t>(0, int64_t(std::floor((c[a] - lev.origin[3 * b + a]) / lev.h))));
+                    dof_level[size_t(q)] = int8_t(l);
+                    gcoord[size_t(q)] = cell;
+                    break;
                 }
             }
         }

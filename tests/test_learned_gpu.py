@@ -164,4 +164,5 @@ def test_tensor_core_wait_that_runs_out_returns_timeout_and_frees_tensor_memory(
     assert err.value.status == 6                      # PCFD_TIMEOUT
     capi.check(lib.pcfd_learned_set_wait(system.handle, 2.0, 0))
     after, zhat1, _ = system.learned_evaluate(inputs, targets, gradients=False)
-    assert after == before and np.array_equal(zhat0, zhat1)
+    # the network output is recomputed bit for bit; the loss is an FP32 sum over threads
+    assert np.array_equal(zhat0, zhat1) and abs(after - before) <= 1e-5 * abs(before)
