@@ -470,7 +470,8 @@ pcfd_status pcfd_sample_slice_host(pcfd_system* system, const double origin[3], 
  * pre-smoothing / coarse correction / post-smoothing of the separate-launch cycle, 9/14/15 one
  * GCRO column orthogonalisation against 3 recycled + 13/5/24 basis vectors, 10/11/12/13 the
  * fused cycle's pre-smoothing / restriction / aggregation hierarchy / prolongation +
- * post-smoothing, 16 the learned network on every brick), measured with CUDA events on the system stream over
+ * post-smoothing, 16 the learned network on every brick, 17 one Chebyshev smoothing step of the
+ * composite cycle's first stage), measured with CUDA events on the system stream over
  * `iterations` back-to-back repetitions on resident scratch vectors. */
 pcfd_status pcfd_time_kernel(pcfd_system* system, int32_t which, int32_t iterations, double* ms_per_launch);
 /* Device-timeline markers on the system stream (slots 0..7) for whole-job timing. */
@@ -481,8 +482,15 @@ pcfd_status pcfd_event_elapsed(pcfd_system* system, int32_t start_slot, int32_t 
  * end waits for them, writes up to `capacity` per-launch times (ms) and the count, and disarms. */
 enum {
     PCFD_PROFILE_STRUCTURED_APPLY = 0,   /* brick-tiled FP64 7-point operator kernel */
-    PCFD_PROFILE_PRECONDITIONER = 1      /* one whole multigrid preconditioner application */
+    PCFD_PROFILE_PRECONDITIONER = 1,     /* one whole multigrid preconditioner application */
+    PCFD_PROFILE_STAGE_SMOOTH = 2        /* one smoothing step of the composite cycle's first stage
+                                            (its stage chain runs uncaptured while this is armed) */
 };
+/* Algorithmic bytes of one launch of a profiled region (each element read once and written once):
+ * region 0 17 B per slot of a non-covered brick; region 2 per stage row its offset, rhs, x,
+ * diagonal, direction read and write and next iterate, per stored coupling its column index and
+ * coefficient.  0 for region 1. */
+pcfd_status pcfd_profile_bytes(pcfd_system* system, int32_t region, double* bytes_per_launch);
 /* 1 when the preconditioner's fine level runs as fused brick kernels (8^3 bricks whose
  * level-0 aggregates follow the brick geometry), 0 when it runs as separate launches. */
 pcfd_status pcfd_preconditioner_fused(pcfd_system* system, int32_t* fused);

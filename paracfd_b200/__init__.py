@@ -16,6 +16,7 @@ from .capi import Options, SolveResult, Topology, check, ptr
 
 PROFILE_STRUCTURED_APPLY = 0
 PROFILE_PRECONDITIONER = 1
+PROFILE_STAGE_SMOOTH = 2
 MG_FP64, MG_FP32 = 0, 1
 MG_CYCLE_REFERENCE, MG_CYCLE_CORRECTED, MG_CYCLE_COMPOSITE = 0, 1, 2
 PRECONDITIONER_MULTIGRID, PRECONDITIONER_LEARNED, PRECONDITIONER_JACOBI, PRECONDITIONER_LEARNED_MULTIGRID = 0, 1, 2, 3
@@ -336,6 +337,12 @@ class CompositeSystem:
         out = capi.ConservationStats()
         check(self._lib.pcfd_core_conservation_stats(self.handle, C.byref(out)))
         return out.as_dict()
+
+    def profile_bytes(self, region: int) -> float:
+        """Algorithmic bytes of one launch of a profiled region (pcfd_profile_bytes)."""
+        out = C.c_double()
+        check(self._lib.pcfd_profile_bytes(self.handle, region, C.byref(out)))
+        return out.value
 
     def autotune(self, iterations: int = 10) -> dict:
         """Picks the brick pipeline's resident CTAs per SM by timing (pcfd_autotune)."""

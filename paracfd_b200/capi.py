@@ -243,6 +243,7 @@ SIGNATURES = {
     "pcfd_learned_apply_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "pcfd_learned_set_wait": (C.c_int, [C.c_void_p, C.c_double, C.c_int32]),
     "pcfd_core_conservation_stats": (C.c_int, [C.c_void_p, C.POINTER(ConservationStats)]),
+    "pcfd_profile_bytes": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_double)]),
     "pcfd_autotune": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(AutotuneReport)]),
     "pcfd_locate_points_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     "pcfd_sample_slice_host": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),

@@ -948,7 +948,7 @@ pcfd_status pcfd_profile_begin(pcfd_system* system, int32_t region, int32_t capa
 {
     return guarded([&] {
         System& s = sys(system);
-        require(region >= PCFD_PROFILE_STRUCTURED_APPLY && region <= PCFD_PROFILE_PRECONDITIONER, "unknown profile region");
+        require(region >= PCFD_PROFILE_STRUCTURED_APPLY && region <= PCFD_PROFILE_STAGE_SMOOTH, "unknown profile region");
         require(capacity > 0 && capacity <= (1 << 16), "profile capacity must be 1..65536");
         while (int(s.profile_events.size()) < 2 * capacity)
         {
@@ -977,6 +977,21 @@ pcfd_status pcfd_profile_end(pcfd_system* system, double* ms_per_launch, int32_t
             ms_per_launch[q] = ms;
         }
         s.profile_used = 0;
+    });
+}
+
+pcfd_status pcfd_profile_bytes(pcfd_system* system, int32_t region, double* bytes_per_launch)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(bytes_per_launch != nullptr, "null output");
+        require(region >= PCFD_PROFILE_STRUCTURED_APPLY && region <= PCFD_PROFILE_STAGE_SMOOTH, "unknown profile region");
+        if (region == PCFD_PROFILE_STRUCTURED_APPLY)
+        {
+            *bytes_per_launch = 17.0 * double(s.active_bricks) * double(s.bs3);   // active_bricks: the non-covered bricks
+        }
+        else if (region == PCFD_PROFILE_STAGE_SMOOTH) *bytes_per_launch = stage_smooth_bytes(s);
+        else *bytes_per_launch = 0.0;
     });
 }
 
@@ -1071,6 +1086,7 @@ pcfd_status pcfd_time_kernel(pcfd_system* system, int32_t which, int32_t iterati
                 break;
             }
             case 16: learned_apply(s, s.scratch_p, s.scratch_out); break;
+            case 17: stage_smooth_once(s); break;
             default: throw Error(PCFD_INVALID_ARG, "unknown kernel id");
             }
         };

@@ -103,6 +103,7 @@ namespace pcfd
     // One level of the aggregation multigrid (host-built CSR, reference amr_pressure.cu:915-1083).
     template <class T> struct MgLevel
     {
+        using value_type = T;
         int cells = 0;
         DBuf<int> row_offset, neighbour, aggregate, restrict_offset, restrict_dof;
         DBuf<T> coefficient, diagonal, rhs, x, temporary, residual;
@@ -316,7 +317,7 @@ namespace pcfd
         System& s;
         bool on;
         ProfileScope(System& sys, int region)
-            : s(sys), on(sys.profile_region == region && 2 * (sys.profile_used + 1) <= int(sys.profile_events.size()))
+            : s(sys), on(region >= 0 && sys.profile_region == region && 2 * (sys.profile_used + 1) <= int(sys.profile_events.size()))
         {
             if (on) cuda_check(cudaEventRecord(s.profile_events[2 * s.profile_used], s.stream), "profile event");
         }
@@ -393,6 +394,8 @@ namespace pcfd
     void launch_convert_pressure(System& s);
     void conservation_stats(System& s, double out[6]);
     int autotune_pipe(System& s, int iterations, int* ctas, double* apply_ms, double* sweep_ms);   // smoother.cu
+    double stage_smooth_bytes(const System& s);   // solver.cu: algorithmic bytes of one first-stage smoothing step
+    void stage_smooth_once(System& s);            // solver.cu: one first-stage Chebyshev step (kernel timing)
     // point location and slice sampling (locator.cu)
     void build_locator(System& s, const pcfd_topology& t);
     void destroy_locator(System& s);

@@ -720,6 +720,8 @@ namespace pcfd
                             c2 = 2.0 * next / delta;
                             rho = next;
                         }
+                        // the first composite stage's steps are the profiled stage-smoothing region
+                        ProfileScope scope(s, index == 0 && s.composite ? PCFD_PROFILE_STAGE_SMOOTH : -1);
                         if (level.coefficient16.p)
                             algebraic_chebyshev_kernel<T, __half><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
                                 level.rhs, level.x, level.temporary, level.residual, level.row_offset, level.neighbour,
@@ -788,7 +790,8 @@ namespace pcfd
         template <class T>
         void run_captured(System& s, std::vector<MgLevel<T>*>& chain, cudaGraphExec_t& exec, int64_t& nodes)
         {
-            if (!s.stream)
+            // uncaptured while the stage-smoothing region is profiled: its launches get event pairs
+            if (!s.stream || s.profile_region == PCFD_PROFILE_STAGE_SMOOTH)
             {
                 mg_level(s, chain.data(), int(chain.size()), 0);
                 return;
@@ -879,6 +882,44 @@ namespace pcfd
         std::vector<MgLevel<double>*> chain;
         for (MgLevel<double>& level : s.inter64) chain.push_back(&level);
         run_captured(s, chain, s.mg_graph_composite, s.mg_graph_composite_launches);
+    }
+
+    // Algorithmic bytes of one step of the first composite stage's smoothing: per row the row
+    // offset, rhs, x, diagonal, the direction read and written and the next iterate (7 values of
+    // 4 B in FP32, 8 B in FP64, offsets 4 B), per stored coupling its column index and coefficient.
+    double stage_smooth_bytes(const System& s)
+    {
+        if (s.composite_fp32 && !s.inter32.empty())
+        {
+            const MgLevel<float>& l = s.inter32.front();
+            return 28.0 * l.cells + (4.0 + (l.coefficient16.p ? 2.0 : 4.0)) * double(l.neighbour.n);
+        }
+        if (!s.inter64.empty())
+        {
+            const MgLevel<double>& l = s.inter64.front();
+            return 52.0 * l.cells + 12.0 * double(l.neighbour.n);
+        }
+        return 0.0;
+    }
+
+    // One Chebyshev step of the first composite stage on its resident buffers (kernel timing).
+    void stage_smooth_once(System& s)
+    {
+        require(s.composite && (!s.inter32.empty() || !s.inter64.empty()), "stage smoothing step: the composite cycle");
+        auto run = [&](auto& level) {
+            using T = typename std::remove_reference_t<decltype(level)>::value_type;
+            if (level.coefficient16.p)
+                algebraic_chebyshev_kernel<T, __half><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
+                    level.rhs, level.x, level.temporary, level.residual, level.row_offset, level.neighbour,
+                    reinterpret_cast<const __half*>(level.coefficient16.p), level.diagonal, level.cells, T(0.5), T(0.7), 0);
+            else
+                algebraic_chebyshev_kernel<T, T><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
+                    level.rhs, level.x, level.temporary, level.residual, level.row_offset, level.neighbour, level.coefficient,
+                    level.diagonal, level.cells, T(0.5), T(0.7), 0);
+        };
+        if (s.composite_fp32) run(s.inter32.front());
+        else run(s.inter64.front());
+        cuda_check(cudaGetLastError(), "stage smoothing step");
     }
 
     template void multigrid_levels<double>(System&, std::vector<MgLevel<double>>&);
