@@ -471,7 +471,7 @@ pcfd_status pcfd_sample_slice_host(pcfd_system* system, const double origin[3], 
  * GCRO column orthogonalisation against 3 recycled + 13/5/24 basis vectors, 10/11/12/13 the
  * fused cycle's pre-smoothing / restriction / aggregation hierarchy / prolongation +
  * post-smoothing, 16 the learned network on every brick, 17 one Chebyshev smoothing step of the
- * composite cycle's first stage), measured with CUDA events on the system stream over
+ * composite cycle's first stage, 18 one delayed-CGS2 column against 13 basis vectors), measured with CUDA events on the system stream over
  * `iterations` back-to-back repetitions on resident scratch vectors. */
 pcfd_status pcfd_time_kernel(pcfd_system* system, int32_t which, int32_t iterations, double* ms_per_launch);
 /* Device-timeline markers on the system stream (slots 0..7) for whole-job timing. */

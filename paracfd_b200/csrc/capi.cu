@@ -1087,6 +1087,15 @@ pcfd_status pcfd_time_kernel(pcfd_system* system, int32_t which, int32_t iterati
             }
             case 16: learned_apply(s, s.scratch_p, s.scratch_out); break;
             case 17: stage_smooth_once(s); break;
+            case 18:
+            {
+                // one delayed-CGS2 column (dot pass, coefficients, update pass) against 13 basis vectors
+                require(s.full_nonorthogonal, "delayed CGS2 needs the GCRO storage");
+                VecSet Q(s.Sp);
+                for (int row = 0; row < 13; ++row) Q.push(s.gmres_v.p + size_t(row) * s.Sp);
+                dcgs_pass(s, Q, s.gmres_v.p + size_t(13) * s.Sp, s.Ad, s.gmres_v.p + size_t(14) * s.Sp, s.dcgs_result);
+                break;
+            }
             default: throw Error(PCFD_INVALID_ARG, "unknown kernel id");
             }
         };

@@ -83,6 +83,11 @@ namespace pcfd
         int incident_dofs = 0, connection_count = 0, regular_count = 0;
         DBuf<int> incident_dof, incident_offset, incident_edge;
         DBuf<int8_t> incident_sign;
+        // the same incidence entries packed for the two-point sums: the edge's other endpoint and
+        // its coefficient, so coefficient * (p[dof] - p[other]) equals sign * coefficient *
+        // (p[lower] - p[upper]) bit for bit with one load chain less
+        DBuf<int> incident_other;
+        DBuf<double> incident_coefficient;
         // connections (coarse/fine then embedded), geometrically ordered endpoints
         DBuf<int> conn_lower, conn_upper, conn_lower_node, conn_upper_node;
         DBuf<double> conn_coefficient, conn_correction, conn_upper_weight, conn_area;

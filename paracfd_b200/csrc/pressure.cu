@@ -146,27 +146,26 @@ namespace pcfd
 
         // Deterministic per-DOF gather of the compact two-point edges (connections first, then
         // regular corrections), reference amr_pressure.cu:105-134 with FP64 coefficients.
+        // Two-point fluxes of the compact edges at each incident DOF, in the reference's per-DOF
+        // order (amr_pressure.cu:105-134): sign * coefficient * (p[lower] - p[upper]), evaluated as
+        // coefficient * (p[dof] - p[other]) from the packed incidence entries (equal bit for bit:
+        // negating a difference or a product is exact).
         __global__ void irregular_orthogonal_gather_kernel(
             const int* __restrict__ incident_dof, const int* __restrict__ incident_offset,
-            const int* __restrict__ incident_edge, const int8_t* __restrict__ incident_sign, int incident_dofs,
-            int connection_count, const int* __restrict__ conn_lower, const int* __restrict__ conn_upper,
-            const double* __restrict__ conn_coefficient, const int* __restrict__ reg_lower,
-            const int* __restrict__ reg_upper, const double* __restrict__ reg_coefficient,
+            const int* __restrict__ incident_other, const double* __restrict__ incident_coefficient, int incident_dofs,
             const uint8_t* __restrict__ active, const double* __restrict__ p, double* __restrict__ out)
         {
             const int node = blockIdx.x * blockDim.x + threadIdx.x;
             if (node >= incident_dofs) return;
+            const int dof = incident_dof[node];
+            const double centre = p[dof];
             double sum = 0.0;
             for (int q = incident_offset[node]; q < incident_offset[node + 1]; ++q)
             {
-                const int e = incident_edge[q];
-                int a, b;
-                double coefficient;
-                if (e < connection_count) { a = conn_lower[e]; b = conn_upper[e]; coefficient = conn_coefficient[e]; }
-                else { const int r = e - connection_count; a = reg_lower[r]; b = reg_upper[r]; coefficient = reg_coefficient[r]; }
-                if (active[a] && active[b]) sum += double(incident_sign[q]) * (coefficient * (p[a] - p[b]));
+                const int other = incident_other[q];
+                if (active[other]) sum += incident_coefficient[q] * (centre - p[other]);
             }
-            out[incident_dof[node]] += sum;
+            out[dof] += sum;
         }
 
         __global__ void reconstruct_gradient_kernel(const int* __restrict__ dof, const int* __restrict__ offset,
@@ -266,8 +265,7 @@ namespace pcfd
         IrregularOperator& o = s.irr;
         if (o.incident_dofs)
             irregular_orthogonal_gather_kernel<<<blocks_for(o.incident_dofs), kThreads, 0, launch_stream(s)>>>(
-                o.incident_dof, o.incident_offset, o.incident_edge, o.incident_sign, o.incident_dofs, o.connection_count,
-                o.conn_lower, o.conn_upper, o.conn_coefficient, o.reg_lower, o.reg_upper, o.reg_coefficient, s.active, p, out);
+                o.incident_dof, o.incident_offset, o.incident_other, o.incident_coefficient, o.incident_dofs, s.active, p, out);
         if (o.gauges)
             gauge_apply_kernel<<<blocks_for(o.gauges), kThreads, 0, launch_stream(s)>>>(o.gauge_dof, o.gauge_coefficient, o.gauges, p, out);
         if (!orthogonal_only && o.gradient_nodes)
@@ -471,17 +469,23 @@ namespace pcfd
             if (a.edge != b.edge) return a.edge < b.edge;
             return a.sign < b.sign;
         });
-        std::vector<int> idof, ioff, iedge;
+        std::vector<int> idof, ioff, iedge, iother;
         std::vector<int8_t> isign;
+        std::vector<double> icoef;
         for (size_t q = 0; q < inc.size(); ++q)
         {
             if (q == 0 || inc[q].dof != inc[q - 1].dof) { idof.push_back(inc[q].dof); ioff.push_back(int(q)); }
             iedge.push_back(inc[q].edge);
             isign.push_back(inc[q].sign);
+            const int e = inc[q].edge;
+            const int lo = e < nc ? lower[e] : rl[e - nc], hi = e < nc ? upper[e] : ru[e - nc];
+            iother.push_back(inc[q].sign > 0 ? hi : lo);
+            icoef.push_back(e < nc ? coefficient[e] : rcoef[e - nc]);
         }
         ioff.push_back(int(inc.size()));
         o.incident_dofs = int(idof.size());
         o.incident_dof.upload(idof); o.incident_offset.upload(ioff); o.incident_edge.upload(iedge); o.incident_sign.upload(isign);
+        o.incident_other.upload(iother); o.incident_coefficient.upload(icoef);
 
         o.gradient_nodes = t.gradient_node_count;
         if (o.gradient_nodes)
@@ -575,8 +579,7 @@ namespace pcfd
             zero_range_kernel<<<blocks_for(s.S - s.structured), kThreads, 0, launch_stream(s)>>>(out, s.structured, s.S);
         if (o.incident_dofs)
             irregular_orthogonal_gather_kernel<<<blocks_for(o.incident_dofs), kThreads, 0, launch_stream(s)>>>(
-                o.incident_dof, o.incident_offset, o.incident_edge, o.incident_sign, o.incident_dofs, o.connection_count,
-                o.conn_lower, o.conn_upper, o.conn_coefficient, o.reg_lower, o.reg_upper, o.reg_coefficient, s.active, p, out);
+                o.incident_dof, o.incident_offset, o.incident_other, o.incident_coefficient, o.incident_dofs, s.active, p, out);
         if (o.gauges)
             gauge_apply_kernel<<<blocks_for(o.gauges), kThreads, 0, launch_stream(s)>>>(o.gauge_dof, o.gauge_coefficient, o.gauges, p, out);
         if (!orthogonal_only && o.gradient_nodes)

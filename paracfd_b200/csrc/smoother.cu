@@ -410,10 +410,8 @@ namespace pcfd
         template <int kMode, class T, class TO, class TC, int kProlong>
         __global__ void finish_deferred_kernel(int count, const int* __restrict__ dof, const int* __restrict__ incident,
             const int* __restrict__ gauge_offset, const double* __restrict__ gauge_coefficient,
-            const int* __restrict__ incident_offset, const int* __restrict__ incident_edge, const int8_t* __restrict__ incident_sign,
-            int connection_count, const int* __restrict__ conn_lower, const int* __restrict__ conn_upper,
-            const double* __restrict__ conn_coefficient, const int* __restrict__ reg_lower, const int* __restrict__ reg_upper,
-            const double* __restrict__ reg_coefficient, const uint8_t* __restrict__ active, const double* __restrict__ diag,
+            const int* __restrict__ incident_offset, const int* __restrict__ incident_other,
+            const double* __restrict__ incident_coefficient, const uint8_t* __restrict__ active, const double* __restrict__ diag,
             const int* __restrict__ aggregate, int base_offset, int base_cells, const TC* __restrict__ e, int64_t structured,
             const T* __restrict__ z, const T* __restrict__ r, const T* __restrict__ t, TO* __restrict__ out,
             double* __restrict__ residual, double omega, double scale, const int* __restrict__ map)
@@ -439,22 +437,20 @@ namespace pcfd
             };
             const int a = dof[d];
             double Az = a < structured ? double(t[a]) : 0.0;
+            const double za = value(a);
             const int node = incident[d];
-            if (node >= 0)
+            if (node >= 0 && active[a])
             {
+                // the compact edges' two-point terms, coefficient * (z_a - z_other): the reference's
+                // sign * coefficient * (z_lower - z_upper) bit for bit (exact negations)
                 double sum = 0.0;
                 for (int q = incident_offset[node]; q < incident_offset[node + 1]; ++q)
                 {
-                    const int edge = incident_edge[q];
-                    int lo, hi;
-                    double coefficient;
-                    if (edge < connection_count) { lo = conn_lower[edge]; hi = conn_upper[edge]; coefficient = conn_coefficient[edge]; }
-                    else { const int rr = edge - connection_count; lo = reg_lower[rr]; hi = reg_upper[rr]; coefficient = reg_coefficient[rr]; }
-                    if (active[lo] && active[hi]) sum += double(incident_sign[q]) * (coefficient * (value(lo) - value(hi)));
+                    const int other = incident_other[q];
+                    if (active[other]) sum += incident_coefficient[q] * (za - value(other));
                 }
                 Az += sum;
             }
-            const double za = value(a);
             for (int g = gauge_offset[d]; g < gauge_offset[d + 1]; ++g) Az += gauge_coefficient[g] * za;
             const double D = diag[a];
             if (kMode == 0)
@@ -730,8 +726,7 @@ namespace pcfd
             if (!f.deferred_count) return;
             finish_deferred_kernel<kMode, T, TO, TC, kProlong><<<blocks_for(f.deferred_count), kThreads, 0, launch_stream(s)>>>(
                 f.deferred_count, f.deferred_dof, f.deferred_incident, f.gauge_offset, f.gauge_coefficient, o.incident_offset,
-                o.incident_edge, o.incident_sign, o.connection_count, o.conn_lower, o.conn_upper, o.conn_coefficient, o.reg_lower,
-                o.reg_upper, o.reg_coefficient, s.active, s.diagonal, s.aggregate, s.base_offset, s.base_cells, e, s.structured, z, r,
+                o.incident_other, o.incident_coefficient, s.active, s.diagonal, s.aggregate, s.base_offset, s.base_cells, e, s.structured, z, r,
                 t, out, f.deferred_residual, omega, s.mg_prolong_scale, s.fine_map.p);
         }
 
