@@ -267,8 +267,11 @@ def inflow_profile(speed: float, centres, step: int) -> np.ndarray:
 # DRAM bytes (read + write) per launch of the roofline kernel, from one ncu capture of
 # `bench.py --kernel-only <k> --workload <w>` (--metrics dram__bytes_read.sum,dram__bytes_write.sum,
 # one pass); keyed by (workload, grid, kernel-only component).  A bench run cannot measure DRAM
-# traffic itself; absent entries report null.
-DRAM_BYTES_PER_LAUNCH: dict = {}
+# traffic itself; absent entries report null.  Stage-1 Chebyshev step on the 16 M-cell cut-cell
+# grid: two captured launches read 113.36 MB each and wrote 7.61 and 4.01 MB (mean taken); the
+# algorithmic figure is 129.4 MB, the difference the part of the 2.0 M-row stage the L2 keeps
+# between launches.
+DRAM_BYTES_PER_LAUNCH: dict = {("paraglider16m", "cutcell", 17): 119_170_000}
 
 
 # ------------------------------------------------------------------------------------------ grids
