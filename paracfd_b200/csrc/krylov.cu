@@ -9,10 +9,13 @@
 //   block_dot     h = Q^T w and w.w                          (reads |Q| + 1 vectors)
 //   block_update  w -= Q h, y += sign * U h_U, then h' = Q^T w (reads |Q| + |U| + 2, writes 2)
 // Coefficients stay on the device between passes; the host reads them once per column.
-// All reductions are deterministic: fixed grid, fixed per-block order, fixed final tree.
+// All reductions are deterministic: a grid fixed per kernel and device (one wave of resident CTAs),
+// fixed per-block order, fixed final tree.
 #include "pcfd_internal.h"
 
 #include <algorithm>
+#include <mutex>
+#include <unordered_map>
 
 namespace pcfd
 {
@@ -250,7 +253,7 @@ namespace pcfd
         // s = Q^T v, t = Q^T w, v.v, v.w, w.w -> partial[block][2 * kMaxSet + 3].
         constexpr int kDcgsStride = 2 * kMaxSet + 4;
         template <int V>
-        __global__ void __launch_bounds__(kThreadsBlock, V >= 8 ? 2 : 1) dcgs_dot_kernel(VecSet Q, const double* __restrict__ vv,
+        __global__ void __launch_bounds__(kThreadsBlock, V >= 8 ? 2 : (V >= 4 ? 3 : 4)) dcgs_dot_kernel(VecSet Q, const double* __restrict__ vv,
             const double* __restrict__ w, const uint8_t* __restrict__ active, Sweep range, double* __restrict__ partial)
         {
             __shared__ double shared[kThreadsBlock / 32][kDcgsStride];
@@ -376,7 +379,7 @@ namespace pcfd
 
         // Pass 2: v <- v / r - Q (s / r) in place, next = (w - (c / r) v_old - Q (t - (c / r) s)) / rho.
         template <int V>
-        __global__ void __launch_bounds__(kThreadsBlock, V >= 8 ? 2 : 1) dcgs_update_kernel(VecSet Q, const double* __restrict__ coefficient,
+        __global__ void __launch_bounds__(kThreadsBlock, V >= 8 ? 2 : 4) dcgs_update_kernel(VecSet Q, const double* __restrict__ coefficient,
             double* __restrict__ vv, const double* __restrict__ w, double* __restrict__ next, const uint8_t* __restrict__ active, Sweep range)
         {
             __shared__ double cv[kMaxSet], cw[kMaxSet];
@@ -432,25 +435,41 @@ namespace pcfd
                          s.Sp};
         }
 
-        // Grid of the block kernels; it depends only on the device, so the reduction order is fixed.
-        int block_grid()
+        // Grid of a block kernel: the CTAs that are resident at once (SMs x CTAs per SM that the
+        // kernel's registers allow), at most 592, the partial buffers' row count.  A grid of more
+        // CTAs than fit leaves a second, partly empty wave behind the first, with every CTA
+        // holding the same share of the sweep.  The grid depends only on the kernel and the
+        // device, so the reduction order is fixed.
+        template <typename Kernel>
+        int block_grid(Kernel kernel)
         {
             static int sms = 0;
+            static std::mutex lock;
+            static std::unordered_map<const void*, int> grids;
+            std::lock_guard<std::mutex> guard(lock);
             if (!sms)
             {
                 int device = 0;
                 cuda_check(cudaGetDevice(&device), "device");
                 cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
             }
-            return std::min(592, 4 * sms);
+            const void* key = reinterpret_cast<const void*>(kernel);
+            auto found = grids.find(key);
+            if (found != grids.end()) return found->second;
+            int resident = 0;
+            cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kernel, kThreadsBlock, 0), "block kernel occupancy");
+            const int grid = std::max(1, std::min(592, std::max(1, resident) * sms));
+            grids.emplace(key, grid);
+            return grid;
         }
 
         template <int kMode>
         int launch_block(System& s, const VecSet& Q, const double* h, double* w, const VecSet& U, double sign, double* y)
         {
-            const int grid = block_grid();
             const int m = std::max(Q.size(), U.size());
+            int grid = 0;
             auto go = [&](auto kernel) {
+                grid = block_grid(kernel);
                 kernel<<<grid, kThreadsBlock, 0, launch_stream(s)>>>(Q, h, w, U, sign, y, s.active, sweep_range(s), s.block_partial);
             };
             if (m <= 4) go(block_kernel<1, kMode>);
@@ -465,6 +484,19 @@ namespace pcfd
             for (int g = 0; g < 2; ++g) require(!set.count[g] || aligned16(set.base[g]), what);
             require(set.size() <= 1 || (set.stride * int64_t(sizeof(double))) % 16 == 0, what);
         }
+    }
+
+    void prime_block_grids()
+    {
+        const auto modes = [](auto kernel1, auto kernel2, auto kernel4, auto kernel8) {
+            block_grid(kernel1); block_grid(kernel2); block_grid(kernel4); block_grid(kernel8);
+        };
+        modes(block_kernel<1, -1>, block_kernel<2, -1>, block_kernel<4, -1>, block_kernel<8, -1>);
+        modes(block_kernel<1, 0>, block_kernel<2, 0>, block_kernel<4, 0>, block_kernel<8, 0>);
+        modes(block_kernel<1, 1>, block_kernel<2, 1>, block_kernel<4, 1>, block_kernel<8, 1>);
+        modes(block_kernel<1, 2>, block_kernel<2, 2>, block_kernel<4, 2>, block_kernel<8, 2>);
+        modes(dcgs_dot_kernel<1>, dcgs_dot_kernel<2>, dcgs_dot_kernel<4>, dcgs_dot_kernel<8>);
+        modes(dcgs_update_kernel<1>, dcgs_update_kernel<2>, dcgs_update_kernel<4>, dcgs_update_kernel<8>);
     }
 
     void block_dot(System& s, const VecSet& Q, const double* w, double* out)
@@ -497,16 +529,21 @@ namespace pcfd
         require(Q.size() <= kMaxSet, "delayed CGS2: too many vectors");
         require(aligned16(v) && aligned16(w) && aligned16(next), "delayed CGS2: vector not 16-byte aligned");
         require_aligned(Q, "delayed CGS2: vector not 16-byte aligned");
-        const int grid = block_grid();
         const int m = Q.size();
         const Sweep range = sweep_range(s);
-        auto dot = [&](auto kernel) { kernel<<<grid, kThreadsBlock, 0, launch_stream(s)>>>(Q, v, w, s.active, range, s.dcgs_partial); };
+        int grid = 0;
+        auto dot = [&](auto kernel) {
+            grid = block_grid(kernel);
+            kernel<<<grid, kThreadsBlock, 0, launch_stream(s)>>>(Q, v, w, s.active, range, s.dcgs_partial);
+        };
         if (m <= 4) dot(dcgs_dot_kernel<1>);
         else if (m <= 8) dot(dcgs_dot_kernel<2>);
         else if (m <= 16) dot(dcgs_dot_kernel<4>);
         else dot(dcgs_dot_kernel<8>);
         dcgs_final_kernel<<<1, 256, 0, launch_stream(s)>>>(s.dcgs_partial, grid, m, coefficient);
-        auto update = [&](auto kernel) { kernel<<<grid, kThreadsBlock, 0, launch_stream(s)>>>(Q, coefficient, v, w, next, s.active, range); };
+        auto update = [&](auto kernel) {
+            kernel<<<block_grid(kernel), kThreadsBlock, 0, launch_stream(s)>>>(Q, coefficient, v, w, next, s.active, range);
+        };
         if (m <= 4) update(dcgs_update_kernel<1>);
         else if (m <= 8) update(dcgs_update_kernel<2>);
         else if (m <= 16) update(dcgs_update_kernel<4>);

@@ -128,9 +128,12 @@ namespace pcfd
             return Ticket{h.x, h.y, h.z, h.w, m->nbr[face], m->nbase[face]};
         }
 
-        template <class T, bool kWithR>
+        // kMapped: also the fine -> stage-1 map entries of the same tile positions (mbuf), so that
+        // the prolongation reads them from shared memory instead of waiting on a global load
+        template <class T, bool kWithR, bool kMapped = false>
         __device__ inline void issue_brick(const Ticket& k, const T* __restrict__ z, const T* __restrict__ r,
-                                           const uint8_t* __restrict__ code, T* tile, T* rbuf, uint8_t* cbuf)
+                                           const uint8_t* __restrict__ code, T* tile, T* rbuf, uint8_t* cbuf,
+                                           const int* __restrict__ map = nullptr, int* mbuf = nullptr)
         {
             const int t = threadIdx.x;
             const int64_t base = int64_t(k.slot) * kC3;
@@ -138,6 +141,7 @@ namespace pcfd
                 const int c = 2 * t, i = c & 7, j = (c >> 3) & 7, kk = c >> 6;
                 copy_pair<T>(tile + tix(i, j, kk), z + base + c, true);
                 if (kWithR) copy_pair<T>(rbuf + c, r + base + c, true);
+                if (kMapped) copy8(mbuf + tix(i, j, kk), map + base + c, true);
             }
             if (t < 32) copy16(cbuf + 16 * t, code + base + 16 * t, true);
             const bool valid = k.nbr >= 0;
@@ -149,25 +153,27 @@ namespace pcfd
                 if (face < 4) { kk = w >> 2; i = (w & 3) * 2; j = face == 2 ? kBS - 1 : 0; hj = face == 2 ? -1 : kBS; hk = kk; }
                 else { i = (w * 2) & 7; j = (w * 2) >> 3; kk = face == 4 ? kBS - 1 : 0; hj = j; hk = face == 4 ? -1 : kBS; }
                 copy_pair<T>(tile + tix(i, hj, hk), z + nb + (kk * kBS + j) * kBS + i, valid);
+                if (kMapped) copy8(mbuf + tix(i, hj, hk), map + nb + (kk * kBS + j) * kBS + i, valid);
             }
             else
             {
                 const int u = t - 128, face = u >> 6, j = u & 7, kk = (u >> 3) & 7;
                 const int i = face == 0 ? kBS - 1 : 0, hi = face == 0 ? -1 : kBS;
                 copy_one<T>(tile + tix(hi, j, kk), z + nb + (kk * kBS + j) * kBS + i, valid);
+                if (kMapped) copy4(mbuf + tix(hi, j, kk), map + nb + (kk * kBS + j) * kBS + i, valid);
             }
         }
 
         // adds the coarse correction to the tile entries this thread copied; kMapped: through the
         // fine -> stage-1 map of the composite cycle, else the geometric level-0 cell
         template <class T, class TC, bool kMapped>
-        __device__ inline void prolong_own(const Ticket& k, const TC* __restrict__ e, double scale, const int* __restrict__ map, T* tile)
+        __device__ inline void prolong_own(const Ticket& k, const TC* __restrict__ e, double scale, const int* __restrict__ mbuf, T* tile)
         {
             const int t = threadIdx.x, l = k.level;
             auto add = [&](int s_tile, int64_t q, int b0, int i, int j, int kk) {
                 if (kMapped)
                 {
-                    const int c = map[q];
+                    const int c = mbuf[s_tile];   // map[q], staged with the tile
                     if (c >= 0) tile[s_tile] += T(scale * double(e[c]));
                 }
                 else tile[s_tile] += T(scale * double(e[base_cell_of(b0, l, i, j, kk)]));
@@ -198,12 +204,85 @@ namespace pcfd
             }
         }
 
+        // What the rows the structured 7-point part does not complete need: compact edges (packed
+        // incidence: other endpoint, coefficient), gauges, the assembled diagonal.
+        struct DeferredView
+        {
+            const int* dof;
+            const int* incident;           // row -> incidence node or -1
+            const int* gauge_offset;
+            const double* gauge_coefficient;
+            const int* incident_offset;
+            const int* incident_other;
+            const double* incident_coefficient;
+            const uint8_t* active;
+            const double* diag;
+            const int* aggregate;          // level-0 aggregate per DOF (reference-cycle prolongation)
+            int base_offset, base_cells;
+            double omega;
+        };
+
+        // Completes deferred row d (DOF a) from its structured part Az and right-hand side rc:
+        // the compact-edge gather and the gauges, in the order of the unfused operator.
+        // kFinish 0: z_new into out[a], 1: residual into residual[d], 2: residual into out[a].
+        template <int kFinish, class T, class TO, class TC, int kProlong>
+        __device__ inline void finish_row(const DeferredView& dv, int d, int a, double Az, double rc, const T* __restrict__ z,
+                                          const TC* __restrict__ e, double scale, const int* __restrict__ map,
+                                          TO* __restrict__ out, double* __restrict__ residual)
+        {
+            auto value = [&](int q) {
+                double v = double(z[q]);
+                if (kProlong && dv.active[q])
+                {
+                    if (kProlong == 2)
+                    {
+                        const int c = map[q];
+                        if (c >= 0) v += scale * double(e[c]);
+                    }
+                    else
+                    {
+                        const int c = dv.aggregate[q] - dv.base_offset;
+                        if (c >= 0 && c < dv.base_cells) v += scale * double(e[c]);
+                    }
+                }
+                return v;
+            };
+            const bool on = dv.active[a];
+            const double za = value(a);
+            const int node = dv.incident[d];
+            if (node >= 0 && on)
+            {
+                // the compact edges' two-point terms, coefficient * (z_a - z_other): the reference's
+                // sign * coefficient * (z_lower - z_upper) bit for bit (exact negations)
+                double sum = 0.0;
+                for (int q = dv.incident_offset[node]; q < dv.incident_offset[node + 1]; ++q)
+                {
+                    const int other = dv.incident_other[q];
+                    if (dv.active[other]) sum += dv.incident_coefficient[q] * (za - value(other));
+                }
+                Az += sum;
+            }
+            for (int g = dv.gauge_offset[d]; g < dv.gauge_offset[d + 1]; ++g) Az += dv.gauge_coefficient[g] * za;
+            const double D = dv.diag[a];
+            if (kFinish == 0)
+            {
+                if (!on) out[a] = TO(0);
+                else out[a] = TO(D > 0.0 ? za + dv.omega * (rc - Az) / D : za);
+            }
+            else if (kFinish == 1) residual[d] = on ? rc - Az : 0.0;
+            else out[a] = TO(on ? rc - Az : 0.0);
+        }
+
+        // CTAs of 256 threads the launch bounds keep resident per SM: six for the float sweeps and
+        // the FP64 operator (<= 40 registers, <= 27 KB shared memory), four for the FP64 sweeps.
+        template <int kMode, class T> constexpr int pipe_resident() { return (sizeof(T) == 4 || kMode == 2) ? 6 : 4; }
+
         // kMode 0: Jacobi sweep, 1: residual restriction, 2: structured apply (out = A_struct z)
         // T: field type of z, r, t (double, or float for the FP32 multigrid); TO: output type.
         // kProlong: 0 none, 1 level-0 cell (reference cycle), 2 mapped (composite cycle);
         // kMode 3: write the residual r - A_struct z (composite cycle's first restriction)
         template <int kMode, class T, class TO, class TC, int kProlong>
-        __global__ void __launch_bounds__(256) brick_pipe_kernel(BrickView v, int64_t bricks, const T* __restrict__ z,
+        __global__ void __launch_bounds__(256, pipe_resident<kMode, T>()) brick_pipe_kernel(BrickView v, int64_t bricks, const T* __restrict__ z,
             const T* __restrict__ r, TO* __restrict__ out, T* __restrict__ t, const TC* __restrict__ e,
             double* __restrict__ partial, const T* __restrict__ damping)
         {
@@ -212,11 +291,12 @@ namespace pcfd
             __shared__ __align__(16) T rbuf[kWithR ? 2 : 1][kC3];
             __shared__ __align__(16) uint8_t cbuf[2][kC3];
             __shared__ double residual[kMode == 1 ? kC3 : 1];
+            __shared__ __align__(16) int mbuf[kProlong == 2 ? 2 : 1][kProlong == 2 ? kTileSize : 1];   // staged map entries
             int64_t b = blockIdx.x;
             if (b >= bricks) return;
             const int64_t G = gridDim.x;
             Ticket cur = load_ticket(v.meta, b);
-            issue_brick<T, kWithR>(cur, z, r, v.code, tile[0], rbuf[0], cbuf[0]);
+            issue_brick<T, kWithR, kProlong == 2>(cur, z, r, v.code, tile[0], rbuf[0], cbuf[0], v.map, mbuf[0]);
             copy_commit();
             Ticket next = b + G < bricks ? load_ticket(v.meta, b + G) : cur;
             for (int it = 0;; ++it)
@@ -226,13 +306,14 @@ namespace pcfd
                 Ticket after = next;
                 if (has_next)
                 {
-                    issue_brick<T, kWithR>(next, z, r, v.code, tile[st ^ 1], rbuf[kWithR ? (st ^ 1) : 0], cbuf[st ^ 1]);
+                    issue_brick<T, kWithR, kProlong == 2>(next, z, r, v.code, tile[st ^ 1], rbuf[kWithR ? (st ^ 1) : 0], cbuf[st ^ 1],
+                                                          v.map, mbuf[kProlong == 2 ? (st ^ 1) : 0]);
                     copy_commit();
                     if (b + 2 * G < bricks) after = load_ticket(v.meta, b + 2 * G);
                     copy_wait<1>();
                 }
                 else copy_wait<0>();
-                if (kProlong) prolong_own<T, TC, kProlong == 2>(cur, e, v.prolong, v.map, tile[st]);
+                if (kProlong) prolong_own<T, TC, kProlong == 2>(cur, e, v.prolong, mbuf[kProlong == 2 ? st : 0], tile[st]);
                 __syncthreads();
                 // ---- compute brick `cur` from buffer st.  Thread t owns cells t and t + 256, so a
                 // warp reads consecutive doubles of the tile (no shared-memory bank replays).
@@ -404,62 +485,22 @@ namespace pcfd
             if (q < end) z[q] = active[q] && diag[q] > 0.0 ? omega * r[q] / diag[q] : 0.0;
         }
 
-        // Completes deferred rows: A_orth z = t (structured part) + compact-edge gather + gauges,
-        // in the order of the unfused launch; kMode 0 writes z_new, 1 writes the row residual.
+        // Completes deferred rows after the pipeline launch: A_orth z = t (structured part) +
+        // compact-edge gather + gauges.  One thread per row: the rows are a sparse, irregular
+        // subset (cut cells, coarse/fine interfaces), so a launch of their own keeps every SM busy
+        // where finishing them inside the brick CTAs left most threads idle (measured slower).
         // kMode 0: z_new, 1: residual into the compact deferred list, 2: residual into out[a]
         template <int kMode, class T, class TO, class TC, int kProlong>
-        __global__ void finish_deferred_kernel(int count, const int* __restrict__ dof, const int* __restrict__ incident,
-            const int* __restrict__ gauge_offset, const double* __restrict__ gauge_coefficient,
-            const int* __restrict__ incident_offset, const int* __restrict__ incident_other,
-            const double* __restrict__ incident_coefficient, const uint8_t* __restrict__ active, const double* __restrict__ diag,
-            const int* __restrict__ aggregate, int base_offset, int base_cells, const TC* __restrict__ e, int64_t structured,
-            const T* __restrict__ z, const T* __restrict__ r, const T* __restrict__ t, TO* __restrict__ out,
-            double* __restrict__ residual, double omega, double scale, const int* __restrict__ map)
+        __global__ void finish_deferred_kernel(DeferredView dv, int count, int64_t structured, const TC* __restrict__ e,
+                                               double scale, const int* __restrict__ map, const T* __restrict__ z,
+                                               const T* __restrict__ r, const T* __restrict__ t, TO* __restrict__ out,
+                                               double* __restrict__ residual)
         {
             const int d = blockIdx.x * blockDim.x + threadIdx.x;
             if (d >= count) return;
-            auto value = [&](int q) {
-                double v = double(z[q]);
-                if (kProlong && active[q])
-                {
-                    if (kProlong == 2)
-                    {
-                        const int c = map[q];
-                        if (c >= 0) v += scale * double(e[c]);
-                    }
-                    else
-                    {
-                        const int c = aggregate[q] - base_offset;
-                        if (c >= 0 && c < base_cells) v += scale * double(e[c]);
-                    }
-                }
-                return v;
-            };
-            const int a = dof[d];
-            double Az = a < structured ? double(t[a]) : 0.0;
-            const double za = value(a);
-            const int node = incident[d];
-            if (node >= 0 && active[a])
-            {
-                // the compact edges' two-point terms, coefficient * (z_a - z_other): the reference's
-                // sign * coefficient * (z_lower - z_upper) bit for bit (exact negations)
-                double sum = 0.0;
-                for (int q = incident_offset[node]; q < incident_offset[node + 1]; ++q)
-                {
-                    const int other = incident_other[q];
-                    if (active[other]) sum += incident_coefficient[q] * (za - value(other));
-                }
-                Az += sum;
-            }
-            for (int g = gauge_offset[d]; g < gauge_offset[d + 1]; ++g) Az += gauge_coefficient[g] * za;
-            const double D = diag[a];
-            if (kMode == 0)
-            {
-                if (!active[a]) out[a] = TO(0);
-                else out[a] = TO(D > 0.0 ? za + omega * (double(r[a]) - Az) / D : za);
-            }
-            else if (kMode == 1) residual[d] = active[a] ? double(r[a]) - Az : 0.0;
-            else out[a] = TO(active[a] ? double(r[a]) - Az : 0.0);
+            const int a = dv.dof[d];
+            finish_row<kMode, T, TO, TC, kProlong>(dv, d, a, a < structured ? double(t[a]) : 0.0, double(r[a]), z, e, scale, map,
+                                                   out, residual);
         }
 
         // base-level right-hand side: brick partials (levels in order) then deferred-row residuals
@@ -718,18 +759,30 @@ namespace pcfd
                              s.fine_map.p};
         }
 
+        // the deferred rows' arrays
+        DeferredView deferred_view(System& s, double omega)
+        {
+            FineSmoother& f = s.fine;
+            const IrregularOperator& o = s.irr;
+            return DeferredView{f.deferred_dof, f.deferred_incident, f.gauge_offset, f.gauge_coefficient, o.incident_offset,
+                                o.incident_other, o.incident_coefficient, s.active, s.diagonal, s.aggregate, s.base_offset,
+                                s.base_cells, omega};
+        }
+
         template <int kMode, class T, class TO, class TC, int kProlong>
         void finish(System& s, const T* z, const T* r, TO* out, const TC* e, const T* t, double omega = 2.0 / 3.0)
         {
             FineSmoother& f = s.fine;
-            const IrregularOperator& o = s.irr;
             if (!f.deferred_count) return;
             finish_deferred_kernel<kMode, T, TO, TC, kProlong><<<blocks_for(f.deferred_count), kThreads, 0, launch_stream(s)>>>(
-                f.deferred_count, f.deferred_dof, f.deferred_incident, f.gauge_offset, f.gauge_coefficient, o.incident_offset,
-                o.incident_other, o.incident_coefficient, s.active, s.diagonal, s.aggregate, s.base_offset, s.base_cells, e, s.structured, z, r,
-                t, out, f.deferred_residual, omega, s.mg_prolong_scale, s.fine_map.p);
+                deferred_view(s, omega), f.deferred_count, s.structured, e, s.mg_prolong_scale, s.fine_map.p, z, r, t, out,
+                f.deferred_residual);
         }
 
+        // Persistent grid of a pipeline kernel: the system's CTAs per SM (autotuned), capped by the
+        // kernel's guaranteed residency (its launch bounds), so that no CTA waits for a second
+        // wave while the others run.
+        template <int kMode, class T>
         int pipe_grid(const System& s)
         {
             static int sms = 0;
@@ -739,7 +792,7 @@ namespace pcfd
                 cuda_check(cudaGetDevice(&device), "device");
                 cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SM count");
             }
-            return std::max(1, std::min(s.active_bricks, s.pipe_ctas_per_sm * sms));
+            return std::max(1, std::min(s.active_bricks, std::min(s.pipe_ctas_per_sm, pipe_resident<kMode, T>()) * sms));
         }
 
         // the working buffers of the fine level in field type T
@@ -765,9 +818,10 @@ namespace pcfd
             FineBuffers<T> w(s.fine);
             const bool cheb = slot >= 0 && w.chebyshev;
             const T* damping = cheb ? w.chebyshev + size_t(slot) * s.fine.cheb_stride : w.damping;
-            brick_pipe_kernel<0, T, TO, TC, kProlong><<<pipe_grid(s), 256, 0, launch_stream(s)>>>(
+            const double omega = cheb ? s.fine.cheb_omega[slot] : 2.0 / 3.0;
+            brick_pipe_kernel<0, T, TO, TC, kProlong><<<pipe_grid<0, T>(s), 256, 0, launch_stream(s)>>>(
                 view(s), s.active_bricks, z, r, out, w.t, e, nullptr, damping);
-            finish<0, T, TO, TC, kProlong>(s, z, r, out, e, w.t, cheb ? s.fine.cheb_omega[slot] : 2.0 / 3.0);
+            finish<0, T, TO, TC, kProlong>(s, z, r, out, e, w.t, omega);
         }
         // the first pre-sweep from z = 0 (slot 0 of the schedule when it is on)
         template <class T> void first_sweep(System& s, const double* r, T* z, T* r_copy)
@@ -785,7 +839,7 @@ namespace pcfd
         {
             FineSmoother& f = s.fine;
             FineBuffers<T> w(f);
-            brick_pipe_kernel<1, T, T, double, 0><<<pipe_grid(s), 256, 0, launch_stream(s)>>>(
+            brick_pipe_kernel<1, T, T, double, 0><<<pipe_grid<1, T>(s), 256, 0, launch_stream(s)>>>(
                 view(s), s.active_bricks, z, r, nullptr, w.t, nullptr, f.partial, w.damping);
             finish<1, T, T, double, 0>(s, z, r, nullptr, nullptr, w.t);
         }
@@ -793,7 +847,7 @@ namespace pcfd
 
     void brick_apply(System& s, const double* p, double* out)
     {
-        brick_pipe_kernel<2, double, double, double, 0><<<pipe_grid(s), 256, 0, launch_stream(s)>>>(
+        brick_pipe_kernel<2, double, double, double, 0><<<pipe_grid<2, double>(s), 256, 0, launch_stream(s)>>>(
             view(s), s.active_bricks, p, nullptr, out, nullptr, nullptr, nullptr, nullptr);
     }
 
@@ -906,7 +960,7 @@ namespace pcfd
             FineSmoother& f = s.fine;
             double* a = f.z.p;
             double* res = s.fine_residual.p;
-            brick_pipe_kernel<3, double, double, TC, 0><<<pipe_grid(s), 256, 0, launch_stream(s)>>>(
+            brick_pipe_kernel<3, double, double, TC, 0><<<pipe_grid<3, double>(s), 256, 0, launch_stream(s)>>>(
                 view(s), s.active_bricks, z, r, res, f.t.p, nullptr, nullptr, f.damping.p);
             finish<2, double, double, TC, 0>(s, z, r, res, static_cast<const TC*>(nullptr), f.t.p);
             gather_first_kernel<TC, double><<<blocks_for(first.cells), kThreads, 0, launch_stream(s)>>>(
@@ -928,7 +982,7 @@ namespace pcfd
             float *a = f.z32.p, *b = f.z32b.p, *r32 = f.r32.p, *res = f.res32.p;
             first_sweep<float>(s, r, a, r32);
             sweep<float, float, float, 0>(s, a, r32, b, nullptr, 1);
-            brick_pipe_kernel<3, float, float, float, 0><<<pipe_grid(s), 256, 0, launch_stream(s)>>>(
+            brick_pipe_kernel<3, float, float, float, 0><<<pipe_grid<3, float>(s), 256, 0, launch_stream(s)>>>(
                 view(s), s.active_bricks, b, r32, res, f.t32.p, nullptr, nullptr, f.damping32.p);
             finish<2, float, float, float, 0>(s, b, r32, res, static_cast<const float*>(nullptr), f.t32.p);
             gather_first_kernel<float, float><<<blocks_for(first.cells), kThreads, 0, launch_stream(s)>>>(
