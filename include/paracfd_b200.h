@@ -464,6 +464,24 @@ pcfd_status pcfd_locate_points_device(pcfd_system* system, const float* d_points
 pcfd_status pcfd_sample_slice_host(pcfd_system* system, const double origin[3], const double edge_u[3],
                                    const double edge_v[3], int32_t nu, int32_t nv, int32_t field, float* out);
 
+/* ---- staggered MAC momentum mode ---------------------------------------------------------- */
+/* The reference's non-default momentum path, DeviceAmrAdvection (amr_advection.cu:1652-1690), on
+ * the resident face velocities (pcfd_set_faces_host / pcfd_get_faces_host, compact per-brick
+ * layout).  Link bytes per face [F] each (host), the caller's geometry preprocessing as in the
+ * DeviceAmrAdvection constructor: bits 0..5 the open -x,+x,-y,+y,-z,+z same-side links, bit 6 the
+ * near-fabric band; faces away from the fabric 0x3f. */
+pcfd_status pcfd_mac_set_links(pcfd_system* system, const uint8_t* links_u, const uint8_t* links_v, const uint8_t* links_w);
+/* DeviceAmrAdvection::advect (amr_advection.cu:1663-1671): MacCormack semi-Lagrangian advection of
+ * every face of every level over dt (FP32, dt rounded to FP32), band faces by the limited MUSCL
+ * update; faces of covered bricks become 0.  Needs the links. */
+pcfd_status pcfd_mac_advect(pcfd_system* system, double dt);
+/* DeviceAmrAdvection::diffuse_smagorinsky (amr_advection.cu:1683-1690): Smagorinsky eddy viscosity
+ * per cell, then one explicit face-diffusion step (nu + mean nut across the face; band faces: nu
+ * along their open links). */
+pcfd_status pcfd_mac_diffuse_smagorinsky(pcfd_system* system, double nu, double cs, double dt);
+/* The cell eddy viscosity [S] (host, FP32) of the last pcfd_mac_diffuse_smagorinsky. */
+pcfd_status pcfd_mac_eddy_viscosity_host(pcfd_system* system, float* nut);
+
 /* ---- instrumentation ---------------------------------------------------------------------- */
 /* Average device time of one launch sequence of `which` (0 full apply, 1 orthogonal apply,
  * 2 preconditioner, 3 divergence, 4 flux correction, 5 FP64 dot, 6/7/8 preconditioner

@@ -96,6 +96,15 @@ def lib():
         L.ref_case_from_mesh_eb.argtypes = [f64p, C.c_int64, C.POINTER(C.c_uint32), C.c_int64, f64p, f64p, C.c_double,
                                             C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double,
                                             C.c_double]
+        u8p = C.POINTER(C.c_uint8)
+        L.ref_mac_links.argtypes = [vp, C.c_double, u8p, u8p, u8p]
+        L.ref_mac_create.restype = vp
+        L.ref_mac_create.argtypes = [vp, C.c_double]
+        L.ref_mac_destroy.argtypes = [vp]
+        L.ref_mac_set_faces.argtypes = [vp, f32p, f32p, f32p]
+        L.ref_mac_advect.argtypes = [vp, C.c_double]
+        L.ref_mac_diffuse_smagorinsky.argtypes = [vp, C.c_double, C.c_double, C.c_double]
+        L.ref_mac_state.argtypes = [vp, f32p, f32p, f32p, f32p]
         _lib = L
     return _lib
 
@@ -264,6 +273,50 @@ class RefCase:
                                           ptr(np.asarray(cf, np.float64), C.c_double), ptr(np.asarray(eb, np.float64), C.c_double),
                                           int(external), C.byref(out)))
         return out.value
+
+
+    def mac_links(self, protection_cells=2.5):
+        """The reference advection's per-face link bytes (compact layout), from the case surface."""
+        out = [np.zeros(self.faces, np.uint8) for _ in range(3)]
+        _check(lib().ref_mac_links(self.handle, protection_cells, *(ptr(a, C.c_uint8) for a in out)))
+        return out
+
+
+class RefMac:
+    """The reference's staggered MAC momentum path (DeviceAmrAdvection on DeviceAmrFields); needs a GPU."""
+
+    def __init__(self, case: RefCase, protection_cells=2.5):
+        self.case = case
+        self.handle = lib().ref_mac_create(case.handle, protection_cells)
+        if not self.handle:
+            raise RuntimeError("reference MAC: " + lib().ref_last_error().decode(errors="replace"))
+
+    def set_faces(self, u, v, w):
+        a = [np.ascontiguousarray(x, np.float32) for x in (u, v, w)]
+        _check(lib().ref_mac_set_faces(self.handle, *(ptr(x, C.c_float) for x in a)))
+
+    def advect(self, dt):
+        _check(lib().ref_mac_advect(self.handle, dt))
+
+    def diffuse_smagorinsky(self, nu, cs, dt):
+        _check(lib().ref_mac_diffuse_smagorinsky(self.handle, nu, cs, dt))
+
+    def state(self):
+        u, v, w = (np.zeros(self.case.faces, np.float32) for _ in range(3))
+        nut = np.zeros(self.case.n, np.float32)
+        _check(lib().ref_mac_state(self.handle, *(ptr(x, C.c_float) for x in (u, v, w, nut))))
+        return (u, v, w), nut
+
+    def close(self):
+        if self.handle:
+            lib().ref_mac_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class RefCore:

@@ -1172,6 +1172,152 @@ int ref_device_core_step(void* handle, double* stats)
     });
 }
 
+namespace
+{
+    // The reference's staggered MAC momentum objects on one case (amr_advection.cu:1652-1690).
+    struct RefMac
+    {
+        RefCase* c = nullptr;
+        std::unique_ptr<DeviceAmrFields> fields;
+        std::unique_ptr<DeviceAmrAdvection> advection;
+    };
+    Vec3d mac_face_centre(const BrickMetadata& brick, double h, int component, int i, int j, int k)
+    {
+        return brick.origin + Vec3d{(i + (component == 0 ? 0.0 : 0.5)) * h, (j + (component == 1 ? 0.0 : 0.5)) * h,
+                                    (k + (component == 2 ? 0.0 : 0.5)) * h};
+    }
+}
+
+// The per-face link bytes of the DeviceAmrAdvection constructor (amr_advection.cu:1655-1659):
+// every face 0x3f; in a brick whose box grown by protection_cells * h meets the surface, a face
+// within that distance of it takes 0x40 plus, when it is off the surface, one bit per axis
+// direction whose h-long segment does not cross the surface; then the interface links that the
+// composite momentum coupling replaces (build_momentum_interface_replaced_links) are cleared.
+// Compact per-brick face layout.
+int ref_mac_links(void* case_handle, double protection_cells, uint8_t* lu, uint8_t* lv, uint8_t* lw)
+{
+    return guarded([&] {
+        RefCase& c = *static_cast<RefCase*>(case_handle);
+        if (!c.bvh) throw std::invalid_argument("MAC links need a case with a surface");
+        const int bs = c.system.brick_size;
+        const std::size_t per = std::size_t((bs + 1) * bs * bs);
+        const std::vector<AmrMacFaceDirectionalLink> replaced = build_momentum_interface_replaced_links(c.system);
+        uint8_t* out[3] = {lu, lv, lw};
+        auto compact = [&](int component, std::size_t slot, int i, int j, int k) {
+            return component == 0 ? u_compact(bs, slot, i, j, k) : (component == 1 ? v_compact(bs, slot, i, j, k) : w_compact(bs, slot, i, j, k));
+        };
+        for (int l = 0; l < int(c.hierarchy.levels().size()); ++l)
+        {
+            const AmrLevel& level = c.hierarchy.levels()[l];
+            const std::size_t slot0 = std::size_t(c.system.level_offset[l]) / std::size_t(bs * bs * bs);
+            for (int comp = 0; comp < 3; ++comp) std::fill(out[comp] + slot0 * per, out[comp] + (slot0 + level.bricks.size()) * per, uint8_t(0x3f));
+            const double radius = protection_cells * level.h;
+            for (int b = 0; b < int(level.bricks.size()); ++b)
+            {
+                const BrickMetadata& record = level.bricks[b];
+                if (!record.active()) continue;
+                const Aabb3d grown{{record.origin.x - radius, record.origin.y - radius, record.origin.z - radius},
+                                   {record.origin.x + bs * level.h + radius, record.origin.y + bs * level.h + radius,
+                                    record.origin.z + bs * level.h + radius}};
+                if (c.bvh->query_aabb(grown).empty()) continue;
+                for (int comp = 0; comp < 3; ++comp)
+                {
+                    const int ni = comp == 0 ? bs + 1 : bs, nj = comp == 1 ? bs + 1 : bs, nk = comp == 2 ? bs + 1 : bs;
+                    for (int k = 0; k < nk; ++k)
+                        for (int j = 0; j < nj; ++j)
+                            for (int i = 0; i < ni; ++i)
+                            {
+                                const Vec3d point = mac_face_centre(record, level.h, comp, i, j, k);
+                                const double distance = c.bvh->distance(point, radius);
+                                if (!std::isfinite(distance)) continue;
+                                uint8_t links = 0x40;
+                                if (distance > 1e-7 * level.h)
+                                    for (int axis = 0; axis < 3; ++axis)
+                                        for (int direction = -1; direction <= 1; direction += 2)
+                                        {
+                                            Vec3d other = point;
+                                            other[axis] += direction * level.h;
+                                            if (!c.bvh->intersect_segment(point, other, 1e-7, 1.0 - 1e-7).hit)
+                                                links |= uint8_t(1u << (2 * axis + (direction > 0)));
+                                        }
+                                out[comp][compact(comp, slot0 + b, i, j, k)] = links;
+                            }
+                }
+            }
+            for (const AmrMacFaceDirectionalLink& link : replaced)
+                if (link.face.level == l)
+                    out[link.face.component][compact(link.face.component, slot0 + link.face.brick, link.face.i, link.face.j, link.face.k)] &=
+                        uint8_t(~(1u << (2 * link.transport_axis + (link.direction > 0))));
+        }
+    });
+}
+
+void* ref_mac_create(void* case_handle, double protection_cells)
+{
+    RefMac* out = nullptr;
+    guarded([&] {
+        auto m = std::make_unique<RefMac>();
+        m->c = static_cast<RefCase*>(case_handle);
+        if (!m->c->bvh) throw std::invalid_argument("MAC advection needs a case with a surface");
+        m->fields = std::make_unique<DeviceAmrFields>(m->c->hierarchy);
+        m->advection = std::make_unique<DeviceAmrAdvection>(m->c->hierarchy, *m->c->bvh, protection_cells, &m->c->system);
+        out = m.release();
+    });
+    return out;
+}
+
+void ref_mac_destroy(void* mac) { delete static_cast<RefMac*>(mac); }
+
+int ref_mac_set_faces(void* mac, const float* u, const float* v, const float* w)
+{
+    return guarded([&] {
+        RefMac& m = *static_cast<RefMac*>(mac);
+        AmrHostFields host(m.c->hierarchy);
+        to_host_fields(*m.c, u, v, w, host);
+        m.fields->upload(host);
+    });
+}
+
+int ref_mac_advect(void* mac, double dt)
+{
+    return guarded([&] {
+        RefMac& m = *static_cast<RefMac*>(mac);
+        m.advection->advect(*m.fields, Real(dt));
+    });
+}
+
+int ref_mac_diffuse_smagorinsky(void* mac, double nu, double cs, double dt)
+{
+    return guarded([&] {
+        RefMac& m = *static_cast<RefMac*>(mac);
+        m.advection->diffuse_smagorinsky(*m.fields, Real(nu), Real(cs), Real(dt));
+    });
+}
+
+int ref_mac_state(void* mac, float* u, float* v, float* w, float* nut)
+{
+    return guarded([&] {
+        RefMac& m = *static_cast<RefMac*>(mac);
+        AmrHostFields host(m.c->hierarchy);
+        m.fields->download(host);
+        from_host_fields(*m.c, host, u, v, w);
+        if (nut)
+        {
+            const int bs = m.c->system.brick_size;
+            for (int l = 0; l < int(m.c->hierarchy.levels().size()); ++l)
+            {
+                const auto& lv = host.levels()[l];
+                const std::size_t slot0 = std::size_t(m.c->system.level_offset[l]) / std::size_t(bs * bs * bs);
+                for (int b = 0; b < int(m.c->hierarchy.levels()[l].bricks.size()); ++b)
+                    for (int k = 0; k < bs; ++k)
+                        for (int j = 0; j < bs; ++j)
+                            for (int i = 0; i < bs; ++i)
+                                nut[(slot0 + b) * std::size_t(bs * bs * bs) + std::size_t((k * bs + j) * bs + i)] = lv.nut[lv.layout.cell_index(b, i, j, k)];
+            }
+        }
+    });
+}
+
 void* ref_core_create(void* case_handle, const ref_core_case* cfg)
 {
     RefCore* out = nullptr;

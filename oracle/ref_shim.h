@@ -128,6 +128,17 @@ int ref_device_core_step(void* core, double* stats6);
 /* Cell-momentum state [S] (FP32) and the FP32 pressure shadow widened to double [S]. */
 int ref_device_core_state(void* core, float* x, float* y, float* z, double* pressure);
 
+/* The reference's staggered MAC momentum path (DeviceAmrAdvection on DeviceAmrFields,
+ * amr_advection.cu:1652-1690) on a case with a surface; faces [B][(bs+1) bs^2] per component in the
+ * compact per-brick layout, nut [S].  ref_mac_links: the constructor's per-face link bytes. */
+int ref_mac_links(void* case_handle, double protection_cells, uint8_t* links_u, uint8_t* links_v, uint8_t* links_w);
+void* ref_mac_create(void* case_handle, double protection_cells);
+void ref_mac_destroy(void* mac);
+int ref_mac_set_faces(void* mac, const float* u, const float* v, const float* w);
+int ref_mac_advect(void* mac, double dt);
+int ref_mac_diffuse_smagorinsky(void* mac, double nu, double cs, double dt);
+int ref_mac_state(void* mac, float* u, float* v, float* w, float* nut);
+
 /* The reference's own GPU path (ExternalAeroCore on the fixture), for the sm_100a baseline arm. */
 void* ref_core_create(void* case_handle, const ref_core_case* config);
 void ref_core_destroy(void* core);

@@ -210,6 +210,23 @@ class CompositeSystem:
         check(self._lib.pcfd_get_faces_host(self.handle, ptr(u, C.c_float), ptr(v, C.c_float), ptr(w, C.c_float)))
         return u, v, w
 
+    # ---- staggered MAC momentum mode (DeviceAmrAdvection) ----
+    def set_mac_links(self, links_u, links_v, links_w):
+        """Per-face link bytes [faces] each: bits 0..5 open same-side links, bit 6 near-fabric band."""
+        lu, lv, lw = (np.ascontiguousarray(a, np.uint8) for a in (links_u, links_v, links_w))
+        check(self._lib.pcfd_mac_set_links(self.handle, ptr(lu, C.c_uint8), ptr(lv, C.c_uint8), ptr(lw, C.c_uint8)))
+
+    def mac_advect(self, dt: float):
+        check(self._lib.pcfd_mac_advect(self.handle, dt))
+
+    def mac_diffuse_smagorinsky(self, nu: float, cs: float, dt: float):
+        check(self._lib.pcfd_mac_diffuse_smagorinsky(self.handle, nu, cs, dt))
+
+    def mac_eddy_viscosity(self) -> np.ndarray:
+        out = np.empty(self.storage_size, np.float32)
+        check(self._lib.pcfd_mac_eddy_viscosity_host(self.handle, ptr(out, C.c_float)))
+        return out
+
     def set_special(self, coarse_fine, embedded):
         cf = np.ascontiguousarray(coarse_fine, np.float32)
         eb = np.ascontiguousarray(embedded, np.float32)

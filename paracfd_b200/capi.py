@@ -248,6 +248,10 @@ SIGNATURES = {
     "pcfd_locate_points_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     "pcfd_sample_slice_host": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
                                          C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_float)]),
+    "pcfd_mac_set_links": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint8), C.POINTER(C.c_uint8), C.POINTER(C.c_uint8)]),
+    "pcfd_mac_advect": (C.c_int, [C.c_void_p, C.c_double]),
+    "pcfd_mac_diffuse_smagorinsky": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double]),
+    "pcfd_mac_eddy_viscosity_host": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
 }
 
 _lib = None

@@ -268,6 +268,7 @@ namespace pcfd
             s.dcgs_result.alloc(size_t(kDcgsCoefficients));
             cuda_check(cudaMallocHost(&s.pinned_dcgs, size_t(2) * kDcgsCoefficients * sizeof(double)), "pinned orthogonalisation scalars");
             for (cudaEvent_t& e : s.dcgs_ready) cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "column event");
+            prime_block_grids();
             // flow state
             s.u.alloc(size_t(s.faces)); s.v.alloc(size_t(s.faces)); s.w.alloc(size_t(s.faces));
             s.divergence.alloc(size_t(s.S));
@@ -280,6 +281,7 @@ namespace pcfd
             build_momentum(s, *s.momentum, t, options ? options->momentum_min_volume_fraction : 0.0);
             build_loads(s, t);
             build_locator(s, t);
+            build_mac(s, t);
             cuda_check(cudaDeviceSynchronize(), "system setup");
         }
 
@@ -332,6 +334,7 @@ namespace pcfd
         if (mg_graph32) cudaGraphExecDestroy(mg_graph32);
         destroy_loads(*this);
         destroy_locator(*this);
+        destroy_mac(*this);
         delete momentum;
         if (pinned) cudaFreeHost(pinned);
         if (pinned_block) cudaFreeHost(pinned_block);
@@ -781,6 +784,46 @@ pcfd_status pcfd_sample_slice_host(pcfd_system* system, const double origin[3], 
         sample_slice(s, origin, edge_u, edge_v, nu, nv, field, s.slice_buffer.p);
         d2h(s, out, s.slice_buffer.p, n);
         sync(s);
+    });
+}
+
+pcfd_status pcfd_mac_set_links(pcfd_system* system, const uint8_t* links_u, const uint8_t* links_v, const uint8_t* links_w)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(links_u && links_v && links_w, "null MAC link array");
+        const uint8_t* host[3] = {links_u, links_v, links_w};
+        mac_set_links(s, host);
+    });
+}
+
+pcfd_status pcfd_mac_advect(pcfd_system* system, double dt)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(std::isfinite(dt) && dt > 0.0, "MAC advection timestep must be positive");
+        mac_advect(s, float(dt));
+        sync(s);
+    });
+}
+
+pcfd_status pcfd_mac_diffuse_smagorinsky(pcfd_system* system, double nu, double cs, double dt)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(std::isfinite(nu) && std::isfinite(cs) && std::isfinite(dt) && nu >= 0.0 && cs >= 0.0 && dt > 0.0,
+                "invalid MAC LES/diffusion parameters");
+        mac_diffuse_smagorinsky(s, float(nu), float(cs), float(dt));
+        sync(s);
+    });
+}
+
+pcfd_status pcfd_mac_eddy_viscosity_host(pcfd_system* system, float* nut)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(nut != nullptr, "null eddy-viscosity buffer");
+        mac_eddy_viscosity(s, nut);
     });
 }
 

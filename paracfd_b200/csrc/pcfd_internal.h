@@ -287,6 +287,7 @@ namespace pcfd
         struct Momentum* momentum = nullptr;
         void* loads = nullptr;                  // surface-load integration state (loads.cu)
         void* locator = nullptr;                // point location / slice sampling state (locator.cu)
+        void* mac = nullptr;                    // staggered MAC momentum state (mac.cu)
         DBuf<float> slice_buffer;               // device output of pcfd_sample_slice_host
         cudaEvent_t markers[8] = {};
         int64_t launches = 0;                   // kernels launched on the system stream so far
@@ -389,6 +390,8 @@ namespace pcfd
     // delayed CGS2 column step: reorthogonalise v against Q in place and write the next basis vector
     // from w; coefficient[0..4*kMaxSet+9) as dcgs_final_kernel documents (krylov.cu)
     void dcgs_pass(System& s, const VecSet& Q, double* v, const double* w, double* next, double* coefficient);
+    // looks up the grid of every block kernel once (an occupancy query), before any stream capture
+    void prime_block_grids();
     constexpr int kDcgsCoefficients = 4 * kMaxSet + 9;
 
     // ---- projection (projection.cu) ----
@@ -404,6 +407,13 @@ namespace pcfd
     // point location and slice sampling (locator.cu)
     void build_locator(System& s, const pcfd_topology& t);
     void destroy_locator(System& s);
+    // staggered MAC momentum mode (mac.cu)
+    void build_mac(System& s, const pcfd_topology& t);
+    void destroy_mac(System& s);
+    void mac_set_links(System& s, const uint8_t* const host[3]);
+    void mac_advect(System& s, float dt);
+    void mac_diffuse_smagorinsky(System& s, float nu, float cs, float dt);
+    void mac_eddy_viscosity(System& s, float* host_nut);
     void locate_points(System& s, const float* d_points, int count, int* d_out);
     void sample_slice(System& s, const double origin[3], const double edge_u[3], const double edge_v[3], int nu, int nv,
                       int field, float* d_out);   // [max |div|, rms, worst V, max |div V|, sum |div V|, sum div V]
