@@ -77,9 +77,9 @@ def parse_args():
     ap.add_argument("--restart", type=int, default=0, help="GCRO columns per cycle (0: the reference's 24)")
     ap.add_argument("--mg-cycle", choices=("reference", "corrected", "composite"), default="composite",
                     help="coarse-correction weighting of the multigrid cycle (pcfd_mg_cycle)")
-    ap.add_argument("--stage-sweeps", type=int, default=0,
-                    help="composite cycle: smoothing steps per stage before and after its correction (0: 6)")
-    ap.add_argument("--chebyshev", type=int, default=0,
+    ap.add_argument("--stage-sweeps", type=int, default=4,
+                    help="composite cycle: smoothing steps per stage before and after its correction (0: the library's 6)")
+    ap.add_argument("--chebyshev", type=int, default=20,
                     help="composite stages: r >= 2 = Chebyshev smoothing on [2/r, 2], 1 = damped Jacobi, 0: r = 30")
     ap.add_argument("--fine-chebyshev", type=int, default=0,
                     help="composite fine sweeps: r >= 2 = Chebyshev-Richardson steps on [2/r, 2], 1 = damped Jacobi, 0: r = 10")

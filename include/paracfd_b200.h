@@ -465,6 +465,14 @@ pcfd_status pcfd_sample_slice_host(pcfd_system* system, const double origin[3], 
                                    const double edge_v[3], int32_t nu, int32_t nv, int32_t field, float* out);
 
 /* ---- staggered MAC momentum mode ---------------------------------------------------------- */
+/* Momentum path of pcfd_core_initialize / pcfd_core_step (ExternalAeroExecutionOptions::
+ * conservative_cell_momentum, external_aero_core.h:108-113). */
+typedef enum pcfd_momentum_mode {
+    PCFD_MOMENTUM_CELL = 0,   /* conservative cell momentum (the reference's default) */
+    PCFD_MOMENTUM_MAC = 1     /* staggered MAC faces: needs pcfd_mac_set_links */
+} pcfd_momentum_mode;
+/* Selects the momentum path; the core needs pcfd_core_initialize again afterwards. */
+pcfd_status pcfd_core_set_momentum_mode(pcfd_system* system, int32_t mode);
 /* The reference's non-default momentum path, DeviceAmrAdvection (amr_advection.cu:1652-1690), on
  * the resident face velocities (pcfd_set_faces_host / pcfd_get_faces_host, compact per-brick
  * layout).  Link bytes per face [F] each (host), the caller's geometry preprocessing as in the
@@ -479,6 +487,12 @@ pcfd_status pcfd_mac_advect(pcfd_system* system, double dt);
  * per cell, then one explicit face-diffusion step (nu + mean nut across the face; band faces: nu
  * along their open links). */
 pcfd_status pcfd_mac_diffuse_smagorinsky(pcfd_system* system, double nu, double cs, double dt);
+/* DeviceCompositeAmrProjection::transport_embedded_apertures(dt, nu, cs, false) (amr_pressure.cu:
+ * 1868-1911), the MAC step's transport of the compact embedded face velocities (special slots
+ * after the coarse/fine ones): node means over apertures and regular carrier faces, LS gradients,
+ * bounded MUSCL along same-axis aperture chains, pairwise Smagorinsky momentum exchange scattered
+ * back to apertures and carrier faces.  FP32 atomics, as the reference. */
+pcfd_status pcfd_mac_transport_apertures(pcfd_system* system, double dt, double nu, double cs);
 /* The cell eddy viscosity [S] (host, FP32) of the last pcfd_mac_diffuse_smagorinsky. */
 pcfd_status pcfd_mac_eddy_viscosity_host(pcfd_system* system, float* nut);
 

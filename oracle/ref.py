@@ -89,6 +89,9 @@ def lib():
         L.ref_device_core_initialize.argtypes = [vp, f64p]
         L.ref_device_core_step.argtypes = [vp, f64p]
         L.ref_device_core_state.argtypes = [vp, f32p, f32p, f32p, f64p]
+        L.ref_device_core_create_mac.restype = vp
+        L.ref_device_core_create_mac.argtypes = [vp, C.POINTER(CoreCase), C.c_int32]
+        L.ref_device_core_faces.argtypes = [vp, f32p, f32p, f32p]
         L.ref_case_from_mesh.restype = vp
         L.ref_case_from_mesh.argtypes = [f64p, C.c_int64, C.POINTER(C.c_uint32), C.c_int64, f64p, f64p, C.c_double,
                                          C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_double]
@@ -105,6 +108,9 @@ def lib():
         L.ref_mac_advect.argtypes = [vp, C.c_double]
         L.ref_mac_diffuse_smagorinsky.argtypes = [vp, C.c_double, C.c_double, C.c_double]
         L.ref_mac_state.argtypes = [vp, f32p, f32p, f32p, f32p]
+        L.ref_mac_set_special.argtypes = [vp, f64p, f64p]
+        L.ref_mac_transport_apertures.argtypes = [vp, C.c_double, C.c_double, C.c_double]
+        L.ref_mac_special.argtypes = [vp, f64p, f64p]
         _lib = L
     return _lib
 
@@ -301,6 +307,20 @@ class RefMac:
     def diffuse_smagorinsky(self, nu, cs, dt):
         _check(lib().ref_mac_diffuse_smagorinsky(self.handle, nu, cs, dt))
 
+    def set_special(self, coarse_fine, embedded):
+        cf = np.ascontiguousarray(coarse_fine, np.float64)
+        eb = np.ascontiguousarray(embedded, np.float64)
+        _check(lib().ref_mac_set_special(self.handle, ptr(cf, C.c_double), ptr(eb, C.c_double)))
+
+    def transport_apertures(self, dt, nu, cs):
+        _check(lib().ref_mac_transport_apertures(self.handle, dt, nu, cs))
+
+    def special(self):
+        cf = np.zeros(self.case.summary["coarse_fine"])
+        eb = np.zeros(self.case.summary["embedded"])
+        _check(lib().ref_mac_special(self.handle, ptr(cf, C.c_double), ptr(eb, C.c_double)))
+        return cf, eb
+
     def state(self):
         u, v, w = (np.zeros(self.case.faces, np.float32) for _ in range(3))
         nut = np.zeros(self.case.n, np.float32)
@@ -372,13 +392,17 @@ def import_topology(topology: Topology) -> RefCase:
 
 
 class RefDeviceCore(RefCore):
-    """The reference's device classes driven with ExternalAeroCore's step sequence on any case."""
+    """The reference's device classes driven with ExternalAeroCore's step sequence on any case
+    (mac=True: its staggered MAC momentum path, smooth fabric wall as asked)."""
 
     def __init__(self, case: RefCase, speed=10.0, rho=1.225, nu=1.5e-5, cfl=0.5, cs=0.10, tolerance=1e-8, max_iterations=600,
-                 min_volume_fraction=0.25):
+                 min_volume_fraction=0.25, mac=False, smooth_wall=True):
         self.case = case
         cfg = CoreCase(speed, rho, nu, cfl, cs, tolerance, max_iterations)
-        self.handle = lib().ref_device_core_create(case.handle, C.byref(cfg), min_volume_fraction)
+        if mac:
+            self.handle = lib().ref_device_core_create_mac(case.handle, C.byref(cfg), int(smooth_wall))
+        else:
+            self.handle = lib().ref_device_core_create(case.handle, C.byref(cfg), min_volume_fraction)
         if not self.handle:
             raise RuntimeError("reference device core: " + lib().ref_last_error().decode(errors="replace"))
 
@@ -399,6 +423,11 @@ class RefDeviceCore(RefCore):
         _check(lib().ref_device_core_state(self.handle, ptr(x, C.c_float), ptr(y, C.c_float), ptr(z, C.c_float),
                                            ptr(p, C.c_double)))
         return (x, y, z), p
+
+    def faces(self):
+        u, v, w = (np.zeros(self.case.faces, np.float32) for _ in range(3))
+        _check(lib().ref_device_core_faces(self.handle, ptr(u, C.c_float), ptr(v, C.c_float), ptr(w, C.c_float)))
+        return u, v, w
 
     def close(self):
         if self.handle:

@@ -1068,6 +1068,8 @@ namespace
         std::unique_ptr<DeviceAmrFields> fields;
         std::unique_ptr<DeviceCompositeAmrProjection> projection;
         std::unique_ptr<DeviceCompositeCellMomentumTransport> momentum;
+        std::unique_ptr<DeviceAmrAdvection> advection;     // staggered MAC mode (no cell momentum)
+        bool smooth_wall = false;                           // MAC mode: the projection's smooth fabric wall
         bool initialized = false;
         double time = 0;
     };
@@ -1091,6 +1093,37 @@ void* ref_device_core_create(void* case_handle, const ref_core_case* cfg, double
         out = core.release();
     });
     return out;
+}
+
+// The same with the staggered MAC momentum path (ExternalAeroExecutionOptions::
+// conservative_cell_momentum = false, the smooth fabric wall as asked): DeviceAmrAdvection with
+// the constructor's 2.5-cell fabric protection instead of the cell-momentum transport.
+void* ref_device_core_create_mac(void* case_handle, const ref_core_case* cfg, int32_t smooth_wall)
+{
+    RefDeviceCore* out = nullptr;
+    guarded([&] {
+        auto core = std::make_unique<RefDeviceCore>();
+        core->c = static_cast<RefCase*>(case_handle);
+        core->cfg = *cfg;
+        RefCase& c = *core->c;
+        if (!c.bvh) throw std::invalid_argument("the MAC mode needs a case with a surface");
+        core->fields = std::make_unique<DeviceAmrFields>(c.hierarchy);
+        core->projection = std::make_unique<DeviceCompositeAmrProjection>(c.system, *core->fields);
+        core->advection = std::make_unique<DeviceAmrAdvection>(c.hierarchy, *c.bvh, 2.5, &c.system);
+        core->smooth_wall = smooth_wall != 0;
+        out = core.release();
+    });
+    return out;
+}
+
+int ref_device_core_faces(void* handle, float* u, float* v, float* w)
+{
+    return guarded([&] {
+        RefDeviceCore& k = *static_cast<RefDeviceCore*>(handle);
+        AmrHostFields host(k.c->hierarchy);
+        k.fields->download(host);
+        from_host_fields(*k.c, host, u, v, w);
+    });
 }
 
 void ref_device_core_destroy(void* core) { delete static_cast<RefDeviceCore*>(core); }
@@ -1128,13 +1161,17 @@ int ref_device_core_initialize(void* handle, double* stats)
         }
         k.fields->upload(fields);
         k.projection->upload_special_fluxes(fluxes);
-        k.momentum->upload_state(state);
-        k.momentum->reconstruct_fluxes(k.projection->coarse_fine_velocity_device(), k.projection->embedded_velocity_device());
+        if (k.momentum)
+        {
+            k.momentum->upload_state(state);
+            k.momentum->reconstruct_fluxes(k.projection->coarse_fine_velocity_device(), k.projection->embedded_velocity_device());
+        }
         k.fields->apply_external_aero_boundaries(speed);
         const double maximum = std::max(1e-9, std::abs(k.cfg.speed)), dt = k.cfg.cfl * c.hierarchy.finest_cell_size() / maximum;
         const auto t0 = std::chrono::steady_clock::now();
+        if (k.advection) k.projection->sync_coarse_fine_from_fields();   // project(false, dt) with its default sync
         const AmrGpuSolveResult r = k.projection->project(Real(k.cfg.rho), Real(dt), k.cfg.projection_tolerance, k.cfg.projection_max_iterations, false);
-        if (r.converged) k.momentum->apply_projected_pressure_gradient(k.projection->pressure(), Real(dt), Real(k.cfg.rho));
+        if (r.converged && k.momentum) k.momentum->apply_projected_pressure_gradient(k.projection->pressure(), Real(dt), Real(k.cfg.rho));
         const auto t1 = std::chrono::steady_clock::now();
         k.initialized = r.converged;
         stats[0] = dt; stats[1] = ms_between(t0, t1); stats[2] = stats[1]; stats[3] = r.iterations; stats[4] = r.converged; stats[5] = r.relative_residual;
@@ -1150,6 +1187,29 @@ int ref_device_core_step(void* handle, double* stats)
         RefCase& c = *k.c;
         const auto t0 = std::chrono::steady_clock::now();
         const double h = c.hierarchy.finest_cell_size();
+        if (k.advection)
+        {
+            // ExternalAeroCore::step, MAC branch (external_aero_core.cpp:304-311, 321-325)
+            const double mass_flux = k.fields->max_abs_velocity(), special = k.projection->max_abs_special_velocity(),
+                         eb_rate = k.projection->max_embedded_cfl_rate();
+            (void)special;
+            const double cfl_rate = std::max({1e-9, std::abs(k.cfg.speed) / h, mass_flux / h, eb_rate}), dt_value = k.cfg.cfl / cfl_rate;
+            const Real dt = Real(dt_value), nu = Real(k.cfg.nu), cs = Real(k.cfg.smagorinsky_cs), speed = Real(k.cfg.speed), rho = Real(k.cfg.rho);
+            k.advection->advect(*k.fields, dt);
+            k.advection->diffuse_smagorinsky(*k.fields, nu, cs, dt);
+            k.fields->apply_external_aero_boundaries(speed);
+            k.projection->transport_embedded_apertures(dt, nu, cs, false);
+            if (k.smooth_wall) k.projection->apply_smooth_fabric_wall_model(dt, nu);
+            const auto p0 = std::chrono::steady_clock::now();
+            k.projection->sync_coarse_fine_from_fields();
+            const AmrGpuSolveResult r = k.projection->project(rho, dt, k.cfg.projection_tolerance, k.cfg.projection_max_iterations, true);
+            const auto p1 = std::chrono::steady_clock::now();
+            if (r.converged) k.time += dt_value;
+            cudaDeviceSynchronize();
+            const auto t1 = std::chrono::steady_clock::now();
+            stats[0] = dt_value; stats[1] = ms_between(t0, t1); stats[2] = ms_between(p0, p1); stats[3] = r.iterations; stats[4] = r.converged; stats[5] = r.relative_residual;
+            return;
+        }
         const double rate = k.momentum->max_outflow_rate(k.projection->coarse_fine_velocity_device(), k.projection->embedded_velocity_device(), true);
         (void)k.fields->max_abs_velocity();
         (void)k.momentum->max_abs_velocity();
@@ -1180,6 +1240,7 @@ namespace
         RefCase* c = nullptr;
         std::unique_ptr<DeviceAmrFields> fields;
         std::unique_ptr<DeviceAmrAdvection> advection;
+        std::unique_ptr<DeviceCompositeAmrProjection> projection;
     };
     Vec3d mac_face_centre(const BrickMetadata& brick, double h, int component, int i, int j, int k)
     {
@@ -1261,6 +1322,7 @@ void* ref_mac_create(void* case_handle, double protection_cells)
         if (!m->c->bvh) throw std::invalid_argument("MAC advection needs a case with a surface");
         m->fields = std::make_unique<DeviceAmrFields>(m->c->hierarchy);
         m->advection = std::make_unique<DeviceAmrAdvection>(m->c->hierarchy, *m->c->bvh, protection_cells, &m->c->system);
+        m->projection = std::make_unique<DeviceCompositeAmrProjection>(m->c->system, *m->fields);
         out = m.release();
     });
     return out;
@@ -1291,6 +1353,35 @@ int ref_mac_diffuse_smagorinsky(void* mac, double nu, double cs, double dt)
     return guarded([&] {
         RefMac& m = *static_cast<RefMac*>(mac);
         m.advection->diffuse_smagorinsky(*m.fields, Real(nu), Real(cs), Real(dt));
+    });
+}
+
+int ref_mac_set_special(void* mac, const double* coarse_fine, const double* embedded)
+{
+    return guarded([&] {
+        RefMac& m = *static_cast<RefMac*>(mac);
+        m.projection->upload_special_fluxes(special_from(*m.c, coarse_fine, embedded));
+    });
+}
+
+// DeviceCompositeAmrProjection::transport_embedded_apertures (amr_pressure.cu:1868-1911) as the
+// MAC step calls it (no molecular fabric wall)
+int ref_mac_transport_apertures(void* mac, double dt, double nu, double cs)
+{
+    return guarded([&] {
+        RefMac& m = *static_cast<RefMac*>(mac);
+        m.projection->transport_embedded_apertures(Real(dt), Real(nu), Real(cs), false);
+    });
+}
+
+int ref_mac_special(void* mac, double* coarse_fine, double* embedded)
+{
+    return guarded([&] {
+        RefMac& m = *static_cast<RefMac*>(mac);
+        CompositeAmrFluxes f;
+        m.projection->download_special_fluxes(f);
+        std::copy(f.coarse_fine_velocity.begin(), f.coarse_fine_velocity.end(), coarse_fine);
+        std::copy(f.embedded_velocity.begin(), f.embedded_velocity.end(), embedded);
     });
 }
 
@@ -1357,9 +1448,12 @@ int ref_device_core_state(void* handle, float* x, float* y, float* z, double* pr
 {
     return guarded([&] {
         RefDeviceCore& k = *static_cast<RefDeviceCore*>(handle);
-        CompositeCellMomentumState st;
-        k.momentum->download_state(st);
-        state_to(st, x, y, z);
+        if (k.momentum)
+        {
+            CompositeCellMomentumState st;
+            k.momentum->download_state(st);
+            state_to(st, x, y, z);
+        }
         if (pressure)
         {
             std::vector<Real> p;

@@ -122,6 +122,10 @@ void* ref_import_topology(const pcfd_topology* topology);
  * (external_aero_core.cpp:245-328) on any case handle (fixture or imported). */
 void* ref_device_core_create(void* case_handle, const ref_core_case* config, double min_volume_fraction);
 void ref_device_core_destroy(void* core);
+/* The same with the staggered MAC momentum path (the smooth fabric wall on or off); faces of its
+ * fields in the compact per-brick layout. */
+void* ref_device_core_create_mac(void* case_handle, const ref_core_case* config, int32_t smooth_wall);
+int ref_device_core_faces(void* core, float* u, float* v, float* w);
 int ref_device_core_initialize(void* core, double* stats6);
 int ref_device_core_step(void* core, double* stats6);
 
@@ -138,6 +142,11 @@ int ref_mac_set_faces(void* mac, const float* u, const float* v, const float* w)
 int ref_mac_advect(void* mac, double dt);
 int ref_mac_diffuse_smagorinsky(void* mac, double nu, double cs, double dt);
 int ref_mac_state(void* mac, float* u, float* v, float* w, float* nut);
+/* Special (coarse/fine, embedded) face velocities of the MAC objects' projection, and its
+ * transport_embedded_apertures(dt, nu, cs, false). */
+int ref_mac_set_special(void* mac, const double* coarse_fine, const double* embedded);
+int ref_mac_transport_apertures(void* mac, double dt, double nu, double cs);
+int ref_mac_special(void* mac, double* coarse_fine, double* embedded);
 
 /* The reference's own GPU path (ExternalAeroCore on the fixture), for the sm_100a baseline arm. */
 void* ref_core_create(void* case_handle, const ref_core_case* config);

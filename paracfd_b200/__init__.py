@@ -21,6 +21,7 @@ MG_FP64, MG_FP32 = 0, 1
 MG_CYCLE_REFERENCE, MG_CYCLE_CORRECTED, MG_CYCLE_COMPOSITE = 0, 1, 2
 PRECONDITIONER_MULTIGRID, PRECONDITIONER_LEARNED, PRECONDITIONER_JACOBI, PRECONDITIONER_LEARNED_MULTIGRID = 0, 1, 2, 3
 LEARNED_TARGET_MULTIGRID, LEARNED_TARGET_BRICK_SOLVE = 0, 1
+MOMENTUM_CELL, MOMENTUM_MAC = 0, 1
 
 
 def learned_parameter_count() -> int:
@@ -221,6 +222,13 @@ class CompositeSystem:
 
     def mac_diffuse_smagorinsky(self, nu: float, cs: float, dt: float):
         check(self._lib.pcfd_mac_diffuse_smagorinsky(self.handle, nu, cs, dt))
+
+    def set_momentum_mode(self, mode: int):
+        """MOMENTUM_CELL (default) or MOMENTUM_MAC for initialize / step; re-initialize afterwards."""
+        check(self._lib.pcfd_core_set_momentum_mode(self.handle, mode))
+
+    def mac_transport_apertures(self, dt: float, nu: float, cs: float):
+        check(self._lib.pcfd_mac_transport_apertures(self.handle, dt, nu, cs))
 
     def mac_eddy_viscosity(self) -> np.ndarray:
         out = np.empty(self.storage_size, np.float32)

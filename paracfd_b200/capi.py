@@ -252,6 +252,8 @@ SIGNATURES = {
     "pcfd_mac_advect": (C.c_int, [C.c_void_p, C.c_double]),
     "pcfd_mac_diffuse_smagorinsky": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double]),
     "pcfd_mac_eddy_viscosity_host": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    "pcfd_mac_transport_apertures": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double]),
+    "pcfd_core_set_momentum_mode": (C.c_int, [C.c_void_p, C.c_int32]),
 }
 
 _lib = None

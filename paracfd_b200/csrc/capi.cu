@@ -282,6 +282,7 @@ namespace pcfd
             build_loads(s, t);
             build_locator(s, t);
             build_mac(s, t);
+            build_apertures(s, t);
             cuda_check(cudaDeviceSynchronize(), "system setup");
         }
 
@@ -335,6 +336,7 @@ namespace pcfd
         destroy_loads(*this);
         destroy_locator(*this);
         destroy_mac(*this);
+        destroy_apertures(*this);
         delete momentum;
         if (pinned) cudaFreeHost(pinned);
         if (pinned_block) cudaFreeHost(pinned_block);
@@ -787,6 +789,17 @@ pcfd_status pcfd_sample_slice_host(pcfd_system* system, const double origin[3], 
     });
 }
 
+pcfd_status pcfd_core_set_momentum_mode(pcfd_system* system, int32_t mode)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(mode == PCFD_MOMENTUM_CELL || mode == PCFD_MOMENTUM_MAC, "momentum mode must be 0 (cell) or 1 (MAC)");
+        require(mode == PCFD_MOMENTUM_CELL || mac_ready(s), "the MAC momentum mode needs pcfd_mac_set_links first");
+        s.momentum_mode = mode;
+        s.initialized = false;
+    });
+}
+
 pcfd_status pcfd_mac_set_links(pcfd_system* system, const uint8_t* links_u, const uint8_t* links_v, const uint8_t* links_w)
 {
     return guarded([&] {
@@ -814,6 +827,17 @@ pcfd_status pcfd_mac_diffuse_smagorinsky(pcfd_system* system, double nu, double 
         require(std::isfinite(nu) && std::isfinite(cs) && std::isfinite(dt) && nu >= 0.0 && cs >= 0.0 && dt > 0.0,
                 "invalid MAC LES/diffusion parameters");
         mac_diffuse_smagorinsky(s, float(nu), float(cs), float(dt));
+        sync(s);
+    });
+}
+
+pcfd_status pcfd_mac_transport_apertures(pcfd_system* system, double dt, double nu, double cs)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(std::isfinite(nu) && std::isfinite(cs) && std::isfinite(dt) && nu >= 0.0 && cs >= 0.0 && dt > 0.0,
+                "invalid aperture transport parameters");
+        mac_transport_apertures(s, float(dt), float(nu), float(cs));
         sync(s);
     });
 }

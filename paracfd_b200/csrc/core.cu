@@ -128,6 +128,22 @@ namespace pcfd
         const double dt = c.cfl * s.h_finest / maximum;
         vec_zero(s, s.pressure);
         std::memset(&stats, 0, sizeof(stats));
+        if (s.momentum_mode == PCFD_MOMENTUM_MAC)
+        {
+            // the MAC mode carries no cell momentum: the projection syncs the coarse/fine slots
+            // from the fine faces first and no impulse follows (external_aero_core.cpp:296-300)
+            mac_sync_coarse_fine(s);
+            stats.pressure = project(s, c.rho, dt, c.projection_tolerance, c.projection_max_iterations, false);
+            stats.dt = dt;
+            stats.max_abs_velocity = mac_max_face_speed(s);
+            stats.max_abs_special_velocity = mac_max_special_speed(s);
+            stats.cfl_velocity = maximum;
+            stats.effective_cfl = maximum * dt / s.h_finest;
+            s.initialized = stats.pressure.converged != 0;
+            stats.physical_time = s.physical_time;
+            cuda_check(cudaStreamSynchronize(s.stream), "initialize");
+            return;
+        }
         stats.pressure = project(s, c.rho, dt, c.projection_tolerance, c.projection_max_iterations, false);
         if (c.pressure_impulse && stats.pressure.converged) momentum_pressure_impulse(s, m, float(dt), float(c.rho), true);
         float cfl[4];
@@ -142,9 +158,55 @@ namespace pcfd
         cuda_check(cudaStreamSynchronize(s.stream), "initialize");
     }
 
+    // ExternalAeroCore::step with the staggered MAC momentum (external_aero_core.cpp:304-311,
+    // 321-325): CFL from the regular faces, the special velocities and the EB aperture rate;
+    // MacCormack advection, LES + face diffusion, boundaries, compact aperture transport, the
+    // smooth fabric wall, then the projection with the coarse/fine slots synced from the fine faces.
+    void core_step_mac(System& s, pcfd_step_stats& stats)
+    {
+        const pcfd_case& c = s.config;
+        cudaEvent_t e0, e1, p0, p1;
+        cuda_check(cudaEventCreate(&e0), "event"); cuda_check(cudaEventCreate(&e1), "event");
+        cuda_check(cudaEventCreate(&p0), "event"); cuda_check(cudaEventCreate(&p1), "event");
+        cuda_check(cudaEventRecord(e0, s.stream), "event");
+        std::memset(&stats, 0, sizeof(stats));
+        const float face_max = mac_max_face_speed(s), special_max = mac_max_special_speed(s), eb_rate = mac_embedded_cfl_rate(s);
+        if (!std::isfinite(face_max) || !std::isfinite(special_max) || !std::isfinite(eb_rate))
+            throw Error(PCFD_INTERNAL, "non-finite regular or embedded-boundary velocity before the time step");
+        const double cfl_rate = std::max({1e-9, std::abs(c.speed) / s.h_finest, double(face_max) / s.h_finest, double(eb_rate)});
+        const double dt_value = c.cfl / cfl_rate;
+        const float dt = float(dt_value), nu = float(c.nu), cs = float(c.smagorinsky_cs), speed = float(c.speed), rho = float(c.rho);
+        mac_advect(s, dt);
+        mac_diffuse_smagorinsky(s, nu, cs, dt);
+        momentum_external_boundaries(s, speed);
+        mac_transport_apertures(s, dt, nu, cs);
+        if (c.smooth_wall) mac_smooth_wall(s, dt, nu);
+        mac_sync_coarse_fine(s);
+        cuda_check(cudaEventRecord(p0, s.stream), "event");
+        stats.pressure = project(s, double(rho), dt_value, c.projection_tolerance, c.projection_max_iterations, true);
+        cuda_check(cudaEventRecord(p1, s.stream), "event");
+        cuda_check(cudaEventRecord(e1, s.stream), "event");
+        cuda_check(cudaEventSynchronize(e1), "step");
+        float ms = 0, pms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventElapsedTime(&pms, p0, p1);
+        cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(p0); cudaEventDestroy(p1);
+        stats.dt = dt_value;
+        stats.max_abs_velocity = std::max(face_max, special_max);
+        stats.max_abs_special_velocity = special_max;
+        stats.max_outflow_rate = eb_rate;
+        stats.cfl_velocity = cfl_rate * s.h_finest;
+        stats.effective_cfl = cfl_rate * dt_value;
+        stats.step_ms = ms;
+        stats.projection_ms = pms;
+        if (stats.pressure.converged) s.physical_time += dt_value;
+        stats.physical_time = s.physical_time;
+    }
+
     void core_step(System& s, pcfd_step_stats& stats)
     {
         require(s.initialized, "the core needs a converged initialization before stepping");
+        if (s.momentum_mode == PCFD_MOMENTUM_MAC) { core_step_mac(s, stats); return; }
         Momentum& m = momentum_of(s);
         const pcfd_case& c = s.config;
         cudaEvent_t e0, e1, p0, p1;

@@ -23,6 +23,7 @@
 #include "locator.h"
 
 #include <algorithm>
+#include <cstring>
 #include <vector>
 
 namespace pcfd
@@ -531,6 +532,38 @@ namespace pcfd
         }
     }
 
+    namespace
+    {
+        // max |face velocity| over the faces of non-covered bricks (DeviceAmrFields::
+        // max_abs_velocity, amr_fields.cu:65-68, 195-198), as float bits in an unsigned int
+        __global__ void mac_max_face_kernel(Faces f, const uint32_t* flags, int64_t per_slot, int64_t per_component, unsigned int* out)
+        {
+            __shared__ float shared[8];
+            float m = 0.0f;
+            for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < 3 * per_component; q += int64_t(gridDim.x) * blockDim.x)
+            {
+                const int c = int(q / per_component);
+                const int64_t i = q % per_component;
+                if (!(flags[i / per_slot] & PCFD_BRICK_COVERED)) m = fmaxf(m, fabsf(f.c[c][i]));
+            }
+            for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, o));
+            if ((threadIdx.x & 31) == 0) shared[threadIdx.x >> 5] = m;
+            __syncthreads();
+            if (threadIdx.x == 0)
+            {
+                for (int w = 1; w < int(blockDim.x >> 5); ++w) m = fmaxf(m, shared[w]);
+                atomicMax(out, __float_as_uint(m));
+            }
+        }
+    }
+
+    inline float uint_bits_to_float(unsigned int bits)
+    {
+        float f;
+        std::memcpy(&f, &bits, sizeof(f));
+        return f;
+    }
+
     // ---- system state and launches ----
     struct MacState
     {
@@ -538,6 +571,7 @@ namespace pcfd
         DBuf<uint32_t> flags;
         DBuf<uint8_t> links[3];
         DBuf<float> forward[3], out[3], nut;
+        DBuf<unsigned int> maximum;
         bool has_links = false;
     };
 
@@ -577,6 +611,7 @@ namespace pcfd
         }
         st->neighbour.upload(neighbour);
         st->flags.upload(flags);
+        st->maximum.alloc(1);
     }
 
     void destroy_mac(System& s)
@@ -643,5 +678,21 @@ namespace pcfd
         require(st.nut.n == size_t(s.S), "MAC eddy viscosity: no diffusion step yet");
         cuda_check(cudaStreamSynchronize(s.stream), "synchronize");
         cuda_check(cudaMemcpy(host_nut, st.nut.p, size_t(s.S) * sizeof(float), cudaMemcpyDeviceToHost), "download eddy viscosity");
+    }
+
+    bool mac_ready(const System& s) { return s.mac && static_cast<const MacState*>(s.mac)->has_links; }
+
+    float mac_max_face_speed(System& s)
+    {
+        MacState& st = mac_state(s);
+        const Faces f{{s.u.p, s.v.p, s.w.p}};
+        const int64_t per_slot = int64_t(s.bs + 1) * s.bs * s.bs, per_component = int64_t(s.B) * per_slot;
+        cuda_check(cudaMemsetAsync(st.maximum.p, 0, sizeof(unsigned int), s.stream), "clear maximum");
+        mac_max_face_kernel<<<int(std::min<int64_t>(592, (3 * per_component + kThreads - 1) / kThreads)), kThreads, 0, launch_stream(s)>>>(
+            f, st.flags, per_slot, per_component, st.maximum);
+        unsigned int bits = 0;
+        cuda_check(cudaMemcpyAsync(&bits, st.maximum.p, sizeof(bits), cudaMemcpyDeviceToHost, s.stream), "read maximum");
+        cuda_check(cudaStreamSynchronize(s.stream), "face maximum");
+        return uint_bits_to_float(bits);
     }
 }

@@ -288,6 +288,8 @@ namespace pcfd
         void* loads = nullptr;                  // surface-load integration state (loads.cu)
         void* locator = nullptr;                // point location / slice sampling state (locator.cu)
         void* mac = nullptr;                    // staggered MAC momentum state (mac.cu)
+        void* apertures = nullptr;              // MAC-mode compact aperture transport state (mac_apertures.cu)
+        int momentum_mode = PCFD_MOMENTUM_CELL; // pcfd_momentum_mode of pcfd_core_initialize / step
         DBuf<float> slice_buffer;               // device output of pcfd_sample_slice_host
         cudaEvent_t markers[8] = {};
         int64_t launches = 0;                   // kernels launched on the system stream so far
@@ -414,6 +416,15 @@ namespace pcfd
     void mac_advect(System& s, float dt);
     void mac_diffuse_smagorinsky(System& s, float nu, float cs, float dt);
     void mac_eddy_viscosity(System& s, float* host_nut);
+    void build_apertures(System& s, const pcfd_topology& t);   // mac_apertures.cu
+    void destroy_apertures(System& s);
+    void mac_transport_apertures(System& s, float dt, float nu, float cs);
+    void mac_sync_coarse_fine(System& s);
+    void mac_smooth_wall(System& s, float dt, float nu);
+    float mac_embedded_cfl_rate(System& s);
+    float mac_max_special_speed(System& s);
+    float mac_max_face_speed(System& s);       // mac.cu
+    bool mac_ready(const System& s);
     void locate_points(System& s, const float* d_points, int count, int* d_out);
     void sample_slice(System& s, const double origin[3], const double edge_u[3], const double edge_v[3], int nu, int nv,
                       int field, float* d_out);   // [max |div|, rms, worst V, max |div V|, sum |div V|, sum div V]

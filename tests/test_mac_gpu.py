@@ -109,3 +109,88 @@ def test_mac_advection_and_diffusion_match_reference(wing):
             # the next check starts from the reference's result
             u, v, w = want
     refm.close()
+
+
+def flow_at(points, component, speed=10.0):
+    """The initial_faces flow evaluated at arbitrary points [n][3], one component per point."""
+    x, y, z = points[:, 0], points[:, 1], points[:, 2]
+    u = speed * (1.0 + 0.2 * np.sin(1.3 * x + 0.7 * y) * np.cos(0.9 * z))
+    v = speed * 0.15 * np.cos(0.8 * x - 1.1 * z) * np.sin(0.6 * y + 0.3)
+    w = speed * 0.1 * np.sin(0.5 * x + 0.9 * y - 0.4 * z)
+    return np.choose(component, [u, v, w]).astype(np.float32)
+
+
+def test_aperture_transport_matches_reference(wing):
+    """transport_embedded_apertures (the MAC step's compact EB face transport) against the
+    reference's own projection on the same faces and special velocities.  Both accumulate node
+    sums with FP32 atomics in launch order, so the results agree to FP32 rounding of those sums
+    (1e-5 of the velocity scale asserted)."""
+    t = wing.topology
+    u, v, w = initial_faces(t)
+    ncf, neb = wing.summary["coarse_fine"], wing.summary["embedded"]
+    assert neb > 0
+    cf_pts = np.ctypeslib.as_array(t.coarse_fine.face_centroid, shape=(ncf * 3,)).reshape(-1, 3)
+    cf_axis = np.ctypeslib.as_array(t.coarse_fine.axis, shape=(ncf,)).astype(int)
+    eb_pts = np.ctypeslib.as_array(t.embedded.face_centroid, shape=(neb * 3,)).reshape(-1, 3)
+    eb_axis = np.ctypeslib.as_array(t.embedded.axis, shape=(neb,)).astype(int)
+    cf = flow_at(cf_pts, cf_axis)
+    eb = flow_at(eb_pts, eb_axis)
+    h = min(t.levels[l].h for l in range(t.level_count))
+    dt = 0.5 * h / 12.0
+    keep = non_covered_faces(t)
+    refm = ref.RefMac(wing, 2.5)
+    refm.set_faces(u, v, w)
+    refm.set_special(cf.astype(np.float64), eb.astype(np.float64))
+    refm.transport_apertures(dt, 1.5e-5, 0.17)
+    (ru, rv, rw), _ = refm.state()
+    rcf, reb = refm.special()
+    refm.close()
+    with CompositeSystem(t) as s:
+        s.set_faces(u, v, w)
+        s.set_special(cf, eb)
+        s.mac_transport_apertures(dt, 1.5e-5, 0.17)
+        gu, gv, gw = s.get_faces()
+        gcf, geb = s.get_special()
+    changed = np.abs(reb - eb).max()
+    err = np.abs(geb - reb).max()
+    print(f"apertures: max |diff| {err:.3e}, max change {changed:.3e}")
+    assert changed > 1e-3
+    assert err <= 1e-5 * 12.0
+    assert np.abs(gcf - rcf).max() <= 1e-6 * 12.0
+    for g, r, orig in ((gu, ru, u), (gv, rv, v), (gw, rw, w)):
+        moved = np.abs(r - orig)[keep].max()
+        diff = np.abs(g - r)[keep].max()
+        print(f"carrier faces: max |diff| {diff:.3e}, max change {moved:.3e}")
+        assert diff <= 1e-5 * 12.0
+
+
+@pytest.mark.parametrize("smooth_wall", [0, 1])
+def test_mac_steps_track_reference(wing, smooth_wall):
+    """Whole MAC-mode steps (ExternalAeroCore::step's staggered branch: advection, LES + diffusion,
+    boundaries, compact aperture transport, the smooth fabric wall when on, coarse/fine sync,
+    projection to 1e-8) against the reference's own device classes in the same sequence: dt and
+    the regular face velocities agree to 1e-4 of the freestream after each of 3 steps."""
+    from paracfd_b200 import MOMENTUM_MAC
+    t = wing.topology
+    settings = dict(speed=10.0, rho=1.225, nu=1.5e-5, cfl=0.5, smagorinsky_cs=0.10, projection_tolerance=1e-8,
+                    projection_max_iterations=600)
+    keep = non_covered_faces(t)
+    core = ref.RefDeviceCore(wing, settings["speed"], settings["rho"], settings["nu"], settings["cfl"],
+                             settings["smagorinsky_cs"], settings["projection_tolerance"],
+                             settings["projection_max_iterations"], mac=True, smooth_wall=bool(smooth_wall))
+    with CompositeSystem(t) as s:
+        s.configure(smooth_wall=smooth_wall, **settings)
+        s.set_mac_links(*wing.mac_links(2.5))
+        s.set_momentum_mode(MOMENTUM_MAC)
+        a, b = s.initialize(), core.initialize()
+        assert a["pressure"]["converged"] and b["converged"]
+        for step in range(3):
+            a, b = s.step(), core.step()
+            assert a["pressure"]["converged"] and b["converged"], (step, a, b)
+            assert abs(a["dt"] - b["dt"]) <= 1e-4 * b["dt"], (step, a["dt"], b["dt"])
+            got, want = s.get_faces(), core.faces()
+            err = max(np.abs(g - r)[keep].max() for g, r in zip(got, want)) / settings["speed"]
+            print(f"MAC step {step} (wall {smooth_wall}): dt {a['dt']:.6e} / {b['dt']:.6e}, face error {err:.3e} of U, "
+                  f"iterations {a['pressure']['iterations']} / {b['iterations']}")
+            assert err <= 1e-4, (step, err)
+    core.close()
