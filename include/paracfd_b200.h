@@ -449,6 +449,9 @@ typedef struct pcfd_autotune_report {
     int32_t chosen;                  /* resident CTAs per SM now used */
 } pcfd_autotune_report;
 pcfd_status pcfd_autotune(pcfd_system* system, int32_t iterations, pcfd_autotune_report* report);
+/* Sets the brick pipeline's resident CTAs per SM (1..8; launches never exceed what the kernels'
+ * launch bounds keep resident).  No result depends on it. */
+pcfd_status pcfd_set_pipeline_ctas(pcfd_system* system, int32_t ctas_per_sm);
 
 /* ---- point location and headless slices ---------------------------------------------------- */
 /* DeviceAmrLocator::locate_points (amr_fields.cu:131-168, 244-249): for each point of d_points

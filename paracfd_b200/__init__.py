@@ -375,6 +375,9 @@ class CompositeSystem:
         check(self._lib.pcfd_autotune(self.handle, iterations, C.byref(out)))
         return out.as_dict()
 
+    def set_pipeline_ctas(self, ctas_per_sm: int):
+        check(self._lib.pcfd_set_pipeline_ctas(self.handle, ctas_per_sm))
+
     def sample_slice(self, origin, edge_u, edge_v, nu: int, nv: int, field: int = 0) -> np.ndarray:
         """Headless slice [nv, nu] of the resident state (field 0 |v|, 1..3 v_x..v_z, 4 pressure)."""
         o, u, v = (np.ascontiguousarray(a, np.float64) for a in (origin, edge_u, edge_v))

@@ -254,6 +254,7 @@ SIGNATURES = {
     "pcfd_mac_eddy_viscosity_host": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
     "pcfd_mac_transport_apertures": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double]),
     "pcfd_core_set_momentum_mode": (C.c_int, [C.c_void_p, C.c_int32]),
+    "pcfd_set_pipeline_ctas": (C.c_int, [C.c_void_p, C.c_int32]),
 }
 
 _lib = None

@@ -765,6 +765,15 @@ pcfd_status pcfd_autotune(pcfd_system* system, int32_t iterations, pcfd_autotune
     });
 }
 
+pcfd_status pcfd_set_pipeline_ctas(pcfd_system* system, int32_t ctas_per_sm)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(ctas_per_sm >= 1 && ctas_per_sm <= 8, "pipeline CTAs per SM: 1..8");
+        s.pipe_ctas_per_sm = ctas_per_sm;
+    });
+}
+
 pcfd_status pcfd_locate_points_device(pcfd_system* system, const float* d_points, int32_t count, int32_t* d_locations)
 {
     return guarded([&] {

@@ -209,7 +209,7 @@ namespace pcfd
         constexpr int kTile = 12;
         __device__ inline int tile_index(int i, int j, int k) { return ((k + 2) * kTile + (j + 2)) * kTile + (i + 2); }
 
-        __global__ void __launch_bounds__(256) transport_brick_kernel(const int* __restrict__ brick_list,
+        __global__ void __launch_bounds__(256, 5) transport_brick_kernel(const int* __restrict__ brick_list,
             const int* __restrict__ brick_level, const int* __restrict__ nbr, const uint32_t* __restrict__ flags,
             const double* __restrict__ level_h, const uint8_t* __restrict__ code, const float* __restrict__ u,
             const float* __restrict__ v, const float* __restrict__ w, const float* __restrict__ x, const float* __restrict__ y,
@@ -250,9 +250,35 @@ namespace pcfd
             }
             __syncthreads();
             const float h = float(level_h[brick_level[slot]]);
-            // face fluxes: face p (0..8) along `axis` lies between tile cells p - 1 (lower) and p
-            for (int q = tid; q < 3 * F; q += 256)
+            // face fluxes: face p (0..8) along `axis` lies between tile cells p - 1 (lower) and p.
+            // The normal velocities of a thread's faces (stored in the brick of each face's lower
+            // cell) are loaded first, all at once, so their latencies overlap.
+            constexpr int kFacesPerThread = (3 * F + 255) / 256;
+            float normals[kFacesPerThread];
+#pragma unroll
+            for (int n = 0; n < kFacesPerThread; ++n)
             {
+                const int q = tid + 256 * n;
+                normals[n] = 0.0f;
+                if (q >= 3 * F) continue;
+                const int axis = q / F, f = q % F, p = f % 9, a = (f / 9) & 7, b = f / 72;
+                const int t0 = axis == 0 ? 1 : 0, t1 = axis == 2 ? 1 : 2;
+                int fs = slot, fi[3];
+                fi[axis] = p; fi[t0] = a; fi[t1] = b;
+                if (p == 0)
+                {
+                    fs = neighbour[2 * axis];
+                    fi[axis] = bs;
+                    if (fs < 0) continue;   // no lower neighbour: the face is closed below
+                }
+                normals[n] = axis == 0 ? u[u_face(bs, fs, fi[0], fi[1], fi[2])]
+                           : (axis == 1 ? v[v_face(bs, fs, fi[0], fi[1], fi[2])] : w[w_face(bs, fs, fi[0], fi[1], fi[2])]);
+            }
+#pragma unroll
+            for (int n = 0; n < kFacesPerThread; ++n)
+            {
+                const int q = tid + 256 * n;
+                if (q >= 3 * F) continue;
                 const int axis = q / F, f = q % F, p = f % 9, a = (f / 9) & 7, b = f / 72;
                 int lo[3];
                 const int t0 = axis == 0 ? 1 : 0, t1 = axis == 2 ? 1 : 2;
@@ -264,12 +290,7 @@ namespace pcfd
                 const uint8_t ca = sc[ta], cb = sc[tb];
                 float* out = flux[axis][f];
                 if (!(ca & CODE_ACTIVE) || !(cb & CODE_ACTIVE) || !face_open(ca, axis)) { out[0] = out[1] = out[2] = 0.0f; continue; }
-                // the face's normal velocity, stored in the brick of its lower cell
-                int fs = slot, fi[3] = {lo[0], lo[1], lo[2]};
-                if (p == 0) { fs = neighbour[2 * axis]; fi[axis] = bs - 1; }
-                ++fi[axis];
-                const float normal = axis == 0 ? u[u_face(bs, fs, fi[0], fi[1], fi[2])]
-                                   : (axis == 1 ? v[v_face(bs, fs, fi[0], fi[1], fi[2])] : w[w_face(bs, fs, fi[0], fi[1], fi[2])]);
+                const float normal = normals[n];
                 const int tl = ta - stride, tu = tb + stride;
                 const bool has_l = (sc[tl] & CODE_ACTIVE) && face_open(sc[tl], axis);
                 const bool has_u = (sc[tu] & CODE_ACTIVE) && face_open(cb, axis);
@@ -778,16 +799,30 @@ namespace pcfd
         __device__ inline void stage_halo(int slot, const int* __restrict__ nbr, const uint8_t* __restrict__ code,
                                           HaloSources<NF> src, float (*tile)[kHalo3], uint8_t* tcode, int* neighbour)
         {
+            // the brick's own values are loaded into registers first (256 threads, two cells each),
+            // so that their latency overlaps the neighbour-table load and the tile clearing
             const int tid = threadIdx.x;
+            const int64_t base = int64_t(slot) * 512;
+            uint8_t own_code[2];
+            float own[2][NF > 0 ? NF : 1];
+#pragma unroll
+            for (int r = 0; r < 2; ++r)
+            {
+                const int q = tid + 256 * r;
+                own_code[r] = code[base + q];
+#pragma unroll
+                for (int f = 0; f < NF; ++f) own[r][f] = src.p[f][base + q];
+            }
             if (tid < 6) neighbour[tid] = nbr[slot * 6 + tid];
             for (int q = tid; q < kHalo3; q += blockDim.x) tcode[q] = 0;
             __syncthreads();
-            const int64_t base = int64_t(slot) * 512;
-            for (int q = tid; q < 512; q += blockDim.x)
+#pragma unroll
+            for (int r = 0; r < 2; ++r)
             {
-                const int t = halo_index(q & 7, (q >> 3) & 7, q >> 6);
-                tcode[t] = code[base + q];
-                for (int f = 0; f < NF; ++f) tile[f][t] = src.p[f][base + q];
+                const int q = tid + 256 * r, t = halo_index(q & 7, (q >> 3) & 7, q >> 6);
+                tcode[t] = own_code[r];
+#pragma unroll
+                for (int f = 0; f < NF; ++f) tile[f][t] = own[r][f];
             }
             for (int q = tid; q < 6 * 64; q += blockDim.x)
             {

@@ -157,10 +157,11 @@ namespace pcfd
         {
             const int node = blockIdx.x * blockDim.x + threadIdx.x;
             if (node >= incident_dofs) return;
-            const int dof = incident_dof[node];
+            const int dof = incident_dof[node], q0 = incident_offset[node], q1 = incident_offset[node + 1];
             const double centre = p[dof];
             double sum = 0.0;
-            for (int q = incident_offset[node]; q < incident_offset[node + 1]; ++q)
+#pragma unroll 2
+            for (int q = q0; q < q1; ++q)
             {
                 const int other = incident_other[q];
                 if (active[other]) sum += incident_coefficient[q] * (centre - p[other]);
@@ -174,9 +175,11 @@ namespace pcfd
         {
             const int node = blockIdx.x * blockDim.x + threadIdx.x;
             if (node >= nodes) return;
+            const int q0 = offset[node], q1 = offset[node + 1];
             const double centre = p[dof[node]];
             double gx = 0, gy = 0, gz = 0;
-            for (int q = offset[node]; q < offset[node + 1]; ++q)
+#pragma unroll 2
+            for (int q = q0; q < q1; ++q)
             {
                 const double d = p[neighbour[q]] - centre;
                 gx += weight[3 * q] * d;
@@ -213,8 +216,9 @@ namespace pcfd
         {
             const int node = blockIdx.x * blockDim.x + threadIdx.x;
             if (node >= incident_dofs) return;
+            const int dof = incident_dof[node], q0 = incident_offset[node], q1 = incident_offset[node + 1];
             double sum = 0.0;
-            for (int q = incident_offset[node]; q < incident_offset[node + 1]; ++q)
+            for (int q = q0; q < q1; ++q)
             {
                 const int e = incident_edge[q];
                 int a, b, ln, un;
@@ -235,7 +239,7 @@ namespace pcfd
                 const double flux = -area * face_derivative(gradient, ln, un, corr, uw);
                 sum += double(incident_sign[q]) * flux;
             }
-            out[incident_dof[node]] += sum;
+            out[dof] += sum;
         }
 
         __global__ void gauge_apply_kernel(const int* dof, const double* coefficient, int count, const double* p, double* out)

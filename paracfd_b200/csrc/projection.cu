@@ -203,7 +203,7 @@ namespace pcfd
         __global__ void structured_correction_kernel(const int* __restrict__ brick_list, int brick_count, int bs_arg,
             const int* __restrict__ brick_level, const int* __restrict__ nbr, const uint32_t* __restrict__ flags,
             const double* __restrict__ level_h, const uint8_t* __restrict__ active, const uint8_t* __restrict__ cut,
-            const double* __restrict__ p, double scale, int outlet, float* u, float* v, float* w)
+            const double* __restrict__ p, double scale, int outlet, float* __restrict__ u, float* __restrict__ v, float* __restrict__ w)
         {
             const int bs = kBS ? kBS : bs_arg;   // 8^3 bricks: index math folded at compile time
             const int c3 = bs * bs * bs;
@@ -213,36 +213,53 @@ namespace pcfd
             const int i = local % bs, j = (local / bs) % bs, k = local / (bs * bs);
             const int64_t a = int64_t(slot) * c3 + local;
             if (!active[a]) return;
-            const double h = level_h[brick_level[slot]];
+            const double h = level_h[brick_level[slot]], pa = p[a];
+            const uint8_t cm = cut[a];
+            // every axis's upper cell, its activity and pressure and the face value are loaded
+            // before any face is written, so the loads of the three axes are in flight together
+            int64_t upper[3];
+            int n[3];
+            float* face[3];
+            bool open[3];
+            double pu[3];
+            float fv[3];
+#pragma unroll
             for (int axis = 0; axis < 3; ++axis)
             {
-                if (cut[a] & (1u << axis)) continue;
                 int q[3] = {i, j, k};
-                int64_t upper = -1;
-                int n = -1;
-                if (++q[axis] < bs) upper = int64_t(slot) * c3 + (q[2] * bs + q[1]) * bs + q[0];
+                upper[axis] = -1;
+                n[axis] = -1;
+                if (++q[axis] < bs) upper[axis] = int64_t(slot) * c3 + (q[2] * bs + q[1]) * bs + q[0];
                 else
                 {
-                    n = nbr[slot * 6 + 2 * axis + 1];
-                    if (n >= 0) { q[axis] = 0; upper = int64_t(n) * c3 + (q[2] * bs + q[1]) * bs + q[0]; }
+                    n[axis] = nbr[slot * 6 + 2 * axis + 1];
+                    if (n[axis] >= 0) { q[axis] = 0; upper[axis] = int64_t(n[axis]) * c3 + (q[2] * bs + q[1]) * bs + q[0]; }
                 }
-                if (upper < 0 || !active[upper]) continue;
                 int f[3] = {i, j, k};
                 ++f[axis];
-                float* face = face_ptr(u, v, w, bs, axis, slot, f[0], f[1], f[2]);
-                const float corrected = float(double(*face) - scale * (p[upper] - p[a]) / h);
-                *face = corrected;
-                if (n >= 0)
+                face[axis] = face_ptr(u, v, w, bs, axis, slot, f[0], f[1], f[2]);
+                open[axis] = !(cm & (1u << axis)) && upper[axis] >= 0;
+                pu[axis] = open[axis] ? p[upper[axis]] : 0.0;
+                fv[axis] = open[axis] ? *face[axis] : 0.0f;
+                open[axis] = open[axis] && active[upper[axis]];
+            }
+#pragma unroll
+            for (int axis = 0; axis < 3; ++axis)
+            {
+                if (!open[axis]) continue;
+                const float corrected = float(double(fv[axis]) - scale * (pu[axis] - pa) / h);
+                *face[axis] = corrected;
+                if (n[axis] >= 0)
                 {
                     int m[3] = {i, j, k};
                     m[axis] = 0;
-                    *face_ptr(u, v, w, bs, axis, n, m[0], m[1], m[2]) = corrected;
+                    *face_ptr(u, v, w, bs, axis, n[axis], m[0], m[1], m[2]) = corrected;
                 }
             }
             if (outlet && (flags[slot] & PCFD_BRICK_XMAX) && i == bs - 1)
             {
-                float* face = u + u_face(bs, slot, bs, j, k);
-                *face = float(double(*face) + scale * p[a] / (0.5 * h));
+                float* f = u + u_face(bs, slot, bs, j, k);
+                *f = float(double(*f) + scale * pa / (0.5 * h));
             }
         }
 

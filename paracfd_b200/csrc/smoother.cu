@@ -247,23 +247,26 @@ namespace pcfd
                 }
                 return v;
             };
+            // the row's independent loads first, so that they are in flight together
+            const int node = dv.incident[d], g0 = dv.gauge_offset[d], g1 = dv.gauge_offset[d + 1];
             const bool on = dv.active[a];
+            const double D = dv.diag[a];
             const double za = value(a);
-            const int node = dv.incident[d];
             if (node >= 0 && on)
             {
                 // the compact edges' two-point terms, coefficient * (z_a - z_other): the reference's
                 // sign * coefficient * (z_lower - z_upper) bit for bit (exact negations)
+                const int q0 = dv.incident_offset[node], q1 = dv.incident_offset[node + 1];
                 double sum = 0.0;
-                for (int q = dv.incident_offset[node]; q < dv.incident_offset[node + 1]; ++q)
+#pragma unroll 2
+                for (int q = q0; q < q1; ++q)
                 {
                     const int other = dv.incident_other[q];
                     if (dv.active[other]) sum += dv.incident_coefficient[q] * (za - value(other));
                 }
                 Az += sum;
             }
-            for (int g = dv.gauge_offset[d]; g < dv.gauge_offset[d + 1]; ++g) Az += dv.gauge_coefficient[g] * za;
-            const double D = dv.diag[a];
+            for (int g = g0; g < g1; ++g) Az += dv.gauge_coefficient[g] * za;
             if (kFinish == 0)
             {
                 if (!on) out[a] = TO(0);
@@ -398,22 +401,62 @@ namespace pcfd
 
         // z = w r / D for every DOF (first sweep from zero); deferred rows read the assembled D.
         // (FP32 multigrid: also writes the float copy of r that the float sweeps read.)
+        // Four consecutive DOFs per thread (one code word, two 16-byte r loads, one 16-byte z and
+        // r-copy store each), so every thread keeps four entries' loads in flight; the last
+        // partial group takes the scalar path.
+        template <class T>
+        __device__ inline T first_sweep_value(uint8_t c, double rq, int64_t q, int level, const T* __restrict__ damping,
+                                              const double* __restrict__ diag, const uint8_t* __restrict__ active, int64_t structured,
+                                              double omega)
+        {
+            if (q >= structured || (c & kDeferred))
+            {
+                const double D = active[q] ? diag[q] : 0.0;
+                return D > 0.0 ? T(omega * rq / D) : T(0);
+            }
+            return c ? T(rq) * damping[level * kDiagonalKinds + diagonal_kind(c)] : T(0);
+        }
         template <class T>
         __global__ void first_sweep_kernel(const uint8_t* __restrict__ code, const int* __restrict__ brick_level,
                                            const T* __restrict__ damping, const double* __restrict__ diag,
                                            const uint8_t* __restrict__ active, const double* __restrict__ r,
                                            T* __restrict__ z, T* __restrict__ r_copy, int64_t structured, int64_t n, double omega)
         {
-            const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-            if (q >= n) return;
-            const uint8_t c = code[q];
-            if (r_copy) r_copy[q] = T(r[q]);
-            if (q >= structured || (c & kDeferred))
+            const int64_t q0 = 4 * (int64_t(blockIdx.x) * blockDim.x + threadIdx.x);
+            if (q0 >= n) return;
+            if (q0 + 4 > n)
             {
-                const double D = active[q] ? diag[q] : 0.0;
-                z[q] = D > 0.0 ? T(omega * r[q] / D) : T(0);
+                for (int64_t q = q0; q < n; ++q)
+                {
+                    if (r_copy) r_copy[q] = T(r[q]);
+                    z[q] = first_sweep_value<T>(code[q], r[q], q, q < structured ? brick_level[q >> 9] : 0, damping, diag, active,
+                                                structured, omega);
+                }
+                return;
             }
-            else z[q] = c ? T(r[q]) * damping[brick_level[q >> 9] * kDiagonalKinds + diagonal_kind(c)] : T(0);
+            const uchar4 c = *reinterpret_cast<const uchar4*>(code + q0);
+            const double2 ra = reinterpret_cast<const double2*>(r + q0)[0], rb = reinterpret_cast<const double2*>(r + q0)[1];
+            const int level = q0 < structured ? brick_level[q0 >> 9] : 0;
+            T out[4];
+            const uint8_t cs[4] = {c.x, c.y, c.z, c.w};
+            const double rs[4] = {ra.x, ra.y, rb.x, rb.y};
+#pragma unroll
+            for (int k = 0; k < 4; ++k) out[k] = first_sweep_value<T>(cs[k], rs[k], q0 + k, level, damping, diag, active, structured, omega);
+            if (sizeof(T) == 4)
+            {
+                *reinterpret_cast<float4*>(z + q0) = make_float4(float(out[0]), float(out[1]), float(out[2]), float(out[3]));
+                if (r_copy) *reinterpret_cast<float4*>(r_copy + q0) = make_float4(float(rs[0]), float(rs[1]), float(rs[2]), float(rs[3]));
+            }
+            else
+            {
+                reinterpret_cast<double2*>(z + q0)[0] = make_double2(double(out[0]), double(out[1]));
+                reinterpret_cast<double2*>(z + q0)[1] = make_double2(double(out[2]), double(out[3]));
+                if (r_copy)
+                {
+                    reinterpret_cast<double2*>(r_copy + q0)[0] = make_double2(rs[0], rs[1]);
+                    reinterpret_cast<double2*>(r_copy + q0)[1] = make_double2(rs[2], rs[3]);
+                }
+            }
         }
 
         // Brick-local block smoother: z = x_k after k Chebyshev iterations for the brick's diagonal
@@ -829,7 +872,7 @@ namespace pcfd
             FineSmoother& f = s.fine;
             FineBuffers<T> w(f);
             const bool cheb = w.chebyshev != nullptr;
-            first_sweep_kernel<T><<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(
+            first_sweep_kernel<T><<<blocks_for((int64_t(s.S) + 3) / 4), kThreads, 0, launch_stream(s)>>>(
                 f.code, s.brick_level, cheb ? w.chebyshev : w.damping, s.diagonal, s.active, r, z, r_copy, s.structured, s.S,
                 cheb ? f.cheb_omega[0] : 2.0 / 3.0);
         }
@@ -871,7 +914,7 @@ namespace pcfd
         if (std::is_same<TC, float>::value && f.z32.n)
         {
             float *a = f.z32.p, *b = f.z32b.p, *r32 = f.r32.p;
-            first_sweep_kernel<float><<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(
+            first_sweep_kernel<float><<<blocks_for((int64_t(s.S) + 3) / 4), kThreads, 0, launch_stream(s)>>>(
                 f.code, s.brick_level, f.damping32.p, s.diagonal, s.active, r, a, r32, s.structured, s.S, 2.0 / 3.0);
             sweep<float, float, TC, 0>(s, a, r32, b, nullptr);
             coarse(b, r32);
@@ -881,7 +924,7 @@ namespace pcfd
         else
         {
             double* a = f.z.p;
-            first_sweep_kernel<double><<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(
+            first_sweep_kernel<double><<<blocks_for((int64_t(s.S) + 3) / 4), kThreads, 0, launch_stream(s)>>>(
                 f.code, s.brick_level, f.damping.p, s.diagonal, s.active, r, a, nullptr, s.structured, s.S, 2.0 / 3.0);
             sweep<double, double, TC, 0>(s, a, r, z, nullptr);
             coarse(z, r);
@@ -1018,7 +1061,7 @@ namespace pcfd
         double* a = f.z.p;
         if (stage == 0)
         {
-            first_sweep_kernel<double><<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(
+            first_sweep_kernel<double><<<blocks_for((int64_t(s.S) + 3) / 4), kThreads, 0, launch_stream(s)>>>(
                 f.code, s.brick_level, f.damping.p, s.diagonal, s.active, r, a, nullptr, s.structured, s.S, 2.0 / 3.0);
             sweep<double, double, double, 0>(s, a, r, z, nullptr);
         }

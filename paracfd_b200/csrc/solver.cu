@@ -619,30 +619,41 @@ namespace pcfd
 
         // One Chebyshev step of a CSR level, fused: r = rhs - A x, d = c1 d + c2 D^-1 r (first step:
         // d = c2 D^-1 r), next = x + d
+        // Every per-row load that does not depend on another (diagonal, iterate, right-hand side,
+        // direction, both row offsets) is issued before the first one is used, and the row loop is
+        // unrolled so that several gathers are in flight; the sums keep the CSR order.
         template <class T, class TK = T>
-        __global__ void algebraic_chebyshev_kernel(const T* rhs, const T* x, T* next, T* d, const int* row_offset, const int* neighbour,
-                                                   const TK* coefficient, const T* diag, int cells, T c1, T c2, int first)
+        __global__ void __launch_bounds__(256) algebraic_chebyshev_kernel(const T* __restrict__ rhs, const T* __restrict__ x,
+            T* __restrict__ next, T* __restrict__ d, const int* __restrict__ row_offset, const int* __restrict__ neighbour,
+            const TK* __restrict__ coefficient, const T* __restrict__ diag, int cells, T c1, T c2, int first)
         {
             const int q = blockIdx.x * blockDim.x + threadIdx.x;
             if (q >= cells) return;
-            if (!(diag[q] > T(0))) { next[q] = T(0); d[q] = T(0); return; }
-            double Ax = double(diag[q]) * double(x[q]);
-            for (int e = row_offset[q]; e < row_offset[q + 1]; ++e) Ax -= coefficient_value(coefficient[e]) * double(x[neighbour[e]]);
-            const T step = c2 * T((double(rhs[q]) - Ax) / double(diag[q]));
-            const T dn = first ? step : c1 * d[q] + step;
+            const T dq = diag[q], xq = x[q], bq = rhs[q], dold = first ? T(0) : d[q];
+            const int e0 = row_offset[q], e1 = row_offset[q + 1];
+            if (!(dq > T(0))) { next[q] = T(0); d[q] = T(0); return; }
+            double Ax = double(dq) * double(xq);
+#pragma unroll 4
+            for (int e = e0; e < e1; ++e) Ax -= coefficient_value(coefficient[e]) * double(x[neighbour[e]]);
+            const T step = c2 * T((double(bq) - Ax) / double(dq));
+            const T dn = first ? step : c1 * dold + step;
             d[q] = dn;
-            next[q] = x[q] + dn;
+            next[q] = xq + dn;
         }
         template <class T, class TK = T>
-        __global__ void algebraic_residual_kernel(const T* rhs, const T* x, T* residual, const int* row_offset, const int* neighbour,
-                                                  const TK* coefficient, const T* diag, int cells)
+        __global__ void __launch_bounds__(256) algebraic_residual_kernel(const T* __restrict__ rhs, const T* __restrict__ x,
+            T* __restrict__ residual, const int* __restrict__ row_offset, const int* __restrict__ neighbour,
+            const TK* __restrict__ coefficient, const T* __restrict__ diag, int cells)
         {
             const int q = blockIdx.x * blockDim.x + threadIdx.x;
             if (q >= cells) return;
-            if (!(diag[q] > T(0))) { residual[q] = T(0); return; }
-            double Ax = double(diag[q]) * double(x[q]);
-            for (int e = row_offset[q]; e < row_offset[q + 1]; ++e) Ax -= coefficient_value(coefficient[e]) * double(x[neighbour[e]]);
-            residual[q] = T(double(rhs[q]) - Ax);
+            const T dq = diag[q], xq = x[q], bq = rhs[q];
+            const int e0 = row_offset[q], e1 = row_offset[q + 1];
+            if (!(dq > T(0))) { residual[q] = T(0); return; }
+            double Ax = double(dq) * double(xq);
+#pragma unroll 4
+            for (int e = e0; e < e1; ++e) Ax -= coefficient_value(coefficient[e]) * double(x[neighbour[e]]);
+            residual[q] = T(double(bq) - Ax);
         }
         template <class T>
         __global__ void restrict_gather_kernel(const int* offset, const int* dof, const T* residual, int cells, T* coarse_rhs)

@@ -252,6 +252,24 @@ def test_composite_cycle_matches_oracle_on_three_level_cut_cell_wing(gpu):
     assert rel(got_ref, want_ref, act) <= 1e-12
 
 
+@pytest.mark.parametrize("precision", [MG_FP64, MG_FP32])
+def test_pipeline_results_do_not_depend_on_its_grid(gpu, precision):
+    """The brick pipeline's persistent CTAs walk bricks b, b + G, ... through a ring of staged
+    bricks; with 1 CTA per SM each CTA walks 7 of the 1,024 bricks of the NACA slab grid, with 6
+    only one or two.  The operator and the composite preconditioner (FP64 and FP32 fine levels)
+    give the same bits for every grid."""
+    rc = ref.naca_slab_case(base_cell_size=1 / 16)
+    r = np.random.default_rng(61).standard_normal(rc.n) * rc.active
+    out = []
+    with CompositeSystem(rc.topology, mg_cycle=2, mg_precision=precision) as s:
+        for ctas in (6, 1, 2, 3):
+            s.set_pipeline_ctas(ctas)
+            out.append((s.apply(r), s.precondition(r)))
+    rc.close()
+    for a, z in out[1:]:
+        assert np.array_equal(a, out[0][0]) and np.array_equal(z, out[0][1])
+
+
 def test_orthogonal_pcg_on_a_grid_without_wls_nodes(gpu):
     """A grid with no cut cells has no WLS gradient nodes; the solve then takes the reference's
     multigrid PCG (solve_orthogonal, amr_pressure.cu:1267-1353): true residual of apply_cpu <= 1e-8."""
