@@ -318,8 +318,12 @@ namespace pcfd
                 else copy_wait<0>();
                 if (kProlong) prolong_own<T, TC, kProlong == 2>(cur, e, v.prolong, mbuf[kProlong == 2 ? st : 0], tile[st]);
                 __syncthreads();
-                // ---- compute brick `cur` from buffer st.  Thread t owns cells t and t + 256, so a
-                // warp reads consecutive doubles of the tile (no shared-memory bank replays).
+                // ---- compute brick `cur` from buffer st.  Thread t owns cell (i, j, k) = (t & 7,
+                // t >> 5, (t >> 3 & 3) + 4 q), q = 0, 1: a warp covers one x-row of 8 cells in each
+                // of four consecutive z-planes.  With rows 12 and planes 120 tile entries apart the
+                // four rows fall on disjoint shared-memory banks (float: 32 banks, offsets 0, 24, 16,
+                // 8 words; double: each half-warp's two rows 240 words apart), so no stencil read
+                // replays; consecutive cells of a row make 32- or 64-byte global segments.
                 const T* F = tile[st];
                 const int l = cur.level;
                 const T h = T(v.level_h[l]);
@@ -330,7 +334,8 @@ namespace pcfd
 #pragma unroll
                 for (int q = 0; q < 2; ++q)
                 {
-                    const int c = threadIdx.x + 256 * q, i = c & 7, j = (c >> 3) & 7, k = c >> 6;
+                    const int i = threadIdx.x & 7, j = threadIdx.x >> 5, k = ((threadIdx.x >> 3) & 3) + 4 * q;
+                    const int c = (k * kBS + j) * kBS + i;
                     const int s = tix(i, j, k);
                     const uint8_t code = cbuf[st][c];
                     const T Az = structured_row<T>(F, s, code, h);
