@@ -266,12 +266,14 @@ def inflow_profile(speed: float, centres, step: int) -> np.ndarray:
 
 # DRAM bytes (read + write) per launch of the roofline kernel, from one ncu capture of
 # `bench.py --kernel-only <k> --workload <w>` (--metrics dram__bytes_read.sum,dram__bytes_write.sum,
-# one pass); keyed by (workload, grid, kernel-only component).  A bench run cannot measure DRAM
+# one pass); keyed by (workload, grid, kernel-only component[, first stage brick-structured]).  A bench run cannot measure DRAM
 # traffic itself; absent entries report null.  Stage-1 Chebyshev step on the 16 M-cell cut-cell
-# grid: two captured launches read 113.36 MB each and wrote 7.61 and 4.01 MB (mean taken); the
-# algorithmic figure is 129.4 MB, the difference the part of the 2.0 M-row stage the L2 keeps
-# between launches.
-DRAM_BYTES_PER_LAUNCH: dict = {("paraglider16m", "cutcell", 17): 119_170_000}
+# grid as CSR: two captured launches read 113.36 MB each and wrote 7.61 and 4.01 MB (mean taken);
+# the algorithmic figure is 129.4 MB, the difference the part of the 2.0 M-row stage the L2 keeps
+# between launches.  The same stage in brick-structured form: 71.91 MB read, 2.69 and 1.16 MB
+# written (mean taken) against 89.9 MB algorithmic.
+DRAM_BYTES_PER_LAUNCH: dict = {("paraglider16m", "cutcell", 17, False): 119_170_000,
+                               ("paraglider16m", "cutcell", 17, True): 73_834_752}
 
 
 # ------------------------------------------------------------------------------------------ grids
@@ -554,6 +556,9 @@ def run_ours(args, ranks: Ranks):
             one_step()
         stage_launches = system.profile_end(capacity)
     stage_bytes = system.profile_bytes(2) if len(stage_launches) else 0.0
+    stage_kernel = ("brick_stage_chebyshev_kernel (first composite stage, 64 rows per 8^3 brick, one Chebyshev step)"
+                    if system.stage_brick_structured else
+                    "algebraic_chebyshev_kernel (first composite stage as CSR, one Chebyshev step)")
 
     # isolated per-component device times on the same resident system (not part of the timed region)
     components = {0: "apply_full", 1: "apply_orthogonal", 2: "preconditioner", 3: "divergence", 4: "flux_correction",
@@ -585,9 +590,10 @@ def run_ours(args, ranks: Ranks):
     if len(stage_launches):
         avg_ms = float(np.mean(stage_launches))
         achieved = stage_bytes / (avg_ms * 1e-3) / 1e9
-        roofline = {"bound": "hbm", "kernel": "algebraic_chebyshev_kernel (first composite stage, one Chebyshev step)",
+        roofline = {"bound": "hbm", "kernel": stage_kernel,
                     "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                    "peak_kind": peak_kind, "traffic": DRAM_BYTES_PER_LAUNCH.get((args.workload, args.grid, 17)),
+                    "peak_kind": peak_kind,
+                    "traffic": DRAM_BYTES_PER_LAUNCH.get((args.workload, args.grid, 17, system.stage_brick_structured)),
                     "algorithmic_bytes_per_launch": int(stage_bytes), "launches_timed": int(len(stage_launches)),
                     "avg_launch_us": round(avg_ms * 1e3, 2),
                     "timing": "CUDA events around each launch over 3 whole steps after the timed region (stage chain "

@@ -194,6 +194,9 @@ typedef struct pcfd_options {
                                         matrices (all but the coarsest) store their off-diagonal
                                         coefficients in FP16; vectors, diagonals and sums stay FP32 or
                                         wider.  0: FP32 */
+    int32_t mg_stage_csr;            /* 1: keep the composite cycle's first stage as CSR rows; 0: with 8^3
+                                        bricks, its brick-structured form (64 rows per brick, face
+                                        neighbours found from the row index, the same couplings) */
 } pcfd_options;
 
 /* Coarse-correction weighting of the multigrid cycle.  The aggregation coarse operators are
@@ -522,10 +525,15 @@ enum {
                                             (its stage chain runs uncaptured while this is armed) */
 };
 /* Algorithmic bytes of one launch of a profiled region (each element read once and written once):
- * region 0 17 B per slot of a non-covered brick; region 2 per stage row its offset, rhs, x,
- * diagonal, direction read and write and next iterate, per stored coupling its column index and
- * coefficient.  0 for region 1. */
+ * region 0 17 B per slot of a non-covered brick; region 2 per stage row its rhs, x, diagonal,
+ * direction read and write and next iterate, then in CSR form the row offset and per stored
+ * coupling its column index and coefficient, in brick-structured form the row's packed face
+ * coefficients, per rest coupling its column index and coefficient and per 4^3 block its six
+ * neighbour blocks.  0 for region 1. */
 pcfd_status pcfd_profile_bytes(pcfd_system* system, int32_t region, double* bytes_per_launch);
+/* 1 when the composite cycle's first stage runs in brick-structured form (64 rows per 8^3 brick,
+ * face neighbours found from the row index), 0 when it runs as CSR or the cycle is not composite. */
+pcfd_status pcfd_stage_brick_structured(pcfd_system* system, int32_t* structured);
 /* 1 when the preconditioner's fine level runs as fused brick kernels (8^3 bricks whose
  * level-0 aggregates follow the brick geometry), 0 when it runs as separate launches. */
 pcfd_status pcfd_preconditioner_fused(pcfd_system* system, int32_t* fused);

@@ -86,12 +86,12 @@ class CompositeSystem:
                  momentum_min_volume_fraction: float = 0.0, fused_smoother: bool = True,
                  mg_cycle: int = 0, gmres_restart: int = 0, mg_stage_sweeps: int = 0, mg_block_iterations: int = 0,
                  mg_stage_chebyshev: int = 0, mg_fine_chebyshev: int = 0, gmres_delayed: int = 0,
-                 gmres_recycle: int = 0, mg_stage_fp16: int = 0):
+                 gmres_recycle: int = 0, mg_stage_fp16: int = 0, mg_stage_csr: int = 0):
         self._lib = capi.load()
         self._topology = topology   # keep the caller's arrays alive during creation
         opts = Options(mg_precision, device, None, momentum_min_volume_fraction, 0 if fused_smoother else 1, mg_cycle,
                        gmres_restart, mg_stage_sweeps, mg_block_iterations, mg_stage_chebyshev, mg_fine_chebyshev,
-                       gmres_delayed, gmres_recycle, mg_stage_fp16)
+                       gmres_delayed, gmres_recycle, mg_stage_fp16, mg_stage_csr)
         handle = C.c_void_p()
         check(self._lib.pcfd_system_create(C.byref(topology), C.byref(opts), C.byref(handle)))
         self.handle = handle
@@ -417,6 +417,13 @@ class CompositeSystem:
     def fused_preconditioner(self) -> bool:
         flag = C.c_int32()
         check(self._lib.pcfd_preconditioner_fused(self.handle, C.byref(flag)))
+        return bool(flag.value)
+
+    @property
+    def stage_brick_structured(self) -> bool:
+        """Whether the composite cycle's first stage runs in brick-structured form."""
+        flag = C.c_int32()
+        check(self._lib.pcfd_stage_brick_structured(self.handle, C.byref(flag)))
         return bool(flag.value)
 
     def launch_count(self) -> int:

@@ -84,7 +84,8 @@ class Options(C.Structure):
                 ("momentum_min_volume_fraction", C.c_double), ("disable_fused_smoother", C.c_int32),
                 ("mg_cycle", C.c_int32), ("gmres_restart", C.c_int32), ("mg_stage_sweeps", C.c_int32),
                 ("mg_block_iterations", C.c_int32), ("mg_stage_chebyshev", C.c_int32), ("mg_fine_chebyshev", C.c_int32),
-                ("gmres_delayed", C.c_int32), ("gmres_recycle", C.c_int32), ("mg_stage_fp16", C.c_int32)]
+                ("gmres_delayed", C.c_int32), ("gmres_recycle", C.c_int32), ("mg_stage_fp16", C.c_int32),
+                ("mg_stage_csr", C.c_int32)]
 
 
 class SolveResult(C.Structure):
@@ -225,6 +226,7 @@ SIGNATURES = {
     "pcfd_core_set_inflow_host": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int64]),
     "pcfd_launch_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "pcfd_preconditioner_fused": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
+    "pcfd_stage_brick_structured": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "pcfd_profile_begin": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
     "pcfd_profile_end": (C.c_int, [C.c_void_p, _f64p, C.c_int32, C.POINTER(C.c_int32)]),
     "pcfd_builder_last_error": (C.c_char_p, []),

@@ -214,6 +214,11 @@ namespace pcfd
                 require(options->mg_stage_fp16 == 1, "mg_stage_fp16 must be 0 or 1");
                 s.mg_stage_fp16 = 1;
             }
+            if (options && options->mg_stage_csr)
+            {
+                require(options->mg_stage_csr == 1, "mg_stage_csr must be 0 or 1");
+                s.mg_stage_csr = 1;
+            }
             if (options && options->gmres_recycle)
             {
                 require(options->gmres_recycle >= -1 && options->gmres_recycle <= System::recycle_capacity, "gmres_recycle must be -1..3");
@@ -252,6 +257,7 @@ namespace pcfd
                 require(s.fine.enabled, "the composite cycle needs the fused fine level (8^3 bricks)");
                 s.composite_fp32 = s.mg_precision == PCFD_MG_FP32 && !s.mg32.empty();
                 build_composite(s, t);
+                attach_deferred_map(s);
             }
             // Krylov storage
             for (DBuf<double>* v : {&s.r, &s.z, &s.dvec, &s.Ad, &s.t, &s.correction, &s.defect, &s.scratch_p, &s.scratch_out,
@@ -266,6 +272,8 @@ namespace pcfd
             cuda_check(cudaMallocHost(&s.pinned_block, size_t(4) * (kMaxSet + 1) * sizeof(double)), "pinned block scalars");
             s.dcgs_partial.alloc(size_t(592) * (2 * kMaxSet + 4));
             s.dcgs_result.alloc(size_t(kDcgsCoefficients));
+            s.dcgs_total.alloc(size_t(2 * kMaxSet + 4));
+            s.dcgs_ticket.alloc(1);
             cuda_check(cudaMallocHost(&s.pinned_dcgs, size_t(2) * kDcgsCoefficients * sizeof(double)), "pinned orthogonalisation scalars");
             for (cudaEvent_t& e : s.dcgs_ready) cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "column event");
             prime_block_grids();
@@ -1068,6 +1076,17 @@ pcfd_status pcfd_profile_bytes(pcfd_system* system, int32_t region, double* byte
         }
         else if (region == PCFD_PROFILE_STAGE_SMOOTH) *bytes_per_launch = stage_smooth_bytes(s);
         else *bytes_per_launch = 0.0;
+    });
+}
+
+pcfd_status pcfd_stage_brick_structured(pcfd_system* system, int32_t* structured)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(structured != nullptr, "null output");
+        *structured = s.composite && ((s.composite_fp32 && !s.inter32.empty() && s.inter32.front().brick_rows.p) ||
+                                      (!s.composite_fp32 && !s.inter64.empty() && s.inter64.front().brick_rows.p))
+                          ? 1 : 0;
     });
 }
 

@@ -193,21 +193,23 @@ namespace pcfd
         __global__ void __launch_bounds__(256) block_final_kernel(const double* __restrict__ partial, int blocks, int count,
                                                                   double* __restrict__ out)
         {
-            __shared__ double shared[8];
+            // thread partials over b = t, t + 256, ..., a warp tree, then the 8 warps in order; no
+            // barrier inside the loop over j, so the sums' loads overlap
+            __shared__ double shared[8][kStride];
+#pragma unroll 4
             for (int j = 0; j <= count; ++j)
             {
                 double v = 0.0;
                 for (int b = threadIdx.x; b < blocks; b += blockDim.x) v += partial[int64_t(b) * kStride + j];
                 v = warp_sum(v);
-                if ((threadIdx.x & 31) == 0) shared[threadIdx.x >> 5] = v;
-                __syncthreads();
-                if (threadIdx.x == 0)
-                {
-                    double t = 0.0;
-                    for (int w = 0; w < 8; ++w) t += shared[w];
-                    out[j] = t;
-                }
-                __syncthreads();
+                if ((threadIdx.x & 31) == 0) shared[threadIdx.x >> 5][j] = v;
+            }
+            __syncthreads();
+            if (threadIdx.x <= count)
+            {
+                double t = 0.0;
+                for (int w = 0; w < 8; ++w) t += shared[w][threadIdx.x];
+                out[threadIdx.x] = t;
             }
         }
 
@@ -252,6 +254,15 @@ namespace pcfd
         // Pass 1 for Q = [C | V_0..V_{j-1}] (final), v = V_j (projected once) and w = A z_j:
         // s = Q^T v, t = Q^T w, v.v, v.w, w.w -> partial[block][2 * kMaxSet + 3].
         constexpr int kDcgsStride = 2 * kMaxSet + 4;
+        // Pairs a thread loads before it sums: with few basis vectors (V <= 2) one pair leaves too
+        // few bytes in flight per SM to cover the load latency, so two pairs of every vector are
+        // loaded up front; with V >= 4 the V loads of one pair already do.
+        // The update kernel holds twice the values per pair (v and next); at V = 2 two pairs
+        // exceed its 64 registers, so it groups only at V = 1.
+        template <int V>
+        __host__ __device__ constexpr int dcgs_group() { return V <= 2 ? 2 : 1; }
+        template <int V>
+        __host__ __device__ constexpr int dcgs_update_group() { return V == 1 ? 2 : 1; }
         template <int V>
         __global__ void __launch_bounds__(kThreadsBlock, V >= 8 ? 2 : (V >= 4 ? 3 : 4)) dcgs_dot_kernel(VecSet Q, const double* __restrict__ vv,
             const double* __restrict__ w, const uint8_t* __restrict__ active, Sweep range, double* __restrict__ partial)
@@ -263,31 +274,47 @@ namespace pcfd
             const int count = Q.size();
             const int lane = threadIdx.x & 31, quarter = lane >> 3, warp = threadIdx.x >> 5;
             const int seg_pair = (warp * kPairsPerWarp) + (lane & 7);
+            constexpr int kGroup = dcgs_group<V>();
             for (int64_t item = blockIdx.x; item < range.items; item += gridDim.x)
             {
                 const int64_t base = range.base(item);
 #pragma unroll 1
-                for (int sub = 0; sub < 256 / kPairsPerPass; ++sub)
+                for (int sub0 = 0; sub0 < 256 / kPairsPerPass; sub0 += kGroup)
                 {
-                    const int64_t e = base + 2 * (seg_pair + kPairsPerPass * sub);
-                    const bool valid = e < range.padded;
-                    const int64_t q = valid ? e >> 1 : 0;
-                    const uchar2 a = valid ? reinterpret_cast<const uchar2*>(active)[q] : make_uchar2(0, 0);
-                    const double2 v0 = valid ? reinterpret_cast<const double2*>(vv)[q] : make_double2(0.0, 0.0);
-                    const double2 w0 = valid ? reinterpret_cast<const double2*>(w)[q] : make_double2(0.0, 0.0);
+                    // all loads of the group first, then the sums in the same order as one pair at a time
+                    uchar2 a[kGroup];
+                    double2 v0[kGroup], w0[kGroup], b[kGroup][V];
 #pragma unroll
-                    for (int u = 0; u < V; ++u)
+                    for (int g = 0; g < kGroup; ++g)
                     {
-                        const int j = V * quarter + u;
-                        const double2 b = valid && j < count ? reinterpret_cast<const double2*>(Q.vec(j))[q] : make_double2(0.0, 0.0);
-                        as[u] += (a.x ? b.x * v0.x : 0.0) + (a.y ? b.y * v0.y : 0.0);
-                        at[u] += (a.x ? b.x * w0.x : 0.0) + (a.y ? b.y * w0.y : 0.0);
+                        const int64_t e = base + 2 * (seg_pair + kPairsPerPass * (sub0 + g));
+                        const bool valid = e < range.padded;
+                        const int64_t q = valid ? e >> 1 : 0;
+                        a[g] = valid ? reinterpret_cast<const uchar2*>(active)[q] : make_uchar2(0, 0);
+                        v0[g] = valid ? reinterpret_cast<const double2*>(vv)[q] : make_double2(0.0, 0.0);
+                        w0[g] = valid ? reinterpret_cast<const double2*>(w)[q] : make_double2(0.0, 0.0);
+#pragma unroll
+                        for (int u = 0; u < V; ++u)
+                        {
+                            const int j = V * quarter + u;
+                            b[g][u] = valid && j < count ? reinterpret_cast<const double2*>(Q.vec(j))[q] : make_double2(0.0, 0.0);
+                        }
                     }
-                    if (quarter == 0)
+#pragma unroll
+                    for (int g = 0; g < kGroup; ++g)
                     {
-                        vv2 += (a.x ? v0.x * v0.x : 0.0) + (a.y ? v0.y * v0.y : 0.0);
-                        vw += (a.x ? v0.x * w0.x : 0.0) + (a.y ? v0.y * w0.y : 0.0);
-                        ww += (a.x ? w0.x * w0.x : 0.0) + (a.y ? w0.y * w0.y : 0.0);
+#pragma unroll
+                        for (int u = 0; u < V; ++u)
+                        {
+                            as[u] += (a[g].x ? b[g][u].x * v0[g].x : 0.0) + (a[g].y ? b[g][u].y * v0[g].y : 0.0);
+                            at[u] += (a[g].x ? b[g][u].x * w0[g].x : 0.0) + (a[g].y ? b[g][u].y * w0[g].y : 0.0);
+                        }
+                        if (quarter == 0)
+                        {
+                            vv2 += (a[g].x ? v0[g].x * v0[g].x : 0.0) + (a[g].y ? v0[g].y * v0[g].y : 0.0);
+                            vw += (a[g].x ? v0[g].x * w0[g].x : 0.0) + (a[g].y ? v0[g].y * w0[g].y : 0.0);
+                            ww += (a[g].x ? w0[g].x * w0[g].x : 0.0) + (a[g].y ? w0[g].y * w0[g].y : 0.0);
+                        }
                     }
                 }
             }
@@ -325,41 +352,48 @@ namespace pcfd
         //   v_new = v / r - Q (s / r),  w_new = w - (c / r) v - Q (t - (c / r) s),  next = w_new / rho.
         // out: [0, 32) s, [32, 64) t, [64, 96) s / r, [96, 128) t - (c / r) s, then v.v, v.w, w.w,
         // r, c, rho, 1 / r, c / r, 1 / rho (rho and r are 0 when their squares are not positive).
+        // One CTA per sum j (grid 2 kMaxSet + 3): thread partials over blocks b = t, t + 256, ...,
+        // a warp tree, then the 8 warps in order, into total[j].  The CTA that finishes last (a
+        // ticket taken after a memory fence, no waiting) forms the coefficients and resets the
+        // ticket for the next launch.
         __global__ void __launch_bounds__(256) dcgs_final_kernel(const double* __restrict__ partial, int blocks, int count,
-                                                                 double* __restrict__ out)
+                                                                 double* total, unsigned* ticket, double* __restrict__ out)
         {
             __shared__ double shared[8];
-            __shared__ double total[kDcgsStride];
-            for (int j = 0; j < 2 * kMaxSet + 3; ++j)
-            {
-                const bool used = j < count || (j >= kMaxSet && j < kMaxSet + count) || j >= 2 * kMaxSet;
-                if (!used)
-                {
-                    if (threadIdx.x == 0) total[j] = 0.0;
-                    continue;
-                }
-                double v = 0.0;
+            __shared__ bool last;
+            const int j = blockIdx.x;
+            const bool used = j < count || (j >= kMaxSet && j < kMaxSet + count) || j >= 2 * kMaxSet;
+            double v = 0.0;
+            if (used)
                 for (int b = threadIdx.x; b < blocks; b += blockDim.x) v += partial[int64_t(b) * kDcgsStride + j];
-                v = warp_sum(v);
-                if ((threadIdx.x & 31) == 0) shared[threadIdx.x >> 5] = v;
-                __syncthreads();
-                if (threadIdx.x == 0)
-                {
-                    double t = 0.0;
-                    for (int w = 0; w < 8; ++w) t += shared[w];
-                    total[j] = t;
-                }
-                __syncthreads();
+            v = warp_sum(v);
+            if ((threadIdx.x & 31) == 0) shared[threadIdx.x >> 5] = v;
+            __syncthreads();
+            if (threadIdx.x == 0)
+            {
+                double t = 0.0;
+                for (int w = 0; w < 8; ++w) t += shared[w];
+                total[j] = t;
+                __threadfence();
+                last = atomicAdd(ticket, 1u) == gridDim.x - 1;
             }
+            __syncthreads();
+            if (!last) return;
+            // the last CTA: every total is in L2 (each writer fenced before its ticket); read them
+            // past L1
+            __shared__ double sum[kDcgsStride];
+            if (threadIdx.x < 2 * kMaxSet + 3) sum[threadIdx.x] = __ldcg(total + threadIdx.x);
+            __syncthreads();
             if (threadIdx.x != 0) return;
+            *ticket = 0u;
             double ss = 0.0, st = 0.0, tt = 0.0;
             for (int l = 0; l < count; ++l)
             {
-                ss += total[l] * total[l];
-                st += total[l] * total[kMaxSet + l];
-                tt += total[kMaxSet + l] * total[kMaxSet + l];
+                ss += sum[l] * sum[l];
+                st += sum[l] * sum[kMaxSet + l];
+                tt += sum[kMaxSet + l] * sum[kMaxSet + l];
             }
-            const double vv = total[2 * kMaxSet], vw = total[2 * kMaxSet + 1], ww = total[2 * kMaxSet + 2];
+            const double vv = sum[2 * kMaxSet], vw = sum[2 * kMaxSet + 1], ww = sum[2 * kMaxSet + 2];
             const double r2 = vv - ss, r = r2 > 0.0 ? sqrt(r2) : 0.0;
             const double c = r > 0.0 ? (vw - st) / r : 0.0;
             const double rho2 = ww - tt - c * c, rho = rho2 > 0.0 ? sqrt(rho2) : 0.0;
@@ -367,10 +401,10 @@ namespace pcfd
             for (int l = 0; l < kMaxSet; ++l)
             {
                 const bool in = l < count;
-                out[l] = in ? total[l] : 0.0;
-                out[kMaxSet + l] = in ? total[kMaxSet + l] : 0.0;
-                out[2 * kMaxSet + l] = in ? total[l] * inv_r : 0.0;
-                out[3 * kMaxSet + l] = in ? total[kMaxSet + l] - c_r * total[l] : 0.0;
+                out[l] = in ? sum[l] : 0.0;
+                out[kMaxSet + l] = in ? sum[kMaxSet + l] : 0.0;
+                out[2 * kMaxSet + l] = in ? sum[l] * inv_r : 0.0;
+                out[3 * kMaxSet + l] = in ? sum[kMaxSet + l] - c_r * sum[l] : 0.0;
             }
             double* sc = out + 4 * kMaxSet;
             sc[0] = vv; sc[1] = vw; sc[2] = ww; sc[3] = r; sc[4] = c; sc[5] = rho; sc[6] = inv_r; sc[7] = c_r;
@@ -393,35 +427,54 @@ namespace pcfd
             const int count = Q.size();
             const int lane = threadIdx.x & 31, quarter = lane >> 3;
             const int seg_pair = ((threadIdx.x >> 5) * kPairsPerWarp) + (lane & 7);
+            constexpr int kGroup = dcgs_update_group<V>();
             for (int64_t item = blockIdx.x; item < range.items; item += gridDim.x)
             {
                 const int64_t base = range.base(item);
 #pragma unroll 1
-                for (int sub = 0; sub < 256 / kPairsPerPass; ++sub)
+                for (int sub0 = 0; sub0 < 256 / kPairsPerPass; sub0 += kGroup)
                 {
-                    const int64_t e = base + 2 * (seg_pair + kPairsPerPass * sub);
-                    const bool valid = e < range.padded;
-                    const int64_t q = valid ? e >> 1 : 0;
-                    const uchar2 a = valid ? reinterpret_cast<const uchar2*>(active)[q] : make_uchar2(0, 0);
-                    const double2 v0 = valid ? reinterpret_cast<const double2*>(vv)[q] : make_double2(0.0, 0.0);
-                    const double2 w0 = valid ? reinterpret_cast<const double2*>(w)[q] : make_double2(0.0, 0.0);
-                    double vx = 0.0, vy = 0.0, wx = 0.0, wy = 0.0;
+                    // loads of the whole group before the first store (v is updated in place)
+                    int64_t q[kGroup];
+                    bool valid[kGroup];
+                    uchar2 a[kGroup];
+                    double2 v0[kGroup], w0[kGroup], b[kGroup][V];
 #pragma unroll
-                    for (int u = 0; u < V; ++u)
+                    for (int g = 0; g < kGroup; ++g)
                     {
-                        const int j = V * quarter + u;
-                        const double2 b = valid && j < count ? reinterpret_cast<const double2*>(Q.vec(j))[q] : make_double2(0.0, 0.0);
-                        vx += cv[j] * b.x; vy += cv[j] * b.y;
-                        wx += cw[j] * b.x; wy += cw[j] * b.y;
+                        const int64_t e = base + 2 * (seg_pair + kPairsPerPass * (sub0 + g));
+                        valid[g] = e < range.padded;
+                        q[g] = valid[g] ? e >> 1 : 0;
+                        a[g] = valid[g] ? reinterpret_cast<const uchar2*>(active)[q[g]] : make_uchar2(0, 0);
+                        v0[g] = valid[g] ? reinterpret_cast<const double2*>(vv)[q[g]] : make_double2(0.0, 0.0);
+                        w0[g] = valid[g] ? reinterpret_cast<const double2*>(w)[q[g]] : make_double2(0.0, 0.0);
+#pragma unroll
+                        for (int u = 0; u < V; ++u)
+                        {
+                            const int j = V * quarter + u;
+                            b[g][u] = valid[g] && j < count ? reinterpret_cast<const double2*>(Q.vec(j))[q[g]] : make_double2(0.0, 0.0);
+                        }
                     }
-                    const double svx = quarter_total(vx), svy = quarter_total(vy), swx = quarter_total(wx), swy = quarter_total(wy);
-                    if (quarter == 0 && valid)
+#pragma unroll
+                    for (int g = 0; g < kGroup; ++g)
                     {
-                        const double2 vn = make_double2(a.x ? inv_r * v0.x - svx : 0.0, a.y ? inv_r * v0.y - svy : 0.0);
-                        const double2 nx = make_double2(a.x ? inv_rho * (w0.x - c_r * v0.x - swx) : 0.0,
-                                                        a.y ? inv_rho * (w0.y - c_r * v0.y - swy) : 0.0);
-                        reinterpret_cast<double2*>(vv)[q] = vn;
-                        reinterpret_cast<double2*>(next)[q] = nx;
+                        double vx = 0.0, vy = 0.0, wx = 0.0, wy = 0.0;
+#pragma unroll
+                        for (int u = 0; u < V; ++u)
+                        {
+                            const int j = V * quarter + u;
+                            vx += cv[j] * b[g][u].x; vy += cv[j] * b[g][u].y;
+                            wx += cw[j] * b[g][u].x; wy += cw[j] * b[g][u].y;
+                        }
+                        const double svx = quarter_total(vx), svy = quarter_total(vy), swx = quarter_total(wx), swy = quarter_total(wy);
+                        if (quarter == 0 && valid[g])
+                        {
+                            const double2 vn = make_double2(a[g].x ? inv_r * v0[g].x - svx : 0.0, a[g].y ? inv_r * v0[g].y - svy : 0.0);
+                            const double2 nx = make_double2(a[g].x ? inv_rho * (w0[g].x - c_r * v0[g].x - swx) : 0.0,
+                                                            a[g].y ? inv_rho * (w0[g].y - c_r * v0[g].y - swy) : 0.0);
+                            reinterpret_cast<double2*>(vv)[q[g]] = vn;
+                            reinterpret_cast<double2*>(next)[q[g]] = nx;
+                        }
                     }
                 }
             }
@@ -540,7 +593,8 @@ namespace pcfd
         else if (m <= 8) dot(dcgs_dot_kernel<2>);
         else if (m <= 16) dot(dcgs_dot_kernel<4>);
         else dot(dcgs_dot_kernel<8>);
-        dcgs_final_kernel<<<1, 256, 0, launch_stream(s)>>>(s.dcgs_partial, grid, m, coefficient);
+        dcgs_final_kernel<<<2 * kMaxSet + 3, 256, 0, launch_stream(s)>>>(s.dcgs_partial, grid, m, s.dcgs_total, s.dcgs_ticket,
+                                                                       coefficient);
         auto update = [&](auto kernel) {
             kernel<<<block_grid(kernel), kThreadsBlock, 0, launch_stream(s)>>>(Q, coefficient, v, w, next, s.active, range);
         };

@@ -114,6 +114,15 @@ namespace pcfd
         DBuf<T> coefficient, diagonal, rhs, x, temporary, residual;
         DBuf<T> inverse;                        // coarsest composite stage: explicit inverse [cells][cells] or empty
         DBuf<uint16_t> coefficient16;           // FP16 copy of the coefficients the kernels read instead (or empty)
+        // The same level in brick-structured form (first composite stage, or empty): rows are 4^3
+        // blocks per fine brick; per row the six face-neighbour coefficients (-z, -y, -x, +x, +y,
+        // +z, in the row's type or FP16) and a descriptor (first rest entry << 5 | rest count),
+        // as 16-byte words; per block its six face-neighbour blocks (-x, +x, -y, +y, -z, +z, or
+        // -1); the couplings no face slot holds as (column, coefficient) rest entries.
+        DBuf<uint4> brick_rows;
+        DBuf<int> brick_neighbour, rest_column;
+        DBuf<T> rest_coefficient;
+        DBuf<uint16_t> rest_coefficient16;
         double prolong = 1.0;                   // weight of the next level's correction added here
         int sweeps = 2;                         // smoothing steps before and after the coarse correction
         int chebyshev = 0;                      // 0: damped Jacobi; r >= 2: Chebyshev on [2 / r, 2]
@@ -127,8 +136,17 @@ namespace pcfd
         bool enabled = false;
         DBuf<uint8_t> code;                     // [S] open faces (bits 0-5), outlet (6), deferred (7)
         int deferred_count = 0;
-        DBuf<int> deferred_dof, deferred_incident, gauge_offset;
+        // Deferred rows packed so that one load gives all a row's indices: {DOF, first edge, map
+        // index of the DOF (composite cycle, else -1), (edges << 8) | (gauges << 2) | (has an
+        // incidence row << 1) | active}.  The edges are the row's compact-edge incidence entries
+        // whose other endpoint is active, in incidence order: {other endpoint, its map index}
+        // and the coefficient.
+        DBuf<int4> deferred_row;
+        DBuf<int2> deferred_edge;
+        DBuf<double> deferred_edge_coefficient;
+        DBuf<int> gauge_offset;
         DBuf<double> gauge_coefficient;
+        bool map_attached = false;              // deferred map indices filled from the composite stage-1 map
         DBuf<int> meta;                         // [active bricks][16] slot, level, level-0 cell, partial, neighbours
         DBuf<double> partial, deferred_residual;
         DBuf<int> gather_offset, gather_entry;  // base cell -> partials (>= 0) / deferred rows (< 0)
@@ -185,6 +203,7 @@ namespace pcfd
         int mg_block_iterations = 0;                             // composite cycle: brick block pre-smoother (pcfd_options)
         int mg_stage_chebyshev = 30;                             // composite stages: Chebyshev ratio, 0 = Jacobi (pcfd_options)
         int mg_stage_fp16 = 0;                                   // composite stages: FP16 coefficients (pcfd_options)
+        int mg_stage_csr = 0;                                    // composite cycle: first stage kept as CSR (pcfd_options)
         int mg_fine_chebyshev = 10;                              // composite fine sweeps: Chebyshev-Richardson ratio, 0 = Jacobi
         cudaStream_t stream = nullptr;
         bool own_stream = false;
@@ -243,6 +262,8 @@ namespace pcfd
         DBuf<double> block_partial;             // [592][kMaxSet + 1] block-kernel partial sums
         DBuf<double> block_result;              // [4][kMaxSet + 1] device coefficients / norms
         DBuf<double> dcgs_partial, dcgs_result; // delayed CGS2 partials [592][2 kMaxSet + 4] and coefficients
+        DBuf<double> dcgs_total;                // [2 kMaxSet + 4] the partials' sums
+        DBuf<unsigned> dcgs_ticket;             // CTAs of the sum kernel done (0 between launches)
         double* pinned_dcgs = nullptr;          // pinned host copies of dcgs_result, two columns
         cudaEvent_t dcgs_ready[2] = {};         // readback of column j lands in slot j & 1
         bool delayed_orthogonalisation = false; // pcfd_options.gmres_delayed
@@ -348,6 +369,7 @@ namespace pcfd
     void preconditioner_stage(System& s, int stage, const double* r, double* z);
     // fused fine level (smoother.cu) around the coarse hierarchy below it (solver.cu)
     void build_fine_smoother(System& s, const pcfd_topology& t, const std::vector<double>& diagonal);
+    void attach_deferred_map(System& s);
     void brick_apply(System& s, const double* p, double* out);   // code-byte structured operator
     void fine_preconditioner_stage(System& s, int stage, const double* r, double* z);
     template <class T> void fine_preconditioner(System& s, const double* r, double* z, std::vector<MgLevel<T>>& levels);

@@ -54,6 +54,12 @@ namespace pcfd
         // start 16-byte aligned (x = -1 at offset 1, x = 0..7 at 2..9, x = 8 at 10).
         constexpr int kP1 = 12, kP2 = 120, kTileSize = 10 * kP2;
         __device__ inline int tix(int i, int j, int k) { return (k + 1) * kP2 + (j + 1) * kP1 + (i + 2); }
+        // Staged right-hand sides and face codes keep each 64-entry z-plane 72 (rhs) or 80 (codes)
+        // entries apart, so that the four z-planes a warp reads at once fall on disjoint
+        // shared-memory banks; a 16-byte copy never crosses a plane.
+        constexpr int kRPlane = 72, kCPlane = 80, kRSize = kBS * kRPlane, kCSize = kBS * kCPlane;
+        __device__ inline int rix(int c) { return c + (kRPlane - 64) * (c >> 6); }
+        __device__ inline int cix(int c) { return c + (kCPlane - 64) * (c >> 6); }
 
         // base cell of cell (i,j,k) of a brick at level l whose (0,0,0) cell lies in base cell `b0`
         __device__ inline int base_cell_of(int b0, int l, int i, int j, int k)
@@ -140,10 +146,10 @@ namespace pcfd
             {
                 const int c = 2 * t, i = c & 7, j = (c >> 3) & 7, kk = c >> 6;
                 copy_pair<T>(tile + tix(i, j, kk), z + base + c, true);
-                if (kWithR) copy_pair<T>(rbuf + c, r + base + c, true);
+                if (kWithR) copy_pair<T>(rbuf + rix(c), r + base + c, true);
                 if (kMapped) copy8(mbuf + tix(i, j, kk), map + base + c, true);
             }
-            if (t < 32) copy16(cbuf + 16 * t, code + base + 16 * t, true);
+            if (t < 32) copy16(cbuf + cix(16 * t), code + base + 16 * t, true);
             const bool valid = k.nbr >= 0;
             const int64_t nb = int64_t(valid ? k.nbr : k.slot) * kC3;   // any valid address when zero-filling
             if (t < 128)
@@ -204,69 +210,68 @@ namespace pcfd
             }
         }
 
-        // What the rows the structured 7-point part does not complete need: compact edges (packed
-        // incidence: other endpoint, coefficient), gauges, the assembled diagonal.
+        // What the rows the structured 7-point part does not complete need: the packed rows and
+        // compact edges (other endpoint with its map index, coefficient), gauges, the assembled
+        // diagonal.
         struct DeferredView
         {
-            const int* dof;
-            const int* incident;           // row -> incidence node or -1
+            const int4* row;
+            const int2* edge;
+            const double* edge_coefficient;
             const int* gauge_offset;
             const double* gauge_coefficient;
-            const int* incident_offset;
-            const int* incident_other;
-            const double* incident_coefficient;
-            const uint8_t* active;
             const double* diag;
             const int* aggregate;          // level-0 aggregate per DOF (reference-cycle prolongation)
             int base_offset, base_cells;
             double omega;
         };
 
-        // Completes deferred row d (DOF a) from its structured part Az and right-hand side rc:
-        // the compact-edge gather and the gauges, in the order of the unfused operator.
+        // Completes deferred row d from its structured part t[a] (structured DOFs) and right-hand
+        // side r[a]: the compact-edge gather and the gauges, in the order of the unfused operator.
         // kFinish 0: z_new into out[a], 1: residual into residual[d], 2: residual into out[a].
+        // The packed row holds every index the row needs, so its gathers are two loads deep.
         template <int kFinish, class T, class TO, class TC, int kProlong>
-        __device__ inline void finish_row(const DeferredView& dv, int d, int a, double Az, double rc, const T* __restrict__ z,
-                                          const TC* __restrict__ e, double scale, const int* __restrict__ map,
-                                          TO* __restrict__ out, double* __restrict__ residual)
+        __device__ inline void finish_row(const DeferredView& dv, int d, int64_t structured, const T* __restrict__ z,
+                                          const T* __restrict__ r, const T* __restrict__ t, const TC* __restrict__ e,
+                                          double scale, TO* __restrict__ out, double* __restrict__ residual)
         {
-            auto value = [&](int q) {
+            const int4 row = dv.row[d];
+            const int a = row.x, edges = row.w >> 8, gauges = (row.w >> 2) & 63;
+            const bool on = row.w & 1, incident = row.w & 2;
+            // the prolonged iterate at DOF q with map index c (active DOFs only)
+            auto value = [&](int q, int c) {
                 double v = double(z[q]);
-                if (kProlong && dv.active[q])
+                if (kProlong == 2)
                 {
-                    if (kProlong == 2)
-                    {
-                        const int c = map[q];
-                        if (c >= 0) v += scale * double(e[c]);
-                    }
-                    else
-                    {
-                        const int c = dv.aggregate[q] - dv.base_offset;
-                        if (c >= 0 && c < dv.base_cells) v += scale * double(e[c]);
-                    }
+                    if (c >= 0) v += scale * double(e[c]);
+                }
+                else if (kProlong == 1)
+                {
+                    const int base = dv.aggregate[q] - dv.base_offset;
+                    if (base >= 0 && base < dv.base_cells) v += scale * double(e[base]);
                 }
                 return v;
             };
             // the row's independent loads first, so that they are in flight together
-            const int node = dv.incident[d], g0 = dv.gauge_offset[d], g1 = dv.gauge_offset[d + 1];
-            const bool on = dv.active[a];
+            double Az = a < structured ? double(t[a]) : 0.0;
+            const double rc = double(r[a]);
             const double D = dv.diag[a];
-            const double za = value(a);
-            if (node >= 0 && on)
+            const double za = on ? value(a, row.z) : double(z[a]);
+            if (incident)
             {
                 // the compact edges' two-point terms, coefficient * (z_a - z_other): the reference's
                 // sign * coefficient * (z_lower - z_upper) bit for bit (exact negations)
-                const int q0 = dv.incident_offset[node], q1 = dv.incident_offset[node + 1];
                 double sum = 0.0;
 #pragma unroll 2
-                for (int q = q0; q < q1; ++q)
+                for (int q = row.y; q < row.y + edges; ++q)
                 {
-                    const int other = dv.incident_other[q];
-                    if (dv.active[other]) sum += dv.incident_coefficient[q] * (za - value(other));
+                    const int2 other = dv.edge[q];
+                    sum += dv.edge_coefficient[q] * (za - value(other.x, other.y));
                 }
                 Az += sum;
             }
-            for (int g = g0; g < g1; ++g) Az += dv.gauge_coefficient[g] * za;
+            if (gauges)
+                for (int g = dv.gauge_offset[d], g1 = g + gauges; g < g1; ++g) Az += dv.gauge_coefficient[g] * za;
             if (kFinish == 0)
             {
                 if (!on) out[a] = TO(0);
@@ -291,8 +296,8 @@ namespace pcfd
         {
             constexpr bool kWithR = kMode != 2;
             __shared__ __align__(16) T tile[2][kTileSize];
-            __shared__ __align__(16) T rbuf[kWithR ? 2 : 1][kC3];
-            __shared__ __align__(16) uint8_t cbuf[2][kC3];
+            __shared__ __align__(16) T rbuf[kWithR ? 2 : 1][kRSize];
+            __shared__ __align__(16) uint8_t cbuf[2][kCSize];
             __shared__ double residual[kMode == 1 ? kC3 : 1];
             __shared__ __align__(16) int mbuf[kProlong == 2 ? 2 : 1][kProlong == 2 ? kTileSize : 1];   // staged map entries
             int64_t b = blockIdx.x;
@@ -323,7 +328,8 @@ namespace pcfd
                 // of four consecutive z-planes.  With rows 12 and planes 120 tile entries apart the
                 // four rows fall on disjoint shared-memory banks (float: 32 banks, offsets 0, 24, 16,
                 // 8 words; double: each half-warp's two rows 240 words apart), so no stencil read
-                // replays; consecutive cells of a row make 32- or 64-byte global segments.
+                // replays (the staged rhs and codes are padded per plane for the same reason);
+                // consecutive cells of a row make 32- or 64-byte global segments.
                 const T* F = tile[st];
                 const int l = cur.level;
                 const T h = T(v.level_h[l]);
@@ -337,12 +343,12 @@ namespace pcfd
                     const int i = threadIdx.x & 7, j = threadIdx.x >> 5, k = ((threadIdx.x >> 3) & 3) + 4 * q;
                     const int c = (k * kBS + j) * kBS + i;
                     const int s = tix(i, j, k);
-                    const uint8_t code = cbuf[st][c];
+                    const uint8_t code = cbuf[st][cix(c)];
                     const T Az = structured_row<T>(F, s, code, h);
                     if (kMode == 2) out[base + c] = TO(Az);
                     else
                     {
-                        const T rc = rbuf[st][c];
+                        const T rc = rbuf[st][rix(c)];
                         if (code & kDeferred) t[base + c] = Az;
                         if (kMode == 0)
                         {
@@ -539,16 +545,23 @@ namespace pcfd
         // where finishing them inside the brick CTAs left most threads idle (measured slower).
         // kMode 0: z_new, 1: residual into the compact deferred list, 2: residual into out[a]
         template <int kMode, class T, class TO, class TC, int kProlong>
-        __global__ void finish_deferred_kernel(DeferredView dv, int count, int64_t structured, const TC* __restrict__ e,
-                                               double scale, const int* __restrict__ map, const T* __restrict__ z,
-                                               const T* __restrict__ r, const T* __restrict__ t, TO* __restrict__ out,
-                                               double* __restrict__ residual)
+        __global__ void __launch_bounds__(256) finish_deferred_kernel(DeferredView dv, int count, int64_t structured,
+                                                                      const TC* __restrict__ e, double scale, const T* __restrict__ z,
+                                                                      const T* __restrict__ r, const T* __restrict__ t,
+                                                                      TO* __restrict__ out, double* __restrict__ residual)
         {
             const int d = blockIdx.x * blockDim.x + threadIdx.x;
             if (d >= count) return;
-            const int a = dv.dof[d];
-            finish_row<kMode, T, TO, TC, kProlong>(dv, d, a, a < structured ? double(t[a]) : 0.0, double(r[a]), z, e, scale, map,
-                                                   out, residual);
+            finish_row<kMode, T, TO, TC, kProlong>(dv, d, structured, z, r, t, e, scale, out, residual);
+        }
+
+        // map indices of the packed deferred rows and edges (composite cycle)
+        __global__ void attach_deferred_map_kernel(int4* __restrict__ row, int rows, int2* __restrict__ edge, int edges,
+                                                   const int* __restrict__ map)
+        {
+            const int i = blockIdx.x * blockDim.x + threadIdx.x;
+            if (i < rows) row[i].z = row[i].w & 1 ? map[row[i].x] : -1;
+            if (i < edges) edge[i].y = map[edge[i].x];
         }
 
         // base-level right-hand side: brick partials (levels in order) then deferred-row residuals
@@ -758,8 +771,49 @@ namespace pcfd
         }
         f.code.upload(code);
         f.deferred_count = int(ddof.size());
-        f.deferred_dof.upload(ddof);
-        f.deferred_incident.upload(dinc);
+        {
+            // packed rows and their edges to active endpoints, in incidence order
+            std::vector<int> ioff, iother;
+            std::vector<double> icoef;
+            if (o.incident_dofs)
+            {
+                ioff.resize(size_t(o.incident_dofs) + 1);
+                cuda_check(cudaMemcpy(ioff.data(), o.incident_offset.p, ioff.size() * sizeof(int), cudaMemcpyDeviceToHost),
+                           "incidence offsets download");
+                iother.resize(size_t(ioff.back()));
+                icoef.resize(size_t(ioff.back()));
+                if (!iother.empty())
+                {
+                    cuda_check(cudaMemcpy(iother.data(), o.incident_other.p, iother.size() * sizeof(int), cudaMemcpyDeviceToHost),
+                               "incidence download");
+                    cuda_check(cudaMemcpy(icoef.data(), o.incident_coefficient.p, icoef.size() * sizeof(double),
+                                          cudaMemcpyDeviceToHost), "incidence download");
+                }
+            }
+            std::vector<int4> rows(ddof.size());
+            std::vector<int2> edges;
+            std::vector<double> ecoef;
+            for (size_t d = 0; d < ddof.size(); ++d)
+            {
+                const int a = ddof[d], node = dinc[d], first = int(edges.size());
+                const bool on = t.active[a] != 0, incident = node >= 0 && on;
+                if (incident)
+                    for (int q = ioff[size_t(node)]; q < ioff[size_t(node) + 1]; ++q)
+                        if (t.active[iother[size_t(q)]])
+                        {
+                            edges.push_back(make_int2(iother[size_t(q)], -1));
+                            ecoef.push_back(icoef[size_t(q)]);
+                        }
+                const int count = int(edges.size()) - first, gauges = goff[d + 1] - goff[d];
+                if (gauges > 63 || count >= (1 << 23)) throw Error(PCFD_INTERNAL, "deferred row: too many gauges or edges");
+                rows[d] = make_int4(a, first, -1, (count << 8) | (gauges << 2) | (incident ? 2 : 0) | (on ? 1 : 0));
+            }
+            if (edges.empty()) { edges.push_back(make_int2(0, -1)); ecoef.push_back(0.0); }
+            f.deferred_row.upload(rows);
+            f.deferred_edge.upload(edges);
+            f.deferred_edge_coefficient.upload(ecoef);
+            f.map_attached = false;
+        }
         f.gauge_offset.upload(goff);
         f.gauge_coefficient.upload(gcoef.empty() ? std::vector<double>(1, 0.0) : gcoef);
         // per active brick, in active-list order: slot, level, base cell, partial offset,
@@ -796,6 +850,22 @@ namespace pcfd
         f.enabled = true;
     }
 
+    // Fills the packed deferred rows' and edges' map indices from the composite cycle's
+    // fine -> stage-1 map (called once the map exists).
+    void attach_deferred_map(System& s)
+    {
+        FineSmoother& f = s.fine;
+        if (!f.enabled || !s.fine_map.p) return;
+        const int rows = f.deferred_count, edges = int(f.deferred_edge.n);
+        const int n = std::max(rows, edges);
+        if (n > 0)
+            attach_deferred_map_kernel<<<blocks_for(n), kThreads, 0, launch_stream(s)>>>(f.deferred_row, rows, f.deferred_edge, edges,
+                                                                                          s.fine_map);
+        cuda_check(cudaGetLastError(), "deferred map indices");
+        cuda_check(cudaStreamSynchronize(launch_stream(s)), "deferred map indices");
+        f.map_attached = true;
+    }
+
     // ==================================================================================
     // launches
     // ==================================================================================
@@ -812,9 +882,8 @@ namespace pcfd
         {
             FineSmoother& f = s.fine;
             const IrregularOperator& o = s.irr;
-            return DeferredView{f.deferred_dof, f.deferred_incident, f.gauge_offset, f.gauge_coefficient, o.incident_offset,
-                                o.incident_other, o.incident_coefficient, s.active, s.diagonal, s.aggregate, s.base_offset,
-                                s.base_cells, omega};
+            return DeferredView{f.deferred_row, f.deferred_edge, f.deferred_edge_coefficient, f.gauge_offset, f.gauge_coefficient,
+                                s.diagonal, s.aggregate, s.base_offset, s.base_cells, omega};
         }
 
         template <int kMode, class T, class TO, class TC, int kProlong>
@@ -822,9 +891,9 @@ namespace pcfd
         {
             FineSmoother& f = s.fine;
             if (!f.deferred_count) return;
+            require(kProlong != 2 || f.map_attached, "deferred rows: composite map indices not attached");
             finish_deferred_kernel<kMode, T, TO, TC, kProlong><<<blocks_for(f.deferred_count), kThreads, 0, launch_stream(s)>>>(
-                deferred_view(s, omega), f.deferred_count, s.structured, e, s.mg_prolong_scale, s.fine_map.p, z, r, t, out,
-                f.deferred_residual);
+                deferred_view(s, omega), f.deferred_count, s.structured, e, s.mg_prolong_scale, z, r, t, out, f.deferred_residual);
         }
 
         // Persistent grid of a pipeline kernel: the system's CTAs per SM (autotuned), capped by the

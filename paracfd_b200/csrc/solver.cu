@@ -110,6 +110,60 @@ namespace pcfd
             d.restrict_dof.upload(h.member);
         }
 
+        // Brick-structured copy of a level numbered as 64 rows per brick (the first composite
+        // stage): every CSR coupling to a face neighbour goes to its face slot, the others to the
+        // row's rest entries, both in CSR order.  `convert` gives the stored coefficient (TK, the
+        // type the kernels read).  Leaves the level in CSR form when a row has more than 31 rest
+        // entries.
+        template <class T, class TK, class Convert>
+        void upload_brick_rows(MgLevel<T>& d, const GraphLevel& h, const std::vector<int>& neighbour, Convert convert,
+                               DBuf<TK>& rest_coefficient)
+        {
+            constexpr int W = (6 * int(sizeof(TK)) + 4 + 15) / 16;
+            if (h.cells % 64 != 0 || neighbour.size() != size_t(h.cells / 64) * 6) return;
+            std::vector<uint4> rows(size_t(h.cells) * W, make_uint4(0u, 0u, 0u, 0u));
+            std::vector<int> rest_column;
+            std::vector<TK> rest_value;
+            for (int q = 0; q < h.cells; ++q)
+            {
+                const int cell = q & 63, i = cell & 3, j = (cell >> 2) & 3, k = cell >> 4;
+                const int* nb = neighbour.data() + 6 * size_t(q >> 6);
+                auto across = [&](int f, int shift) { return nb[f] >= 0 ? nb[f] * 64 + cell + shift : -1; };
+                const int n[6] = {k > 0 ? q - 16 : across(4, 48), j > 0 ? q - 4 : across(2, 12), i > 0 ? q - 1 : across(0, 3),
+                                  i < 3 ? q + 1 : across(1, -3),  j < 3 ? q + 4 : across(3, -12), k < 3 ? q + 16 : across(5, -48)};
+                TK c[6];
+                bool set[6] = {false, false, false, false, false, false};
+                for (int f = 0; f < 6; ++f) c[f] = convert(0.0);
+                const int first = int(rest_column.size());
+                for (int e = h.row_offset[size_t(q)]; e < h.row_offset[size_t(q) + 1]; ++e)
+                {
+                    const int column = h.neighbour[size_t(e)];
+                    int f = 0;
+                    while (f < 6 && (set[f] || n[f] != column)) ++f;
+                    if (f < 6)
+                    {
+                        c[f] = convert(h.weight[size_t(e)]);
+                        set[f] = true;
+                    }
+                    else
+                    {
+                        rest_column.push_back(column);
+                        rest_value.push_back(convert(h.weight[size_t(e)]));
+                    }
+                }
+                const int count = int(rest_column.size()) - first;
+                if (count > 31 || first >= (1 << 27)) return;
+                const uint32_t descriptor = (uint32_t(first) << 5) | uint32_t(count);
+                unsigned char* row = reinterpret_cast<unsigned char*>(rows.data() + size_t(q) * W);
+                std::memcpy(row, c, sizeof(c));
+                std::memcpy(row + sizeof(c), &descriptor, sizeof(descriptor));
+            }
+            d.brick_rows.upload(rows);
+            d.brick_neighbour.upload(neighbour);
+            d.rest_column.upload(rest_column);
+            rest_coefficient.upload(rest_value);
+        }
+
         double connection_factor(const pcfd_connections& c, int e)
         {
             const double f = c.orthogonal_gradient_factor[e];
@@ -406,9 +460,12 @@ namespace pcfd
     void build_composite(System& s, const pcfd_topology& t)
     {
         const int bs = t.brick_size, c3 = bs * bs * bs, S = t.storage_size;
-        // every active structured DOF: level and global cell coordinates at that level
+        // every active structured DOF: level and global cell coordinates at that level, and the
+        // brick slot that holds the cell
         std::vector<int8_t> dof_level(size_t(S), -1);
         std::vector<std::array<int64_t, 3>> gcoord(static_cast<size_t>(S));
+        std::vector<int> dof_slot(size_t(S), -1), level_slot(size_t(t.level_count) + 1, 0);
+        for (int l = 0; l < t.level_count; ++l) level_slot[size_t(l) + 1] = level_slot[size_t(l)] + t.levels[l].brick_count;
         for (int l = 0; l < t.level_count; ++l)
         {
             const pcfd_level& lev = t.levels[l];
@@ -420,6 +477,7 @@ namespace pcfd
                     const int q = lev.level_offset + b * c3 + c;
                     if (!t.active[q]) continue;
                     dof_level[q] = int8_t(l);
+                    dof_slot[q] = level_slot[size_t(l)] + b;
                     gcoord[q] = {int64_t(lev.coord[3 * b]) * bs + c % bs, int64_t(lev.coord[3 * b + 1]) * bs + (c / bs) % bs,
                             int64_t(lev.coord[3 * b + 2]) * bs + c / (bs * bs)};
                 }
@@ -457,6 +515,7 @@ namespace pcfd
                         cell[size_t(a)] = int64_t(lev.coord[3 * b + a]) * bs +
                                           std::min<int64_t>(bs - 1, std::max<int64_t>(0, int64_t(std::floor((c[a] - lev.origin[3 * b + a]) / lev.h))));
                     dof_level[size_t(q)] = int8_t(l);
+                    dof_slot[size_t(q)] = level_slot[size_t(l)] + b;
                     gcoord[size_t(q)] = cell;
                     break;
                 }
@@ -467,10 +526,59 @@ namespace pcfd
         };
         // stage maps: stage k merges the level-l cells at global cell coordinates g into the cell
         // (l, g >> k) of the same level, so the maps nest (stage k -> k + 1 halves every index);
-        // stages stop at 512 cells or when a coarsening no longer shrinks the grid
+        // stages stop at 512 cells or when a coarsening no longer shrinks the grid.
+        // With 8^3 bricks a stage-1 cell never leaves its brick, so stage 1 is numbered as 64 rows
+        // per non-covered brick (brick rank * 64 + x + 4 y + 16 z of the 4^3 block, rows without a
+        // member stay empty): the brick-structured smoothing kernels find a row's face neighbours
+        // from its index.  Later stages are numbered in order of first appearance.
+        std::vector<int> slot_rank(size_t(level_slot.back()), -1), brick_neighbour;
+        int ranks = 0;
+        if (bs == 8)
+            for (int l = 0; l < t.level_count; ++l)
+                for (int b = 0; b < t.levels[l].brick_count; ++b)
+                    if (!(t.levels[l].flags[b] & PCFD_BRICK_COVERED)) slot_rank[size_t(level_slot[size_t(l)] + b)] = ranks++;
+        if (bs == 8)
+        {
+            brick_neighbour.assign(size_t(ranks) * 6, -1);
+            for (int l = 0; l < t.level_count; ++l)
+            {
+                const pcfd_level& lev = t.levels[l];
+                for (int b = 0; b < lev.brick_count; ++b)
+                {
+                    const int r = slot_rank[size_t(level_slot[size_t(l)] + b)];
+                    if (r < 0) continue;
+                    for (int f = 0; f < 6; ++f)
+                    {
+                        const int n = lev.neighbors[b * 6 + f];
+                        if (n >= 0 && !(lev.flags[n] & PCFD_BRICK_COVERED))
+                            brick_neighbour[size_t(r) * 6 + f] = slot_rank[size_t(level_slot[size_t(l)] + n)];
+                    }
+                }
+            }
+        }
         std::vector<std::vector<int>> map;
         std::vector<int> stage_cells;
-        for (int k = 1; k <= 16; ++k)
+        if (bs == 8 && ranks > 0)
+        {
+            std::vector<int> m(size_t(S), -1);
+            for (int q = 0; q < S; ++q)
+            {
+                const int l = dof_level[q];
+                if (l < 0) continue;
+                const int slot = dof_slot[q], b = slot - level_slot[size_t(l)];
+                const int* coord = t.levels[l].coord + 3 * b;
+                int local[3];
+                for (int a = 0; a < 3; ++a) local[a] = int(gcoord[q][size_t(a)] - int64_t(coord[a]) * bs) >> 1;
+                if (slot_rank[size_t(slot)] < 0 || local[0] < 0 || local[0] > 3 || local[1] < 0 || local[1] > 3 || local[2] < 0 ||
+                    local[2] > 3)
+                    throw Error(PCFD_INTERNAL, "composite cycle: a stage-1 cell outside its brick");
+                m[q] = slot_rank[size_t(slot)] * 64 + local[0] + 4 * local[1] + 16 * local[2];
+            }
+            map.push_back(std::move(m));
+            stage_cells.push_back(ranks * 64);
+        }
+        const bool first_is_coarsest = !stage_cells.empty() && stage_cells.front() <= 512;
+        for (int k = int(map.size()) + 1; k <= 16 && !first_is_coarsest; ++k)
         {
             std::vector<int> m(size_t(S), -1);
             std::unordered_map<uint64_t, int> index;
@@ -545,6 +653,20 @@ namespace pcfd
                     }
                     s.inter32[k].coefficient16.upload(bits);
                 }
+            if (!brick_neighbour.empty() && stages.size() > 1 && !s.mg_stage_csr)
+            {
+                MgLevel<float>& first_stage = s.inter32.front();
+                if (first_stage.coefficient16.p)
+                    upload_brick_rows<float, uint16_t>(first_stage, stages[0], brick_neighbour, [](double w) {
+                        const __half hv = __float2half_rn(float(w));
+                        uint16_t bits;
+                        std::memcpy(&bits, &hv, sizeof(bits));
+                        return bits;
+                    }, first_stage.rest_coefficient16);
+                else
+                    upload_brick_rows<float, float>(first_stage, stages[0], brick_neighbour, [](double w) { return float(w); },
+                                                    first_stage.rest_coefficient);
+            }
         }
         else
         {
@@ -557,6 +679,9 @@ namespace pcfd
                 s.inter64[k].chebyshev = s.mg_stage_chebyshev;
             }
             if (!inverse.empty()) s.inter64.back().inverse.upload(inverse);
+            if (!brick_neighbour.empty() && stages.size() > 1 && !s.mg_stage_csr)
+                upload_brick_rows<double, double>(s.inter64.front(), stages[0], brick_neighbour, [](double w) { return w; },
+                                                  s.inter64.front().rest_coefficient);
         }
         s.composite = true;
     }
@@ -640,6 +765,99 @@ namespace pcfd
             d[q] = dn;
             next[q] = xq + dn;
         }
+        // ---- brick-structured stage (rows as 4^3 blocks per fine brick) ------------------------
+        // A row's face neighbours follow from its index: inside the block at offsets 16, 4, 1, across
+        // a block face the facing cell of the neighbour block (BrickStage::neighbour).  Only the
+        // couplings that are not face neighbours (coarse/fine, cut-cell) keep a column index.
+        template <class TK> struct BrickStage
+        {
+            const uint4* rows;            // stage_row_words<TK>() 16-byte words per row
+            const int* neighbour;         // [blocks][6]: -x, +x, -y, +y, -z, +z
+            const int* rest_column;
+            const TK* rest_coefficient;
+        };
+        template <class TK> __host__ __device__ constexpr int stage_row_words() { return (6 * int(sizeof(TK)) + 4 + 15) / 16; }
+
+        // Decodes a row: six coefficients (-z, -y, -x, +x, +y, +z) then the rest descriptor, packed
+        // little-endian from the row's first byte.
+        __device__ inline void load_stage_row(const uint4* __restrict__ rows, int q, __half (&c)[6], uint32_t& rest)
+        {
+            const uint4 w = rows[q];
+            c[0] = __ushort_as_half(static_cast<unsigned short>(w.x & 0xffffu)); c[1] = __ushort_as_half(static_cast<unsigned short>(w.x >> 16));
+            c[2] = __ushort_as_half(static_cast<unsigned short>(w.y & 0xffffu)); c[3] = __ushort_as_half(static_cast<unsigned short>(w.y >> 16));
+            c[4] = __ushort_as_half(static_cast<unsigned short>(w.z & 0xffffu)); c[5] = __ushort_as_half(static_cast<unsigned short>(w.z >> 16));
+            rest = w.w;
+        }
+        __device__ inline void load_stage_row(const uint4* __restrict__ rows, int q, float (&c)[6], uint32_t& rest)
+        {
+            const uint4 w0 = rows[2 * int64_t(q)], w1 = rows[2 * int64_t(q) + 1];
+            c[0] = __uint_as_float(w0.x); c[1] = __uint_as_float(w0.y); c[2] = __uint_as_float(w0.z); c[3] = __uint_as_float(w0.w);
+            c[4] = __uint_as_float(w1.x); c[5] = __uint_as_float(w1.y);
+            rest = w1.z;
+        }
+        __device__ inline void load_stage_row(const uint4* __restrict__ rows, int q, double (&c)[6], uint32_t& rest)
+        {
+            const uint4 w0 = rows[4 * int64_t(q)], w1 = rows[4 * int64_t(q) + 1], w2 = rows[4 * int64_t(q) + 2];
+            c[0] = __hiloint2double(int(w0.y), int(w0.x)); c[1] = __hiloint2double(int(w0.w), int(w0.z));
+            c[2] = __hiloint2double(int(w1.y), int(w1.x)); c[3] = __hiloint2double(int(w1.w), int(w1.z));
+            c[4] = __hiloint2double(int(w2.y), int(w2.x)); c[5] = __hiloint2double(int(w2.w), int(w2.z));
+            rest = rows[4 * int64_t(q) + 3].x;
+        }
+
+        // Ax - (off-diagonal part of row q) x: face neighbours in the order -z, -y, -x, +x, +y, +z,
+        // then the rest entries; a face slot with a zero coefficient loads nothing.
+        template <class T, class TK>
+        __device__ inline double brick_stage_product(int q, double Ax, const TK (&c)[6], uint32_t rest, const T* __restrict__ x,
+                                                     const BrickStage<TK>& st)
+        {
+            const int cell = q & 63, i = cell & 3, j = (cell >> 2) & 3, k = cell >> 4;
+            const int* nb = st.neighbour + 6 * (q >> 6);
+            const int n[6] = {k > 0 ? q - 16 : nb[4] * 64 + cell + 48, j > 0 ? q - 4 : nb[2] * 64 + cell + 12,
+                              i > 0 ? q - 1 : nb[0] * 64 + cell + 3,   i < 3 ? q + 1 : nb[1] * 64 + cell - 3,
+                              j < 3 ? q + 4 : nb[3] * 64 + cell - 12,  k < 3 ? q + 16 : nb[5] * 64 + cell - 48};
+            double v[6];
+#pragma unroll
+            for (int f = 0; f < 6; ++f) v[f] = coefficient_value(c[f]) != 0.0 ? double(x[n[f]]) : 0.0;
+#pragma unroll
+            for (int f = 0; f < 6; ++f) Ax -= coefficient_value(c[f]) * v[f];
+            const int r0 = int(rest >> 5), r1 = r0 + int(rest & 31u);
+#pragma unroll 2
+            for (int e = r0; e < r1; ++e) Ax -= coefficient_value(st.rest_coefficient[e]) * double(x[st.rest_column[e]]);
+            return Ax;
+        }
+
+        // algebraic_chebyshev_kernel on a brick-structured stage
+        template <class T, class TK>
+        __global__ void __launch_bounds__(256) brick_stage_chebyshev_kernel(const T* __restrict__ rhs, const T* __restrict__ x,
+            T* __restrict__ next, T* __restrict__ d, BrickStage<TK> st, const T* __restrict__ diag, int cells, T c1, T c2, int first)
+        {
+            const int q = blockIdx.x * blockDim.x + threadIdx.x;
+            if (q >= cells) return;
+            const T dq = diag[q], xq = x[q], bq = rhs[q], dold = first ? T(0) : d[q];
+            TK c[6];
+            uint32_t rest;
+            load_stage_row(st.rows, q, c, rest);
+            if (!(dq > T(0))) { next[q] = T(0); d[q] = T(0); return; }
+            const double Ax = brick_stage_product<T, TK>(q, double(dq) * double(xq), c, rest, x, st);
+            const T step = c2 * T((double(bq) - Ax) / double(dq));
+            const T dn = first ? step : c1 * dold + step;
+            d[q] = dn;
+            next[q] = xq + dn;
+        }
+        template <class T, class TK>
+        __global__ void __launch_bounds__(256) brick_stage_residual_kernel(const T* __restrict__ rhs, const T* __restrict__ x,
+            T* __restrict__ residual, BrickStage<TK> st, const T* __restrict__ diag, int cells)
+        {
+            const int q = blockIdx.x * blockDim.x + threadIdx.x;
+            if (q >= cells) return;
+            const T dq = diag[q], xq = x[q], bq = rhs[q];
+            TK c[6];
+            uint32_t rest;
+            load_stage_row(st.rows, q, c, rest);
+            if (!(dq > T(0))) { residual[q] = T(0); return; }
+            residual[q] = T(double(bq) - brick_stage_product<T, TK>(q, double(dq) * double(xq), c, rest, x, st));
+        }
+
         template <class T, class TK = T>
         __global__ void __launch_bounds__(256) algebraic_residual_kernel(const T* __restrict__ rhs, const T* __restrict__ x,
             T* __restrict__ residual, const int* __restrict__ row_offset, const int* __restrict__ neighbour,
@@ -654,6 +872,14 @@ namespace pcfd
 #pragma unroll 4
             for (int e = e0; e < e1; ++e) Ax -= coefficient_value(coefficient[e]) * double(x[neighbour[e]]);
             residual[q] = T(double(bq) - Ax);
+        }
+        template <class T> BrickStage<T> brick_stage(const MgLevel<T>& l)
+        {
+            return BrickStage<T>{l.brick_rows, l.brick_neighbour, l.rest_column, l.rest_coefficient};
+        }
+        template <class T> BrickStage<__half> brick_stage16(const MgLevel<T>& l)
+        {
+            return BrickStage<__half>{l.brick_rows, l.brick_neighbour, l.rest_column, reinterpret_cast<const __half*>(l.rest_coefficient16.p)};
         }
         template <class T>
         __global__ void restrict_gather_kernel(const int* offset, const int* dof, const T* residual, int cells, T* coarse_rhs)
@@ -733,7 +959,15 @@ namespace pcfd
                         }
                         // the first composite stage's steps are the profiled stage-smoothing region
                         ProfileScope scope(s, index == 0 && s.composite ? PCFD_PROFILE_STAGE_SMOOTH : -1);
-                        if (level.coefficient16.p)
+                        if (level.brick_rows.p && level.coefficient16.p)
+                            brick_stage_chebyshev_kernel<T, __half><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
+                                level.rhs, level.x, level.temporary, level.residual, brick_stage16(level), level.diagonal, level.cells,
+                                T(c1), T(c2), sweep == 0 ? 1 : 0);
+                        else if (level.brick_rows.p)
+                            brick_stage_chebyshev_kernel<T, T><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
+                                level.rhs, level.x, level.temporary, level.residual, brick_stage(level), level.diagonal, level.cells,
+                                T(c1), T(c2), sweep == 0 ? 1 : 0);
+                        else if (level.coefficient16.p)
                             algebraic_chebyshev_kernel<T, __half><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
                                 level.rhs, level.x, level.temporary, level.residual, level.row_offset, level.neighbour,
                                 reinterpret_cast<const __half*>(level.coefficient16.p), level.diagonal, level.cells, T(c1), T(c2),
@@ -772,7 +1006,13 @@ namespace pcfd
                 return;
             }
             smooth(level.sweeps);
-            if (level.coefficient16.p)
+            if (level.brick_rows.p && level.coefficient16.p)
+                brick_stage_residual_kernel<T, __half><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
+                    level.rhs, level.x, level.residual, brick_stage16(level), level.diagonal, level.cells);
+            else if (level.brick_rows.p)
+                brick_stage_residual_kernel<T, T><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
+                    level.rhs, level.x, level.residual, brick_stage(level), level.diagonal, level.cells);
+            else if (level.coefficient16.p)
                 algebraic_residual_kernel<T, __half><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
                     level.rhs, level.x, level.residual, level.row_offset, level.neighbour,
                     reinterpret_cast<const __half*>(level.coefficient16.p), level.diagonal, level.cells);
@@ -895,21 +1135,22 @@ namespace pcfd
         run_captured(s, chain, s.mg_graph_composite, s.mg_graph_composite_launches);
     }
 
-    // Algorithmic bytes of one step of the first composite stage's smoothing: per row the row
-    // offset, rhs, x, diagonal, the direction read and written and the next iterate (7 values of
-    // 4 B in FP32, 8 B in FP64, offsets 4 B), per stored coupling its column index and coefficient.
+    // Algorithmic bytes of one step of the first composite stage's smoothing, each array read
+    // once: per row rhs, x, diagonal, the direction read and written and the next iterate (4 B
+    // each in FP32, 8 B in FP64), then in CSR form the row offset (4 B) and per stored coupling
+    // its column index and coefficient; in brick-structured form the row's 16-byte words, per rest
+    // entry its column and coefficient and per block its six neighbour blocks.
     double stage_smooth_bytes(const System& s)
     {
-        if (s.composite_fp32 && !s.inter32.empty())
-        {
-            const MgLevel<float>& l = s.inter32.front();
-            return 28.0 * l.cells + (4.0 + (l.coefficient16.p ? 2.0 : 4.0)) * double(l.neighbour.n);
-        }
-        if (!s.inter64.empty())
-        {
-            const MgLevel<double>& l = s.inter64.front();
-            return 52.0 * l.cells + 12.0 * double(l.neighbour.n);
-        }
+        auto bytes = [](const auto& l, double value) {
+            const double coefficient = l.coefficient16.p ? 2.0 : value;
+            if (l.brick_rows.p)
+                return 6.0 * value * l.cells + 16.0 * double(l.brick_rows.n) + (4.0 + coefficient) * double(l.rest_column.n) +
+                       24.0 * double(l.cells / 64);
+            return 6.0 * value * l.cells + 4.0 * l.cells + (4.0 + coefficient) * double(l.neighbour.n);
+        };
+        if (s.composite_fp32 && !s.inter32.empty()) return bytes(s.inter32.front(), 4.0);
+        if (!s.inter64.empty()) return bytes(s.inter64.front(), 8.0);
         return 0.0;
     }
 
@@ -919,7 +1160,15 @@ namespace pcfd
         require(s.composite && (!s.inter32.empty() || !s.inter64.empty()), "stage smoothing step: the composite cycle");
         auto run = [&](auto& level) {
             using T = typename std::remove_reference_t<decltype(level)>::value_type;
-            if (level.coefficient16.p)
+            if (level.brick_rows.p && level.coefficient16.p)
+                brick_stage_chebyshev_kernel<T, __half><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
+                    level.rhs, level.x, level.temporary, level.residual, brick_stage16(level), level.diagonal, level.cells, T(0.5),
+                    T(0.7), 0);
+            else if (level.brick_rows.p)
+                brick_stage_chebyshev_kernel<T, T><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
+                    level.rhs, level.x, level.temporary, level.residual, brick_stage(level), level.diagonal, level.cells, T(0.5),
+                    T(0.7), 0);
+            else if (level.coefficient16.p)
                 algebraic_chebyshev_kernel<T, __half><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
                     level.rhs, level.x, level.temporary, level.residual, level.row_offset, level.neighbour,
                     reinterpret_cast<const __half*>(level.coefficient16.p), level.diagonal, level.cells, T(0.5), T(0.7), 0);

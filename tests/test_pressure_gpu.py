@@ -287,3 +287,24 @@ def test_orthogonal_pcg_on_a_grid_without_wls_nodes(gpu):
         true = np.linalg.norm((b - rc.apply(x))[act]) / np.linalg.norm(b[act])
         assert true <= 1e-8 * 1.01, (precision, true, res)
     rc.close()
+
+
+@pytest.mark.parametrize("precision,fp16,tolerance", [(MG_FP64, 0, 1e-13), (MG_FP32, 0, 1e-5), (MG_FP32, 1, 1e-5)])
+def test_brick_structured_first_stage_matches_csr_stage(gpu, precision, fp16, tolerance):
+    """The first composite stage as 64 rows per 8^3 brick (face neighbours from the row index,
+    the other couplings as rest entries) holds the same couplings as its CSR rows; only the order
+    of each row's double-precision sum differs.  On the NACA slab (1 level) and the 3-level
+    cut-cell wing (coarse/fine and cut-cell couplings in the rest entries) the preconditioner
+    agrees with the CSR stage to rounding."""
+    from tests.test_loads_gpu import WING3
+    for rc in (ref.naca_slab_case(base_cell_size=1 / 16), ref.workload_case(WING3)):
+        r = np.random.default_rng(67).standard_normal(rc.n) * rc.active
+        act = rc.active.astype(bool)
+        out = []
+        for csr in (0, 1):
+            with CompositeSystem(rc.topology, mg_cycle=2, mg_precision=precision, mg_stage_fp16=fp16,
+                                 mg_stage_csr=csr) as s:
+                assert s.stage_brick_structured == (csr == 0)
+                out.append(s.precondition(r))
+        rc.close()
+        assert rel(out[0], out[1], act) <= tolerance
