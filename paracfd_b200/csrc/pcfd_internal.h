@@ -147,6 +147,7 @@ namespace pcfd
         DBuf<int> gauge_offset;
         DBuf<double> gauge_coefficient;
         bool map_attached = false;              // deferred map indices filled from the composite stage-1 map
+        DBuf<int> stage_neighbour;              // composite cycle: [active bricks][6] face-neighbour brick ranks or -1
         DBuf<int> meta;                         // [active bricks][16] slot, level, level-0 cell, partial, neighbours
         DBuf<double> partial, deferred_residual;
         DBuf<int> gather_offset, gather_entry;  // base cell -> partials (>= 0) / deferred rows (< 0)
@@ -243,6 +244,7 @@ namespace pcfd
         std::vector<MgLevel<double>> inter64;
         std::vector<MgLevel<float>> inter32;    // the same stages in float (FP32 multigrid)
         DBuf<int> fine_map, fine_restrict_offset, fine_restrict_dof;   // fine DOF -> first coarse cell
+        bool first_stage_bricks = false;        // stage 1 numbered by brick rank: the restriction CSR lists EB fragments only
         DBuf<double> fine_residual;             // [S] r - A_orth z before the first restriction
         FineSmoother fine;
         cudaGraphExec_t mg_graph64 = nullptr, mg_graph32 = nullptr, mg_graph_composite = nullptr;   // captured hierarchies
@@ -337,6 +339,32 @@ namespace pcfd
     {
         ++s.launches;
         return s.stream;
+    }
+
+    // Programmatic dependent launch for chains of short dependent kernels (the multigrid stages):
+    // launch_chained lets the kernel be scheduled while the previous kernel on the stream drains.
+    // Such a kernel starts with chain_wait() (it returns once the previous grid has completed and
+    // its memory is visible), so nothing it reads or writes overlaps the previous kernel, and then
+    // calls chain_release() so that the next kernel may be scheduled once all its CTAs run.
+    // Without a programmatic predecessor both are no-ops.
+    __device__ __forceinline__ void chain_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+    __device__ __forceinline__ void chain_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+    template <typename T> struct Exactly { using type = T; };   // keeps Params deduced from the kernel only
+    template <typename... Params>
+    inline void launch_chained(System& s, void (*kernel)(Params...), unsigned grid, unsigned block,
+                               typename Exactly<Params>::type... args)
+    {
+        cudaLaunchConfig_t config{};
+        config.gridDim = dim3(grid);
+        config.blockDim = dim3(block);
+        config.dynamicSmemBytes = 0;
+        config.stream = launch_stream(s);
+        cudaLaunchAttribute attribute{};
+        attribute.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attribute.val.programmaticStreamSerializationAllowed = 1;
+        config.attrs = &attribute;
+        config.numAttrs = 1;
+        cuda_check(cudaLaunchKernelEx(&config, kernel, args...), "chained launch");
     }
 
     // Records a start/stop event pair on the system stream around one launch of the region being

@@ -47,7 +47,10 @@ namespace pcfd
             const double* level_h;
             const uint8_t* code;
             double prolong;            // scale of the prolonged coarse correction
-            const int* map;            // composite cycle: fine DOF -> first stage cell (mapped prolongation)
+            // composite cycle: per brick (active-list order = brick rank) the rank of each face
+            // neighbour or -1.  Stage 1 is numbered rank * 64 + (i >> 1) + 4 (j >> 1) + 16 (k >> 1),
+            // so the prolongation computes a cell's stage-1 row instead of loading it.
+            const int* stage_neighbour;
         };
 
         // Shared tile of one brick plus its face halos: rows of 12 doubles so that interior rows
@@ -123,23 +126,20 @@ namespace pcfd
         // What one thread needs of a brick: the head and the neighbour of the halo face it copies.
         struct Ticket
         {
-            int slot, level, base, partial, nbr, nbase;
+            int slot, level, base, partial, nbr, nbase, rank, nrank;
         };
         __device__ inline int halo_face(int t) { return t < 128 ? 2 + (t >> 5) : ((t - 128) >> 6); }
-        __device__ inline Ticket load_ticket(const BrickMeta* meta, int64_t b)
+        __device__ inline Ticket load_ticket(const BrickView& v, int64_t b)
         {
-            const BrickMeta* m = meta + b;
+            const BrickMeta* m = v.meta + b;
             const int4 h = *reinterpret_cast<const int4*>(m);
             const int face = halo_face(threadIdx.x);
-            return Ticket{h.x, h.y, h.z, h.w, m->nbr[face], m->nbase[face]};
+            return Ticket{h.x, h.y, h.z, h.w, m->nbr[face], m->nbase[face], int(b), v.stage_neighbour ? v.stage_neighbour[6 * b + face] : -1};
         }
 
-        // kMapped: also the fine -> stage-1 map entries of the same tile positions (mbuf), so that
-        // the prolongation reads them from shared memory instead of waiting on a global load
-        template <class T, bool kWithR, bool kMapped = false>
+        template <class T, bool kWithR>
         __device__ inline void issue_brick(const Ticket& k, const T* __restrict__ z, const T* __restrict__ r,
-                                           const uint8_t* __restrict__ code, T* tile, T* rbuf, uint8_t* cbuf,
-                                           const int* __restrict__ map = nullptr, int* mbuf = nullptr)
+                                           const uint8_t* __restrict__ code, T* tile, T* rbuf, uint8_t* cbuf)
         {
             const int t = threadIdx.x;
             const int64_t base = int64_t(k.slot) * kC3;
@@ -147,7 +147,6 @@ namespace pcfd
                 const int c = 2 * t, i = c & 7, j = (c >> 3) & 7, kk = c >> 6;
                 copy_pair<T>(tile + tix(i, j, kk), z + base + c, true);
                 if (kWithR) copy_pair<T>(rbuf + rix(c), r + base + c, true);
-                if (kMapped) copy8(mbuf + tix(i, j, kk), map + base + c, true);
             }
             if (t < 32) copy16(cbuf + cix(16 * t), code + base + 16 * t, true);
             const bool valid = k.nbr >= 0;
@@ -159,38 +158,36 @@ namespace pcfd
                 if (face < 4) { kk = w >> 2; i = (w & 3) * 2; j = face == 2 ? kBS - 1 : 0; hj = face == 2 ? -1 : kBS; hk = kk; }
                 else { i = (w * 2) & 7; j = (w * 2) >> 3; kk = face == 4 ? kBS - 1 : 0; hj = j; hk = face == 4 ? -1 : kBS; }
                 copy_pair<T>(tile + tix(i, hj, hk), z + nb + (kk * kBS + j) * kBS + i, valid);
-                if (kMapped) copy8(mbuf + tix(i, hj, hk), map + nb + (kk * kBS + j) * kBS + i, valid);
             }
             else
             {
                 const int u = t - 128, face = u >> 6, j = u & 7, kk = (u >> 3) & 7;
                 const int i = face == 0 ? kBS - 1 : 0, hi = face == 0 ? -1 : kBS;
                 copy_one<T>(tile + tix(hi, j, kk), z + nb + (kk * kBS + j) * kBS + i, valid);
-                if (kMapped) copy4(mbuf + tix(hi, j, kk), map + nb + (kk * kBS + j) * kBS + i, valid);
             }
         }
 
-        // adds the coarse correction to the tile entries this thread copied; kMapped: through the
-        // fine -> stage-1 map of the composite cycle, else the geometric level-0 cell
+        // adds the coarse correction to the tile entries this thread copied; kMapped: the composite
+        // cycle's stage-1 row of the cell (its brick's rank * 64 + the 2x2x2 block of the cell;
+        // an inactive cell's tile entry takes a correction too, but no open face reads it), else
+        // the geometric level-0 cell
         template <class T, class TC, bool kMapped>
-        __device__ inline void prolong_own(const Ticket& k, const TC* __restrict__ e, double scale, const int* __restrict__ mbuf, T* tile)
+        __device__ inline void prolong_own(const Ticket& k, const TC* __restrict__ e, double scale, T* tile)
         {
             const int t = threadIdx.x, l = k.level;
             auto add = [&](int s_tile, int64_t q, int b0, int i, int j, int kk) {
-                if (kMapped)
-                {
-                    const int c = mbuf[s_tile];   // map[q], staged with the tile
-                    if (c >= 0) tile[s_tile] += T(scale * double(e[c]));
-                }
+                if (kMapped) tile[s_tile] += T(scale * double(e[b0 * 64 + (i >> 1) + 4 * (j >> 1) + 16 * (kk >> 1)]));
                 else tile[s_tile] += T(scale * double(e[base_cell_of(b0, l, i, j, kk)]));
             };
             {
                 const int c = 2 * t, i = c & 7, j = (c >> 3) & 7, kk = c >> 6;
                 const int64_t q = int64_t(k.slot) * kC3 + c;
-                add(tix(i, j, kk), q, k.base, i, j, kk);
-                add(tix(i + 1, j, kk), q + 1, k.base, i + 1, j, kk);
+                const int own = kMapped ? k.rank : k.base;
+                add(tix(i, j, kk), q, own, i, j, kk);
+                add(tix(i + 1, j, kk), q + 1, own, i + 1, j, kk);
             }
-            if (k.nbr < 0) return;
+            if (k.nbr < 0 || (kMapped && k.nrank < 0)) return;
+            const int other = kMapped ? k.nrank : k.nbase;
             const int64_t nb = int64_t(k.nbr) * kC3;
             if (t < 128)
             {
@@ -199,14 +196,14 @@ namespace pcfd
                 if (face < 4) { kk = w >> 2; i = (w & 3) * 2; j = face == 2 ? kBS - 1 : 0; hj = face == 2 ? -1 : kBS; hk = kk; }
                 else { i = (w * 2) & 7; j = (w * 2) >> 3; kk = face == 4 ? kBS - 1 : 0; hj = j; hk = face == 4 ? -1 : kBS; }
                 const int64_t q = nb + (kk * kBS + j) * kBS + i;
-                add(tix(i, hj, hk), q, k.nbase, i, j, kk);
-                add(tix(i + 1, hj, hk), q + 1, k.nbase, i + 1, j, kk);
+                add(tix(i, hj, hk), q, other, i, j, kk);
+                add(tix(i + 1, hj, hk), q + 1, other, i + 1, j, kk);
             }
             else
             {
                 const int u = t - 128, face = u >> 6, j = u & 7, kk = (u >> 3) & 7;
                 const int i = face == 0 ? kBS - 1 : 0, hi = face == 0 ? -1 : kBS;
-                add(tix(hi, j, kk), nb + (kk * kBS + j) * kBS + i, k.nbase, i, j, kk);
+                add(tix(hi, j, kk), nb + (kk * kBS + j) * kBS + i, other, i, j, kk);
             }
         }
 
@@ -299,14 +296,13 @@ namespace pcfd
             __shared__ __align__(16) T rbuf[kWithR ? 2 : 1][kRSize];
             __shared__ __align__(16) uint8_t cbuf[2][kCSize];
             __shared__ double residual[kMode == 1 ? kC3 : 1];
-            __shared__ __align__(16) int mbuf[kProlong == 2 ? 2 : 1][kProlong == 2 ? kTileSize : 1];   // staged map entries
             int64_t b = blockIdx.x;
             if (b >= bricks) return;
             const int64_t G = gridDim.x;
-            Ticket cur = load_ticket(v.meta, b);
-            issue_brick<T, kWithR, kProlong == 2>(cur, z, r, v.code, tile[0], rbuf[0], cbuf[0], v.map, mbuf[0]);
+            Ticket cur = load_ticket(v, b);
+            issue_brick<T, kWithR>(cur, z, r, v.code, tile[0], rbuf[0], cbuf[0]);
             copy_commit();
-            Ticket next = b + G < bricks ? load_ticket(v.meta, b + G) : cur;
+            Ticket next = b + G < bricks ? load_ticket(v, b + G) : cur;
             for (int it = 0;; ++it)
             {
                 const int st = it & 1;
@@ -314,14 +310,13 @@ namespace pcfd
                 Ticket after = next;
                 if (has_next)
                 {
-                    issue_brick<T, kWithR, kProlong == 2>(next, z, r, v.code, tile[st ^ 1], rbuf[kWithR ? (st ^ 1) : 0], cbuf[st ^ 1],
-                                                          v.map, mbuf[kProlong == 2 ? (st ^ 1) : 0]);
+                    issue_brick<T, kWithR>(next, z, r, v.code, tile[st ^ 1], rbuf[kWithR ? (st ^ 1) : 0], cbuf[st ^ 1]);
                     copy_commit();
-                    if (b + 2 * G < bricks) after = load_ticket(v.meta, b + 2 * G);
+                    if (b + 2 * G < bricks) after = load_ticket(v, b + 2 * G);
                     copy_wait<1>();
                 }
                 else copy_wait<0>();
-                if (kProlong) prolong_own<T, TC, kProlong == 2>(cur, e, v.prolong, mbuf[kProlong == 2 ? st : 0], tile[st]);
+                if (kProlong) prolong_own<T, TC, kProlong == 2>(cur, e, v.prolong, tile[st]);
                 __syncthreads();
                 // ---- compute brick `cur` from buffer st.  Thread t owns cell (i, j, k) = (t & 7,
                 // t >> 5, (t >> 3 & 3) + 4 q), q = 0, 1: a warp covers one x-row of 8 cells in each
@@ -874,7 +869,7 @@ namespace pcfd
         BrickView view(System& s)
         {
             return BrickView{reinterpret_cast<const BrickMeta*>(s.fine.meta.p), s.d_level_h, s.fine.code, s.mg_prolong_scale,
-                             s.fine_map.p};
+                             s.fine.stage_neighbour.p};
         }
 
         // the deferred rows' arrays
@@ -933,6 +928,7 @@ namespace pcfd
         void sweep(System& s, const T* z, const T* r, TO* out, const TC* e, int slot = -1)
         {
             FineBuffers<T> w(s.fine);
+            require(kProlong != 2 || s.fine.stage_neighbour.p, "mapped prolongation: stage-1 brick ranks not set");
             const bool cheb = slot >= 0 && w.chebyshev;
             const T* damping = cheb ? w.chebyshev + size_t(slot) * s.fine.cheb_stride : w.damping;
             const double omega = cheb ? s.fine.cheb_omega[slot] : 2.0 / 3.0;
@@ -1021,6 +1017,43 @@ namespace pcfd
             rhs[c] = TC(sum);
         }
 
+        // The same gather with stage 1 numbered by brick rank: row c's structured members are the
+        // 2x2x2 block (c & 63) of brick slot[c >> 6], summed in ascending DOF order (inactive DOFs
+        // hold a zero residual), then its EB fragments from the CSR.
+        template <class TC, class TR>
+        __global__ void __launch_bounds__(256) gather_first_brick_kernel(int cells, const int* __restrict__ slot,
+            const int* __restrict__ offset, const int* __restrict__ dof, const TR* __restrict__ residual, TC* __restrict__ rhs)
+        {
+            const int c = blockIdx.x * blockDim.x + threadIdx.x;
+            if (c >= cells) return;
+            const int block = c & 63;
+            const int64_t base = int64_t(slot[c >> 6]) * kC3 + 2 * (block & 3) + 16 * ((block >> 2) & 3) + 128 * (block >> 4);
+            const int q0 = offset[c], q1 = offset[c + 1];
+            TR v[8];
+#pragma unroll
+            for (int m = 0; m < 4; ++m)
+            {
+                v[2 * m] = residual[base + 64 * (m >> 1) + 8 * (m & 1)];
+                v[2 * m + 1] = residual[base + 64 * (m >> 1) + 8 * (m & 1) + 1];
+            }
+            double sum = 0.0;
+#pragma unroll
+            for (int m = 0; m < 8; ++m) sum += v[m];
+            for (int q = q0; q < q1; ++q) sum += residual[dof[q]];
+            rhs[c] = TC(sum);
+        }
+
+        template <class TC, class TR>
+        void gather_first(System& s, const TR* residual, MgLevel<TC>& first)
+        {
+            if (s.first_stage_bricks)
+                gather_first_brick_kernel<TC, TR><<<blocks_for(first.cells), kThreads, 0, launch_stream(s)>>>(
+                    first.cells, s.active_brick_list, s.fine_restrict_offset, s.fine_restrict_dof, residual, first.rhs);
+            else
+                gather_first_kernel<TC, TR><<<blocks_for(first.cells), kThreads, 0, launch_stream(s)>>>(
+                    first.cells, s.fine_restrict_offset, s.fine_restrict_dof, residual, first.rhs);
+        }
+
         // residual of the pre-smoothed z, its gather into stage 1, the stage V-cycle, the weighted
         // prolongation fused into the first post-sweep, one more post-sweep
         template <class TC> void composite_tail(System& s, const double* r, double* z, MgLevel<TC>& first, bool schedule = true);
@@ -1080,8 +1113,7 @@ namespace pcfd
             brick_pipe_kernel<3, double, double, TC, 0><<<pipe_grid<3, double>(s), 256, 0, launch_stream(s)>>>(
                 view(s), s.active_bricks, z, r, res, f.t.p, nullptr, nullptr, f.damping.p);
             finish<2, double, double, TC, 0>(s, z, r, res, static_cast<const TC*>(nullptr), f.t.p);
-            gather_first_kernel<TC, double><<<blocks_for(first.cells), kThreads, 0, launch_stream(s)>>>(
-                first.cells, s.fine_restrict_offset, s.fine_restrict_dof, res, first.rhs);
+            gather_first<TC, double>(s, res, first);
             cuda_check(cudaMemsetAsync(first.x, 0, size_t(first.cells) * sizeof(TC), s.stream), "clear stage correction");
             composite_levels(s);
             sweep<double, double, TC, 2>(s, z, r, a, first.x.p, schedule ? 2 : -1);
@@ -1102,8 +1134,7 @@ namespace pcfd
             brick_pipe_kernel<3, float, float, float, 0><<<pipe_grid<3, float>(s), 256, 0, launch_stream(s)>>>(
                 view(s), s.active_bricks, b, r32, res, f.t32.p, nullptr, nullptr, f.damping32.p);
             finish<2, float, float, float, 0>(s, b, r32, res, static_cast<const float*>(nullptr), f.t32.p);
-            gather_first_kernel<float, float><<<blocks_for(first.cells), kThreads, 0, launch_stream(s)>>>(
-                first.cells, s.fine_restrict_offset, s.fine_restrict_dof, res, first.rhs);
+            gather_first<float, float>(s, res, first);
             cuda_check(cudaMemsetAsync(first.x, 0, size_t(first.cells) * sizeof(float), s.stream), "clear stage correction");
             composite_levels(s);
             sweep<float, float, float, 2>(s, b, r32, a, first.x.p, 2);

@@ -576,6 +576,10 @@ namespace pcfd
             }
             map.push_back(std::move(m));
             stage_cells.push_back(ranks * 64);
+            // the fused fine level computes stage-1 rows from brick ranks (its active bricks are the
+            // non-covered bricks in the same order)
+            if (ranks != s.active_bricks) throw Error(PCFD_INTERNAL, "composite cycle: brick ranks do not match the active bricks");
+            s.fine.stage_neighbour.upload(brick_neighbour);
         }
         const bool first_is_coarsest = !stage_cells.empty() && stage_cells.front() <= 512;
         for (int k = int(map.size()) + 1; k <= 16 && !first_is_coarsest; ++k)
@@ -619,10 +623,20 @@ namespace pcfd
             }
             group_members(level.parent, stage_cells[size_t(k) + 1], level.member_offset, level.member);
         }
-        // fine -> stage 1 map and restriction CSR (DOF order kept)
+        // fine -> stage 1 map and restriction CSR (DOF order kept).  With stage 1 numbered by brick
+        // rank, a row's structured members follow from its index and only the EB fragments
+        // mapped to it are listed.
         const std::vector<int>& first = map[0];
         std::vector<int> roff, rdof;
-        group_members(first, stage_cells[0], roff, rdof);
+        s.first_stage_bricks = s.fine.stage_neighbour.p != nullptr;
+        if (s.first_stage_bricks)
+        {
+            std::vector<int> fragments(first);
+            std::fill(fragments.begin(), fragments.begin() + std::min<size_t>(fragments.size(), size_t(s.structured)), -1);
+            group_members(fragments, stage_cells[0], roff, rdof);
+        }
+        else
+            group_members(first, stage_cells[0], roff, rdof);
         s.fine_map.upload(first);
         s.fine_restrict_offset.upload(roff);
         s.fine_restrict_dof.upload(rdof);
@@ -734,6 +748,8 @@ namespace pcfd
         template <class T>
         __global__ void dense_apply_kernel(const T* __restrict__ inverse, const T* __restrict__ rhs, T* __restrict__ x, int n)
         {
+            chain_wait();
+            chain_release();
             const int row = int((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
             if (row >= n) return;
             double acc = 0.0;
@@ -752,6 +768,8 @@ namespace pcfd
             T* __restrict__ next, T* __restrict__ d, const int* __restrict__ row_offset, const int* __restrict__ neighbour,
             const TK* __restrict__ coefficient, const T* __restrict__ diag, int cells, T c1, T c2, int first)
         {
+            chain_wait();
+            chain_release();
             const int q = blockIdx.x * blockDim.x + threadIdx.x;
             if (q >= cells) return;
             const T dq = diag[q], xq = x[q], bq = rhs[q], dold = first ? T(0) : d[q];
@@ -765,6 +783,24 @@ namespace pcfd
             d[q] = dn;
             next[q] = xq + dn;
         }
+        // The first Chebyshev step from x = 0 (every pre-smoothing of a stage correction): the
+        // residual is the right-hand side, so d = c2 D^-1 rhs and next = 0 + d without reading the
+        // matrix or the iterate; the same values as the general step.
+        template <class T>
+        __global__ void __launch_bounds__(256) chebyshev_zero_start_kernel(const T* __restrict__ rhs, T* __restrict__ next,
+                                                                           T* __restrict__ d, const T* __restrict__ diag, int cells, T c2)
+        {
+            chain_wait();
+            chain_release();
+            const int q = blockIdx.x * blockDim.x + threadIdx.x;
+            if (q >= cells) return;
+            const T dq = diag[q], bq = rhs[q];
+            if (!(dq > T(0))) { next[q] = T(0); d[q] = T(0); return; }
+            const T step = c2 * T(double(bq) / double(dq));
+            d[q] = step;
+            next[q] = T(0) + step;
+        }
+
         // ---- brick-structured stage (rows as 4^3 blocks per fine brick) ------------------------
         // A row's face neighbours follow from its index: inside the block at offsets 16, 4, 1, across
         // a block face the facing cell of the neighbour block (BrickStage::neighbour).  Only the
@@ -831,6 +867,8 @@ namespace pcfd
         __global__ void __launch_bounds__(256) brick_stage_chebyshev_kernel(const T* __restrict__ rhs, const T* __restrict__ x,
             T* __restrict__ next, T* __restrict__ d, BrickStage<TK> st, const T* __restrict__ diag, int cells, T c1, T c2, int first)
         {
+            chain_wait();
+            chain_release();
             const int q = blockIdx.x * blockDim.x + threadIdx.x;
             if (q >= cells) return;
             const T dq = diag[q], xq = x[q], bq = rhs[q], dold = first ? T(0) : d[q];
@@ -848,6 +886,8 @@ namespace pcfd
         __global__ void __launch_bounds__(256) brick_stage_residual_kernel(const T* __restrict__ rhs, const T* __restrict__ x,
             T* __restrict__ residual, BrickStage<TK> st, const T* __restrict__ diag, int cells)
         {
+            chain_wait();
+            chain_release();
             const int q = blockIdx.x * blockDim.x + threadIdx.x;
             if (q >= cells) return;
             const T dq = diag[q], xq = x[q], bq = rhs[q];
@@ -863,6 +903,8 @@ namespace pcfd
             T* __restrict__ residual, const int* __restrict__ row_offset, const int* __restrict__ neighbour,
             const TK* __restrict__ coefficient, const T* __restrict__ diag, int cells)
         {
+            chain_wait();
+            chain_release();
             const int q = blockIdx.x * blockDim.x + threadIdx.x;
             if (q >= cells) return;
             const T dq = diag[q], xq = x[q], bq = rhs[q];
@@ -884,6 +926,8 @@ namespace pcfd
         template <class T>
         __global__ void restrict_gather_kernel(const int* offset, const int* dof, const T* residual, int cells, T* coarse_rhs)
         {
+            chain_wait();
+            chain_release();
             const int c = blockIdx.x * blockDim.x + threadIdx.x;
             if (c >= cells) return;
             double sum = 0.0;
@@ -893,6 +937,8 @@ namespace pcfd
         template <class T>
         __global__ void prolong_add_kernel(const int* aggregate, int cells, const T* coarse_x, T* fine_x, T scale)
         {
+            chain_wait();
+            chain_release();
             const int q = blockIdx.x * blockDim.x + threadIdx.x;
             if (q < cells && aggregate[q] >= 0) fine_x[q] += scale * coarse_x[aggregate[q]];
         }
@@ -939,7 +985,9 @@ namespace pcfd
         {
             MgLevel<T>& level = *chain[index];
             const T omega = T(kOmega);
-            auto smooth = [&](int sweeps) {
+            // from_zero: x is 0 on entry (pre-smoothing of a correction), so the first Chebyshev
+            // step needs neither the matrix nor x
+            auto smooth = [&](int sweeps, bool from_zero) {
                 if (level.chebyshev >= 2)
                 {
                     // Chebyshev polynomial smoothing on [2 / ratio, 2] (D^-1 A of a diagonally dominant
@@ -957,23 +1005,30 @@ namespace pcfd
                             c2 = 2.0 * next / delta;
                             rho = next;
                         }
-                        // the first composite stage's steps are the profiled stage-smoothing region
+                        if (from_zero && sweep == 0)
+                        {
+                            launch_chained(s, chebyshev_zero_start_kernel<T>, blocks_for(level.cells), kThreads,
+                                level.rhs, level.temporary, level.residual, level.diagonal, level.cells, T(c2));
+                            std::swap(level.x.p, level.temporary.p);
+                            continue;
+                        }
+                        // the first composite stage's full steps are the profiled stage-smoothing region
                         ProfileScope scope(s, index == 0 && s.composite ? PCFD_PROFILE_STAGE_SMOOTH : -1);
                         if (level.brick_rows.p && level.coefficient16.p)
-                            brick_stage_chebyshev_kernel<T, __half><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
+                            launch_chained(s, brick_stage_chebyshev_kernel<T, __half>, blocks_for(level.cells), kThreads,
                                 level.rhs, level.x, level.temporary, level.residual, brick_stage16(level), level.diagonal, level.cells,
                                 T(c1), T(c2), sweep == 0 ? 1 : 0);
                         else if (level.brick_rows.p)
-                            brick_stage_chebyshev_kernel<T, T><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
+                            launch_chained(s, brick_stage_chebyshev_kernel<T, T>, blocks_for(level.cells), kThreads,
                                 level.rhs, level.x, level.temporary, level.residual, brick_stage(level), level.diagonal, level.cells,
                                 T(c1), T(c2), sweep == 0 ? 1 : 0);
                         else if (level.coefficient16.p)
-                            algebraic_chebyshev_kernel<T, __half><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
+                            launch_chained(s, algebraic_chebyshev_kernel<T, __half>, blocks_for(level.cells), kThreads,
                                 level.rhs, level.x, level.temporary, level.residual, level.row_offset, level.neighbour,
                                 reinterpret_cast<const __half*>(level.coefficient16.p), level.diagonal, level.cells, T(c1), T(c2),
                                 sweep == 0 ? 1 : 0);
                         else
-                            algebraic_chebyshev_kernel<T, T><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
+                            launch_chained(s, algebraic_chebyshev_kernel<T, T>, blocks_for(level.cells), kThreads,
                                 level.rhs, level.x, level.temporary, level.residual, level.row_offset, level.neighbour, level.coefficient,
                                 level.diagonal, level.cells, T(c1), T(c2), sweep == 0 ? 1 : 0);
                         std::swap(level.x.p, level.temporary.p);
@@ -996,37 +1051,42 @@ namespace pcfd
             if (index + 1 == count)
             {
                 if (level.inverse.p)
-                    dense_apply_kernel<T><<<blocks_for(int64_t(level.cells) * 32), kThreads, 0, launch_stream(s)>>>(level.inverse, level.rhs,
+                    launch_chained(s, dense_apply_kernel<T>, blocks_for(int64_t(level.cells) * 32), kThreads, level.inverse, level.rhs,
                                                                                                               level.x, level.cells);
                 else if (level.cells <= 4096)
                     coarse_jacobi_kernel<T, 4><<<1, 1024, 0, launch_stream(s)>>>(level.rhs, level.x, level.temporary, level.row_offset,
                         level.neighbour, level.coefficient, level.diagonal, level.cells, omega, 96);
                 else
-                    smooth(96);
+                    smooth(96, true);
                 return;
             }
-            smooth(level.sweeps);
+            smooth(level.sweeps, true);
             if (level.brick_rows.p && level.coefficient16.p)
-                brick_stage_residual_kernel<T, __half><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
+                launch_chained(s, brick_stage_residual_kernel<T, __half>, blocks_for(level.cells), kThreads,
                     level.rhs, level.x, level.residual, brick_stage16(level), level.diagonal, level.cells);
             else if (level.brick_rows.p)
-                brick_stage_residual_kernel<T, T><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
+                launch_chained(s, brick_stage_residual_kernel<T, T>, blocks_for(level.cells), kThreads,
                     level.rhs, level.x, level.residual, brick_stage(level), level.diagonal, level.cells);
             else if (level.coefficient16.p)
-                algebraic_residual_kernel<T, __half><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
+                launch_chained(s, algebraic_residual_kernel<T, __half>, blocks_for(level.cells), kThreads,
                     level.rhs, level.x, level.residual, level.row_offset, level.neighbour,
                     reinterpret_cast<const __half*>(level.coefficient16.p), level.diagonal, level.cells);
             else
-                algebraic_residual_kernel<T, T><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(
+                launch_chained(s, algebraic_residual_kernel<T, T>, blocks_for(level.cells), kThreads,
                     level.rhs, level.x, level.residual, level.row_offset, level.neighbour, level.coefficient, level.diagonal, level.cells);
             MgLevel<T>& coarse = *chain[index + 1];
-            restrict_gather_kernel<T><<<blocks_for(coarse.cells), kThreads, 0, launch_stream(s)>>>(
+            launch_chained(s, restrict_gather_kernel<T>, blocks_for(coarse.cells), kThreads,
                 level.restrict_offset, level.restrict_dof, level.residual, coarse.cells, coarse.rhs);
-            cuda_check(cudaMemsetAsync(coarse.x, 0, size_t(coarse.cells) * sizeof(T), s.stream), "clear coarse correction");
+            // the coarse correction starts from 0; only a first step that reads x needs it cleared
+            const bool coarsest = index + 2 == count;
+            const bool writes_x_first = coarse.chebyshev >= 2 ? !(coarsest && !coarse.inverse.p && coarse.cells <= 4096)
+                                                              : (coarsest && coarse.inverse.p);
+            if (!writes_x_first)
+                cuda_check(cudaMemsetAsync(coarse.x, 0, size_t(coarse.cells) * sizeof(T), s.stream), "clear coarse correction");
             mg_level(s, chain, count, index + 1);
-            prolong_add_kernel<T><<<blocks_for(level.cells), kThreads, 0, launch_stream(s)>>>(level.aggregate, level.cells, coarse.x, level.x,
+            launch_chained(s, prolong_add_kernel<T>, blocks_for(level.cells), kThreads, level.aggregate, level.cells, coarse.x, level.x,
                                                                                              T(level.prolong));
-            smooth(level.sweeps);
+            smooth(level.sweeps, false);
         }
 
         template <class T> void mg_level(System& s, std::vector<MgLevel<T>>& levels, int index)
