@@ -91,6 +91,9 @@ def parse_args():
                     help="GCRO recycled pairs kept between solves: 1..3, -1 none (default), 0: the reference's 3")
     ap.add_argument("--block-iterations", type=int, default=0,
                     help="composite cycle: Chebyshev iterations of the brick block pre-smoother (0: Jacobi pre-sweeps)")
+    ap.add_argument("--initial-guess", choices=("previous", "extrapolated"), default="extrapolated",
+                    help="step projections start from the last pressure (the reference's warm start) or from "
+                         "2 p_n - p_(n-1) of the last two")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU sample of the ours arm")
     ap.add_argument("--no-reference-gpu", action="store_true", help="reference arm: skip the sm_100a reference run")
     ap.add_argument("--profile-region", type=int, default=0, help="PCFD_PROFILE_* region timed per launch")
@@ -493,6 +496,7 @@ def run_ours(args, ranks: Ranks):
     bricks = non_covered_bricks(grid.topology)
     system = make_system(args, grid, ranks.local)
     system.configure(speed=spec.speed, **spec.case)
+    system.set_initial_guess(1 if args.initial_guess == "extrapolated" else 0)
     tune = system.autotune(5) if not args.no_autotune else None
     slots = system.inflow_layout()
     faces = len(slots) * spec.brick_size ** 2
@@ -606,6 +610,8 @@ def run_ours(args, ranks: Ranks):
         "config": line_config(args, grid, n),
         "projection_ms": round(statistics.mean(s["projection_ms"] for s in stats), 3),
         "iterations_per_step": round(statistics.mean(s["pressure"]["iterations"] for s in stats), 2),
+        "initial_guess": {"previous": "last pressure (the reference's warm start)",
+                          "extrapolated": "2 p_n - p_(n-1) of the last two converged pressures"}[args.initial_guess],
         "final_residual_max": max(s["pressure"]["relative_residual"] for s in stats),
         "unconverged_steps": failed,
         "init_projection": {"iterations": init["pressure"]["iterations"], "ms": round(init["projection_ms"], 3)},

@@ -366,6 +366,13 @@ pcfd_status pcfd_projection_project(pcfd_system* system, double rho, double dt, 
  * events on the system stream) -- the same right-hand side and start for every preconditioner
  * being compared. */
 pcfd_status pcfd_projection_keep_start(pcfd_system* system, int32_t keep);
+
+/* No reference counterpart.  Initial guess of the step projections, which the reference
+ * warm-starts from the last pressure (mode 0, the default).  Mode 1 starts from the linear
+ * extrapolation 2 p_n - p_(n-1) of the last two converged step pressures (the plain warm start
+ * while fewer than two exist, after initialization, pcfd_set_pressure_host or a projection that
+ * did not converge).  The solve still ends at the same relative residual; only its start moves. */
+pcfd_status pcfd_core_set_initial_guess(pcfd_system* system, int32_t mode);
 pcfd_status pcfd_projection_resolve(pcfd_system* system, double tolerance, int32_t max_iterations, double* ms,
                                     pcfd_solve_result* result);
 

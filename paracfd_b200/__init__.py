@@ -150,6 +150,11 @@ class CompositeSystem:
                                                  max_iterations, int(x0 is not None), C.byref(res)))
         return x, res.as_dict()
 
+    def set_initial_guess(self, mode: int):
+        """Step projections start from the last pressure (0, the reference's warm start) or from
+        2 p_n - p_(n-1) of the last two converged pressures (1)."""
+        check(self._lib.pcfd_core_set_initial_guess(self.handle, int(mode)))
+
     def keep_projection_start(self, keep: bool = True):
         check(self._lib.pcfd_projection_keep_start(self.handle, int(keep)))
 

@@ -232,6 +232,7 @@ SIGNATURES = {
     "pcfd_builder_last_error": (C.c_char_p, []),
     "pcfd_set_preconditioner": (C.c_int, [C.c_void_p, C.c_int32]),
     "pcfd_projection_keep_start": (C.c_int, [C.c_void_p, C.c_int32]),
+    "pcfd_core_set_initial_guess": (C.c_int, [C.c_void_p, C.c_int32]),
     "pcfd_projection_resolve": (C.c_int, [C.c_void_p, C.c_double, C.c_int32, C.POINTER(C.c_double),
                                           C.POINTER(SolveResult)]),
     "pcfd_learned_parameter_count": (C.c_int, [C.POINTER(C.c_int64)]),

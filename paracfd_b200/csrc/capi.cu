@@ -510,6 +510,7 @@ pcfd_status pcfd_set_pressure_host(pcfd_system* system, const double* p)
         System& s = sys(system);
         require_finite(p, size_t(s.S), "pressure state");
         h2d(s, s.pressure.p, p, size_t(s.S));
+        s.previous_valid = false;
         launch_convert_pressure(s);
         sync(s);
     });
@@ -903,6 +904,17 @@ pcfd_status pcfd_preconditioner_fused(pcfd_system* system, int32_t* fused)
         System& s = sys(system);
         require(fused != nullptr, "null output");
         *fused = s.fine.enabled ? 1 : 0;
+    });
+}
+
+pcfd_status pcfd_core_set_initial_guess(pcfd_system* system, int32_t mode)
+{
+    return guarded([&] {
+        System& s = sys(system);
+        require(mode == 0 || mode == 1, "initial guess mode must be 0 or 1");
+        if (mode == 1 && !s.pressure_previous.p) s.pressure_previous.alloc(size_t(s.Sp));
+        s.initial_guess = mode;
+        s.previous_valid = false;
     });
 }
 

@@ -90,12 +90,37 @@ namespace pcfd
         return *s.momentum;
     }
 
+    // p <- 2 p - previous and previous <- p (the old p), elementwise
+    __global__ void extrapolate_pressure_kernel(double* __restrict__ p, double* __restrict__ previous, int64_t n)
+    {
+        const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+        if (q >= n) return;
+        const double a = p[q], b = previous[q];
+        previous[q] = a;
+        p[q] = 2.0 * a - b;
+    }
+
+    // the initial guess of a warm step projection (pcfd_core_set_initial_guess)
+    void initial_guess(System& s, bool warm)
+    {
+        if (!warm) { s.previous_valid = false; return; }
+        if (s.initial_guess != 1 || !s.pressure_previous.p) return;
+        if (s.previous_valid)
+            extrapolate_pressure_kernel<<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(s.pressure, s.pressure_previous, s.S);
+        else
+            cuda_check(cudaMemcpyAsync(s.pressure_previous, s.pressure, size_t(s.S) * sizeof(double), cudaMemcpyDeviceToDevice, s.stream),
+                       "keep pressure");
+        s.previous_valid = true;
+    }
+
     pcfd_solve_result project(System& s, double rho, double dt, double tolerance, int max_iterations, bool warm)
     {
         launch_integrated_flux(s);
         launch_normalize(s, rho / dt, true);
+        initial_guess(s, warm);
         if (s.keep_projection_start) save_projection_start(s, warm);
         const pcfd_solve_result r = solve(s, s.pressure, s.rhs, tolerance, max_iterations, warm);
+        if (!r.converged) s.previous_valid = false;
         if (r.converged)
         {
             launch_convert_pressure(s);

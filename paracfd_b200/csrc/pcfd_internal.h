@@ -301,6 +301,11 @@ namespace pcfd
         bool keep_projection_start = false, start_saved = false, start_warm = false;
         int start_recycle_count = 0;
         DBuf<double> start_pressure, start_recycle_u, start_recycle_c;
+        // initial guess of a warm projection: 0 = the last pressure (the reference's warm start),
+        // 1 = 2 p_n - p_(n-1) from the last two converged pressures (pressure_previous = p_n)
+        int initial_guess = 0;
+        DBuf<double> pressure_previous;
+        bool previous_valid = false;
 
         // preconditioner of the Krylov solvers (pcfd_preconditioner) and the learned network state
         int preconditioner = PCFD_PRECONDITIONER_MULTIGRID;
