@@ -91,7 +91,7 @@ def parse_args():
                     help="GCRO recycled pairs kept between solves: 1..3, -1 none (default), 0: the reference's 3")
     ap.add_argument("--block-iterations", type=int, default=0,
                     help="composite cycle: Chebyshev iterations of the brick block pre-smoother (0: Jacobi pre-sweeps)")
-    ap.add_argument("--initial-guess", choices=("previous", "extrapolated"), default="extrapolated",
+    ap.add_argument("--initial-guess", choices=("previous", "extrapolated", "quadratic"), default="extrapolated",
                     help="step projections start from the last pressure (the reference's warm start) or from "
                          "2 p_n - p_(n-1) of the last two")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU sample of the ours arm")
@@ -496,7 +496,7 @@ def run_ours(args, ranks: Ranks):
     bricks = non_covered_bricks(grid.topology)
     system = make_system(args, grid, ranks.local)
     system.configure(speed=spec.speed, **spec.case)
-    system.set_initial_guess(1 if args.initial_guess == "extrapolated" else 0)
+    system.set_initial_guess({"previous": 0, "extrapolated": 1, "quadratic": 2}[args.initial_guess])
     tune = system.autotune(5) if not args.no_autotune else None
     slots = system.inflow_layout()
     faces = len(slots) * spec.brick_size ** 2
@@ -611,7 +611,8 @@ def run_ours(args, ranks: Ranks):
         "projection_ms": round(statistics.mean(s["projection_ms"] for s in stats), 3),
         "iterations_per_step": round(statistics.mean(s["pressure"]["iterations"] for s in stats), 2),
         "initial_guess": {"previous": "last pressure (the reference's warm start)",
-                          "extrapolated": "2 p_n - p_(n-1) of the last two converged pressures"}[args.initial_guess],
+                          "extrapolated": "2 p_n - p_(n-1) of the last two converged pressures",
+                          "quadratic": "3 p_n - 3 p_(n-1) + p_(n-2) of the last three converged pressures"}[args.initial_guess],
         "final_residual_max": max(s["pressure"]["relative_residual"] for s in stats),
         "unconverged_steps": failed,
         "init_projection": {"iterations": init["pressure"]["iterations"], "ms": round(init["projection_ms"], 3)},

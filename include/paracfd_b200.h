@@ -369,9 +369,11 @@ pcfd_status pcfd_projection_keep_start(pcfd_system* system, int32_t keep);
 
 /* No reference counterpart.  Initial guess of the step projections, which the reference
  * warm-starts from the last pressure (mode 0, the default).  Mode 1 starts from the linear
- * extrapolation 2 p_n - p_(n-1) of the last two converged step pressures (the plain warm start
- * while fewer than two exist, after initialization, pcfd_set_pressure_host or a projection that
- * did not converge).  The solve still ends at the same relative residual; only its start moves. */
+ * extrapolation 2 p_n - p_(n-1) of the last two converged step pressures, mode 2 from the
+ * quadratic 3 p_n - 3 p_(n-1) + p_(n-2) of the last three; with fewer converged pressures
+ * (after initialization, pcfd_set_pressure_host or a projection that did not converge) the
+ * highest order they allow.  The solve still ends at the same relative residual; only its start
+ * moves. */
 pcfd_status pcfd_core_set_initial_guess(pcfd_system* system, int32_t mode);
 pcfd_status pcfd_projection_resolve(pcfd_system* system, double tolerance, int32_t max_iterations, double* ms,
                                     pcfd_solve_result* result);

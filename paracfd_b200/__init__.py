@@ -151,8 +151,9 @@ class CompositeSystem:
         return x, res.as_dict()
 
     def set_initial_guess(self, mode: int):
-        """Step projections start from the last pressure (0, the reference's warm start) or from
-        2 p_n - p_(n-1) of the last two converged pressures (1)."""
+        """Step projections start from the last pressure (0, the reference's warm start), from
+        2 p_n - p_(n-1) of the last two converged pressures (1) or from 3 p_n - 3 p_(n-1) + p_(n-2)
+        of the last three (2)."""
         check(self._lib.pcfd_core_set_initial_guess(self.handle, int(mode)))
 
     def keep_projection_start(self, keep: bool = True):

@@ -510,7 +510,7 @@ pcfd_status pcfd_set_pressure_host(pcfd_system* system, const double* p)
         System& s = sys(system);
         require_finite(p, size_t(s.S), "pressure state");
         h2d(s, s.pressure.p, p, size_t(s.S));
-        s.previous_valid = false;
+        s.previous_count = 0;
         launch_convert_pressure(s);
         sync(s);
     });
@@ -911,10 +911,11 @@ pcfd_status pcfd_core_set_initial_guess(pcfd_system* system, int32_t mode)
 {
     return guarded([&] {
         System& s = sys(system);
-        require(mode == 0 || mode == 1, "initial guess mode must be 0 or 1");
-        if (mode == 1 && !s.pressure_previous.p) s.pressure_previous.alloc(size_t(s.Sp));
+        require(mode >= 0 && mode <= 2, "initial guess mode must be 0, 1 or 2");
+        if (mode >= 1 && !s.pressure_previous.p) s.pressure_previous.alloc(size_t(s.Sp));
+        if (mode == 2 && !s.pressure_previous2.p) s.pressure_previous2.alloc(size_t(s.Sp));
         s.initial_guess = mode;
-        s.previous_valid = false;
+        s.previous_count = 0;
     });
 }
 

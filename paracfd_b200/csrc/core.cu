@@ -90,27 +90,43 @@ namespace pcfd
         return *s.momentum;
     }
 
-    // p <- 2 p - previous and previous <- p (the old p), elementwise
-    __global__ void extrapolate_pressure_kernel(double* __restrict__ p, double* __restrict__ previous, int64_t n)
+    // Extrapolation in time from the last converged pressures, elementwise: with order 1,
+    // p <- 2 p - previous; with order 2, p <- 3 p - 3 previous + previous2 and previous2 <- previous;
+    // then previous <- p (the old p).  previous2 may be null for order 1.
+    __global__ void extrapolate_pressure_kernel(double* __restrict__ p, double* __restrict__ previous, double* __restrict__ previous2,
+                                                int64_t n, int order)
     {
         const int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
         if (q >= n) return;
         const double a = p[q], b = previous[q];
+        if (order == 2)
+        {
+            const double c = previous2[q];
+            previous2[q] = b;
+            p[q] = 3.0 * (a - b) + c;
+        }
+        else
+        {
+            if (previous2) previous2[q] = b;
+            p[q] = 2.0 * a - b;
+        }
         previous[q] = a;
-        p[q] = 2.0 * a - b;
     }
 
-    // the initial guess of a warm step projection (pcfd_core_set_initial_guess)
+    // the initial guess of a warm step projection (pcfd_core_set_initial_guess): the highest
+    // extrapolation order the valid history allows, up to the chosen one
     void initial_guess(System& s, bool warm)
     {
-        if (!warm) { s.previous_valid = false; return; }
-        if (s.initial_guess != 1 || !s.pressure_previous.p) return;
-        if (s.previous_valid)
-            extrapolate_pressure_kernel<<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(s.pressure, s.pressure_previous, s.S);
-        else
+        if (!warm) { s.previous_count = 0; return; }
+        if (s.initial_guess == 0 || !s.pressure_previous.p) return;
+        const int order = std::min(s.initial_guess, s.previous_count);
+        if (order == 0)
             cuda_check(cudaMemcpyAsync(s.pressure_previous, s.pressure, size_t(s.S) * sizeof(double), cudaMemcpyDeviceToDevice, s.stream),
                        "keep pressure");
-        s.previous_valid = true;
+        else
+            extrapolate_pressure_kernel<<<blocks_for(s.S), kThreads, 0, launch_stream(s)>>>(s.pressure, s.pressure_previous,
+                                                                                           s.pressure_previous2.p, s.S, order);
+        s.previous_count = std::min(s.previous_count + 1, s.initial_guess);
     }
 
     pcfd_solve_result project(System& s, double rho, double dt, double tolerance, int max_iterations, bool warm)
@@ -120,7 +136,7 @@ namespace pcfd
         initial_guess(s, warm);
         if (s.keep_projection_start) save_projection_start(s, warm);
         const pcfd_solve_result r = solve(s, s.pressure, s.rhs, tolerance, max_iterations, warm);
-        if (!r.converged) s.previous_valid = false;
+        if (!r.converged) s.previous_count = 0;
         if (r.converged)
         {
             launch_convert_pressure(s);

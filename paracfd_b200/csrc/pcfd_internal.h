@@ -302,10 +302,11 @@ namespace pcfd
         int start_recycle_count = 0;
         DBuf<double> start_pressure, start_recycle_u, start_recycle_c;
         // initial guess of a warm projection: 0 = the last pressure (the reference's warm start),
-        // 1 = 2 p_n - p_(n-1) from the last two converged pressures (pressure_previous = p_n)
+        // 1 = 2 p_n - p_(n-1), 2 = 3 p_n - 3 p_(n-1) + p_(n-2) from the last converged pressures
+        // (pressure_previous holds p_(n-1), pressure_previous2 p_(n-2); previous_count of them valid)
         int initial_guess = 0;
-        DBuf<double> pressure_previous;
-        bool previous_valid = false;
+        DBuf<double> pressure_previous, pressure_previous2;
+        int previous_count = 0;
 
         // preconditioner of the Krylov solvers (pcfd_preconditioner) and the learned network state
         int preconditioner = PCFD_PRECONDITIONER_MULTIGRID;
