@@ -254,97 +254,93 @@ namespace pcfd
         // Pass 1 for Q = [C | V_0..V_{j-1}] (final), v = V_j (projected once) and w = A z_j:
         // s = Q^T v, t = Q^T w, v.v, v.w, w.w -> partial[block][2 * kMaxSet + 3].
         constexpr int kDcgsStride = 2 * kMaxSet + 4;
-        // Pairs a thread loads before it sums: with few basis vectors (V <= 2) one pair leaves too
-        // few bytes in flight per SM to cover the load latency, so two pairs of every vector are
-        // loaded up front; with V >= 4 the V loads of one pair already do.
-        // The update kernel holds twice the values per pair (v and next); at V = 2 two pairs
-        // exceed its 64 registers, so it groups only at V = 1.
+        // Warp w of a CTA takes basis vectors [V w, V w + V), V = ceil(m / 8), and its 32 lanes walk
+        // consecutive element pairs, so every load of a warp reads 512 contiguous bytes of one
+        // vector.  Every warp reads v and w as well (mostly from L1); warp 0 also sums v.v, v.w and
+        // w.w.  A lane loads kGroup sub-blocks of pairs before it sums, to keep enough bytes in
+        // flight with few vectors per warp.  Each sum is per lane over the CTA's items, then a warp
+        // reduction; partial[block][j] holds the owning warp's sum.
         template <int V>
         __host__ __device__ constexpr int dcgs_group() { return V <= 2 ? 2 : 1; }
         template <int V>
-        __host__ __device__ constexpr int dcgs_update_group() { return V == 1 ? 2 : 1; }
-        template <int V>
-        __global__ void __launch_bounds__(kThreadsBlock, V >= 8 ? 2 : (V >= 4 ? 3 : 4)) dcgs_dot_kernel(VecSet Q, const double* __restrict__ vv,
+        __global__ void __launch_bounds__(kThreadsBlock) dcgs_dot_kernel(VecSet Q, const double* __restrict__ vv,
             const double* __restrict__ w, const uint8_t* __restrict__ active, Sweep range, double* __restrict__ partial)
         {
-            __shared__ double shared[kThreadsBlock / 32][kDcgsStride];
+            __shared__ double shared[kDcgsStride];
             double as[V], at[V], vv2 = 0.0, vw = 0.0, ww = 0.0;
 #pragma unroll
             for (int u = 0; u < V; ++u) { as[u] = 0.0; at[u] = 0.0; }
             const int count = Q.size();
-            const int lane = threadIdx.x & 31, quarter = lane >> 3, warp = threadIdx.x >> 5;
-            const int seg_pair = (warp * kPairsPerWarp) + (lane & 7);
+            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+            const int first = V * warp;
+            const bool norms = warp == 0;
             constexpr int kGroup = dcgs_group<V>();
-            for (int64_t item = blockIdx.x; item < range.items; item += gridDim.x)
-            {
-                const int64_t base = range.base(item);
-#pragma unroll 1
-                for (int sub0 = 0; sub0 < 256 / kPairsPerPass; sub0 += kGroup)
+            constexpr int kSubBlocks = 512 / 64;       // an item is 512 entries = 8 sub-blocks of 32 pairs
+            if (first < count || norms)
+                for (int64_t item = blockIdx.x; item < range.items; item += gridDim.x)
                 {
-                    // all loads of the group first, then the sums in the same order as one pair at a time
-                    uchar2 a[kGroup];
-                    double2 v0[kGroup], w0[kGroup], b[kGroup][V];
-#pragma unroll
-                    for (int g = 0; g < kGroup; ++g)
+                    const int64_t base = range.base(item);
+#pragma unroll 1
+                    for (int sub0 = 0; sub0 < kSubBlocks; sub0 += kGroup)
                     {
-                        const int64_t e = base + 2 * (seg_pair + kPairsPerPass * (sub0 + g));
-                        const bool valid = e < range.padded;
-                        const int64_t q = valid ? e >> 1 : 0;
-                        a[g] = valid ? reinterpret_cast<const uchar2*>(active)[q] : make_uchar2(0, 0);
-                        v0[g] = valid ? reinterpret_cast<const double2*>(vv)[q] : make_double2(0.0, 0.0);
-                        w0[g] = valid ? reinterpret_cast<const double2*>(w)[q] : make_double2(0.0, 0.0);
+                        uchar2 a[kGroup];
+                        double2 v0[kGroup], w0[kGroup], b[kGroup][V];
 #pragma unroll
-                        for (int u = 0; u < V; ++u)
+                        for (int g = 0; g < kGroup; ++g)
                         {
-                            const int j = V * quarter + u;
-                            b[g][u] = valid && j < count ? reinterpret_cast<const double2*>(Q.vec(j))[q] : make_double2(0.0, 0.0);
+                            const int64_t e = base + 2 * (32 * (sub0 + g) + lane);
+                            const bool valid = e < range.padded;
+                            const int64_t q = valid ? e >> 1 : 0;
+                            a[g] = valid ? reinterpret_cast<const uchar2*>(active)[q] : make_uchar2(0, 0);
+                            v0[g] = valid ? reinterpret_cast<const double2*>(vv)[q] : make_double2(0.0, 0.0);
+                            w0[g] = valid ? reinterpret_cast<const double2*>(w)[q] : make_double2(0.0, 0.0);
+#pragma unroll
+                            for (int u = 0; u < V; ++u)
+                                b[g][u] = valid && first + u < count ? reinterpret_cast<const double2*>(Q.vec(first + u))[q]
+                                                                     : make_double2(0.0, 0.0);
                         }
-                    }
 #pragma unroll
-                    for (int g = 0; g < kGroup; ++g)
-                    {
+                        for (int g = 0; g < kGroup; ++g)
+                        {
 #pragma unroll
-                        for (int u = 0; u < V; ++u)
-                        {
-                            as[u] += (a[g].x ? b[g][u].x * v0[g].x : 0.0) + (a[g].y ? b[g][u].y * v0[g].y : 0.0);
-                            at[u] += (a[g].x ? b[g][u].x * w0[g].x : 0.0) + (a[g].y ? b[g][u].y * w0[g].y : 0.0);
-                        }
-                        if (quarter == 0)
-                        {
-                            vv2 += (a[g].x ? v0[g].x * v0[g].x : 0.0) + (a[g].y ? v0[g].y * v0[g].y : 0.0);
-                            vw += (a[g].x ? v0[g].x * w0[g].x : 0.0) + (a[g].y ? v0[g].y * w0[g].y : 0.0);
-                            ww += (a[g].x ? w0[g].x * w0[g].x : 0.0) + (a[g].y ? w0[g].y * w0[g].y : 0.0);
+                            for (int u = 0; u < V; ++u)
+                            {
+                                as[u] += (a[g].x ? b[g][u].x * v0[g].x : 0.0) + (a[g].y ? b[g][u].y * v0[g].y : 0.0);
+                                at[u] += (a[g].x ? b[g][u].x * w0[g].x : 0.0) + (a[g].y ? b[g][u].y * w0[g].y : 0.0);
+                            }
+                            if (norms)
+                            {
+                                vv2 += (a[g].x ? v0[g].x * v0[g].x : 0.0) + (a[g].y ? v0[g].y * v0[g].y : 0.0);
+                                vw += (a[g].x ? v0[g].x * w0[g].x : 0.0) + (a[g].y ? v0[g].y * w0[g].y : 0.0);
+                                ww += (a[g].x ? w0[g].x * w0[g].x : 0.0) + (a[g].y ? w0[g].y * w0[g].y : 0.0);
+                            }
                         }
                     }
                 }
-            }
+            for (int j = threadIdx.x; j < kDcgsStride; j += blockDim.x) shared[j] = 0.0;
+            __syncthreads();
 #pragma unroll
             for (int u = 0; u < V; ++u)
             {
-                const double x = segment_sum(as[u]), y = segment_sum(at[u]);
-                if ((lane & 7) == 0)
+                const double x = warp_sum(as[u]), y = warp_sum(at[u]);
+                if (lane == 0 && first + u < count)
                 {
-                    shared[warp][V * quarter + u] = x;
-                    shared[warp][kMaxSet + V * quarter + u] = y;
+                    shared[first + u] = x;
+                    shared[kMaxSet + first + u] = y;
                 }
             }
-            const double a1 = segment_sum(vv2), a2 = segment_sum(vw), a3 = segment_sum(ww);
-            if (lane == 0)
+            if (norms)
             {
-                shared[warp][2 * kMaxSet] = a1;
-                shared[warp][2 * kMaxSet + 1] = a2;
-                shared[warp][2 * kMaxSet + 2] = a3;
+                const double a1 = warp_sum(vv2), a2 = warp_sum(vw), a3 = warp_sum(ww);
+                if (lane == 0)
+                {
+                    shared[2 * kMaxSet] = a1;
+                    shared[2 * kMaxSet + 1] = a2;
+                    shared[2 * kMaxSet + 2] = a3;
+                }
             }
             __syncthreads();
-            for (int j = threadIdx.x; j < kDcgsStride - 1; j += blockDim.x)
-            {
-                const bool used = j < count || (j >= kMaxSet && j < kMaxSet + count) || j >= 2 * kMaxSet;
-                double v = 0.0;
-                if (used)
-#pragma unroll
-                    for (int wp = 0; wp < kThreadsBlock / 32; ++wp) v += shared[wp][j];
-                partial[int64_t(blockIdx.x) * kDcgsStride + j] = v;
-            }
+            for (int j = threadIdx.x; j < kDcgsStride - 1; j += blockDim.x) partial[int64_t(blockIdx.x) * kDcgsStride + j] = shared[j];
         }
 
         // Sums the pass-1 partials (fixed order) and forms the update coefficients:
@@ -412,8 +408,12 @@ namespace pcfd
         }
 
         // Pass 2: v <- v / r - Q (s / r) in place, next = (w - (c / r) v_old - Q (t - (c / r) s)) / rho.
-        template <int V>
-        __global__ void __launch_bounds__(kThreadsBlock, V >= 8 ? 2 : 4) dcgs_update_kernel(VecSet Q, const double* __restrict__ coefficient,
+        // One element pair per thread; the thread walks the basis vectors in order (j = 0, 1, ...)
+        // in chunks of eight loads in flight, so each warp reads 512 contiguous bytes of every
+        // vector and no sum crosses lanes.  (The dot pass keeps split lanes: its 2m + 3 running
+        // sums per element would not fit one thread's registers.)
+        constexpr int kUpdateChunk = 8;
+        __global__ void __launch_bounds__(kThreadsBlock) dcgs_update_kernel(VecSet Q, const double* __restrict__ coefficient,
             double* __restrict__ vv, const double* __restrict__ w, double* __restrict__ next, const uint8_t* __restrict__ active, Sweep range)
         {
             __shared__ double cv[kMaxSet], cw[kMaxSet];
@@ -425,58 +425,34 @@ namespace pcfd
             __syncthreads();
             const double inv_r = coefficient[4 * kMaxSet + 6], c_r = coefficient[4 * kMaxSet + 7], inv_rho = coefficient[4 * kMaxSet + 8];
             const int count = Q.size();
-            const int lane = threadIdx.x & 31, quarter = lane >> 3;
-            const int seg_pair = ((threadIdx.x >> 5) * kPairsPerWarp) + (lane & 7);
-            constexpr int kGroup = dcgs_update_group<V>();
             for (int64_t item = blockIdx.x; item < range.items; item += gridDim.x)
             {
-                const int64_t base = range.base(item);
-#pragma unroll 1
-                for (int sub0 = 0; sub0 < 256 / kPairsPerPass; sub0 += kGroup)
+                const int64_t e = range.base(item) + 2 * threadIdx.x;
+                if (e >= range.padded) continue;
+                const int64_t q = e >> 1;
+                double vx = 0.0, vy = 0.0, wx = 0.0, wy = 0.0;
+                for (int j0 = 0; j0 < count; j0 += kUpdateChunk)
                 {
-                    // loads of the whole group before the first store (v is updated in place)
-                    int64_t q[kGroup];
-                    bool valid[kGroup];
-                    uchar2 a[kGroup];
-                    double2 v0[kGroup], w0[kGroup], b[kGroup][V];
+                    double2 b[kUpdateChunk];
 #pragma unroll
-                    for (int g = 0; g < kGroup; ++g)
+                    for (int u = 0; u < kUpdateChunk; ++u)
+                        b[u] = j0 + u < count ? reinterpret_cast<const double2*>(Q.vec(j0 + u))[q] : make_double2(0.0, 0.0);
+#pragma unroll
+                    for (int u = 0; u < kUpdateChunk; ++u)
                     {
-                        const int64_t e = base + 2 * (seg_pair + kPairsPerPass * (sub0 + g));
-                        valid[g] = e < range.padded;
-                        q[g] = valid[g] ? e >> 1 : 0;
-                        a[g] = valid[g] ? reinterpret_cast<const uchar2*>(active)[q[g]] : make_uchar2(0, 0);
-                        v0[g] = valid[g] ? reinterpret_cast<const double2*>(vv)[q[g]] : make_double2(0.0, 0.0);
-                        w0[g] = valid[g] ? reinterpret_cast<const double2*>(w)[q[g]] : make_double2(0.0, 0.0);
-#pragma unroll
-                        for (int u = 0; u < V; ++u)
-                        {
-                            const int j = V * quarter + u;
-                            b[g][u] = valid[g] && j < count ? reinterpret_cast<const double2*>(Q.vec(j))[q[g]] : make_double2(0.0, 0.0);
-                        }
-                    }
-#pragma unroll
-                    for (int g = 0; g < kGroup; ++g)
-                    {
-                        double vx = 0.0, vy = 0.0, wx = 0.0, wy = 0.0;
-#pragma unroll
-                        for (int u = 0; u < V; ++u)
-                        {
-                            const int j = V * quarter + u;
-                            vx += cv[j] * b[g][u].x; vy += cv[j] * b[g][u].y;
-                            wx += cw[j] * b[g][u].x; wy += cw[j] * b[g][u].y;
-                        }
-                        const double svx = quarter_total(vx), svy = quarter_total(vy), swx = quarter_total(wx), swy = quarter_total(wy);
-                        if (quarter == 0 && valid[g])
-                        {
-                            const double2 vn = make_double2(a[g].x ? inv_r * v0[g].x - svx : 0.0, a[g].y ? inv_r * v0[g].y - svy : 0.0);
-                            const double2 nx = make_double2(a[g].x ? inv_rho * (w0[g].x - c_r * v0[g].x - swx) : 0.0,
-                                                            a[g].y ? inv_rho * (w0[g].y - c_r * v0[g].y - swy) : 0.0);
-                            reinterpret_cast<double2*>(vv)[q[g]] = vn;
-                            reinterpret_cast<double2*>(next)[q[g]] = nx;
-                        }
+                        if (j0 + u >= count) break;
+                        const double sv = cv[j0 + u], sw = cw[j0 + u];
+                        vx += sv * b[u].x; vy += sv * b[u].y;
+                        wx += sw * b[u].x; wy += sw * b[u].y;
                     }
                 }
+                const uchar2 a = reinterpret_cast<const uchar2*>(active)[q];
+                const double2 v0 = reinterpret_cast<const double2*>(vv)[q], w0 = reinterpret_cast<const double2*>(w)[q];
+                const double2 vn = make_double2(a.x ? inv_r * v0.x - vx : 0.0, a.y ? inv_r * v0.y - vy : 0.0);
+                const double2 nx = make_double2(a.x ? inv_rho * (w0.x - c_r * v0.x - wx) : 0.0,
+                                                a.y ? inv_rho * (w0.y - c_r * v0.y - wy) : 0.0);
+                reinterpret_cast<double2*>(vv)[q] = vn;
+                reinterpret_cast<double2*>(next)[q] = nx;
             }
         }
 
@@ -548,8 +524,8 @@ namespace pcfd
         modes(block_kernel<1, 0>, block_kernel<2, 0>, block_kernel<4, 0>, block_kernel<8, 0>);
         modes(block_kernel<1, 1>, block_kernel<2, 1>, block_kernel<4, 1>, block_kernel<8, 1>);
         modes(block_kernel<1, 2>, block_kernel<2, 2>, block_kernel<4, 2>, block_kernel<8, 2>);
-        modes(dcgs_dot_kernel<1>, dcgs_dot_kernel<2>, dcgs_dot_kernel<4>, dcgs_dot_kernel<8>);
-        modes(dcgs_update_kernel<1>, dcgs_update_kernel<2>, dcgs_update_kernel<4>, dcgs_update_kernel<8>);
+        modes(dcgs_dot_kernel<1>, dcgs_dot_kernel<2>, dcgs_dot_kernel<3>, dcgs_dot_kernel<4>);
+        block_grid(dcgs_update_kernel);
     }
 
     void block_dot(System& s, const VecSet& Q, const double* w, double* out)
@@ -589,19 +565,15 @@ namespace pcfd
             grid = block_grid(kernel);
             kernel<<<grid, kThreadsBlock, 0, launch_stream(s)>>>(Q, v, w, s.active, range, s.dcgs_partial);
         };
-        if (m <= 4) dot(dcgs_dot_kernel<1>);
-        else if (m <= 8) dot(dcgs_dot_kernel<2>);
-        else if (m <= 16) dot(dcgs_dot_kernel<4>);
-        else dot(dcgs_dot_kernel<8>);
+        // V = ceil(m / 8) basis vectors per warp (kMaxSet = 32)
+        if (m <= 8) dot(dcgs_dot_kernel<1>);
+        else if (m <= 16) dot(dcgs_dot_kernel<2>);
+        else if (m <= 24) dot(dcgs_dot_kernel<3>);
+        else dot(dcgs_dot_kernel<4>);
         dcgs_final_kernel<<<2 * kMaxSet + 3, 256, 0, launch_stream(s)>>>(s.dcgs_partial, grid, m, s.dcgs_total, s.dcgs_ticket,
                                                                        coefficient);
-        auto update = [&](auto kernel) {
-            kernel<<<block_grid(kernel), kThreadsBlock, 0, launch_stream(s)>>>(Q, coefficient, v, w, next, s.active, range);
-        };
-        if (m <= 4) update(dcgs_update_kernel<1>);
-        else if (m <= 8) update(dcgs_update_kernel<2>);
-        else if (m <= 16) update(dcgs_update_kernel<4>);
-        else update(dcgs_update_kernel<8>);
+        dcgs_update_kernel<<<block_grid(dcgs_update_kernel), kThreadsBlock, 0, launch_stream(s)>>>(Q, coefficient, v, w, next, s.active,
+                                                                                                  range);
     }
 
     void block_combine(System& s, const VecSet& Z, const Coefficients& c, double* y, bool accumulate)
