@@ -602,6 +602,21 @@ def run_ours(args, ranks: Ranks):
                     "avg_launch_us": round(avg_ms * 1e3, 2),
                     "timing": "CUDA events around each launch over 3 whole steps after the timed region (stage chain "
                               "launched uncaptured)"}
+    # the Krylov orthogonalisation (a quarter of the step): one delayed-CGS2 column against 13 basis
+    # vectors on the resident system, its algorithmic bytes from the library
+    roofline_orthogonalisation = None
+    try:
+        column_ms = system.time_kernel(18, 10)
+        column_bytes = system.profile_bytes(3)
+        achieved = column_bytes / (column_ms * 1e-3) / 1e9
+        roofline_orthogonalisation = {
+            "bound": "hbm", "kernel": "delayed CGS2 column against 13 basis vectors (dcgs_dot_kernel, dcgs_final_kernel, "
+                                      "dcgs_update_kernel)",
+            "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "peak_kind": peak_kind, "algorithmic_bytes_per_launch": int(column_bytes), "avg_launch_us": round(column_ms * 1e3, 2),
+            "timing": "CUDA events over 10 back-to-back columns on resident vectors, after the timed region"}
+    except Exception:
+        pass
     line = {
         "metric": METRIC,
         "value": round(value, 4), "unit": "steps/s", "n_gpus": n, "steps": args.steps, "warmup": args.warmup,
@@ -624,6 +639,7 @@ def run_ours(args, ranks: Ranks):
         "component_ms": kernel_ms,
         "roofline": roofline,
         "roofline_operator": roofline_operator,
+        "roofline_orthogonalisation": roofline_orthogonalisation,
         "profiled_region": {"region": region_names.get(args.profile_region), "launches": int(len(per_launch)),
                             "avg_ms": region_ms},
         "cpu_baseline": None,

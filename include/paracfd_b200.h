@@ -530,15 +530,21 @@ pcfd_status pcfd_event_elapsed(pcfd_system* system, int32_t start_slot, int32_t 
 enum {
     PCFD_PROFILE_STRUCTURED_APPLY = 0,   /* brick-tiled FP64 7-point operator kernel */
     PCFD_PROFILE_PRECONDITIONER = 1,     /* one whole multigrid preconditioner application */
-    PCFD_PROFILE_STAGE_SMOOTH = 2        /* one smoothing step of the composite cycle's first stage
+    PCFD_PROFILE_STAGE_SMOOTH = 2,       /* one smoothing step of the composite cycle's first stage
                                             (its stage chain runs uncaptured while this is armed) */
+    PCFD_PROFILE_DCGS_COLUMN = 3         /* bytes only (pcfd_profile_begin refuses it): one delayed-CGS2
+                                            column against 13 basis vectors, the sequence that
+                                            pcfd_time_kernel 18 times */
 };
 /* Algorithmic bytes of one launch of a profiled region (each element read once and written once):
  * region 0 17 B per slot of a non-covered brick; region 2 per stage row its rhs, x, diagonal,
  * direction read and write and next iterate, then in CSR form the row offset and per stored
  * coupling its column index and coefficient, in brick-structured form the row's packed face
  * coefficients, per rest coupling its column index and coefficient and per 4^3 block its six
- * neighbour blocks.  0 for region 1. */
+ * neighbour blocks; region 3 per entry of the Krylov vectors' sweep (the non-covered bricks' slots
+ * and the fragments) 258 B: the dot pass reads the 13 basis vectors, v and w (8 B each) and the
+ * active flag, the update pass reads them again and writes v and the next vector.  0 for
+ * region 1. */
 pcfd_status pcfd_profile_bytes(pcfd_system* system, int32_t region, double* bytes_per_launch);
 /* 1 when the composite cycle's first stage runs in brick-structured form (64 rows per 8^3 brick,
  * face neighbours found from the row index), 0 when it runs as CSR or the cycle is not composite. */

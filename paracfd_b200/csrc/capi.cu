@@ -1082,12 +1082,13 @@ pcfd_status pcfd_profile_bytes(pcfd_system* system, int32_t region, double* byte
     return guarded([&] {
         System& s = sys(system);
         require(bytes_per_launch != nullptr, "null output");
-        require(region >= PCFD_PROFILE_STRUCTURED_APPLY && region <= PCFD_PROFILE_STAGE_SMOOTH, "unknown profile region");
+        require(region >= PCFD_PROFILE_STRUCTURED_APPLY && region <= PCFD_PROFILE_DCGS_COLUMN, "unknown profile region");
         if (region == PCFD_PROFILE_STRUCTURED_APPLY)
         {
             *bytes_per_launch = 17.0 * double(s.active_bricks) * double(s.bs3);   // active_bricks: the non-covered bricks
         }
         else if (region == PCFD_PROFILE_STAGE_SMOOTH) *bytes_per_launch = stage_smooth_bytes(s);
+        else if (region == PCFD_PROFILE_DCGS_COLUMN) *bytes_per_launch = 258.0 * double(krylov_sweep_entries(s));
         else *bytes_per_launch = 0.0;
     });
 }

@@ -515,6 +515,13 @@ namespace pcfd
         }
     }
 
+    int64_t krylov_sweep_entries(const System& s)
+    {
+        const Sweep range = sweep_range(s);
+        if (!range.bricks) return range.padded;
+        return range.brick_count * 512 + std::max<int64_t>(0, range.padded - range.structured);
+    }
+
     void prime_block_grids()
     {
         const auto modes = [](auto kernel1, auto kernel2, auto kernel4, auto kernel8) {

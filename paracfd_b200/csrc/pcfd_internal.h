@@ -410,6 +410,7 @@ namespace pcfd
     template <class T> void multigrid_levels(System& s, std::vector<MgLevel<T>>& levels);
     void build_composite(System& s, const pcfd_topology& t);
     void composite_levels(System& s);                 // V-cycle below the fine level, composite chain
+    int64_t krylov_sweep_entries(const System& s);    // vector entries the Krylov block kernels sweep
     void composite_preconditioner(System& s, const double* r, double* z);   // smoother.cu
     void learned_preconditioner(System& s, const double* r, double* z, bool coarse);   // smoother.cu
     pcfd_solve_result solve(System& s, double* x, const double* b, double tolerance, int max_iterations, bool warm);
