@@ -167,27 +167,53 @@ namespace pcfd
             }
         }
 
+        // Composite cycle: the two stage-1 correction values this thread's prolongation adds, staged
+        // with the tile by the thread itself (its own copy wait then covers them): [0] the row of
+        // its own two cells (they share a 2x2x2 block), [1] the row of its halo cells in the face
+        // neighbour (zero-filled without one).
+        template <class TC>
+        __device__ inline void issue_stage_values(const Ticket& k, const TC* __restrict__ e, TC* ebuf)
+        {
+            const int t = threadIdx.x;
+            const int c = 2 * t, i = c & 7, j = (c >> 3) & 7, kk = c >> 6;
+            copy_one<TC>(ebuf + 2 * t, e + int64_t(k.rank) * 64 + (i >> 1) + 4 * (j >> 1) + 16 * (kk >> 1), true);
+            const bool valid = k.nbr >= 0 && k.nrank >= 0;
+            int hi, hj, hk;
+            if (t < 128)
+            {
+                const int face = 2 + (t >> 5), w = t & 31;
+                if (face < 4) { hk = w >> 2; hi = (w & 3) * 2; hj = face == 2 ? kBS - 1 : 0; }
+                else { hi = (w * 2) & 7; hj = (w * 2) >> 3; hk = face == 4 ? kBS - 1 : 0; }
+            }
+            else
+            {
+                const int u = t - 128, face = u >> 6;
+                hj = u & 7; hk = (u >> 3) & 7; hi = face == 0 ? kBS - 1 : 0;
+            }
+            copy_one<TC>(ebuf + 2 * t + 1, e + int64_t(valid ? k.nrank : k.rank) * 64 + (hi >> 1) + 4 * (hj >> 1) + 16 * (hk >> 1), valid);
+        }
+
         // adds the coarse correction to the tile entries this thread copied; kMapped: the composite
         // cycle's stage-1 row of the cell (its brick's rank * 64 + the 2x2x2 block of the cell;
-        // an inactive cell's tile entry takes a correction too, but no open face reads it), else
-        // the geometric level-0 cell
+        // an inactive cell's tile entry takes a correction too, but no open face reads it), read
+        // from the values this thread staged (ebuf), else the geometric level-0 cell
         template <class T, class TC, bool kMapped>
-        __device__ inline void prolong_own(const Ticket& k, const TC* __restrict__ e, double scale, T* tile)
+        __device__ inline void prolong_own(const Ticket& k, const TC* __restrict__ e, double scale, T* tile, const TC* ebuf)
         {
             const int t = threadIdx.x, l = k.level;
             auto add = [&](int s_tile, int64_t q, int b0, int i, int j, int kk) {
-                if (kMapped) tile[s_tile] += T(scale * double(e[b0 * 64 + (i >> 1) + 4 * (j >> 1) + 16 * (kk >> 1)]));
+                if (kMapped) tile[s_tile] += T(scale * double(ebuf[2 * t + b0]));
                 else tile[s_tile] += T(scale * double(e[base_cell_of(b0, l, i, j, kk)]));
             };
             {
                 const int c = 2 * t, i = c & 7, j = (c >> 3) & 7, kk = c >> 6;
                 const int64_t q = int64_t(k.slot) * kC3 + c;
-                const int own = kMapped ? k.rank : k.base;
+                const int own = kMapped ? 0 : k.base;
                 add(tix(i, j, kk), q, own, i, j, kk);
                 add(tix(i + 1, j, kk), q + 1, own, i + 1, j, kk);
             }
             if (k.nbr < 0 || (kMapped && k.nrank < 0)) return;
-            const int other = kMapped ? k.nrank : k.nbase;
+            const int other = kMapped ? 1 : k.nbase;
             const int64_t nb = int64_t(k.nbr) * kC3;
             if (t < 128)
             {
@@ -296,11 +322,13 @@ namespace pcfd
             __shared__ __align__(16) T rbuf[kWithR ? 2 : 1][kRSize];
             __shared__ __align__(16) uint8_t cbuf[2][kCSize];
             __shared__ double residual[kMode == 1 ? kC3 : 1];
+            __shared__ __align__(16) TC ebuf[kProlong == 2 ? 2 : 1][kProlong == 2 ? 512 : 1];   // per thread: own, halo
             int64_t b = blockIdx.x;
             if (b >= bricks) return;
             const int64_t G = gridDim.x;
             Ticket cur = load_ticket(v, b);
             issue_brick<T, kWithR>(cur, z, r, v.code, tile[0], rbuf[0], cbuf[0]);
+            if (kProlong == 2) issue_stage_values<TC>(cur, e, ebuf[0]);
             copy_commit();
             Ticket next = b + G < bricks ? load_ticket(v, b + G) : cur;
             for (int it = 0;; ++it)
@@ -311,12 +339,13 @@ namespace pcfd
                 if (has_next)
                 {
                     issue_brick<T, kWithR>(next, z, r, v.code, tile[st ^ 1], rbuf[kWithR ? (st ^ 1) : 0], cbuf[st ^ 1]);
+                    if (kProlong == 2) issue_stage_values<TC>(next, e, ebuf[st ^ 1]);
                     copy_commit();
                     if (b + 2 * G < bricks) after = load_ticket(v, b + 2 * G);
                     copy_wait<1>();
                 }
                 else copy_wait<0>();
-                if (kProlong) prolong_own<T, TC, kProlong == 2>(cur, e, v.prolong, tile[st]);
+                if (kProlong) prolong_own<T, TC, kProlong == 2>(cur, e, v.prolong, tile[st], ebuf[kProlong == 2 ? st : 0]);
                 __syncthreads();
                 // ---- compute brick `cur` from buffer st.  Thread t owns cell (i, j, k) = (t & 7,
                 // t >> 5, (t >> 3 & 3) + 4 q), q = 0, 1: a warp covers one x-row of 8 cells in each
