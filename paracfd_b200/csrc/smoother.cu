@@ -905,7 +905,6 @@ namespace pcfd
         DeferredView deferred_view(System& s, double omega)
         {
             FineSmoother& f = s.fine;
-            const IrregularOperator& o = s.irr;
             return DeferredView{f.deferred_row, f.deferred_edge, f.deferred_edge_coefficient, f.gauge_offset, f.gauge_coefficient,
                                 s.diagonal, s.aggregate, s.base_offset, s.base_cells, omega};
         }
