@@ -47,7 +47,7 @@ namespace pcfd
             }
         };
 
-        // ---- split-lane block kernels ----------------------------------------------------------
+        // ---- split-lane block kernels (CGS2, three passes) ------------------------------------------
         // Four lanes share one element pair (16 bytes of every vector): lane l handles pair
         // (l & 7) of an 8-pair warp segment and vectors [V * (l >> 3), V * (l >> 3) + V), V = 1, 2,
         // 4 or 8 for up to 4, 8, 16 or 32 vectors.  Each basis entry is loaded exactly once and a
@@ -410,8 +410,8 @@ namespace pcfd
         // Pass 2: v <- v / r - Q (s / r) in place, next = (w - (c / r) v_old - Q (t - (c / r) s)) / rho.
         // One element pair per thread; the thread walks the basis vectors in order (j = 0, 1, ...)
         // in chunks of eight loads in flight, so each warp reads 512 contiguous bytes of every
-        // vector and no sum crosses lanes.  (The dot pass keeps split lanes: its 2m + 3 running
-        // sums per element would not fit one thread's registers.)
+        // vector and no sum crosses lanes.  (The dot pass cannot do the same: 2m + 3 running sums
+        // per thread would not fit its registers, so it splits the vectors across warps instead.)
         constexpr int kUpdateChunk = 8;
         __global__ void __launch_bounds__(kThreadsBlock) dcgs_update_kernel(VecSet Q, const double* __restrict__ coefficient,
             double* __restrict__ vv, const double* __restrict__ w, double* __restrict__ next, const uint8_t* __restrict__ active, Sweep range)
